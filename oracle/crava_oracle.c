@@ -1,0 +1,824 @@
+/*
+ * crava_oracle.c -- plain-C restatement of the reference's Fourier-domain
+ * AVO inversion hot path.  TEST INFRASTRUCTURE ONLY (see crava_oracle.h):
+ * the product never links or calls it.
+ *
+ * Each function names the reference file:line it restates.  The FP32 solve
+ * keeps the reference's float operation order (lib_matr.c) so that, built
+ * with -ffp-contract=off, it reproduces the reference harness bit for bit
+ * on identical Fourier-domain inputs.  The FFT is an independent
+ * double-precision mixed-radix DFT rounded to float, so FFT outputs agree
+ * with FFTW 2.1.2 (single precision) to float rounding, not bit for bit.
+ */
+#include "crava_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_TOL 1e-20 /* libs/lib/lib_matr.c:20 */
+#define ORC_MAXT 16
+
+typedef struct { float re, im; } cf;
+typedef struct { double re, im; } cd;
+
+/* ------------------------------------------------------------------ */
+/* 1-D complex DFT, double precision, recursive mixed radix.           */
+/* sign = -1 forward (FFTW_FORWARD), +1 backward; unnormalised.        */
+/* ------------------------------------------------------------------ */
+static int smallest_factor(int n) {
+  for (int p = 2; p * p <= n; ++p)
+    if (n % p == 0) return p;
+  return n;
+}
+
+static void dft_rec(const cd *in, int istride, cd *out, int n, int sign,
+                    cd *tmp) {
+  if (n == 1) { out[0] = in[0]; return; }
+  int p = smallest_factor(n), m = n / p;
+  for (int r = 0; r < p; ++r)
+    dft_rec(in + (long)r * istride, istride * p, out + (long)r * m, m, sign, tmp);
+  /* combine: X[k + m q] = sum_r W_n^{r (k + m q)} sub_r[k] */
+  for (int k = 0; k < m; ++k) {
+    for (int q = 0; q < p; ++q) {
+      int kk = k + m * q;
+      double sr = 0.0, si = 0.0;
+      for (int r = 0; r < p; ++r) {
+        long e = ((long)r * kk) % n;
+        double ang = sign * 2.0 * M_PI * (double)e / (double)n;
+        double c = cos(ang), s = sin(ang);
+        cd v = out[(long)r * m + k];
+        sr += v.re * c - v.im * s;
+        si += v.re * s + v.im * c;
+      }
+      tmp[kk].re = sr; tmp[kk].im = si;
+    }
+  }
+  memcpy(out, tmp, sizeof(cd) * n);
+}
+
+static void dft1d(cd *x, int n, int sign) {
+  cd *in = (cd *)malloc(sizeof(cd) * n), *tmp = (cd *)malloc(sizeof(cd) * n);
+  memcpy(in, x, sizeof(cd) * n);
+  dft_rec(in, 1, x, n, sign, tmp);
+  free(in); free(tmp);
+}
+
+/* ------------------------------------------------------------------ */
+/* 3-D in-place R2C / C2R with FFTGrid scaling.                         */
+/* fftInPlace: src/fftgrid.cpp:1803-1829; invFFTInPlace: :1831-1862;    */
+/* transform: rfftw3d_create_plan(nzp,nyp,nxp) + rfftwnd_one_*          */
+/* (libs/fft/rfftw/rfftwnd.c:180,558,564): real-to-half-complex along   */
+/* x, complex along y and z, forward sign -, unnormalised.              */
+/* ------------------------------------------------------------------ */
+static void scale_real(float *g, long rsize, float s) {
+  for (long i = 0; i < rsize; ++i) g[i] *= s; /* multiplyByScalar :1992 */
+}
+
+int orc_fft_r2c(float *grid, int nxp, int nyp, int nzp, int type) {
+  int cnxp = nxp / 2 + 1, rnxp = 2 * cnxp;
+  long rsize = (long)rnxp * nyp * nzp;
+  if (type != ORC_COVARIANCE)
+    scale_real(grid, rsize, 1.0f / sqrtf((float)(nxp * nyp * nzp)));
+  int nmax = nxp > nyp ? nxp : nyp; if (nzp > nmax) nmax = nzp;
+  cd *line = (cd *)malloc(sizeof(cd) * nmax);
+  cf *c = (cf *)grid;
+  /* x: real -> half complex, per (y,z) row */
+  for (long row = 0; row < (long)nyp * nzp; ++row) {
+    float *r = grid + row * rnxp;
+    for (int i = 0; i < nxp; ++i) { line[i].re = r[i]; line[i].im = 0.0; }
+    dft1d(line, nxp, -1);
+    cf *o = c + row * cnxp;
+    for (int i = 0; i < cnxp; ++i) { o[i].re = (float)line[i].re; o[i].im = (float)line[i].im; }
+  }
+  /* y and z: complex */
+  for (int k = 0; k < nzp; ++k)
+    for (int i = 0; i < cnxp; ++i) {
+      cf *b = c + (long)k * cnxp * nyp + i;
+      for (int j = 0; j < nyp; ++j) { line[j].re = b[(long)j * cnxp].re; line[j].im = b[(long)j * cnxp].im; }
+      dft1d(line, nyp, -1);
+      for (int j = 0; j < nyp; ++j) { b[(long)j * cnxp].re = (float)line[j].re; b[(long)j * cnxp].im = (float)line[j].im; }
+    }
+  for (int j = 0; j < nyp; ++j)
+    for (int i = 0; i < cnxp; ++i) {
+      cf *b = c + (long)j * cnxp + i;
+      long st = (long)cnxp * nyp;
+      for (int k = 0; k < nzp; ++k) { line[k].re = b[k * st].re; line[k].im = b[k * st].im; }
+      dft1d(line, nzp, -1);
+      for (int k = 0; k < nzp; ++k) { b[k * st].re = (float)line[k].re; b[k * st].im = (float)line[k].im; }
+    }
+  free(line);
+  return 0;
+}
+
+int orc_fft_c2r(float *grid, int nxp, int nyp, int nzp, int type) {
+  int cnxp = nxp / 2 + 1, rnxp = 2 * cnxp;
+  long rsize = (long)rnxp * nyp * nzp;
+  int nmax = nxp > nyp ? nxp : nyp; if (nzp > nmax) nmax = nzp;
+  cd *line = (cd *)malloc(sizeof(cd) * nmax);
+  cf *c = (cf *)grid;
+  for (int j = 0; j < nyp; ++j)
+    for (int i = 0; i < cnxp; ++i) {
+      cf *b = c + (long)j * cnxp + i;
+      long st = (long)cnxp * nyp;
+      for (int k = 0; k < nzp; ++k) { line[k].re = b[k * st].re; line[k].im = b[k * st].im; }
+      dft1d(line, nzp, +1);
+      for (int k = 0; k < nzp; ++k) { b[k * st].re = (float)line[k].re; b[k * st].im = (float)line[k].im; }
+    }
+  for (int k = 0; k < nzp; ++k)
+    for (int i = 0; i < cnxp; ++i) {
+      cf *b = c + (long)k * cnxp * nyp + i;
+      for (int j = 0; j < nyp; ++j) { line[j].re = b[(long)j * cnxp].re; line[j].im = b[(long)j * cnxp].im; }
+      dft1d(line, nyp, +1);
+      for (int j = 0; j < nyp; ++j) { b[(long)j * cnxp].re = (float)line[j].re; b[(long)j * cnxp].im = (float)line[j].im; }
+    }
+  /* x: half complex -> real.  The imaginary parts of the DC and (even nxp)
+   * Nyquist terms are ignored, as a real-output inverse transform does. */
+  double *xr = (double *)malloc(sizeof(double) * nxp);
+  for (long row = 0; row < (long)nyp * nzp; ++row) {
+    cf *in = c + row * cnxp;
+    for (int i = 0; i < nxp; ++i) { line[i].re = 0; line[i].im = 0; }
+    line[0].re = in[0].re;
+    for (int i = 1; i < cnxp; ++i) {
+      if (2 * i == nxp) { line[i].re = in[i].re; continue; }
+      line[i].re = in[i].re; line[i].im = in[i].im;
+      line[nxp - i].re = in[i].re; line[nxp - i].im = -in[i].im;
+    }
+    dft1d(line, nxp, +1);
+    for (int i = 0; i < nxp; ++i) xr[i] = line[i].re;
+    float *r = grid + row * rnxp;
+    for (int i = 0; i < nxp; ++i) r[i] = (float)xr[i];
+    r[nxp] = 0.0f;
+    if (rnxp > nxp + 1) r[nxp + 1] = 0.0f;
+  }
+  free(xr); free(line);
+  float scale;
+  if (type == ORC_COVARIANCE) scale = (float)(1.0 / ((double)nxp * nyp * nzp));
+  else scale = (float)(1.0 / sqrt((float)(nxp * nyp * nzp)));
+  scale_real(grid, rsize, scale);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Wavelet tables per kz.                                               */
+/* ------------------------------------------------------------------ */
+/* Wavelet::findNorm on a real wavelet (src/wavelet.cpp:789-808). */
+static float time_norm(const float *w, int n) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += (double)(w[i] * w[i]);
+  return (float)sqrt(s);
+}
+
+/* Wavelet1D::fft1DInPlace (src/wavelet.cpp:246-261): unnormalised real
+ * forward transform, nzp/2+1 coefficients. */
+static void real_spectrum(const float *w, int n, cf *out) {
+  cd *line = (cd *)malloc(sizeof(cd) * n);
+  for (int i = 0; i < n; ++i) { line[i].re = w[i]; line[i].im = 0.0; }
+  dft1d(line, n, -1);
+  for (int i = 0; i < n / 2 + 1; ++i) { out[i].re = (float)line[i].re; out[i].im = (float)line[i].im; }
+  free(line);
+}
+
+/* Wavelet::getCAmp(k) (src/wavelet.cpp:308-324): Hermitian mirror. */
+static cf get_camp(const cf *s, int nzp, int k) {
+  int cnzp = nzp / 2 + 1;
+  cf v;
+  if (k < cnzp) { v.re = s[k].re; v.im = s[k].im; }
+  else { v.re = s[nzp - k].re; v.im = -s[nzp - k].im; }
+  return v;
+}
+
+/* errorSmooth3 = central(backward(forward(w))) -- the three Wavelet1D
+ * difference constructors of src/wavelet1D.cpp:420-479. */
+static void smooth3(const float *w, int n, float *g) {
+  float *e = (float *)malloc(sizeof(float) * n), *f = (float *)malloc(sizeof(float) * n);
+  for (int i = 0; i < n; ++i) e[i] = (i == n - 1) ? w[0] - w[i] : w[i + 1] - w[i];
+  for (int i = 0; i < n; ++i) f[i] = (i == 0) ? e[0] - e[n - 1] : e[i] - e[i - 1];
+  for (int i = 0; i < n; ++i) {
+    if (i == 0) g[i] = (float)(0.5 * (f[1] - f[n - 1]));
+    else if (i == n - 1) g[i] = (float)(0.5 * (f[0] - f[i - 1]));
+    else g[i] = (float)(0.5 * (f[i + 1] - f[i - 1]));
+  }
+  free(e); free(f);
+}
+
+/* Builds the per-kz vectors of crava.cpp:1042-1058 (constant thickness):
+ * fillkW (:1336-1344), diff1Operator (src/wavelet1D.cpp:368-394),
+ * lib_matrProdScalVecCpx, fillkWNorm (:1346-1355), errMult3 = 1, and the
+ * band gate (:1044,1098). */
+int orc_kz_tables(const crava_oracle_params *p, float *wd_, float *e1_,
+                  float *e2_, float *e3, int *inv) {
+  int nzp = p->nzp, nt = p->ntheta, cnzp = nzp / 2 + 1;
+  if (nt < 1 || nt > ORC_MAXT) return 1;
+  cf *wd = (cf *)wd_, *e1 = (cf *)e1_, *e2 = (cf *)e2_;
+  cf *W = (cf *)malloc(sizeof(cf) * cnzp * nt), *G = (cf *)malloc(sizeof(cf) * cnzp * nt);
+  cf *D = (cf *)malloc(sizeof(cf) * cnzp);
+  float *g = (float *)malloc(sizeof(float) * nzp), *dop = (float *)calloc(nzp, sizeof(float));
+  float wn[ORC_MAXT], gn[ORC_MAXT];
+  for (int l = 0; l < nt; ++l) {
+    const float *w = p->wavelet + (long)l * nzp;
+    wn[l] = p->wavelet_norm ? p->wavelet_norm[l] : time_norm(w, nzp);
+    real_spectrum(w, nzp, W + (long)l * cnzp);
+    smooth3(w, nzp, g);
+    gn[l] = time_norm(g, nzp);
+    real_spectrum(g, nzp, G + (long)l * cnzp);
+  }
+  dop[0] = -1.0f; dop[nzp - 1] = 1.0f;
+  real_spectrum(dop, nzp, D);
+  for (int k = 0; k < nzp; ++k) {
+    int mk = k < nzp - k ? k : nzp - k;
+    float realFrequency = (float)((p->nz * 1000.0f) / (p->lz * nzp) * mk);
+    inv[k] = (realFrequency > p->low_cut * p->min_rel_thick) && (realFrequency < p->high_cut);
+    cf kD = get_camp(D, nzp, k);
+    for (int l = 0; l < nt; ++l) {
+      cf a = get_camp(W + (long)l * cnzp, nzp, k);
+      cf kw; kw.re = a.re; kw.im = -a.im;
+      cf r; r.re = kD.re * kw.re - kD.im * kw.im; r.im = kD.re * kw.im + kD.im * kw.re;
+      wd[(long)k * nt + l] = r;
+      e1[(long)k * nt + l].re = a.re / wn[l];
+      e1[(long)k * nt + l].im = -(a.im / wn[l]);
+      cf b = get_camp(G + (long)l * cnzp, nzp, k);
+      e2[(long)k * nt + l].re = b.re / gn[l];
+      e2[(long)k * nt + l].im = -(b.im / gn[l]);
+      e3[(long)k * nt + l] = 1.0f;
+    }
+  }
+  free(W); free(G); free(D); free(g); free(dop);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* FP32 complex kernels, float operation order of libs/lib/lib_matr.c   */
+/* ------------------------------------------------------------------ */
+/* lib_matrCholCpx, libs/lib/lib_matr.c:78-167 */
+static int chol_f(int n, cf m[][ORC_MAXT]) {
+  cf lr; float help;
+  float factor = m[0][0].re;
+  if (factor <= 0) return 1;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) { m[i][j].re = m[i][j].re / factor; m[i][j].im = m[i][j].im / factor; }
+  for (int i = 0; i < n; ++i) {
+    if ((double)m[i][i].re <= ORC_TOL) return 1;
+    for (int j = 0; j < i; ++j) {
+      lr.re = 0.0f; lr.im = 0.0f;
+      for (int k = 0; k < j; ++k) {
+        lr.re += (m[i][k].re * m[j][k].re) + (m[i][k].im * m[j][k].im);
+        lr.im += -(m[i][k].re * m[j][k].im) + (m[i][k].im * m[j][k].re);
+      }
+      help = m[j][j].re * m[j][j].re + m[j][j].im * m[j][j].im;
+      m[i][j].re = ((m[i][j].re - lr.re) * m[j][j].re + (m[i][j].im - lr.im) * m[j][j].im) / help;
+      /* the reference reads the just-updated real part here (:130) */
+      m[i][j].im = ((m[i][j].im - lr.im) * m[j][j].re - (m[i][j].re - lr.re) * m[j][j].im) / help;
+    }
+    lr.re = 0.0f;
+    for (int k = 0; k < i; ++k) lr.re += (m[i][k].re * m[i][k].re) + (m[i][k].im * m[i][k].im);
+    lr.re = m[i][i].re - lr.re;
+    if ((double)lr.re <= ORC_TOL) return 1;
+    m[i][i].re = (float)sqrt(lr.re);
+    m[i][i].im = 0.0f;
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      m[i][j].re *= (float)sqrt(factor);
+      m[i][j].im *= (float)sqrt(factor);
+    }
+  return 0;
+}
+
+/* lib_matrAXeqBMatCpx, libs/lib/lib_matr.c:330-365 (B is n x nc) */
+static void axeqb_f(int n, cf L[][ORC_MAXT], cf B[][3], int nc) {
+  cf lx; float help;
+  for (int c = 0; c < nc; ++c) {
+    for (int i = 0; i < n; ++i) {
+      lx = B[i][c];
+      for (int j = 0; j < i; ++j) {
+        lx.re -= (B[j][c].re * L[i][j].re - B[j][c].im * L[i][j].im);
+        lx.im -= (B[j][c].im * L[i][j].re + B[j][c].re * L[i][j].im);
+      }
+      help = (L[i][i].re * L[i][i].re + L[i][i].im * L[i][i].im);
+      B[i][c].re = (lx.re * L[i][i].re + lx.im * L[i][i].im) / help;
+      B[i][c].im = (lx.im * L[i][i].re - lx.re * L[i][i].im) / help;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      lx = B[i][c];
+      for (int j = n - 1; j > i; --j) {
+        lx.re = lx.re - (B[j][c].re * L[j][i].re + B[j][c].im * L[j][i].im);
+        lx.im = lx.im - (-B[j][c].re * L[j][i].im + B[j][c].im * L[j][i].re);
+      }
+      help = (L[i][i].re * L[i][i].re + L[i][i].im * L[i][i].im);
+      B[i][c].re = (lx.re * L[i][i].re - lx.im * L[i][i].im) / help;
+      B[i][c].im = (lx.im * L[i][i].re + lx.re * L[i][i].im) / help;
+    }
+  }
+}
+
+/* getNextParameterCovariance, src/seismicparametersholder.cpp:355-427 */
+static void prior3_f(const double *v0, const cf c[6], cf S[3][3]) {
+  static const int ip[6] = {0, 1, 2, 0, 0, 1}, iq[6] = {0, 1, 2, 1, 2, 2};
+  for (int t = 0; t < 6; ++t) {
+    float v = (float)v0[ip[t] * 3 + iq[t]];
+    float x = c[t].re;
+    if (v0[ip[t] * 3 + iq[t]] != 0) x = x / v;
+    float a = sqrtf(x * x);
+    S[ip[t]][iq[t]].re = a * v; S[ip[t]][iq[t]].im = 0.0f;
+    if (ip[t] != iq[t]) { S[iq[t]][ip[t]].re = a * v; S[iq[t]][ip[t]].im = -0.0f; }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Per-bin posterior, FP32, restating crava.cpp:1042-1151 with          */
+/* getNextErrorVariance (:1297-1334).                                   */
+/* ------------------------------------------------------------------ */
+int orc_posterior_fp32_t(const crava_oracle_params *p, const float *wd_,
+                         const float *e1_, const float *e2_, const float *e3,
+                         const int *inv, float *const *mu_, float *const *data_,
+                         float *const *cov_, const float *err_corr,
+                         long long *chol_fail) {
+  int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta;
+  int cnxp = nxp / 2 + 1;
+  if (nt < 1 || nt > ORC_MAXT) return 1;
+  const cf *wd = (const cf *)wd_, *e1 = (const cf *)e1_, *e2 = (const cf *)e2_;
+  cf *mu[3], *data[ORC_MAXT], *cov[6];
+  for (int q = 0; q < 3; ++q) mu[q] = (cf *)mu_[q];
+  for (int l = 0; l < nt; ++l) data[l] = (cf *)data_[l];
+  for (int q = 0; q < 6; ++q) cov[q] = (cf *)cov_[q];
+  const cf *ec = (const cf *)err_corr;
+  long long fails = 0;
+  double wnc = p->wnc;
+  cf K[ORC_MAXT][3], KS[ORC_MAXT][3], KScc[3][ORC_MAXT], M[ORC_MAXT][ORC_MAXT], E[ORC_MAXT][ORC_MAXT];
+  cf S[3][3], R[3][3], mean[3], ans[3], dat[ORC_MAXT], res[ORC_MAXT], dm[ORC_MAXT];
+  memset(E, 0, sizeof E); memset(ans, 0, sizeof ans);
+  for (int k = 0; k < nzp; ++k) {
+    const cf *w = wd + (long)k * nt, *m1 = e1 + (long)k * nt, *m2 = e2 + (long)k * nt;
+    const float *m3 = e3 + (long)k * nt;
+    for (int l = 0; l < nt; ++l)
+      for (int q = 0; q < 3; ++q) { K[l][q].re = w[l].re * p->A[l * 3 + q]; K[l][q].im = w[l].im * p->A[l * 3 + q]; }
+    for (int j = 0; j < nyp; ++j)
+      for (int i = 0; i < cnxp; ++i) {
+        long idx = i + (long)cnxp * (j + (long)nyp * k);
+        for (int q = 0; q < 3; ++q) mean[q] = mu[q][idx];
+        for (int l = 0; l < nt; ++l) { dat[l] = data[l][idx]; res[l] = dat[l]; }
+        cf c6[6];
+        for (int q = 0; q < 6; ++q) c6[q] = cov[q][idx];
+        prior3_f(p->var0, c6, S);
+        cf t = ec[idx];
+        float lam = sqrtf(t.re * t.re);
+        if (inv[k]) {
+          for (int l = 0; l < nt; ++l)
+            for (int m = 0; m < nt; ++m) {
+              double th = p->theta_cov[l * nt + m];
+              E[l][m].re = (float)(0.5 * (1.0 - wnc) * th * lam * (m1[l].re * m1[m].re + m1[l].im * m1[m].im));
+              E[l][m].re += (float)(0.5 * (1.0 - wnc) * th * lam * (m2[l].re * m2[m].re + m2[l].im * m2[m].im));
+              if (l == m) {
+                E[l][m].re += (float)(wnc * th * m3[l] * m3[l]);
+                E[l][m].im = 0.0f;
+              } else {
+                E[l][m].im = (float)(0.5 * (1.0 - wnc) * th * lam * (-m1[l].re * m1[m].im + m1[l].im * m1[m].re));
+                E[l][m].im += (float)(0.5 * (1.0 - wnc) * th * lam * (-m2[l].re * m2[m].im + m2[l].im * m2[m].re));
+              }
+            }
+          /* KS = K S  (lib_matrProdCpx) */
+          for (int l = 0; l < nt; ++l)
+            for (int q = 0; q < 3; ++q) {
+              cf x = {0.0f, 0.0f};
+              for (int r = 0; r < 3; ++r) {
+                x.re += K[l][r].re * S[r][q].re - K[l][r].im * S[r][q].im;
+                x.im += K[l][r].im * S[r][q].re + K[l][r].re * S[r][q].im;
+              }
+              KS[l][q] = x;
+            }
+          /* M = KS K^H (lib_matrProdAdjointCpx) ; M += E */
+          for (int l = 0; l < nt; ++l)
+            for (int m = 0; m < nt; ++m) {
+              cf x = {0.0f, 0.0f};
+              for (int r = 0; r < 3; ++r) {
+                x.re += KS[l][r].re * K[m][r].re + KS[l][r].im * K[m][r].im;
+                x.im += KS[l][r].im * K[m][r].re - KS[l][r].re * K[m][r].im;
+              }
+              M[l][m] = x;
+            }
+          for (int l = 0; l < nt; ++l)
+            for (int m = 0; m < nt; ++m) { M[l][m].re += E[l][m].re; M[l][m].im += E[l][m].im; }
+          int flag = chol_f(nt, M);
+          if (flag == 0) {
+            for (int l = 0; l < nt; ++l)
+              for (int q = 0; q < 3; ++q) { KScc[q][l].re = KS[l][q].re; KScc[q][l].im = -KS[l][q].im; }
+            axeqb_f(nt, M, KS, 3);
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) {
+                cf x = {0.0f, 0.0f};
+                for (int l = 0; l < nt; ++l) {
+                  x.re += KScc[a][l].re * KS[l][b].re - KScc[a][l].im * KS[l][b].im;
+                  x.im += KScc[a][l].im * KS[l][b].re + KScc[a][l].re * KS[l][b].im;
+                }
+                R[a][b] = x;
+              }
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) { S[a][b].re -= R[a][b].re; S[a][b].im -= R[a][b].im; }
+            for (int l = 0; l < nt; ++l) {
+              cf x = {0.0f, 0.0f};
+              for (int q = 0; q < 3; ++q) {
+                x.re += K[l][q].re * mean[q].re - K[l][q].im * mean[q].im;
+                x.im += K[l][q].im * mean[q].re + K[l][q].re * mean[q].im;
+              }
+              dm[l] = x;
+            }
+            for (int l = 0; l < nt; ++l) { dat[l].re -= dm[l].re; dat[l].im -= dm[l].im; }
+            for (int q = 0; q < 3; ++q) {
+              cf x = {0.0f, 0.0f};
+              for (int l = 0; l < nt; ++l) {
+                x.re += KS[l][q].re * dat[l].re + KS[l][q].im * dat[l].im;
+                x.im += -KS[l][q].im * dat[l].re + KS[l][q].re * dat[l].im;
+              }
+              ans[q] = x;
+            }
+            for (int q = 0; q < 3; ++q) { mean[q].re += ans[q].re; mean[q].im += ans[q].im; }
+            for (int l = 0; l < nt; ++l) {
+              cf x = {0.0f, 0.0f};
+              for (int q = 0; q < 3; ++q) {
+                x.re += K[l][q].re * mean[q].re - K[l][q].im * mean[q].im;
+                x.im += K[l][q].im * mean[q].re + K[l][q].re * mean[q].im;
+              }
+              dat[l] = x;
+            }
+            for (int l = 0; l < nt; ++l) { res[l].re -= dat[l].re; res[l].im -= dat[l].im; }
+          } else {
+            ++fails;
+          }
+        }
+        for (int q = 0; q < 3; ++q) mu[q][idx] = mean[q];
+        cov[0][idx] = S[0][0]; cov[1][idx] = S[1][1]; cov[2][idx] = S[2][2];
+        cov[3][idx] = S[0][1]; cov[4][idx] = S[0][2]; cov[5][idx] = S[1][2];
+        for (int l = 0; l < nt; ++l) data[l][idx] = res[l];
+      }
+  }
+  if (chol_fail) *chol_fail = fails;
+  return 0;
+}
+
+int orc_posterior_fp32(const crava_oracle_params *p, float *const *mu,
+                       float *const *data, float *const *cov,
+                       const float *err_corr, long long *chol_fail) {
+  int nzp = p->nzp, nt = p->ntheta;
+  if (nt < 1 || nt > ORC_MAXT) return 1;
+  float *wd = (float *)malloc(sizeof(cf) * nzp * nt), *e1 = (float *)malloc(sizeof(cf) * nzp * nt);
+  float *e2 = (float *)malloc(sizeof(cf) * nzp * nt);
+  float *e3 = (float *)malloc(sizeof(float) * nzp * nt);
+  int *inv = (int *)malloc(sizeof(int) * nzp);
+  orc_kz_tables(p, wd, e1, e2, e3, inv);
+  int rc = orc_posterior_fp32_t(p, wd, e1, e2, e3, inv, mu, data, cov, err_corr, chol_fail);
+  free(wd); free(e1); free(e2); free(e3); free(inv);
+  return rc;
+}
+
+/* ------------------------------------------------------------------ */
+/* FP64 twin: the same algorithm (prior |Re| rule, M00 pre-scaled        */
+/* Cholesky with the TOL test, substitutions, Schur update), carried in  */
+/* double from the float spectra.                                        */
+/* ------------------------------------------------------------------ */
+static int chol_d(int n, cd m[][ORC_MAXT]) {
+  double factor = m[0][0].re;
+  if (factor <= 0) return 1;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) { m[i][j].re /= factor; m[i][j].im /= factor; }
+  for (int i = 0; i < n; ++i) {
+    if (m[i][i].re <= ORC_TOL) return 1;
+    for (int j = 0; j < i; ++j) {
+      double lre = 0, lim = 0;
+      for (int k = 0; k < j; ++k) {
+        lre += m[i][k].re * m[j][k].re + m[i][k].im * m[j][k].im;
+        lim += -m[i][k].re * m[j][k].im + m[i][k].im * m[j][k].re;
+      }
+      double h = m[j][j].re * m[j][j].re + m[j][j].im * m[j][j].im;
+      double ar = m[i][j].re - lre, ai = m[i][j].im - lim;
+      m[i][j].re = (ar * m[j][j].re + ai * m[j][j].im) / h;
+      m[i][j].im = (ai * m[j][j].re - ar * m[j][j].im) / h;
+    }
+    double d = 0;
+    for (int k = 0; k < i; ++k) d += m[i][k].re * m[i][k].re + m[i][k].im * m[i][k].im;
+    d = m[i][i].re - d;
+    if (d <= ORC_TOL) return 1;
+    m[i][i].re = sqrt(d); m[i][i].im = 0.0;
+  }
+  double sf = sqrt(factor);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) { m[i][j].re *= sf; m[i][j].im *= sf; }
+  return 0;
+}
+
+static void axeqb_d(int n, cd L[][ORC_MAXT], cd B[][3], int nc) {
+  for (int c = 0; c < nc; ++c) {
+    for (int i = 0; i < n; ++i) {
+      double xr = B[i][c].re, xi = B[i][c].im;
+      for (int j = 0; j < i; ++j) {
+        xr -= B[j][c].re * L[i][j].re - B[j][c].im * L[i][j].im;
+        xi -= B[j][c].im * L[i][j].re + B[j][c].re * L[i][j].im;
+      }
+      double h = L[i][i].re * L[i][i].re + L[i][i].im * L[i][i].im;
+      B[i][c].re = (xr * L[i][i].re + xi * L[i][i].im) / h;
+      B[i][c].im = (xi * L[i][i].re - xr * L[i][i].im) / h;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      double xr = B[i][c].re, xi = B[i][c].im;
+      for (int j = n - 1; j > i; --j) {
+        xr -= B[j][c].re * L[j][i].re + B[j][c].im * L[j][i].im;
+        xi -= -B[j][c].re * L[j][i].im + B[j][c].im * L[j][i].re;
+      }
+      double h = L[i][i].re * L[i][i].re + L[i][i].im * L[i][i].im;
+      B[i][c].re = (xr * L[i][i].re - xi * L[i][i].im) / h;
+      B[i][c].im = (xi * L[i][i].re + xr * L[i][i].im) / h;
+    }
+  }
+}
+
+int orc_posterior_fp64(const crava_oracle_params *p, const float *const *mu_,
+                       const float *const *data_, const float *const *cov_,
+                       const float *err_corr, double *const *mu_out,
+                       double *const *cov_out, double *const *res_out,
+                       long long *chol_fail) {
+  int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta;
+  int cnxp = nxp / 2 + 1;
+  if (nt < 1 || nt > ORC_MAXT) return 1;
+  cf *wd = (cf *)malloc(sizeof(cf) * nzp * nt), *e1 = (cf *)malloc(sizeof(cf) * nzp * nt);
+  cf *e2 = (cf *)malloc(sizeof(cf) * nzp * nt);
+  float *e3 = (float *)malloc(sizeof(float) * nzp * nt);
+  int *inv = (int *)malloc(sizeof(int) * nzp);
+  orc_kz_tables(p, (float *)wd, (float *)e1, (float *)e2, e3, inv);
+  static const int ip[6] = {0, 1, 2, 0, 0, 1}, iq[6] = {0, 1, 2, 1, 2, 2};
+  long long fails = 0;
+  double wnc = p->wnc;
+  cd K[ORC_MAXT][3], KS[ORC_MAXT][3], KSo[ORC_MAXT][3], M[ORC_MAXT][ORC_MAXT];
+  cd S[3][3], mean[3], dat[ORC_MAXT], res[ORC_MAXT];
+  for (int k = 0; k < nzp; ++k) {
+    const cf *w = wd + (long)k * nt, *m1 = e1 + (long)k * nt, *m2 = e2 + (long)k * nt;
+    const float *m3 = e3 + (long)k * nt;
+    for (int l = 0; l < nt; ++l)
+      for (int q = 0; q < 3; ++q) { K[l][q].re = (double)w[l].re * p->A[l * 3 + q]; K[l][q].im = (double)w[l].im * p->A[l * 3 + q]; }
+    for (int j = 0; j < nyp; ++j)
+      for (int i = 0; i < cnxp; ++i) {
+        long idx = i + (long)cnxp * (j + (long)nyp * k);
+        for (int q = 0; q < 3; ++q) { const cf *g = (const cf *)mu_[q]; mean[q].re = g[idx].re; mean[q].im = g[idx].im; }
+        for (int l = 0; l < nt; ++l) { const cf *g = (const cf *)data_[l]; dat[l].re = g[idx].re; dat[l].im = g[idx].im; res[l] = dat[l]; }
+        for (int t = 0; t < 6; ++t) {
+          const cf *g = (const cf *)cov_[t];
+          double v = p->var0[ip[t] * 3 + iq[t]], x = g[idx].re;
+          double a = (v != 0) ? fabs(x / v) * v : fabs(x);
+          S[ip[t]][iq[t]].re = a; S[ip[t]][iq[t]].im = 0;
+          S[iq[t]][ip[t]].re = a; S[iq[t]][ip[t]].im = 0;
+        }
+        double lam = fabs((double)((const cf *)err_corr)[idx].re);
+        if (inv[k]) {
+          for (int l = 0; l < nt; ++l)
+            for (int m = 0; m < nt; ++m) {
+              double th = p->theta_cov[l * nt + m], c = 0.5 * (1.0 - wnc) * th * lam;
+              double er = c * ((double)m1[l].re * m1[m].re + (double)m1[l].im * m1[m].im)
+                        + c * ((double)m2[l].re * m2[m].re + (double)m2[l].im * m2[m].im);
+              double ei = 0.0;
+              if (l == m) er += wnc * th * (double)m3[l] * m3[l];
+              else ei = c * (-(double)m1[l].re * m1[m].im + (double)m1[l].im * m1[m].re)
+                      + c * (-(double)m2[l].re * m2[m].im + (double)m2[l].im * m2[m].re);
+              M[l][m].re = er; M[l][m].im = ei;
+            }
+          for (int l = 0; l < nt; ++l)
+            for (int q = 0; q < 3; ++q) {
+              double xr = 0, xi = 0;
+              for (int r = 0; r < 3; ++r) {
+                xr += K[l][r].re * S[r][q].re - K[l][r].im * S[r][q].im;
+                xi += K[l][r].im * S[r][q].re + K[l][r].re * S[r][q].im;
+              }
+              KS[l][q].re = xr; KS[l][q].im = xi; KSo[l][q] = KS[l][q];
+            }
+          for (int l = 0; l < nt; ++l)
+            for (int m = 0; m < nt; ++m) {
+              double xr = 0, xi = 0;
+              for (int r = 0; r < 3; ++r) {
+                xr += KS[l][r].re * K[m][r].re + KS[l][r].im * K[m][r].im;
+                xi += KS[l][r].im * K[m][r].re - KS[l][r].re * K[m][r].im;
+              }
+              M[l][m].re += xr; M[l][m].im += xi;
+            }
+          if (chol_d(nt, M) == 0) {
+            axeqb_d(nt, M, KS, 3);
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) {
+                double xr = 0, xi = 0;
+                for (int l = 0; l < nt; ++l) {
+                  xr += KSo[l][a].re * KS[l][b].re + KSo[l][a].im * KS[l][b].im;
+                  xi += KSo[l][a].re * KS[l][b].im - KSo[l][a].im * KS[l][b].re;
+                }
+                S[a][b].re -= xr; S[a][b].im -= xi;
+              }
+            cd dm[ORC_MAXT], ans[3];
+            for (int l = 0; l < nt; ++l) {
+              double xr = 0, xi = 0;
+              for (int q = 0; q < 3; ++q) {
+                xr += K[l][q].re * mean[q].re - K[l][q].im * mean[q].im;
+                xi += K[l][q].im * mean[q].re + K[l][q].re * mean[q].im;
+              }
+              dm[l].re = dat[l].re - xr; dm[l].im = dat[l].im - xi;
+            }
+            for (int q = 0; q < 3; ++q) {
+              double xr = 0, xi = 0;
+              for (int l = 0; l < nt; ++l) {
+                xr += KS[l][q].re * dm[l].re + KS[l][q].im * dm[l].im;
+                xi += -KS[l][q].im * dm[l].re + KS[l][q].re * dm[l].im;
+              }
+              ans[q].re = xr; ans[q].im = xi;
+            }
+            for (int q = 0; q < 3; ++q) { mean[q].re += ans[q].re; mean[q].im += ans[q].im; }
+            for (int l = 0; l < nt; ++l) {
+              double xr = 0, xi = 0;
+              for (int q = 0; q < 3; ++q) {
+                xr += K[l][q].re * mean[q].re - K[l][q].im * mean[q].im;
+                xi += K[l][q].im * mean[q].re + K[l][q].re * mean[q].im;
+              }
+              res[l].re -= xr; res[l].im -= xi;
+            }
+          } else {
+            ++fails;
+          }
+        }
+        for (int q = 0; q < 3; ++q) { mu_out[q][2 * idx] = mean[q].re; mu_out[q][2 * idx + 1] = mean[q].im; }
+        for (int t = 0; t < 6; ++t) { cov_out[t][2 * idx] = S[ip[t]][iq[t]].re; cov_out[t][2 * idx + 1] = S[ip[t]][iq[t]].im; }
+        for (int l = 0; l < nt; ++l) { res_out[l][2 * idx] = res[l].re; res_out[l][2 * idx + 1] = res[l].im; }
+      }
+  }
+  if (chol_fail) *chol_fail = fails;
+  free(wd); free(e1); free(e2); free(e3); free(inv);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* The timed unit: forward FFT of 3 means (PARAMETER), ntheta stacks     */
+/* (DATA), 6 prior covariances and the noise correlation (COVARIANCE);   */
+/* the solve; inverse FFT of 3 posterior means, ntheta residuals and 6   */
+/* posterior covariances (crava.cpp:175-190, 1003, 1012, 1181-1206, 218).*/
+/* ------------------------------------------------------------------ */
+int orc_unit_fp32(const crava_oracle_params *p, float *const *mu,
+                  float *const *data, float *const *cov, float *err_corr,
+                  long long *chol_fail) {
+  int nx = p->nxp, ny = p->nyp, nz = p->nzp;
+  for (int q = 0; q < 3; ++q) orc_fft_r2c(mu[q], nx, ny, nz, ORC_PARAMETER);
+  for (int l = 0; l < p->ntheta; ++l) orc_fft_r2c(data[l], nx, ny, nz, ORC_DATA);
+  for (int q = 0; q < 6; ++q) orc_fft_r2c(cov[q], nx, ny, nz, ORC_COVARIANCE);
+  orc_fft_r2c(err_corr, nx, ny, nz, ORC_COVARIANCE);
+  int rc = orc_posterior_fp32(p, mu, data, cov, err_corr, chol_fail);
+  for (int q = 0; q < 3; ++q) orc_fft_c2r(mu[q], nx, ny, nz, ORC_PARAMETER);
+  for (int l = 0; l < p->ntheta; ++l) orc_fft_c2r(data[l], nx, ny, nz, ORC_DATA);
+  for (int q = 0; q < 6; ++q) orc_fft_c2r(cov[q], nx, ny, nz, ORC_COVARIANCE);
+  return rc;
+}
+
+/* ------------------------------------------------------------------ */
+/* RNG: LCG x <- 69069 x + 1 (mod 2^32), u = x / 2^32, with the          */
+/* Marsaglia-Bray normal generator (libs/lib/random.cpp:38-119,          */
+/* constants libs/lib/random.h:12-15).                                   */
+/* ------------------------------------------------------------------ */
+typedef struct { uint32_t s; } lcg_t;
+static double lcg_u(lcg_t *g) {
+  g->s = 69069u * g->s + 1u;
+  return (double)g->s * (1.0 / 4294967296.0);
+}
+static double mb_g(double x) {
+  const double a = 17.49731196, b = 2.36785163, c = 2.15787544;
+  double ax = fabs(x), r = a * exp(-x * x / 2.0);
+  if (ax < 1.0) r -= 2.0 * b * (3.0 - x * x) + c * (1.5 - ax);
+  else if (ax < 1.5) r -= b * (3.0 - ax) * (3.0 - ax) + c * (1.5 - ax);
+  else r -= b * (3.0 - ax) * (3.0 - ax);
+  return r;
+}
+static double lcg_norm(lcg_t *g) {
+  double u = lcg_u(g), x;
+  if (u < 0.8638) {
+    double u1 = lcg_u(g), u2 = lcg_u(g), u3 = lcg_u(g);
+    x = 2.0 * (u1 + u2 + u3) - 3.0;
+  } else if (u < 0.9745) {
+    double u1 = lcg_u(g), u2 = lcg_u(g);
+    x = 1.5 * (u1 + u2 - 1.0);
+  } else if (u < 0.9973002039) {
+    double u1, u2;
+    do { u1 = lcg_u(g); u2 = lcg_u(g); x = 6.0 * u1 - 3.0; } while (0.358 * u2 > mb_g(x));
+  } else {
+    double s, t;
+    do {
+      double v1, v2, w;
+      do {
+        double u1 = lcg_u(g), u2 = lcg_u(g);
+        v1 = 2.0 * u1 - 1.0; v2 = 2.0 * u2 - 1.0; w = v1 * v1 + v2 * v2;
+      } while (w >= 1.0);
+      double c = sqrt((9.0 - 2.0 * log(w)) / w);
+      s = c * v1; t = c * v2;
+    } while (fabs(s) <= 3.0 && fabs(t) <= 3.0);
+    x = fabs(s) > 3.0 ? s : t;
+  }
+  return x;
+}
+
+unsigned int orc_rng_fill_normal(unsigned int seed, double *out, long long n) {
+  lcg_t g = {seed};
+  for (long long i = 0; i < n; ++i) out[i] = lcg_norm(&g);
+  return g.s;
+}
+
+/* FFTGrid::fillInComplexNoise, src/fftgrid.cpp:1213-1263 (including the
+ * reference's parity test on the linear index for the last x plane). */
+unsigned int orc_noise_fill(float *grid, int nxp, int nyp, int nzp,
+                            unsigned int seed) {
+  lcg_t g = {seed};
+  int cnxp = nxp / 2 + 1;
+  long csize = (long)cnxp * nyp * nzp;
+  cf *c = (cf *)grid;
+  float sd = (float)(1 / sqrt(2.0));
+  for (long i = 0; i < csize; ++i) {
+    if (((i % cnxp) == 0) || (((i % cnxp) == cnxp - 1) && ((i % 2) == 1))) {
+      long xs = i % cnxp, jk = (i - xs) / cnxp;
+      long jj = jk % nyp, kk = jk / nyp;
+      long jc = jj == 0 ? 0 : nyp - jj, kc = kk == 0 ? 0 : nzp - kk;
+      long jkc = jc + kc * nyp;
+      if (jkc == jk) { c[i].re = (float)lcg_norm(&g); c[i].im = 0; }
+      else if (jkc > jk) { c[i].re = (float)(sd * lcg_norm(&g)); c[i].im = (float)(sd * lcg_norm(&g)); }
+      else { long ci = jkc * cnxp + xs; c[i].re = c[ci].re; c[i].im = -c[ci].im; }
+    } else {
+      c[i].re = (float)(sd * lcg_norm(&g));
+      c[i].im = (float)(sd * lcg_norm(&g));
+    }
+  }
+  return g.s;
+}
+
+/* Crava::simulate per-bin body, src/crava.cpp:1482-1521: rebuild the
+ * Hermitian 3x3 from 6 posterior spectra, Cholesky, seed <- L seed
+ * (lib_matrProdCholVec, lib_matr.c:453-470); zero on failure. */
+int orc_sim_filter(int nxp, int nyp, int nzp, const float *const *cov_,
+                   float *const *seed_, long long *chol_fail) {
+  long csize = (long)(nxp / 2 + 1) * nyp * nzp;
+  const cf *cv[6]; cf *sd[3];
+  for (int t = 0; t < 6; ++t) cv[t] = (const cf *)cov_[t];
+  for (int q = 0; q < 3; ++q) sd[q] = (cf *)seed_[q];
+  long long fails = 0;
+  cf P[ORC_MAXT][ORC_MAXT];
+  for (long i = 0; i < csize; ++i) {
+    P[0][0] = cv[0][i]; P[1][1] = cv[1][i]; P[2][2] = cv[2][i];
+    P[0][1] = cv[3][i]; P[0][2] = cv[4][i]; P[1][2] = cv[5][i];
+    P[1][0].re = P[0][1].re; P[1][0].im = -P[0][1].im;
+    P[2][0].re = P[0][2].re; P[2][0].im = -P[0][2].im;
+    P[2][1].re = P[1][2].re; P[2][1].im = -P[1][2].im;
+    cf z[3] = {sd[0][i], sd[1][i], sd[2][i]}, o[3];
+    if (chol_f(3, P) == 0) {
+      for (int a = 0; a < 3; ++a) {
+        o[a].re = 0.0f; o[a].im = 0.0f;
+        for (int b = 0; b < a + 1; ++b) {
+          o[a].re += P[a][b].re * z[b].re - P[a][b].im * z[b].im;
+          o[a].im += P[a][b].re * z[b].im + P[a][b].im * z[b].re;
+        }
+      }
+    } else {
+      ++fails;
+      for (int a = 0; a < 3; ++a) { o[a].re = 0.0f; o[a].im = 0.0f; }
+    }
+    for (int q = 0; q < 3; ++q) sd[q][i] = o[q];
+  }
+  if (chol_fail) *chol_fail = fails;
+  return 0;
+}
+
+/* Same filter carried in double (for the GPU filter's tolerance check). */
+int orc_sim_filter_fp64(int nxp, int nyp, int nzp, const float *const *cov_,
+                        float *const *seed_, long long *chol_fail) {
+  long csize = (long)(nxp / 2 + 1) * nyp * nzp;
+  const cf *cv[6]; cf *sd[3];
+  for (int t = 0; t < 6; ++t) cv[t] = (const cf *)cov_[t];
+  for (int q = 0; q < 3; ++q) sd[q] = (cf *)seed_[q];
+  long long fails = 0;
+  cd P[ORC_MAXT][ORC_MAXT];
+  for (long i = 0; i < csize; ++i) {
+    const cf *src[6] = {cv[0] + i, cv[1] + i, cv[2] + i, cv[3] + i, cv[4] + i, cv[5] + i};
+    P[0][0].re = src[0]->re; P[0][0].im = src[0]->im;
+    P[1][1].re = src[1]->re; P[1][1].im = src[1]->im;
+    P[2][2].re = src[2]->re; P[2][2].im = src[2]->im;
+    P[0][1].re = src[3]->re; P[0][1].im = src[3]->im;
+    P[0][2].re = src[4]->re; P[0][2].im = src[4]->im;
+    P[1][2].re = src[5]->re; P[1][2].im = src[5]->im;
+    P[1][0].re = P[0][1].re; P[1][0].im = -P[0][1].im;
+    P[2][0].re = P[0][2].re; P[2][0].im = -P[0][2].im;
+    P[2][1].re = P[1][2].re; P[2][1].im = -P[1][2].im;
+    cd z[3];
+    for (int q = 0; q < 3; ++q) { z[q].re = sd[q][i].re; z[q].im = sd[q][i].im; }
+    if (chol_d(3, P) == 0) {
+      for (int a = 0; a < 3; ++a) {
+        double xr = 0, xi = 0;
+        for (int b = 0; b <= a; ++b) {
+          xr += P[a][b].re * z[b].re - P[a][b].im * z[b].im;
+          xi += P[a][b].re * z[b].im + P[a][b].im * z[b].re;
+        }
+        sd[a][i].re = (float)xr; sd[a][i].im = (float)xi;
+      }
+    } else {
+      ++fails;
+      for (int a = 0; a < 3; ++a) { sd[a][i].re = 0.0f; sd[a][i].im = 0.0f; }
+    }
+  }
+  if (chol_fail) *chol_fail = fails;
+  return 0;
+}

@@ -1,0 +1,414 @@
+/*
+ * ref_harness.cpp -- drives the reference's own numerics, compiled from its
+ * sources (FFTW 2.1.2 single precision, libs/lib/lib_matr.c,
+ * libs/lib/random.cpp), in the order src/crava.cpp drives them.
+ * TEST INFRASTRUCTURE ONLY: built by oracle/Makefile into oracle/_ref/ and
+ * used to pin the restatement in crava_oracle.c and as the timed CPU
+ * baseline.  src/crava.cpp itself cannot be compiled without a CBLAS, so
+ * the per-bin loop below restates src/crava.cpp:1042-1151 while every
+ * numerical call in it is the reference's own function.
+ */
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "fftw.h"
+#include "rfftw.h"
+#include "lib/lib_matr.h"
+#define private public /* read RandomGen's static state after a draw */
+#include "lib/random.h"
+#undef private
+
+#include "crava_oracle.h"
+
+/* random.cpp's file constructor links against NRLib::OpenRead; the harness
+ * never calls it, so this minimal definition only satisfies the linker. */
+namespace NRLib {
+void OpenRead(std::ifstream &stream, const std::string &filename,
+              std::ios_base::openmode mode) {
+  stream.open(filename.c_str(), mode);
+}
+}  // namespace NRLib
+
+namespace {
+
+/* FFTGrid::multiplyByScalar, src/fftgrid.cpp:1992-2000 */
+void multiply_by_scalar(float *g, long rsize, float s) {
+  for (long i = 0; i < rsize; ++i) g[i] *= s;
+}
+
+fftw_complex **alloc_mat(int n1, int n2) {
+  fftw_complex **m = new fftw_complex *[n1];
+  for (int i = 0; i < n1; ++i) {
+    m[i] = new fftw_complex[n2];
+    std::memset(m[i], 0, sizeof(fftw_complex) * n2);
+  }
+  return m;
+}
+void free_mat(fftw_complex **m, int n1) {
+  for (int i = 0; i < n1; ++i) delete[] m[i];
+  delete[] m;
+}
+
+/* Wavelet::fft1DInPlace (src/wavelet.cpp:246-261) on a copy. */
+std::vector<fftw_complex> spectrum1d(const float *w, int nzp) {
+  int cnzp = nzp / 2 + 1;
+  fftw_real *r = static_cast<fftw_real *>(fftw_malloc(2 * cnzp * sizeof(fftw_real)));
+  for (int i = 0; i < 2 * cnzp; ++i) r[i] = i < nzp ? w[i] : 0.0f;
+  rfftwnd_plan plan = rfftwnd_create_plan(1, &nzp, FFTW_REAL_TO_COMPLEX,
+                                          FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_one_real_to_complex(plan, r, reinterpret_cast<fftw_complex *>(r));
+  fftwnd_destroy_plan(plan);
+  std::vector<fftw_complex> out(cnzp);
+  std::memcpy(out.data(), r, sizeof(fftw_complex) * cnzp);
+  fftw_free(r);
+  return out;
+}
+
+/* Wavelet::getCAmp(k), src/wavelet.cpp:308-324 */
+fftw_complex get_camp(const std::vector<fftw_complex> &c, int nzp, int k) {
+  fftw_complex v;
+  if (k < nzp / 2 + 1) { v.re = c[k].re; v.im = c[k].im; }
+  else { v.re = c[nzp - k].re; v.im = -c[nzp - k].im; }
+  return v;
+}
+
+/* Wavelet::findNorm on a real wavelet, src/wavelet.cpp:789-808 */
+float find_norm(const float *w, int n) {
+  double norm2 = 0.0;
+  for (int i = 0; i < n; ++i) norm2 += static_cast<double>(w[i] * w[i]);
+  return static_cast<float>(std::sqrt(norm2));
+}
+
+struct KzTables {
+  std::vector<fftw_complex> wd, e1, e2;
+  std::vector<float> e3;
+  std::vector<int> inv;
+};
+
+/* crava.cpp:952-976, 1024-1058 for the constant-thickness branch. */
+void build_tables(const crava_oracle_params *p, KzTables &t) {
+  const int nzp = p->nzp, nt = p->ntheta;
+  std::vector<std::vector<fftw_complex>> W(nt), G(nt);
+  std::vector<float> wn(nt), gn(nt);
+  std::vector<float> e(nzp), f(nzp), g(nzp);
+  for (int l = 0; l < nt; ++l) {
+    const float *w = p->wavelet + static_cast<long>(l) * nzp;
+    wn[l] = p->wavelet_norm ? p->wavelet_norm[l] : find_norm(w, nzp);
+    W[l] = spectrum1d(w, nzp);
+    /* Wavelet1D difference constructors, src/wavelet1D.cpp:420-479 */
+    for (int i = 0; i < nzp; ++i) e[i] = (i == nzp - 1) ? w[0] - w[i] : w[i + 1] - w[i];
+    for (int i = 0; i < nzp; ++i) f[i] = (i == 0) ? e[0] - e[nzp - 1] : e[i] - e[i - 1];
+    for (int i = 0; i < nzp; ++i) {
+      if (i == 0) g[i] = static_cast<fftw_real>(0.5 * (f[i + 1] - f[nzp - 1]));
+      else if (i == nzp - 1) g[i] = static_cast<fftw_real>(0.5 * (f[0] - f[i - 1]));
+      else g[i] = static_cast<fftw_real>(0.5 * (f[i + 1] - f[i - 1]));
+    }
+    gn[l] = find_norm(g.data(), nzp);
+    G[l] = spectrum1d(g.data(), nzp);
+  }
+  /* Wavelet1D(FIRSTORDERFORWARDDIFF, nz, nzp), src/wavelet1D.cpp:368-394 */
+  std::vector<float> d(nzp, 0.0f);
+  d[0] = -1.0f; d[nzp - 1] = 1.0f;
+  std::vector<fftw_complex> D = spectrum1d(d.data(), nzp);
+
+  t.wd.resize(static_cast<size_t>(nzp) * nt); t.e1.resize(t.wd.size());
+  t.e2.resize(t.wd.size()); t.e3.resize(t.wd.size()); t.inv.resize(nzp);
+  std::vector<fftw_complex> kW(nt);
+  for (int k = 0; k < nzp; ++k) {
+    float realFrequency = static_cast<float>((p->nz * 1000.0f) / (p->lz * nzp) * std::min(k, nzp - k));
+    t.inv[k] = realFrequency > p->low_cut * p->min_rel_thick && realFrequency < p->high_cut;
+    fftw_complex kD = get_camp(D, nzp, k);
+    for (int l = 0; l < nt; ++l) {  /* fillkW, crava.cpp:1336-1344 */
+      kW[l].re = float(get_camp(W[l], nzp, k).re);
+      kW[l].im = -float(get_camp(W[l], nzp, k).im);
+    }
+    lib_matrProdScalVecCpx(kD, kW.data(), nt);
+    for (int l = 0; l < nt; ++l) {
+      size_t o = static_cast<size_t>(k) * nt + l;
+      t.wd[o] = kW[l];
+      /* fillkWNorm, crava.cpp:1346-1355 */
+      t.e1[o].re = float(get_camp(W[l], nzp, k).re / wn[l]);
+      t.e1[o].im = -float(get_camp(W[l], nzp, k).im / wn[l]);
+      t.e2[o].re = float(get_camp(G[l], nzp, k).re / gn[l]);
+      t.e2[o].im = -float(get_camp(G[l], nzp, k).im / gn[l]);
+      t.e3[o] = 1.0f; /* lib_matrFillOnesVecCpx(errMult3) */
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+/* FFTGrid::fftInPlace, src/fftgrid.cpp:1803-1829 */
+int ref_fft_r2c(float *grid, int nxp, int nyp, int nzp, int type) {
+  long rsize = 2L * (nxp / 2 + 1) * nyp * nzp;
+  if (type != ORC_COVARIANCE)
+    multiply_by_scalar(grid, rsize, 1.0f / std::sqrt(static_cast<float>(nxp * nyp * nzp)));
+  rfftwnd_plan plan = rfftw3d_create_plan(nzp, nyp, nxp, FFTW_REAL_TO_COMPLEX,
+                                          FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_one_real_to_complex(plan, grid, reinterpret_cast<fftw_complex *>(grid));
+  fftwnd_destroy_plan(plan);
+  return 0;
+}
+
+/* FFTGrid::invFFTInPlace, src/fftgrid.cpp:1831-1862 */
+int ref_fft_c2r(float *grid, int nxp, int nyp, int nzp, int type) {
+  long rsize = 2L * (nxp / 2 + 1) * nyp * nzp;
+  float scale;
+  if (type == ORC_COVARIANCE) scale = float(1.0 / (nxp * nyp * nzp));
+  else scale = float(1.0 / std::sqrt(float(nxp * nyp * nzp)));
+  rfftwnd_plan plan = rfftw3d_create_plan(nzp, nyp, nxp, FFTW_COMPLEX_TO_REAL,
+                                          FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_one_complex_to_real(plan, reinterpret_cast<fftw_complex *>(grid), grid);
+  fftwnd_destroy_plan(plan);
+  multiply_by_scalar(grid, rsize, scale);
+  return 0;
+}
+
+int ref_kz_tables(const crava_oracle_params *p, float *wd, float *e1, float *e2,
+                  float *e3, int *inv) {
+  if (p->ntheta < 1 || p->ntheta > 16) return 1;
+  KzTables t;
+  build_tables(p, t);
+  size_t n = t.wd.size();
+  std::memcpy(wd, t.wd.data(), n * sizeof(fftw_complex));
+  std::memcpy(e1, t.e1.data(), n * sizeof(fftw_complex));
+  std::memcpy(e2, t.e2.data(), n * sizeof(fftw_complex));
+  std::memcpy(e3, t.e3.data(), n * sizeof(float));
+  std::memcpy(inv, t.inv.data(), t.inv.size() * sizeof(int));
+  return 0;
+}
+
+/* Crava::computePostMeanResidAndFFTCov hot loop, src/crava.cpp:1042-1151,
+ * with SeismicParametersHolder::getNextParameterCovariance
+ * (src/seismicparametersholder.cpp:355-427) and
+ * Crava::getNextErrorVariance (src/crava.cpp:1297-1334). */
+int ref_posterior_fp32_t(const crava_oracle_params *p, const float *wd,
+                         const float *e1, const float *e2, const float *e3,
+                         const int *inv, float *const *mu_, float *const *data_,
+                         float *const *cov_, const float *err_corr,
+                         long long *chol_fail) {
+  const int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta;
+  const int cnxp = nxp / 2 + 1;
+  if (nt < 1 || nt > 16) return 1;
+  KzTables t;
+  size_t n = static_cast<size_t>(nzp) * nt;
+  t.wd.assign(reinterpret_cast<const fftw_complex *>(wd), reinterpret_cast<const fftw_complex *>(wd) + n);
+  t.e1.assign(reinterpret_cast<const fftw_complex *>(e1), reinterpret_cast<const fftw_complex *>(e1) + n);
+  t.e2.assign(reinterpret_cast<const fftw_complex *>(e2), reinterpret_cast<const fftw_complex *>(e2) + n);
+  t.e3.assign(e3, e3 + n);
+  t.inv.assign(inv, inv + nzp);
+  fftw_complex *mu[3], *data[16], *cov[6];
+  for (int q = 0; q < 3; ++q) mu[q] = reinterpret_cast<fftw_complex *>(mu_[q]);
+  for (int l = 0; l < nt; ++l) data[l] = reinterpret_cast<fftw_complex *>(data_[l]);
+  for (int q = 0; q < 6; ++q) cov[q] = reinterpret_cast<fftw_complex *>(cov_[q]);
+  const fftw_complex *ec = reinterpret_cast<const fftw_complex *>(err_corr);
+  const double *v0 = p->var0;
+  float wnc = p->wnc;
+
+  fftw_complex *ijkData = new fftw_complex[nt], *ijkDataMean = new fftw_complex[nt];
+  fftw_complex *ijkRes = new fftw_complex[nt], *ijkMean = new fftw_complex[3];
+  fftw_complex *ijkAns = new fftw_complex[3];
+  fftw_complex **K = alloc_mat(nt, 3), **KS = alloc_mat(nt, 3), **KScc = alloc_mat(3, nt);
+  fftw_complex **parVar = alloc_mat(3, 3), **margVar = alloc_mat(nt, nt);
+  fftw_complex **errVar = alloc_mat(nt, nt), **reduceVar = alloc_mat(3, 3);
+  std::vector<float> A(p->A, p->A + 3 * nt);
+  std::vector<float *> Arows(nt);
+  for (int l = 0; l < nt; ++l) Arows[l] = &A[3 * l];
+  long long fails = 0;
+
+  for (int k = 0; k < nzp; ++k) {
+    fftw_complex *kW = &t.wd[static_cast<size_t>(k) * nt];
+    fftw_complex *errMult1 = &t.e1[static_cast<size_t>(k) * nt];
+    fftw_complex *errMult2 = &t.e2[static_cast<size_t>(k) * nt];
+    float *errMult3 = &t.e3[static_cast<size_t>(k) * nt];
+    lib_matrProdDiagCpxR(kW, Arows.data(), nt, 3, K);
+    bool invert_frequency = t.inv[k] != 0;
+    for (int j = 0; j < nyp; ++j) {
+      for (int i = 0; i < cnxp; ++i) {
+        long idx = i + static_cast<long>(cnxp) * (j + static_cast<long>(nyp) * k);
+        ijkMean[0] = mu[0][idx]; ijkMean[1] = mu[1][idx]; ijkMean[2] = mu[2][idx];
+        for (int l = 0; l < nt; ++l) { ijkData[l] = data[l][idx]; ijkRes[l] = ijkData[l]; }
+
+        /* getNextParameterCovariance */
+        fftw_complex iiTmp = cov[0][idx], jjTmp = cov[1][idx], kkTmp = cov[2][idx];
+        fftw_complex ijTmp = cov[3][idx], ikTmp = cov[4][idx], jkTmp = cov[5][idx];
+        if (v0[0] != 0) iiTmp.re = iiTmp.re / static_cast<float>(v0[0]);
+        if (v0[4] != 0) jjTmp.re = jjTmp.re / static_cast<float>(v0[4]);
+        if (v0[8] != 0) kkTmp.re = kkTmp.re / static_cast<float>(v0[8]);
+        if (v0[1] != 0) ijTmp.re = ijTmp.re / static_cast<float>(v0[1]);
+        if (v0[2] != 0) ikTmp.re = ikTmp.re / static_cast<float>(v0[2]);
+        if (v0[5] != 0) jkTmp.re = jkTmp.re / static_cast<float>(v0[5]);
+        float ii = float(std::sqrt(iiTmp.re * iiTmp.re)), jj = float(std::sqrt(jjTmp.re * jjTmp.re));
+        float kk = float(std::sqrt(kkTmp.re * kkTmp.re)), ij = float(std::sqrt(ijTmp.re * ijTmp.re));
+        float ik = float(std::sqrt(ikTmp.re * ikTmp.re)), jk = float(std::sqrt(jkTmp.re * jkTmp.re));
+        parVar[0][0].re = ii * static_cast<float>(v0[0]); parVar[0][0].im = 0.0;
+        parVar[1][1].re = jj * static_cast<float>(v0[4]); parVar[1][1].im = 0.0;
+        parVar[2][2].re = kk * static_cast<float>(v0[8]); parVar[2][2].im = 0.0;
+        parVar[0][1].re = ij * static_cast<float>(v0[1]); parVar[0][1].im = 0.0;
+        parVar[1][0].re = ij * static_cast<float>(v0[1]); parVar[1][0].im = -0.0f;
+        parVar[0][2].re = ik * static_cast<float>(v0[2]); parVar[0][2].im = 0.0;
+        parVar[2][0].re = ik * static_cast<float>(v0[2]); parVar[2][0].im = -0.0f;
+        parVar[1][2].re = jk * static_cast<float>(v0[5]); parVar[1][2].im = 0.0;
+        parVar[2][1].re = jk * static_cast<float>(v0[5]); parVar[2][1].im = -0.0f;
+
+        /* getNextErrorVariance */
+        fftw_complex ijkTmp = ec[idx];
+        float lam = float(std::sqrt(ijkTmp.re * ijkTmp.re));
+        if (invert_frequency) {
+          for (int l = 0; l < nt; ++l)
+            for (int m = 0; m < nt; ++m) {
+              double th = p->theta_cov[l * nt + m];
+              errVar[l][m].re = float(0.5 * (1.0 - wnc) * th * lam * (errMult1[l].re * errMult1[m].re + errMult1[l].im * errMult1[m].im));
+              errVar[l][m].re += float(0.5 * (1.0 - wnc) * th * lam * (errMult2[l].re * errMult2[m].re + errMult2[l].im * errMult2[m].im));
+              if (l == m) {
+                errVar[l][m].re += float(wnc * th * errMult3[l] * errMult3[l]);
+                errVar[l][m].im = 0.0;
+              } else {
+                errVar[l][m].im = float(0.5 * (1.0 - wnc) * th * lam * (-errMult1[l].re * errMult1[m].im + errMult1[l].im * errMult1[m].re));
+                errVar[l][m].im += float(0.5 * (1.0 - wnc) * th * lam * (-errMult2[l].re * errMult2[m].im + errMult2[l].im * errMult2[m].re));
+              }
+            }
+
+          lib_matrProdCpx(K, parVar, nt, 3, 3, KS);
+          lib_matrProdAdjointCpx(KS, K, nt, 3, nt, margVar);
+          lib_matrAddMatCpx(errVar, nt, nt, margVar);
+          int cholFlag = lib_matrCholCpx(nt, margVar);
+          if (cholFlag == 0) {
+            lib_matrAdjoint(KS, nt, 3, KScc);
+            lib_matrAXeqBMatCpx(nt, margVar, KS, 3);
+            lib_matrProdCpx(KScc, KS, 3, nt, 3, reduceVar);
+            lib_matrSubtMatCpx(reduceVar, 3, 3, parVar);
+            lib_matrProdMatVecCpx(K, ijkMean, nt, 3, ijkDataMean);
+            lib_matrSubtVecCpx(ijkDataMean, nt, ijkData);
+            lib_matrProdAdjointMatVecCpx(KS, ijkData, 3, nt, ijkAns);
+            lib_matrAddVecCpx(ijkAns, 3, ijkMean);
+            lib_matrProdMatVecCpx(K, ijkMean, nt, 3, ijkData);
+            lib_matrSubtVecCpx(ijkData, nt, ijkRes);
+          } else {
+            ++fails;
+          }
+        }
+        mu[0][idx] = ijkMean[0]; mu[1][idx] = ijkMean[1]; mu[2][idx] = ijkMean[2];
+        cov[0][idx] = parVar[0][0]; cov[1][idx] = parVar[1][1]; cov[2][idx] = parVar[2][2];
+        cov[3][idx] = parVar[0][1]; cov[4][idx] = parVar[0][2]; cov[5][idx] = parVar[1][2];
+        for (int l = 0; l < nt; ++l) data[l][idx] = ijkRes[l];
+      }
+    }
+  }
+  if (chol_fail) *chol_fail = fails;
+  delete[] ijkData; delete[] ijkDataMean; delete[] ijkRes; delete[] ijkMean; delete[] ijkAns;
+  free_mat(K, nt); free_mat(KS, nt); free_mat(KScc, 3); free_mat(parVar, 3);
+  free_mat(margVar, nt); free_mat(errVar, nt); free_mat(reduceVar, 3);
+  return 0;
+}
+
+int ref_posterior_fp32(const crava_oracle_params *p, float *const *mu,
+                       float *const *data, float *const *cov,
+                       const float *err_corr, long long *chol_fail) {
+  if (p->ntheta < 1 || p->ntheta > 16) return 1;
+  KzTables t;
+  build_tables(p, t);
+  return ref_posterior_fp32_t(p, reinterpret_cast<const float *>(t.wd.data()),
+                              reinterpret_cast<const float *>(t.e1.data()),
+                              reinterpret_cast<const float *>(t.e2.data()), t.e3.data(),
+                              t.inv.data(), mu, data, cov, err_corr, chol_fail);
+}
+
+/* The timed unit (forward FFTs, solve, inverse FFTs). */
+int ref_unit_fp32(const crava_oracle_params *p, float *const *mu,
+                  float *const *data, float *const *cov, float *err_corr,
+                  long long *chol_fail) {
+  int nx = p->nxp, ny = p->nyp, nz = p->nzp;
+  for (int q = 0; q < 3; ++q) ref_fft_r2c(mu[q], nx, ny, nz, ORC_PARAMETER);
+  for (int l = 0; l < p->ntheta; ++l) ref_fft_r2c(data[l], nx, ny, nz, ORC_DATA);
+  for (int q = 0; q < 6; ++q) ref_fft_r2c(cov[q], nx, ny, nz, ORC_COVARIANCE);
+  ref_fft_r2c(err_corr, nx, ny, nz, ORC_COVARIANCE);
+  int rc = ref_posterior_fp32(p, mu, data, cov, err_corr, chol_fail);
+  for (int q = 0; q < 3; ++q) ref_fft_c2r(mu[q], nx, ny, nz, ORC_PARAMETER);
+  for (int l = 0; l < p->ntheta; ++l) ref_fft_c2r(data[l], nx, ny, nz, ORC_DATA);
+  for (int q = 0; q < 6; ++q) ref_fft_c2r(cov[q], nx, ny, nz, ORC_COVARIANCE);
+  return rc;
+}
+
+unsigned int ref_rng_fill_normal(unsigned int seed, double *out, long long n) {
+  RandomGen gen(seed);
+  for (long long i = 0; i < n; ++i) out[i] = RandomGen::rnorm01();
+  return RandomGen::seed_;
+}
+
+/* FFTGrid::fillInComplexNoise, src/fftgrid.cpp:1213-1263 */
+unsigned int ref_noise_fill(float *grid, int nxp, int nyp, int nzp,
+                            unsigned int seed) {
+  RandomGen gen(seed);
+  RandomGen *ranGen = &gen;
+  fftw_complex *cvalue_ = reinterpret_cast<fftw_complex *>(grid);
+  int cnxp_ = nxp / 2 + 1, nyp_ = nyp, nzp_ = nzp;
+  int csize_ = cnxp_ * nyp * nzp;
+  float std = float(1 / std::sqrt(2.0));
+  for (int i = 0; i < csize_; i++) {
+    if (((i % cnxp_) == 0) || (((i % cnxp_) == cnxp_ - 1) && ((i % 2) == 1))) {
+      int xshift = i % cnxp_;
+      int jkind = (i - xshift) / cnxp_;
+      int jind = jkind % nyp_;
+      int kind = int(jkind / nyp_);
+      int jccind = jind == 0 ? 0 : nyp_ - jind;
+      int kccind = kind == 0 ? 0 : nzp_ - kind;
+      int jkccind = jccind + kccind * nyp_;
+      if (jkccind == jkind) {
+        cvalue_[i].re = float(ranGen->rnorm01());
+        cvalue_[i].im = 0;
+      } else if (jkccind > jkind) {
+        cvalue_[i].re = float(std * ranGen->rnorm01());
+        cvalue_[i].im = float(std * ranGen->rnorm01());
+      } else {
+        int cci = jkccind * cnxp_ + xshift;
+        cvalue_[i].re = cvalue_[cci].re;
+        cvalue_[i].im = -cvalue_[cci].im;
+      }
+    } else {
+      cvalue_[i].re = float(std * ranGen->rnorm01());
+      cvalue_[i].im = float(std * ranGen->rnorm01());
+    }
+  }
+  return RandomGen::seed_;
+}
+
+/* Crava::simulate per-bin body, src/crava.cpp:1482-1521 */
+int ref_sim_filter(int nxp, int nyp, int nzp, const float *const *cov_,
+                   float *const *seed_, long long *chol_fail) {
+  long csize = static_cast<long>(nxp / 2 + 1) * nyp * nzp;
+  const fftw_complex *cv[6];
+  fftw_complex *sd[3];
+  for (int q = 0; q < 6; ++q) cv[q] = reinterpret_cast<const fftw_complex *>(cov_[q]);
+  for (int q = 0; q < 3; ++q) sd[q] = reinterpret_cast<fftw_complex *>(seed_[q]);
+  fftw_complex **ijkPostCov = alloc_mat(3, 3);
+  fftw_complex ijkSeed[3];
+  long long fails = 0;
+  for (long i = 0; i < csize; ++i) {
+    ijkPostCov[0][0] = cv[0][i]; ijkPostCov[1][1] = cv[1][i]; ijkPostCov[2][2] = cv[2][i];
+    ijkPostCov[0][1] = cv[3][i]; ijkPostCov[0][2] = cv[4][i]; ijkPostCov[1][2] = cv[5][i];
+    ijkPostCov[1][0].re = ijkPostCov[0][1].re; ijkPostCov[1][0].im = -ijkPostCov[0][1].im;
+    ijkPostCov[2][0].re = ijkPostCov[0][2].re; ijkPostCov[2][0].im = -ijkPostCov[0][2].im;
+    ijkPostCov[2][1].re = ijkPostCov[1][2].re; ijkPostCov[2][1].im = -ijkPostCov[1][2].im;
+    ijkSeed[0] = sd[0][i]; ijkSeed[1] = sd[1][i]; ijkSeed[2] = sd[2][i];
+    int cholFlag = lib_matrCholCpx(3, ijkPostCov);
+    if (cholFlag == 0) {
+      lib_matrProdCholVec(3, ijkPostCov, ijkSeed);
+    } else {
+      ++fails;
+      for (int l = 0; l < 3; l++) { ijkSeed[l].re = 0.0; ijkSeed[l].im = 0.0; }
+    }
+    sd[0][i] = ijkSeed[0]; sd[1][i] = ijkSeed[1]; sd[2][i] = ijkSeed[2];
+  }
+  free_mat(ijkPostCov, 3);
+  if (chol_fail) *chol_fail = fails;
+  return 0;
+}
+
+}  /* extern "C" */
