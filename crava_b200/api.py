@@ -1,0 +1,333 @@
+"""Python binding of the C ABI (include/crava_gpu.h) over ctypes.
+
+PyTorch provides device memory and streams; every computation runs in the
+in-tree CUDA library crava_b200/lib/libcrava_gpu.so.  There is no CPU path:
+if the library or a CUDA device is missing, the calls raise.
+
+The classes mirror the reference interface this path replaces:
+  FFTGrid  -- a padded grid in HBM with fftInPlace / invFFTInPlace
+              (src/fftgrid.h:110-143 of the reference);
+  Crava    -- computePostMeanResidAndFFTCov and simulate on a set of grids
+              (src/crava.h:35-79).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcrava_gpu.so")
+
+MAX_THETA = 8
+OK = 0
+STATUS = {0: "ok", 1: "invalid argument", 2: "allocation failed", 3: "CUDA error",
+          4: "device wait timed out", 5: "call out of order", 6: "no CUDA device"}
+DATA, PARAMETER, COVARIANCE = 1, 2, 3
+FP64, MIXED, FP32 = 0, 1, 2
+
+F32P = C.POINTER(C.c_float)
+F64P = C.POINTER(C.c_double)
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nxp", C.c_int), ("nyp", C.c_int), ("nzp", C.c_int), ("ntheta", C.c_int),
+        ("nz", C.c_int), ("precision", C.c_int),
+        ("lz", C.c_double), ("min_rel_thick", C.c_double),
+        ("low_cut", C.c_float), ("high_cut", C.c_float), ("wnc", C.c_float),
+        ("reserved", C.c_float),
+        ("wavelet", F32P), ("wavelet_norm", F32P), ("A", F32P),
+        ("theta_cov", F64P), ("var0", F64P),
+    ]
+
+
+class Grids(C.Structure):
+    _fields_ = [("mu", C.c_void_p * 3), ("data", C.c_void_p * MAX_THETA),
+                ("cov", C.c_void_p * 6), ("err_corr", C.c_void_p)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("chol_fail_bins", C.c_longlong), ("nonfinite_bins", C.c_longlong),
+                ("ms_forward", C.c_float), ("ms_solve", C.c_float),
+                ("ms_inverse", C.c_float), ("ms_total", C.c_float)]
+
+
+SYMBOLS = {
+    "crava_gpu_create": ([C.POINTER(Params), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "crava_gpu_destroy": ([C.c_void_p], C.c_int),
+    "crava_gpu_status_string": ([C.c_int], C.c_char_p),
+    "crava_gpu_fft_r2c": ([C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "crava_gpu_fft_c2r": ([C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "crava_gpu_posterior": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
+    "crava_gpu_posterior_unit": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
+    "crava_gpu_posterior_unit_host": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
+    "crava_gpu_host_register": ([C.c_void_p, C.c_uint64], C.c_int),
+    "crava_gpu_host_unregister": ([C.c_void_p], C.c_int),
+    "crava_gpu_noise_fill": ([C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64], C.c_int),
+    "crava_gpu_sim_filter": ([C.c_void_p, C.c_void_p * 6, C.c_void_p * 3], C.c_int),
+    "crava_gpu_simulate": ([C.c_void_p, C.c_void_p * 6, C.c_void_p * 3, C.c_uint64, C.c_int,
+                            C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "crava_gpu_get_stats": ([C.c_void_p, C.POINTER(Stats)], C.c_int),
+    "crava_gpu_kz_tables": ([C.c_void_p, F32P, F32P, F32P, F32P, C.POINTER(C.c_int)], C.c_int),
+    "crava_gpu_set_kz_tables": ([C.c_void_p, F32P, F32P, F32P, F32P, C.POINTER(C.c_int)], C.c_int),
+    "crava_gpu_launch_count": ([], C.c_longlong),
+}
+
+_lib = None
+
+
+class CravaGpuError(RuntimeError):
+    pass
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads the CUDA library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise CravaGpuError(f"CUDA library not built: {path} (run crava_b200/build.py)")
+    lib = C.CDLL(path)
+    for name, (args, res) in SYMBOLS.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != OK:
+        msg = load_library().crava_gpu_status_string(rc).decode()
+        raise CravaGpuError(f"{what}: status {rc} ({msg})")
+
+
+def launch_count() -> int:
+    return int(load_library().crava_gpu_launch_count())
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class Context:
+    """A crava_gpu_ctx bound to one device and one CUDA stream."""
+
+    def __init__(self, case, device: int = 0, stream=None, precision: int = MIXED,
+                 wavelet_norm=None):
+        import torch
+
+        lib = load_library()
+        self._keep = []
+        wav = np.ascontiguousarray(case.wavelet, dtype=np.float32)
+        A = np.ascontiguousarray(case.A, dtype=np.float32)
+        th = np.ascontiguousarray(case.theta_cov, dtype=np.float64)
+        v0 = np.ascontiguousarray(case.var0, dtype=np.float64)
+        self._keep += [wav, A, th, v0]
+        wn = None
+        if wavelet_norm is not None:
+            wn = np.ascontiguousarray(wavelet_norm, dtype=np.float32)
+            self._keep.append(wn)
+        self.params = Params(case.nxp, case.nyp, case.nzp, case.ntheta, case.nz, precision,
+                             case.lz, case.min_rel_thick, case.low_cut, case.high_cut, case.wnc,
+                             0.0, wav.ctypes.data_as(F32P),
+                             wn.ctypes.data_as(F32P) if wn is not None else None,
+                             A.ctypes.data_as(F32P), th.ctypes.data_as(F64P),
+                             v0.ctypes.data_as(F64P))
+        self.case = case
+        self.device = device
+        self.stream = stream if stream is not None else torch.cuda.current_stream(device)
+        self.precision = precision
+        h = C.c_void_p()
+        check(lib.crava_gpu_create(C.byref(self.params), device, C.c_void_p(self.stream.cuda_stream),
+                                   C.byref(h)), "crava_gpu_create")
+        self.handle = h
+        self.lib = lib
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.crava_gpu_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- grids
+    def grids(self, mu, data, cov, err):
+        g = Grids()
+        for q in range(3):
+            g.mu[q] = mu[q].data_ptr()
+        for l in range(len(data)):
+            g.data[l] = data[l].data_ptr()
+        for t in range(6):
+            g.cov[t] = cov[t].data_ptr()
+        g.err_corr = err.data_ptr()
+        return g
+
+    def fft_r2c(self, grid, grid_type):
+        check(self.lib.crava_gpu_fft_r2c(self.handle, _ptr(grid), grid_type), "fft_r2c")
+
+    def fft_c2r(self, grid, grid_type):
+        check(self.lib.crava_gpu_fft_c2r(self.handle, _ptr(grid), grid_type), "fft_c2r")
+
+    def posterior(self, mu, data, cov, err, precision=None):
+        g = self.grids(mu, data, cov, err)
+        p = self.precision if precision is None else precision
+        check(self.lib.crava_gpu_posterior(self.handle, C.byref(g), p), "posterior")
+
+    def posterior_unit(self, mu, data, cov, err, precision=None):
+        g = self.grids(mu, data, cov, err)
+        p = self.precision if precision is None else precision
+        check(self.lib.crava_gpu_posterior_unit(self.handle, C.byref(g), p), "posterior_unit")
+
+    def posterior_unit_host(self, mu, data, cov, err, precision=None):
+        """Host tensors (CPU, ideally pinned); synchronous."""
+        g = self.grids(mu, data, cov, err)
+        p = self.precision if precision is None else precision
+        check(self.lib.crava_gpu_posterior_unit_host(self.handle, C.byref(g), p), "posterior_unit_host")
+
+    def noise_fill(self, grid, seed, stream_id):
+        check(self.lib.crava_gpu_noise_fill(self.handle, _ptr(grid), seed, stream_id), "noise_fill")
+
+    def sim_filter(self, cov, seeds):
+        cv = (C.c_void_p * 6)(*[c.data_ptr() for c in cov])
+        sd = (C.c_void_p * 3)(*[s.data_ptr() for s in seeds])
+        check(self.lib.crava_gpu_sim_filter(self.handle, cv, sd), "sim_filter")
+
+    def simulate(self, cov, post_mean, seed, first_index, outs):
+        """outs: list of 3*count real grids (device)."""
+        cv = (C.c_void_p * 6)(*[c.data_ptr() for c in cov])
+        pm = (C.c_void_p * 3)(*[m.data_ptr() for m in post_mean])
+        count = len(outs) // 3
+        arr = (C.c_void_p * max(1, len(outs)))(*[o.data_ptr() for o in outs])
+        check(self.lib.crava_gpu_simulate(self.handle, cv, pm, seed, first_index, count, arr), "simulate")
+
+    def stats(self) -> Stats:
+        s = Stats()
+        check(self.lib.crava_gpu_get_stats(self.handle, C.byref(s)), "get_stats")
+        return s
+
+    def kz_tables(self):
+        nzp, nt = self.case.nzp, self.case.ntheta
+        n = nzp * nt
+        wd = np.zeros(2 * n, np.float32); e1 = np.zeros(2 * n, np.float32)
+        e2 = np.zeros(2 * n, np.float32); e3 = np.zeros(n, np.float32)
+        inv = np.zeros(nzp, np.int32)
+        check(self.lib.crava_gpu_kz_tables(self.handle, wd.ctypes.data_as(F32P), e1.ctypes.data_as(F32P),
+                                           e2.ctypes.data_as(F32P), e3.ctypes.data_as(F32P),
+                                           inv.ctypes.data_as(C.POINTER(C.c_int))), "kz_tables")
+        cpx = lambda a: a.view(np.complex64).reshape(nzp, nt)
+        return cpx(wd), cpx(e1), cpx(e2), e3.reshape(nzp, nt), inv
+
+    def set_kz_tables(self, tables):
+        wd, e1, e2, e3, inv = tables
+        f32 = lambda a: np.ascontiguousarray(a.view(np.float32) if a.dtype == np.complex64 else a,
+                                             dtype=np.float32)
+        wd, e1, e2, e3 = f32(wd), f32(e1), f32(e2), f32(e3)
+        inv = np.ascontiguousarray(inv, dtype=np.int32)
+        check(self.lib.crava_gpu_set_kz_tables(self.handle, wd.ctypes.data_as(F32P), e1.ctypes.data_as(F32P),
+                                               e2.ctypes.data_as(F32P), e3.ctypes.data_as(F32P),
+                                               inv.ctypes.data_as(C.POINTER(C.c_int))), "set_kz_tables")
+
+
+def to_device(arr, device=0):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).to(f"cuda:{device}")
+
+
+def complex_view(t, nxp):
+    """[nzp, nyp, rnxp] float tensor/array -> [nzp, nyp, cnxp] complex view."""
+    if isinstance(t, np.ndarray):
+        return t.view(np.complex64)[..., : nxp // 2 + 1]
+    import torch
+
+    return torch.view_as_complex(t.view(*t.shape[:-1], -1, 2))[..., : nxp // 2 + 1]
+
+
+class FFTGrid:
+    """A padded grid resident in HBM -- the device counterpart of the
+    reference's FFTGrid (src/fftgrid.h): same layout, same grid types,
+    fftInPlace / invFFTInPlace with the same scalings."""
+
+    def __init__(self, ctx: Context, values=None, grid_type: int = PARAMETER):
+        import torch
+
+        c = ctx.case
+        self.ctx = ctx
+        self.nxp, self.nyp, self.nzp = c.nxp, c.nyp, c.nzp
+        self.type = grid_type
+        shape = (c.nzp, c.nyp, 2 * (c.nxp // 2 + 1))
+        if values is None:
+            self.t = torch.zeros(shape, dtype=torch.float32, device=f"cuda:{ctx.device}")
+        else:
+            self.t = to_device(np.asarray(values, dtype=np.float32).reshape(shape), ctx.device)
+        self.is_transformed = False
+
+    def setType(self, grid_type):
+        self.type = grid_type
+
+    def getType(self):
+        return self.type
+
+    def getIsTransformed(self):
+        return self.is_transformed
+
+    def fftInPlace(self):
+        assert not self.is_transformed
+        self.ctx.fft_r2c(self.t, self.type)
+        self.is_transformed = True
+
+    def invFFTInPlace(self):
+        assert self.is_transformed
+        self.ctx.fft_c2r(self.t, self.type)
+        self.is_transformed = False
+
+    def numpy(self):
+        return self.t.cpu().numpy()
+
+
+class Crava:
+    """The hot path of the reference's Crava on device grids.
+
+    computePostMeanResidAndFFTCov: transformed means / stacks in, posterior
+    mean (real domain), residual (transformed) and posterior covariance
+    (transformed) out, as src/crava.cpp:887-1295 leaves them (the means are
+    inverse transformed at :1181-1183; residuals and covariances stay in the
+    Fourier domain)."""
+
+    def __init__(self, ctx: Context, mu, data, cov, err_corr):
+        self.ctx = ctx
+        self.mu, self.data, self.cov, self.err = mu, data, cov, err_corr
+
+    def computePostMeanResidAndFFTCov(self, precision=None):
+        for g in self.cov + [self.err]:
+            if not g.getIsTransformed():
+                g.fftInPlace()
+        self.ctx.posterior([g.t for g in self.mu], [g.t for g in self.data],
+                           [g.t for g in self.cov], self.err.t, precision)
+        for g in self.mu:
+            g.invFFTInPlace()
+        return 0
+
+    def getPostAlpha(self):
+        return self.mu[0]
+
+    def getPostBeta(self):
+        return self.mu[1]
+
+    def getPostRho(self):
+        return self.mu[2]
+
+    def simulate(self, seed, n_sim, first_index=0):
+        """n_sim realisations (list of [alpha, beta, rho] FFTGrids)."""
+        ctx = self.ctx
+        outs = [FFTGrid(ctx, grid_type=PARAMETER) for _ in range(3 * n_sim)]
+        ctx.simulate([g.t for g in self.cov], [g.t for g in self.mu], seed, first_index,
+                     [o.t for o in outs])
+        return [outs[3 * r: 3 * r + 3] for r in range(n_sim)]

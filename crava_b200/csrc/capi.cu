@@ -1,0 +1,442 @@
+// capi.cu -- the C ABI (include/crava_gpu.h): contexts, argument checks,
+// stream ordering, statistics and the host-buffer entry point.
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+#include "sim.cuh"
+#include "solve.cuh"
+
+namespace crava {
+
+static std::atomic<long long> g_launches{0};
+void note_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches() { return g_launches.load(std::memory_order_relaxed); }
+
+static thread_local std::string g_last_error;
+void set_last_error(cudaError_t e, const char *what, const char *file, int line) {
+  char buf[512];
+  std::snprintf(buf, sizeof buf, "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  g_last_error = buf;
+}
+
+}  // namespace crava
+
+using namespace crava;
+
+struct crava_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  crava_gpu_params p{};
+  std::vector<float> wavelet, wnorm, A;
+  std::vector<double> theta, var0;
+  Geom g{};
+  FftPlans plans{};
+  KzTables tables{};
+  SolveConsts consts{};
+  DevCounters *counters = nullptr;  // device
+  cudaEvent_t ev[4] = {};           // start, after forward, after solve, end
+  bool timed = false;               // events of the last call are valid
+  // host-buffer path
+  float *work = nullptr;  // (10 + ntheta) grids
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> grid_ev;
+};
+
+namespace {
+
+int check_ctx(const crava_gpu_ctx *c) { return c ? CRAVA_GPU_OK : CRAVA_GPU_ERR_ARG; }
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    else prev = -1;
+  }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+bool smooth_2357(int n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+int validate(const crava_gpu_params *p) {
+  if (!p) return CRAVA_GPU_ERR_ARG;
+  if (p->nxp < 2 || p->nyp < 1 || p->nzp < 2) return CRAVA_GPU_ERR_ARG;
+  if (!smooth_2357(p->nxp) || !smooth_2357(p->nyp) || !smooth_2357(p->nzp)) return CRAVA_GPU_ERR_ARG;
+  // line lengths held in shared memory by the transform kernels
+  if (p->nxp > 8192 || p->nyp > 4096 || p->nzp > 4096) return CRAVA_GPU_ERR_ARG;
+  if (p->ntheta < 1 || p->ntheta > CRAVA_GPU_MAX_THETA) return CRAVA_GPU_ERR_ARG;
+  if (!p->wavelet || !p->A || !p->theta_cov || !p->var0) return CRAVA_GPU_ERR_ARG;
+  if (p->nz < 1 || !(p->lz > 0.0)) return CRAVA_GPU_ERR_ARG;
+  if (p->precision < CRAVA_SOLVE_FP64 || p->precision > CRAVA_SOLVE_FP32) return CRAVA_GPU_ERR_ARG;
+  return CRAVA_GPU_OK;
+}
+
+SolveGrids to_solve_grids(const crava_gpu_grids *gr, int nt) {
+  SolveGrids s{};
+  for (int q = 0; q < 3; ++q) s.mu[q] = reinterpret_cast<float2 *>(gr->mu[q]);
+  for (int l = 0; l < nt; ++l) s.data[l] = reinterpret_cast<float2 *>(gr->data[l]);
+  for (int t = 0; t < 6; ++t) s.cov[t] = reinterpret_cast<float2 *>(gr->cov[t]);
+  s.err = reinterpret_cast<const float2 *>(gr->err_corr);
+  return s;
+}
+
+int check_grids(const crava_gpu_ctx *c, const crava_gpu_grids *gr) {
+  if (!gr) return CRAVA_GPU_ERR_ARG;
+  for (int q = 0; q < 3; ++q) if (!gr->mu[q]) return CRAVA_GPU_ERR_ARG;
+  for (int l = 0; l < c->p.ntheta; ++l) if (!gr->data[l]) return CRAVA_GPU_ERR_ARG;
+  for (int t = 0; t < 6; ++t) if (!gr->cov[t]) return CRAVA_GPU_ERR_ARG;
+  if (!gr->err_corr) return CRAVA_GPU_ERR_ARG;
+  // float2 access needs 8-byte alignment
+  auto mis = [](const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 7u) != 0; };
+  for (int q = 0; q < 3; ++q) if (mis(gr->mu[q])) return CRAVA_GPU_ERR_ARG;
+  for (int l = 0; l < c->p.ntheta; ++l) if (mis(gr->data[l])) return CRAVA_GPU_ERR_ARG;
+  for (int t = 0; t < 6; ++t) if (mis(gr->cov[t])) return CRAVA_GPU_ERR_ARG;
+  if (mis(gr->err_corr)) return CRAVA_GPU_ERR_ARG;
+  return CRAVA_GPU_OK;
+}
+
+int valid_precision(int prec) {
+  return prec >= CRAVA_SOLVE_FP64 && prec <= CRAVA_SOLVE_FP32;
+}
+
+int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision, bool timed) {
+  const cudaStream_t s = c->stream;
+  const int nt = c->p.ntheta;
+  int rc;
+  CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
+  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  for (int q = 0; q < 3; ++q)
+    if ((rc = fft3d_r2c(c->plans, gr->mu[q], CRAVA_GRID_PARAMETER, s))) return rc;
+  for (int l = 0; l < nt; ++l)
+    if ((rc = fft3d_r2c(c->plans, gr->data[l], CRAVA_GRID_DATA, s))) return rc;
+  for (int t = 0; t < 6; ++t)
+    if ((rc = fft3d_r2c(c->plans, gr->cov[t], CRAVA_GRID_COVARIANCE, s))) return rc;
+  if ((rc = fft3d_r2c(c->plans, gr->err_corr, CRAVA_GRID_COVARIANCE, s))) return rc;
+  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  SolveGrids sg = to_solve_grids(gr, nt);
+  if ((rc = posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
+                            precision, c->counters, s)))
+    return rc;
+  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  for (int q = 0; q < 3; ++q)
+    if ((rc = fft3d_c2r(c->plans, gr->mu[q], CRAVA_GRID_PARAMETER, s))) return rc;
+  for (int l = 0; l < nt; ++l)
+    if ((rc = fft3d_c2r(c->plans, gr->data[l], CRAVA_GRID_DATA, s))) return rc;
+  for (int t = 0; t < 6; ++t)
+    if ((rc = fft3d_c2r(c->plans, gr->cov[t], CRAVA_GRID_COVARIANCE, s))) return rc;
+  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  c->timed = timed;
+  return CRAVA_GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *crava_gpu_status_string(int status) {
+  switch (status) {
+    case CRAVA_GPU_OK: return "ok";
+    case CRAVA_GPU_ERR_ARG: return "invalid argument";
+    case CRAVA_GPU_ERR_ALLOC: return "allocation failed";
+    case CRAVA_GPU_ERR_CUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
+    case CRAVA_GPU_ERR_TIMEOUT: return "device wait timed out";
+    case CRAVA_GPU_ERR_STATE: return "call out of order";
+    case CRAVA_GPU_ERR_NODEV: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+long long crava_gpu_launch_count(void) { return launches(); }
+
+int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
+                     crava_gpu_ctx **out) {
+  if (!out) return CRAVA_GPU_ERR_ARG;
+  *out = nullptr;
+  int rc = validate(params);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return CRAVA_GPU_ERR_NODEV;
+  if (device < 0 || device >= ndev) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(device);
+  auto *c = new (std::nothrow) crava_gpu_ctx();
+  if (!c) return CRAVA_GPU_ERR_ALLOC;
+  c->device = device;
+  c->stream = static_cast<cudaStream_t>(stream);
+  c->p = *params;
+  const int nt = params->ntheta, nzp = params->nzp;
+  c->wavelet.assign(params->wavelet, params->wavelet + (size_t)nt * nzp);
+  if (params->wavelet_norm) c->wnorm.assign(params->wavelet_norm, params->wavelet_norm + nt);
+  c->A.assign(params->A, params->A + 3 * nt);
+  c->theta.assign(params->theta_cov, params->theta_cov + nt * nt);
+  c->var0.assign(params->var0, params->var0 + 9);
+  c->p.wavelet = c->wavelet.data();
+  c->p.wavelet_norm = c->wnorm.empty() ? nullptr : c->wnorm.data();
+  c->p.A = c->A.data();
+  c->p.theta_cov = c->theta.data();
+  c->p.var0 = c->var0.data();
+  c->g = Geom::make(params->nxp, params->nyp, params->nzp);
+  c->consts.nt = nt;
+  c->consts.wnc = params->wnc;
+  for (int l = 0; l < nt; ++l) {
+    for (int q = 0; q < 3; ++q) c->consts.A[l][q] = c->A[3 * l + q];
+    for (int m = 0; m < nt; ++m) c->consts.theta[l][m] = c->theta[l * nt + m];
+  }
+  const double *v = c->var0.data();
+  c->consts.var0[0] = v[0]; c->consts.var0[1] = v[4]; c->consts.var0[2] = v[8];
+  c->consts.var0[3] = v[1]; c->consts.var0[4] = v[2]; c->consts.var0[5] = v[5];
+
+  auto fail = [&](int code) { crava_gpu_destroy(c); return code; };
+  if ((rc = fft_plans_create(c->g, &c->plans))) return fail(rc);
+  if ((rc = kz_tables_alloc(nzp, nt, &c->tables))) return fail(rc);
+  if (cudaMalloc(&c->counters, sizeof(DevCounters)) != cudaSuccess) return fail(CRAVA_GPU_ERR_ALLOC);
+  for (auto &e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+  if ((rc = kz_tables_build(c->p, &c->tables, c->stream))) return fail(rc);
+  *out = c;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_destroy(crava_gpu_ctx *c) {
+  if (!c) return CRAVA_GPU_OK;
+  DeviceGuard guard(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  else cudaDeviceSynchronize();
+  fft_plans_destroy(&c->plans);
+  kz_tables_free(&c->tables);
+  cudaFree(c->counters);
+  cudaFree(c->work);
+  for (auto &e : c->ev) if (e) cudaEventDestroy(e);
+  for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
+  delete c;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_fft_r2c(crava_gpu_ctx *c, float *grid, int type) {
+  if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
+  if (type < CRAVA_GRID_DATA || type > CRAVA_GRID_COVARIANCE) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  return fft3d_r2c(c->plans, grid, type, c->stream);
+}
+
+int crava_gpu_fft_c2r(crava_gpu_ctx *c, float *grid, int type) {
+  if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
+  if (type < CRAVA_GRID_DATA || type > CRAVA_GRID_COVARIANCE) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  return fft3d_c2r(c->plans, grid, type, c->stream);
+}
+
+int crava_gpu_posterior(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {
+  int rc;
+  if ((rc = check_ctx(c)) || (rc = check_grids(c, gr))) return rc;
+  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), c->stream));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
+  SolveGrids sg = to_solve_grids(gr, c->p.ntheta);
+  rc = posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
+                       precision, c->counters, c->stream);
+  if (rc) return rc;
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
+  c->timed = true;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_posterior_unit(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {
+  int rc;
+  if ((rc = check_ctx(c)) || (rc = check_grids(c, gr))) return rc;
+  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  return run_unit(c, gr, precision, true);
+}
+
+int crava_gpu_host_register(void *ptr, uint64_t bytes) {
+  if (!ptr || !bytes) return CRAVA_GPU_ERR_ARG;
+  cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault);
+  if (e != cudaSuccess) { set_last_error(e, "cudaHostRegister", __FILE__, __LINE__); return CRAVA_GPU_ERR_CUDA; }
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_host_unregister(void *ptr) {
+  if (!ptr) return CRAVA_GPU_ERR_ARG;
+  cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) { set_last_error(e, "cudaHostUnregister", __FILE__, __LINE__); return CRAVA_GPU_ERR_CUDA; }
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, int precision) {
+  int rc;
+  if ((rc = check_ctx(c)) || (rc = check_grids(c, hg))) return rc;
+  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  const int nt = c->p.ntheta, ngrid = 10 + nt;
+  const size_t gbytes = (size_t)c->g.rsize * sizeof(float);
+  if (!c->work) {
+    if (cudaMalloc(&c->work, gbytes * ngrid) != cudaSuccess) { c->work = nullptr; return CRAVA_GPU_ERR_ALLOC; }
+    CRAVA_CUDA_TRY(cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
+    CRAVA_CUDA_TRY(cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
+    c->grid_ev.assign(2 * ngrid + 1, nullptr);
+    for (auto &e : c->grid_ev) CRAVA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  // device grids, in ABI order: mu(3), data(nt), cov(6), err
+  crava_gpu_grids dg{};
+  std::vector<float *> host(ngrid), dev(ngrid);
+  std::vector<int> type(ngrid);
+  int i = 0;
+  for (int q = 0; q < 3; ++q, ++i) { host[i] = hg->mu[q]; type[i] = CRAVA_GRID_PARAMETER; }
+  for (int l = 0; l < nt; ++l, ++i) { host[i] = hg->data[l]; type[i] = CRAVA_GRID_DATA; }
+  for (int t = 0; t < 6; ++t, ++i) { host[i] = hg->cov[t]; type[i] = CRAVA_GRID_COVARIANCE; }
+  host[i] = hg->err_corr; type[i] = CRAVA_GRID_COVARIANCE;
+  for (int k = 0; k < ngrid; ++k) dev[k] = c->work + (size_t)k * c->g.rsize;
+  i = 0;
+  for (int q = 0; q < 3; ++q) dg.mu[q] = dev[i++];
+  for (int l = 0; l < nt; ++l) dg.data[l] = dev[i++];
+  for (int t = 0; t < 6; ++t) dg.cov[t] = dev[i++];
+  dg.err_corr = dev[i];
+
+  const cudaStream_t s = c->stream;
+  CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  // the copy stream must not overtake earlier work on the compute stream
+  CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[2 * ngrid], s));
+  CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->grid_ev[2 * ngrid], 0));
+  for (int k = 0; k < ngrid; ++k) {
+    CRAVA_CUDA_TRY(cudaMemcpyAsync(dev[k], host[k], gbytes, cudaMemcpyHostToDevice, c->s_in));
+    CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[k], c->s_in));
+    CRAVA_CUDA_TRY(cudaStreamWaitEvent(s, c->grid_ev[k], 0));
+    if ((rc = fft3d_r2c(c->plans, dev[k], type[k], s))) return rc;
+  }
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  SolveGrids sg = to_solve_grids(&dg, nt);
+  if ((rc = posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
+                            precision, c->counters, s)))
+    return rc;
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  for (int k = 0; k < ngrid - 1; ++k) {  // the noise correlation is not an output
+    if ((rc = fft3d_c2r(c->plans, dev[k], type[k], s))) return rc;
+    CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[ngrid + k], s));
+    CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->grid_ev[ngrid + k], 0));
+    CRAVA_CUDA_TRY(cudaMemcpyAsync(host[k], dev[k], gbytes, cudaMemcpyDeviceToHost, c->s_out));
+  }
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  c->timed = true;
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->s_out));
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_noise_fill(crava_gpu_ctx *c, float *grid, uint64_t seed, uint64_t stream_id) {
+  if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  return noise_fill(c->g, reinterpret_cast<float2 *>(grid), seed, stream_id, c->stream);
+}
+
+int crava_gpu_sim_filter(crava_gpu_ctx *c, const float *const cov[6], float *const seed[3]) {
+  if (check_ctx(c) || !cov || !seed) return CRAVA_GPU_ERR_ARG;
+  const float2 *cv[6];
+  float2 *sd[3];
+  for (int t = 0; t < 6; ++t) {
+    if (!cov[t] || (reinterpret_cast<uintptr_t>(cov[t]) & 7u)) return CRAVA_GPU_ERR_ARG;
+    cv[t] = reinterpret_cast<const float2 *>(cov[t]);
+  }
+  for (int q = 0; q < 3; ++q) {
+    if (!seed[q] || (reinterpret_cast<uintptr_t>(seed[q]) & 7u)) return CRAVA_GPU_ERR_ARG;
+    sd[q] = reinterpret_cast<float2 *>(seed[q]);
+  }
+  DeviceGuard guard(c->device);
+  CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), c->stream));
+  c->timed = false;
+  return sim_filter(c->g, cv, sd, c->counters, c->stream);
+}
+
+int crava_gpu_simulate(crava_gpu_ctx *c, const float *const cov[6], const float *const post_mean[3],
+                       uint64_t seed, int first_index, int count, float *const *out) {
+  if (check_ctx(c) || !cov || !post_mean || !out || count < 0 || first_index < 0) return CRAVA_GPU_ERR_ARG;
+  const float2 *cv[6];
+  for (int t = 0; t < 6; ++t) {
+    if (!cov[t] || (reinterpret_cast<uintptr_t>(cov[t]) & 7u)) return CRAVA_GPU_ERR_ARG;
+    cv[t] = reinterpret_cast<const float2 *>(cov[t]);
+  }
+  for (int q = 0; q < 3; ++q)
+    if (!post_mean[q] || (reinterpret_cast<uintptr_t>(post_mean[q]) & 7u)) return CRAVA_GPU_ERR_ARG;
+  for (int r = 0; r < 3 * count; ++r)
+    if (!out[r] || (reinterpret_cast<uintptr_t>(out[r]) & 7u)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  const cudaStream_t s = c->stream;
+  int rc;
+  CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  for (int r = 0; r < count; ++r) {
+    float2 *o[3];
+    for (int q = 0; q < 3; ++q) o[q] = reinterpret_cast<float2 *>(out[3 * r + q]);
+    const uint64_t stream0 = 3ull * (uint64_t)(first_index + r);
+    if ((rc = noise_filter(c->g, cv, o, seed, stream0, c->counters, s))) return rc;
+    for (int q = 0; q < 3; ++q)
+      if ((rc = fft3d_c2r(c->plans, out[3 * r + q], CRAVA_GRID_PARAMETER, s, post_mean[q]))) return rc;
+  }
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  c->timed = true;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_get_stats(crava_gpu_ctx *c, crava_gpu_stats *st) {
+  if (check_ctx(c) || !st) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  DevCounters h{};
+  CRAVA_CUDA_TRY(cudaMemcpy(&h, c->counters, sizeof h, cudaMemcpyDeviceToHost));
+  std::memset(st, 0, sizeof *st);
+  st->chol_fail_bins = (long long)h.chol_fail;
+  st->nonfinite_bins = (long long)h.nonfinite;
+  if (c->timed) {
+    cudaEventElapsedTime(&st->ms_forward, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&st->ms_solve, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&st->ms_inverse, c->ev[2], c->ev[3]);
+    cudaEventElapsedTime(&st->ms_total, c->ev[0], c->ev[3]);
+  }
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_kz_tables(crava_gpu_ctx *c, float *wd, float *e1, float *e2, float *e3, int *inv) {
+  if (check_ctx(c) || !wd || !e1 || !e2 || !e3 || !inv) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  const size_t n = (size_t)c->p.nzp * c->p.ntheta;
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CRAVA_CUDA_TRY(cudaMemcpy(wd, c->tables.wd, n * sizeof(float2), cudaMemcpyDeviceToHost));
+  CRAVA_CUDA_TRY(cudaMemcpy(e1, c->tables.e1, n * sizeof(float2), cudaMemcpyDeviceToHost));
+  CRAVA_CUDA_TRY(cudaMemcpy(e2, c->tables.e2, n * sizeof(float2), cudaMemcpyDeviceToHost));
+  CRAVA_CUDA_TRY(cudaMemcpy(e3, c->tables.e3, n * sizeof(float), cudaMemcpyDeviceToHost));
+  CRAVA_CUDA_TRY(cudaMemcpy(inv, c->tables.inv, (size_t)c->p.nzp * sizeof(int), cudaMemcpyDeviceToHost));
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_set_kz_tables(crava_gpu_ctx *c, const float *wd, const float *e1, const float *e2,
+                            const float *e3, const int *inv) {
+  if (check_ctx(c) || !wd || !e1 || !e2 || !e3 || !inv) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  const size_t n = (size_t)c->p.nzp * c->p.ntheta;
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CRAVA_CUDA_TRY(cudaMemcpy(c->tables.wd, wd, n * sizeof(float2), cudaMemcpyHostToDevice));
+  CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e1, e1, n * sizeof(float2), cudaMemcpyHostToDevice));
+  CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e2, e2, n * sizeof(float2), cudaMemcpyHostToDevice));
+  CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e3, e3, n * sizeof(float), cudaMemcpyHostToDevice));
+  CRAVA_CUDA_TRY(cudaMemcpy(c->tables.inv, inv, (size_t)c->p.nzp * sizeof(int), cudaMemcpyHostToDevice));
+  return CRAVA_GPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,350 @@
+// fft.cu -- 3-D real<->complex transforms on the reference's padded layout.
+//
+// Replaces FFTGrid::fftInPlace / invFFTInPlace (src/fftgrid.cpp:1803-1862),
+// which call FFTW 2.1.2's rfftw3d (real-to-half-complex along x, complex
+// along y and z, unnormalised, forward sign -) and scale by 1/sqrt(N)
+// (DATA, PARAMETER) or 1 forward / 1/N inverse (COVARIANCE).
+//
+// Three passes, each one read and one write of the grid:
+//   rows  (x): each CTA transforms ROWS rows of nxp reals; an even nxp is
+//              done as one nxp/2-point complex FFT of the packed row and a
+//              split step (the row's float pairs are read as float2).
+//   cols  (y): each CTA transforms TX adjacent x-columns of one z-plane.
+//   cols  (z): each CTA transforms TX adjacent x-columns of one y-row.
+// Lines live in shared memory and go through the Stockham engine of
+// fft_core.cuh.  The scalings are fused into the first (forward) or last
+// (inverse) pass.
+#include <math.h>
+#include <stdio.h>
+
+#include <vector>
+
+#include "fft.cuh"
+#include "fft_core.cuh"
+
+namespace crava {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRows = 16;    // rows per CTA in the x pass
+constexpr int kColTile = 8;  // x-columns per CTA in the y / z passes
+
+struct RowArgs {
+  float *grid;
+  long long nrows;  // nyp * nzp
+  int rnxp;         // floats per row
+  int nxp;
+  RadixList rl;     // line length: nxp/2 (even) or nxp (odd)
+  const float2 *tw;
+  const float2 *post;  // e^{-2 pi i k/nxp}, k <= nxp/2 (even nxp)
+  const float *addend; // inverse only: real grid added to the output (or null)
+  float scale;
+};
+
+struct ColArgs {
+  float2 *data;
+  int ninner;              // cnxp
+  long long elem_stride;   // between consecutive line elements (float2)
+  long long outer_stride;  // between CTAs along blockIdx.y (float2)
+  RadixList rl;
+  const float2 *tw;
+  float scale;
+};
+
+// ------------------------------------------------------------------ x pass
+template <int DIR, bool EVEN>
+__global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = a.rl.n;            // complex line length
+  const int ld = n + 1;            // shared row pitch
+  float2 *twl = sm;                // n
+  float2 *post = twl + n;          // n + 1 (even only)
+  float2 *bufA = post + (EVEN ? n + 1 : 0);
+  float2 *bufB = bufA + kRows * ld;
+  const long long row0 = (long long)blockIdx.x * kRows;
+  const int nrows = (int)min((long long)kRows, a.nrows - row0);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n; i += blockDim.x) twl[i] = a.tw[i];
+  if (EVEN)
+    for (int i = tid; i <= n; i += blockDim.x) post[i] = a.post[i];
+  __syncthreads();
+
+  if (DIR < 0) {
+    // forward: load
+    for (int idx = tid; idx < kRows * n; idx += blockDim.x) {
+      int r = idx / n, m = idx % n;
+      float2 v = make_float2(0.f, 0.f);
+      if (r < nrows) {
+        const float *row = a.grid + (row0 + r) * a.rnxp;
+        if (EVEN) v = reinterpret_cast<const float2 *>(row)[m];
+        else v = make_float2(row[m], 0.f);
+        v = cscale(v, a.scale);
+      }
+      bufA[r * ld + m] = v;
+    }
+  } else {
+    // inverse: load the half spectrum and build the line to transform
+    for (int idx = tid; idx < kRows * n; idx += blockDim.x) {
+      int r = idx / n, k = idx % n;
+      float2 v = make_float2(0.f, 0.f);
+      if (r < nrows) {
+        const float2 *X = reinterpret_cast<const float2 *>(a.grid + (row0 + r) * a.rnxp);
+        if (EVEN) {
+          // Z'[k] = (X_k + conj X_{h-k}) + i W^{-k} (X_k - conj X_{h-k}),
+          // imaginary parts of DC and Nyquist ignored.
+          float2 xk = X[k], xm = X[n - k];
+          if (k == 0) { xk.y = 0.f; xm.y = 0.f; }
+          xm.y = -xm.y;
+          float2 e = cadd(xk, xm);
+          float2 w = post[k];
+          w.y = -w.y;  // W^{-k}
+          float2 o = cmul(csub(xk, xm), w);
+          v = make_float2(e.x - o.y, e.y + o.x);
+        } else {
+          const int c = n / 2 + 1;
+          if (k == 0) v = make_float2(X[0].x, 0.f);
+          else if (k < c) v = X[k];
+          else { v = X[n - k]; v.y = -v.y; }
+        }
+      }
+      bufA[r * ld + k] = v;
+    }
+  }
+  __syncthreads();
+  int which = stockham_lines<DIR>(bufA, bufB, a.rl.r, a.rl.nr, n, twl, kRows, ld, 1, false);
+  const float2 *res = which ? bufB : bufA;
+
+  if (DIR < 0) {
+    if (EVEN) {
+      // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{h-k})/2, O = -i (Z_k - conj Z_{h-k})/2
+      for (int idx = tid; idx < kRows * (n + 1); idx += blockDim.x) {
+        int r = idx / (n + 1), k = idx % (n + 1);
+        if (r >= nrows) continue;
+        float2 zk = res[r * ld + (k == n ? 0 : k)];
+        float2 zm = res[r * ld + (k == 0 ? 0 : n - k)];
+        zm.y = -zm.y;
+        float2 e = cscale(cadd(zk, zm), 0.5f);
+        float2 d = csub(zk, zm);
+        float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        float2 X = cadd(e, cmul(post[k], o));
+        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = X;
+      }
+    } else {
+      const int c = n / 2 + 1;
+      for (int idx = tid; idx < kRows * c; idx += blockDim.x) {
+        int r = idx / c, k = idx % c;
+        if (r >= nrows) continue;
+        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = res[r * ld + k];
+      }
+    }
+  } else {
+    if (EVEN) {
+      for (int idx = tid; idx < kRows * (n + 1); idx += blockDim.x) {
+        int r = idx / (n + 1), m = idx % (n + 1);
+        if (r >= nrows) continue;
+        float2 v = make_float2(0.f, 0.f);
+        if (m < n) {
+          v = cscale(res[r * ld + m], a.scale);
+          if (a.addend) v = cadd(v, reinterpret_cast<const float2 *>(a.addend + (row0 + r) * a.rnxp)[m]);
+        }
+        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[m] = v;
+      }
+    } else {
+      for (int idx = tid; idx < kRows * (n + 1); idx += blockDim.x) {
+        int r = idx / (n + 1), m = idx % (n + 1);
+        if (r >= nrows) continue;
+        float v = 0.f;
+        if (m < n) {
+          v = res[r * ld + m].x * a.scale;
+          if (a.addend) v += a.addend[(row0 + r) * a.rnxp + m];
+        }
+        a.grid[(row0 + r) * a.rnxp + m] = v;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ y / z pass
+template <int DIR>
+__global__ void __launch_bounds__(kThreads) k_cols(ColArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = a.rl.n;
+  float2 *twl = sm;
+  float2 *bufA = twl + n;
+  float2 *bufB = bufA + kColTile * n;
+  const int x0 = blockIdx.x * kColTile;
+  const int nx = min(kColTile, a.ninner - x0);
+  float2 *base = a.data + (long long)blockIdx.y * a.outer_stride + x0;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n; i += blockDim.x) twl[i] = a.tw[i];
+  for (int idx = tid; idx < kColTile * n; idx += blockDim.x) {
+    int t = idx % kColTile, m = idx / kColTile;
+    bufA[m * kColTile + t] = t < nx ? base[m * a.elem_stride + t] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  int which = stockham_lines<DIR>(bufA, bufB, a.rl.r, a.rl.nr, n, twl, kColTile, 1, kColTile, true);
+  const float2 *res = which ? bufB : bufA;
+  for (int idx = tid; idx < kColTile * n; idx += blockDim.x) {
+    int t = idx % kColTile, m = idx / kColTile;
+    if (t < nx) base[m * a.elem_stride + t] = cscale(res[m * kColTile + t], a.scale);
+  }
+}
+
+int set_smem(const void *fn, size_t bytes) {
+  static int dev_max = -1;
+  if (dev_max < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  }
+  if ((long)bytes > dev_max) return CRAVA_GPU_ERR_ARG;
+  if (bytes > 48 * 1024) CRAVA_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return CRAVA_GPU_OK;
+}
+
+int line_plan_create(int n, LinePlan *p) {
+  if (!radix_list(n, &p->rl)) return CRAVA_GPU_ERR_ARG;
+  std::vector<float2> tw(n);
+  for (int k = 0; k < n; ++k) {
+    double ang = -2.0 * M_PI * (double)k / (double)n;
+    tw[k] = make_float2((float)cos(ang), (float)sin(ang));
+  }
+  CRAVA_CUDA_TRY(cudaMalloc(&p->tw, sizeof(float2) * n));
+  CRAVA_CUDA_TRY(cudaMemcpy(p->tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  return CRAVA_GPU_OK;
+}
+
+}  // namespace
+
+bool radix_list(int n, RadixList *out) {
+  out->n = n;
+  out->nr = 0;
+  if (n < 1) return false;
+  int m = n;
+  // radix 8 while possible, then 4, then 2; then the odd primes.
+  while (m % 8 == 0) { out->r[out->nr++] = 8; m /= 8; }
+  while (m % 4 == 0) { out->r[out->nr++] = 4; m /= 4; }
+  while (m % 2 == 0) { out->r[out->nr++] = 2; m /= 2; }
+  const int odd[3] = {3, 5, 7};
+  for (int i = 0; i < 3; ++i)
+    while (m % odd[i] == 0) {
+      if (out->nr >= 16) return false;
+      out->r[out->nr++] = odd[i];
+      m /= odd[i];
+    }
+  return m == 1 && out->nr <= 16;
+}
+
+float forward_scale(const Geom &g, int type) {
+  if (type == CRAVA_GRID_COVARIANCE) return 1.0f;
+  return 1.0f / sqrtf((float)(g.nxp * g.nyp * g.nzp));
+}
+float inverse_scale(const Geom &g, int type) {
+  if (type == CRAVA_GRID_COVARIANCE) return (float)(1.0 / ((double)g.nxp * g.nyp * g.nzp));
+  return (float)(1.0 / sqrt((float)(g.nxp * g.nyp * g.nzp)));
+}
+
+int fft_plans_create(const Geom &g, FftPlans *p) {
+  p->g = g;
+  p->x_even = (g.nxp % 2) == 0;
+  int rc;
+  if ((rc = line_plan_create(p->x_even ? g.nxp / 2 : g.nxp, &p->x))) return rc;
+  if ((rc = line_plan_create(g.nyp, &p->y))) return rc;
+  if ((rc = line_plan_create(g.nzp, &p->z))) return rc;
+  if (p->x_even) {
+    int h = g.nxp / 2;
+    std::vector<float2> post(h + 1);
+    for (int k = 0; k <= h; ++k) {
+      double ang = -2.0 * M_PI * (double)k / (double)g.nxp;
+      post[k] = make_float2((float)cos(ang), (float)sin(ang));
+    }
+    CRAVA_CUDA_TRY(cudaMalloc(&p->xpost, sizeof(float2) * (h + 1)));
+    CRAVA_CUDA_TRY(cudaMemcpy(p->xpost, post.data(), sizeof(float2) * (h + 1), cudaMemcpyHostToDevice));
+  }
+  return CRAVA_GPU_OK;
+}
+
+void fft_plans_destroy(FftPlans *p) {
+  cudaFree(p->x.tw); cudaFree(p->y.tw); cudaFree(p->z.tw); cudaFree(p->xpost);
+  p->x.tw = p->y.tw = p->z.tw = p->xpost = nullptr;
+}
+
+int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t s,
+             const float *addend) {
+  RowArgs a;
+  a.addend = addend;
+  a.grid = grid;
+  a.nrows = (long long)p.g.nyp * p.g.nzp;
+  a.rnxp = p.g.rnxp;
+  a.nxp = p.g.nxp;
+  a.rl = p.x.rl;
+  a.tw = p.x.tw;
+  a.post = p.xpost;
+  a.scale = scale;
+  const int n = a.rl.n;
+  size_t smem = sizeof(float2) * (n + (p.x_even ? n + 1 : 0) + 2 * kRows * (n + 1));
+  dim3 grd((unsigned)((a.nrows + kRows - 1) / kRows));
+  const void *fn;
+  if (dir < 0) fn = p.x_even ? (const void *)k_rows<-1, true> : (const void *)k_rows<-1, false>;
+  else fn = p.x_even ? (const void *)k_rows<1, true> : (const void *)k_rows<1, false>;
+  int rc = set_smem(fn, smem);
+  if (rc) return rc;
+  if (dir < 0) {
+    if (p.x_even) k_rows<-1, true><<<grd, kThreads, smem, s>>>(a);
+    else k_rows<-1, false><<<grd, kThreads, smem, s>>>(a);
+  } else {
+    if (p.x_even) k_rows<1, true><<<grd, kThreads, smem, s>>>(a);
+    else k_rows<1, false><<<grd, kThreads, smem, s>>>(a);
+  }
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
+static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
+                long long outer_stride, int nouter, int dir, float scale, cudaStream_t s) {
+  ColArgs a;
+  a.data = data;
+  a.ninner = ninner;
+  a.elem_stride = es;
+  a.outer_stride = outer_stride;
+  a.rl = lp.rl;
+  a.tw = lp.tw;
+  a.scale = scale;
+  const int n = lp.rl.n;
+  size_t smem = sizeof(float2) * (n + 2 * kColTile * n);
+  dim3 grd((ninner + kColTile - 1) / kColTile, nouter);
+  const void *fn = dir < 0 ? (const void *)k_cols<-1> : (const void *)k_cols<1>;
+  int rc = set_smem(fn, smem);
+  if (rc) return rc;
+  if (dir < 0) k_cols<-1><<<grd, kThreads, smem, s>>>(a);
+  else k_cols<1><<<grd, kThreads, smem, s>>>(a);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
+int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
+  const Geom &g = p.g;
+  return cols(p.y, grid, g.cnxp, g.cnxp, (long long)g.cnxp * g.nyp, g.nzp, dir, 1.0f, s);
+}
+
+int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
+  const Geom &g = p.g;
+  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, s);
+}
+
+int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s) {
+  int rc;
+  if ((rc = fft_rows(p, grid, -1, forward_scale(p.g, type), s))) return rc;
+  if ((rc = fft_cols_y(p, reinterpret_cast<float2 *>(grid), -1, s))) return rc;
+  return fft_cols_z(p, reinterpret_cast<float2 *>(grid), -1, s);
+}
+
+int fft3d_c2r(const FftPlans &p, float *grid, int type, cudaStream_t s, const float *addend) {
+  int rc;
+  if ((rc = fft_cols_z(p, reinterpret_cast<float2 *>(grid), 1, s))) return rc;
+  if ((rc = fft_cols_y(p, reinterpret_cast<float2 *>(grid), 1, s))) return rc;
+  return fft_rows(p, grid, 1, inverse_scale(p.g, type), s, addend);
+}
+
+}  // namespace crava

@@ -1,0 +1,51 @@
+// fft.cuh -- 3-D real<->complex transforms on the reference's padded layout.
+#pragma once
+
+#include "common.cuh"
+
+namespace crava {
+
+// Radices of one line length, largest first (8, 4, 2, 3, 5, 7).
+struct RadixList {
+  int n;
+  int nr;
+  int r[16];
+};
+
+// Plan for one line length: radix list and twiddle table e^{-2 pi i k/n}
+// (n entries, float2) in device memory.
+struct LinePlan {
+  RadixList rl;
+  float2 *tw = nullptr;
+};
+
+// Plans of one grid geometry.
+struct FftPlans {
+  Geom g;
+  bool x_even = true;
+  LinePlan x;        // length nxp/2 (even nxp) or nxp (odd)
+  LinePlan y;        // length nyp
+  LinePlan z;        // length nzp
+  float2 *xpost = nullptr;  // e^{-2 pi i k/nxp}, k = 0..nxp/2 (even nxp)
+};
+
+bool radix_list(int n, RadixList *out);
+int fft_plans_create(const Geom &g, FftPlans *p);
+void fft_plans_destroy(FftPlans *p);
+
+// In-place transforms of one grid with the FFTGrid scaling of `type`.
+int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s);
+// addend (optional): real grid added to the output (posterior mean of a realisation).
+int fft3d_c2r(const FftPlans &p, float *grid, int type, cudaStream_t s,
+              const float *addend = nullptr);
+
+// Individual passes (used by the fused paths).
+int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t s,
+             const float *addend = nullptr);
+int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
+int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
+
+float forward_scale(const Geom &g, int type);
+float inverse_scale(const Geom &g, int type);
+
+}  // namespace crava

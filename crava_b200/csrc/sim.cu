@@ -1,0 +1,241 @@
+// sim.cu -- posterior realisations: seeded complex noise and the per-bin
+// Cholesky filter.  Compiled with -fmad=false so the FP32 filter rounds
+// like the reference's (libs/lib/lib_matr.c:78-167, 453-470).
+//
+// Replaces Crava::simulate (src/crava.cpp:1415-1599) per realisation:
+//   FFTGrid::fillInComplexNoise x3 (src/fftgrid.cpp:1213-1263),
+//   per bin: rebuild the Hermitian posterior 3x3 from 6 spectra, Cholesky,
+//   seed <- L seed, zero on failure (src/crava.cpp:1482-1521),
+//   invFFTInPlace x3 and add of the posterior mean (:1537-1573).
+// The reference draws the noise from one sequential LCG; here every bin's
+// value is a pure function of (seed, stream, bin) through Philox-4x32-10
+// (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2,
+// 3", SC 2011) and a Box-Muller transform, so realisations match the
+// reference in distribution, not in value.
+#include <math.h>
+
+#include "sim.cuh"
+
+namespace crava {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------- Philox-4x32-10
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox_round(U4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+  uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+  return U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+}
+
+__device__ __forceinline__ U4 philox10(U4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    c = philox_round(c, k0, k1);
+    k0 += W0; k1 += W1;
+  }
+  return c;
+}
+
+// Two independent N(0,1) values for (seed, stream, counter), Box-Muller.
+__device__ __forceinline__ float2 normal2(uint64_t seed, uint64_t stream, uint64_t ctr) {
+  U4 c{(uint32_t)ctr, (uint32_t)(ctr >> 32), (uint32_t)stream, (uint32_t)(stream >> 32)};
+  U4 r = philox10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  // u1 in (0, 1], u2 in [0, 1)
+  float u1 = ((float)(r.x >> 8) + 1.0f) * (1.0f / 16777216.0f);
+  float u2 = (float)(r.y >> 8) * (1.0f / 16777216.0f);
+  float rad = sqrtf(-2.0f * logf(u1));
+  float s, co;
+  sincospif(2.0f * u2, &s, &co);
+  return make_float2(rad * co, rad * s);
+}
+
+// The value FFTGrid::fillInComplexNoise puts in bin i (rules of
+// src/fftgrid.cpp:1221-1257, including the parity test on the linear index
+// for the last x plane).  Each independent draw is made at the counter of
+// the bin the reference draws it for; a mirrored bin re-draws its partner.
+__device__ __forceinline__ float2 noise_bin(long long i, int cnxp, int nyp, int nzp,
+                                            uint64_t seed, uint64_t stream) {
+  const float sd = 0.70710678118654752440f;  // float(1/sqrt(2.0))
+  const long long xs = i % cnxp;
+  if (xs == 0 || (xs == cnxp - 1 && (i % 2) == 1)) {
+    const long long jk = (i - xs) / cnxp;
+    const long long j = jk % nyp, k = jk / nyp;
+    const long long jc = j == 0 ? 0 : nyp - j, kc = k == 0 ? 0 : nzp - k;
+    const long long jkc = jc + kc * nyp;
+    if (jkc == jk) {
+      float2 n = normal2(seed, stream, (uint64_t)i);
+      return make_float2(n.x, 0.0f);
+    }
+    if (jkc > jk) {
+      float2 n = normal2(seed, stream, (uint64_t)i);
+      return make_float2(sd * n.x, sd * n.y);
+    }
+    const long long ci = jkc * cnxp + xs;
+    float2 n = normal2(seed, stream, (uint64_t)ci);
+    return make_float2(sd * n.x, -(sd * n.y));
+  }
+  float2 n = normal2(seed, stream, (uint64_t)i);
+  return make_float2(sd * n.x, sd * n.y);
+}
+
+__global__ void __launch_bounds__(kThreads) k_noise(float2 *g, long long csize, int cnxp, int nyp,
+                                                    int nzp, uint64_t seed, uint64_t stream) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < csize) g[i] = noise_bin(i, cnxp, nyp, nzp, seed, stream);
+}
+
+// lib_matrCholCpx on the 3x3 posterior covariance (reference operation order).
+__device__ __forceinline__ int chol3_ref(float2 (*m)[3]) {
+  float2 lr;
+  float help;
+  float factor = m[0][0].x;
+  if (factor <= 0) return 1;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { m[i][j].x = m[i][j].x / factor; m[i][j].y = m[i][j].y / factor; }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if ((double)m[i][i].x <= 1e-20) return 1;
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      lr.x = 0.0f; lr.y = 0.0f;
+#pragma unroll
+      for (int k = 0; k < j; ++k) {
+        lr.x += (m[i][k].x * m[j][k].x) + (m[i][k].y * m[j][k].y);
+        lr.y += -(m[i][k].x * m[j][k].y) + (m[i][k].y * m[j][k].x);
+      }
+      help = m[j][j].x * m[j][j].x + m[j][j].y * m[j][j].y;
+      m[i][j].x = ((m[i][j].x - lr.x) * m[j][j].x + (m[i][j].y - lr.y) * m[j][j].y) / help;
+      m[i][j].y = ((m[i][j].y - lr.y) * m[j][j].x - (m[i][j].x - lr.x) * m[j][j].y) / help;
+    }
+    lr.x = 0.0f;
+#pragma unroll
+    for (int k = 0; k < i; ++k) lr.x += (m[i][k].x * m[i][k].x) + (m[i][k].y * m[i][k].y);
+    lr.x = m[i][i].x - lr.x;
+    if ((double)lr.x <= 1e-20) return 1;
+    m[i][i].x = sqrtf(lr.x);
+    m[i][i].y = 0.0f;
+  }
+  const float sf = sqrtf(factor);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j <= i; ++j) { m[i][j].x *= sf; m[i][j].y *= sf; }
+  return 0;
+}
+
+// seed <- L seed (lib_matrProdCholVec), zero on failure.  Returns failure.
+__device__ __forceinline__ bool filter_bin(const float2 *const *cov, long long i, float2 z[3]) {
+  float2 P[3][3];
+  P[0][0] = cov[0][i]; P[1][1] = cov[1][i]; P[2][2] = cov[2][i];
+  P[0][1] = cov[3][i]; P[0][2] = cov[4][i]; P[1][2] = cov[5][i];
+  P[1][0] = make_float2(P[0][1].x, -P[0][1].y);
+  P[2][0] = make_float2(P[0][2].x, -P[0][2].y);
+  P[2][1] = make_float2(P[1][2].x, -P[1][2].y);
+  if (chol3_ref(P) == 0) {
+    float2 o[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      o[a] = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int b = 0; b < a + 1; ++b) {
+        o[a].x += P[a][b].x * z[b].x - P[a][b].y * z[b].y;
+        o[a].y += P[a][b].x * z[b].y + P[a][b].y * z[b].x;
+      }
+    }
+    z[0] = o[0]; z[1] = o[1]; z[2] = o[2];
+    return false;
+  }
+  z[0] = z[1] = z[2] = make_float2(0.0f, 0.0f);
+  return true;
+}
+
+struct FilterArgs {
+  const float2 *cov[6];
+  float2 *seed[3];
+  long long csize;
+  DevCounters *counters;
+};
+
+__device__ __forceinline__ void count_fail(DevCounters *c, bool fail) {
+  unsigned m = __activemask();
+  unsigned b = __ballot_sync(m, fail);
+  if (b && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&c->chol_fail, (unsigned long long)__popc(b));
+}
+
+__global__ void __launch_bounds__(kThreads) k_filter(FilterArgs a) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.csize) return;
+  float2 z[3] = {a.seed[0][i], a.seed[1][i], a.seed[2][i]};
+  bool f = filter_bin(a.cov, i, z);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) a.seed[q][i] = z[q];
+  if (a.counters) count_fail(a.counters, f);
+}
+
+struct NoiseFilterArgs {
+  const float2 *cov[6];
+  float2 *out[3];
+  long long csize;
+  int cnxp, nyp, nzp;
+  uint64_t seed, stream0;  // parameter p uses stream stream0 + p
+  DevCounters *counters;
+};
+
+__global__ void __launch_bounds__(kThreads) k_noise_filter(NoiseFilterArgs a) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.csize) return;
+  float2 z[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) z[q] = noise_bin(i, a.cnxp, a.nyp, a.nzp, a.seed, a.stream0 + q);
+  bool f = filter_bin(a.cov, i, z);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) a.out[q][i] = z[q];
+  if (a.counters) count_fail(a.counters, f);
+}
+
+}  // namespace
+
+int noise_fill(const Geom &g, float2 *grid, uint64_t seed, uint64_t stream, cudaStream_t s) {
+  dim3 grd((unsigned)((g.csize + kThreads - 1) / kThreads));
+  k_noise<<<grd, kThreads, 0, s>>>(grid, g.csize, g.cnxp, g.nyp, g.nzp, seed, stream);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
+int sim_filter(const Geom &g, const float2 *const cov[6], float2 *const seed[3],
+               DevCounters *counters, cudaStream_t s) {
+  FilterArgs a;
+  for (int t = 0; t < 6; ++t) a.cov[t] = cov[t];
+  for (int q = 0; q < 3; ++q) a.seed[q] = seed[q];
+  a.csize = g.csize;
+  a.counters = counters;
+  dim3 grd((unsigned)((g.csize + kThreads - 1) / kThreads));
+  k_filter<<<grd, kThreads, 0, s>>>(a);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
+int noise_filter(const Geom &g, const float2 *const cov[6], float2 *const out[3],
+                 uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s) {
+  NoiseFilterArgs a;
+  for (int t = 0; t < 6; ++t) a.cov[t] = cov[t];
+  for (int q = 0; q < 3; ++q) a.out[q] = out[q];
+  a.csize = g.csize;
+  a.cnxp = g.cnxp; a.nyp = g.nyp; a.nzp = g.nzp;
+  a.seed = seed; a.stream0 = stream0;
+  a.counters = counters;
+  dim3 grd((unsigned)((g.csize + kThreads - 1) / kThreads));
+  k_noise_filter<<<grd, kThreads, 0, s>>>(a);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
+}  // namespace crava

@@ -1,0 +1,53 @@
+// solve.cuh -- per-kz operator tables and the per-bin posterior solve.
+#pragma once
+
+#include "common.cuh"
+
+namespace crava {
+
+// Device-resident per-kz tables of one context (see kz_tables_build).
+struct KzTables {
+  float2 *wd = nullptr;  // [nzp][nt]  D(k) * conj-wavelet: K = diag(wd) A
+  float2 *e1 = nullptr;  // [nzp][nt]  errMult1
+  float2 *e2 = nullptr;  // [nzp][nt]  errMult2
+  float *e3 = nullptr;   // [nzp][nt]  errMult3
+  int *inv = nullptr;    // [nzp]      invert_frequency
+};
+
+// Constants of the solve, passed by value (kernel parameter space).
+struct SolveConsts {
+  int nt;
+  float wnc;
+  float A[CRAVA_GPU_MAX_THETA][3];
+  double theta[CRAVA_GPU_MAX_THETA][CRAVA_GPU_MAX_THETA];
+  double var0[6];  // (0,0) (1,1) (2,2) (0,1) (0,2) (1,2)
+};
+
+struct SolveGrids {
+  float2 *mu[3];
+  float2 *data[CRAVA_GPU_MAX_THETA];
+  float2 *cov[6];
+  const float2 *err;
+};
+
+struct DevCounters {
+  unsigned long long chol_fail;
+  unsigned long long nonfinite;
+};
+
+int kz_tables_alloc(int nzp, int nt, KzTables *t);
+void kz_tables_free(KzTables *t);
+// Builds the tables from the wavelets on the device (params: host struct).
+int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s);
+
+// Per-bin solve over csize bins; plane = cnxp * nyp bins per kz.
+int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g,
+                    long long csize, long long plane, int precision,
+                    DevCounters *counters, cudaStream_t s);
+// FP32 form with the reference's operation order (separate translation
+// unit compiled without FMA contraction).
+int posterior_solve_fp32ref(const SolveConsts &c, const KzTables &t,
+                            const SolveGrids &g, long long csize, long long plane,
+                            DevCounters *counters, cudaStream_t s);
+
+}  // namespace crava

@@ -139,7 +139,7 @@ def ricker(t_ms, peak_hz):
 
 def ricker_fft_order(nzp, dt, peak_hz=25.0, nsamples=81, scale=1.0):
     w = np.zeros(nzp, dtype=np.float32)
-    half = nsamples // 2
+    half = min(nsamples // 2, (nzp - 1) // 2)
     for n in range(-half, half + 1):
         w[n % nzp] = np.float32(ricker(n * dt, peak_hz)) * np.float32(scale)
     return w
@@ -192,7 +192,7 @@ def make_case(nxp=64, nyp=64, nzp=128, angles_deg=(10.0, 20.0, 30.0), noise_frac
     fields = []
     for _ in range(3):
         w = rng.standard_normal((nzp, nyp, nxp))
-        fields.append(np.fft.irfftn(filt * np.fft.rfftn(w), s=(nzp, nyp, nxp)))
+        fields.append(np.fft.irfftn(filt * np.fft.rfftn(w), s=(nzp, nyp, nxp), axes=(0, 1, 2)))
     truth = []
     for p in range(3):
         f = sum(L0[p, q] * fields[q] for q in range(3))

@@ -1,0 +1,187 @@
+/*
+ * crava_gpu.h -- C ABI of the B200 (sm_100a) Fourier-domain Bayesian AVO
+ * inversion hot path.
+ *
+ * Every entry point replaces one piece of the reference's CPU path and keeps
+ * its data layout and semantics.  Grids are device (HBM) buffers in the
+ * reference's padded layout: one float buffer of rsize = rnxp*nyp*nzp floats,
+ * rnxp = 2*(nxp/2+1), real index i + rnxp*j + rnxp*nyp*k; after a forward
+ * transform the same bytes hold cnxp*nyp*nzp complex (re, im) pairs at index
+ * i + cnxp*j + cnxp*nyp*k, cnxp = nxp/2+1 (reference src/fftgrid.cpp:37-67,
+ * 1418-1431, 1698).  All calls are asynchronous on the context's stream and
+ * return a status code; nothing calls exit().  Plain C types only.
+ */
+#ifndef CRAVA_GPU_H
+#define CRAVA_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRAVA_GPU_MAX_THETA 8
+
+/* Status codes (the reference returns int and calls exit(1) on fatal
+ * conditions, e.g. src/crava.cpp:381-387; here every failure is a code). */
+enum crava_gpu_status {
+  CRAVA_GPU_OK = 0,
+  CRAVA_GPU_ERR_ARG = 1,     /* bad size, pointer, count or parameter     */
+  CRAVA_GPU_ERR_ALLOC = 2,   /* device or pinned-host allocation failed   */
+  CRAVA_GPU_ERR_CUDA = 3,    /* a CUDA call or kernel launch failed       */
+  CRAVA_GPU_ERR_TIMEOUT = 4, /* a bounded device wait gave up             */
+  CRAVA_GPU_ERR_STATE = 5,   /* call out of order (e.g. no stats pending) */
+  CRAVA_GPU_ERR_NODEV = 6    /* no usable CUDA device                     */
+};
+
+/* Grid types: FFTGrid::gridTypes (src/fftgrid.h:172).  They select the
+ * scaling of fftInPlace / invFFTInPlace (src/fftgrid.cpp:1817, 1848-1859):
+ * DATA and PARAMETER are scaled by 1/sqrt(N) both ways, COVARIANCE is
+ * unscaled forward and scaled by 1/N on the inverse. */
+enum crava_grid_type {
+  CRAVA_GRID_DATA = 1,
+  CRAVA_GRID_PARAMETER = 2,
+  CRAVA_GRID_COVARIANCE = 3
+};
+
+/* Arithmetic of the per-bin solve. */
+enum crava_solve_precision {
+  CRAVA_SOLVE_FP64 = 0,  /* plain form: covariances, Cholesky and posterior in FP64     */
+  CRAVA_SOLVE_MIXED = 1, /* FP32 build + Cholesky, one FP64 refinement step on the
+                            residual, FP64 Schur subtraction for the posterior cov   */
+  CRAVA_SOLVE_FP32 = 2   /* FP32 throughout, the reference's own arithmetic          */
+};
+
+/* Inversion parameters (what Crava::Crava gathers from ModelSettings,
+ * ModelAVODynamic and SeismicParametersHolder, src/crava.cpp:73-120).
+ * Host pointers; copied at crava_gpu_create. */
+typedef struct crava_gpu_params {
+  int nxp, nyp, nzp;          /* padded grid (2,3,5,7-smooth, as the reference pads)   */
+  int ntheta;                 /* angle stacks, 1..CRAVA_GPU_MAX_THETA                  */
+  int nz;                     /* unpadded layers: realFrequency = nz*1000/(lz*nzp)*k   */
+  int precision;              /* default crava_solve_precision                         */
+  double lz;                  /* simbox thickness in ms (Simbox::getlz)                */
+  double min_rel_thick;       /* Simbox::getMinRelThick                                */
+  float low_cut, high_cut;    /* frequency band in Hz (lowCut_, highCut_)              */
+  float wnc;                  /* white-noise component (wnc_)                          */
+  float reserved;
+  const float *wavelet;       /* [ntheta][nzp] wavelet samples in FFT order (rAmp_)    */
+  const float *wavelet_norm;  /* [ntheta] Wavelet::getNorm, or NULL = time-domain norm */
+  const float *A;             /* [ntheta][3] reflection matrix (A_)                    */
+  const double *theta_cov;    /* [ntheta][ntheta] errThetaCov_                         */
+  const double *var0;         /* [3][3] priorVar0_                                     */
+} crava_gpu_params;
+
+/* Device grids of one posterior.  mu: meanAlpha_, meanBeta_, meanRho_;
+ * data: seisData_[l]; cov: covAlpha, covBeta, covRho, crCovAlphaBeta,
+ * crCovAlphaRho, crCovBetaRho (SeismicParametersHolder order); err_corr: errCorr_. */
+typedef struct crava_gpu_grids {
+  float *mu[3];
+  float *data[CRAVA_GPU_MAX_THETA];
+  float *cov[6];
+  float *err_corr;
+} crava_gpu_grids;
+
+/* Statistics of the last solve or simulation (replaces the reference's
+ * silent prior fallback counts and its timing report). */
+typedef struct crava_gpu_stats {
+  long long chol_fail_bins;   /* inverted bins whose Cholesky failed (prior kept)     */
+  long long nonfinite_bins;   /* bins with a non-finite output                         */
+  float ms_forward;           /* device time of the forward transforms                 */
+  float ms_solve;             /* device time of the per-bin solve                      */
+  float ms_inverse;           /* device time of the inverse transforms                 */
+  float ms_total;             /* device time of the whole call                         */
+} crava_gpu_stats;
+
+typedef struct crava_gpu_ctx crava_gpu_ctx;
+
+/* Creates a context on `device` issuing work on `stream` (a cudaStream_t,
+ * NULL = the legacy default stream).  Builds the per-kz operator tables on
+ * the device from the wavelets (the set-up of computePostMeanResidAndFFTCov,
+ * src/crava.cpp:952-1058).  Replaces: Crava::Crava's set-up, src/crava.cpp:49-120. */
+int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
+                     crava_gpu_ctx **out);
+int crava_gpu_destroy(crava_gpu_ctx *ctx);
+const char *crava_gpu_status_string(int status);
+
+/* In-place 3-D real-to-complex transform with the FFTGrid scaling of
+ * grid_type.  Replaces FFTGrid::fftInPlace, src/fftgrid.cpp:1803-1829. */
+int crava_gpu_fft_r2c(crava_gpu_ctx *ctx, float *grid, int grid_type);
+
+/* In-place 3-D complex-to-real transform.  Replaces
+ * FFTGrid::invFFTInPlace, src/fftgrid.cpp:1831-1862. */
+int crava_gpu_fft_c2r(crava_gpu_ctx *ctx, float *grid, int grid_type);
+
+/* Per-(kx,ky,kz) posterior solve on transformed grids, in place:
+ * mu <- posterior mean, data <- residual, cov <- posterior covariance
+ * (err_corr is read).  Replaces the loop of
+ * Crava::computePostMeanResidAndFFTCov, src/crava.cpp:1042-1151. */
+int crava_gpu_posterior(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
+                        int precision);
+
+/* The whole posterior unit on real-domain grids, in place: forward
+ * transforms of 3 means, ntheta stacks, 6 covariances and the noise
+ * correlation; the solve; inverse transforms of 3 posterior means,
+ * ntheta residuals and 6 posterior covariances.  Replaces
+ * src/crava.cpp:175-190 (transforms), 1003, 1012, 1042-1151, 1181-1206, 218. */
+int crava_gpu_posterior_unit(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
+                             int precision);
+
+/* The same unit on HOST buffers (layout as above): uploads, runs and
+ * downloads, overlapping copies with the transforms.  Host buffers should
+ * be page-locked (see crava_gpu_host_register) for full PCIe speed.
+ * Synchronous: returns when the outputs are in host memory.  This is the
+ * entry point a CPU-resident Crava (fftw_malloc'd FFTGrid buffers) calls. */
+int crava_gpu_posterior_unit_host(crava_gpu_ctx *ctx,
+                                  const crava_gpu_grids *host_grids,
+                                  int precision);
+int crava_gpu_host_register(void *ptr, uint64_t bytes);
+int crava_gpu_host_unregister(void *ptr);
+
+/* Complex N(0,1) noise spectrum with the Hermitian rules of
+ * FFTGrid::fillInComplexNoise (src/fftgrid.cpp:1213-1263), drawn from a
+ * counter-based generator (Philox-4x32-10): bin values are a pure function
+ * of (seed, stream_id, bin), so realisations are reproducible and resumable.
+ * Replaces FFTGrid::fillInComplexNoise with RandomGen. */
+int crava_gpu_noise_fill(crava_gpu_ctx *ctx, float *grid, uint64_t seed,
+                         uint64_t stream_id);
+
+/* Per-bin filter of three noise spectra through the Cholesky factor of the
+ * posterior covariance spectra (FP32, as the reference): seed <- L seed,
+ * zero where the factorisation fails.  Replaces src/crava.cpp:1482-1521. */
+int crava_gpu_sim_filter(crava_gpu_ctx *ctx, const float *const cov[6],
+                         float *const seed[3]);
+
+/* `count` posterior realisations: noise + filter (one fused pass), inverse
+ * transform (PARAMETER scaling), plus the real-domain posterior mean.
+ * Realisation r uses stream ids 3*(first_index+r)+{0,1,2}.  out[3*r+p]
+ * receives parameter p of realisation r (real grids).  cov: transformed
+ * posterior covariance grids; post_mean: real-domain posterior means.
+ * Replaces Crava::simulate, src/crava.cpp:1415-1599 (per realisation:
+ * fillInComplexNoise x3, filter, invFFTInPlace x3, add). */
+int crava_gpu_simulate(crava_gpu_ctx *ctx, const float *const cov[6],
+                       const float *const post_mean[3], uint64_t seed,
+                       int first_index, int count, float *const *out);
+
+/* Waits for the context's stream and returns the statistics of the last
+ * posterior / simulation call. */
+int crava_gpu_get_stats(crava_gpu_ctx *ctx, crava_gpu_stats *stats);
+
+/* Copies the device-built per-kz tables to host memory (for checking):
+ * wd/e1/e2 [nzp][ntheta] complex, e3 [nzp][ntheta], inv [nzp]. */
+int crava_gpu_kz_tables(crava_gpu_ctx *ctx, float *wd, float *e1, float *e2,
+                        float *e3, int *inv);
+
+/* Replaces the per-kz tables with caller-supplied ones (same layout as
+ * crava_gpu_kz_tables), e.g. spectra computed by the reference's own FFTW
+ * (src/crava.cpp:952-976, 1024-1058).  Host pointers; synchronous. */
+int crava_gpu_set_kz_tables(crava_gpu_ctx *ctx, const float *wd, const float *e1,
+                            const float *e2, const float *e3, const int *inv);
+
+/* Number of kernels this library launched so far in this process. */
+long long crava_gpu_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,91 @@
+"""First end-to-end GPU checks against the CPU oracle (small grids)."""
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-30))
+
+
+@pytest.mark.parametrize("shape", [(16, 12, 32), (20, 18, 30), (15, 16, 20), (64, 64, 128)])
+@pytest.mark.parametrize("gtype", [api.DATA, api.COVARIANCE])
+def test_fft_roundtrip_and_oracle(shape, gtype):
+    nx, ny, nz = shape
+    case = synth.make_case(nx, ny, nz, (10.0, 20.0), 0.1, seed=5)
+    ctx = api.Context(case)
+    g = case.data[0] if gtype == api.DATA else case.cov[0]
+    t = api.to_device(g)
+    ctx.fft_r2c(t, gtype)
+    out = t.cpu().numpy()
+    ref = O.fft_r2c(g, nx, ny, nz, gtype, "orc")
+    assert rel(api.complex_view(out, nx), O.complex_view(ref, nx)) < 1e-6
+    ctx.fft_c2r(t, gtype)
+    back = t.cpu().numpy()
+    assert rel(back[..., :nx], g[..., :nx]) < 1e-6
+
+
+def _spectra_dev(case, sp):
+    mu = [api.to_device(g) for g in sp["mu"]]
+    data = [api.to_device(g) for g in sp["data"]]
+    cov = [api.to_device(g) for g in sp["cov"]]
+    err = api.to_device(sp["err"])
+    return mu, data, cov, err
+
+
+@pytest.mark.parametrize("shape,angles", [((16, 12, 32), (10.0, 20.0, 30.0)),
+                                          ((20, 18, 30), (0.0, 10.0, 20.0, 30.0, 40.0)),
+                                          ((15, 16, 20), (5.0, 25.0))])
+def test_solve_fp32_bitexact_vs_reference_order(shape, angles):
+    case = synth.make_case(*shape, angles, 0.1, seed=7)
+    sp = O.forward_spectra(case, "orc")
+    tables = O.kz_tables(case, "orc")
+    ctx = api.Context(case)
+    ctx.set_kz_tables(tables)
+    mu, data, cov, err = _spectra_dev(case, sp)
+    ctx.posterior(mu, data, cov, err, api.FP32)
+    st = ctx.stats()
+    omu, ores, ocov, ofail = O.posterior_fp32_tables(case, sp, tables, "orc")
+    nx = case.nxp
+    for g, o in zip(mu + data + cov, omu + ores + ocov):
+        a = api.complex_view(g.cpu().numpy(), nx)
+        b = O.complex_view(o, nx)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), rel(a, b)
+    assert st.chol_fail_bins == ofail
+
+
+@pytest.mark.parametrize("prec,tol", [(api.FP64, 1e-7), (api.MIXED, 1e-5)])
+@pytest.mark.parametrize("noise", [0.1, 0.01])
+def test_solve_vs_fp64_oracle(prec, tol, noise):
+    case = synth.make_case(16, 12, 64, (0.0, 10.0, 20.0, 30.0, 40.0), noise, seed=11)
+    sp = O.forward_spectra(case, "orc")
+    tables = O.kz_tables(case, "orc")
+    ctx = api.Context(case)
+    ctx.set_kz_tables(tables)
+    mu, data, cov, err = _spectra_dev(case, sp)
+    ctx.posterior(mu, data, cov, err, prec)
+    dmu, dres, dcov, dfail = O.posterior_fp64(case, sp)
+    nx = case.nxp
+    errs = []
+    for g, o in zip(mu + data + cov, dmu + dres + dcov):
+        errs.append(rel(api.complex_view(g.cpu().numpy(), nx), o))
+    assert max(errs) < tol, errs
+
+
+def test_unit_vs_reference_unit():
+    case = synth.config_small()
+    ctx = api.Context(case)
+    mu = [api.to_device(g) for g in case.mu]
+    data = [api.to_device(g) for g in case.data]
+    cov = [api.to_device(g) for g in case.cov]
+    err = api.to_device(case.err_corr)
+    ctx.posterior_unit(mu, data, cov, err, api.FP32)
+    which = "ref" if O.have_ref() else "orc"
+    omu, ores, ocov, ofail = O.unit_fp32(case, which)
+    nx = case.nxp
+    for g, o in zip(mu + data + cov, omu + ores + ocov):
+        assert rel(g.cpu().numpy()[..., :nx], o[..., :nx]) < 2e-5
