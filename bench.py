@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the posterior unit: posterior cells/s at 256x256x512, 5 angles.
+
+One step = one posterior unit on one seeded synthetic case (the timed unit of
+the reference: forward transforms of 3 means, 5 stacks, 6 prior covariances
+and the noise correlation; the per-(kx,ky,kz) solve; inverse transforms of 3
+posterior means, 5 residuals and 6 posterior covariances).
+posterior cells/s = nxp*nyp*nzp / step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl crava_b200|reference]
+
+Own arm: inputs resident in HBM (2.0 GB per step, larger than L2), outputs
+written out of place so each step reads pristine inputs; device time with
+CUDA events over K steps, max over ranks.  `e2e` runs the same unit through
+crava_gpu_posterior_unit_host with pinned host buffers (copies timed).
+Reference arm: the reference's own CPU code (FFTW 2.1.2 + lib_matr.c,
+oracle/_ref) on the host cores, on a bounded sample of the same unit.
+Multi-GPU (torchrun): every rank runs its own independent unit (weak
+scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "posterior cells/s at 256x256x512x5 angles, mixed vs FP64 form; % HBM roofline"
+ANGLES5 = (0.0, 10.0, 20.0, 30.0, 40.0)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="crava_b200", choices=["crava_b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp32"])
+    ap.add_argument("--grid", default="256,256,512")
+    ap.add_argument("--noise", type=float, default=0.10)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- CPU sample
+def cpu_sample_unit(nxp, nyp, nzp, nt, which="ref", seed=0):
+    """Times the reference CPU path on a bounded sample of one unit and
+    returns (seconds per unit, description).  The sample: one forward
+    transform of a DATA grid, one of a COVARIANCE grid and one inverse
+    transform at the full grid size (FFTW 2.1.2 with its per-call plan, as
+    FFTGrid does), and the per-bin solve on a 64x64xnzp case with the same
+    angles and kz band, scaled per bin.  Unit time = (3+nt) r2c(scaled)
+    + 7 r2c(covariance) + (9+nt) c2r + solve * csize_full / csize_sample."""
+    import numpy as np
+
+    from crava_b200 import synth
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(seed)
+    rnxp = 2 * (nxp // 2 + 1)
+    g = rng.standard_normal((nzp, nyp, rnxp)).astype(np.float32)
+    t0 = time.perf_counter(); a = O.fft_r2c(g, nxp, nyp, nzp, 1, which); t_r2c = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.fft_r2c(g, nxp, nyp, nzp, 3, which); t_r2c_cov = time.perf_counter() - t0
+    t0 = time.perf_counter(); O.fft_c2r(a, nxp, nyp, nzp, 1, which); t_c2r = time.perf_counter() - t0
+    del g, a
+    small = synth.make_case(64, 64, nzp, ANGLES5[:nt] if nt <= 5 else tuple(range(nt)), 0.10, seed + 7)
+    # spectra with the reference scalings; numpy keeps the set-up short
+    def spec(x, scale):
+        c = np.fft.rfftn(x[..., :64].astype(np.float64), axes=(0, 1, 2)) * scale
+        out = np.zeros(x.shape, np.float32)
+        out.view(np.complex64)[...] = c.astype(np.complex64)
+        return out
+    n = 64 * 64 * nzp
+    s = 1.0 / math.sqrt(n)
+    sp = {"mu": [spec(x, s) for x in small.mu], "data": [spec(x, s) for x in small.data],
+          "cov": [spec(x, 1.0) for x in small.cov], "err": spec(small.err_corr, 1.0)}
+    t0 = time.perf_counter(); O.posterior_fp32(small, sp, which); t_solve = time.perf_counter() - t0
+    csize_full = (nxp // 2 + 1) * nyp * nzp
+    csize_small = 33 * 64 * nzp
+    t_unit = ((3 + nt) * t_r2c + 7 * t_r2c_cov + (9 + nt) * t_c2r
+              + t_solve * csize_full / csize_small)
+    desc = (f"one r2c (DATA), one r2c (COVARIANCE), one c2r at {nxp}x{nyp}x{nzp} "
+            f"({t_r2c:.2f}/{t_r2c_cov:.2f}/{t_c2r:.2f} s) and the per-bin solve on a 64x64x{nzp}x{nt} "
+            f"case ({t_solve:.2f} s), scaled to one unit: {t_unit:.1f} s")
+    return t_unit, desc
+
+
+def _ref_worker(args):
+    nxp, nyp, nzp, nt, which, seed = args
+    t, _ = cpu_sample_unit(nxp, nyp, nzp, nt, which, seed)
+    return t
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.path = tempfile.mktemp(prefix="crava_clocks_", suffix=".csv")
+        self.proc = None
+        self.dev = device_index
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- own arm
+def run_own(args):
+    import numpy as np
+    import torch
+
+    from crava_b200 import api, synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    nxp, nyp, nzp = (int(x) for x in args.grid.split(","))
+    nt = 5
+    prec = {"mixed": api.MIXED, "fp64": api.FP64, "fp32": api.FP32}[args.precision]
+
+    case = synth.make_case(nxp, nyp, nzp, ANGLES5, args.noise, seed=2 + rank,
+                           wavelet_scale_range=(0.8, 1.2))
+    stream = torch.cuda.Stream(dev)
+    ctx = api.Context(case, device=dev, stream=stream, precision=prec)
+    d = lambda gs: [api.to_device(g, dev) for g in gs]
+    src = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
+    dst = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(precision, steps, profile):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        for _ in range(args.warmup):
+            ctx.posterior_unit_oop(src, dst, precision)
+        ctx.set_profiling(profile)
+        ctx.profile()  # reset
+        barrier()
+        torch.cuda.synchronize(dev)
+        n0 = api.launch_count()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(steps):
+                ctx.posterior_unit_oop(src, dst, precision)
+            ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        launches = api.launch_count() - n0
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        return ev0.elapsed_time(ev1) / steps, launches, prof
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    ms, launches, prof = timed_steps(prec, args.steps, True)
+    clk = clocks.stop()
+    ms = max_over_ranks(ms)
+    st = ctx.stats()
+    cells = nxp * nyp * nzp
+    value = world * cells / (ms * 1e-3)
+
+    fp64_value = None
+    if not args.no_fp64_compare and prec != api.FP64:
+        ms64, _, _ = timed_steps(api.FP64, max(10, args.steps // 4), False)
+        ms64 = max_over_ranks(ms64)
+        fp64_value = world * cells / (ms64 * 1e-3)
+
+    # e2e through the host-buffer entry point (pinned host memory)
+    host = [torch.from_numpy(g).pin_memory() for g in case.grids()]
+    pristine = [g.copy() for g in case.grids()]
+    hmu, hdata, hcov, herr = host[:3], host[3:3 + nt], host[3 + nt:9 + nt], host[9 + nt]
+    ctx.posterior_unit_host(hmu, hdata, hcov, herr, prec)  # warm-up (allocates the work grids)
+    e2e_ms = []
+    for _ in range(max(1, args.e2e_steps)):
+        for h, p in zip(host, pristine):
+            h.numpy()[...] = p
+        barrier()
+        t0 = time.perf_counter()
+        ctx.posterior_unit_host(hmu, hdata, hcov, herr, prec)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = max_over_ranks(statistics.median(e2e_ms))
+    gbytes = case.mu[0].nbytes
+    h2d = (10 + nt) * gbytes
+    d2h = (9 + nt) * gbytes
+
+    roof = None
+    if prof:
+        name, (n, tot, bpl) = max(prof.items(), key=lambda kv: kv[1][1])
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except Exception:
+            pass
+        peak = peaks.get("hbm_gbs") or 6650.0
+        achieved = bpl / (tot / n * 1e-3) / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+                tr = json.load(f)
+            key = f"{nxp}x{nyp}x{nzp}"
+            traffic = tr.get(key, {}).get(name)
+        except Exception:
+            pass
+        roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
+                "bytes_per_launch": bpl, "launches": n, "avg_ms": round(tot / n, 5),
+                "share": round(tot / sum(v[1] for v in prof.values()), 4)}
+    kernels = {k: {"launches": v[0], "ms": round(v[1], 4),
+                   "GB/s": round(v[2] / (v[1] / v[0] * 1e-3) / 1e9, 1)} for k, v in prof.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            which = "ref" if O.have_ref() else "orc"
+            t_unit, desc = cpu_sample_unit(nxp, nyp, nzp, nt, which)
+            cpu = {"value": cells / t_unit, "unit": "cells/s", "cores": 1,
+                   "kind": "reference" if which == "ref" else "port", "sample": desc}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "cells/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": {"mixed": "f32+f64", "fp64": "f64", "fp32": "f32"}[args.precision],
+        "data": "synthetic (seeded prior realisation, Ricker wavelets, Aki-Richards, 10% noise)",
+        "config": {"workload": f"posterior unit {nxp}x{nyp}x{nzp}, 5 angles, {args.precision} solve",
+                   "grid": [nxp, nyp, nzp], "ntheta": nt, "precision": args.precision,
+                   "l2": "inputs larger than L2 (%.2f GB read per step)" % ((10 + nt) * gbytes / 1e9),
+                   "parallelism": f"replicas{world}"},
+        "e2e": {"value": world * cells / (e2e_step * 1e-3), "unit": "cells/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "fp64_form_value": fp64_value,
+        "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
+        "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
+        "kernels": kernels,
+        "chol_fail_bins": st.chol_fail_bins, "nonfinite_bins": st.nonfinite_bins,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    nxp, nyp, nzp = (int(x) for x in args.grid.split(","))
+    nt = 5
+    which = "ref" if O.have_ref() else "orc"
+    if which != "ref":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (the reference's FFTW 2.1.2 + lib_matr.c build) is missing"}))
+        return
+    import multiprocessing as mp
+
+    ncpu = os.cpu_count() or 1
+    workers = args.workers or max(1, min(ncpu, 16))
+    ctxm = mp.get_context("spawn")
+    with ctxm.Pool(workers) as pool:
+        for w in range(args.warmup):
+            pool.map(_ref_worker, [(nxp, nyp, nzp, nt, which, 100 + i) for i in range(workers)])
+        per_step = []
+        t_start = time.perf_counter()
+        for s in range(args.steps):
+            ts = pool.map(_ref_worker, [(nxp, nyp, nzp, nt, which, 200 + i) for i in range(workers)])
+            per_step.append(sum(nxp * nyp * nzp / t for t in ts))
+        wall = time.perf_counter() - t_start
+    value = statistics.median(per_step)
+    _, desc = (None, f"each of {workers} processes times the reference CPU path (FFTW 2.1.2 + lib_matr.c) "
+                     f"on a bounded sample of one {nxp}x{nyp}x{nzp}x{nt} unit: one forward DATA, one "
+                     f"forward COVARIANCE and one inverse transform at full size plus the per-bin solve "
+                     f"on a 64x64x{nzp} case, scaled to the unit; value = sum over processes")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": nxp * nyp * nzp / value * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "config": {"workload": f"posterior unit {nxp}x{nyp}x{nzp}, 5 angles, reference CPU",
+                                           "grid": [nxp, nyp, nzp], "ntheta": nt},
+           "cpu_baseline": {"value": value, "unit": "cells/s", "cores": workers, "kind": "reference",
+                            "sample": desc},
+           "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "wall_s": wall}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_own(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -48,6 +48,11 @@ class Grids(C.Structure):
                 ("cov", C.c_void_p * 6), ("err_corr", C.c_void_p)]
 
 
+class KernelProfile(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("total_ms", C.c_double),
+                ("bytes_per_launch", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("chol_fail_bins", C.c_longlong), ("nonfinite_bins", C.c_longlong),
                 ("ms_forward", C.c_float), ("ms_solve", C.c_float),
@@ -62,6 +67,9 @@ SYMBOLS = {
     "crava_gpu_fft_c2r": ([C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "crava_gpu_posterior": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
     "crava_gpu_posterior_unit": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
+    "crava_gpu_posterior_unit_oop": ([C.c_void_p, C.POINTER(Grids), C.POINTER(Grids), C.c_int], C.c_int),
+    "crava_gpu_set_profiling": ([C.c_void_p, C.c_int], C.c_int),
+    "crava_gpu_get_profile": ([C.c_void_p, C.POINTER(KernelProfile), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_posterior_unit_host": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
     "crava_gpu_host_register": ([C.c_void_p, C.c_uint64], C.c_int),
     "crava_gpu_host_unregister": ([C.c_void_p], C.c_int),
@@ -184,6 +192,25 @@ class Context:
         g = self.grids(mu, data, cov, err)
         p = self.precision if precision is None else precision
         check(self.lib.crava_gpu_posterior_unit(self.handle, C.byref(g), p), "posterior_unit")
+
+    def posterior_unit_oop(self, src, dst, precision=None):
+        """src, dst: (mu, data, cov, err) tuples of device tensors."""
+        gi = self.grids(*src)
+        go = self.grids(*dst)
+        p = self.precision if precision is None else precision
+        check(self.lib.crava_gpu_posterior_unit_oop(self.handle, C.byref(gi), C.byref(go), p),
+              "posterior_unit_oop")
+
+    def set_profiling(self, enable=True):
+        check(self.lib.crava_gpu_set_profiling(self.handle, int(bool(enable))), "set_profiling")
+
+    def profile(self):
+        """{name: (launches, total_ms, bytes_per_launch)}; resets the counters."""
+        arr = (KernelProfile * 16)()
+        n = C.c_int(0)
+        check(self.lib.crava_gpu_get_profile(self.handle, arr, 16, C.byref(n)), "get_profile")
+        return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms, arr[i].bytes_per_launch)
+                for i in range(min(n.value, 16))}
 
     def posterior_unit_host(self, mu, data, cov, err, precision=None):
         """Host tensors (CPU, ideally pinned); synchronous."""

@@ -42,6 +42,13 @@ struct crava_gpu_ctx {
   DevCounters *counters = nullptr;  // device
   cudaEvent_t ev[4] = {};           // start, after forward, after solve, end
   bool timed = false;               // events of the last call are valid
+  // per-kernel profiling (events around each launch when enabled)
+  bool prof = false;
+  struct Rec { int kind; cudaEvent_t a, b; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double prof_ms[16] = {};
+  long long prof_n[16] = {};
   // host-buffer path
   float *work = nullptr;  // (10 + ntheta) grids
   cudaStream_t s_in = nullptr, s_out = nullptr;
@@ -105,37 +112,104 @@ int check_grids(const crava_gpu_ctx *c, const crava_gpu_grids *gr) {
   return CRAVA_GPU_OK;
 }
 
+enum ProfKind {
+  K_ROWS_FWD, K_COLS_Y_FWD, K_COLS_Z_FWD, K_SOLVE, K_COLS_Z_INV, K_COLS_Y_INV, K_ROWS_INV,
+  K_SIM, K_NKINDS
+};
+const char *kKindName[K_NKINDS] = {"fft_rows_r2c", "fft_cols_y_fwd", "fft_cols_z_fwd", "posterior_solve",
+                                   "fft_cols_z_inv", "fft_cols_y_inv", "fft_rows_c2r", "sim_noise_filter"};
+
+cudaEvent_t pool_get(crava_gpu_ctx *c) {
+  if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Records an event pair around one launch when profiling is on.
+struct Scope {
+  crava_gpu_ctx *c;
+  int kind;
+  cudaEvent_t a = nullptr;
+  Scope(crava_gpu_ctx *ctx, int k) : c(ctx), kind(k) {
+    if (c->prof) { a = pool_get(c); cudaEventRecord(a, c->stream); }
+  }
+  ~Scope() {
+    if (c->prof && a) {
+      cudaEvent_t b = pool_get(c);
+      cudaEventRecord(b, c->stream);
+      c->recs.push_back({kind, a, b});
+    }
+  }
+};
+
+void prof_collect(crava_gpu_ctx *c) {
+  for (auto &r : c->recs) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      c->prof_ms[r.kind] += ms;
+      c->prof_n[r.kind] += 1;
+    }
+    c->pool.push_back(r.a);
+    c->pool.push_back(r.b);
+  }
+  c->recs.clear();
+}
+
+int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type) {
+  int rc;
+  { Scope sc(c, K_ROWS_FWD); if ((rc = fft_rows(c->plans, dst, -1, forward_scale(c->g, type), c->stream, nullptr, src))) return rc; }
+  { Scope sc(c, K_COLS_Y_FWD); if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
+  { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
+  return CRAVA_GPU_OK;
+}
+
+int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend = nullptr) {
+  int rc;
+  { Scope sc(c, K_COLS_Z_INV); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc; }
+  { Scope sc(c, K_COLS_Y_INV); if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc; }
+  { Scope sc(c, K_ROWS_INV); if ((rc = fft_rows(c->plans, grid, 1, inverse_scale(c->g, type), c->stream, addend))) return rc; }
+  return CRAVA_GPU_OK;
+}
+
+int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {
+  Scope sc(c, K_SOLVE);
+  SolveGrids sg = to_solve_grids(gr, c->p.ntheta);
+  return posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
+                         precision, c->counters, c->stream);
+}
+
 int valid_precision(int prec) {
   return prec >= CRAVA_SOLVE_FP64 && prec <= CRAVA_SOLVE_FP32;
 }
 
-int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision, bool timed) {
+// The posterior unit reading the real inputs from `in` and leaving the
+// outputs in `out` (in == out is the reference's in-place behaviour).
+int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids *out,
+             int precision) {
   const cudaStream_t s = c->stream;
   const int nt = c->p.ntheta;
   int rc;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
-  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   for (int q = 0; q < 3; ++q)
-    if ((rc = fft3d_r2c(c->plans, gr->mu[q], CRAVA_GRID_PARAMETER, s))) return rc;
+    if ((rc = pass_forward(c, in->mu[q], out->mu[q], CRAVA_GRID_PARAMETER))) return rc;
   for (int l = 0; l < nt; ++l)
-    if ((rc = fft3d_r2c(c->plans, gr->data[l], CRAVA_GRID_DATA, s))) return rc;
+    if ((rc = pass_forward(c, in->data[l], out->data[l], CRAVA_GRID_DATA))) return rc;
   for (int t = 0; t < 6; ++t)
-    if ((rc = fft3d_r2c(c->plans, gr->cov[t], CRAVA_GRID_COVARIANCE, s))) return rc;
-  if ((rc = fft3d_r2c(c->plans, gr->err_corr, CRAVA_GRID_COVARIANCE, s))) return rc;
-  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  SolveGrids sg = to_solve_grids(gr, nt);
-  if ((rc = posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
-                            precision, c->counters, s)))
-    return rc;
-  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+    if ((rc = pass_forward(c, in->cov[t], out->cov[t], CRAVA_GRID_COVARIANCE))) return rc;
+  if ((rc = pass_forward(c, in->err_corr, out->err_corr, CRAVA_GRID_COVARIANCE))) return rc;
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  if ((rc = pass_solve(c, out, precision))) return rc;
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   for (int q = 0; q < 3; ++q)
-    if ((rc = fft3d_c2r(c->plans, gr->mu[q], CRAVA_GRID_PARAMETER, s))) return rc;
+    if ((rc = pass_inverse(c, out->mu[q], CRAVA_GRID_PARAMETER))) return rc;
   for (int l = 0; l < nt; ++l)
-    if ((rc = fft3d_c2r(c->plans, gr->data[l], CRAVA_GRID_DATA, s))) return rc;
+    if ((rc = pass_inverse(c, out->data[l], CRAVA_GRID_DATA))) return rc;
   for (int t = 0; t < 6; ++t)
-    if ((rc = fft3d_c2r(c->plans, gr->cov[t], CRAVA_GRID_COVARIANCE, s))) return rc;
-  if (timed) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  c->timed = timed;
+    if ((rc = pass_inverse(c, out->cov[t], CRAVA_GRID_COVARIANCE))) return rc;
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  c->timed = true;
   return CRAVA_GPU_OK;
 }
 
@@ -217,6 +291,8 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->work);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
+  for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  for (auto &e : c->pool) cudaEventDestroy(e);
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_out) cudaStreamDestroy(c->s_out);
   delete c;
@@ -227,14 +303,14 @@ int crava_gpu_fft_r2c(crava_gpu_ctx *c, float *grid, int type) {
   if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
   if (type < CRAVA_GRID_DATA || type > CRAVA_GRID_COVARIANCE) return CRAVA_GPU_ERR_ARG;
   DeviceGuard guard(c->device);
-  return fft3d_r2c(c->plans, grid, type, c->stream);
+  return pass_forward(c, grid, grid, type);
 }
 
 int crava_gpu_fft_c2r(crava_gpu_ctx *c, float *grid, int type) {
   if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
   if (type < CRAVA_GRID_DATA || type > CRAVA_GRID_COVARIANCE) return CRAVA_GPU_ERR_ARG;
   DeviceGuard guard(c->device);
-  return fft3d_c2r(c->plans, grid, type, c->stream);
+  return pass_inverse(c, grid, type);
 }
 
 int crava_gpu_posterior(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {
@@ -245,10 +321,7 @@ int crava_gpu_posterior(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precisi
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), c->stream));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], c->stream));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], c->stream));
-  SolveGrids sg = to_solve_grids(gr, c->p.ntheta);
-  rc = posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
-                       precision, c->counters, c->stream);
-  if (rc) return rc;
+  if ((rc = pass_solve(c, gr, precision))) return rc;
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], c->stream));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], c->stream));
   c->timed = true;
@@ -260,7 +333,47 @@ int crava_gpu_posterior_unit(crava_gpu_ctx *c, const crava_gpu_grids *gr, int pr
   if ((rc = check_ctx(c)) || (rc = check_grids(c, gr))) return rc;
   if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
   DeviceGuard guard(c->device);
-  return run_unit(c, gr, precision, true);
+  return run_unit(c, gr, gr, precision);
+}
+
+int crava_gpu_posterior_unit_oop(crava_gpu_ctx *c, const crava_gpu_grids *in,
+                                 const crava_gpu_grids *out, int precision) {
+  int rc;
+  if ((rc = check_ctx(c)) || (rc = check_grids(c, in)) || (rc = check_grids(c, out))) return rc;
+  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  return run_unit(c, in, out, precision);
+}
+
+int crava_gpu_set_profiling(crava_gpu_ctx *c, int enable) {
+  if (check_ctx(c)) return CRAVA_GPU_ERR_ARG;
+  c->prof = enable != 0;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_get_profile(crava_gpu_ctx *c, crava_gpu_kernel_profile *out, int max, int *count) {
+  if (check_ctx(c) || !count || (max > 0 && !out)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  prof_collect(c);
+  const double G = (double)c->g.csize * 8.0;  // bytes of one grid
+  const int nt = c->p.ntheta;
+  int n = 0;
+  for (int k = 0; k < K_NKINDS; ++k) {
+    if (!c->prof_n[k]) continue;
+    if (n < max) {
+      crava_gpu_kernel_profile &o = out[n];
+      std::memset(&o, 0, sizeof o);
+      std::snprintf(o.name, sizeof o.name, "%s", kKindName[k]);
+      o.launches = c->prof_n[k];
+      o.total_ms = c->prof_ms[k];
+      o.bytes_per_launch = k == K_SOLVE ? (double)(19 + 2 * nt) * G : k == K_SIM ? 9.0 * G : 2.0 * G;
+    }
+    ++n;
+  }
+  *count = n;
+  for (int k = 0; k < K_NKINDS; ++k) { c->prof_ms[k] = 0.0; c->prof_n[k] = 0; }
+  return CRAVA_GPU_OK;
 }
 
 int crava_gpu_host_register(void *ptr, uint64_t bytes) {
@@ -317,16 +430,13 @@ int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, i
     CRAVA_CUDA_TRY(cudaMemcpyAsync(dev[k], host[k], gbytes, cudaMemcpyHostToDevice, c->s_in));
     CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[k], c->s_in));
     CRAVA_CUDA_TRY(cudaStreamWaitEvent(s, c->grid_ev[k], 0));
-    if ((rc = fft3d_r2c(c->plans, dev[k], type[k], s))) return rc;
+    if ((rc = pass_forward(c, dev[k], dev[k], type[k]))) return rc;
   }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  SolveGrids sg = to_solve_grids(&dg, nt);
-  if ((rc = posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
-                            precision, c->counters, s)))
-    return rc;
+  if ((rc = pass_solve(c, &dg, precision))) return rc;
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   for (int k = 0; k < ngrid - 1; ++k) {  // the noise correlation is not an output
-    if ((rc = fft3d_c2r(c->plans, dev[k], type[k], s))) return rc;
+    if ((rc = pass_inverse(c, dev[k], type[k]))) return rc;
     CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[ngrid + k], s));
     CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->grid_ev[ngrid + k], 0));
     CRAVA_CUDA_TRY(cudaMemcpyAsync(host[k], dev[k], gbytes, cudaMemcpyDeviceToHost, c->s_out));
@@ -383,9 +493,12 @@ int crava_gpu_simulate(crava_gpu_ctx *c, const float *const cov[6], const float 
     float2 *o[3];
     for (int q = 0; q < 3; ++q) o[q] = reinterpret_cast<float2 *>(out[3 * r + q]);
     const uint64_t stream0 = 3ull * (uint64_t)(first_index + r);
-    if ((rc = noise_filter(c->g, cv, o, seed, stream0, c->counters, s))) return rc;
+    {
+      Scope sc(c, K_SIM);
+      if ((rc = noise_filter(c->g, cv, o, seed, stream0, c->counters, s))) return rc;
+    }
     for (int q = 0; q < 3; ++q)
-      if ((rc = fft3d_c2r(c->plans, out[3 * r + q], CRAVA_GRID_PARAMETER, s, post_mean[q]))) return rc;
+      if ((rc = pass_inverse(c, out[3 * r + q], CRAVA_GRID_PARAMETER, post_mean[q]))) return rc;
   }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));

@@ -32,6 +32,7 @@ constexpr int kColTile = 8;  // x-columns per CTA in the y / z passes
 
 struct RowArgs {
   float *grid;
+  const float *src;  // forward: input grid (may equal grid)
   long long nrows;  // nyp * nzp
   int rnxp;         // floats per row
   int nxp;
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
       int r = idx / n, m = idx % n;
       float2 v = make_float2(0.f, 0.f);
       if (r < nrows) {
-        const float *row = a.grid + (row0 + r) * a.rnxp;
+        const float *row = a.src + (row0 + r) * a.rnxp;
         if (EVEN) v = reinterpret_cast<const float2 *>(row)[m];
         else v = make_float2(row[m], 0.f);
         v = cscale(v, a.scale);
@@ -271,9 +272,10 @@ void fft_plans_destroy(FftPlans *p) {
 }
 
 int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t s,
-             const float *addend) {
+             const float *addend, const float *src) {
   RowArgs a;
   a.addend = addend;
+  a.src = src ? src : grid;
   a.grid = grid;
   a.nrows = (long long)p.g.nyp * p.g.nzp;
   a.rnxp = p.g.rnxp;

@@ -40,8 +40,9 @@ int fft3d_c2r(const FftPlans &p, float *grid, int type, cudaStream_t s,
               const float *addend = nullptr);
 
 // Individual passes (used by the fused paths).
+// src (forward only, optional): read the real input from src, write grid.
 int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t s,
-             const float *addend = nullptr);
+             const float *addend = nullptr, const float *src = nullptr);
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
 

@@ -127,6 +127,14 @@ int crava_gpu_posterior(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
 int crava_gpu_posterior_unit(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
                              int precision);
 
+/* The same unit reading the real inputs from `in` and writing every output
+ * (and the transformed noise correlation) to `out`; `in` is left unchanged.
+ * in == out gives crava_gpu_posterior_unit.  The first transform pass of
+ * each grid reads `in` and writes `out`, so the traffic is that of the
+ * in-place call. */
+int crava_gpu_posterior_unit_oop(crava_gpu_ctx *ctx, const crava_gpu_grids *in,
+                                 const crava_gpu_grids *out, int precision);
+
 /* The same unit on HOST buffers (layout as above): uploads, runs and
  * downloads, overlapping copies with the transforms.  Host buffers should
  * be page-locked (see crava_gpu_host_register) for full PCIe speed.
@@ -177,6 +185,22 @@ int crava_gpu_kz_tables(crava_gpu_ctx *ctx, float *wd, float *e1, float *e2,
  * (src/crava.cpp:952-976, 1024-1058).  Host pointers; synchronous. */
 int crava_gpu_set_kz_tables(crava_gpu_ctx *ctx, const float *wd, const float *e1,
                             const float *e2, const float *e3, const int *inv);
+
+/* Per-kernel device time (profiling mode records a CUDA event pair around
+ * every launch of this context; off by default).  bytes_per_launch is the
+ * algorithmic traffic of one launch: 2 grids for a transform pass (read +
+ * write), (19 + 2 ntheta) grids for the solve, 9 grids for the noise filter. */
+typedef struct crava_gpu_kernel_profile {
+  char name[32];
+  long long launches;
+  double total_ms;
+  double bytes_per_launch;
+} crava_gpu_kernel_profile;
+int crava_gpu_set_profiling(crava_gpu_ctx *ctx, int enable);
+/* Synchronises, returns the accumulated records (up to max) and resets them;
+ * *count receives the number of kernel kinds seen. */
+int crava_gpu_get_profile(crava_gpu_ctx *ctx, crava_gpu_kernel_profile *out,
+                          int max, int *count);
 
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
