@@ -68,6 +68,8 @@ SYMBOLS = {
     "crava_gpu_posterior": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
     "crava_gpu_posterior_unit": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
     "crava_gpu_posterior_unit_oop": ([C.c_void_p, C.POINTER(Grids), C.POINTER(Grids), C.c_int], C.c_int),
+    "crava_gpu_set_fused": ([C.c_void_p, C.c_int], C.c_int),
+    "crava_gpu_fused_available": ([C.c_void_p, C.c_int], C.c_int),
     "crava_gpu_set_profiling": ([C.c_void_p, C.c_int], C.c_int),
     "crava_gpu_get_profile": ([C.c_void_p, C.POINTER(KernelProfile), C.c_int, C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_posterior_unit_host": ([C.c_void_p, C.POINTER(Grids), C.c_int], C.c_int),
@@ -200,6 +202,13 @@ class Context:
         p = self.precision if precision is None else precision
         check(self.lib.crava_gpu_posterior_unit_oop(self.handle, C.byref(gi), C.byref(go), p),
               "posterior_unit_oop")
+
+    def set_fused(self, enable=True):
+        check(self.lib.crava_gpu_set_fused(self.handle, int(bool(enable))), "set_fused")
+
+    def fused_available(self, precision=None):
+        p = self.precision if precision is None else precision
+        return bool(self.lib.crava_gpu_fused_available(self.handle, p))
 
     def set_profiling(self, enable=True):
         check(self.lib.crava_gpu_set_profiling(self.handle, int(bool(enable))), "set_profiling")

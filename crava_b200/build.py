@@ -25,6 +25,7 @@ SOURCES = {
     "solve.cu": [],
     "solve_ref.cu": ["-fmad=false"],
     "sim.cu": ["-fmad=false"],
+    "unit.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -11,6 +11,7 @@
 #include "fft.cuh"
 #include "sim.cuh"
 #include "solve.cuh"
+#include "unit.cuh"
 
 namespace crava {
 
@@ -42,12 +43,17 @@ struct crava_gpu_ctx {
   DevCounters *counters = nullptr;  // device
   cudaEvent_t ev[4] = {};           // start, after forward, after solve, end
   bool timed = false;               // events of the last call are valid
+  // fused unit (plane kernels + z/solve kernel) and its workspace
+  UnitPlan uplan{};
+  bool fused = false;  // the three-pass path is faster today; set_fused(1) selects the fused kernels
+  float2 *W = nullptr;  // (10 + ntheta) grids in the column-pair layout
   // per-kernel profiling (events around each launch when enabled)
   bool prof = false;
-  struct Rec { int kind; cudaEvent_t a, b; };
+  struct Rec { int kind; cudaEvent_t a, b; double bytes; };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
   double prof_ms[16] = {};
+  double prof_bytes[16] = {};
   long long prof_n[16] = {};
   // host-buffer path
   float *work = nullptr;  // (10 + ntheta) grids
@@ -114,10 +120,11 @@ int check_grids(const crava_gpu_ctx *c, const crava_gpu_grids *gr) {
 
 enum ProfKind {
   K_ROWS_FWD, K_COLS_Y_FWD, K_COLS_Z_FWD, K_SOLVE, K_COLS_Z_INV, K_COLS_Y_INV, K_ROWS_INV,
-  K_SIM, K_NKINDS
+  K_SIM, K_PLANE_FWD, K_ZSOLVE, K_PLANE_INV, K_NKINDS
 };
 const char *kKindName[K_NKINDS] = {"fft_rows_r2c", "fft_cols_y_fwd", "fft_cols_z_fwd", "posterior_solve",
-                                   "fft_cols_z_inv", "fft_cols_y_inv", "fft_rows_c2r", "sim_noise_filter"};
+                                   "fft_cols_z_inv", "fft_cols_y_inv", "fft_rows_c2r", "sim_noise_filter",
+                                   "unit_plane_fwd", "unit_zsolve", "unit_plane_inv"};
 
 cudaEvent_t pool_get(crava_gpu_ctx *c) {
   if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
@@ -130,15 +137,17 @@ cudaEvent_t pool_get(crava_gpu_ctx *c) {
 struct Scope {
   crava_gpu_ctx *c;
   int kind;
+  double bytes;
   cudaEvent_t a = nullptr;
-  Scope(crava_gpu_ctx *ctx, int k) : c(ctx), kind(k) {
+  // bytes: algorithmic traffic of the launch (default: per kind, see get_profile)
+  Scope(crava_gpu_ctx *ctx, int k, double b = -1.0) : c(ctx), kind(k), bytes(b) {
     if (c->prof) { a = pool_get(c); cudaEventRecord(a, c->stream); }
   }
   ~Scope() {
     if (c->prof && a) {
       cudaEvent_t b = pool_get(c);
       cudaEventRecord(b, c->stream);
-      c->recs.push_back({kind, a, b});
+      c->recs.push_back({kind, a, b, bytes});
     }
   }
 };
@@ -147,7 +156,14 @@ void prof_collect(crava_gpu_ctx *c) {
   for (auto &r : c->recs) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      const double G = (double)c->g.csize * 8.0;  // bytes of one grid
+      const int nt = c->p.ntheta;
+      double bytes = r.bytes >= 0 ? r.bytes
+                   : r.kind == K_SOLVE ? (double)(19 + 2 * nt) * G
+                   : r.kind == K_SIM   ? 9.0 * G
+                                       : 2.0 * G;
       c->prof_ms[r.kind] += ms;
+      c->prof_bytes[r.kind] += bytes;
       c->prof_n[r.kind] += 1;
     }
     c->pool.push_back(r.a);
@@ -183,10 +199,75 @@ int valid_precision(int prec) {
   return prec >= CRAVA_SOLVE_FP64 && prec <= CRAVA_SOLVE_FP32;
 }
 
+int ensure_workspace(crava_gpu_ctx *c) {
+  if (c->W) return CRAVA_GPU_OK;
+  const size_t n = (size_t)(10 + c->p.ntheta) * (size_t)c->uplan.wgrid;
+  if (cudaMalloc(&c->W, n * sizeof(float2)) != cudaSuccess) { c->W = nullptr; return CRAVA_GPU_ERR_ALLOC; }
+  return CRAVA_GPU_OK;
+}
+
+bool use_fused(const crava_gpu_ctx *c, int precision) {
+  return c->fused && c->uplan.ok && precision != CRAVA_SOLVE_FP32;
+}
+
+// Grids of a crava_gpu_grids in unit order (mu 3, data nt, cov 6, err) with
+// their FFTGrid types.
+int unit_order(const crava_gpu_ctx *c, const crava_gpu_grids *g, float **ptr, int *type) {
+  int i = 0;
+  for (int q = 0; q < 3; ++q) { ptr[i] = g->mu[q]; type[i++] = CRAVA_GRID_PARAMETER; }
+  for (int l = 0; l < c->p.ntheta; ++l) { ptr[i] = g->data[l]; type[i++] = CRAVA_GRID_DATA; }
+  for (int t = 0; t < 6; ++t) { ptr[i] = g->cov[t]; type[i++] = CRAVA_GRID_COVARIANCE; }
+  ptr[i] = g->err_corr; type[i++] = CRAVA_GRID_COVARIANCE;
+  return i;
+}
+
+// Fused unit: plane forward (all grids, one launch), z transform + solve +
+// inverse z (one launch), plane inverse (outputs, one launch).  The noise
+// correlation output is not written (its transform stays in the workspace).
+int run_unit_fused(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids *out,
+                   int precision) {
+  const cudaStream_t s = c->stream;
+  int rc;
+  if ((rc = ensure_workspace(c))) return rc;
+  float *src[kMaxUnitGrids], *dst[kMaxUnitGrids];
+  int type[kMaxUnitGrids];
+  const int G = unit_order(c, in, src, type);
+  unit_order(c, out, dst, type);
+  float2 *w[kMaxUnitGrids];
+  float fs[kMaxUnitGrids], is[kMaxUnitGrids];
+  for (int i = 0; i < G; ++i) {
+    w[i] = c->W + (size_t)i * c->uplan.wgrid;
+    fs[i] = forward_scale(c->g, type[i]);
+    is[i] = inverse_scale(c->g, type[i]);
+  }
+  const double gb = (double)c->g.csize * 8.0;
+  const double wb = (double)c->uplan.wgrid * 8.0;
+  CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  {
+    Scope sc(c, K_PLANE_FWD, G * (gb + wb));
+    if ((rc = unit_plane_forward(c->uplan, c->plans, src, w, fs, G, s))) return rc;
+  }
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  {
+    Scope sc(c, K_ZSOLVE, (2 * G - 1) * wb);
+    if ((rc = unit_zsolve(c->uplan, c->plans, c->consts, c->tables, w, precision, c->counters, s))) return rc;
+  }
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  {
+    Scope sc(c, K_PLANE_INV, (G - 1) * (gb + wb));
+    if ((rc = unit_plane_inverse(c->uplan, c->plans, w, dst, is, nullptr, G - 1, s))) return rc;
+  }
+  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  c->timed = true;
+  return CRAVA_GPU_OK;
+}
+
 // The posterior unit reading the real inputs from `in` and leaving the
 // outputs in `out` (in == out is the reference's in-place behaviour).
 int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids *out,
              int precision) {
+  if (use_fused(c, precision)) return run_unit_fused(c, in, out, precision);
   const cudaStream_t s = c->stream;
   const int nt = c->p.ntheta;
   int rc;
@@ -271,6 +352,7 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
 
   auto fail = [&](int code) { crava_gpu_destroy(c); return code; };
   if ((rc = fft_plans_create(c->g, &c->plans))) return fail(rc);
+  unit_plan(c->g, nt, &c->uplan);
   if ((rc = kz_tables_alloc(nzp, nt, &c->tables))) return fail(rc);
   if (cudaMalloc(&c->counters, sizeof(DevCounters)) != cudaSuccess) return fail(CRAVA_GPU_ERR_ALLOC);
   for (auto &e : c->ev)
@@ -289,6 +371,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   kz_tables_free(&c->tables);
   cudaFree(c->counters);
   cudaFree(c->work);
+  cudaFree(c->W);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
@@ -345,6 +428,17 @@ int crava_gpu_posterior_unit_oop(crava_gpu_ctx *c, const crava_gpu_grids *in,
   return run_unit(c, in, out, precision);
 }
 
+int crava_gpu_set_fused(crava_gpu_ctx *c, int enable) {
+  if (check_ctx(c)) return CRAVA_GPU_ERR_ARG;
+  c->fused = enable != 0;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_fused_available(crava_gpu_ctx *c, int precision) {
+  if (check_ctx(c)) return 0;
+  return c->uplan.ok && precision != CRAVA_SOLVE_FP32;
+}
+
 int crava_gpu_set_profiling(crava_gpu_ctx *c, int enable) {
   if (check_ctx(c)) return CRAVA_GPU_ERR_ARG;
   c->prof = enable != 0;
@@ -356,8 +450,6 @@ int crava_gpu_get_profile(crava_gpu_ctx *c, crava_gpu_kernel_profile *out, int m
   DeviceGuard guard(c->device);
   CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
   prof_collect(c);
-  const double G = (double)c->g.csize * 8.0;  // bytes of one grid
-  const int nt = c->p.ntheta;
   int n = 0;
   for (int k = 0; k < K_NKINDS; ++k) {
     if (!c->prof_n[k]) continue;
@@ -367,12 +459,12 @@ int crava_gpu_get_profile(crava_gpu_ctx *c, crava_gpu_kernel_profile *out, int m
       std::snprintf(o.name, sizeof o.name, "%s", kKindName[k]);
       o.launches = c->prof_n[k];
       o.total_ms = c->prof_ms[k];
-      o.bytes_per_launch = k == K_SOLVE ? (double)(19 + 2 * nt) * G : k == K_SIM ? 9.0 * G : 2.0 * G;
+      o.bytes_per_launch = c->prof_bytes[k] / (double)c->prof_n[k];
     }
     ++n;
   }
   *count = n;
-  for (int k = 0; k < K_NKINDS; ++k) { c->prof_ms[k] = 0.0; c->prof_n[k] = 0; }
+  for (int k = 0; k < K_NKINDS; ++k) { c->prof_ms[k] = 0.0; c->prof_bytes[k] = 0.0; c->prof_n[k] = 0; }
   return CRAVA_GPU_OK;
 }
 
@@ -426,17 +518,42 @@ int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, i
   // the copy stream must not overtake earlier work on the compute stream
   CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[2 * ngrid], s));
   CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->grid_ev[2 * ngrid], 0));
+  const bool fused = use_fused(c, precision);
+  if (fused && (rc = ensure_workspace(c))) return rc;
+  const double gb = (double)c->g.csize * 8.0, wb = (double)c->uplan.wgrid * 8.0;
   for (int k = 0; k < ngrid; ++k) {
     CRAVA_CUDA_TRY(cudaMemcpyAsync(dev[k], host[k], gbytes, cudaMemcpyHostToDevice, c->s_in));
     CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[k], c->s_in));
     CRAVA_CUDA_TRY(cudaStreamWaitEvent(s, c->grid_ev[k], 0));
-    if ((rc = pass_forward(c, dev[k], dev[k], type[k]))) return rc;
+    if (fused) {
+      Scope sc(c, K_PLANE_FWD, gb + wb);
+      float2 *wk = c->W + (size_t)k * c->uplan.wgrid;
+      const float fsc = forward_scale(c->g, type[k]);
+      const float *src = dev[k];
+      if ((rc = unit_plane_forward(c->uplan, c->plans, &src, &wk, &fsc, 1, s))) return rc;
+    } else if ((rc = pass_forward(c, dev[k], dev[k], type[k]))) {
+      return rc;
+    }
   }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  if ((rc = pass_solve(c, &dg, precision))) return rc;
+  if (fused) {
+    float2 *w[kMaxUnitGrids];
+    for (int k = 0; k < ngrid; ++k) w[k] = c->W + (size_t)k * c->uplan.wgrid;
+    Scope sc(c, K_ZSOLVE, (2 * ngrid - 1) * wb);
+    if ((rc = unit_zsolve(c->uplan, c->plans, c->consts, c->tables, w, precision, c->counters, s))) return rc;
+  } else if ((rc = pass_solve(c, &dg, precision))) {
+    return rc;
+  }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   for (int k = 0; k < ngrid - 1; ++k) {  // the noise correlation is not an output
-    if ((rc = pass_inverse(c, dev[k], type[k]))) return rc;
+    if (fused) {
+      Scope sc(c, K_PLANE_INV, gb + wb);
+      const float2 *wk = c->W + (size_t)k * c->uplan.wgrid;
+      const float isc = inverse_scale(c->g, type[k]);
+      if ((rc = unit_plane_inverse(c->uplan, c->plans, &wk, &dev[k], &isc, nullptr, 1, s))) return rc;
+    } else if ((rc = pass_inverse(c, dev[k], type[k]))) {
+      return rc;
+    }
     CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[ngrid + k], s));
     CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->grid_ev[ngrid + k], 0));
     CRAVA_CUDA_TRY(cudaMemcpyAsync(host[k], dev[k], gbytes, cudaMemcpyDeviceToHost, c->s_out));

@@ -55,7 +55,7 @@ struct ColArgs {
 
 // ------------------------------------------------------------------ x pass
 template <int DIR, bool EVEN>
-__global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
+__global__ void __launch_bounds__(kThreads) k_rows(const __grid_constant__ RowArgs a) {
   extern __shared__ float2 sm[];
   const int n = a.rl.n;            // complex line length
   const int ld = n + 1;            // shared row pitch
@@ -72,18 +72,19 @@ __global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
   __syncthreads();
 
   if (DIR < 0) {
-    // forward: load
+    // forward: load (asynchronous copies for an even row; the scale is
+    // applied after the transform)
     for (int idx = tid; idx < kRows * n; idx += blockDim.x) {
       int r = idx / n, m = idx % n;
-      float2 v = make_float2(0.f, 0.f);
       if (r < nrows) {
         const float *row = a.src + (row0 + r) * a.rnxp;
-        if (EVEN) v = reinterpret_cast<const float2 *>(row)[m];
-        else v = make_float2(row[m], 0.f);
-        v = cscale(v, a.scale);
+        if (EVEN) cp_async8(bufA + r * ld + m, reinterpret_cast<const float2 *>(row) + m);
+        else bufA[r * ld + m] = make_float2(__ldg(row + m), 0.f);
+      } else {
+        bufA[r * ld + m] = make_float2(0.f, 0.f);
       }
-      bufA[r * ld + m] = v;
     }
+    cp_async_wait_all();
   } else {
     // inverse: load the half spectrum and build the line to transform
     for (int idx = tid; idx < kRows * n; idx += blockDim.x) {
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
     }
   }
   __syncthreads();
-  int which = stockham_lines<DIR>(bufA, bufB, a.rl.r, a.rl.nr, n, twl, kRows, ld, 1, false);
+  int which = stockham<DIR, false>(bufA, ld, 1, bufB, ld, 1, a.rl, twl, kRows);
   const float2 *res = which ? bufB : bufA;
 
   if (DIR < 0) {
@@ -129,14 +130,14 @@ __global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
         float2 d = csub(zk, zm);
         float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
         float2 X = cadd(e, cmul(post[k], o));
-        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = X;
+        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = cscale(X, a.scale);
       }
     } else {
       const int c = n / 2 + 1;
       for (int idx = tid; idx < kRows * c; idx += blockDim.x) {
         int r = idx / c, k = idx % c;
         if (r >= nrows) continue;
-        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = res[r * ld + k];
+        reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = cscale(res[r * ld + k], a.scale);
       }
     }
   } else {
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kThreads) k_rows(RowArgs a) {
 
 // ------------------------------------------------------------------ y / z pass
 template <int DIR>
-__global__ void __launch_bounds__(kThreads) k_cols(ColArgs a) {
+__global__ void __launch_bounds__(kThreads) k_cols(const __grid_constant__ ColArgs a) {
   extern __shared__ float2 sm[];
   const int n = a.rl.n;
   float2 *twl = sm;
@@ -181,12 +182,41 @@ __global__ void __launch_bounds__(kThreads) k_cols(ColArgs a) {
   for (int i = tid; i < n; i += blockDim.x) twl[i] = a.tw[i];
   for (int idx = tid; idx < kColTile * n; idx += blockDim.x) {
     int t = idx % kColTile, m = idx / kColTile;
-    bufA[m * kColTile + t] = t < nx ? base[m * a.elem_stride + t] : make_float2(0.f, 0.f);
+    if (t < nx) cp_async8(bufA + m * kColTile + t, base + m * a.elem_stride + t);
+    else bufA[m * kColTile + t] = make_float2(0.f, 0.f);
   }
+  cp_async_wait_all();
   __syncthreads();
-  int which = stockham_lines<DIR>(bufA, bufB, a.rl.r, a.rl.nr, n, twl, kColTile, 1, kColTile, true);
+  int which = stockham<DIR, true>(bufA, 1, kColTile, bufB, 1, kColTile, a.rl, twl, kColTile);
   const float2 *res = which ? bufB : bufA;
   for (int idx = tid; idx < kColTile * n; idx += blockDim.x) {
+    int t = idx % kColTile, m = idx / kColTile;
+    if (t < nx) base[m * a.elem_stride + t] = cscale(res[m * kColTile + t], a.scale);
+  }
+}
+
+// The same column pass with the line length N a compile-time constant.
+template <int N, int DIR>
+__global__ void __launch_bounds__(kThreads) k_cols_ct(const __grid_constant__ ColArgs a) {
+  extern __shared__ float2 sm[];
+  float2 *twl = sm;
+  float2 *bufA = twl + N;
+  float2 *bufB = bufA + kColTile * N;
+  const int x0 = blockIdx.x * kColTile;
+  const int nx = min(kColTile, a.ninner - x0);
+  float2 *base = a.data + (long long)blockIdx.y * a.outer_stride + x0;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += blockDim.x) twl[i] = a.tw[i];
+  for (int idx = tid; idx < kColTile * N; idx += blockDim.x) {
+    int t = idx % kColTile, m = idx / kColTile;
+    if (t < nx) cp_async8(bufA + m * kColTile + t, base + m * a.elem_stride + t);
+    else bufA[m * kColTile + t] = make_float2(0.f, 0.f);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int which = stockham_ct<N, DIR, true, kColTile, 1, kColTile, 1, kColTile>(bufA, bufB, twl);
+  const float2 *res = which ? bufB : bufA;
+  for (int idx = tid; idx < kColTile * N; idx += blockDim.x) {
     int t = idx % kColTile, m = idx / kColTile;
     if (t < nx) base[m * a.elem_stride + t] = cscale(res[m * kColTile + t], a.scale);
   }
@@ -223,18 +253,30 @@ bool radix_list(int n, RadixList *out) {
   out->nr = 0;
   if (n < 1) return false;
   int m = n;
+  int r[16];
+  int nr = 0;
   // radix 8 while possible, then 4, then 2; then the odd primes.
-  while (m % 8 == 0) { out->r[out->nr++] = 8; m /= 8; }
-  while (m % 4 == 0) { out->r[out->nr++] = 4; m /= 4; }
-  while (m % 2 == 0) { out->r[out->nr++] = 2; m /= 2; }
-  const int odd[3] = {3, 5, 7};
-  for (int i = 0; i < 3; ++i)
-    while (m % odd[i] == 0) {
-      if (out->nr >= 16) return false;
-      out->r[out->nr++] = odd[i];
-      m /= odd[i];
+  const int order[6] = {8, 4, 2, 3, 5, 7};
+  for (int i = 0; i < 6; ++i)
+    while (m % order[i] == 0) {
+      if (nr >= 16) return false;
+      r[nr++] = order[i];
+      m /= order[i];
     }
-  return m == 1 && out->nr <= 16;
+  if (m != 1) return false;
+  int Ns = 1;
+  for (int s = 0; s < nr; ++s) {
+    Stage &st = out->st[s];
+    st.R = r[s];
+    st.Ns = Ns;
+    st.m = n / r[s];
+    st.tstep = n / (Ns * r[s]);
+    st.fNs = make_fastdiv((uint32_t)Ns);
+    st.fm = make_fastdiv((uint32_t)st.m);
+    Ns *= r[s];
+  }
+  out->nr = nr;
+  return true;
 }
 
 float forward_scale(const Geom &g, int type) {
@@ -316,6 +358,20 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
   const int n = lp.rl.n;
   size_t smem = sizeof(float2) * (n + 2 * kColTile * n);
   dim3 grd((ninner + kColTile - 1) / kColTile, nouter);
+#define CRAVA_COLS_CT(NN)                                                                   \
+  if (n == NN) {                                                                            \
+    const void *f = dir < 0 ? (const void *)k_cols_ct<NN, -1> : (const void *)k_cols_ct<NN, 1>; \
+    int r2 = set_smem(f, smem);                                                             \
+    if (r2) return r2;                                                                      \
+    if (dir < 0) k_cols_ct<NN, -1><<<grd, kThreads, smem, s>>>(a);                          \
+    else k_cols_ct<NN, 1><<<grd, kThreads, smem, s>>>(a);                                   \
+    CRAVA_LAUNCH_CHECK();                                                                   \
+    return CRAVA_GPU_OK;                                                                    \
+  }
+  CRAVA_COLS_CT(64) CRAVA_COLS_CT(128) CRAVA_COLS_CT(256) CRAVA_COLS_CT(512)
+  CRAVA_COLS_CT(96) CRAVA_COLS_CT(160) CRAVA_COLS_CT(192) CRAVA_COLS_CT(200) CRAVA_COLS_CT(300)
+  CRAVA_COLS_CT(384)
+#undef CRAVA_COLS_CT
   const void *fn = dir < 0 ? (const void *)k_cols<-1> : (const void *)k_cols<1>;
   int rc = set_smem(fn, smem);
   if (rc) return rc;

@@ -2,15 +2,9 @@
 #pragma once
 
 #include "common.cuh"
+#include "fft_core.cuh"
 
 namespace crava {
-
-// Radices of one line length, largest first (8, 4, 2, 3, 5, 7).
-struct RadixList {
-  int n;
-  int nr;
-  int r[16];
-};
 
 // Plan for one line length: radix list and twiddle table e^{-2 pi i k/n}
 // (n entries, float2) in device memory.

@@ -142,71 +142,217 @@ template <int DIR> struct Dft<3, DIR> : DftOdd<3, DIR> {};
 template <int DIR> struct Dft<5, DIR> : DftOdd<5, DIR> {};
 template <int DIR> struct Dft<7, DIR> : DftOdd<7, DIR> {};
 
-// One Stockham stage for every line held in shared memory.
-//   src/dst : line l element m at  l*ls + m*es
-//   tw      : e^{-2 pi i k/n}, k < n (shared memory)
-//   mapping : lines_fastest -> task = j*nlines + l, else task = l*(n/R) + j
-template <int R, int DIR>
-__device__ __forceinline__ void stockham_stage(const float2 *__restrict__ src,
-                                               float2 *__restrict__ dst, int n,
-                                               int Ns, const float2 *tw,
-                                               int nlines, int ls, int es,
-                                               bool lines_fastest, int tid,
+// Asynchronous global -> shared copies (cp.async, sm_80+): many copies per
+// thread stay in flight until cp_async_wait_all().
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+// Division by a runtime constant d >= 1 as a multiply-high and a shift
+// (round-up method of Granlund and Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994), valid for n < 2^31.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+__host__ __device__ inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f;
+  f.d = d;
+  f.s = 0;
+  while ((1u << f.s) < d) ++f.s;
+  f.m = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << f.s) - d)) / d + 1);
+  return f;
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
+  return (__umulhi(n, f.m) + n) >> f.s;
+}
+
+// One radix stage of a length-n line: R, the product Ns of the radices
+// before it, m = n / R, the twiddle step n / (Ns R), and fast dividers.
+struct Stage {
+  int R, Ns, m, tstep;
+  FastDiv fNs, fm;
+};
+
+// Radices of one line length, largest first (8, 4, 2, 3, 5, 7), with the
+// per-stage constants precomputed on the host.
+struct RadixList {
+  int n;
+  int nr;
+  Stage st[16];
+};
+
+// One Stockham stage over `nlines` lines held in shared memory:
+//   src line l element e at l*sls + e*ses, dst at l*dls + e*des.
+// LF (lines fastest): consecutive threads take consecutive lines, which is
+// conflict-free when the lines are adjacent words (element-major layouts);
+// otherwise consecutive threads take consecutive butterflies of one line.
+// Twiddles: tw[k] = e^{-2 pi i k / n}; the index q * base * tstep < n.
+template <int R, int DIR, bool LF>
+__device__ __forceinline__ void stockham_stage(const float2 *__restrict__ src, int sls, int ses,
+                                               float2 *__restrict__ dst, int dls, int des,
+                                               const Stage &sp, const float2 *__restrict__ tw,
+                                               int nlines, const FastDiv &fl, int tid,
                                                int nthreads) {
-  const int m = n / R;
+  const int m = sp.m;
   const int tasks = nlines * m;
-  const int tstep = n / (Ns * R);
   for (int task = tid; task < tasks; task += nthreads) {
     int l, j;
-    if (lines_fastest) { l = task % nlines; j = task / nlines; }
-    else { j = task % m; l = task / m; }
-    const float2 *s = src + l * ls;
+    if (LF) { j = (int)fdiv((uint32_t)task, fl); l = task - j * nlines; }
+    else { l = (int)fdiv((uint32_t)task, sp.fm); j = task - l * m; }
+    const int jq = (int)fdiv((uint32_t)j, sp.fNs);
+    const int base = j - jq * sp.Ns;
+    const float2 *sl = src + l * sls;
     float2 v[R];
-    const int base = j % Ns;
 #pragma unroll
-    for (int q = 0; q < R; ++q) v[q] = s[(j + q * m) * es];
+    for (int q = 0; q < R; ++q) v[q] = sl[(j + q * m) * ses];
     if (base != 0) {
-      const int step = base * tstep;
+      const int step = base * sp.tstep;
 #pragma unroll
       for (int q = 1; q < R; ++q) {
-        float2 w = tw[(q * step) % n];
+        float2 w = tw[q * step];
         if (DIR > 0) w.y = -w.y;
         v[q] = cmul(v[q], w);
       }
     }
     Dft<R, DIR>::run(v);
-    const int idxD = (j / Ns) * Ns * R + base;
-    float2 *d = dst + l * ls;
+    float2 *dl = dst + l * dls;
+    const int idxD = jq * sp.Ns * R + base;
 #pragma unroll
-    for (int q = 0; q < R; ++q) d[(idxD + q * Ns) * es] = v[q];
+    for (int q = 0; q < R; ++q) dl[(idxD + q * sp.Ns) * des] = v[q];
   }
 }
 
-// Runs every stage; returns which buffer (0 = a, 1 = b) holds the result.
-// The caller must __syncthreads() after filling `a` and `tw`.
-template <int DIR>
-__device__ int stockham_lines(float2 *a, float2 *b, const int *radix, int nr,
-                              int n, const float2 *tw, int nlines, int ls,
-                              int es, bool lines_fastest) {
+// All stages of a line transform, alternating between buffer a (layout
+// als/aes) and b (bls/bes).  Returns 0 if the result is in a, 1 if in b.
+// The caller synchronises before the call; every stage ends with a barrier.
+template <int DIR, bool LF>
+__device__ int stockham(float2 *a, int als, int aes, float2 *b, int bls, int bes,
+                        const RadixList &rl, const float2 *tw, int nlines) {
   const int tid = threadIdx.x, nt = blockDim.x;
+  const FastDiv fl = make_fastdiv((uint32_t)(nlines > 0 ? nlines : 1));
   float2 *src = a, *dst = b;
-  int Ns = 1, which = 0;
-  for (int st = 0; st < nr; ++st) {
-    const int R = radix[st];
-    switch (R) {
-      case 8: stockham_stage<8, DIR>(src, dst, n, Ns, tw, nlines, ls, es, lines_fastest, tid, nt); break;
-      case 4: stockham_stage<4, DIR>(src, dst, n, Ns, tw, nlines, ls, es, lines_fastest, tid, nt); break;
-      case 2: stockham_stage<2, DIR>(src, dst, n, Ns, tw, nlines, ls, es, lines_fastest, tid, nt); break;
-      case 3: stockham_stage<3, DIR>(src, dst, n, Ns, tw, nlines, ls, es, lines_fastest, tid, nt); break;
-      case 5: stockham_stage<5, DIR>(src, dst, n, Ns, tw, nlines, ls, es, lines_fastest, tid, nt); break;
-      default: stockham_stage<7, DIR>(src, dst, n, Ns, tw, nlines, ls, es, lines_fastest, tid, nt); break;
+  int sls = als, ses = aes, dls = bls, des = bes;
+  int which = 0;
+  for (int s = 0; s < rl.nr; ++s) {
+    const Stage &sp = rl.st[s];
+    switch (sp.R) {
+      case 8: stockham_stage<8, DIR, LF>(src, sls, ses, dst, dls, des, sp, tw, nlines, fl, tid, nt); break;
+      case 4: stockham_stage<4, DIR, LF>(src, sls, ses, dst, dls, des, sp, tw, nlines, fl, tid, nt); break;
+      case 2: stockham_stage<2, DIR, LF>(src, sls, ses, dst, dls, des, sp, tw, nlines, fl, tid, nt); break;
+      case 3: stockham_stage<3, DIR, LF>(src, sls, ses, dst, dls, des, sp, tw, nlines, fl, tid, nt); break;
+      case 5: stockham_stage<5, DIR, LF>(src, sls, ses, dst, dls, des, sp, tw, nlines, fl, tid, nt); break;
+      default: stockham_stage<7, DIR, LF>(src, sls, ses, dst, dls, des, sp, tw, nlines, fl, tid, nt); break;
     }
     __syncthreads();
-    Ns *= R;
     float2 *t = src; src = dst; dst = t;
+    int x = sls; sls = dls; dls = x;
+    x = ses; ses = des; des = x;
     which ^= 1;
   }
   return which;
+}
+
+}  // namespace crava
+
+namespace crava {
+
+// ---------------------------------------------------------------------------
+// Compile-time Stockham engine: the line length N, the number of lines NL
+// and the strides are template constants, so every index, stride and
+// twiddle step folds to constants (no runtime division).
+// Radices: 8 while possible, then 4, then 2, then 3, 5, 7 (as radix_list).
+// ---------------------------------------------------------------------------
+struct CtRadix {
+  __host__ __device__ static constexpr int at(int n, int s) {
+    int m = n, r = 1;
+    for (int i = 0; i <= s; ++i) {
+      r = (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : 1;
+      m /= r;
+    }
+    return r;
+  }
+  __host__ __device__ static constexpr int count(int n) {
+    int m = n, c = 0;
+    while (m > 1) {
+      int r = (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : m;
+      m /= r;
+      ++c;
+    }
+    return c;
+  }
+  __host__ __device__ static constexpr int ns(int n, int s) {
+    int p = 1;
+    for (int i = 0; i < s; ++i) p *= at(n, i);
+    return p;
+  }
+  __host__ __device__ static constexpr bool supported(int n) {
+    int m = n;
+    while (m % 2 == 0) m /= 2;
+    while (m % 3 == 0) m /= 3;
+    while (m % 5 == 0) m /= 5;
+    while (m % 7 == 0) m /= 7;
+    return m == 1 && n > 1;
+  }
+};
+
+template <int N, int R, int NS, int DIR, bool LF, int NL, int SLS, int SES, int DLS, int DES>
+__device__ __forceinline__ void ct_stage(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                         const float2 *__restrict__ tw, int tid, int nth) {
+  constexpr int M = N / R;
+  constexpr int TASKS = NL * M;
+  constexpr int TSTEP = N / (NS * R);
+  for (int task = tid; task < TASKS; task += nth) {
+    int l, j;
+    if (LF) { l = task % NL; j = task / NL; }
+    else { j = task % M; l = task / M; }
+    const int base = j % NS;
+    const float2 *sl = src + l * SLS + j * SES;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = sl[q * M * SES];
+    if (NS > 1 && base != 0) {
+      const int step = base * TSTEP;
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        float2 w = tw[q * step];
+        if (DIR > 0) w.y = -w.y;
+        v[q] = cmul(v[q], w);
+      }
+    }
+    Dft<R, DIR>::run(v);
+    float2 *dl = dst + l * DLS + ((j / NS) * NS * R + base) * DES;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dl[q * NS * DES] = v[q];
+  }
+}
+
+template <int N, int DIR, bool LF, int NL, int ALS, int AES, int BLS, int BES, int S>
+struct CtStages {
+  static __device__ __forceinline__ void run(float2 *a, float2 *b, const float2 *tw, int tid, int nth) {
+    if constexpr (S < CtRadix::count(N)) {
+      constexpr int R = CtRadix::at(N, S);
+      constexpr int NS = CtRadix::ns(N, S);
+      ct_stage<N, R, NS, DIR, LF, NL, ALS, AES, BLS, BES>(a, b, tw, tid, nth);
+      __syncthreads();
+      CtStages<N, DIR, LF, NL, BLS, BES, ALS, AES, S + 1>::run(b, a, tw, tid, nth);
+    }
+  }
+};
+
+// All stages; returns 0 if the result is in a, 1 if in b (odd stage count).
+template <int N, int DIR, bool LF, int NL, int ALS, int AES, int BLS, int BES>
+__device__ __forceinline__ int stockham_ct(float2 *a, float2 *b, const float2 *tw) {
+  CtStages<N, DIR, LF, NL, ALS, AES, BLS, BES, 0>::run(a, b, tw, threadIdx.x, blockDim.x);
+  return CtRadix::count(N) & 1;
 }
 
 }  // namespace crava

@@ -20,15 +20,14 @@
 #include <math.h>
 
 #include "solve.cuh"
+#include "solve_bin.cuh"
 
 namespace crava {
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr double kTol = 1e-20;  // libs/lib/lib_matr.c:20
-
-__host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+using sb::tri;
 
 // ------------------------------------------------------------------ tables
 __global__ void k_kz_tables(const float *__restrict__ wav,
@@ -112,101 +111,6 @@ __global__ void k_kz_tables(const float *__restrict__ wav,
   }
 }
 
-// ------------------------------------------------------------------ helpers
-struct Sym3d { double s00, s11, s22, s01, s02, s12; };
-
-__device__ __forceinline__ double sget(const Sym3d &s, int a, int b) {
-  if (a > b) { int t = a; a = b; b = t; }
-  return a == 0 ? (b == 0 ? s.s00 : b == 1 ? s.s01 : s.s02) : a == 1 ? (b == 1 ? s.s11 : s.s12) : s.s22;
-}
-
-// getNextParameterCovariance in double: S_pq = |Re(c)/v| v (no division if v == 0).
-__device__ __forceinline__ Sym3d prior_d(const float2 c6[6], const double v[6]) {
-  double r[6];
-#pragma unroll
-  for (int t = 0; t < 6; ++t) {
-    double x = c6[t].x;
-    r[t] = v[t] != 0.0 ? fabs(x / v[t]) * v[t] : fabs(x);
-  }
-  return Sym3d{r[0], r[1], r[2], r[3], r[4], r[5]};
-}
-
-// Same in float, with the reference's operations (float divide, |.|, float multiply).
-__device__ __forceinline__ void prior_f(const float2 c6[6], const double v[6], float r[6]) {
-#pragma unroll
-  for (int t = 0; t < 6; ++t) {
-    float vf = (float)v[t];
-    float x = c6[t].x;
-    if (v[t] != 0.0) x = x / vf;
-    r[t] = fabsf(x) * vf;
-  }
-}
-
-// Hermitian Cholesky M = L L^H on the lower triangle (tri() indexing), with
-// the reference's failure rules applied to M / M00.
-template <int NT, typename T2, typename T>
-__device__ __forceinline__ bool cholesky(T2 *L) {
-  const T factor = L[0].x;
-  if (!(factor > T(0))) return false;
-  const T tol = (T)kTol * factor;
-#pragma unroll
-  for (int i = 0; i < NT; ++i) {
-    if (!(L[tri(i, i)].x > tol)) return false;
-#pragma unroll
-    for (int j = 0; j < i; ++j) {
-      T2 s = L[tri(i, j)];
-#pragma unroll
-      for (int k = 0; k < j; ++k) {
-        T2 a = L[tri(i, k)], b = L[tri(j, k)];
-        s.x -= a.x * b.x + a.y * b.y;
-        s.y -= a.y * b.x - a.x * b.y;
-      }
-      T inv = T(1) / L[tri(j, j)].x;
-      s.x *= inv; s.y *= inv;
-      L[tri(i, j)] = s;
-    }
-    T d = L[tri(i, i)].x;
-#pragma unroll
-    for (int k = 0; k < i; ++k) d -= L[tri(i, k)].x * L[tri(i, k)].x + L[tri(i, k)].y * L[tri(i, k)].y;
-    if (!(d > tol)) return false;
-    L[tri(i, i)].x = sqrt(d);
-    L[tri(i, i)].y = T(0);
-  }
-  return true;
-}
-
-// Solves L L^H X = B in place for the 3 columns of B.
-template <int NT, typename T2, typename T>
-__device__ __forceinline__ void chol_solve3(const T2 *L, T2 (*B)[3]) {
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-#pragma unroll
-    for (int i = 0; i < NT; ++i) {
-      T2 s = B[i][c];
-#pragma unroll
-      for (int j = 0; j < i; ++j) {
-        T2 l = L[tri(i, j)], x = B[j][c];
-        s.x -= l.x * x.x - l.y * x.y;
-        s.y -= l.x * x.y + l.y * x.x;
-      }
-      T inv = T(1) / L[tri(i, i)].x;
-      B[i][c].x = s.x * inv; B[i][c].y = s.y * inv;
-    }
-#pragma unroll
-    for (int i = NT - 1; i >= 0; --i) {
-      T2 s = B[i][c];
-#pragma unroll
-      for (int j = i + 1; j < NT; ++j) {
-        T2 l = L[tri(j, i)], x = B[j][c];  // conj(l) * x
-        s.x -= l.x * x.x + l.y * x.y;
-        s.y -= l.x * x.y - l.y * x.x;
-      }
-      T inv = T(1) / L[tri(i, i)].x;
-      B[i][c].x = s.x * inv; B[i][c].y = s.y * inv;
-    }
-  }
-}
-
 struct SolveArgs {
   SolveConsts c;
   SolveGrids g;
@@ -215,27 +119,11 @@ struct SolveArgs {
   DevCounters *counters;
 };
 
-__device__ __forceinline__ void count(DevCounters *ctr, bool fail, bool nonfinite) {
-  unsigned m = __activemask();
-  unsigned bf = __ballot_sync(m, fail), bn = __ballot_sync(m, nonfinite);
-  int leader = __ffs(m) - 1;
-  if ((threadIdx.x & 31) == leader) {
-    if (bf) atomicAdd(&ctr->chol_fail, (unsigned long long)__popc(bf));
-    if (bn) atomicAdd(&ctr->nonfinite, (unsigned long long)__popc(bn));
-  }
-}
-
-__device__ __forceinline__ bool fin2(float2 v) { return isfinite(v.x) && isfinite(v.y); }
-
-// PREC 0: FP64 throughout.  PREC 1: FP32 build and factorisation, one FP64
-// refinement step on the residual K S - M X0, FP64 Schur update and mean.
 template <int NT, int PREC>
 __global__ void __launch_bounds__(kThreads) k_solve(SolveArgs a) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= a.csize) return;
   const int k = (int)(idx / a.plane);
-  const SolveConsts &c = a.c;
-
   float2 mu[3], d[NT], c6[6];
 #pragma unroll
   for (int q = 0; q < 3; ++q) mu[q] = a.g.mu[q][idx];
@@ -245,207 +133,17 @@ __global__ void __launch_bounds__(kThreads) k_solve(SolveArgs a) {
   for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
   const float2 ec = a.g.err[idx];
   const bool inv = a.t.inv[k] != 0;
-
-  const Sym3d S = prior_d(c6, c.var0);
-  float2 out_mu[3], out_r[NT];
-  double2 Sp[6];  // posterior (0,0) (1,1) (2,2) (0,1) (0,2) (1,2)
-  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
-  bool fail = false;
-  bool solved = false;
-  if (PREC == 1) {
-    float sf[6];
-    prior_f(c6, c.var0, sf);
-#pragma unroll
-    for (int t = 0; t < 6; ++t) Sp[t] = make_double2(sf[t], 0.0);
-  } else {
-#pragma unroll
-    for (int t = 0; t < 6; ++t) Sp[t] = make_double2(sget(S, pa[t], pb[t]), 0.0);
-  }
-
-  if (inv) {
-    const float2 *wdk = a.t.wd + (long long)k * NT;
-    const float2 *e1k = a.t.e1 + (long long)k * NT;
-    const float2 *e2k = a.t.e2 + (long long)k * NT;
-    const float *e3k = a.t.e3 + (long long)k * NT;
-    float2 wd[NT], e1[NT], e2[NT];
-    float e3[NT];
-#pragma unroll
-    for (int l = 0; l < NT; ++l) { wd[l] = __ldg(wdk + l); e1[l] = __ldg(e1k + l); e2[l] = __ldg(e2k + l); e3[l] = __ldg(e3k + l); }
-    const double lam = fabs((double)ec.x);
-    const double cc = 0.5 * (1.0 - (double)c.wnc);
-
-    // A S (real, double) and K S = diag(wd) A S
-    double AS[NT][3];
-#pragma unroll
-    for (int l = 0; l < NT; ++l)
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        AS[l][q] = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) + (double)c.A[l][2] * sget(S, 2, q);
-    double2 X[NT][3];
-
-    if (PREC == 0) {
-      double2 L[NT * (NT + 1) / 2];
-#pragma unroll
-      for (int l = 0; l < NT; ++l)
-#pragma unroll
-        for (int m = 0; m <= l; ++m) {
-          double B = AS[l][0] * c.A[m][0] + AS[l][1] * c.A[m][1] + AS[l][2] * c.A[m][2];
-          double2 w = dmulc(make_double2(wd[l].x, wd[l].y), make_double2(wd[m].x, wd[m].y));
-          double th = c.theta[l][m];
-          double2 n1 = dmulc(make_double2(e1[l].x, e1[l].y), make_double2(e1[m].x, e1[m].y));
-          double2 n2 = dmulc(make_double2(e2[l].x, e2[l].y), make_double2(e2[m].x, e2[m].y));
-          double f = cc * th * lam;
-          double2 v = make_double2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
-          if (l == m) { v.x += (double)c.wnc * th * (double)e3[l] * (double)e3[l]; v.y = 0.0; }
-          L[tri(l, m)] = v;
-        }
-#pragma unroll
-      for (int l = 0; l < NT; ++l)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) X[l][q] = make_double2(wd[l].x * AS[l][q], wd[l].y * AS[l][q]);
-      if (cholesky<NT, double2, double>(L)) {
-        chol_solve3<NT, double2, double>(L, X);
-        solved = true;
-      } else {
-        fail = true;
-      }
-    } else {
-      // FP32 build and factorisation
-      float sf[6];
-      prior_f(c6, c.var0, sf);
-      auto sgf = [&](int p, int q) -> float {
-        if (p > q) { int t = p; p = q; q = t; }
-        return p == 0 ? (q == 0 ? sf[0] : q == 1 ? sf[3] : sf[4]) : p == 1 ? (q == 1 ? sf[1] : sf[5]) : sf[2];
-      };
-      float ASf[NT][3];
-#pragma unroll
-      for (int l = 0; l < NT; ++l)
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-          ASf[l][q] = c.A[l][0] * sgf(0, q) + c.A[l][1] * sgf(1, q) + c.A[l][2] * sgf(2, q);
-      float2 Lf[NT * (NT + 1) / 2];
-      const float ff = (float)(cc * lam);
-#pragma unroll
-      for (int l = 0; l < NT; ++l)
-#pragma unroll
-        for (int m = 0; m <= l; ++m) {
-          float B = ASf[l][0] * c.A[m][0] + ASf[l][1] * c.A[m][1] + ASf[l][2] * c.A[m][2];
-          float2 w = cmulc(wd[l], wd[m]);
-          float th = (float)c.theta[l][m];
-          float2 n1 = cmulc(e1[l], e1[m]), n2 = cmulc(e2[l], e2[m]);
-          float f = ff * th;
-          float2 v = make_float2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
-          if (l == m) { v.x += c.wnc * th * e3[l] * e3[l]; v.y = 0.f; }
-          Lf[tri(l, m)] = v;
-        }
-      float2 Xf[NT][3];
-#pragma unroll
-      for (int l = 0; l < NT; ++l)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) Xf[l][q] = make_float2(wd[l].x * ASf[l][q], wd[l].y * ASf[l][q]);
-      if (cholesky<NT, float2, float>(Lf)) {
-        chol_solve3<NT, float2, float>(Lf, Xf);
-        // FP64 residual of the exact system: Rd = KS - M X0.
-        float2 Rf[NT][3];
-#pragma unroll
-        for (int l = 0; l < NT; ++l) {
-          double2 acc[3];
-#pragma unroll
-          for (int q = 0; q < 3; ++q) acc[q] = make_double2(wd[l].x * AS[l][q], wd[l].y * AS[l][q]);
-#pragma unroll
-          for (int m = 0; m < NT; ++m) {
-            // M_lm in double (Hermitian: M_lm = conj(M_ml))
-            double B = AS[l][0] * c.A[m][0] + AS[l][1] * c.A[m][1] + AS[l][2] * c.A[m][2];
-            double2 w = dmulc(make_double2(wd[l].x, wd[l].y), make_double2(wd[m].x, wd[m].y));
-            double th = c.theta[l][m];
-            double2 n1 = dmulc(make_double2(e1[l].x, e1[l].y), make_double2(e1[m].x, e1[m].y));
-            double2 n2 = dmulc(make_double2(e2[l].x, e2[l].y), make_double2(e2[m].x, e2[m].y));
-            double f = cc * th * lam;
-            double2 Mv = make_double2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
-            if (l == m) { Mv.x += (double)c.wnc * th * (double)e3[l] * (double)e3[l]; Mv.y = 0.0; }
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-              double2 x = make_double2(Xf[m][q].x, Xf[m][q].y);
-              acc[q] = dsub(acc[q], dmul(Mv, x));
-            }
-          }
-#pragma unroll
-          for (int q = 0; q < 3; ++q) Rf[l][q] = make_float2((float)acc[q].x, (float)acc[q].y);
-        }
-        chol_solve3<NT, float2, float>(Lf, Rf);
-#pragma unroll
-        for (int l = 0; l < NT; ++l)
-#pragma unroll
-          for (int q = 0; q < 3; ++q)
-            X[l][q] = make_double2((double)Xf[l][q].x + (double)Rf[l][q].x, (double)Xf[l][q].y + (double)Rf[l][q].y);
-        solved = true;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) Sp[t] = make_double2(sget(S, pa[t], pb[t]), 0.0);
-      } else {
-        fail = true;
-      }
-    }
-
-    if (solved) {
-      // S_post = S - (KS)^H X   (FP64)
-#pragma unroll
-      for (int t = 0; t < 6; ++t) {
-        const int p = pa[t], q = pb[t];
-        double2 r = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int l = 0; l < NT; ++l) {
-          double2 ks = make_double2(wd[l].x * AS[l][p], wd[l].y * AS[l][p]);
-          r = dadd(r, dmulc(X[l][q], ks));  // conj(ks) * X
-        }
-        Sp[t] = make_double2(Sp[t].x - r.x, Sp[t].y - r.y);
-      }
-      // mean and residual
-      double2 v[NT];
-#pragma unroll
-      for (int l = 0; l < NT; ++l) {
-        double2 km = make_double2(0, 0);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) km = dadd(km, make_double2(c.A[l][q] * (double)mu[q].x, c.A[l][q] * (double)mu[q].y));
-        km = dmul(make_double2(wd[l].x, wd[l].y), km);
-        v[l] = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
-      }
-      double2 mp[3];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        double2 s = make_double2(mu[q].x, mu[q].y);
-#pragma unroll
-        for (int l = 0; l < NT; ++l) s = dadd(s, dmulc(v[l], X[l][q]));  // conj(X) v
-        mp[q] = s;
-        out_mu[q] = make_float2((float)s.x, (float)s.y);
-      }
-#pragma unroll
-      for (int l = 0; l < NT; ++l) {
-        double2 km = make_double2(0, 0);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) km = dadd(km, make_double2(c.A[l][q] * mp[q].x, c.A[l][q] * mp[q].y));
-        km = dmul(make_double2(wd[l].x, wd[l].y), km);
-        out_r[l] = make_float2((float)((double)d[l].x - km.x), (float)((double)d[l].y - km.y));
-      }
-    }
-  }
-  if (!solved) {
-#pragma unroll
-    for (int q = 0; q < 3; ++q) out_mu[q] = mu[q];
-#pragma unroll
-    for (int l = 0; l < NT; ++l) out_r[l] = d[l];
-  }
+  const long long o = (long long)k * NT;
+  bool fail = sb::solve_bin<NT, PREC>(a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
+                                      mu, d, c6, ec);
   bool nonfinite = false;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) { a.g.mu[q][idx] = out_mu[q]; nonfinite |= !fin2(out_mu[q]); }
+  for (int q = 0; q < 3; ++q) { a.g.mu[q][idx] = mu[q]; nonfinite |= !sb::fin2(mu[q]); }
 #pragma unroll
-  for (int l = 0; l < NT; ++l) { a.g.data[l][idx] = out_r[l]; nonfinite |= !fin2(out_r[l]); }
+  for (int l = 0; l < NT; ++l) { a.g.data[l][idx] = d[l]; nonfinite |= !sb::fin2(d[l]); }
 #pragma unroll
-  for (int t = 0; t < 6; ++t) {
-    float2 o = make_float2((float)Sp[t].x, (float)Sp[t].y);
-    a.g.cov[t][idx] = o;
-    nonfinite |= !fin2(o);
-  }
-  if (a.counters) count(a.counters, fail, nonfinite);
+  for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
+  if (a.counters) sb::count(a.counters, fail, nonfinite);
 }
 
 template <int PREC>

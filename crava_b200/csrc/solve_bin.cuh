@@ -1,0 +1,669 @@
+// solve_bin.cuh -- the per-bin posterior solve as a device function, shared
+// by the standalone solve kernel (solve.cu) and the fused z-transform + solve
+// kernel (unit.cu).  See solve.cu for the algebra and the reference lines.
+#pragma once
+
+#include <math.h>
+
+#include "solve.cuh"
+
+namespace crava {
+namespace sb {
+
+constexpr double kTol = 1e-20;  // libs/lib/lib_matr.c:20
+
+__host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+
+struct Sym3d { double s00, s11, s22, s01, s02, s12; };
+
+__device__ __forceinline__ double sget(const Sym3d &s, int a, int b) {
+  if (a > b) { int t = a; a = b; b = t; }
+  return a == 0 ? (b == 0 ? s.s00 : b == 1 ? s.s01 : s.s02) : a == 1 ? (b == 1 ? s.s11 : s.s12) : s.s22;
+}
+
+// getNextParameterCovariance in double: S_pq = |Re(c)/v| v (no division if v == 0).
+__device__ __forceinline__ Sym3d prior_d(const float2 c6[6], const double v[6]) {
+  double r[6];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    double x = c6[t].x;
+    r[t] = v[t] != 0.0 ? fabs(x / v[t]) * v[t] : fabs(x);
+  }
+  return Sym3d{r[0], r[1], r[2], r[3], r[4], r[5]};
+}
+
+// Same in float, with the reference's operations (float divide, |.|, float multiply).
+__device__ __forceinline__ void prior_f(const float2 c6[6], const double v[6], float r[6]) {
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    float vf = (float)v[t];
+    float x = c6[t].x;
+    if (v[t] != 0.0) x = x / vf;
+    r[t] = fabsf(x) * vf;
+  }
+}
+
+// Hermitian Cholesky M = L L^H on the lower triangle (tri() indexing), with
+// the reference's failure rules applied to M / M00.
+template <int NT, typename T2, typename T>
+__device__ __forceinline__ bool cholesky(T2 *L) {
+  const T factor = L[0].x;
+  if (!(factor > T(0))) return false;
+  const T tol = (T)kTol * factor;
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    if (!(L[tri(i, i)].x > tol)) return false;
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      T2 s = L[tri(i, j)];
+#pragma unroll
+      for (int k = 0; k < j; ++k) {
+        T2 a = L[tri(i, k)], b = L[tri(j, k)];
+        s.x -= a.x * b.x + a.y * b.y;
+        s.y -= a.y * b.x - a.x * b.y;
+      }
+      T inv = T(1) / L[tri(j, j)].x;
+      s.x *= inv; s.y *= inv;
+      L[tri(i, j)] = s;
+    }
+    T d = L[tri(i, i)].x;
+#pragma unroll
+    for (int k = 0; k < i; ++k) d -= L[tri(i, k)].x * L[tri(i, k)].x + L[tri(i, k)].y * L[tri(i, k)].y;
+    if (!(d > tol)) return false;
+    L[tri(i, i)].x = sqrt(d);
+    L[tri(i, i)].y = T(0);
+  }
+  return true;
+}
+
+// Solves L L^H X = B in place for the 3 columns of B.
+template <int NT, typename T2, typename T>
+__device__ __forceinline__ void chol_solve3(const T2 *L, T2 (*B)[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      T2 s = B[i][c];
+#pragma unroll
+      for (int j = 0; j < i; ++j) {
+        T2 l = L[tri(i, j)], x = B[j][c];
+        s.x -= l.x * x.x - l.y * x.y;
+        s.y -= l.x * x.y + l.y * x.x;
+      }
+      T inv = T(1) / L[tri(i, i)].x;
+      B[i][c].x = s.x * inv; B[i][c].y = s.y * inv;
+    }
+#pragma unroll
+    for (int i = NT - 1; i >= 0; --i) {
+      T2 s = B[i][c];
+#pragma unroll
+      for (int j = i + 1; j < NT; ++j) {
+        T2 l = L[tri(j, i)], x = B[j][c];  // conj(l) * x
+        s.x -= l.x * x.x + l.y * x.y;
+        s.y -= l.x * x.y - l.y * x.x;
+      }
+      T inv = T(1) / L[tri(i, i)].x;
+      B[i][c].x = s.x * inv; B[i][c].y = s.y * inv;
+    }
+  }
+}
+
+__device__ __forceinline__ void count(DevCounters *ctr, bool fail, bool nonfinite) {
+  unsigned m = __activemask();
+  unsigned bf = __ballot_sync(m, fail), bn = __ballot_sync(m, nonfinite);
+  int leader = __ffs(m) - 1;
+  if ((threadIdx.x & 31) == leader) {
+    if (bf) atomicAdd(&ctr->chol_fail, (unsigned long long)__popc(bf));
+    if (bn) atomicAdd(&ctr->nonfinite, (unsigned long long)__popc(bn));
+  }
+}
+
+__device__ __forceinline__ bool fin2(float2 v) { return isfinite(v.x) && isfinite(v.y); }
+
+// PREC 0: FP64 throughout.  PREC 1: FP32 build and factorisation, one FP64
+// refinement step on the residual K S - M X0, FP64 Schur update and mean.
+
+// FP64 form, one right-hand side at a time to bound register use: M (lower
+// triangle, double) is built and factorised; then for each column q of
+// K S the system M x = (K S)_q is solved, the posterior covariance entries
+// (p, q), p <= q, are updated (S_pq - (KS)_p^H x) and the mean correction
+// conj(x)^T (d - K mu) is accumulated.  Same algebra as the dense form.
+template <int NT>
+__device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float2 *__restrict__ wdk,
+                                               const float2 *__restrict__ e1k,
+                                               const float2 *__restrict__ e2k,
+                                               const float *__restrict__ e3k, bool inv,
+                                               float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+  const Sym3d S = prior_d(c6, c.var0);
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
+  if (!inv) return false;
+  double2 L[NT * (NT + 1) / 2];
+  {
+    const double lam = fabs((double)ec.x);
+    const double cc = 0.5 * (1.0 - (double)c.wnc) * lam;
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      double as0 = 0, as1 = 0, as2 = 0;  // (A S)_l
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        as0 += (double)c.A[l][r] * sget(S, r, 0);
+        as1 += (double)c.A[l][r] * sget(S, r, 1);
+        as2 += (double)c.A[l][r] * sget(S, r, 2);
+      }
+      const float2 wl = __ldg(wdk + l), e1l = __ldg(e1k + l), e2l = __ldg(e2k + l);
+#pragma unroll
+      for (int m = 0; m <= l; ++m) {
+        const double B = as0 * c.A[m][0] + as1 * c.A[m][1] + as2 * c.A[m][2];
+        const float2 wm = __ldg(wdk + m), e1m = __ldg(e1k + m), e2m = __ldg(e2k + m);
+        const double2 w = dmulc(make_double2(wl.x, wl.y), make_double2(wm.x, wm.y));
+        const double2 n1 = dmulc(make_double2(e1l.x, e1l.y), make_double2(e1m.x, e1m.y));
+        const double2 n2 = dmulc(make_double2(e2l.x, e2l.y), make_double2(e2m.x, e2m.y));
+        const double f = cc * c.theta[l][m];
+        double2 v = make_double2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
+        if (l == m) {
+          const double e3 = (double)__ldg(e3k + l);
+          v.x += (double)c.wnc * c.theta[l][l] * e3 * e3;
+          v.y = 0.0;
+        }
+        L[tri(l, m)] = v;
+      }
+    }
+  }
+  if (!cholesky<NT, double2, double>(L)) return true;
+  double2 mp[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double2 x[NT];
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      const double as = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) +
+                        (double)c.A[l][2] * sget(S, 2, q);
+      const float2 wl = __ldg(wdk + l);
+      x[l] = make_double2(wl.x * as, wl.y * as);
+    }
+    // L y = x, then L^H x = y
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      double2 s = x[i];
+#pragma unroll
+      for (int j = 0; j < i; ++j) {
+        const double2 lij = L[tri(i, j)], xj = x[j];
+        s.x -= lij.x * xj.x - lij.y * xj.y;
+        s.y -= lij.x * xj.y + lij.y * xj.x;
+      }
+      const double inv_d = 1.0 / L[tri(i, i)].x;
+      x[i] = make_double2(s.x * inv_d, s.y * inv_d);
+    }
+#pragma unroll
+    for (int i = NT - 1; i >= 0; --i) {
+      double2 s = x[i];
+#pragma unroll
+      for (int j = i + 1; j < NT; ++j) {
+        const double2 lji = L[tri(j, i)], xj = x[j];  // conj(lji) * xj
+        s.x -= lji.x * xj.x + lji.y * xj.y;
+        s.y -= lji.x * xj.y - lji.y * xj.x;
+      }
+      const double inv_d = 1.0 / L[tri(i, i)].x;
+      x[i] = make_double2(s.x * inv_d, s.y * inv_d);
+    }
+    // posterior covariance entries (p, q), p <= q
+#pragma unroll
+    for (int p = 0; p <= q; ++p) {
+      double2 r = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int l = 0; l < NT; ++l) {
+        const double as = (double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
+                          (double)c.A[l][2] * sget(S, 2, p);
+        const float2 wl = __ldg(wdk + l);
+        r = dadd(r, dmulc(x[l], make_double2(wl.x * as, wl.y * as)));  // conj(ks) x
+      }
+      const int t = p == q ? p : (p == 0 ? (q == 1 ? 3 : 4) : 5);
+      c6[t] = make_float2((float)(sget(S, p, q) - r.x), (float)(-r.y));
+    }
+    // mean correction conj(x)^T (d - K mu)
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        km = dadd(km, make_double2(c.A[l][r] * (double)mu[r].x, c.A[l][r] * (double)mu[r].y));
+      const float2 wl = __ldg(wdk + l);
+      km = dmul(make_double2(wl.x, wl.y), km);
+      const double2 v = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
+      acc = dadd(acc, dmulc(v, x[l]));
+    }
+    mp[q] = dadd(mp[q], acc);
+  }
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * mp[r].x, c.A[l][r] * mp[r].y));
+    const float2 wl = __ldg(wdk + l);
+    km = dmul(make_double2(wl.x, wl.y), km);
+    d[l] = make_float2((float)((double)d[l].x - km.x), (float)((double)d[l].y - km.y));
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) mu[q] = make_float2((float)mp[q].x, (float)mp[q].y);
+  return false;
+}
+
+// Mixed form, one right-hand side at a time: M is built in FP32 and
+// factorised in FP32 (Lf); M is also kept in FP64 (Md, lower triangle) for
+// the refinement residual.  For each column q of K S: x0 = M^-1 (KS)_q in
+// FP32, r = (KS)_q - M x0 in FP64, x = x0 + M^-1 r (FP32 solve of r, FP64
+// add); the posterior covariance entries S_pq - (KS)_p^H x and the mean
+// correction are formed in FP64.
+template <int NT>
+__device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const float2 *__restrict__ wdk,
+                                                const float2 *__restrict__ e1k,
+                                                const float2 *__restrict__ e2k,
+                                                const float *__restrict__ e3k, bool inv,
+                                                float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+  const Sym3d S = prior_d(c6, c.var0);
+  float sf[6];
+  prior_f(c6, c.var0, sf);
+  // outside the band (or on failure) the reference keeps its float prior
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int t = 0; t < 6; ++t) c6[t] = make_float2(sf[t], 0.f);
+  if (!inv) return false;
+  auto sgf = [&](int p, int q) -> float {
+    if (p > q) { int t = p; p = q; q = t; }
+    return p == 0 ? (q == 0 ? sf[0] : q == 1 ? sf[3] : sf[4]) : p == 1 ? (q == 1 ? sf[1] : sf[5]) : sf[2];
+  };
+  float2 Lf[NT * (NT + 1) / 2];
+  double2 Md[NT * (NT + 1) / 2];
+  {
+    const double lam = fabs((double)ec.x);
+    const double cc = 0.5 * (1.0 - (double)c.wnc) * lam;
+    const float ccf = (float)cc;
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      double as0 = 0, as1 = 0, as2 = 0;
+      float af0 = 0.f, af1 = 0.f, af2 = 0.f;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        as0 += (double)c.A[l][r] * sget(S, r, 0);
+        as1 += (double)c.A[l][r] * sget(S, r, 1);
+        as2 += (double)c.A[l][r] * sget(S, r, 2);
+        af0 += c.A[l][r] * sgf(r, 0);
+        af1 += c.A[l][r] * sgf(r, 1);
+        af2 += c.A[l][r] * sgf(r, 2);
+      }
+      const float2 wl = __ldg(wdk + l), e1l = __ldg(e1k + l), e2l = __ldg(e2k + l);
+#pragma unroll
+      for (int m = 0; m <= l; ++m) {
+        const float2 wm = __ldg(wdk + m), e1m = __ldg(e1k + m), e2m = __ldg(e2k + m);
+        const double th = c.theta[l][m];
+        // FP64 copy
+        {
+          const double B = as0 * c.A[m][0] + as1 * c.A[m][1] + as2 * c.A[m][2];
+          const double2 w = dmulc(make_double2(wl.x, wl.y), make_double2(wm.x, wm.y));
+          const double2 n1 = dmulc(make_double2(e1l.x, e1l.y), make_double2(e1m.x, e1m.y));
+          const double2 n2 = dmulc(make_double2(e2l.x, e2l.y), make_double2(e2m.x, e2m.y));
+          const double f = cc * th;
+          double2 v = make_double2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
+          if (l == m) {
+            const double e3 = (double)__ldg(e3k + l);
+            v.x += (double)c.wnc * th * e3 * e3;
+            v.y = 0.0;
+          }
+          Md[tri(l, m)] = v;
+        }
+        // FP32 build
+        {
+          const float B = af0 * c.A[m][0] + af1 * c.A[m][1] + af2 * c.A[m][2];
+          const float2 w = cmulc(wl, wm), n1 = cmulc(e1l, e1m), n2 = cmulc(e2l, e2m);
+          const float f = ccf * (float)th;
+          float2 v = make_float2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
+          if (l == m) {
+            const float e3 = __ldg(e3k + l);
+            v.x += c.wnc * (float)th * e3 * e3;
+            v.y = 0.f;
+          }
+          Lf[tri(l, m)] = v;
+        }
+      }
+    }
+  }
+  if (!cholesky<NT, float2, float>(Lf)) return true;
+#pragma unroll
+  for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
+  double2 mp[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double2 ks[NT];
+    float2 x0[NT][3];  // column 0 used; solver works on [.][3] arrays
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      const double as = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) +
+                        (double)c.A[l][2] * sget(S, 2, q);
+      const float2 wl = __ldg(wdk + l);
+      ks[l] = make_double2(wl.x * as, wl.y * as);
+      x0[l][0] = make_float2((float)ks[l].x, (float)ks[l].y);
+    }
+    // x0 = M^-1 ks (FP32), column 0 only
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      float2 sacc = x0[i][0];
+#pragma unroll
+      for (int j = 0; j < i; ++j) {
+        const float2 lij = Lf[tri(i, j)], xj = x0[j][0];
+        sacc.x -= lij.x * xj.x - lij.y * xj.y;
+        sacc.y -= lij.x * xj.y + lij.y * xj.x;
+      }
+      const float id = 1.f / Lf[tri(i, i)].x;
+      x0[i][0] = make_float2(sacc.x * id, sacc.y * id);
+    }
+#pragma unroll
+    for (int i = NT - 1; i >= 0; --i) {
+      float2 sacc = x0[i][0];
+#pragma unroll
+      for (int j = i + 1; j < NT; ++j) {
+        const float2 lji = Lf[tri(j, i)], xj = x0[j][0];
+        sacc.x -= lji.x * xj.x + lji.y * xj.y;
+        sacc.y -= lji.x * xj.y - lji.y * xj.x;
+      }
+      const float id = 1.f / Lf[tri(i, i)].x;
+      x0[i][0] = make_float2(sacc.x * id, sacc.y * id);
+    }
+    // FP64 residual r = ks - Md x0, stored as the float right-hand side
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      double2 acc = ks[l];
+#pragma unroll
+      for (int m = 0; m < NT; ++m) {
+        const double2 Mlm = m <= l ? Md[tri(l, m)] : make_double2(Md[tri(m, l)].x, -Md[tri(m, l)].y);
+        acc = dsub(acc, dmul(Mlm, make_double2(x0[m][0].x, x0[m][0].y)));
+      }
+      x0[l][1] = make_float2((float)acc.x, (float)acc.y);
+    }
+    // correction solve (FP32) on column 1
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      float2 sacc = x0[i][1];
+#pragma unroll
+      for (int j = 0; j < i; ++j) {
+        const float2 lij = Lf[tri(i, j)], xj = x0[j][1];
+        sacc.x -= lij.x * xj.x - lij.y * xj.y;
+        sacc.y -= lij.x * xj.y + lij.y * xj.x;
+      }
+      const float id = 1.f / Lf[tri(i, i)].x;
+      x0[i][1] = make_float2(sacc.x * id, sacc.y * id);
+    }
+#pragma unroll
+    for (int i = NT - 1; i >= 0; --i) {
+      float2 sacc = x0[i][1];
+#pragma unroll
+      for (int j = i + 1; j < NT; ++j) {
+        const float2 lji = Lf[tri(j, i)], xj = x0[j][1];
+        sacc.x -= lji.x * xj.x + lji.y * xj.y;
+        sacc.y -= lji.x * xj.y - lji.y * xj.x;
+      }
+      const float id = 1.f / Lf[tri(i, i)].x;
+      x0[i][1] = make_float2(sacc.x * id, sacc.y * id);
+    }
+    double2 x[NT];
+#pragma unroll
+    for (int l = 0; l < NT; ++l)
+      x[l] = make_double2((double)x0[l][0].x + (double)x0[l][1].x, (double)x0[l][0].y + (double)x0[l][1].y);
+    // FP64 Schur update of the entries (p, q), p <= q
+#pragma unroll
+    for (int p = 0; p <= q; ++p) {
+      double2 r = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int l = 0; l < NT; ++l) {
+        const double as = (double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
+                          (double)c.A[l][2] * sget(S, 2, p);
+        const float2 wl = __ldg(wdk + l);
+        r = dadd(r, dmulc(x[l], make_double2(wl.x * as, wl.y * as)));
+      }
+      const int t = p == q ? p : (p == 0 ? (q == 1 ? 3 : 4) : 5);
+      c6[t] = make_float2((float)(sget(S, p, q) - r.x), (float)(-r.y));
+    }
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        km = dadd(km, make_double2(c.A[l][r] * (double)mu[r].x, c.A[l][r] * (double)mu[r].y));
+      const float2 wl = __ldg(wdk + l);
+      km = dmul(make_double2(wl.x, wl.y), km);
+      const double2 v = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
+      acc = dadd(acc, dmulc(v, x[l]));
+    }
+    mp[q] = dadd(mp[q], acc);
+  }
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * mp[r].x, c.A[l][r] * mp[r].y));
+    const float2 wl = __ldg(wdk + l);
+    km = dmul(make_double2(wl.x, wl.y), km);
+    d[l] = make_float2((float)((double)d[l].x - km.x), (float)((double)d[l].y - km.y));
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) mu[q] = make_float2((float)mp[q].x, (float)mp[q].y);
+  return false;
+}
+
+// One bin.  In: mu[3], d[NT], c6[6] (the six prior spectra), ec (noise
+// correlation spectrum), the bin's kz tables and its band flag.  Out (in
+// place): mu <- posterior mean, d <- residual, c6 <- posterior covariance
+// (0,0) (1,1) (2,2) (0,1) (0,2) (1,2).  Returns true when an inverted bin's
+// factorisation failed (the prior is kept, as src/crava.cpp:1109-1111).
+// PREC 0: FP64 throughout.  PREC 1: FP32 build and factorisation, one FP64
+// refinement step on the residual K S - M X0, FP64 Schur update and mean.
+template <int NT, int PREC>
+__device__ __forceinline__ bool solve_bin(const SolveConsts &c, const float2 *__restrict__ wdk,
+                                          const float2 *__restrict__ e1k,
+                                          const float2 *__restrict__ e2k,
+                                          const float *__restrict__ e3k, bool inv,
+                                          float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+  if (PREC == 0) return solve_bin_fp64<NT>(c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
+  if (PREC == 1) return solve_bin_mixed<NT>(c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
+  float2 out_mu[3], out_r[NT];
+  const Sym3d S = prior_d(c6, c.var0);
+  double2 Sp[6];  // posterior (0,0) (1,1) (2,2) (0,1) (0,2) (1,2)
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+  bool fail = false;
+  bool solved = false;
+  if (PREC == 1) {
+    float sf[6];
+    prior_f(c6, c.var0, sf);
+#pragma unroll
+    for (int t = 0; t < 6; ++t) Sp[t] = make_double2(sf[t], 0.0);
+  } else {
+#pragma unroll
+    for (int t = 0; t < 6; ++t) Sp[t] = make_double2(sget(S, pa[t], pb[t]), 0.0);
+  }
+
+  if (inv) {
+    float2 wd[NT], e1[NT], e2[NT];
+    float e3[NT];
+#pragma unroll
+    for (int l = 0; l < NT; ++l) { wd[l] = __ldg(wdk + l); e1[l] = __ldg(e1k + l); e2[l] = __ldg(e2k + l); e3[l] = __ldg(e3k + l); }
+    const double lam = fabs((double)ec.x);
+    const double cc = 0.5 * (1.0 - (double)c.wnc);
+
+    // A S (real, double) and K S = diag(wd) A S
+    double AS[NT][3];
+#pragma unroll
+    for (int l = 0; l < NT; ++l)
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        AS[l][q] = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) + (double)c.A[l][2] * sget(S, 2, q);
+    double2 X[NT][3];
+
+    if (PREC == 0) {
+      double2 L[NT * (NT + 1) / 2];
+#pragma unroll
+      for (int l = 0; l < NT; ++l)
+#pragma unroll
+        for (int m = 0; m <= l; ++m) {
+          double B = AS[l][0] * c.A[m][0] + AS[l][1] * c.A[m][1] + AS[l][2] * c.A[m][2];
+          double2 w = dmulc(make_double2(wd[l].x, wd[l].y), make_double2(wd[m].x, wd[m].y));
+          double th = c.theta[l][m];
+          double2 n1 = dmulc(make_double2(e1[l].x, e1[l].y), make_double2(e1[m].x, e1[m].y));
+          double2 n2 = dmulc(make_double2(e2[l].x, e2[l].y), make_double2(e2[m].x, e2[m].y));
+          double f = cc * th * lam;
+          double2 v = make_double2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
+          if (l == m) { v.x += (double)c.wnc * th * (double)e3[l] * (double)e3[l]; v.y = 0.0; }
+          L[tri(l, m)] = v;
+        }
+#pragma unroll
+      for (int l = 0; l < NT; ++l)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) X[l][q] = make_double2(wd[l].x * AS[l][q], wd[l].y * AS[l][q]);
+      if (cholesky<NT, double2, double>(L)) {
+        chol_solve3<NT, double2, double>(L, X);
+        solved = true;
+      } else {
+        fail = true;
+      }
+    } else {
+      // FP32 build and factorisation
+      float sf[6];
+      prior_f(c6, c.var0, sf);
+      auto sgf = [&](int p, int q) -> float {
+        if (p > q) { int t = p; p = q; q = t; }
+        return p == 0 ? (q == 0 ? sf[0] : q == 1 ? sf[3] : sf[4]) : p == 1 ? (q == 1 ? sf[1] : sf[5]) : sf[2];
+      };
+      float ASf[NT][3];
+#pragma unroll
+      for (int l = 0; l < NT; ++l)
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          ASf[l][q] = c.A[l][0] * sgf(0, q) + c.A[l][1] * sgf(1, q) + c.A[l][2] * sgf(2, q);
+      float2 Lf[NT * (NT + 1) / 2];
+      const float ff = (float)(cc * lam);
+#pragma unroll
+      for (int l = 0; l < NT; ++l)
+#pragma unroll
+        for (int m = 0; m <= l; ++m) {
+          float B = ASf[l][0] * c.A[m][0] + ASf[l][1] * c.A[m][1] + ASf[l][2] * c.A[m][2];
+          float2 w = cmulc(wd[l], wd[m]);
+          float th = (float)c.theta[l][m];
+          float2 n1 = cmulc(e1[l], e1[m]), n2 = cmulc(e2[l], e2[m]);
+          float f = ff * th;
+          float2 v = make_float2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
+          if (l == m) { v.x += c.wnc * th * e3[l] * e3[l]; v.y = 0.f; }
+          Lf[tri(l, m)] = v;
+        }
+      float2 Xf[NT][3];
+#pragma unroll
+      for (int l = 0; l < NT; ++l)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) Xf[l][q] = make_float2(wd[l].x * ASf[l][q], wd[l].y * ASf[l][q]);
+      if (cholesky<NT, float2, float>(Lf)) {
+        chol_solve3<NT, float2, float>(Lf, Xf);
+        // FP64 residual of the exact system: Rd = KS - M X0.
+        float2 Rf[NT][3];
+#pragma unroll
+        for (int l = 0; l < NT; ++l) {
+          double2 acc[3];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) acc[q] = make_double2(wd[l].x * AS[l][q], wd[l].y * AS[l][q]);
+#pragma unroll
+          for (int m = 0; m < NT; ++m) {
+            // M_lm in double (Hermitian: M_lm = conj(M_ml))
+            double B = AS[l][0] * c.A[m][0] + AS[l][1] * c.A[m][1] + AS[l][2] * c.A[m][2];
+            double2 w = dmulc(make_double2(wd[l].x, wd[l].y), make_double2(wd[m].x, wd[m].y));
+            double th = c.theta[l][m];
+            double2 n1 = dmulc(make_double2(e1[l].x, e1[l].y), make_double2(e1[m].x, e1[m].y));
+            double2 n2 = dmulc(make_double2(e2[l].x, e2[l].y), make_double2(e2[m].x, e2[m].y));
+            double f = cc * th * lam;
+            double2 Mv = make_double2(w.x * B + f * (n1.x + n2.x), w.y * B + f * (n1.y + n2.y));
+            if (l == m) { Mv.x += (double)c.wnc * th * (double)e3[l] * (double)e3[l]; Mv.y = 0.0; }
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              double2 x = make_double2(Xf[m][q].x, Xf[m][q].y);
+              acc[q] = dsub(acc[q], dmul(Mv, x));
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 3; ++q) Rf[l][q] = make_float2((float)acc[q].x, (float)acc[q].y);
+        }
+        chol_solve3<NT, float2, float>(Lf, Rf);
+#pragma unroll
+        for (int l = 0; l < NT; ++l)
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+            X[l][q] = make_double2((double)Xf[l][q].x + (double)Rf[l][q].x, (double)Xf[l][q].y + (double)Rf[l][q].y);
+        solved = true;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) Sp[t] = make_double2(sget(S, pa[t], pb[t]), 0.0);
+      } else {
+        fail = true;
+      }
+    }
+
+    if (solved) {
+      // S_post = S - (KS)^H X   (FP64)
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        const int p = pa[t], q = pb[t];
+        double2 r = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int l = 0; l < NT; ++l) {
+          double2 ks = make_double2(wd[l].x * AS[l][p], wd[l].y * AS[l][p]);
+          r = dadd(r, dmulc(X[l][q], ks));  // conj(ks) * X
+        }
+        Sp[t] = make_double2(Sp[t].x - r.x, Sp[t].y - r.y);
+      }
+      // mean and residual
+      double2 v[NT];
+#pragma unroll
+      for (int l = 0; l < NT; ++l) {
+        double2 km = make_double2(0, 0);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) km = dadd(km, make_double2(c.A[l][q] * (double)mu[q].x, c.A[l][q] * (double)mu[q].y));
+        km = dmul(make_double2(wd[l].x, wd[l].y), km);
+        v[l] = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
+      }
+      double2 mp[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        double2 s = make_double2(mu[q].x, mu[q].y);
+#pragma unroll
+        for (int l = 0; l < NT; ++l) s = dadd(s, dmulc(v[l], X[l][q]));  // conj(X) v
+        mp[q] = s;
+        out_mu[q] = make_float2((float)s.x, (float)s.y);
+      }
+#pragma unroll
+      for (int l = 0; l < NT; ++l) {
+        double2 km = make_double2(0, 0);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) km = dadd(km, make_double2(c.A[l][q] * mp[q].x, c.A[l][q] * mp[q].y));
+        km = dmul(make_double2(wd[l].x, wd[l].y), km);
+        out_r[l] = make_float2((float)((double)d[l].x - km.x), (float)((double)d[l].y - km.y));
+      }
+    }
+  }
+  if (!solved) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) out_mu[q] = mu[q];
+#pragma unroll
+    for (int l = 0; l < NT; ++l) out_r[l] = d[l];
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) mu[q] = out_mu[q];
+#pragma unroll
+  for (int l = 0; l < NT; ++l) d[l] = out_r[l];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)Sp[t].x, (float)Sp[t].y);
+  return fail;
+}
+
+}  // namespace sb
+}  // namespace crava

@@ -186,6 +186,18 @@ int crava_gpu_kz_tables(crava_gpu_ctx *ctx, float *wd, float *e1, float *e2,
 int crava_gpu_set_kz_tables(crava_gpu_ctx *ctx, const float *wd, const float *e1,
                             const float *e2, const float *e3, const int *inv);
 
+/* The unit calls use the three-pass transforms (x, y, z) and the separate
+ * per-bin solve by default.  After set_fused(ctx, 1) they use the fused
+ * kernels instead (xy-plane transforms with a thread block cluster, and one
+ * kernel for the z transform, the per-bin solve and the inverse z
+ * transform) when the grid fits them and the precision is FP64 or MIXED.
+ * The fused unit does not write the noise-correlation output grid (its
+ * transform is kept internally); the three-pass unit leaves it transformed.
+ * fused_available reports whether a call with `precision` could take the
+ * fused path. */
+int crava_gpu_set_fused(crava_gpu_ctx *ctx, int enable);
+int crava_gpu_fused_available(crava_gpu_ctx *ctx, int precision);
+
 /* Per-kernel device time (profiling mode records a CUDA event pair around
  * every launch of this context; off by default).  bytes_per_launch is the
  * algorithmic traffic of one launch: 2 grids for a transform pass (read +
