@@ -160,16 +160,10 @@ def run_own(args):
 
     from crava_b200 import api, synth
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
+    from crava_b200 import dist as D
 
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    rank, world, local = D.rank_env()
+    dist = D.init("nccl", timeout_s=300)
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
     nxp, nyp, nzp = (int(x) for x in args.grid.split(","))
@@ -186,15 +180,10 @@ def run_own(args):
     torch.cuda.synchronize(dev)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        D.barrier(dist)
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return D.max_over_ranks(dist, x, device=f"cuda:{dev}")
 
     def timed_steps(precision, steps, profile):
         ev0 = torch.cuda.Event(enable_timing=True)

@@ -1,0 +1,163 @@
+// crava_device.hpp -- C++ host classes over the C ABI (include/crava_gpu.h),
+// mirroring the reference interfaces this library replaces:
+//
+//   FFTGridDevice  the device counterpart of FFTGrid (src/fftgrid.h): one
+//                  padded grid in HBM, the same grid types and the same
+//                  fftInPlace / invFFTInPlace scalings;
+//   CravaDevice    the hot path of Crava (src/crava.h):
+//                  computePostMeanResidAndFFTCov and simulate.
+//
+// Header only; link with crava_b200/lib/libcrava_gpu.so and the CUDA
+// runtime.  Errors throw crava_b200::Error carrying the ABI status.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "crava_gpu.h"
+
+namespace crava_b200 {
+
+class Error : public std::runtime_error {
+ public:
+  Error(const std::string &what, int status)
+      : std::runtime_error(what + ": " + crava_gpu_status_string(status)), status_(status) {}
+  int status() const { return status_; }
+
+ private:
+  int status_;
+};
+
+inline void check(int status, const char *what) {
+  if (status != CRAVA_GPU_OK) throw Error(what, status);
+}
+
+// A padded grid resident in HBM (layout of src/fftgrid.cpp:37-67).
+class FFTGridDevice {
+ public:
+  // FFTGrid::gridTypes (src/fftgrid.h:172)
+  enum gridTypes { CTMISSING, DATA, PARAMETER, COVARIANCE };
+
+  FFTGridDevice(crava_gpu_ctx *ctx, int nxp, int nyp, int nzp, int type = PARAMETER)
+      : ctx_(ctx), nxp_(nxp), nyp_(nyp), nzp_(nzp), type_(type) {
+    cnxp_ = nxp / 2 + 1;
+    rnxp_ = 2 * cnxp_;
+    rsize_ = (long long)rnxp_ * nyp * nzp;
+    csize_ = (long long)cnxp_ * nyp * nzp;
+    if (cudaMalloc(&data_, sizeof(float) * rsize_) != cudaSuccess) throw Error("FFTGridDevice", CRAVA_GPU_ERR_ALLOC);
+  }
+  ~FFTGridDevice() { cudaFree(data_); }
+  FFTGridDevice(const FFTGridDevice &) = delete;
+  FFTGridDevice &operator=(const FFTGridDevice &) = delete;
+
+  void setType(int t) { type_ = t; }
+  int getType() const { return type_; }
+  bool getIsTransformed() const { return transformed_; }
+  void setTransformedStatus(bool s) { transformed_ = s; }
+  int getNxp() const { return nxp_; }
+  int getNyp() const { return nyp_; }
+  int getNzp() const { return nzp_; }
+  int getCNxp() const { return cnxp_; }
+  int getRNxp() const { return rnxp_; }
+  long long getcsize() const { return csize_; }
+  long long getrsize() const { return rsize_; }
+  float *devicePtr() { return data_; }
+
+  // FFTGrid::fftInPlace (src/fftgrid.cpp:1803-1829)
+  void fftInPlace() {
+    if (transformed_) throw Error("fftInPlace on a transformed grid", CRAVA_GPU_ERR_STATE);
+    check(crava_gpu_fft_r2c(ctx_, data_, type_), "fftInPlace");
+    transformed_ = true;
+  }
+  // FFTGrid::invFFTInPlace (src/fftgrid.cpp:1831-1862)
+  void invFFTInPlace() {
+    if (!transformed_) throw Error("invFFTInPlace on a real grid", CRAVA_GPU_ERR_STATE);
+    check(crava_gpu_fft_c2r(ctx_, data_, type_), "invFFTInPlace");
+    transformed_ = false;
+  }
+  // Bulk replacements of the setNextReal / getNextReal cursors.
+  void upload(const float *host, bool transformed = false) {
+    if (cudaMemcpy(data_, host, sizeof(float) * rsize_, cudaMemcpyHostToDevice) != cudaSuccess)
+      throw Error("upload", CRAVA_GPU_ERR_CUDA);
+    transformed_ = transformed;
+  }
+  void download(float *host) const {
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(host, data_, sizeof(float) * rsize_, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw Error("download", CRAVA_GPU_ERR_CUDA);
+  }
+
+ private:
+  crava_gpu_ctx *ctx_;
+  int nxp_, nyp_, nzp_, cnxp_, rnxp_;
+  long long rsize_, csize_;
+  int type_;
+  bool transformed_ = false;
+  float *data_ = nullptr;
+};
+
+// The hot path of Crava on device grids.
+class CravaDevice {
+ public:
+  CravaDevice(const crava_gpu_params &p, int device = 0, cudaStream_t stream = nullptr) {
+    check(crava_gpu_create(&p, device, stream, &ctx_), "crava_gpu_create");
+    nt_ = p.ntheta;
+  }
+  ~CravaDevice() { crava_gpu_destroy(ctx_); }
+  CravaDevice(const CravaDevice &) = delete;
+  CravaDevice &operator=(const CravaDevice &) = delete;
+
+  crava_gpu_ctx *ctx() { return ctx_; }
+
+  // Crava::computePostMeanResidAndFFTCov (src/crava.cpp:887-1295): means
+  // and stacks arrive transformed (src/crava.cpp:175-190); the prior
+  // covariances and the noise correlation are transformed here (:1003,
+  // :1012); on return the means hold the real-domain posterior mean
+  // (:1181-1183), the stacks the residual spectra and the covariances the
+  // posterior covariance spectra.  Returns 0, as the reference does.
+  int computePostMeanResidAndFFTCov(FFTGridDevice *mu[3], FFTGridDevice **data, FFTGridDevice *cov[6],
+                                    FFTGridDevice *errCorr, int precision = CRAVA_SOLVE_MIXED) {
+    for (int t = 0; t < 6; ++t)
+      if (!cov[t]->getIsTransformed()) cov[t]->fftInPlace();
+    if (!errCorr->getIsTransformed()) errCorr->fftInPlace();
+    crava_gpu_grids g{};
+    for (int q = 0; q < 3; ++q) g.mu[q] = mu[q]->devicePtr();
+    for (int l = 0; l < nt_; ++l) g.data[l] = data[l]->devicePtr();
+    for (int t = 0; t < 6; ++t) g.cov[t] = cov[t]->devicePtr();
+    g.err_corr = errCorr->devicePtr();
+    check(crava_gpu_posterior(ctx_, &g, precision), "computePostMeanResidAndFFTCov");
+    for (int q = 0; q < 3; ++q) mu[q]->invFFTInPlace();
+    return 0;
+  }
+
+  // Crava::simulate (src/crava.cpp:1415-1599) for `count` realisations:
+  // out[3 r + p] receives parameter p of realisation r (real domain).
+  int simulate(FFTGridDevice *postCov[6], FFTGridDevice *postMean[3], uint64_t seed, int firstIndex,
+               std::vector<FFTGridDevice *> &out) {
+    const float *cv[6];
+    const float *pm[3];
+    for (int t = 0; t < 6; ++t) cv[t] = postCov[t]->devicePtr();
+    for (int p = 0; p < 3; ++p) pm[p] = postMean[p]->devicePtr();
+    std::vector<float *> o(out.size());
+    for (size_t i = 0; i < out.size(); ++i) o[i] = out[i]->devicePtr();
+    check(crava_gpu_simulate(ctx_, cv, pm, seed, firstIndex, (int)(out.size() / 3), o.data()),
+          "simulate");
+    for (auto *g : out) g->setTransformedStatus(false);
+    return 0;
+  }
+
+  crava_gpu_stats stats() {
+    crava_gpu_stats s{};
+    check(crava_gpu_get_stats(ctx_, &s), "get_stats");
+    return s;
+  }
+
+ private:
+  crava_gpu_ctx *ctx_ = nullptr;
+  int nt_ = 0;
+};
+
+}  // namespace crava_b200

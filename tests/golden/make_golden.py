@@ -1,0 +1,69 @@
+"""Generates the golden fixtures of tests/golden/ from the reference's own
+numerics (oracle/_ref: FFTW 2.1.2, lib_matr.c and random.cpp compiled from
+the reference sources, driven as src/crava.cpp drives them).
+
+Run in a checkout where the reference tree is present:
+    python tests/golden/make_golden.py
+The fixtures hold the seeded inputs and the reference outputs, so the tests
+need neither the reference tree nor the generator's numpy version.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from crava_b200 import synth  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+CASES = {
+    "c3_12x10x16": dict(shape=(12, 10, 16), angles=(10.0, 20.0, 30.0), noise=0.10, seed=101, scale=None),
+    "c5_10x8x24": dict(shape=(10, 8, 24), angles=(0.0, 10.0, 20.0, 30.0, 40.0), noise=0.30, seed=102,
+                       scale=(0.8, 1.2)),
+    "c2_9x8x20_odd": dict(shape=(9, 8, 20), angles=(5.0, 25.0), noise=0.01, seed=103, scale=None),
+}
+
+
+def make_case(spec):
+    return synth.make_case(*spec["shape"], spec["angles"], spec["noise"], spec["seed"],
+                           wavelet_scale_range=spec["scale"])
+
+
+def main():
+    if not O.have_ref():
+        O.build(ref=True)
+    for name, spec in CASES.items():
+        case = make_case(spec)
+        nx, ny, nz = case.nxp, case.nyp, case.nzp
+        wd, e1, e2, e3, inv = O.kz_tables(case, "ref")
+        sp = O.forward_spectra(case, "ref")
+        pmu, pres, pcov, pfail = O.posterior_fp32_tables(case, sp, (wd, e1, e2, e3, inv), "ref")
+        umu, ures, ucov, ufail = O.unit_fp32(case, "ref")
+        seeds = [O.noise_fill(nx, ny, nz, 1000 + s, "ref")[0] for s in range(3)]
+        sim, sfail = O.sim_filter(nx, ny, nz, pcov, seeds, "ref")
+        out = dict(
+            nxp=nx, nyp=ny, nzp=nz, angles=np.array(spec["angles"]), noise_frac=spec["noise"],
+            seed=spec["seed"], wavelet=case.wavelet, A=case.A, theta_cov=case.theta_cov,
+            var0=case.var0, low_cut=case.low_cut, high_cut=case.high_cut, wnc=case.wnc,
+            nz=case.nz, lz=case.lz, min_rel_thick=case.min_rel_thick, dt=case.dt,
+            mu=np.stack(case.mu), data=np.stack(case.data), cov=np.stack(case.cov),
+            err_corr=case.err_corr,
+            tab_wd=wd, tab_e1=e1, tab_e2=e2, tab_e3=e3, tab_inv=inv,
+            spec_mu=np.stack(sp["mu"]), spec_data=np.stack(sp["data"]), spec_cov=np.stack(sp["cov"]),
+            spec_err=sp["err"],
+            post_mu=np.stack(pmu), post_res=np.stack(pres), post_cov=np.stack(pcov), post_fail=pfail,
+            unit_mu=np.stack(umu), unit_res=np.stack(ures), unit_cov=np.stack(ucov), unit_fail=ufail,
+            sim_noise=np.stack(seeds), sim=np.stack(sim), sim_fail=sfail,
+        )
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(name, "written")
+    normals, state = O.rng_normal(23665, 256, "ref")
+    np.savez_compressed(os.path.join(HERE, "rng_23665.npz"), normals=normals, state=state)
+    print("rng written")
+
+
+if __name__ == "__main__":
+    main()

@@ -12,7 +12,8 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-30))
 
 
-@pytest.mark.parametrize("shape", [(16, 12, 32), (20, 18, 30), (15, 16, 20), (64, 64, 128)])
+@pytest.mark.parametrize("shape", [(16, 12, 32), (20, 18, 30), (15, 16, 20), (64, 64, 128),
+                                   (96, 200, 30), (192, 160, 24), (75, 21, 35), (128, 128, 256)])
 @pytest.mark.parametrize("gtype", [api.DATA, api.COVARIANCE])
 def test_fft_roundtrip_and_oracle(shape, gtype):
     nx, ny, nz = shape
@@ -89,3 +90,17 @@ def test_unit_vs_reference_unit():
     nx = case.nxp
     for g, o in zip(mu + data + cov, omu + ores + ocov):
         assert rel(g.cpu().numpy()[..., :nx], o[..., :nx]) < 2e-5
+
+
+def test_host_entry_matches_device_unit():
+    case = synth.make_case(32, 24, 64, (0.0, 15.0, 30.0), 0.1, seed=9)
+    ctx = api.Context(case)
+    d = lambda gs: [api.to_device(g) for g in gs]
+    mu, data, cov, err = d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0]
+    ctx.posterior_unit(mu, data, cov, err, api.MIXED)
+    import torch
+    h = [torch.from_numpy(g.copy()).pin_memory() for g in case.grids()]
+    nt = case.ntheta
+    ctx.posterior_unit_host(h[:3], h[3:3 + nt], h[3 + nt:9 + nt], h[9 + nt], api.MIXED)
+    for a, b in zip(mu + data + cov, h[:9 + nt]):
+        assert np.array_equal(a.cpu().numpy()[..., :32], b.numpy()[..., :32])

@@ -1,0 +1,104 @@
+"""Pins the CPU oracle (plain-C restatement) against the reference's own
+numerics: the committed golden fixtures (made by tests/golden/make_golden.py
+from oracle/_ref) and, when it is built, oracle/_ref itself."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import golden_cases as GC
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("name", GC.NAMES)
+def test_solve_bitexact_vs_golden(name):
+    """With the reference's spectra and kz tables, the restated FP32 solve
+    reproduces the reference's lib_matr results bit for bit."""
+    case, z = GC.load(name)
+    mu, res, cov, fail = O.posterior_fp32_tables(case, GC.spectra(z), GC.tables(z), "orc")
+    for a, b in zip(mu + res + cov, list(z["post_mu"]) + list(z["post_res"]) + list(z["post_cov"])):
+        assert np.array_equal(bits(a), bits(b))
+    assert fail == int(z["post_fail"])
+
+
+@pytest.mark.parametrize("name", GC.NAMES)
+def test_fft_vs_golden(name):
+    """The restated 3-D R2C equals FFTW 2.1.2's to float rounding."""
+    case, z = GC.load(name)
+    n = (case.nxp, case.nyp, case.nzp)
+    for g, ref, t in [(case.data[0], z["spec_data"][0], 1), (case.cov[1], z["spec_cov"][1], 3),
+                      (case.mu[0], z["spec_mu"][0], 2)]:
+        a = O.complex_view(O.fft_r2c(g, *n, t, "orc"), case.nxp)
+        b = O.complex_view(ref, case.nxp)
+        assert rel(a, b) < 5e-7
+
+
+@pytest.mark.parametrize("name", GC.NAMES)
+def test_tables_vs_golden(name):
+    case, z = GC.load(name)
+    wd, e1, e2, e3, inv = O.kz_tables(case, "orc")
+    assert np.array_equal(inv, z["tab_inv"])
+    assert np.array_equal(e3, z["tab_e3"])
+    for a, b in [(wd, z["tab_wd"]), (e1, z["tab_e1"]), (e2, z["tab_e2"])]:
+        assert np.abs(a - b).max() <= 2e-6 * max(np.abs(b).max(), 1e-30)
+
+
+@pytest.mark.parametrize("name", GC.NAMES)
+def test_unit_vs_golden(name):
+    """The whole unit (restated FFT + solve) against the reference unit."""
+    case, z = GC.load(name)
+    mu, res, cov, fail = O.unit_fp32(case, "orc")
+    nx = case.nxp
+    for a, b in zip(mu + res + cov, list(z["unit_mu"]) + list(z["unit_res"]) + list(z["unit_cov"])):
+        assert rel(a[..., :nx], b[..., :nx]) < 2e-5
+    assert fail == int(z["unit_fail"])
+
+
+def test_rng_bitexact_vs_golden():
+    z = np.load(GC.HERE + "/rng_23665.npz")
+    normals, state = O.rng_normal(23665, len(z["normals"]), "orc")
+    assert np.array_equal(normals, z["normals"])
+    assert state == int(z["state"])
+
+
+@pytest.mark.parametrize("name", GC.NAMES)
+def test_noise_and_filter_vs_golden(name):
+    case, z = GC.load(name)
+    nx, ny, nzp = case.nxp, case.nyp, case.nzp
+    c = case.cnxp
+    for s in range(3):
+        g, _ = O.noise_fill(nx, ny, nzp, 1000 + s, "orc")
+        assert np.array_equal(bits(g[..., :2 * c]), bits(z["sim_noise"][s][..., :2 * c]))
+    sim, fail = O.sim_filter(nx, ny, nzp, list(z["post_cov"]), list(z["sim_noise"]), "orc")
+    for a, b in zip(sim, z["sim"]):
+        assert np.array_equal(bits(a[..., :2 * c]), bits(b[..., :2 * c]))
+    assert fail == int(z["sim_fail"])
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("shape,angles", [((16, 12, 32), (10.0, 20.0, 30.0)),
+                                          ((20, 18, 30), (0.0, 10.0, 20.0, 30.0, 40.0))])
+def test_solve_bitexact_vs_ref_live(shape, angles):
+    from crava_b200 import synth
+    case = synth.make_case(*shape, angles, 0.1, seed=3)
+    sp = O.forward_spectra(case, "ref")
+    tb = O.kz_tables(case, "ref")
+    a = O.posterior_fp32_tables(case, sp, tb, "orc")
+    b = O.posterior_fp32_tables(case, sp, tb, "ref")
+    for x, y in zip(a[0] + a[1] + a[2], b[0] + b[1] + b[2]):
+        assert np.array_equal(bits(x), bits(y))
+    assert a[3] == b[3]
+
+
+def test_fp64_twin_close_to_fp32():
+    case, z = GC.load("c3_12x10x16")
+    mu, res, cov, fail = O.posterior_fp64(case, GC.spectra(z))
+    nx = case.nxp
+    for a, b in zip(mu + cov, list(z["post_mu"]) + list(z["post_cov"])):
+        assert rel(O.complex_view(b, nx), a) < 1e-4
