@@ -16,6 +16,7 @@
 // (inverse) pass.
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include <vector>
 
@@ -222,6 +223,129 @@ __global__ void __launch_bounds__(kThreads) k_cols_ct(const __grid_constant__ Co
   }
 }
 
+// Row (x) pass for an even nxp, N = nxp / 2 a compile-time constant, in
+// place: RR rows per CTA held element-major ([m][r], odd pitch RR + 1).
+constexpr int kRR = 32;
+template <int N, int DIR>
+__global__ void __launch_bounds__(kThreads) k_rows_ip(const __grid_constant__ RowArgs a) {
+  constexpr int P = kRR + 1;
+  extern __shared__ float2 sm[];
+  float2 *twl = sm;            // N
+  float2 *post = twl + N;      // N + 1
+  float2 *buf = post + N + 1;  // N * P
+  const long long row0 = (long long)blockIdx.x * kRR;
+  const int nrows = (int)min((long long)kRR, a.nrows - row0);
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
+  for (int i = tid; i <= N; i += kThreads) post[i] = a.post[i];
+  if (DIR < 0) {
+    // batched loads: U independent loads in flight per thread
+    constexpr int U = 8;
+    for (int base = tid; base < kRR * N; base += kThreads * U) {
+      float2 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + u * kThreads;
+        const int r = idx / N, m = idx % N;
+        v[u] = (idx < kRR * N && r < nrows)
+                   ? reinterpret_cast<const float2 *>(a.src + (row0 + r) * a.rnxp)[m]
+                   : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + u * kThreads;
+        if (idx < kRR * N) buf[(idx % N) * P + idx / N] = v[u];
+      }
+    }
+  } else {
+    __syncthreads();
+    // Z'[k] = (X_k + conj X_{h-k}) + i W^{-k} (X_k - conj X_{h-k}); the
+    // imaginary parts of DC and Nyquist are ignored, as a C2R does.
+    constexpr int U = 4;
+    for (int base = tid; base < kRR * N; base += kThreads * U) {
+      float2 xk[U], xm[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + u * kThreads;
+        const int r = idx / N, k = idx % N;
+        if (idx < kRR * N && r < nrows) {
+          const float2 *X = reinterpret_cast<const float2 *>(a.grid + (row0 + r) * a.rnxp);
+          xk[u] = X[k];
+          xm[u] = X[N - k];
+        } else {
+          xk[u] = xm[u] = make_float2(0.f, 0.f);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int idx = base + u * kThreads;
+        if (idx >= kRR * N) continue;
+        const int r = idx / N, k = idx % N;
+        float2 x0 = xk[u], x1 = xm[u];
+        if (k == 0) { x0.y = 0.f; x1.y = 0.f; }
+        x1.y = -x1.y;
+        const float2 e = cadd(x0, x1);
+        float2 w = post[k];
+        w.y = -w.y;
+        const float2 o = cmul(csub(x0, x1), w);
+        buf[k * P + r] = make_float2(e.x - o.y, e.y + o.x);
+      }
+    }
+  }
+  __syncthreads();
+  stockham_ip<N, DIR, kRR, 1, P, kThreads>(buf, twl);
+  if (DIR < 0) {
+    // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{h-k})/2, O = -i (Z_k - conj Z_{h-k})/2
+    for (int idx = tid; idx < kRR * (N + 1); idx += kThreads) {
+      const int r = idx / (N + 1), k = idx % (N + 1);
+      if (r >= nrows) continue;
+      const float2 zk = buf[(k == N ? 0 : k) * P + r];
+      float2 zm = buf[(k == 0 ? 0 : N - k) * P + r];
+      zm.y = -zm.y;
+      const float2 e = cscale(cadd(zk, zm), 0.5f);
+      const float2 d = csub(zk, zm);
+      const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+      reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+    }
+  } else {
+    for (int idx = tid; idx < kRR * (N + 1); idx += kThreads) {
+      const int r = idx / (N + 1), m = idx % (N + 1);
+      if (r >= nrows) continue;
+      float2 v = make_float2(0.f, 0.f);
+      if (m < N) {
+        v = cscale(buf[m * P + r], a.scale);
+        if (a.addend) v = cadd(v, reinterpret_cast<const float2 *>(a.addend + (row0 + r) * a.rnxp)[m]);
+      }
+      reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[m] = v;
+    }
+  }
+}
+
+// Column pass, in-place register-staged transform, TX columns per CTA.
+template <int N, int DIR, int TX>
+__global__ void __launch_bounds__(kThreads) k_cols_ip(const __grid_constant__ ColArgs a) {
+  extern __shared__ float2 sm[];
+  float2 *twl = sm;
+  float2 *buf = twl + N;
+  const int x0 = blockIdx.x * TX;
+  const int nx = min(TX, a.ninner - x0);
+  float2 *base = a.data + (long long)blockIdx.y * a.outer_stride + x0;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
+  for (int idx = tid; idx < TX * N; idx += kThreads) {
+    const int t = idx % TX, m = idx / TX;
+    if (t < nx) cp_async8(buf + m * TX + t, base + m * a.elem_stride + t);
+    else buf[m * TX + t] = make_float2(0.f, 0.f);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  stockham_ip<N, DIR, TX, 1, TX, kThreads>(buf, twl);
+  for (int idx = tid; idx < TX * N; idx += kThreads) {
+    const int t = idx % TX, m = idx / TX;
+    if (t < nx) base[m * a.elem_stride + t] = cscale(buf[m * TX + t], a.scale);
+  }
+}
+
 int set_smem(const void *fn, size_t bytes) {
   static int dev_max = -1;
   if (dev_max < 0) {
@@ -327,6 +451,23 @@ int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t 
   a.post = p.xpost;
   a.scale = scale;
   const int n = a.rl.n;
+  if (p.x_even) {
+    const size_t sm2 = sizeof(float2) * (n + n + 1 + (size_t)n * (kRR + 1));
+    const dim3 g2((unsigned)((a.nrows + kRR - 1) / kRR));
+#define CRAVA_ROWS_IP(NN)                                                                    \
+    if (n == NN) {                                                                           \
+      const void *f = dir < 0 ? (const void *)k_rows_ip<NN, -1> : (const void *)k_rows_ip<NN, 1>; \
+      int r2 = set_smem(f, sm2);                                                             \
+      if (r2) return r2;                                                                     \
+      if (dir < 0) k_rows_ip<NN, -1><<<g2, kThreads, sm2, s>>>(a);                           \
+      else k_rows_ip<NN, 1><<<g2, kThreads, sm2, s>>>(a);                                    \
+      CRAVA_LAUNCH_CHECK();                                                                  \
+      return CRAVA_GPU_OK;                                                                   \
+    }
+    CRAVA_ROWS_IP(32) CRAVA_ROWS_IP(48) CRAVA_ROWS_IP(64) CRAVA_ROWS_IP(96) CRAVA_ROWS_IP(128)
+    CRAVA_ROWS_IP(256)
+#undef CRAVA_ROWS_IP
+  }
   size_t smem = sizeof(float2) * (n + (p.x_even ? n + 1 : 0) + 2 * kRows * (n + 1));
   dim3 grd((unsigned)((a.nrows + kRows - 1) / kRows));
   const void *fn;
@@ -345,6 +486,19 @@ int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t 
   return CRAVA_GPU_OK;
 }
 
+// Column tile width of the in-place column pass (0 selects the ping-pong
+// pass); CRAVA_COLS_TX=0|8|16 overrides the default for measurements.
+static int cols_tile_width(int n) {
+  static int tx = -1;
+  if (tx < 0) {
+    const char *e = getenv("CRAVA_COLS_TX");
+    tx = e ? atoi(e) : -2;
+    if (tx != 0 && tx != 8 && tx != 16) tx = -2;
+  }
+  if (tx != -2) return tx;
+  return n <= 256 ? 16 : 8;  // measured best on B200 at 256x256x512
+}
+
 static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
                 long long outer_stride, int nouter, int dir, float scale, cudaStream_t s) {
   ColArgs a;
@@ -358,7 +512,25 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
   const int n = lp.rl.n;
   size_t smem = sizeof(float2) * (n + 2 * kColTile * n);
   dim3 grd((ninner + kColTile - 1) / kColTile, nouter);
+  const int tx = cols_tile_width(n);
 #define CRAVA_COLS_CT(NN)                                                                   \
+  if (n == NN && tx > 0) {                                                                  \
+    const dim3 g2((ninner + tx - 1) / tx, nouter);                                          \
+    const size_t sm2 = sizeof(float2) * (NN + (size_t)tx * NN);                             \
+    const void *f = tx == 16 ? (dir < 0 ? (const void *)k_cols_ip<NN, -1, 16> : (const void *)k_cols_ip<NN, 1, 16>) \
+                             : (dir < 0 ? (const void *)k_cols_ip<NN, -1, 8> : (const void *)k_cols_ip<NN, 1, 8>);  \
+    int r2 = set_smem(f, sm2);                                                              \
+    if (r2) return r2;                                                                      \
+    if (tx == 16) {                                                                         \
+      if (dir < 0) k_cols_ip<NN, -1, 16><<<g2, kThreads, sm2, s>>>(a);                      \
+      else k_cols_ip<NN, 1, 16><<<g2, kThreads, sm2, s>>>(a);                               \
+    } else {                                                                                \
+      if (dir < 0) k_cols_ip<NN, -1, 8><<<g2, kThreads, sm2, s>>>(a);                       \
+      else k_cols_ip<NN, 1, 8><<<g2, kThreads, sm2, s>>>(a);                                \
+    }                                                                                       \
+    CRAVA_LAUNCH_CHECK();                                                                   \
+    return CRAVA_GPU_OK;                                                                    \
+  }                                                                                         \
   if (n == NN) {                                                                            \
     const void *f = dir < 0 ? (const void *)k_cols_ct<NN, -1> : (const void *)k_cols_ct<NN, 1>; \
     int r2 = set_smem(f, smem);                                                             \

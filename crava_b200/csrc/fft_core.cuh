@@ -356,3 +356,73 @@ __device__ __forceinline__ int stockham_ct(float2 *a, float2 *b, const float2 *t
 }
 
 }  // namespace crava
+
+namespace crava {
+
+// In-place compile-time Stockham: each stage first reads every butterfly
+// input of this thread into registers, synchronises, then writes the
+// outputs into the same buffer.  Halves the shared memory of the
+// ping-pong form.  NTH is the block size (compile-time).
+template <int N, int R, int NS, int DIR, int NL, int LS, int ES, int NTH>
+__device__ __forceinline__ void ct_stage_ip(float2 *buf, const float2 *__restrict__ tw, int tid) {
+  constexpr int M = N / R;
+  constexpr int TSTEP = N / (NS * R);
+  static_assert(NTH % NL == 0, "block size must be a multiple of the line count");
+  // Lines fastest: thread tid always works on line l = tid % NL; its
+  // butterflies are j = j0 + i * JS.
+  constexpr int JS = NTH / NL;
+  constexpr int PER = (M + JS - 1) / JS;
+  const int l = tid % NL;
+  const int j0 = tid / NL;
+  float2 *lb = buf + l * LS;
+  float2 v[PER][R];
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = j0 + i * JS;
+    if (M % JS == 0 || j < M) {
+      const float2 *sl = lb + j * ES;
+#pragma unroll
+      for (int q = 0; q < R; ++q) v[i][q] = sl[q * M * ES];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int j = j0 + i * JS;
+    if (M % JS == 0 || j < M) {
+      const int base = j % NS;
+      if (NS > 1 && base != 0) {
+        const int step = base * TSTEP;
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+          float2 w = tw[q * step];
+          if (DIR > 0) w.y = -w.y;
+          v[i][q] = cmul(v[i][q], w);
+        }
+      }
+      Dft<R, DIR>::run(v[i]);
+      float2 *dl = lb + ((j - base) * R + base) * ES;
+#pragma unroll
+      for (int q = 0; q < R; ++q) dl[q * NS * ES] = v[i][q];
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int DIR, int NL, int LS, int ES, int NTH, int S>
+struct CtStagesIp {
+  static __device__ __forceinline__ void run(float2 *buf, const float2 *tw, int tid) {
+    if constexpr (S < CtRadix::count(N)) {
+      ct_stage_ip<N, CtRadix::at(N, S), CtRadix::ns(N, S), DIR, NL, LS, ES, NTH>(buf, tw, tid);
+      CtStagesIp<N, DIR, NL, LS, ES, NTH, S + 1>::run(buf, tw, tid);
+    }
+  }
+};
+
+// Transforms NL lines of length N in place (caller syncs before).
+template <int N, int DIR, int NL, int LS, int ES, int NTH>
+__device__ __forceinline__ void stockham_ip(float2 *buf, const float2 *tw) {
+  CtStagesIp<N, DIR, NL, LS, ES, NTH, 0>::run(buf, tw, threadIdx.x);
+}
+
+}  // namespace crava

@@ -44,9 +44,11 @@ __device__ __forceinline__ void prior_f(const float2 c6[6], const double v[6], f
 }
 
 // Hermitian Cholesky M = L L^H on the lower triangle (tri() indexing), with
-// the reference's failure rules applied to M / M00.
+// the reference's failure rules applied to M / M00.  The reciprocals of the
+// diagonal of L are returned in rd (one division per column, reused by the
+// substitutions).
 template <int NT, typename T2, typename T>
-__device__ __forceinline__ bool cholesky(T2 *L) {
+__device__ __forceinline__ bool cholesky(T2 *L, T *rd) {
   const T factor = L[0].x;
   if (!(factor > T(0))) return false;
   const T tol = (T)kTol * factor;
@@ -62,18 +64,25 @@ __device__ __forceinline__ bool cholesky(T2 *L) {
         s.x -= a.x * b.x + a.y * b.y;
         s.y -= a.y * b.x - a.x * b.y;
       }
-      T inv = T(1) / L[tri(j, j)].x;
-      s.x *= inv; s.y *= inv;
+      s.x *= rd[j]; s.y *= rd[j];
       L[tri(i, j)] = s;
     }
     T d = L[tri(i, i)].x;
 #pragma unroll
     for (int k = 0; k < i; ++k) d -= L[tri(i, k)].x * L[tri(i, k)].x + L[tri(i, k)].y * L[tri(i, k)].y;
     if (!(d > tol)) return false;
-    L[tri(i, i)].x = sqrt(d);
+    const T sq = sqrt(d);
+    L[tri(i, i)].x = sq;
     L[tri(i, i)].y = T(0);
+    rd[i] = T(1) / sq;
   }
   return true;
+}
+
+template <int NT, typename T2, typename T>
+__device__ __forceinline__ bool cholesky(T2 *L) {
+  T rd[NT];
+  return cholesky<NT, T2, T>(L, rd);
 }
 
 // Solves L L^H X = B in place for the 3 columns of B.
@@ -171,7 +180,8 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
       }
     }
   }
-  if (!cholesky<NT, double2, double>(L)) return true;
+  double rd[NT];
+  if (!cholesky<NT, double2, double>(L, rd)) return true;
   double2 mp[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
@@ -195,8 +205,7 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
         s.x -= lij.x * xj.x - lij.y * xj.y;
         s.y -= lij.x * xj.y + lij.y * xj.x;
       }
-      const double inv_d = 1.0 / L[tri(i, i)].x;
-      x[i] = make_double2(s.x * inv_d, s.y * inv_d);
+      x[i] = make_double2(s.x * rd[i], s.y * rd[i]);
     }
 #pragma unroll
     for (int i = NT - 1; i >= 0; --i) {
@@ -207,8 +216,7 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
         s.x -= lji.x * xj.x + lji.y * xj.y;
         s.y -= lji.x * xj.y - lji.y * xj.x;
       }
-      const double inv_d = 1.0 / L[tri(i, i)].x;
-      x[i] = make_double2(s.x * inv_d, s.y * inv_d);
+      x[i] = make_double2(s.x * rd[i], s.y * rd[i]);
     }
     // posterior covariance entries (p, q), p <= q
 #pragma unroll
@@ -332,7 +340,8 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
       }
     }
   }
-  if (!cholesky<NT, float2, float>(Lf)) return true;
+  float rdf[NT];
+  if (!cholesky<NT, float2, float>(Lf, rdf)) return true;
 #pragma unroll
   for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
   double2 mp[3];
@@ -360,8 +369,7 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
         sacc.x -= lij.x * xj.x - lij.y * xj.y;
         sacc.y -= lij.x * xj.y + lij.y * xj.x;
       }
-      const float id = 1.f / Lf[tri(i, i)].x;
-      x0[i][0] = make_float2(sacc.x * id, sacc.y * id);
+      x0[i][0] = make_float2(sacc.x * rdf[i], sacc.y * rdf[i]);
     }
 #pragma unroll
     for (int i = NT - 1; i >= 0; --i) {
@@ -372,8 +380,7 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
         sacc.x -= lji.x * xj.x + lji.y * xj.y;
         sacc.y -= lji.x * xj.y - lji.y * xj.x;
       }
-      const float id = 1.f / Lf[tri(i, i)].x;
-      x0[i][0] = make_float2(sacc.x * id, sacc.y * id);
+      x0[i][0] = make_float2(sacc.x * rdf[i], sacc.y * rdf[i]);
     }
     // FP64 residual r = ks - Md x0, stored as the float right-hand side
 #pragma unroll
@@ -396,8 +403,7 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
         sacc.x -= lij.x * xj.x - lij.y * xj.y;
         sacc.y -= lij.x * xj.y + lij.y * xj.x;
       }
-      const float id = 1.f / Lf[tri(i, i)].x;
-      x0[i][1] = make_float2(sacc.x * id, sacc.y * id);
+      x0[i][1] = make_float2(sacc.x * rdf[i], sacc.y * rdf[i]);
     }
 #pragma unroll
     for (int i = NT - 1; i >= 0; --i) {
@@ -408,8 +414,7 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
         sacc.x -= lji.x * xj.x + lji.y * xj.y;
         sacc.y -= lji.x * xj.y - lji.y * xj.x;
       }
-      const float id = 1.f / Lf[tri(i, i)].x;
-      x0[i][1] = make_float2(sacc.x * id, sacc.y * id);
+      x0[i][1] = make_float2(sacc.x * rdf[i], sacc.y * rdf[i]);
     }
     double2 x[NT];
 #pragma unroll
