@@ -18,6 +18,7 @@
 // M00 <= 0 or a pivot of M/M00 is <= 1e-20 (libs/lib/lib_matr.c:20,
 // 103-105, 114, 145), the bin keeps mu, S and r = d.
 #include <math.h>
+#include <stdlib.h>
 
 #include "solve.cuh"
 #include "solve_bin.cuh"
@@ -119,8 +120,8 @@ struct SolveArgs {
   DevCounters *counters;
 };
 
-template <int NT, int PREC>
-__global__ void __launch_bounds__(kThreads) k_solve(SolveArgs a) {
+template <int NT, int PREC, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= a.csize) return;
   const int k = (int)(idx / a.plane);
@@ -146,22 +147,43 @@ __global__ void __launch_bounds__(kThreads) k_solve(SolveArgs a) {
   if (a.counters) sb::count(a.counters, fail, nonfinite);
 }
 
-template <int PREC>
-int launch_solve(const SolveArgs &a, int nt, cudaStream_t s) {
+template <int PREC, int MINB>
+int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
   dim3 grd((unsigned)((a.csize + kThreads - 1) / kThreads));
   switch (nt) {
-    case 1: k_solve<1, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 2: k_solve<2, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 3: k_solve<3, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 4: k_solve<4, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 5: k_solve<5, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 6: k_solve<6, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 7: k_solve<7, PREC><<<grd, kThreads, 0, s>>>(a); break;
-    case 8: k_solve<8, PREC><<<grd, kThreads, 0, s>>>(a); break;
+    case 1: k_solve<1, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 2: k_solve<2, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 3: k_solve<3, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 4: k_solve<4, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 5: k_solve<5, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 6: k_solve<6, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 7: k_solve<7, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
+    case 8: k_solve<8, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
     default: return CRAVA_GPU_ERR_ARG;
   }
   CRAVA_LAUNCH_CHECK();
   return CRAVA_GPU_OK;
+}
+
+// Blocks per SM of the solve kernel (register budget 255 / 128 / 80);
+// CRAVA_SOLVE_MINB overrides the default for measurements.
+static int solve_minb() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("CRAVA_SOLVE_MINB");
+    v = e ? atoi(e) : 1;
+    if (v < 1 || v > 3) v = 1;
+  }
+  return v;
+}
+
+template <int PREC>
+int launch_solve(const SolveArgs &a, int nt, cudaStream_t s) {
+  switch (solve_minb()) {
+    case 2: return launch_solve_b<PREC, 2>(a, nt, s);
+    case 3: return launch_solve_b<PREC, 3>(a, nt, s);
+    default: return launch_solve_b<PREC, 1>(a, nt, s);
+  }
 }
 
 }  // namespace
