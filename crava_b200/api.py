@@ -83,6 +83,8 @@ SYMBOLS = {
     "crava_gpu_kz_tables": ([C.c_void_p, F32P, F32P, F32P, F32P, C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_set_kz_tables": ([C.c_void_p, F32P, F32P, F32P, F32P, C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_launch_count": ([], C.c_longlong),
+    "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
+                                     C.POINTER(Stats)], C.c_int),
 }
 
 _lib = None

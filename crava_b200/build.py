@@ -26,6 +26,7 @@ SOURCES = {
     "solve_ref.cu": ["-fmad=false"],
     "sim.cu": ["-fmad=false"],
     "unit.cu": [],
+    "noalloc.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -307,6 +307,9 @@ const char *crava_gpu_status_string(int status) {
     case CRAVA_GPU_ERR_TIMEOUT: return "device wait timed out";
     case CRAVA_GPU_ERR_STATE: return "call out of order";
     case CRAVA_GPU_ERR_NODEV: return "no CUDA device";
+    case CRAVA_GPU_ERR_TOO_LARGE:
+      return "size exceeds the static scratch of crava_gpu_posterior_noalloc "
+             "(nzp <= 4096, nzp * ntheta <= 16384)";
     default: return "unknown status";
   }
 }

@@ -229,6 +229,20 @@ int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s) {
   return CRAVA_GPU_OK;
 }
 
+int kz_tables_build_device(const crava_gpu_params &p, const float *d_wavelet,
+                           const float *d_norm, KzTables *t, cudaStream_t s) {
+  const int nzp = p.nzp, nt = p.ntheta;
+  const int nth = 256;
+  const int cnzp = nzp / 2 + 1;
+  size_t smem = sizeof(double) * (2 * nzp + 2 * nth) + sizeof(float2) * 2 * cnzp + sizeof(float) * 4 * nzp;
+  if (smem > 48 * 1024)
+    CRAVA_CUDA_TRY(cudaFuncSetAttribute(k_kz_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_kz_tables<<<nt, nth, smem, s>>>(d_wavelet, d_norm, d_norm != nullptr, nzp, nt, p.nz, p.lz,
+                                    p.min_rel_thick, p.low_cut, p.high_cut, *t);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
 int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g,
                     long long csize, long long plane, int precision,
                     DevCounters *counters, cudaStream_t s) {

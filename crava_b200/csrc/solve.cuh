@@ -40,6 +40,11 @@ void kz_tables_free(KzTables *t);
 // Builds the tables from the wavelets on the device (params: host struct).
 int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s);
 
+// Builds the tables from wavelets already in device memory (d_norm may be
+// null); launches one kernel on s and allocates nothing.
+int kz_tables_build_device(const crava_gpu_params &p, const float *d_wavelet,
+                           const float *d_norm, KzTables *t, cudaStream_t s);
+
 // Per-bin solve over csize bins; plane = cnxp * nyp bins per kz.
 int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g,
                     long long csize, long long plane, int precision,

@@ -31,7 +31,9 @@ enum crava_gpu_status {
   CRAVA_GPU_ERR_CUDA = 3,    /* a CUDA call or kernel launch failed       */
   CRAVA_GPU_ERR_TIMEOUT = 4, /* a bounded device wait gave up             */
   CRAVA_GPU_ERR_STATE = 5,   /* call out of order (e.g. no stats pending) */
-  CRAVA_GPU_ERR_NODEV = 6    /* no usable CUDA device                     */
+  CRAVA_GPU_ERR_NODEV = 6,   /* no usable CUDA device                     */
+  CRAVA_GPU_ERR_TOO_LARGE = 7 /* sizes beyond the static scratch of
+                                 crava_gpu_posterior_noalloc              */
 };
 
 /* Grid types: FFTGrid::gridTypes (src/fftgrid.h:172).  They select the
@@ -213,6 +215,26 @@ int crava_gpu_set_profiling(crava_gpu_ctx *ctx, int enable);
  * *count receives the number of kernel kinds seen. */
 int crava_gpu_get_profile(crava_gpu_ctx *ctx, crava_gpu_kernel_profile *out,
                           int max, int *count);
+
+/* The per-bin posterior solve of crava_gpu_posterior for callers that cannot
+ * allocate device memory: those whose HBM is owned by their own arena (a
+ * framework's caching allocator, a pool reserved up front), where a
+ * cudaMalloc fails or breaks the owner's accounting, and loops that cannot
+ * take the synchronisation an allocation may imply.  Needs no context and
+ * allocates nothing: its scratch (staged wavelets, per-kz tables, counters)
+ * is one static device array of about 0.5 MB, held by every GPU that loads
+ * the library until exit.  Limits: nzp <= 4096 and nzp * ntheta <= 16384,
+ * else CRAVA_GPU_ERR_TOO_LARGE.  params: host; grids: transformed device
+ * grids, updated in place as by crava_gpu_posterior; stream: a cudaStream_t
+ * (NULL = legacy default stream) on the current device.  stats may be NULL
+ * (asynchronous); if given, the call waits for the stream and fills the
+ * failure counts (no timings).  The first call on a device sets up the
+ * scratch address for that device -- make it before any stream capture.
+ * Calls overlapping on the GPU share the scratch and race: serialise them.
+ * This entry point has no counterpart in the reference. */
+int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
+                                const crava_gpu_grids *grids, int precision,
+                                void *stream, crava_gpu_stats *stats);
 
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
