@@ -65,6 +65,49 @@ struct Dft<8, DIR> {
   }
 };
 
+// Radix 16 as 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2:
+//   Y[n2][k1] = DFT4_n1(x[4 n1 + n2]),  Y *= W16^(n2 k1),  X[k1 + 4 k2] = DFT4_n2(Y[.][k1]).
+template <int DIR>
+struct Dft<16, DIR> {
+  static __device__ __forceinline__ float2 tw16(float2 a, int m) {
+    // a * e^{DIR 2 pi i m / 16}, m in 1..9
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    const float h = 0.70710678118654752440f;
+    float c, sn;
+    switch (m) {
+      case 1: c = c1; sn = s1; break;
+      case 2: c = h; sn = h; break;
+      case 3: c = s1; sn = c1; break;
+      case 4: c = 0.f; sn = 1.f; break;
+      case 6: c = -h; sn = h; break;
+      default: c = -c1; sn = -s1; break;  // m = 9
+    }
+    sn = DIR * sn;
+    return make_float2(a.x * c - a.y * sn, a.x * sn + a.y * c);
+  }
+  static __device__ __forceinline__ void run(float2 *v) {
+    float2 y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      float2 a[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+      Dft<4, DIR>::run(a);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = a[k1];
+    }
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+      for (int k1 = 1; k1 < 4; ++k1) y[n2][k1] = tw16(y[n2][k1], n2 * k1);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      float2 b[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      Dft<4, DIR>::run(b);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
+    }
+  }
+};
+
 // Odd prime radix by the symmetric pairing a_k = v_k + v_{R-k},
 // b_k = v_k - v_{R-k}: X_q = v_0 + sum_k cos(2 pi k q/R) a_k
 //                          + DIR i sum_k sin(2 pi k q/R) b_k, X_{R-q} = conj-pair.
@@ -272,23 +315,25 @@ namespace crava {
 // Radices: 8 while possible, then 4, then 2, then 3, 5, 7 (as radix_list).
 // ---------------------------------------------------------------------------
 struct CtRadix {
-  __host__ __device__ static constexpr int at(int n, int s) {
-    int m = n, r = 1;
-    for (int i = 0; i <= s; ++i) {
-      r = (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : 1;
-      m /= r;
-    }
-    return r;
+  // Radix sequence: 8 while possible, then 4, then 2, then 3, 5, 7; or, when
+  // it takes fewer stages, 16 while possible first (e.g. 256 = 16 x 16).
+  __host__ __device__ static constexpr int pick(int m, bool use16) {
+    return (use16 && m % 16 == 0) ? 16
+         : (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2
+         : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : m;
   }
-  __host__ __device__ static constexpr int count(int n) {
+  __host__ __device__ static constexpr int stages(int n, bool use16) {
     int m = n, c = 0;
-    while (m > 1) {
-      int r = (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : (m % 3 == 0) ? 3 : (m % 5 == 0) ? 5 : (m % 7 == 0) ? 7 : m;
-      m /= r;
-      ++c;
-    }
+    while (m > 1) { m /= pick(m, use16); ++c; }
     return c;
   }
+  __host__ __device__ static constexpr bool use16(int n) { return stages(n, true) < stages(n, false); }
+  __host__ __device__ static constexpr int at(int n, int s) {
+    int m = n, r = 1;
+    for (int i = 0; i <= s; ++i) { r = pick(m, use16(n)); m /= r; }
+    return r;
+  }
+  __host__ __device__ static constexpr int count(int n) { return stages(n, use16(n)); }
   __host__ __device__ static constexpr int ns(int n, int s) {
     int p = 1;
     for (int i = 0; i < s; ++i) p *= at(n, i);
@@ -303,6 +348,9 @@ struct CtRadix {
     return m == 1 && n > 1;
   }
 };
+static_assert(CtRadix::count(256) == 2 && CtRadix::at(256, 0) == 16, "radix plan");
+static_assert(CtRadix::count(128) == 2 && CtRadix::at(128, 1) == 8, "radix plan");
+static_assert(CtRadix::count(512) == 3 && CtRadix::at(512, 0) == 8, "radix plan");
 
 template <int N, int R, int NS, int DIR, bool LF, int NL, int SLS, int SES, int DLS, int DES>
 __device__ __forceinline__ void ct_stage(const float2 *__restrict__ src, float2 *__restrict__ dst,
