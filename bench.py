@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-simulation", action="store_true")
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
     return ap.parse_args()
 
@@ -240,6 +241,33 @@ def run_own(args):
     h2d = (10 + nt) * gbytes
     d2h = (9 + nt) * gbytes
 
+    # simulation: realisations of the posterior (Crava::simulate) from the
+    # posterior covariance spectra, 8 realisations per call
+    sim = None
+    if not args.no_simulation:
+        covf = [g.clone() for g in dst[2]]
+        for g in covf:
+            ctx.fft_r2c(g, api.COVARIANCE)
+        R = 8
+        outs = [torch.empty_like(dst[0][0]) for _ in range(3 * R)]
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            for w in range(2):
+                ctx.simulate(covf, dst[0], 11, 0, outs)
+            torch.cuda.synchronize(dev)
+            nsim = 3
+            ev0.record(stream)
+            for k in range(nsim):
+                ctx.simulate(covf, dst[0], 11, R * k, outs)
+            ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_call = max_over_ranks(ev0.elapsed_time(ev1) / nsim)
+        sim = {"value": world * R / (ms_call * 1e-3), "unit": "realisations/s",
+               "ms_per_realisation": ms_call / R, "batch": R,
+               "grid": [nxp, nyp, nzp]}
+        del covf, outs
+
     roof = None
     if prof:
         name, (n, tot, bpl) = max(prof.items(), key=lambda kv: kv[1][1])
@@ -297,6 +325,7 @@ def run_own(args):
         "clocks": clk,
         "fp64_form_value": fp64_value,
         "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
+        "simulation": sim,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,
         "chol_fail_bins": st.chol_fail_bins, "nonfinite_bins": st.nonfinite_bins,

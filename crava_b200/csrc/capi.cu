@@ -609,16 +609,19 @@ int crava_gpu_simulate(crava_gpu_ctx *c, const float *const cov[6], const float 
   int rc;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  for (int r = 0; r < count; ++r) {
-    float2 *o[3];
-    for (int q = 0; q < 3; ++q) o[q] = reinterpret_cast<float2 *>(out[3 * r + q]);
-    const uint64_t stream0 = 3ull * (uint64_t)(first_index + r);
+  // batches of up to 8 realisations share one read and one factorisation
+  // of the posterior covariance spectra per bin
+  for (int r0 = 0; r0 < count; r0 += 8) {
+    const int nr = count - r0 < 8 ? count - r0 : 8;
+    float2 *o[24];
+    for (int k = 0; k < 3 * nr; ++k) o[k] = reinterpret_cast<float2 *>(out[3 * r0 + k]);
+    const uint64_t stream0 = 3ull * (uint64_t)(first_index + r0);
     {
-      Scope sc(c, K_SIM);
-      if ((rc = noise_filter(c->g, cv, o, seed, stream0, c->counters, s))) return rc;
+      Scope sc(c, K_SIM, (6.0 + 3.0 * nr) * (double)c->g.csize * 8.0);
+      if ((rc = noise_filter_multi(c->g, cv, o, nr, seed, stream0, c->counters, s))) return rc;
     }
-    for (int q = 0; q < 3; ++q)
-      if ((rc = pass_inverse(c, out[3 * r + q], CRAVA_GRID_PARAMETER, post_mean[q]))) return rc;
+    for (int k = 0; k < 3 * nr; ++k)
+      if ((rc = pass_inverse(c, out[3 * r0 + k], CRAVA_GRID_PARAMETER, post_mean[k % 3]))) return rc;
   }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));

@@ -201,7 +201,74 @@ __global__ void __launch_bounds__(kThreads) k_noise_filter(NoiseFilterArgs a) {
   if (a.counters) count_fail(a.counters, f);
 }
 
+// Several realisations per pass: the posterior Cholesky factor of each bin
+// is computed once and applied to the noise of every realisation
+// (realisation r, parameter p uses stream stream0 + 3 r + p).
+constexpr int kMaxSimBatch = 8;
+struct NoiseFilterMultiArgs {
+  const float2 *cov[6];
+  float2 *out[3 * kMaxSimBatch];
+  int nreal;
+  long long csize;
+  int cnxp, nyp, nzp;
+  uint64_t seed, stream0;
+  DevCounters *counters;
+};
+
+__global__ void __launch_bounds__(kThreads) k_noise_filter_multi(const __grid_constant__ NoiseFilterMultiArgs a) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.csize) return;
+  float2 P[3][3];
+  P[0][0] = a.cov[0][i]; P[1][1] = a.cov[1][i]; P[2][2] = a.cov[2][i];
+  P[0][1] = a.cov[3][i]; P[0][2] = a.cov[4][i]; P[1][2] = a.cov[5][i];
+  P[1][0] = make_float2(P[0][1].x, -P[0][1].y);
+  P[2][0] = make_float2(P[0][2].x, -P[0][2].y);
+  P[2][1] = make_float2(P[1][2].x, -P[1][2].y);
+  const bool ok = chol3_ref(P) == 0;
+  for (int r = 0; r < a.nreal; ++r) {
+    float2 z[3], o[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) z[q] = noise_bin(i, a.cnxp, a.nyp, a.nzp, a.seed, a.stream0 + 3ull * r + q);
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      o[p] = make_float2(0.0f, 0.0f);
+      if (ok) {
+#pragma unroll
+        for (int b = 0; b < p + 1; ++b) {
+          o[p].x += P[p][b].x * z[b].x - P[p][b].y * z[b].y;
+          o[p].y += P[p][b].x * z[b].y + P[p][b].y * z[b].x;
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < 3; ++p) a.out[3 * r + p][i] = o[p];
+  }
+  if (a.counters) {
+    unsigned m = __activemask();
+    unsigned b = __ballot_sync(m, !ok);
+    if (b && (threadIdx.x & 31) == __ffs(m) - 1)
+      atomicAdd(&a.counters->chol_fail, (unsigned long long)__popc(b) * (unsigned long long)a.nreal);
+  }
+}
+
 }  // namespace
+
+int noise_filter_multi(const Geom &g, const float2 *const cov[6], float2 *const *out, int nreal,
+                       uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s) {
+  if (nreal < 1 || nreal > kMaxSimBatch) return CRAVA_GPU_ERR_ARG;
+  NoiseFilterMultiArgs a;
+  for (int t = 0; t < 6; ++t) a.cov[t] = cov[t];
+  for (int k = 0; k < 3 * nreal; ++k) a.out[k] = out[k];
+  a.nreal = nreal;
+  a.csize = g.csize;
+  a.cnxp = g.cnxp; a.nyp = g.nyp; a.nzp = g.nzp;
+  a.seed = seed; a.stream0 = stream0;
+  a.counters = counters;
+  dim3 grd((unsigned)((g.csize + kThreads - 1) / kThreads));
+  k_noise_filter_multi<<<grd, kThreads, 0, s>>>(a);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
 
 int noise_fill(const Geom &g, float2 *grid, uint64_t seed, uint64_t stream, cudaStream_t s) {
   dim3 grd((unsigned)((g.csize + kThreads - 1) / kThreads));

@@ -13,4 +13,8 @@ int sim_filter(const Geom &g, const float2 *const cov[6], float2 *const seed[3],
 int noise_filter(const Geom &g, const float2 *const cov[6], float2 *const out[3],
                  uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s);
 
+// nreal (<= 8) realisations in one pass: out[3 r + p], streams stream0 + 3 r + p.
+int noise_filter_multi(const Geom &g, const float2 *const cov[6], float2 *const *out, int nreal,
+                       uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s);
+
 }  // namespace crava

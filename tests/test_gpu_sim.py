@@ -121,3 +121,23 @@ def test_realisations_match_posterior_covariance():
         for q in range(3):
             if p != q:
                 assert abs(C[p, q]) < 0.03, C
+
+
+def test_batched_realisations_equal_single_calls():
+    """Realisation r of one call of 11 (batches of 8 + 3) equals the call
+    that makes realisation r alone: each realisation depends only on (seed, r)."""
+    case = synth.make_case(16, 12, 32, (10.0, 25.0), 0.1, seed=3)
+    ctx = api.Context(case)
+    d = lambda gs: [api.to_device(g) for g in gs]
+    mu, cov = d(case.mu), d(case.cov)
+    for g in cov:
+        ctx.fft_r2c(g, api.COVARIANCE)
+    R = 11
+    outs = [torch.zeros_like(mu[0]) for _ in range(3 * R)]
+    ctx.simulate(cov, mu, 77, 5, outs)
+    for r in (0, 7, 8, 10):
+        one = [torch.zeros_like(mu[0]) for _ in range(3)]
+        ctx.simulate(cov, mu, 77, 5 + r, one)
+        for p in range(3):
+            assert torch.equal(one[p], outs[3 * r + p]), (r, p)
+    assert not torch.equal(outs[0], outs[3])
