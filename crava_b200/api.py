@@ -59,6 +59,19 @@ class Stats(C.Structure):
                 ("ms_inverse", C.c_float), ("ms_total", C.c_float)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("cols_y_tile", C.c_int), ("cols_z_tile", C.c_int), ("fused", C.c_int),
+                ("ms", C.c_float)]
+
+
+class Vintage(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("inp", Grids), ("out", Grids), ("precision", C.c_int),
+                ("nsim", C.c_int), ("seed", C.c_uint64), ("first_index", C.c_uint64),
+                ("sim_out", C.POINTER(C.c_void_p))]
+
+
+BATCH_AUTOTUNE, BATCH_NO_GRAPH = 1, 2
+
 SYMBOLS = {
     "crava_gpu_create": ([C.POINTER(Params), C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
     "crava_gpu_destroy": ([C.c_void_p], C.c_int),
@@ -83,6 +96,15 @@ SYMBOLS = {
     "crava_gpu_kz_tables": ([C.c_void_p, F32P, F32P, F32P, F32P, C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_set_kz_tables": ([C.c_void_p, F32P, F32P, F32P, F32P, C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_launch_count": ([], C.c_longlong),
+    "crava_gpu_get_tuning": ([C.c_void_p, C.POINTER(Tuning)], C.c_int),
+    "crava_gpu_set_tuning": ([C.c_void_p, C.POINTER(Tuning)], C.c_int),
+    "crava_gpu_autotune": ([C.c_void_p, C.POINTER(Grids), C.POINTER(Grids), C.c_int, C.c_int,
+                            C.POINTER(Tuning)], C.c_int),
+    "crava_gpu_batch_create": ([C.POINTER(Vintage), C.c_int, C.c_int, C.c_void_p,
+                                C.POINTER(C.c_void_p)], C.c_int),
+    "crava_gpu_batch_run": ([C.c_void_p], C.c_int),
+    "crava_gpu_batch_sync": ([C.c_void_p], C.c_int),
+    "crava_gpu_batch_destroy": ([C.c_void_p], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -205,6 +227,25 @@ class Context:
         check(self.lib.crava_gpu_posterior_unit_oop(self.handle, C.byref(gi), C.byref(go), p),
               "posterior_unit_oop")
 
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        check(self.lib.crava_gpu_get_tuning(self.handle, C.byref(t)), "get_tuning")
+        return t
+
+    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0):
+        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0)
+        check(self.lib.crava_gpu_set_tuning(self.handle, C.byref(t)), "set_tuning")
+
+    def autotune(self, src, dst, precision=None, reps=2) -> Tuning:
+        """Times every launch-shape candidate on the out-of-place unit
+        src -> dst and keeps the fastest (synchronous)."""
+        gi, go = self.grids(*src), self.grids(*dst)
+        p = self.precision if precision is None else precision
+        t = Tuning()
+        check(self.lib.crava_gpu_autotune(self.handle, C.byref(gi), C.byref(go), p, reps, C.byref(t)),
+              "autotune")
+        return t
+
     def set_fused(self, enable=True):
         check(self.lib.crava_gpu_set_fused(self.handle, int(bool(enable))), "set_fused")
 
@@ -271,6 +312,55 @@ class Context:
         check(self.lib.crava_gpu_set_kz_tables(self.handle, wd.ctypes.data_as(F32P), e1.ctypes.data_as(F32P),
                                                e2.ctypes.data_as(F32P), e3.ctypes.data_as(F32P),
                                                inv.ctypes.data_as(C.POINTER(C.c_int))), "set_kz_tables")
+
+
+class Batch:
+    """Vintages (one Context each) inverted and sampled as one CUDA graph
+    launch per run.  vintages: dicts with ctx, src and dst ((mu, data, cov,
+    err) tuples of device tensors), precision, and optionally nsim, seed,
+    first_index and sims (3 * nsim device grids)."""
+
+    def __init__(self, vintages, flags=0, stream=None):
+        lib = load_library()
+        self.lib = lib
+        self._keep = []
+        arr = (Vintage * len(vintages))()
+        for k, v in enumerate(vintages):
+            ctx = v["ctx"]
+            nsim = int(v.get("nsim", 0))
+            sims = v.get("sims", [])
+            assert len(sims) == 3 * nsim
+            ptrs = (C.c_void_p * max(1, 3 * nsim))(*[t.data_ptr() for t in sims])
+            self._keep += [ptrs, v]
+            arr[k].ctx = ctx.handle
+            arr[k].inp = ctx.grids(*v["src"])
+            arr[k].out = ctx.grids(*v["dst"])
+            arr[k].precision = v.get("precision", ctx.precision)
+            arr[k].nsim = nsim
+            arr[k].seed = int(v.get("seed", 0))
+            arr[k].first_index = int(v.get("first_index", 0))
+            arr[k].sim_out = C.cast(ptrs, C.POINTER(C.c_void_p)) if nsim else None
+        h = C.c_void_p()
+        sp = C.c_void_p(stream.cuda_stream) if stream is not None else None
+        check(lib.crava_gpu_batch_create(arr, len(vintages), flags, sp, C.byref(h)), "batch_create")
+        self.handle = h
+
+    def run(self):
+        check(self.lib.crava_gpu_batch_run(self.handle), "batch_run")
+
+    def sync(self):
+        check(self.lib.crava_gpu_batch_sync(self.handle), "batch_sync")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.crava_gpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def to_device(arr, device=0):

@@ -27,6 +27,7 @@ SOURCES = {
     "sim.cu": ["-fmad=false"],
     "unit.cu": [],
     "noalloc.cu": [],
+    "batch.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -7,11 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "common.cuh"
-#include "fft.cuh"
-#include "sim.cuh"
-#include "solve.cuh"
-#include "unit.cuh"
+#include "context.cuh"
 
 namespace crava {
 
@@ -26,53 +22,36 @@ void set_last_error(cudaError_t e, const char *what, const char *file, int line)
   g_last_error = buf;
 }
 
+static std::mutex g_smem_mu;
+static std::vector<std::pair<std::pair<int, const void *>, size_t>> g_smem;
+
+int func_smem(const void *fn, size_t bytes) {
+  int dev = 0;
+  CRAVA_CUDA_TRY(cudaGetDevice(&dev));
+  static int dev_max = -1;
+  std::lock_guard<std::mutex> lock(g_smem_mu);
+  if (dev_max < 0) CRAVA_CUDA_TRY(cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if ((long long)bytes > dev_max) return CRAVA_GPU_ERR_ARG;
+  if (bytes <= 48 * 1024) return CRAVA_GPU_OK;
+  for (auto &e : g_smem)
+    if (e.first.first == dev && e.first.second == fn) {
+      if (e.second >= bytes) return CRAVA_GPU_OK;
+      CRAVA_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+      e.second = bytes;
+      return CRAVA_GPU_OK;
+    }
+  CRAVA_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  g_smem.push_back({{dev, fn}, bytes});
+  return CRAVA_GPU_OK;
+}
+
 }  // namespace crava
 
 using namespace crava;
 
-struct crava_gpu_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  crava_gpu_params p{};
-  std::vector<float> wavelet, wnorm, A;
-  std::vector<double> theta, var0;
-  Geom g{};
-  FftPlans plans{};
-  KzTables tables{};
-  SolveConsts consts{};
-  DevCounters *counters = nullptr;  // device
-  cudaEvent_t ev[4] = {};           // start, after forward, after solve, end
-  bool timed = false;               // events of the last call are valid
-  // fused unit (plane kernels + z/solve kernel) and its workspace
-  UnitPlan uplan{};
-  bool fused = false;  // the three-pass path is faster today; set_fused(1) selects the fused kernels
-  float2 *W = nullptr;  // (10 + ntheta) grids in the column-pair layout
-  // per-kernel profiling (events around each launch when enabled)
-  bool prof = false;
-  struct Rec { int kind; cudaEvent_t a, b; double bytes; };
-  std::vector<Rec> recs;
-  std::vector<cudaEvent_t> pool;
-  double prof_ms[16] = {};
-  double prof_bytes[16] = {};
-  long long prof_n[16] = {};
-  // host-buffer path
-  float *work = nullptr;  // (10 + ntheta) grids
-  cudaStream_t s_in = nullptr, s_out = nullptr;
-  std::vector<cudaEvent_t> grid_ev;
-};
-
-namespace {
+namespace crava {
 
 int check_ctx(const crava_gpu_ctx *c) { return c ? CRAVA_GPU_OK : CRAVA_GPU_ERR_ARG; }
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
-    else prev = -1;
-  }
-  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
-};
 
 bool smooth_2357(int n) {
   if (n < 1) return false;
@@ -180,7 +159,7 @@ int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type) {
   return CRAVA_GPU_OK;
 }
 
-int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend = nullptr) {
+int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend) {
   int rc;
   { Scope sc(c, K_COLS_Z_INV); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc; }
   { Scope sc(c, K_COLS_Y_INV); if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc; }
@@ -221,6 +200,34 @@ int unit_order(const crava_gpu_ctx *c, const crava_gpu_grids *g, float **ptr, in
   return i;
 }
 
+int stage_event(crava_gpu_ctx *c, int i) {
+  if (!c->capture) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[i], c->stream));
+  return CRAVA_GPU_OK;
+}
+
+int simulate_batches(crava_gpu_ctx *c, const float2 *const cv[6], const float *const post_mean[3],
+                     uint64_t seed, uint64_t first, int count, float *const *out,
+                     const unsigned long long *epoch, unsigned long long epoch_stride) {
+  int rc;
+  // batches of up to 8 realisations share one read and one factorisation
+  // of the posterior covariance spectra per bin
+  for (int r0 = 0; r0 < count; r0 += 8) {
+    const int nr = count - r0 < 8 ? count - r0 : 8;
+    float2 *o[24];
+    for (int k = 0; k < 3 * nr; ++k) o[k] = reinterpret_cast<float2 *>(out[3 * r0 + k]);
+    const uint64_t stream0 = 3ull * (first + (uint64_t)r0);
+    {
+      Scope sc(c, K_SIM, (6.0 + 3.0 * nr) * (double)c->g.csize * 8.0);
+      if ((rc = noise_filter_multi(c->g, cv, o, nr, seed, stream0, epoch, 3ull * epoch_stride,
+                                   c->counters, c->stream)))
+        return rc;
+    }
+    for (int k = 0; k < 3 * nr; ++k)
+      if ((rc = pass_inverse(c, out[3 * r0 + k], CRAVA_GRID_PARAMETER, post_mean[k % 3]))) return rc;
+  }
+  return CRAVA_GPU_OK;
+}
+
 // Fused unit: plane forward (all grids, one launch), z transform + solve +
 // inverse z (one launch), plane inverse (outputs, one launch).  The noise
 // correlation output is not written (its transform stays in the workspace).
@@ -243,23 +250,23 @@ int run_unit_fused(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_
   const double gb = (double)c->g.csize * 8.0;
   const double wb = (double)c->uplan.wgrid * 8.0;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  if ((rc = stage_event(c, 0))) return rc;
   {
     Scope sc(c, K_PLANE_FWD, G * (gb + wb));
     if ((rc = unit_plane_forward(c->uplan, c->plans, src, w, fs, G, s))) return rc;
   }
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  if ((rc = stage_event(c, 1))) return rc;
   {
     Scope sc(c, K_ZSOLVE, (2 * G - 1) * wb);
     if ((rc = unit_zsolve(c->uplan, c->plans, c->consts, c->tables, w, precision, c->counters, s))) return rc;
   }
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  if ((rc = stage_event(c, 2))) return rc;
   {
     Scope sc(c, K_PLANE_INV, (G - 1) * (gb + wb));
     if ((rc = unit_plane_inverse(c->uplan, c->plans, w, dst, is, nullptr, G - 1, s))) return rc;
   }
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  c->timed = true;
+  if ((rc = stage_event(c, 3))) return rc;
+  c->timed = !c->capture;
   return CRAVA_GPU_OK;
 }
 
@@ -272,7 +279,7 @@ int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids 
   const int nt = c->p.ntheta;
   int rc;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  if ((rc = stage_event(c, 0))) return rc;
   for (int q = 0; q < 3; ++q)
     if ((rc = pass_forward(c, in->mu[q], out->mu[q], CRAVA_GRID_PARAMETER))) return rc;
   for (int l = 0; l < nt; ++l)
@@ -280,21 +287,21 @@ int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids 
   for (int t = 0; t < 6; ++t)
     if ((rc = pass_forward(c, in->cov[t], out->cov[t], CRAVA_GRID_COVARIANCE))) return rc;
   if ((rc = pass_forward(c, in->err_corr, out->err_corr, CRAVA_GRID_COVARIANCE))) return rc;
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  if ((rc = stage_event(c, 1))) return rc;
   if ((rc = pass_solve(c, out, precision))) return rc;
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  if ((rc = stage_event(c, 2))) return rc;
   for (int q = 0; q < 3; ++q)
     if ((rc = pass_inverse(c, out->mu[q], CRAVA_GRID_PARAMETER))) return rc;
   for (int l = 0; l < nt; ++l)
     if ((rc = pass_inverse(c, out->data[l], CRAVA_GRID_DATA))) return rc;
   for (int t = 0; t < 6; ++t)
     if ((rc = pass_inverse(c, out->cov[t], CRAVA_GRID_COVARIANCE))) return rc;
-  CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  c->timed = true;
+  if ((rc = stage_event(c, 3))) return rc;
+  c->timed = !c->capture;
   return CRAVA_GPU_OK;
 }
 
-}  // namespace
+}  // namespace crava
 
 extern "C" {
 
@@ -609,20 +616,8 @@ int crava_gpu_simulate(crava_gpu_ctx *c, const float *const cov[6], const float 
   int rc;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  // batches of up to 8 realisations share one read and one factorisation
-  // of the posterior covariance spectra per bin
-  for (int r0 = 0; r0 < count; r0 += 8) {
-    const int nr = count - r0 < 8 ? count - r0 : 8;
-    float2 *o[24];
-    for (int k = 0; k < 3 * nr; ++k) o[k] = reinterpret_cast<float2 *>(out[3 * r0 + k]);
-    const uint64_t stream0 = 3ull * (uint64_t)(first_index + r0);
-    {
-      Scope sc(c, K_SIM, (6.0 + 3.0 * nr) * (double)c->g.csize * 8.0);
-      if ((rc = noise_filter_multi(c->g, cv, o, nr, seed, stream0, c->counters, s))) return rc;
-    }
-    for (int k = 0; k < 3 * nr; ++k)
-      if ((rc = pass_inverse(c, out[3 * r0 + k], CRAVA_GRID_PARAMETER, post_mean[k % 3]))) return rc;
-  }
+  if ((rc = simulate_batches(c, cv, post_mean, seed, (uint64_t)first_index, count, out, nullptr, 0)))
+    return rc;
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));

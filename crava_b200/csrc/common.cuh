@@ -34,6 +34,11 @@ long long launches();
 
 void set_last_error(cudaError_t e, const char *what, const char *file, int line);
 
+// Raises fn's dynamic shared-memory limit to `bytes` on the current device
+// when it is not already that high (one cudaFuncSetAttribute per kernel and
+// size, so launches recorded into a CUDA graph make no attribute calls).
+int func_smem(const void *fn, size_t bytes);
+
 // ---------------------------------------------------------------- complex
 struct __align__(8) cfloat { float x, y; };
 

@@ -1,0 +1,78 @@
+// context.cuh -- the state behind the C ABI's crava_gpu_ctx handle and the
+// internal steps that the entry points compose (capi.cu, batch.cu).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+#include "sim.cuh"
+#include "solve.cuh"
+#include "unit.cuh"
+
+struct crava_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  crava_gpu_params p{};
+  std::vector<float> wavelet, wnorm, A;
+  std::vector<double> theta, var0;
+  crava::Geom g{};
+  crava::FftPlans plans{};
+  crava::KzTables tables{};
+  crava::SolveConsts consts{};
+  crava::DevCounters *counters = nullptr;  // device
+  cudaEvent_t ev[4] = {};           // start, after forward, after solve, end
+  bool timed = false;               // events of the last call are valid
+  // fused unit (plane kernels + z/solve kernel) and its workspace
+  crava::UnitPlan uplan{};
+  bool fused = false;  // the three-pass path is faster today; set_fused(1) selects the fused kernels
+  float2 *W = nullptr;  // (10 + ntheta) grids in the column-pair layout
+  // per-kernel profiling (events around each launch when enabled)
+  bool prof = false;
+  struct Rec { int kind; cudaEvent_t a, b; double bytes; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double prof_ms[16] = {};
+  double prof_bytes[16] = {};
+  long long prof_n[16] = {};
+  // host-buffer path
+  float *work = nullptr;  // (10 + ntheta) grids
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> grid_ev;
+  // set while a batch captures this context's work into a CUDA graph: the
+  // stage-timing events are not recorded (they would become graph nodes)
+  bool capture = false;
+};
+
+namespace crava {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+    else prev = -1;
+  }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+int check_grids(const crava_gpu_ctx *c, const crava_gpu_grids *gr);
+int valid_precision(int prec);
+bool use_fused(const crava_gpu_ctx *c, int precision);
+// Forward transform of one grid, src -> dst (src == dst: in place).
+int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type);
+// Inverse transform in place; addend (optional) is added to the real output.
+int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend = nullptr);
+int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision);
+// Transforms, solve and inverse transforms (in == out: in place).
+int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids *out,
+             int precision);
+// Records stage event i on the context's stream (skipped during capture).
+int stage_event(crava_gpu_ctx *c, int i);
+// count realisations from the posterior covariance spectra cv: realisation
+// r uses noise streams 3 (first + r) + p, plus 3 epoch_stride (*epoch) when
+// epoch is given (a device counter), and gets post_mean added.
+int simulate_batches(crava_gpu_ctx *c, const float2 *const cv[6], const float *const post_mean[3],
+                     uint64_t seed, uint64_t first, int count, float *const *out,
+                     const unsigned long long *epoch, unsigned long long epoch_stride);
+
+}  // namespace crava

@@ -346,17 +346,7 @@ __global__ void __launch_bounds__(kThreads) k_cols_ip(const __grid_constant__ Co
   }
 }
 
-int set_smem(const void *fn, size_t bytes) {
-  static int dev_max = -1;
-  if (dev_max < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  }
-  if ((long)bytes > dev_max) return CRAVA_GPU_ERR_ARG;
-  if (bytes > 48 * 1024) CRAVA_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  return CRAVA_GPU_OK;
-}
+int set_smem(const void *fn, size_t bytes) { return func_smem(fn, bytes); }
 
 int line_plan_create(int n, LinePlan *p) {
   if (!radix_list(n, &p->rl)) return CRAVA_GPU_ERR_ARG;
@@ -500,7 +490,7 @@ static int cols_tile_width(int n) {
 }
 
 static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
-                long long outer_stride, int nouter, int dir, float scale, cudaStream_t s) {
+                long long outer_stride, int nouter, int dir, float scale, int tile, cudaStream_t s) {
   ColArgs a;
   a.data = data;
   a.ninner = ninner;
@@ -512,7 +502,7 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
   const int n = lp.rl.n;
   size_t smem = sizeof(float2) * (n + 2 * kColTile * n);
   dim3 grd((ninner + kColTile - 1) / kColTile, nouter);
-  const int tx = cols_tile_width(n);
+  const int tx = tile >= 0 ? tile : cols_tile_width(n);
 #define CRAVA_COLS_CT(NN)                                                                   \
   if (n == NN && tx > 0) {                                                                  \
     const dim3 g2((ninner + tx - 1) / tx, nouter);                                          \
@@ -553,14 +543,20 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
   return CRAVA_GPU_OK;
 }
 
+bool cols_tunable(int n) {
+  for (int m : {64, 128, 256, 512, 96, 160, 192, 200, 300, 384})
+    if (n == m) return true;
+  return false;
+}
+
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  return cols(p.y, grid, g.cnxp, g.cnxp, (long long)g.cnxp * g.nyp, g.nzp, dir, 1.0f, s);
+  return cols(p.y, grid, g.cnxp, g.cnxp, (long long)g.cnxp * g.nyp, g.nzp, dir, 1.0f, p.tile_y, s);
 }
 
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, s);
+  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z, s);
 }
 
 int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s) {

@@ -21,7 +21,14 @@ struct FftPlans {
   LinePlan y;        // length nyp
   LinePlan z;        // length nzp
   float2 *xpost = nullptr;  // e^{-2 pi i k/nxp}, k = 0..nxp/2 (even nxp)
+  // column tile of the y and z passes: -1 default, 0 ping-pong pass,
+  // 8 or 16 columns per CTA in the in-place pass (lengths with compiled
+  // kernels only; other lengths use the generic pass)
+  int tile_y = -1, tile_z = -1;
 };
+
+// Whether length n has compiled column kernels (tile choices 0, 8, 16).
+bool cols_tunable(int n);
 
 bool radix_list(int n, RadixList *out);
 int fft_plans_create(const Geom &g, FftPlans *p);

@@ -212,6 +212,8 @@ struct NoiseFilterMultiArgs {
   long long csize;
   int cnxp, nyp, nzp;
   uint64_t seed, stream0;
+  const unsigned long long *epoch;  // optional device counter: stream0 += epoch_mul * (*epoch)
+  unsigned long long epoch_mul;
   DevCounters *counters;
 };
 
@@ -225,10 +227,11 @@ __global__ void __launch_bounds__(kThreads) k_noise_filter_multi(const __grid_co
   P[2][0] = make_float2(P[0][2].x, -P[0][2].y);
   P[2][1] = make_float2(P[1][2].x, -P[1][2].y);
   const bool ok = chol3_ref(P) == 0;
+  const uint64_t stream0 = a.stream0 + (a.epoch ? a.epoch_mul * *a.epoch : 0ull);
   for (int r = 0; r < a.nreal; ++r) {
     float2 z[3], o[3];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) z[q] = noise_bin(i, a.cnxp, a.nyp, a.nzp, a.seed, a.stream0 + 3ull * r + q);
+    for (int q = 0; q < 3; ++q) z[q] = noise_bin(i, a.cnxp, a.nyp, a.nzp, a.seed, stream0 + 3ull * r + q);
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
       o[p] = make_float2(0.0f, 0.0f);
@@ -254,7 +257,8 @@ __global__ void __launch_bounds__(kThreads) k_noise_filter_multi(const __grid_co
 }  // namespace
 
 int noise_filter_multi(const Geom &g, const float2 *const cov[6], float2 *const *out, int nreal,
-                       uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s) {
+                       uint64_t seed, uint64_t stream0, const unsigned long long *epoch,
+                       unsigned long long epoch_mul, DevCounters *counters, cudaStream_t s) {
   if (nreal < 1 || nreal > kMaxSimBatch) return CRAVA_GPU_ERR_ARG;
   NoiseFilterMultiArgs a;
   for (int t = 0; t < 6; ++t) a.cov[t] = cov[t];
@@ -263,6 +267,7 @@ int noise_filter_multi(const Geom &g, const float2 *const cov[6], float2 *const 
   a.csize = g.csize;
   a.cnxp = g.cnxp; a.nyp = g.nyp; a.nzp = g.nzp;
   a.seed = seed; a.stream0 = stream0;
+  a.epoch = epoch; a.epoch_mul = epoch_mul;
   a.counters = counters;
   dim3 grd((unsigned)((g.csize + kThreads - 1) / kThreads));
   k_noise_filter_multi<<<grd, kThreads, 0, s>>>(a);

@@ -13,8 +13,11 @@ int sim_filter(const Geom &g, const float2 *const cov[6], float2 *const seed[3],
 int noise_filter(const Geom &g, const float2 *const cov[6], float2 *const out[3],
                  uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s);
 
-// nreal (<= 8) realisations in one pass: out[3 r + p], streams stream0 + 3 r + p.
+// nreal (<= 8) realisations in one pass: out[3 r + p], streams
+// stream0 + 3 r + p, plus epoch_mul * (*epoch) when epoch (a device
+// counter) is given.
 int noise_filter_multi(const Geom &g, const float2 *const cov[6], float2 *const *out, int nreal,
-                       uint64_t seed, uint64_t stream0, DevCounters *counters, cudaStream_t s);
+                       uint64_t seed, uint64_t stream0, const unsigned long long *epoch,
+                       unsigned long long epoch_mul, DevCounters *counters, cudaStream_t s);
 
 }  // namespace crava

@@ -395,7 +395,7 @@ int unit_plane_forward(const UnitPlan &p, const FftPlans &f, const float *const 
   fill_plane_args(p, f, &a);
   for (int i = 0; i < n; ++i) { a.src_r[i] = src[i]; a.w[i] = w[i]; a.scale[i] = scale[i]; }
   a.nitems = n * p.g.nzp;
-  CRAVA_CUDA_TRY(cudaFuncSetAttribute(k_plane_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.plane_smem));
+  { int rc = func_smem((const void *)k_plane_fwd, p.plane_smem); if (rc) return rc; }
   return launch_cluster(k_plane_fwd, a.nitems, p.CS, p.plane_smem, s, a);
 }
 
@@ -412,7 +412,7 @@ int unit_plane_inverse(const UnitPlan &p, const FftPlans &f, const float2 *const
     a.add[i] = addend ? addend[i] : nullptr;
   }
   a.nitems = n * p.g.nzp;
-  CRAVA_CUDA_TRY(cudaFuncSetAttribute(k_plane_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.plane_smem));
+  { int rc = func_smem((const void *)k_plane_inv, p.plane_smem); if (rc) return rc; }
   return launch_cluster(k_plane_inv, a.nitems, p.CS, p.plane_smem, s, a);
 }
 
@@ -422,8 +422,7 @@ static int launch_z(const ZArgs &a, int nt, const UnitPlan &p, cudaStream_t s) {
   const int smem = (int)p.z_smem;
 #define CRAVA_Z_CASE(N)                                                                       \
   case N:                                                                                     \
-    CRAVA_CUDA_TRY(cudaFuncSetAttribute(k_zsolve<N, PREC>,                                    \
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, smem));  \
+    { int rc_ = func_smem((const void *)k_zsolve<N, PREC>, (size_t)smem); if (rc_) return rc_; } \
     k_zsolve<N, PREC><<<grd, kThreads, smem, s>>>(a);                                         \
     break;
   switch (nt) {

@@ -236,6 +236,76 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
                                 const crava_gpu_grids *grids, int precision,
                                 void *stream, crava_gpu_stats *stats);
 
+/* Launch shapes of a context.  cols_y_tile / cols_z_tile: columns per CTA
+ * of the y and z column transforms (-1 the built-in choice, 0 the
+ * out-of-place pass, 8 or 16 the in-place pass; lengths without compiled
+ * column kernels ignore it); fused: the fused unit kernels (1) or the
+ * three passes (0); ms: one unit's measured time (autotune output only).
+ * No counterpart in the reference (FFTW plans are fixed there). */
+typedef struct crava_gpu_tuning {
+  int cols_y_tile;
+  int cols_z_tile;
+  int fused;
+  float ms;
+} crava_gpu_tuning;
+int crava_gpu_get_tuning(crava_gpu_ctx *ctx, crava_gpu_tuning *out);
+int crava_gpu_set_tuning(crava_gpu_ctx *ctx, const crava_gpu_tuning *t);
+
+/* Autotuner: times the out-of-place unit (crava_gpu_posterior_unit_oop, in
+ * -> out) under every launch-shape candidate of this geometry, reps timed
+ * runs after one warm-up each, keeps the fastest on the context and
+ * returns it in best (may be NULL).  in and out must not share a grid (the
+ * inputs are read again by every candidate); out is overwritten.
+ * Synchronous.  No counterpart in the reference. */
+int crava_gpu_autotune(crava_gpu_ctx *ctx, const crava_gpu_grids *in,
+                       const crava_gpu_grids *out, int precision, int reps,
+                       crava_gpu_tuning *best);
+
+/* Batch: several vintages (one context each, grids of any size), each
+ * inverted and sampled, replayed as one CUDA graph launch.  Per vintage and
+ * run: the posterior unit from `in` into `out` in the reference's order --
+ * forward transforms, per-bin solve, inverse transforms of the posterior
+ * means and residuals (Crava::computePostMeanResidAndFFTCov,
+ * src/crava.cpp:952-1220) -- then nsim realisations from the posterior
+ * covariance spectra (Crava::simulate, src/crava.cpp:1415-1599), then the
+ * inverse transforms of the six covariance grids.  Run e (0, 1, ...) draws
+ * realisations first_index + e*nsim + r, r < nsim, each with the noise of
+ * crava_gpu_simulate for that index, so replays give fresh, reproducible
+ * realisations.  Vintages run on separate branches of the graph. */
+typedef struct crava_gpu_vintage {
+  crava_gpu_ctx *ctx;
+  crava_gpu_grids in;      /* real inputs (read, not written)            */
+  crava_gpu_grids out;     /* outputs, layout of crava_gpu_posterior_unit */
+  int precision;
+  int nsim;                /* realisations per run (0: none)             */
+  uint64_t seed;
+  uint64_t first_index;
+  float *const *sim_out;   /* 3 * nsim real grids: alpha, beta, rho of
+                              realisation r at 3 r + 0, 1, 2            */
+} crava_gpu_vintage;
+
+typedef struct crava_gpu_batch crava_gpu_batch;
+enum crava_gpu_batch_flags {
+  CRAVA_BATCH_AUTOTUNE = 1, /* autotune each context before capture      */
+  CRAVA_BATCH_NO_GRAPH = 2  /* enqueue the work on every run, no graph   */
+};
+/* Validates, (optionally) autotunes, runs the batch once uncaptured (this
+ * allocates the contexts' workspaces) and captures it into a graph.  The
+ * warm-up run does not count as a run.  stream: the cudaStream_t the
+ * batch runs on (NULL: the batch creates one).  All contexts on one device,
+ * profiling off.  A context's workspaces and counters are shared with its
+ * other calls: make none while a run is in flight (after
+ * crava_gpu_batch_sync they are free again).  Each vintage's `in` and `out`
+ * grids must be distinct (the inputs are read again on every run). */
+int crava_gpu_batch_create(const crava_gpu_vintage *vintages, int n, int flags,
+                           void *stream, crava_gpu_batch **out);
+/* One run of every vintage: one cudaGraphLaunch on the batch stream
+ * (asynchronous). */
+int crava_gpu_batch_run(crava_gpu_batch *b);
+/* Waits for the batch stream. */
+int crava_gpu_batch_sync(crava_gpu_batch *b);
+int crava_gpu_batch_destroy(crava_gpu_batch *b);
+
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
 

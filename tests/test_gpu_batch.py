@@ -1,0 +1,136 @@
+"""Launch-shape choices, the autotuner and the vintage batch (CUDA graph):
+every tile choice gives the same transform, and a batch run gives exactly
+what the separate entry points give."""
+import numpy as np
+import pytest
+import torch
+
+from crava_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-30))
+
+
+# every column length with compiled kernels, as y and as z
+TILE_SHAPES = [(8, 64, 128), (8, 256, 512), (8, 96, 160), (8, 192, 200), (8, 300, 384),
+               (8, 128, 64), (8, 384, 300)]
+
+
+@pytest.mark.parametrize("shape", TILE_SHAPES)
+def test_column_tiles_match_numpy(shape):
+    nx, ny, nz = shape
+    case = synth.make_case(nx, ny, nz, (10.0,), 0.1, seed=4)
+    ctx = api.Context(case)
+    g = case.data[0]
+    ref = np.fft.rfftn(g[..., :nx].astype(np.float64), axes=(0, 1, 2)) / np.sqrt(nx * ny * nz)
+    res = {}
+    for ty in (16, 8, 0):
+        for tz in (16, 8, 0):
+            ctx.set_tuning(ty, tz, 0)
+            t = api.to_device(g)
+            ctx.fft_r2c(t, api.DATA)
+            out = api.complex_view(t.cpu().numpy(), nx).copy()
+            assert rel(out, ref) < 2e-6, (ty, tz)
+            ctx.fft_c2r(t, api.DATA)
+            assert rel(t.cpu().numpy()[..., :nx], g[..., :nx]) < 2e-6, (ty, tz)
+            res[(ty, tz)] = out
+    # the in-place pass does the same arithmetic per line whatever the tile
+    assert np.array_equal(res[(16, 16)], res[(8, 8)])
+    assert np.array_equal(res[(16, 8)], res[(8, 16)])
+
+
+def _dev(case):
+    d = lambda gs: [api.to_device(g) for g in gs]
+    return d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0]
+
+
+def test_autotune_keeps_the_fastest_and_the_results():
+    case = synth.make_case(64, 64, 128, (10.0, 20.0, 30.0), 0.1, seed=8)
+    ctx = api.Context(case, precision=api.FP64)
+    src, dst = _dev(case), _dev(case)
+    ref = _dev(case)
+    ctx.posterior_unit_oop(src, ref, api.FP64)
+    best = ctx.autotune(src, dst, api.FP64, reps=2)
+    assert best.ms > 0.0
+    t = ctx.tuning()
+    assert (t.cols_y_tile, t.cols_z_tile, t.fused) == (best.cols_y_tile, best.cols_z_tile, best.fused)
+    ctx.posterior_unit_oop(src, dst, api.FP64)
+    for a, b in zip(dst[0] + dst[1] + dst[2], ref[0] + ref[1] + ref[2]):
+        assert rel(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
+    with pytest.raises(api.CravaGpuError):
+        ctx.autotune(src, src, api.FP64)  # inputs would be overwritten
+
+
+def _separate(ctx, case, nsim, seed, first, precision):
+    """The batch's work through the separate entry points (reference order:
+    transforms, solve, inverse means/residuals, realisations, inverse
+    covariances)."""
+    mu, data, cov, err = _dev(case)
+    for g in mu:
+        ctx.fft_r2c(g, api.PARAMETER)
+    for g in data:
+        ctx.fft_r2c(g, api.DATA)
+    for g in cov + [err]:
+        ctx.fft_r2c(g, api.COVARIANCE)
+    ctx.posterior(mu, data, cov, err, precision)
+    for g in mu:
+        ctx.fft_c2r(g, api.PARAMETER)
+    for g in data:
+        ctx.fft_c2r(g, api.DATA)
+    sims = [torch.zeros_like(mu[0]) for _ in range(3 * nsim)]
+    if nsim:
+        ctx.simulate(cov, mu, seed, first, sims)
+    for g in cov:
+        ctx.fft_c2r(g, api.COVARIANCE)
+    return mu, data, cov, sims
+
+
+@pytest.mark.parametrize("flags", [0, api.BATCH_NO_GRAPH])
+def test_batch_matches_separate_calls(flags):
+    cases = [synth.make_case(32, 24, 64, (10.0, 20.0, 30.0), 0.1, seed=31),
+             synth.make_case(20, 18, 30, (0.0, 10.0, 20.0, 30.0, 40.0), 0.1, seed=32),
+             synth.make_case(64, 48, 40, (5.0, 25.0), 0.1, seed=33)]
+    nsims, seeds, firsts = [3, 2, 0], [5, 6, 7], [0, 10, 0]
+    precs = [api.MIXED, api.FP64, api.FP64]
+    ctxs = [api.Context(c, precision=p) for c, p in zip(cases, precs)]
+    ctxs[2].set_fused(True)  # the fused unit inside the graph too
+    vint, dsts, simss = [], [], []
+    for c, ctx, n, s, f, p in zip(cases, ctxs, nsims, seeds, firsts, precs):
+        src, dst = _dev(c), _dev(c)
+        sims = [torch.zeros_like(src[0][0]) for _ in range(3 * n)]
+        vint.append(dict(ctx=ctx, src=src, dst=dst, precision=p, nsim=n, seed=s, first_index=f,
+                         sims=sims))
+        dsts.append(dst)
+        simss.append(sims)
+    b = api.Batch(vint, flags)
+    n0 = api.launch_count()
+    for run in range(2):
+        b.run()
+        b.sync()
+        for k, (c, ctx) in enumerate(zip(cases, ctxs)):
+            if k == 2:
+                ref = _dev(c)
+                ctx.posterior_unit_oop(_dev(c), ref, precs[k])
+                mu, data, cov = ref[0], ref[1], ref[2]
+                sims = []
+            else:
+                mu, data, cov, sims = _separate(ctx, c, nsims[k], seeds[k],
+                                                firsts[k] + run * nsims[k], precs[k])
+            mine = dsts[k]
+            for a, r in zip(mine[0] + mine[1] + mine[2], mu + data + cov):
+                assert torch.equal(a, r), (run, k)
+            for a, r in zip(simss[k], sims):
+                assert torch.equal(a, r), (run, k)
+    assert api.launch_count() - n0 > 0
+    b.close()
+
+
+def test_batch_rejects_in_place_vintages():
+    case = synth.make_case(16, 12, 32, (10.0,), 0.1, seed=1)
+    ctx = api.Context(case)
+    g = _dev(case)
+    with pytest.raises(api.CravaGpuError):
+        api.Batch([dict(ctx=ctx, src=g, dst=g, precision=api.FP64)])
