@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-simulation", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
     return ap.parse_args()
 
@@ -105,25 +108,84 @@ def _ref_worker(args):
 
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock, max clock and throttle reasons sampled every 20 ms through
+    NVML in a thread while the timed region runs (read-only queries); falls
+    back to `nvidia-smi -lms` when NVML is not importable."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("sw_power_cap", 0x4), ("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20),
+               ("hw_thermal_slowdown", 0x40), ("hw_power_brake_slowdown", 0x80))
 
     def __init__(self, device_index):
-        self.path = tempfile.mktemp(prefix="crava_clocks_", suffix=".csv")
-        self.proc = None
         self.dev = device_index
+        self.samples = []
+        self.thread = None
+        self.proc = None
+
+    def _nvml_handle(self):
+        import pynvml as N
+        import torch
+
+        N.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            return N, N.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        import threading
+
         try:
+            N, h = self._nvml_handle()
+        except Exception:
+            return self._start_smi()
+        reasons_fn = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            N.nvmlDeviceGetCurrentClocksThrottleReasons
+        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        self.stop_flag = threading.Event()
+
+        def sample():
+            self.samples.append((N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM), mx, int(reasons_fn(h))))
+
+        sample()
+
+        def loop():
+            while not self.stop_flag.wait(0.02):
+                try:
+                    sample()
+                except Exception:
+                    break
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+
+    def _start_smi(self):
+        import time as _t
+
+        try:
+            self.path = tempfile.mktemp(prefix="crava_clocks_", suffix=".csv")
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "100", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+            t0 = _t.time()
+            while _t.time() - t0 < 5 and os.path.getsize(self.path) == 0:
+                _t.sleep(0.05)
         except Exception:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            sm = [x[0] for x in self.samples]
+            reasons = sorted({n for _, _, r in self.samples for n, bit in self.REASONS if r & bit})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(x[1] for x in self.samples),
+                    "reasons": reasons, "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -151,10 +213,131 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 # ----------------------------------------------------------------- own arm
+VINTAGES = [(128, 128, 256), (192, 160, 384), (256, 256, 512), (96, 200, 300)]
+
+
+def run_batch(args, case256, dev, stream, max_over_ranks):
+    """Time-lapse batch: four vintages of uneven size, 5 angles each, every
+    run = posterior unit + nsim realisations per vintage, replayed as one
+    CUDA graph launch (launch shapes autotuned per vintage first)."""
+    import torch
+
+    from crava_b200 import api, synth
+
+    R = args.batch_sims
+    vint, ctxs = [], []
+    cells = 0
+    for k, shp in enumerate(VINTAGES):
+        c = case256 if (case256 is not None and shp == (256, 256, 512)) else \
+            synth.make_case(*shp, ANGLES5, args.noise, seed=40 + k, wavelet_scale_range=(0.8, 1.2))
+        ctx = api.Context(c, device=dev, stream=stream, precision=api.MIXED)
+        d = lambda gs: [api.to_device(g, dev) for g in gs]
+        src = (d(c.mu), d(c.data), d(c.cov), d([c.err_corr])[0])
+        dst = (d(c.mu), d(c.data), d(c.cov), d([c.err_corr])[0])
+        sims = [torch.empty_like(src[0][0]) for _ in range(3 * R)]
+        vint.append(dict(ctx=ctx, src=src, dst=dst, precision=api.MIXED, nsim=R, seed=100 + k,
+                         first_index=0, sims=sims))
+        ctxs.append(ctx)
+        cells += shp[0] * shp[1] * shp[2]
+
+    def timed(b, runs):
+        for _ in range(2):
+            b.run()
+        b.sync()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        n0 = api.launch_count()
+        for _ in range(runs):
+            b.run()
+        ev1.record(stream)
+        b.sync()
+        torch.cuda.synchronize(dev)
+        return max_over_ranks(ev0.elapsed_time(ev1) / runs), (api.launch_count() - n0) // runs
+
+    g = api.Batch(vint, api.BATCH_AUTOTUNE, stream=stream)
+    tunings = [{"cols_y_tile": t.cols_y_tile, "cols_z_tile": t.cols_z_tile, "fused": t.fused}
+               for t in (ctx.tuning() for ctx in ctxs)]
+    ms_graph, kern = timed(g, 5)
+    g.close()
+    e = api.Batch(vint, api.BATCH_NO_GRAPH, stream=stream)
+    ms_eager, _ = timed(e, 3)
+    e.close()
+    for ctx in ctxs:
+        ctx.close()
+    del vint
+    torch.cuda.empty_cache()
+    return {"workload": "vintages %s x 5 angles, mixed solve, %d realisations each, one graph launch per run"
+                        % (["x".join(map(str, v)) for v in VINTAGES], R),
+            "ms_per_run": ms_graph, "ms_per_run_eager": ms_eager,
+            "cells_per_s": cells / (ms_graph * 1e-3),
+            "realisations_per_s": len(VINTAGES) * R / (ms_graph * 1e-3),
+            "kernels_per_run": kern, "tuning": tunings}
+
+
+def run_adjoint(ctx, case, src, dev):
+    """Log marginal likelihood + adjoint at the bench size: time of one
+    evaluation (value and all gradients) and the largest relative gap to
+    central finite differences (step 1e-3 relative, FP64) over the wavelet
+    scales, noise variances and 8 in-band wavelet-spectrum components."""
+    import numpy as np
+    import torch
+
+    from crava_b200 import api
+
+    g = [[t.clone() for t in src[0]], [t.clone() for t in src[1]], [t.clone() for t in src[2]],
+         src[3].clone()]
+    for t in g[0]:
+        ctx.fft_r2c(t, api.PARAMETER)
+    for t in g[1]:
+        ctx.fft_r2c(t, api.DATA)
+    for t in g[2] + [g[3]]:
+        ctx.fft_r2c(t, api.COVARIANCE)
+    torch.cuda.synchronize(dev)
+    nt, cn = case.ntheta, case.nzp // 2 + 1
+    spec = np.fft.fft(case.wavelet.astype(np.float64), axis=-1)[:, :cn].T.copy()
+    s0 = np.ones(nt)
+    v0 = np.diag(case.theta_cov).copy()
+    ctx.loglik_grad(*g, s0, v0, spec)  # warm-up
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        L, gs, gv, gw, nf = ctx.loglik_grad(*g, s0, v0, spec)
+    ms = (time.perf_counter() - t0) * 1e3 / reps
+    worst = 0.0
+
+    def fd(f, x0, i, h):
+        xp, xm = x0.copy(), x0.copy()
+        xp[i] += h
+        xm[i] -= h
+        return (f(xp) - f(xm)) / (2 * h)
+
+    checks = []
+    for i in range(nt):
+        checks.append((fd(lambda s: ctx.loglik_grad(*g, s, v0, spec)[0], s0, i, 1e-3), gs[i]))
+        checks.append((fd(lambda v: ctx.loglik_grad(*g, s0, v, spec)[0], v0, i, 1e-3 * v0[i]), gv[i]))
+    _, _, _, _, inv = ctx.kz_tables()
+    band = [k for k in range(1, cn - 1) if inv[k]]
+    flat = np.stack([spec.real, spec.imag], -1).reshape(-1)
+    gflat = np.stack([gw.real, gw.imag], -1).reshape(-1)
+    f = lambda x: ctx.loglik_grad(*g, s0, v0, x.reshape(cn, nt, 2))[0]
+    for k, l in [(band[0], 0), (band[len(band) // 3], 1), (band[len(band) // 2], 2), (band[-1], 4)]:
+        for part in (0, 1):
+            i = (k * nt + l) * 2 + part
+            checks.append((fd(f, flat, i, 1e-3 * abs(spec[k, l])), gflat[i]))
+    for a, b in checks:
+        worst = max(worst, abs(a - b) / max(abs(a), abs(b), 1e-300))
+    del g
+    return {"workload": "log marginal likelihood + adjoint, %dx%dx%d, %d angles (FP64)"
+                        % (case.nxp, case.nyp, case.nzp, nt),
+            "ms_per_eval": ms, "loglik": L, "failed_bins": nf,
+            "fd_checked": len(checks), "fd_max_rel_err": worst}
+
+
 def run_own(args):
     import numpy as np
     import torch
@@ -268,6 +451,15 @@ def run_own(args):
                "grid": [nxp, nyp, nzp]}
         del covf, outs
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(ctx, case, src, dev)
+
+    batch = None
+    if not args.no_batch:
+        batch = run_batch(args, case if (nxp, nyp, nzp) == (256, 256, 512) else None, dev, stream,
+                          max_over_ranks)
+
     roof = None
     if prof:
         name, (n, tot, bpl) = max(prof.items(), key=lambda kv: kv[1][1])
@@ -326,6 +518,8 @@ def run_own(args):
         "fp64_form_value": fp64_value,
         "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
         "simulation": sim,
+        "batch": batch,
+        "adjoint": adjoint,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,
         "chol_fail_bins": st.chol_fail_bins, "nonfinite_bins": st.nonfinite_bins,

@@ -105,6 +105,8 @@ SYMBOLS = {
     "crava_gpu_batch_run": ([C.c_void_p], C.c_int),
     "crava_gpu_batch_sync": ([C.c_void_p], C.c_int),
     "crava_gpu_batch_destroy": ([C.c_void_p], C.c_int),
+    "crava_gpu_loglik_grad": ([C.c_void_p, C.POINTER(Grids), F64P, F64P, F64P, F64P, F64P, F64P, F64P,
+                               C.POINTER(C.c_longlong)], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -245,6 +247,31 @@ class Context:
         check(self.lib.crava_gpu_autotune(self.handle, C.byref(gi), C.byref(go), p, reps, C.byref(t)),
               "autotune")
         return t
+
+    def loglik_grad(self, mu, data, cov, err, wavelet_scale=None, noise_var=None, wavelet_spec=None):
+        """Log marginal likelihood of the transformed data and its gradients
+        (crava_gpu_loglik_grad).  wavelet_spec / the returned spectrum
+        gradient: complex [nzp/2+1, ntheta].  Returns (L, g_scale, g_noise,
+        g_spec, failed_bins)."""
+        nt, cn = self.case.ntheta, self.case.nzp // 2 + 1
+        g = self.grids(mu, data, cov, err)
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        sc, nv = f64(wavelet_scale), f64(noise_var)
+        sp = None
+        if wavelet_spec is not None:
+            w = np.asarray(wavelet_spec)
+            sp = np.ascontiguousarray(np.stack([w.real, w.imag], -1), dtype=np.float64) \
+                if np.iscomplexobj(w) else f64(w)
+            assert sp.size == cn * nt * 2
+        ptr = lambda a: a.ctypes.data_as(F64P) if a is not None else None
+        L = C.c_double(0.0)
+        gs, gv = np.zeros(nt), np.zeros(nt)
+        gw = np.zeros((cn, nt, 2))
+        nf = C.c_longlong(0)
+        check(self.lib.crava_gpu_loglik_grad(self.handle, C.byref(g), ptr(sc), ptr(nv), ptr(sp),
+                                             C.byref(L), ptr(gs), ptr(gv), ptr(gw), C.byref(nf)),
+              "loglik_grad")
+        return L.value, gs, gv, gw[..., 0] + 1j * gw[..., 1], nf.value
 
     def set_fused(self, enable=True):
         check(self.lib.crava_gpu_set_fused(self.handle, int(bool(enable))), "set_fused")

@@ -28,6 +28,7 @@ SOURCES = {
     "unit.cu": [],
     "noalloc.cu": [],
     "batch.cu": [],
+    "loglik.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -306,6 +306,30 @@ int crava_gpu_batch_run(crava_gpu_batch *b);
 int crava_gpu_batch_sync(crava_gpu_batch *b);
 int crava_gpu_batch_destroy(crava_gpu_batch *b);
 
+/* Gaussian log marginal likelihood of the seismic spectra and its adjoint.
+ * Per inverted bin the data spectra are CN(K mu, M) with
+ * M = K S K^H + N, the matrices of crava_gpu_posterior (K = diag(w) A,
+ * w_l(kz) = s_l D(kz) conj(W_l(kz)), D(kz) = exp(2 pi i kz/nzp) - 1, S the
+ * prior covariance, N the noise covariance with angle l's variance v_l
+ * replacing theta_cov[l][l] at fixed correlations).  Returns
+ *   L = sum_k c_k (-log det M_k - r_k^H M_k^-1 r_k),  r = d - K mu,
+ * c_k = 2 off the kx = 0 and Nyquist planes (the stored half spectrum
+ * stands for the full one), and dL/ds_l, dL/dv_l and dL/dW_l(kz) for
+ * kz = 0 .. nzp/2 (complex: dL/dRe + i dL/dIm, W(nzp-kz) = conj(W(kz))).
+ * grids: transformed, as crava_gpu_posterior takes them; not modified.
+ * wavelet_scale [ntheta] (NULL: 1), noise_var [ntheta] (NULL: theta_cov
+ * diagonal), wavelet_spec [nzp/2+1][ntheta] (re, im) (NULL: the DFT of the
+ * context's wavelets).  Outputs may be NULL except loglik; failed_bins:
+ * inverted bins whose M did not factor (left out).  The noise colouring
+ * tables (e1, e2, e3) stay fixed.  FP64; synchronous.  Recomputes M and
+ * its factor per bin (nothing of a forward pass is stored).  No
+ * counterpart in the reference (its wavelet and noise estimates are not
+ * gradient-based). */
+int crava_gpu_loglik_grad(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
+                          const double *wavelet_scale, const double *noise_var,
+                          const double *wavelet_spec, double *loglik, double *g_scale,
+                          double *g_noise, double *g_spec, long long *failed_bins);
+
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
 
