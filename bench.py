@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-simulation", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-forward", action="store_true")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
     return ap.parse_args()
@@ -279,6 +280,33 @@ def run_batch(args, case256, dev, stream, max_over_ranks):
             "kernels_per_run": kern, "tuning": tunings}
 
 
+def run_forward(ctx, case, src, dev, stream, max_over_ranks):
+    """Synthetic seismic (Crava::computeSyntSeismic) of the three parameter
+    grids for all angles: device time per call and HBM rate against the
+    algorithmic (3 + ntheta) grids per call."""
+    import torch
+
+    m = src[0]
+    outs = [torch.empty_like(m[0]) for _ in range(case.ntheta)]
+    for _ in range(3):
+        ctx.synt_seismic(*m, outs)
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    reps = 10
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.synt_seismic(*m, outs)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / reps)
+    gbytes = (3 + case.ntheta) * m[0].numel() * 4
+    del outs
+    return {"workload": "synthetic seismic %dx%dx%d, %d angles" % (case.nxp, case.nyp, case.nzp, case.ntheta),
+            "ms_per_call": ms, "cells_per_s": case.nxp * case.nyp * case.nzp / (ms * 1e-3),
+            "algorithmic_GB": gbytes / 1e9, "GB/s": gbytes / (ms * 1e-3) / 1e9}
+
+
 def run_adjoint(ctx, case, src, dev):
     """Log marginal likelihood + adjoint at the bench size: time of one
     evaluation (value and all gradients) and the largest relative gap to
@@ -451,6 +479,10 @@ def run_own(args):
                "grid": [nxp, nyp, nzp]}
         del covf, outs
 
+    fwd = None
+    if not args.no_forward:
+        fwd = run_forward(ctx, case, src, dev, stream, max_over_ranks)
+
     adjoint = None
     if not args.no_adjoint:
         adjoint = run_adjoint(ctx, case, src, dev)
@@ -520,6 +552,7 @@ def run_own(args):
         "simulation": sim,
         "batch": batch,
         "adjoint": adjoint,
+        "forward_model": fwd,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,
         "chol_fail_bins": st.chol_fail_bins, "nonfinite_bins": st.nonfinite_bins,

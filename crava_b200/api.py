@@ -107,6 +107,8 @@ SYMBOLS = {
     "crava_gpu_batch_destroy": ([C.c_void_p], C.c_int),
     "crava_gpu_loglik_grad": ([C.c_void_p, C.POINTER(Grids), F64P, F64P, F64P, F64P, F64P, F64P, F64P,
                                C.POINTER(C.c_longlong)], C.c_int),
+    "crava_gpu_synt_seismic": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                C.POINTER(C.c_void_p)], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -272,6 +274,13 @@ class Context:
                                              C.byref(L), ptr(gs), ptr(gv), ptr(gw), C.byref(nf)),
               "loglik_grad")
         return L.value, gs, gv, gw[..., 0] + 1j * gw[..., 1], nf.value
+
+    def synt_seismic(self, alpha, beta, rho, outs, nx=0, ny=0):
+        """Synthetic seismic of the real parameter grids into outs (one real
+        grid per angle), Crava::computeSyntSeismic."""
+        arr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        check(self.lib.crava_gpu_synt_seismic(self.handle, _ptr(alpha), _ptr(beta), _ptr(rho), nx, ny, arr),
+              "synt_seismic")
 
     def set_fused(self, enable=True):
         check(self.lib.crava_gpu_set_fused(self.handle, int(bool(enable))), "set_fused")

@@ -29,6 +29,7 @@ SOURCES = {
     "noalloc.cu": [],
     "batch.cu": [],
     "loglik.cu": [],
+    "forward.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -382,6 +382,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->counters);
   cudaFree(c->work);
   cudaFree(c->W);
+  cudaFree(c->synt_H);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }

@@ -42,6 +42,8 @@ struct crava_gpu_ctx {
   // set while a batch captures this context's work into a CUDA graph: the
   // stage-timing events are not recorded (they would become graph nodes)
   bool capture = false;
+  // synthetic seismic: per-angle spectral filters [ntheta][nzp] (device)
+  float2 *synt_H = nullptr;
 };
 
 namespace crava {

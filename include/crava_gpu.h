@@ -330,6 +330,20 @@ int crava_gpu_loglik_grad(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
                           const double *wavelet_spec, double *loglik, double *g_scale,
                           double *g_noise, double *g_spec, long long *failed_bins);
 
+/* Synthetic seismic, Crava::computeSyntSeismic (src/crava.cpp:1666-1719)
+ * with computeSeismicImpedance (:1632-1663), constant thickness: for each
+ * angle l, out[l] (real padded grid) receives imp = sum_p A[l][p] m_p on
+ * every cell; on the traces x < nx, y < ny the layers z >= nz are replaced
+ * by the reference's linear taper between layers 0 and nz-1, and the trace
+ * is differenced forward in z (cyclic) and multiplied in the Fourier
+ * domain by conj(W_l(kz)), the unnormalised spectrum of wavelet l (the
+ * reference's getCAmp(k, 1)), then transformed back (1/nzp).  alpha, beta,
+ * rho: real padded grids, not modified; nx, ny: unpadded lateral sizes
+ * (0: nxp, nyp); nz: the context's.  nz = nzp - 1 is rejected (the
+ * reference's taper divides by nzp - nz - 1).  Asynchronous. */
+int crava_gpu_synt_seismic(crava_gpu_ctx *ctx, const float *alpha, const float *beta,
+                           const float *rho, int nx, int ny, float *const *out);
+
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
 

@@ -822,3 +822,63 @@ int orc_sim_filter_fp64(int nxp, int nyp, int nzp, const float *const *cov_,
   if (chol_fail) *chol_fail = fails;
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Synthetic seismic: Crava::computeSyntSeismic (src/crava.cpp:1666-1719)
+ * with computeSeismicImpedance (:1632-1663), constant thickness: per
+ * angle, the impedance combination on every real cell; per trace
+ * x < nx, y < ny the linear taper over the padding layers, the cyclic
+ * forward difference (Wavelet1D FIRSTORDERFORWARDDIFF,
+ * src/wavelet1D.cpp:420-440), the unnormalised spectrum times conj(W(k))
+ * for k <= nzp/2 (getCAmp(k, 1), src/wavelet.cpp:327-385), and the
+ * inverse transform scaled by 1/nzp (src/wavelet.cpp:264-280).  The 1-D
+ * transforms here are double precision.                                */
+/* ------------------------------------------------------------------ */
+int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
+                     const float *A, const float *wavelet, const float *const *m,
+                     float *const *out) {
+  int cnxp = nxp / 2 + 1, rnxp = 2 * cnxp, cnzp = nzp / 2 + 1;
+  long plane = (long)rnxp * nyp, rsize = plane * nzp;
+  float *imp = (float *)malloc(sizeof(float) * nzp), *dif = (float *)malloc(sizeof(float) * nzp);
+  cd *W = (cd *)malloc(sizeof(cd) * nzp), *x = (cd *)malloc(sizeof(cd) * nzp);
+  if (nz < 1 || nz > nzp || nx > nxp || ny > nyp) return 1;
+  for (int l = 0; l < ntheta; ++l) {
+    const float *a = A + 3 * l;
+    for (int k = 0; k < nzp; ++k) { W[k].re = wavelet[(long)l * nzp + k]; W[k].im = 0.0; }
+    dft1d(W, nzp, -1);
+    float *o = out[l];
+    for (long c = 0; c < rsize; ++c) {
+      float v = 0.0f;
+      v += m[0][c] * a[0];
+      v += m[1][c] * a[1];
+      v += m[2][c] * a[2];
+      o[c] = v;
+    }
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        long t = i + (long)rnxp * j;
+        int k;
+        for (k = 0; k < nz; ++k) imp[k] = o[t + k * plane];
+        float fac = 1.0f / (float)(nzp - nz - 1);
+        for (; k < nzp; ++k) imp[k] = fac * ((float)(k - nz) * imp[0] + (float)(nzp - k - 1) * imp[nz - 1]);
+        for (k = 0; k < nzp; ++k) dif[k] = (k == nzp - 1) ? imp[0] - imp[k] : imp[k + 1] - imp[k];
+        for (k = 0; k < nzp; ++k) { x[k].re = dif[k]; x[k].im = 0.0; }
+        dft1d(x, nzp, -1);
+        for (k = 0; k < cnzp; ++k) {
+          cd r = x[k], w = W[k], sv;
+          sv.re = r.re * w.re + r.im * w.im;
+          sv.im = -r.re * w.im + r.im * w.re;
+          x[k] = sv;
+        }
+        /* Hermitian completion of the half spectrum, as a c2r transform
+         * reads it (imaginary parts of k = 0 and nzp/2 dropped) */
+        x[0].im = 0.0;
+        if (nzp % 2 == 0) x[nzp / 2].im = 0.0;
+        for (k = cnzp; k < nzp; ++k) { x[k].re = x[nzp - k].re; x[k].im = -x[nzp - k].im; }
+        dft1d(x, nzp, +1);
+        for (k = 0; k < nzp; ++k) o[t + k * plane] = (float)(x[k].re / (double)nzp);
+      }
+  }
+  free(imp); free(dif); free(W); free(x);
+  return 0;
+}

@@ -83,6 +83,12 @@ int orc_sim_filter(int nxp, int nyp, int nzp, const float *const *cov,
                    float *const *seed, long long *chol_fail);
 int orc_sim_filter_fp64(int nxp, int nyp, int nzp, const float *const *cov,
                         float *const *seed, long long *chol_fail);
+/* Crava::computeSyntSeismic + computeSeismicImpedance (constant thickness):
+ * m[3] real padded grids, out[ntheta] real padded grids; nx, ny, nz the
+ * unpadded sizes; wavelet [ntheta][nzp], A [ntheta][3]. */
+int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
+                     const float *A, const float *wavelet, const float *const *m,
+                     float *const *out);
 
 /* ---- reference harness (ref_harness.cpp, built into oracle/_ref) ---- */
 int ref_fft_r2c(float *grid, int nxp, int nyp, int nzp, int type);
@@ -105,6 +111,9 @@ unsigned int ref_noise_fill(float *grid, int nxp, int nyp, int nzp,
                             unsigned int seed);
 int ref_sim_filter(int nxp, int nyp, int nzp, const float *const *cov,
                    float *const *seed, long long *chol_fail);
+int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
+                     const float *A, const float *wavelet, const float *const *m,
+                     float *const *out);
 
 #ifdef __cplusplus
 }

@@ -89,6 +89,9 @@ def _load(which: str):
     f = getattr(lib, f"{p}_sim_filter")
     f.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(F32P), C.POINTER(F32P), C.POINTER(C.c_longlong)]
     f.restype = C.c_int
+    f = getattr(lib, f"{p}_synt_seismic")
+    f.argtypes = [C.c_int] * 7 + [F32P, F32P, C.POINTER(F32P), C.POINTER(F32P)]
+    f.restype = C.c_int
     if which == "orc":
         f = lib.orc_posterior_fp64
         f.argtypes = [C.POINTER(Params), C.POINTER(F32P), C.POINTER(F32P), C.POINTER(F32P), F32P,
@@ -254,6 +257,23 @@ def sim_filter(nxp, nyp, nzp, cov, seeds, which="orc", fp64=False):
     rc = fn(nxp, nyp, nzp, _ptrs(cov), _ptrs(sd), C.byref(fails))
     assert rc == 0
     return sd, fails.value
+
+
+def synt_seismic(case, m, nx=None, ny=None, nz=None, which="orc"):
+    """Synthetic seismic of the real padded grids m = (alpha, beta, rho):
+    one real padded grid per angle (Crava::computeSyntSeismic)."""
+    lib = _load(which)
+    nx = case.nxp if nx is None else nx
+    ny = case.nyp if ny is None else ny
+    nz = case.nz if nz is None else nz
+    mm = [np.ascontiguousarray(g, dtype=np.float32) for g in m]
+    out = [np.zeros_like(mm[0]) for _ in range(case.ntheta)]
+    A = np.ascontiguousarray(case.A, dtype=np.float32)
+    wav = np.ascontiguousarray(case.wavelet, dtype=np.float32)
+    rc = getattr(lib, f"{which}_synt_seismic")(case.nxp, case.nyp, case.nzp, nx, ny, nz, case.ntheta,
+                                               _fp(A), _fp(wav), _ptrs(mm), _ptrs(out))
+    assert rc == 0
+    return out
 
 
 def complex_view(g, nxp):

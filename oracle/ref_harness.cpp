@@ -144,6 +144,67 @@ void build_tables(const crava_oracle_params *p, KzTables &t) {
 
 extern "C" {
 
+/* Crava::computeSyntSeismic (src/crava.cpp:1666-1719) with
+ * computeSeismicImpedance (:1632-1663), constant thickness (relThick and
+ * local stretch 1, the local wavelet equal to the global one): the trace
+ * loop with the reference's Wavelet1D operations restated on plain arrays
+ * and the reference's FFTW doing the 1-D transforms. */
+int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int nt,
+                     const float *A, const float *wavelet, const float *const *m,
+                     float *const *out) {
+  const int cnxp = nxp / 2 + 1, rnxp = 2 * cnxp, cnzp = nzp / 2 + 1, rnzp = 2 * cnzp;
+  const long plane = static_cast<long>(rnxp) * nyp, rsize = plane * nzp;
+  if (nz < 1 || nz > nzp || nx > nxp || ny > nyp) return 1;
+  fftw_real *res = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  std::vector<float> imp(nzp);
+  rfftwnd_plan fwd = rfftwnd_create_plan(1, &nzp, FFTW_REAL_TO_COMPLEX, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_plan inv = rfftwnd_create_plan(1, &nzp, FFTW_COMPLEX_TO_REAL, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  for (int l = 0; l < nt; ++l) {
+    std::vector<fftw_complex> W = spectrum1d(wavelet + static_cast<long>(l) * nzp, nzp);
+    float *o = out[l];
+    for (long c = 0; c < rsize; ++c) {  /* computeSeismicImpedance */
+      float v = 0;
+      v += m[0][c] * A[3 * l + 0];
+      v += m[1][c] * A[3 * l + 1];
+      v += m[2][c] * A[3 * l + 2];
+      o[c] = v;
+    }
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        const long t = i + static_cast<long>(rnxp) * j;
+        int k;
+        for (k = 0; k < nz; ++k) imp[k] = o[t + k * plane];
+        float fac = 1.0f / static_cast<float>(nzp - nz - 1);
+        for (; k < nzp; ++k) imp[k] = fac * ((k - nz) * imp[0] + (nzp - k - 1) * imp[nz - 1]);
+        for (k = 0; k < nzp; ++k) res[k] = (k == nzp - 1) ? imp[0] - imp[k] : imp[k + 1] - imp[k];
+        for (; k < rnzp; ++k) res[k] = 0.0f;
+        rfftwnd_one_real_to_complex(fwd, res, reinterpret_cast<fftw_complex *>(res));
+        fftw_complex *rc = reinterpret_cast<fftw_complex *>(res);
+        for (k = 0; k < cnzp; ++k) {
+          fftw_complex r = rc[k], w, sv;
+          /* getCAmp(k, 1.0f): interpolation at omega = k with weight 0 */
+          float omega = float(k) / 1.0f;
+          int omL = int(std::floor(omega)), omU = int(std::floor(omega)) + 1;
+          if (omU >= cnzp) omU -= 1;
+          float dOmega = omega - float(omL);
+          w.re = W[omL].re * (1.0f - dOmega) + W[omU].re * dOmega;
+          w.im = (W[omL].im * (1.0f - dOmega) + W[omU].im * dOmega);
+          w.re /= 1.0f; w.im /= 1.0f;
+          sv.re = r.re * w.re + r.im * w.im;
+          sv.im = -r.re * w.im + r.im * w.re;
+          rc[k] = sv;
+        }
+        rfftwnd_one_complex_to_real(inv, rc, res);
+        double scale = static_cast<double>(1.0 / static_cast<double>(nzp));
+        for (k = 0; k < nzp; ++k) o[t + k * plane] = static_cast<fftw_real>(res[k] * scale);
+      }
+  }
+  fftwnd_destroy_plan(fwd);
+  fftwnd_destroy_plan(inv);
+  fftw_free(res);
+  return 0;
+}
+
 /* FFTGrid::fftInPlace, src/fftgrid.cpp:1803-1829 */
 int ref_fft_r2c(float *grid, int nxp, int nyp, int nzp, int type) {
   long rsize = 2L * (nxp / 2 + 1) * nyp * nzp;

@@ -32,9 +32,38 @@ def make_case(spec):
                            wavelet_scale_range=spec["scale"])
 
 
+# Synthetic seismic: golden case geometry and wavelets, seeded N(0,1)
+# parameter grids, unpadded sizes (nx, ny, nz) exercising the taper and
+# the untouched traces.
+SYNT = {
+    "c3_12x10x16": [(12, 10, 16), (11, 9, 13)],
+    "c2_9x8x20_odd": [(9, 8, 20), (7, 8, 17)],
+    "c5_10x8x24": [(10, 8, 21)],
+}
+
+
+def make_synt():
+    from tests import golden_cases as GC
+
+    out = {}
+    for name, sizes in SYNT.items():
+        case, _ = GC.load(name)
+        rng = np.random.default_rng(7)
+        m = [rng.standard_normal(case.mu[0].shape).astype(np.float32) for _ in range(3)]
+        out[f"{name}_m"] = np.stack(m)
+        for k, (nx, ny, nz) in enumerate(sizes):
+            out[f"{name}_{k}_size"] = np.array([nx, ny, nz])
+            out[f"{name}_{k}_out"] = np.stack(O.synt_seismic(case, m, nx, ny, nz, "ref"))
+    np.savez_compressed(os.path.join(HERE, "synt_seismic.npz"), **out)
+    print("synt_seismic written")
+
+
 def main():
     if not O.have_ref():
         O.build(ref=True)
+    if "--synt-only" in sys.argv:
+        make_synt()
+        return
     for name, spec in CASES.items():
         case = make_case(spec)
         nx, ny, nz = case.nxp, case.nyp, case.nzp
@@ -63,6 +92,7 @@ def main():
     normals, state = O.rng_normal(23665, 256, "ref")
     np.savez_compressed(os.path.join(HERE, "rng_23665.npz"), normals=normals, state=state)
     print("rng written")
+    make_synt()
 
 
 if __name__ == "__main__":
