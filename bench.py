@@ -280,6 +280,44 @@ def run_batch(args, case256, dev, stream, max_over_ranks):
             "kernels_per_run": kern, "tuning": tunings}
 
 
+def run_prior_fill(ctx, case, dst, dev, stream, max_over_ranks):
+    """The six prior covariance grids and the noise correlation grid built on
+    the device (fillInParamCorr x Sigma0, fillInErrCorr) instead of uploaded:
+    device time per set and the HBM rate of its 7 grid writes."""
+    import numpy as np
+    import torch
+
+    from crava_b200 import api, synth
+
+    cxy = synth.corr_xy(case.nxp, case.nyp, 25.0, 25.0, 500.0)
+    circ = synth.circ_corr_t(case.nzp, case.dt, 20.0, case.low_cut)
+    cov, err = dst[2], dst[3]
+
+    def once():
+        ctx.fill_prior_cov(cxy, circ, 0.0, 0.0, cov)
+        ctx.fill_err_corr(cxy, 0.0, 0.0, err)
+
+    for _ in range(3):
+        once()
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    reps = 10
+    ev0.record(stream)
+    for _ in range(reps):
+        once()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / reps)
+    same = all(np.array_equal(g.cpu().numpy()[..., :case.nxp], h[..., :case.nxp])
+               for g, h in zip(cov, case.cov))
+    gbytes = 7 * cov[0].numel() * 4
+    return {"workload": "6 prior covariance grids + noise correlation, %dx%dx%d"
+                        % (case.nxp, case.nyp, case.nzp),
+            "ms_per_set": ms, "GB/s": gbytes / (ms * 1e-3) / 1e9,
+            "equal_to_uploaded_grids": same}
+
+
 def run_forward(ctx, case, src, dev, stream, max_over_ranks):
     """Synthetic seismic (Crava::computeSyntSeismic) of the three parameter
     grids for all angles: device time per call and HBM rate against the
@@ -479,6 +517,8 @@ def run_own(args):
                "grid": [nxp, nyp, nzp]}
         del covf, outs
 
+    prior = run_prior_fill(ctx, case, dst, dev, stream, max_over_ranks)
+
     fwd = None
     if not args.no_forward:
         fwd = run_forward(ctx, case, src, dev, stream, max_over_ranks)
@@ -553,6 +593,7 @@ def run_own(args):
         "batch": batch,
         "adjoint": adjoint,
         "forward_model": fwd,
+        "prior_fill": prior,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,
         "chol_fail_bins": st.chol_fail_bins, "nonfinite_bins": st.nonfinite_bins,

@@ -109,6 +109,10 @@ SYMBOLS = {
                                C.POINTER(C.c_longlong)], C.c_int),
     "crava_gpu_synt_seismic": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                 C.POINTER(C.c_void_p)], C.c_int),
+    "crava_gpu_circ_corr_t": ([F32P, C.c_int, C.c_int, C.c_int, F32P], C.c_int),
+    "crava_gpu_fill_prior_cov": ([C.c_void_p, F32P, F32P, C.c_float, C.c_float, C.POINTER(C.c_void_p)],
+                                 C.c_int),
+    "crava_gpu_fill_err_corr": ([C.c_void_p, F32P, C.c_float, C.c_float, C.c_void_p], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -275,6 +279,23 @@ class Context:
               "loglik_grad")
         return L.value, gs, gv, gw[..., 0] + 1j * gw[..., 1], nf.value
 
+    def fill_prior_cov(self, corr_xy, circ_corr_t, grad_i, grad_j, cov):
+        """The six prior covariance grids (SeismicParametersHolder::
+        initializeCorrelations) written on the device into cov."""
+        cxy = np.ascontiguousarray(corr_xy, dtype=np.float32)
+        cc = np.ascontiguousarray(circ_corr_t, dtype=np.float32)
+        assert cxy.size == self.case.nxp * self.case.nyp and cc.size == self.case.nzp
+        arr = (C.c_void_p * 6)(*[g.data_ptr() for g in cov])
+        check(self.lib.crava_gpu_fill_prior_cov(self.handle, cxy.ctypes.data_as(F32P), cc.ctypes.data_as(F32P),
+                                                grad_i, grad_j, arr), "fill_prior_cov")
+
+    def fill_err_corr(self, corr_xy, grad_i, grad_j, err):
+        """The noise correlation grid (FFTGrid::fillInErrCorr) on the device."""
+        cxy = np.ascontiguousarray(corr_xy, dtype=np.float32)
+        assert cxy.size == self.case.nxp * self.case.nyp
+        check(self.lib.crava_gpu_fill_err_corr(self.handle, cxy.ctypes.data_as(F32P), grad_i, grad_j,
+                                               _ptr(err)), "fill_err_corr")
+
     def synt_seismic(self, alpha, beta, rho, outs, nx=0, ny=0):
         """Synthetic seismic of the real parameter grids into outs (one real
         grid per angle), Crava::computeSyntSeismic."""
@@ -348,6 +369,16 @@ class Context:
         check(self.lib.crava_gpu_set_kz_tables(self.handle, wd.ctypes.data_as(F32P), e1.ctypes.data_as(F32P),
                                                e2.ctypes.data_as(F32P), e3.ctypes.data_as(F32P),
                                                inv.ctypes.data_as(C.POINTER(C.c_int))), "set_kz_tables")
+
+
+def circ_corr_t(prior_corr_t, low_int_cut, nzp):
+    """Circular temporal prior correlation (crava_gpu_circ_corr_t; host
+    computation, no GPU needed)."""
+    pc = np.ascontiguousarray(prior_corr_t, dtype=np.float32)
+    out = np.zeros(nzp, np.float32)
+    check(load_library().crava_gpu_circ_corr_t(pc.ctypes.data_as(F32P), pc.size, low_int_cut, nzp,
+                                               out.ctypes.data_as(F32P)), "circ_corr_t")
+    return out
 
 
 class Batch:

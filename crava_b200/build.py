@@ -30,6 +30,7 @@ SOURCES = {
     "batch.cu": [],
     "loglik.cu": [],
     "forward.cu": [],
+    "prior.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -383,6 +383,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->work);
   cudaFree(c->W);
   cudaFree(c->synt_H);
+  cudaFree(c->prior_buf);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }

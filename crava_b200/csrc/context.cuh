@@ -44,6 +44,8 @@ struct crava_gpu_ctx {
   bool capture = false;
   // synthetic seismic: per-angle spectral filters [ntheta][nzp] (device)
   float2 *synt_H = nullptr;
+  // prior fills: lateral [nyp][nxp] then temporal [nzp] correlation (device)
+  float *prior_buf = nullptr;
 };
 
 namespace crava {

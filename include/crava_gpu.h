@@ -344,6 +344,37 @@ int crava_gpu_loglik_grad(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
 int crava_gpu_synt_seismic(crava_gpu_ctx *ctx, const float *alpha, const float *beta,
                            const float *rho, int nx, int ny, float *const *out);
 
+/* Circular temporal prior correlation on nzp samples:
+ * SeismicParametersHolder::computeCircCorrT + makeCircCorrTPosDef
+ * (src/seismicparametersholder.cpp:430-499): prior_corr_t[0..n) mirrored
+ * onto the cyclic axis, its spectrum replaced by its modulus and zeroed for
+ * k <= low_int_cut, transformed back and normalised to 1 at lag 0.  Host
+ * computation (double-precision transforms), no context, no GPU.  Returns
+ * CRAVA_GPU_ERR_ARG where the reference aborts (value at lag 0 <= 1e-5). */
+int crava_gpu_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
+                          float *circ_corr_t);
+
+/* The six prior covariance grids on the device:
+ * SeismicParametersHolder::initializeCorrelations
+ * (src/seismicparametersholder.cpp:196-221), i.e. FFTGrid::fillInParamCorr
+ * (src/fftgrid.cpp:1118-1164) times float(var0[p][q]) for (p, q) = (0,0),
+ * (1,1), (2,2), (0,1), (0,2), (1,2).  corr_xy: host [nyp][nxp] lateral
+ * correlation (ModelGeneral::findCorrXYGrid, src/modelgeneral.cpp:
+ * 4072-4110, index i + nxp j); circ_corr_t: host [nzp]
+ * (crava_gpu_circ_corr_t); grad_i, grad_j: the correlation direction
+ * gradients.  cov: six device grids, written in the real padded layout
+ * (padding cells RMISSING * var0, as the reference leaves them).  Same
+ * float operations as the reference: bit-identical grids.  Asynchronous
+ * (the host arrays are copied before the call returns). */
+int crava_gpu_fill_prior_cov(crava_gpu_ctx *ctx, const float *corr_xy, const float *circ_corr_t,
+                             float grad_i, float grad_j, float *const cov[6]);
+
+/* The noise correlation grid errCorr on the device: FFTGrid::fillInErrCorr
+ * (src/fftgrid.cpp:1064-1116), corr_xy as above.  Bit-identical to the
+ * reference's grid.  Asynchronous. */
+int crava_gpu_fill_err_corr(crava_gpu_ctx *ctx, const float *corr_xy, float grad_i, float grad_j,
+                            float *err_corr);
+
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
 

@@ -882,3 +882,101 @@ int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int nthe
   free(imp); free(dif); free(W); free(x);
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Prior and noise correlation grids.                                   */
+/* computeCircCorrT + makeCircCorrTPosDef                               */
+/* (src/seismicparametersholder.cpp:430-499); transforms in double.     */
+/* ------------------------------------------------------------------ */
+int orc_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
+                    float *circ_corr_t) {
+  int cn = nzp / 2 + 1;
+  cd *x = (cd *)malloc(sizeof(cd) * nzp);
+  if (!prior_corr_t || n < 1 || prior_corr_t[0] == 0.0f) { free(x); return 1; }
+  for (int k = 0; k < nzp; ++k) {
+    int refk = k < cn ? k : nzp - k;
+    x[k].re = refk < n ? prior_corr_t[refk] : 0.0;
+    x[k].im = 0.0;
+  }
+  dft1d(x, nzp, -1);
+  for (int k = 0; k < cn; ++k) {
+    double m = k <= low_int_cut ? 0.0 : (double)(float)sqrt(x[k].re * x[k].re + x[k].im * x[k].im);
+    x[k].re = m; x[k].im = 0.0;
+  }
+  for (int k = cn; k < nzp; ++k) x[k] = x[nzp - k];
+  dft1d(x, nzp, +1);
+  if (!((float)x[0].re > 1.e-5f)) { free(x); return 1; }
+  float scale = 1.0f / (float)x[0].re;
+  for (int k = 0; k < nzp; ++k) circ_corr_t[k] = (float)x[k].re * scale;
+  free(x);
+  return 0;
+}
+
+/* cycleI / cycleJ of src/fftgrid.cpp:1082-1087 and :1130-1135 */
+static int cyc(int i, int n) {
+  int c = i - n;
+  if (i < -c) c = i;
+  return c;
+}
+
+/* FFTGrid::fillInParamCorr (src/fftgrid.cpp:1118-1164), then
+ * multiplyByScalar(float(var0_pq)) over every cell (:1992-2000) as
+ * SeismicParametersHolder::initializeCorrelations does (:196-221). */
+int orc_fill_prior_cov(int nxp, int nyp, int nzp, const float *corr_xy,
+                       const float *circ, float gradI, float gradJ,
+                       const double *var0, float *const *cov) {
+  int rnxp = 2 * (nxp / 2 + 1);
+  const int pq[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+  long idx = 0;
+  for (int k = 0; k < nzp; ++k)
+    for (int j = 0; j < nyp; ++j)
+      for (int i = 0; i < rnxp; ++i, ++idx) {
+        float value;
+        if (i < nxp) {
+          int cycleI = cyc(i, nxp), cycleJ = cyc(j, nyp);
+          float subK = k + cycleI * gradI + cycleJ * gradJ;
+          int baseK = (int)floorf(subK);
+          subK -= baseK;
+          while (baseK < 0) baseK += nzp;
+          while (baseK >= nzp) baseK -= nzp;
+          value = (1 - subK) * circ[baseK];
+          if (baseK != nzp - 1) value += subK * circ[baseK + 1];
+          else value += subK * circ[0];
+          value *= corr_xy[i + nxp * j];
+        } else {
+          value = -99999.0f; /* RMISSING */
+        }
+        for (int t = 0; t < 6; ++t) cov[t][idx] = value * (float)var0[3 * pq[t][0] + pq[t][1]];
+      }
+  return 0;
+}
+
+/* FFTGrid::fillInErrCorr (src/fftgrid.cpp:1064-1116). */
+int orc_fill_err_corr(int nxp, int nyp, int nzp, const float *corr_xy,
+                      float gradI, float gradJ, float *err) {
+  int rnxp = 2 * (nxp / 2 + 1), range = 1;
+  long idx = 0;
+  for (int k = 0; k < nzp; ++k)
+    for (int j = 0; j < nyp; ++j)
+      for (int i = 0; i < rnxp; ++i, ++idx) {
+        int cycleI = cyc(i, nxp), cycleJ = cyc(j, nyp);
+        float subK = k + cycleI * gradI + cycleJ * gradJ;
+        float value;
+        if (i < nxp) {
+          if (fabsf(subK) < range * 1.0f || fabsf(subK - nzp) < range * 1.0f) {
+            int baseK = (int)subK;
+            subK -= baseK;
+            while (baseK < -range) baseK += nzp;
+            while (baseK >= range) baseK -= nzp;
+            if (baseK < 0) { baseK = -1 - baseK; subK = 1 - subK; }
+            value = (1 - subK) * corr_xy[i + nxp * j];
+          } else {
+            value = 0;
+          }
+        } else {
+          value = -99999.0f;
+        }
+        err[idx] = value;
+      }
+  return 0;
+}

@@ -86,6 +86,16 @@ int orc_sim_filter_fp64(int nxp, int nyp, int nzp, const float *const *cov,
 /* Crava::computeSyntSeismic + computeSeismicImpedance (constant thickness):
  * m[3] real padded grids, out[ntheta] real padded grids; nx, ny, nz the
  * unpadded sizes; wavelet [ntheta][nzp], A [ntheta][3]. */
+/* computeCircCorrT + makeCircCorrTPosDef (circ_corr_t [nzp]). */
+int orc_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
+                    float *circ_corr_t);
+/* fillInParamCorr times var0 (six grids) and fillInErrCorr (one grid);
+ * corr_xy [nyp][nxp], var0 [3][3]. */
+int orc_fill_prior_cov(int nxp, int nyp, int nzp, const float *corr_xy,
+                       const float *circ_corr_t, float grad_i, float grad_j,
+                       const double *var0, float *const *cov);
+int orc_fill_err_corr(int nxp, int nyp, int nzp, const float *corr_xy,
+                      float grad_i, float grad_j, float *err_corr);
 int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
                      const float *A, const float *wavelet, const float *const *m,
                      float *const *out);
@@ -111,6 +121,8 @@ unsigned int ref_noise_fill(float *grid, int nxp, int nyp, int nzp,
                             unsigned int seed);
 int ref_sim_filter(int nxp, int nyp, int nzp, const float *const *cov,
                    float *const *seed, long long *chol_fail);
+int ref_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
+                    float *circ_corr_t);
 int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
                      const float *A, const float *wavelet, const float *const *m,
                      float *const *out);

@@ -89,6 +89,16 @@ def _load(which: str):
     f = getattr(lib, f"{p}_sim_filter")
     f.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(F32P), C.POINTER(F32P), C.POINTER(C.c_longlong)]
     f.restype = C.c_int
+    f = getattr(lib, f"{p}_circ_corr_t")
+    f.argtypes = [F32P, C.c_int, C.c_int, C.c_int, F32P]
+    f.restype = C.c_int
+    if which == "orc":
+        f = lib.orc_fill_prior_cov
+        f.argtypes = [C.c_int, C.c_int, C.c_int, F32P, F32P, C.c_float, C.c_float, F64P, C.POINTER(F32P)]
+        f.restype = C.c_int
+        f = lib.orc_fill_err_corr
+        f.argtypes = [C.c_int, C.c_int, C.c_int, F32P, C.c_float, C.c_float, F32P]
+        f.restype = C.c_int
     f = getattr(lib, f"{p}_synt_seismic")
     f.argtypes = [C.c_int] * 7 + [F32P, F32P, C.POINTER(F32P), C.POINTER(F32P)]
     f.restype = C.c_int
@@ -273,6 +283,37 @@ def synt_seismic(case, m, nx=None, ny=None, nz=None, which="orc"):
     rc = getattr(lib, f"{which}_synt_seismic")(case.nxp, case.nyp, case.nzp, nx, ny, nz, case.ntheta,
                                                _fp(A), _fp(wav), _ptrs(mm), _ptrs(out))
     assert rc == 0
+    return out
+
+
+def circ_corr_t(prior_corr_t, low_int_cut, nzp, which="orc"):
+    """computeCircCorrT + makeCircCorrTPosDef."""
+    lib = _load(which)
+    pc = np.ascontiguousarray(prior_corr_t, dtype=np.float32)
+    out = np.zeros(nzp, np.float32)
+    rc = getattr(lib, f"{which}_circ_corr_t")(_fp(pc), pc.size, low_int_cut, nzp, _fp(out))
+    assert rc == 0
+    return out
+
+
+def fill_prior_cov(nxp, nyp, nzp, corr_xy, circ, grad_i, grad_j, var0):
+    """fillInParamCorr x var0 for the six covariance grids (restatement)."""
+    lib = _load("orc")
+    cxy = np.ascontiguousarray(corr_xy, dtype=np.float32)
+    cc = np.ascontiguousarray(circ, dtype=np.float32)
+    v0 = np.ascontiguousarray(var0, dtype=np.float64)
+    out = [np.zeros((nzp, nyp, 2 * (nxp // 2 + 1)), np.float32) for _ in range(6)]
+    assert lib.orc_fill_prior_cov(nxp, nyp, nzp, _fp(cxy), _fp(cc), grad_i, grad_j, _dp(v0),
+                                  _ptrs(out)) == 0
+    return out
+
+
+def fill_err_corr(nxp, nyp, nzp, corr_xy, grad_i, grad_j):
+    """fillInErrCorr (restatement)."""
+    lib = _load("orc")
+    cxy = np.ascontiguousarray(corr_xy, dtype=np.float32)
+    out = np.zeros((nzp, nyp, 2 * (nxp // 2 + 1)), np.float32)
+    assert lib.orc_fill_err_corr(nxp, nyp, nzp, _fp(cxy), grad_i, grad_j, _fp(out)) == 0
     return out
 
 

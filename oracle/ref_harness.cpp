@@ -144,6 +144,45 @@ void build_tables(const crava_oracle_params *p, KzTables &t) {
 
 extern "C" {
 
+/* SeismicParametersHolder::computeCircCorrT + makeCircCorrTPosDef
+ * (src/seismicparametersholder.cpp:430-499) with FFTGrid::fft1DzInPlace /
+ * invFFT1DzInPlace (src/fftgrid.cpp:2002-2037): the reference's FFTW. */
+int ref_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
+                    float *circ_corr_t) {
+  if (!prior_corr_t || n < 1 || prior_corr_t[0] == 0.0f) return 1;
+  const int cn = nzp / 2 + 1;
+  fftw_real *c = static_cast<fftw_real *>(fftw_malloc(2 * cn * sizeof(fftw_real)));
+  for (int k = 0; k < 2 * cn; ++k) {
+    if (k < nzp) {
+      int refk = k < cn ? k : nzp - k;
+      c[k] = refk < n ? prior_corr_t[refk] : 0.0f;
+    } else {
+      c[k] = -99999.0f;
+    }
+  }
+  rfftwnd_plan fwd = rfftwnd_create_plan(1, &nzp, FFTW_REAL_TO_COMPLEX, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_one_real_to_complex(fwd, c, reinterpret_cast<fftw_complex *>(c));
+  fftwnd_destroy_plan(fwd);
+  fftw_complex *f = reinterpret_cast<fftw_complex *>(c);
+  for (int k = 0; k < cn; ++k) {
+    if (k <= low_int_cut) f[k].re = 0.0;
+    else f[k].re = float(std::sqrt(f[k].re * f[k].re + f[k].im * f[k].im));
+    f[k].im = 0.0;
+  }
+  rfftwnd_plan inv = rfftwnd_create_plan(1, &nzp, FFTW_COMPLEX_TO_REAL, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_one_complex_to_real(inv, f, c);
+  fftwnd_destroy_plan(inv);
+  int rc = 0;
+  if (c[0] > 1.e-5f) {
+    float scale = float(1.0f / c[0]);
+    for (int k = 0; k < nzp; ++k) circ_corr_t[k] = c[k] * scale;
+  } else {
+    rc = 1;
+  }
+  fftw_free(c);
+  return rc;
+}
+
 /* Crava::computeSyntSeismic (src/crava.cpp:1666-1719) with
  * computeSeismicImpedance (:1632-1663), constant thickness (relThick and
  * local stretch 1, the local wavelet equal to the global one): the trace

@@ -121,3 +121,40 @@ def test_synt_seismic_vs_golden():
             for a, b in zip(out, z[f"{name}_{k}_out"]):
                 assert rel(a, b) < 1e-6, (name, k)
             k += 1
+
+
+def _corr_t(nzp, dt=4.0, t_range=20.0):
+    i = np.arange(nzp // 2 + 2)
+    return np.exp(-3.0 * (dt * i / t_range) ** 2).astype(np.float32)
+
+
+@pytest.mark.parametrize("nzp,low_int_cut", [(32, 0), (128, 2), (300, 6), (512, 10)])
+def test_circ_corr_t_restatement_and_library(nzp, low_int_cut):
+    """computeCircCorrT + makeCircCorrTPosDef: the restatement and the
+    library's host routine agree with each other and, when it is built,
+    with the reference's FFTW version to float rounding."""
+    from crava_b200 import api
+
+    ct = _corr_t(nzp)
+    a = O.circ_corr_t(ct, low_int_cut, nzp, "orc")
+    b = api.circ_corr_t(ct, low_int_cut, nzp)
+    assert np.abs(a - b).max() <= 2e-7
+    if O.have_ref():
+        r = O.circ_corr_t(ct, low_int_cut, nzp, "ref")
+        assert np.abs(a - r).max() <= 1e-6
+
+
+def test_prior_fills_match_synthetic_cases():
+    """fillInParamCorr x var0 and fillInErrCorr restated equal the grids
+    the seeded cases carry (same float operations) on every real cell."""
+    from crava_b200 import synth
+
+    for shape in [(16, 12, 32), (15, 16, 20)]:
+        nx, ny, nz = shape
+        case = synth.make_case(nx, ny, nz, (10.0,), 0.1, seed=1)
+        cxy = synth.corr_xy(nx, ny, 25.0, 25.0, 500.0)
+        circ = synth.circ_corr_t(nz, 4.0, 20.0, 5.0)
+        cov = O.fill_prior_cov(nx, ny, nz, cxy, circ, 0.0, 0.0, case.var0)
+        for g, h in zip(cov, case.cov):
+            assert np.array_equal(bits(g[..., :nx]), bits(h[..., :nx]))
+        assert np.array_equal(bits(O.fill_err_corr(nx, ny, nz, cxy, 0.0, 0.0)), bits(case.err_corr))
