@@ -113,6 +113,9 @@ SYMBOLS = {
     "crava_gpu_fill_prior_cov": ([C.c_void_p, F32P, F32P, C.c_float, C.c_float, C.POINTER(C.c_void_p)],
                                  C.c_int),
     "crava_gpu_fill_err_corr": ([C.c_void_p, F32P, C.c_float, C.c_float, C.c_void_p], C.c_int),
+    "crava_gpu_posterior_unit_host_async": ([C.c_void_p, C.POINTER(Grids), C.POINTER(Grids), C.c_int],
+                                            C.c_int),
+    "crava_gpu_host_wait": ([C.c_void_p], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -326,6 +329,17 @@ class Context:
         g = self.grids(mu, data, cov, err)
         p = self.precision if precision is None else precision
         check(self.lib.crava_gpu_posterior_unit_host(self.handle, C.byref(g), p), "posterior_unit_host")
+
+    def posterior_unit_host_async(self, src, dst, precision=None):
+        """src, dst: (mu, data, cov, err) tuples of host tensors (pinned);
+        returns once enqueued; call host_wait() before touching them."""
+        gi, go = self.grids(*src), self.grids(*dst)
+        p = self.precision if precision is None else precision
+        check(self.lib.crava_gpu_posterior_unit_host_async(self.handle, C.byref(gi), C.byref(go), p),
+              "posterior_unit_host_async")
+
+    def host_wait(self):
+        check(self.lib.crava_gpu_host_wait(self.handle), "host_wait")
 
     def noise_fill(self, grid, seed, stream_id):
         check(self.lib.crava_gpu_noise_fill(self.handle, _ptr(grid), seed, stream_id), "noise_fill")

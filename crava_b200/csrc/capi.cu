@@ -368,6 +368,7 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
   if ((rc = kz_tables_build(c->p, &c->tables, c->stream))) return fail(rc);
+  if ((rc = kz_order_build(nzp, &c->tables, c->stream))) return fail(rc);
   *out = c;
   return CRAVA_GPU_OK;
 }
@@ -377,6 +378,8 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   DeviceGuard guard(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   else cudaDeviceSynchronize();
+  if (c->s_out) cudaStreamSynchronize(c->s_out);
+  if (c->s_in) cudaStreamSynchronize(c->s_in);
   fft_plans_destroy(&c->plans);
   kz_tables_free(&c->tables);
   cudaFree(c->counters);
@@ -386,6 +389,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->prior_buf);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
+  for (auto &e : c->slot_done) if (e) cudaEventDestroy(e);
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto &e : c->pool) cudaEventDestroy(e);
   if (c->s_in) cudaStreamDestroy(c->s_in);
@@ -494,30 +498,55 @@ int crava_gpu_host_unregister(void *ptr) {
   return CRAVA_GPU_OK;
 }
 
-int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, int precision) {
-  int rc;
-  if ((rc = check_ctx(c)) || (rc = check_grids(c, hg))) return rc;
-  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
-  DeviceGuard guard(c->device);
-  const int nt = c->p.ntheta, ngrid = 10 + nt;
+}  // extern "C"
+
+namespace crava {
+
+// Device work grids for the host-buffer path: `slots` sets of (10 + nt)
+// grids, copy streams and events (reallocated when more slots are needed).
+static int ensure_host_work(crava_gpu_ctx *c, int slots) {
+  const int ngrid = 10 + c->p.ntheta;
   const size_t gbytes = (size_t)c->g.rsize * sizeof(float);
-  if (!c->work) {
-    if (cudaMalloc(&c->work, gbytes * ngrid) != cudaSuccess) { c->work = nullptr; return CRAVA_GPU_ERR_ALLOC; }
+  if (c->work_slots < slots) {
+    if (c->work) {
+      CRAVA_CUDA_TRY(cudaDeviceSynchronize());
+      cudaFree(c->work);
+      c->work = nullptr;
+      c->work_slots = 0;
+    }
+    if (cudaMalloc(&c->work, gbytes * ngrid * slots) != cudaSuccess) { c->work = nullptr; return CRAVA_GPU_ERR_ALLOC; }
+    c->work_slots = slots;
+  }
+  if (!c->s_in) {
     CRAVA_CUDA_TRY(cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
     CRAVA_CUDA_TRY(cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
     c->grid_ev.assign(2 * ngrid + 1, nullptr);
     for (auto &e : c->grid_ev) CRAVA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : c->slot_done) CRAVA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
-  // device grids, in ABI order: mu(3), data(nt), cov(6), err
+  return CRAVA_GPU_OK;
+}
+
+// One host-buffer unit on work slot `slot`: uploads `in` (each grid's
+// copy overlapping the transforms of those before it), solves, and
+// downloads the outputs into `out` (each grid as soon as its inverse
+// transform is done).  Stream-ordered, returns once enqueued.
+static int enqueue_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hin, const crava_gpu_grids *hout,
+                             int precision, int slot, bool order_after_compute) {
+  int rc;
+  const int nt = c->p.ntheta, ngrid = 10 + nt;
+  const size_t gbytes = (size_t)c->g.rsize * sizeof(float);
   crava_gpu_grids dg{};
-  std::vector<float *> host(ngrid), dev(ngrid);
+  std::vector<const float *> hsrc(ngrid);
+  std::vector<float *> hdst(ngrid), dev(ngrid);
   std::vector<int> type(ngrid);
   int i = 0;
-  for (int q = 0; q < 3; ++q, ++i) { host[i] = hg->mu[q]; type[i] = CRAVA_GRID_PARAMETER; }
-  for (int l = 0; l < nt; ++l, ++i) { host[i] = hg->data[l]; type[i] = CRAVA_GRID_DATA; }
-  for (int t = 0; t < 6; ++t, ++i) { host[i] = hg->cov[t]; type[i] = CRAVA_GRID_COVARIANCE; }
-  host[i] = hg->err_corr; type[i] = CRAVA_GRID_COVARIANCE;
-  for (int k = 0; k < ngrid; ++k) dev[k] = c->work + (size_t)k * c->g.rsize;
+  for (int q = 0; q < 3; ++q, ++i) { hsrc[i] = hin->mu[q]; hdst[i] = hout->mu[q]; type[i] = CRAVA_GRID_PARAMETER; }
+  for (int l = 0; l < nt; ++l, ++i) { hsrc[i] = hin->data[l]; hdst[i] = hout->data[l]; type[i] = CRAVA_GRID_DATA; }
+  for (int t = 0; t < 6; ++t, ++i) { hsrc[i] = hin->cov[t]; hdst[i] = hout->cov[t]; type[i] = CRAVA_GRID_COVARIANCE; }
+  hsrc[i] = hin->err_corr; hdst[i] = hout->err_corr; type[i] = CRAVA_GRID_COVARIANCE;
+  float *base = c->work + (size_t)slot * ngrid * c->g.rsize;
+  for (int k = 0; k < ngrid; ++k) dev[k] = base + (size_t)k * c->g.rsize;
   i = 0;
   for (int q = 0; q < 3; ++q) dg.mu[q] = dev[i++];
   for (int l = 0; l < nt; ++l) dg.data[l] = dev[i++];
@@ -527,14 +556,19 @@ int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, i
   const cudaStream_t s = c->stream;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  // the copy stream must not overtake earlier work on the compute stream
-  CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[2 * ngrid], s));
-  CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->grid_ev[2 * ngrid], 0));
+  if (order_after_compute) {
+    // the copy stream must not overtake earlier work on the compute stream
+    CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[2 * ngrid], s));
+    CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->grid_ev[2 * ngrid], 0));
+  }
+  // the slot's grids are free once the step that used them last has
+  // downloaded its outputs
+  CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->slot_done[slot], 0));
   const bool fused = use_fused(c, precision);
   if (fused && (rc = ensure_workspace(c))) return rc;
   const double gb = (double)c->g.csize * 8.0, wb = (double)c->uplan.wgrid * 8.0;
   for (int k = 0; k < ngrid; ++k) {
-    CRAVA_CUDA_TRY(cudaMemcpyAsync(dev[k], host[k], gbytes, cudaMemcpyHostToDevice, c->s_in));
+    CRAVA_CUDA_TRY(cudaMemcpyAsync(dev[k], hsrc[k], gbytes, cudaMemcpyHostToDevice, c->s_in));
     CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[k], c->s_in));
     CRAVA_CUDA_TRY(cudaStreamWaitEvent(s, c->grid_ev[k], 0));
     if (fused) {
@@ -568,12 +602,50 @@ int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, i
     }
     CRAVA_CUDA_TRY(cudaEventRecord(c->grid_ev[ngrid + k], s));
     CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_out, c->grid_ev[ngrid + k], 0));
-    CRAVA_CUDA_TRY(cudaMemcpyAsync(host[k], dev[k], gbytes, cudaMemcpyDeviceToHost, c->s_out));
+    CRAVA_CUDA_TRY(cudaMemcpyAsync(hdst[k], dev[k], gbytes, cudaMemcpyDeviceToHost, c->s_out));
   }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  CRAVA_CUDA_TRY(cudaEventRecord(c->slot_done[slot], c->s_out));
   c->timed = true;
+  return CRAVA_GPU_OK;
+}
+
+}  // namespace crava
+
+extern "C" {
+
+int crava_gpu_posterior_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hg, int precision) {
+  int rc;
+  if ((rc = check_ctx(c)) || (rc = check_grids(c, hg))) return rc;
+  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  if ((rc = ensure_host_work(c, 1))) return rc;
+  if ((rc = enqueue_unit_host(c, hg, hg, precision, 0, true))) return rc;
   CRAVA_CUDA_TRY(cudaStreamSynchronize(c->s_out));
-  CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_posterior_unit_host_async(crava_gpu_ctx *c, const crava_gpu_grids *hin,
+                                        const crava_gpu_grids *hout, int precision) {
+  int rc;
+  if ((rc = check_ctx(c)) || (rc = check_grids(c, hin)) || (rc = check_grids(c, hout))) return rc;
+  if (!valid_precision(precision)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  if ((rc = ensure_host_work(c, 2))) return rc;
+  const int slot = (int)(c->host_seq & 1);
+  if ((rc = enqueue_unit_host(c, hin, hout, precision, slot, c->host_seq == 0))) return rc;
+  ++c->host_seq;
+  return CRAVA_GPU_OK;
+}
+
+int crava_gpu_host_wait(crava_gpu_ctx *c) {
+  if (check_ctx(c)) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  if (c->s_out) CRAVA_CUDA_TRY(cudaStreamSynchronize(c->s_out));
+  if (c->s_in) CRAVA_CUDA_TRY(cudaStreamSynchronize(c->s_in));
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->host_seq = 0;
   return CRAVA_GPU_OK;
 }
 
@@ -669,7 +741,7 @@ int crava_gpu_set_kz_tables(crava_gpu_ctx *c, const float *wd, const float *e1, 
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e2, e2, n * sizeof(float2), cudaMemcpyHostToDevice));
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e3, e3, n * sizeof(float), cudaMemcpyHostToDevice));
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.inv, inv, (size_t)c->p.nzp * sizeof(int), cudaMemcpyHostToDevice));
-  return CRAVA_GPU_OK;
+  return kz_order_build(c->p.nzp, &c->tables, c->stream);
 }
 
 }  // extern "C"

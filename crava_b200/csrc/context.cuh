@@ -36,9 +36,12 @@ struct crava_gpu_ctx {
   double prof_bytes[16] = {};
   long long prof_n[16] = {};
   // host-buffer path
-  float *work = nullptr;  // (10 + ntheta) grids
+  float *work = nullptr;  // (10 + ntheta) grids per slot, 1 or 2 slots
+  int work_slots = 0;
   cudaStream_t s_in = nullptr, s_out = nullptr;
   std::vector<cudaEvent_t> grid_ev;
+  cudaEvent_t slot_done[2] = {};  // last download of a slot's step
+  long long host_seq = 0;          // asynchronous host steps enqueued
   // set while a batch captures this context's work into a CUDA graph: the
   // stage-timing events are not recorded (they would become graph nodes)
   bool capture = false;

@@ -20,6 +20,8 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <vector>
+
 #include "solve.cuh"
 #include "solve_bin.cuh"
 
@@ -117,23 +119,39 @@ struct SolveArgs {
   SolveGrids g;
   KzTables t;
   long long csize, plane;
+  long long bpp;  // blocks per kz plane
   DevCounters *counters;
 };
 
+// Block b works on plane order[b / bpp] (bpp blocks per kz plane), so
+// every block sees one band flag.  Band-gated bins read and write only the
+// six covariance spectra: the solve runs in place, and their mean and data
+// spectra stay as they are.
 template <int NT, int PREC, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= a.csize) return;
-  const int k = (int)(idx / a.plane);
-  float2 mu[3], d[NT], c6[6];
+  const int slot = (int)(blockIdx.x / a.bpp);
+  const long long off = (long long)(blockIdx.x % a.bpp) * blockDim.x + threadIdx.x;
+  if (off >= a.plane) return;
+  const int k = a.t.order ? a.t.order[slot] : slot;
+  const long long idx = (long long)k * a.plane + off;
+  const bool inv = a.t.inv[k] != 0;
+  float2 c6[6];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
+  if (!inv) {
+    sb::prior_only<PREC>(a.c, c6);
+    bool nonfinite = false;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
+    if (a.counters) sb::count(a.counters, false, nonfinite);
+    return;
+  }
+  float2 mu[3], d[NT];
 #pragma unroll
   for (int q = 0; q < 3; ++q) mu[q] = a.g.mu[q][idx];
 #pragma unroll
   for (int l = 0; l < NT; ++l) d[l] = a.g.data[l][idx];
-#pragma unroll
-  for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
   const float2 ec = a.g.err[idx];
-  const bool inv = a.t.inv[k] != 0;
   const long long o = (long long)k * NT;
   bool fail = sb::solve_bin<NT, PREC>(a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
                                       mu, d, c6, ec);
@@ -149,7 +167,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
 
 template <int PREC, int MINB>
 int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
-  dim3 grd((unsigned)((a.csize + kThreads - 1) / kThreads));
+  dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
   switch (nt) {
     case 1: k_solve<1, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
     case 2: k_solve<2, PREC, MINB><<<grd, kThreads, 0, s>>>(a); break;
@@ -200,7 +218,28 @@ int kz_tables_alloc(int nzp, int nt, KzTables *t) {
 
 void kz_tables_free(KzTables *t) {
   cudaFree(t->wd); cudaFree(t->e1); cudaFree(t->e2); cudaFree(t->e3); cudaFree(t->inv);
+  cudaFree(t->order);
   *t = KzTables{};
+}
+
+int kz_order_build(int nzp, KzTables *t, cudaStream_t s) {
+  std::vector<int> inv(nzp), order;
+  CRAVA_CUDA_TRY(cudaMemcpyAsync(inv.data(), t->inv, sizeof(int) * nzp, cudaMemcpyDeviceToHost, s));
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<int> heavy, light;
+  for (int k = 0; k < nzp; ++k) (inv[k] ? heavy : light).push_back(k);
+  const long long nh = (long long)heavy.size();
+  size_t ih = 0, il = 0;
+  for (long long i = 0; i < nzp; ++i) {
+    // Bresenham: the i-th slot takes a heavy plane when the heavy share so
+    // far falls behind nh / nzp
+    const bool take_heavy = ih < heavy.size() && ((long long)ih * nzp < (i + 1) * nh || il == light.size());
+    order.push_back(take_heavy ? heavy[ih++] : light[il++]);
+  }
+  if (!t->order) CRAVA_CUDA_TRY(cudaMalloc(&t->order, sizeof(int) * nzp));
+  CRAVA_CUDA_TRY(cudaMemcpyAsync(t->order, order.data(), sizeof(int) * nzp, cudaMemcpyHostToDevice, s));
+  CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+  return CRAVA_GPU_OK;
 }
 
 int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s) {
@@ -249,6 +288,7 @@ int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g
   if (precision == CRAVA_SOLVE_FP32) return posterior_solve_fp32ref(c, t, g, csize, plane, counters, s);
   SolveArgs a;
   a.c = c; a.g = g; a.t = t; a.csize = csize; a.plane = plane; a.counters = counters;
+  a.bpp = (plane + kThreads - 1) / kThreads;
   if (precision == CRAVA_SOLVE_FP64) return launch_solve<0>(a, c.nt, s);
   if (precision == CRAVA_SOLVE_MIXED) return launch_solve<1>(a, c.nt, s);
   return CRAVA_GPU_ERR_ARG;

@@ -12,6 +12,8 @@ struct KzTables {
   float2 *e2 = nullptr;  // [nzp][nt]  errMult2
   float *e3 = nullptr;   // [nzp][nt]  errMult3
   int *inv = nullptr;    // [nzp]      invert_frequency
+  int *order = nullptr;  // [nzp]      plane visiting order of the solve
+                         //            (null: natural order)
 };
 
 // Constants of the solve, passed by value (kernel parameter space).
@@ -36,6 +38,10 @@ struct DevCounters {
 };
 
 int kz_tables_alloc(int nzp, int nt, KzTables *t);
+// Fills t->order from t->inv (synchronises s): inverted (compute-heavy)
+// and band-gated (memory-only) planes interleaved evenly, so the solve's
+// blocks keep both the FP64 pipes and HBM busy.
+int kz_order_build(int nzp, KzTables *t, cudaStream_t s);
 void kz_tables_free(KzTables *t);
 // Builds the tables from the wavelets on the device (params: host struct).
 int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s);

@@ -462,6 +462,23 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
   return false;
 }
 
+// A band-gated bin: only the prior covariance is written (mu and the data
+// stay as they are), in the arithmetic of the PREC form.
+template <int PREC>
+__device__ __forceinline__ void prior_only(const SolveConsts &c, float2 c6[6]) {
+  if (PREC == 0) {
+    const Sym3d S = prior_d(c6, c.var0);
+    const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
+  } else {
+    float sf[6];
+    prior_f(c6, c.var0, sf);
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c6[t] = make_float2(sf[t], 0.f);
+  }
+}
+
 // One bin.  In: mu[3], d[NT], c6[6] (the six prior spectra), ec (noise
 // correlation spectrum), the bin's kz tables and its band flag.  Out (in
 // place): mu <- posterior mean, d <- residual, c6 <- posterior covariance

@@ -145,6 +145,20 @@ int crava_gpu_posterior_unit_oop(crava_gpu_ctx *ctx, const crava_gpu_grids *in,
 int crava_gpu_posterior_unit_host(crava_gpu_ctx *ctx,
                                   const crava_gpu_grids *host_grids,
                                   int precision);
+
+/* The host-buffer unit, asynchronous and two deep: uploads `in`, runs the
+ * unit and downloads its outputs into `out` (out == in: in place, as
+ * crava_gpu_posterior_unit_host), returning once the work is enqueued.
+ * Consecutive calls alternate between two device work sets, so one call's
+ * downloads overlap the next call's uploads (PCIe is full duplex).  The
+ * host grids of a call must stay untouched until crava_gpu_host_wait
+ * returns, and the `out` grids of calls in flight must be distinct; pin
+ * them (crava_gpu_host_register) for asynchronous copies.  No counterpart
+ * in the reference. */
+int crava_gpu_posterior_unit_host_async(crava_gpu_ctx *ctx, const crava_gpu_grids *in,
+                                        const crava_gpu_grids *out, int precision);
+/* Waits for every asynchronous host-buffer unit of the context. */
+int crava_gpu_host_wait(crava_gpu_ctx *ctx);
 int crava_gpu_host_register(void *ptr, uint64_t bytes);
 int crava_gpu_host_unregister(void *ptr);
 
