@@ -407,6 +407,11 @@ __device__ __forceinline__ int stockham_ct(float2 *a, float2 *b, const float2 *t
 
 namespace crava {
 
+// Element pitch (float2) of a TX-line in-place column buffer.  (A pitch of
+// 9 for 8 lines removes the first stage's write conflicts but adds
+// conflicts to every load and measured 20 % slower at 512 points.)
+__host__ __device__ constexpr int cols_pitch(int tx) { return tx; }
+
 // In-place compile-time Stockham: each stage first reads every butterfly
 // input of this thread into registers, synchronises, then writes the
 // outputs into the same buffer.  Halves the shared memory of the

@@ -71,10 +71,11 @@ __device__ __forceinline__ bool cholesky(T2 *L, T *rd) {
 #pragma unroll
     for (int k = 0; k < i; ++k) d -= L[tri(i, k)].x * L[tri(i, k)].x + L[tri(i, k)].y * L[tri(i, k)].y;
     if (!(d > tol)) return false;
-    const T sq = sqrt(d);
-    L[tri(i, i)].x = sq;
+    // one reciprocal square root gives both the pivot and its reciprocal
+    const T r = rsqrt(d);
+    L[tri(i, i)].x = d * r;
     L[tri(i, i)].y = T(0);
-    rd[i] = T(1) / sq;
+    rd[i] = r;
   }
   return true;
 }
