@@ -332,18 +332,20 @@ __global__ void __launch_bounds__(kThreads) k_cols_ip(const __grid_constant__ Co
   float2 *base = a.data + (long long)blockIdx.y * a.outer_stride + x0;
   const int tid = threadIdx.x;
   constexpr int ES = cols_pitch(TX);
+  constexpr int PADR = cols_padr(N, TX);
   for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
   for (int idx = tid; idx < TX * N; idx += kThreads) {
     const int t = idx % TX, m = idx / TX;
-    if (t < nx) cp_async8(buf + m * ES + t, base + m * a.elem_stride + t);
-    else buf[m * ES + t] = make_float2(0.f, 0.f);
+    float2 *dst = buf + pad_row<PADR>(m) * ES + t;
+    if (t < nx) cp_async8(dst, base + m * a.elem_stride + t);
+    else *dst = make_float2(0.f, 0.f);
   }
   cp_async_wait_all();
   __syncthreads();
-  stockham_ip<N, DIR, TX, 1, ES, kThreads>(buf, twl);
+  stockham_ip<N, DIR, TX, 1, ES, kThreads, PADR>(buf, twl);
   for (int idx = tid; idx < TX * N; idx += kThreads) {
     const int t = idx % TX, m = idx / TX;
-    if (t < nx) base[m * a.elem_stride + t] = cscale(buf[m * ES + t], a.scale);
+    if (t < nx) base[m * a.elem_stride + t] = cscale(buf[pad_row<PADR>(m) * ES + t], a.scale);
   }
 }
 
@@ -507,7 +509,8 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
 #define CRAVA_COLS_CT(NN)                                                                   \
   if (n == NN && tx > 0) {                                                                  \
     const dim3 g2((ninner + tx - 1) / tx, nouter);                                          \
-    const size_t sm2 = sizeof(float2) * (NN + (size_t)cols_pitch(tx) * NN);                 \
+    const size_t sm2 = sizeof(float2) * (NN + (size_t)cols_pitch(tx) *                      \
+                                         padded_rows(NN, cols_padr(NN, tx)));               \
     const void *f = tx == 16 ? (dir < 0 ? (const void *)k_cols_ip<NN, -1, 16> : (const void *)k_cols_ip<NN, 1, 16>) \
                              : (dir < 0 ? (const void *)k_cols_ip<NN, -1, 8> : (const void *)k_cols_ip<NN, 1, 8>);  \
     int r2 = set_smem(f, sm2);                                                              \

@@ -412,11 +412,27 @@ namespace crava {
 // conflicts to every load and measured 20 % slower at 512 points.)
 __host__ __device__ constexpr int cols_pitch(int tx) { return tx; }
 
+// Row padding of a TX-line column buffer of length n: one spare row after
+// every PADR rows (0: none).  With 8 lines (16 banks per row) the first
+// stage of a power-of-two radix R writes rows R apart from the four
+// butterflies a warp holds, all in the same 16 banks; a spare row every R
+// rows would move every other butterfly to the other 16 banks.  Measured
+// at 512 points it removes the conflicts but not the time (the pass is
+// issue-bound and the row arithmetic costs what the conflicts did), so it
+// is off.
+__host__ __device__ constexpr int cols_padr(int, int) { return 0; }
+// Physical row of logical row e (PADR a power of two or 0).
+template <int PADR>
+__host__ __device__ __forceinline__ constexpr int pad_row(int e) { return PADR ? e + e / PADR : e; }
+// Rows a padded buffer of n elements needs.
+__host__ __device__ constexpr int padded_rows(int n, int padr) { return padr ? n + n / padr : n; }
+
 // In-place compile-time Stockham: each stage first reads every butterfly
 // input of this thread into registers, synchronises, then writes the
 // outputs into the same buffer.  Halves the shared memory of the
-// ping-pong form.  NTH is the block size (compile-time).
-template <int N, int R, int NS, int DIR, int NL, int LS, int ES, int NTH>
+// ping-pong form.  NTH is the block size (compile-time); element e of a
+// line sits at row pad_row<PADR>(e).
+template <int N, int R, int NS, int DIR, int NL, int LS, int ES, int NTH, int PADR>
 __device__ __forceinline__ void ct_stage_ip(float2 *buf, const float2 *__restrict__ tw, int tid) {
   constexpr int M = N / R;
   constexpr int TSTEP = N / (NS * R);
@@ -433,9 +449,8 @@ __device__ __forceinline__ void ct_stage_ip(float2 *buf, const float2 *__restric
   for (int i = 0; i < PER; ++i) {
     const int j = j0 + i * JS;
     if (M % JS == 0 || j < M) {
-      const float2 *sl = lb + j * ES;
 #pragma unroll
-      for (int q = 0; q < R; ++q) v[i][q] = sl[q * M * ES];
+      for (int q = 0; q < R; ++q) v[i][q] = lb[pad_row<PADR>(j + q * M) * ES];
     }
   }
   __syncthreads();
@@ -454,28 +469,28 @@ __device__ __forceinline__ void ct_stage_ip(float2 *buf, const float2 *__restric
         }
       }
       Dft<R, DIR>::run(v[i]);
-      float2 *dl = lb + ((j - base) * R + base) * ES;
+      const int e0 = (j - base) * R + base;
 #pragma unroll
-      for (int q = 0; q < R; ++q) dl[q * NS * ES] = v[i][q];
+      for (int q = 0; q < R; ++q) lb[pad_row<PADR>(e0 + q * NS) * ES] = v[i][q];
     }
   }
   __syncthreads();
 }
 
-template <int N, int DIR, int NL, int LS, int ES, int NTH, int S>
+template <int N, int DIR, int NL, int LS, int ES, int NTH, int PADR, int S>
 struct CtStagesIp {
   static __device__ __forceinline__ void run(float2 *buf, const float2 *tw, int tid) {
     if constexpr (S < CtRadix::count(N)) {
-      ct_stage_ip<N, CtRadix::at(N, S), CtRadix::ns(N, S), DIR, NL, LS, ES, NTH>(buf, tw, tid);
-      CtStagesIp<N, DIR, NL, LS, ES, NTH, S + 1>::run(buf, tw, tid);
+      ct_stage_ip<N, CtRadix::at(N, S), CtRadix::ns(N, S), DIR, NL, LS, ES, NTH, PADR>(buf, tw, tid);
+      CtStagesIp<N, DIR, NL, LS, ES, NTH, PADR, S + 1>::run(buf, tw, tid);
     }
   }
 };
 
 // Transforms NL lines of length N in place (caller syncs before).
-template <int N, int DIR, int NL, int LS, int ES, int NTH>
+template <int N, int DIR, int NL, int LS, int ES, int NTH, int PADR = 0>
 __device__ __forceinline__ void stockham_ip(float2 *buf, const float2 *tw) {
-  CtStagesIp<N, DIR, NL, LS, ES, NTH, 0>::run(buf, tw, threadIdx.x);
+  CtStagesIp<N, DIR, NL, LS, ES, NTH, PADR, 0>::run(buf, tw, threadIdx.x);
 }
 
 }  // namespace crava

@@ -68,34 +68,36 @@ __global__ void __launch_bounds__(kThreads) k_synt(const __grid_constant__ SyntA
   const long long base = x0 + (long long)a.cnxp * y;
   for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
   constexpr int ES = cols_pitch(TX);
+  constexpr int PADR = cols_padr(N, TX);
   for (int idx = tid; idx < TX * N; idx += kThreads) {
     const int t = idx % TX, m = idx / TX;
-    buf[m * ES + t] = x0 + t < a.cnxp ? imp_at(a, base + m * plane + t) : make_float2(0.f, 0.f);
+    buf[pad_row<PADR>(m) * ES + t] = x0 + t < a.cnxp ? imp_at(a, base + m * plane + t) : make_float2(0.f, 0.f);
   }
   __syncthreads();
   if (y < a.ny && a.nz < N) {
     for (int idx = tid; idx < TX * (N - a.nz); idx += kThreads) {
       const int t = idx % TX, m = a.nz + idx / TX;
-      const float2 v0 = buf[t], vl = buf[(a.nz - 1) * ES + t];
-      buf[m * ES + t] = make_float2(taper(v0.x, vl.x, m, a.nz, N), taper(v0.y, vl.y, m, a.nz, N));
+      const float2 v0 = buf[t], vl = buf[pad_row<PADR>(a.nz - 1) * ES + t];
+      buf[pad_row<PADR>(m) * ES + t] = make_float2(taper(v0.x, vl.x, m, a.nz, N), taper(v0.y, vl.y, m, a.nz, N));
     }
   }
   __syncthreads();
-  stockham_ip<N, -1, TX, 1, ES, kThreads>(buf, twl);
+  stockham_ip<N, -1, TX, 1, ES, kThreads, PADR>(buf, twl);
   __syncthreads();
   for (int idx = tid; idx < TX * N; idx += kThreads) {
     const int t = idx % TX, m = idx / TX;
-    buf[m * ES + t] = cmul(buf[m * ES + t], __ldg(a.H + m));
+    float2 *b = buf + pad_row<PADR>(m) * ES + t;
+    *b = cmul(*b, __ldg(a.H + m));
   }
   __syncthreads();
-  stockham_ip<N, 1, TX, 1, ES, kThreads>(buf, twl);
+  stockham_ip<N, 1, TX, 1, ES, kThreads, PADR>(buf, twl);
   __syncthreads();
   for (int idx = tid; idx < TX * N; idx += kThreads) {
     const int t = idx % TX, m = idx / TX;
     const int p = x0 + t;
     if (p >= a.cnxp) continue;
     const long long g = base + m * plane + t;
-    float2 v = buf[m * ES + t];
+    float2 v = buf[pad_row<PADR>(m) * ES + t];
     const bool fx = 2 * p < a.nx, fy = 2 * p + 1 < a.nx;
     if (y >= a.ny || !fx || !fy) {
       const float2 raw = imp_at(a, g);
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(kThreads) k_synt_fixup(const __grid_constant__
 template <int N>
 int launch_synt(const SyntArgs &a, cudaStream_t s) {
   constexpr int TX = 8;
-  const size_t smem = sizeof(float2) * (N + (size_t)cols_pitch(TX) * N);
+  const size_t smem = sizeof(float2) * (N + (size_t)cols_pitch(TX) * padded_rows(N, cols_padr(N, TX)));
   int rc = func_smem((const void *)k_synt<N, TX>, smem);
   if (rc) return rc;
   const dim3 grd((unsigned)((a.cnxp + TX - 1) / TX), (unsigned)a.nyp);
