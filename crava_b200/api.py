@@ -37,7 +37,7 @@ class Params(C.Structure):
         ("nz", C.c_int), ("precision", C.c_int),
         ("lz", C.c_double), ("min_rel_thick", C.c_double),
         ("low_cut", C.c_float), ("high_cut", C.c_float), ("wnc", C.c_float),
-        ("reserved", C.c_float),
+        ("thickness_mode", C.c_int),
         ("wavelet", F32P), ("wavelet_norm", F32P), ("A", F32P),
         ("theta_cov", F64P), ("var0", F64P),
     ]
@@ -177,7 +177,7 @@ class Context:
             self._keep.append(wn)
         self.params = Params(case.nxp, case.nyp, case.nzp, case.ntheta, case.nz, precision,
                              case.lz, case.min_rel_thick, case.low_cut, case.high_cut, case.wnc,
-                             0.0, wav.ctypes.data_as(F32P),
+                             int(getattr(case, "thickness_mode", 0)), wav.ctypes.data_as(F32P),
                              wn.ctypes.data_as(F32P) if wn is not None else None,
                              A.ctypes.data_as(F32P), th.ctypes.data_as(F64P),
                              v0.ctypes.data_as(F64P))

@@ -70,6 +70,7 @@ int validate(const crava_gpu_params *p) {
   if (!p->wavelet || !p->A || !p->theta_cov || !p->var0) return CRAVA_GPU_ERR_ARG;
   if (p->nz < 1 || !(p->lz > 0.0)) return CRAVA_GPU_ERR_ARG;
   if (p->precision < CRAVA_SOLVE_FP64 || p->precision > CRAVA_SOLVE_FP32) return CRAVA_GPU_ERR_ARG;
+  if (p->thickness_mode != 0 && p->thickness_mode != 1) return CRAVA_GPU_ERR_ARG;
   return CRAVA_GPU_OK;
 }
 

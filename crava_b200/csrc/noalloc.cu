@@ -92,6 +92,7 @@ extern "C" int crava_gpu_posterior_noalloc(const crava_gpu_params *p, const crav
   if (p->nxp < 2 || p->nyp < 1 || p->nzp < 2 || !smooth_2357(p->nzp)) return CRAVA_GPU_ERR_ARG;
   if (p->ntheta < 1 || p->ntheta > CRAVA_GPU_MAX_THETA || p->nz < 1 || !(p->lz > 0.0)) return CRAVA_GPU_ERR_ARG;
   if (precision < CRAVA_SOLVE_FP64 || precision > CRAVA_SOLVE_FP32) return CRAVA_GPU_ERR_ARG;
+  if (p->thickness_mode != 0 && p->thickness_mode != 1) return CRAVA_GPU_ERR_ARG;
   if ((size_t)p->nzp > kMaxNzp || (size_t)p->nzp * p->ntheta > kMaxKzTheta) return CRAVA_GPU_ERR_TOO_LARGE;
   auto mis = [](const void *q) { return !q || (reinterpret_cast<uintptr_t>(q) & 7u) != 0; };
   for (int q = 0; q < 3; ++q) if (mis(g->mu[q])) return CRAVA_GPU_ERR_ARG;

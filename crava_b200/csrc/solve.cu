@@ -36,7 +36,7 @@ using sb::tri;
 __global__ void k_kz_tables(const float *__restrict__ wav,
                             const float *__restrict__ wnorm_in, int has_norm,
                             int nzp, int nt, int nz, double lz, double mrt,
-                            float low_cut, float high_cut, KzTables t) {
+                            float low_cut, float high_cut, int mode, KzTables t) {
   extern __shared__ double shd[];
   const int l = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
   const int cnzp = nzp / 2 + 1;
@@ -99,13 +99,46 @@ __global__ void k_kz_tables(const float *__restrict__ wav,
     float2 cg = k < cnzp ? G[k] : make_float2(G[nzp - k].x, -G[nzp - k].y);
     // diff1Operator: FFT of [-1, 0, ..., 0, 1] = -1 + e^{2 pi i k/nzp}
     float2 kD = make_float2((float)(cs[k] - 1.0), (float)sn[k]);
-    float2 kw = make_float2(ca.x, -ca.y);  // fillkW (src/crava.cpp:1336-1344)
-    float2 wd = make_float2(kD.x * kw.x - kD.y * kw.y, kD.x * kw.y + kD.y * kw.x);
     const long long o = (long long)k * nt + l;
-    t.wd[o] = wd;
-    t.e1[o] = make_float2(ca.x / wn, -(ca.y / wn));  // fillkWNorm (:1346-1355)
-    t.e2[o] = make_float2(cg.x / gn, -(cg.y / gn));
-    t.e3[o] = 1.0f;
+    if (mode == 1) {
+      // non-constant thickness (src/crava.cpp:1059-1083): K = diag(D) A,
+      // errMult1 = 1/|W|, errMult2 = D3/|E3| with D3 the spectrum of the
+      // central difference of the backward difference of the difference
+      // operator (:938-940), here i (sin 2t - 2 sin t), t = 2 pi k / nzp;
+      // errMult3 = fillInverseAbskWRobust (:1358-1384)
+      t.wd[o] = kD;
+      t.e1[o] = make_float2(1.0f / wn, 0.0f);
+      const double s1 = sn[k], s2 = sn[(int)((2LL * k) % nzp)];
+      const float m2 = 1.0f / gn;
+      t.e2[o] = make_float2(0.0f * m2, (float)(s2 - 2.0 * s1) * m2);
+      // getCAmp(k, 0.999): the spectrum of the slightly stretched wavelet
+      const int refk = k < cnzp ? k : nzp - k;
+      const float scale = 0.999f;
+      const float omega = __fdiv_rn((float)refk, scale);
+      float2 vf = make_float2(0.0f, 0.0f);
+      if (omega < (float)cnzp) {
+        const int omL = (int)floorf(omega);
+        int omU = omL + 1;
+        if (omU >= cnzp) omU -= 1;
+        const float dO = __fsub_rn(omega, (float)omL), dL = __fsub_rn(1.0f, dO);
+        vf.x = __fadd_rn(__fmul_rn(W[omL].x, dL), __fmul_rn(W[omU].x, dO));
+        vf.y = __fadd_rn(__fmul_rn(W[omL].y, dL), __fmul_rn(W[omU].y, dO));
+        if (k >= cnzp) vf.y = -vf.y;
+      }
+      vf.x = __fdiv_rn(vf.x, scale);
+      vf.y = __fdiv_rn(vf.y, scale);
+      const float mod = __fadd_rn(__fmul_rn(ca.x, ca.x), __fmul_rn(ca.y, ca.y));
+      const float modF = __fadd_rn(__fmul_rn(vf.x, vf.x), __fmul_rn(vf.y, vf.y));
+      const float maxMod = fmaxf(mod, modF);
+      // float(1.0 / sqrt(maxMod)): the float square root, a double quotient
+      t.e3[o] = maxMod > 0.0f ? (float)(1.0 / (double)__fsqrt_rn(maxMod)) : wn * nzp * nzp * 100.0f;
+    } else {
+      float2 kw = make_float2(ca.x, -ca.y);  // fillkW (src/crava.cpp:1336-1344)
+      t.wd[o] = make_float2(kD.x * kw.x - kD.y * kw.y, kD.x * kw.y + kD.y * kw.x);
+      t.e1[o] = make_float2(ca.x / wn, -(ca.y / wn));  // fillkWNorm (:1346-1355)
+      t.e2[o] = make_float2(cg.x / gn, -(cg.y / gn));
+      t.e3[o] = 1.0f;
+    }
     if (l == 0) {
       int mk = k < nzp - k ? k : nzp - k;
       float rf = (float)((nz * 1000.0f) / (lz * nzp) * mk);  // src/crava.cpp:1044
@@ -257,7 +290,7 @@ int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s) {
   if (smem > 48 * 1024)
     CRAVA_CUDA_TRY(cudaFuncSetAttribute(k_kz_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_kz_tables<<<nt, nth, smem, s>>>(dw, dn, p.wavelet_norm != nullptr, nzp, nt, p.nz, p.lz,
-                                    p.min_rel_thick, p.low_cut, p.high_cut, *t);
+                                    p.min_rel_thick, p.low_cut, p.high_cut, p.thickness_mode, *t);
   cudaError_t le = cudaGetLastError();
   cudaError_t se = cudaStreamSynchronize(s);
   cudaFree(dw);
@@ -277,7 +310,7 @@ int kz_tables_build_device(const crava_gpu_params &p, const float *d_wavelet,
   if (smem > 48 * 1024)
     CRAVA_CUDA_TRY(cudaFuncSetAttribute(k_kz_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_kz_tables<<<nt, nth, smem, s>>>(d_wavelet, d_norm, d_norm != nullptr, nzp, nt, p.nz, p.lz,
-                                    p.min_rel_thick, p.low_cut, p.high_cut, *t);
+                                    p.min_rel_thick, p.low_cut, p.high_cut, p.thickness_mode, *t);
   CRAVA_LAUNCH_CHECK();
   return CRAVA_GPU_OK;
 }

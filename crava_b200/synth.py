@@ -67,6 +67,7 @@ class Case:
     cov: list                  # 6 x float32 [nzp, nyp, rnxp]
     err_corr: np.ndarray       # float32 [nzp, nyp, rnxp]
     truth: list = field(default_factory=list)
+    thickness_mode: int = 0    # 0 constant thickness, 1 non-constant (data divided by the wavelet)
 
     @property
     def ntheta(self):

@@ -66,7 +66,11 @@ typedef struct crava_gpu_params {
   double min_rel_thick;       /* Simbox::getMinRelThick                                */
   float low_cut, high_cut;    /* frequency band in Hz (lowCut_, highCut_)              */
   float wnc;                  /* white-noise component (wnc_)                          */
-  float reserved;
+  int thickness_mode;         /* 0: constant thickness (Simbox::getIsConstantThick), K =
+                                 diag(D conj W) A; 1: non-constant thickness, the data
+                                 already divided by the local scale wavelet
+                                 (src/crava.cpp:1059-1083): K = diag(D) A, errMult1 =
+                                 1/|W|, errMult2 = D3/|E3|, errMult3 = robust 1/|W(k)| */
   const float *wavelet;       /* [ntheta][nzp] wavelet samples in FFT order (rAmp_)    */
   const float *wavelet_norm;  /* [ntheta] Wavelet::getNorm, or NULL = time-domain norm */
   const float *A;             /* [ntheta][3] reflection matrix (A_)                    */

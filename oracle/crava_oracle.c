@@ -189,6 +189,36 @@ static cf get_camp(const cf *s, int nzp, int k) {
   return v;
 }
 
+/* Wavelet::getCAmp(k, scale) (src/wavelet.cpp:327-385): the spectrum of
+ * the wavelet stretched by `scale`, linear interpolation between bins. */
+static cf get_camp_scaled(const cf *s, int nzp, int k, float scale) {
+  int cnzp = nzp / 2 + 1, refk = k < cnzp ? k : nzp - k;
+  cf v;
+  float omega = (float)refk / scale;
+  if (omega >= cnzp) { v.re = 0.0f; v.im = 0.0f; }
+  else {
+    int omL = (int)floorf(omega), omU = (int)floorf(omega) + 1;
+    if (omU >= cnzp) omU -= 1;
+    float dOmega = omega - (float)omL;
+    v.re = s[omL].re * (1.0f - dOmega) + s[omU].re * dOmega;
+    if (k < cnzp) v.im = (s[omL].im * (1.0f - dOmega) + s[omU].im * dOmega);
+    else v.im = (-s[omL].im * (1.0f - dOmega) - s[omU].im * dOmega);
+  }
+  v.re /= scale; v.im /= scale;
+  return v;
+}
+
+/* Crava::fillInverseAbskWRobust (src/crava.cpp:1358-1384) for one angle. */
+static float inverse_abs_robust(const cf *W, int nzp, int k, float norm) {
+  cf value = get_camp(W, nzp, k), valueFine = get_camp_scaled(W, nzp, k, 0.999f);
+  float modulus = value.re * value.re + value.im * value.im;
+  float modulusFine = valueFine.re * valueFine.re + valueFine.im * valueFine.im;
+  float maxMod = modulus > modulusFine ? modulus : modulusFine;
+  /* sqrt of a float argument resolves to the float overload in C++ */
+  if (maxMod > 0.0) return (float)(1.0 / (double)sqrtf(maxMod));
+  return norm * nzp * nzp * 100.0f;
+}
+
 /* errorSmooth3 = central(backward(forward(w))) -- the three Wavelet1D
  * difference constructors of src/wavelet1D.cpp:420-479. */
 static void smooth3(const float *w, int n, float *g) {
@@ -226,11 +256,37 @@ int orc_kz_tables(const crava_oracle_params *p, float *wd_, float *e1_,
   }
   dop[0] = -1.0f; dop[nzp - 1] = 1.0f;
   real_spectrum(dop, nzp, D);
+  cf *D3 = (cf *)malloc(sizeof(cf) * cnzp);
+  {
+    /* diff3Operator = central(backward(diff1Operator)), src/crava.cpp:938-940 */
+    float *d2 = (float *)malloc(sizeof(float) * nzp), *d3 = (float *)malloc(sizeof(float) * nzp);
+    for (int i = 0; i < nzp; ++i) d2[i] = (i == 0) ? dop[0] - dop[nzp - 1] : dop[i] - dop[i - 1];
+    for (int i = 0; i < nzp; ++i) {
+      if (i == 0) d3[i] = (float)(0.5 * (d2[1] - d2[nzp - 1]));
+      else if (i == nzp - 1) d3[i] = (float)(0.5 * (d2[0] - d2[i - 1]));
+      else d3[i] = (float)(0.5 * (d2[i + 1] - d2[i - 1]));
+    }
+    real_spectrum(d3, nzp, D3);
+    free(d2); free(d3);
+  }
   for (int k = 0; k < nzp; ++k) {
     int mk = k < nzp - k ? k : nzp - k;
     float realFrequency = (float)((p->nz * 1000.0f) / (p->lz * nzp) * mk);
     inv[k] = (realFrequency > p->low_cut * p->min_rel_thick) && (realFrequency < p->high_cut);
     cf kD = get_camp(D, nzp, k);
+    if (p->thickness_mode == 1) {
+      /* non-constant thickness, src/crava.cpp:1059-1083 */
+      cf kD3 = get_camp(D3, nzp, k);
+      for (int l = 0; l < nt; ++l) {
+        long o = (long)k * nt + l;
+        wd[o] = kD;
+        e1[o].re = 1.0f / wn[l]; e1[o].im = 0.0f;
+        float m2 = 1.0f / gn[l];
+        e2[o].re = kD3.re * m2; e2[o].im = kD3.im * m2;
+        e3[o] = inverse_abs_robust(W + (long)l * cnzp, nzp, k, wn[l]);
+      }
+      continue;
+    }
     for (int l = 0; l < nt; ++l) {
       cf a = get_camp(W + (long)l * cnzp, nzp, k);
       cf kw; kw.re = a.re; kw.im = -a.im;
@@ -244,7 +300,7 @@ int orc_kz_tables(const crava_oracle_params *p, float *wd_, float *e1_,
       e3[(long)k * nt + l] = 1.0f;
     }
   }
-  free(W); free(G); free(D); free(g); free(dop);
+  free(W); free(G); free(D); free(D3); free(g); free(dop);
   return 0;
 }
 

@@ -36,7 +36,7 @@ typedef struct crava_oracle_params {
   double min_rel_thick;       /* simbox min relative thickness             */
   float low_cut, high_cut;    /* frequency band (Hz)                        */
   float wnc;                  /* white-noise component                      */
-  float reserved;
+  int thickness_mode;         /* 0 constant thickness, 1 non-constant         */
   const float  *wavelet;      /* [ntheta][nzp] time samples, FFT order      */
   const float  *wavelet_norm; /* [ntheta] or NULL (time-domain L2 norm)     */
   const float  *A;            /* [ntheta][3] reflection matrix              */

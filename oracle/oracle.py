@@ -34,7 +34,7 @@ class Params(C.Structure):
         ("nz", C.c_int), ("precision", C.c_int),
         ("lz", C.c_double), ("min_rel_thick", C.c_double),
         ("low_cut", C.c_float), ("high_cut", C.c_float), ("wnc", C.c_float),
-        ("reserved", C.c_float),
+        ("thickness_mode", C.c_int),
         ("wavelet", F32P), ("wavelet_norm", F32P), ("A", F32P),
         ("theta_cov", F64P), ("var0", F64P),
     ]
@@ -141,7 +141,8 @@ def make_params(case, keep=None):
     v0 = np.ascontiguousarray(case.var0, dtype=np.float64)
     keep += [wav, A, th, v0]
     p = Params(case.nxp, case.nyp, case.nzp, case.ntheta, case.nz, 0, case.lz,
-               case.min_rel_thick, case.low_cut, case.high_cut, case.wnc, 0.0,
+               case.min_rel_thick, case.low_cut, case.high_cut, case.wnc,
+               int(getattr(case, "thickness_mode", 0)),
                _fp(wav), None, _fp(A), _dp(th), _dp(v0))
     return p, keep
 

@@ -8,6 +8,7 @@
  * the per-bin loop below restates src/crava.cpp:1042-1151 while every
  * numerical call in it is the reference's own function.
  */
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -76,6 +77,31 @@ fftw_complex get_camp(const std::vector<fftw_complex> &c, int nzp, int k) {
   return v;
 }
 
+/* Wavelet::getCAmp(k, scale), src/wavelet.cpp:327-385 */
+fftw_complex get_camp_scaled(const std::vector<fftw_complex> &c, int nzp, int k, float scale) {
+  const int cnzp = nzp / 2 + 1;
+  fftw_complex value;
+  float omega, dOmega;
+  int omU, omL;
+  const int refk = k < cnzp ? k : nzp - k;
+  omega = float(refk) / scale;
+  if (omega >= cnzp) {
+    value.re = 0.0f;
+    value.im = 0.0f;
+  } else {
+    omL = int(std::floor(omega));
+    omU = int(std::floor(omega)) + 1;
+    if (omU >= cnzp) omU -= 1;
+    dOmega = omega - float(omL);
+    value.re = c[omL].re * (1.0f - dOmega) + c[omU].re * dOmega;
+    if (k < cnzp) value.im = (c[omL].im * (1.0f - dOmega) + c[omU].im * dOmega);
+    else value.im = (-c[omL].im * (1.0f - dOmega) - c[omU].im * dOmega);
+  }
+  value.re /= scale;
+  value.im /= scale;
+  return value;
+}
+
 /* Wavelet::findNorm on a real wavelet, src/wavelet.cpp:789-808 */
 float find_norm(const float *w, int n) {
   double norm2 = 0.0;
@@ -114,6 +140,16 @@ void build_tables(const crava_oracle_params *p, KzTables &t) {
   std::vector<float> d(nzp, 0.0f);
   d[0] = -1.0f; d[nzp - 1] = 1.0f;
   std::vector<fftw_complex> D = spectrum1d(d.data(), nzp);
+  /* diff3Operator (src/crava.cpp:938-940): backward then central
+   * difference of diff1Operator (src/wavelet1D.cpp:420-479) */
+  std::vector<float> d2(nzp), d3(nzp);
+  for (int i = 0; i < nzp; ++i) d2[i] = (i == 0) ? d[0] - d[nzp - 1] : d[i] - d[i - 1];
+  for (int i = 0; i < nzp; ++i) {
+    if (i == 0) d3[i] = static_cast<fftw_real>(0.5 * (d2[i + 1] - d2[nzp - 1]));
+    else if (i == nzp - 1) d3[i] = static_cast<fftw_real>(0.5 * (d2[0] - d2[i - 1]));
+    else d3[i] = static_cast<fftw_real>(0.5 * (d2[i + 1] - d2[i - 1]));
+  }
+  std::vector<fftw_complex> D3 = spectrum1d(d3.data(), nzp);
 
   t.wd.resize(static_cast<size_t>(nzp) * nt); t.e1.resize(t.wd.size());
   t.e2.resize(t.wd.size()); t.e3.resize(t.wd.size()); t.inv.resize(nzp);
@@ -122,6 +158,29 @@ void build_tables(const crava_oracle_params *p, KzTables &t) {
     float realFrequency = static_cast<float>((p->nz * 1000.0f) / (p->lz * nzp) * std::min(k, nzp - k));
     t.inv[k] = realFrequency > p->low_cut * p->min_rel_thick && realFrequency < p->high_cut;
     fftw_complex kD = get_camp(D, nzp, k);
+    if (p->thickness_mode == 1) {
+      /* non-constant thickness branch, src/crava.cpp:1059-1083 */
+      fftw_complex kD3 = get_camp(D3, nzp, k);
+      for (int l = 0; l < nt; ++l) {
+        size_t o = static_cast<size_t>(k) * nt + l;
+        t.wd[o] = kD;                                     /* K = DA */
+        t.e1[o].re = 1.0f; t.e1[o].im = 0.0f;             /* lib_matrFillOnesVecCpx */
+        t.e1[o].re /= wn[l];
+        t.e2[o] = kD3;
+        float errorSmoothMult = 1.0f / gn[l];
+        t.e2[o].re *= errorSmoothMult;
+        t.e2[o].im *= errorSmoothMult;
+        /* fillInverseAbskWRobust, src/crava.cpp:1358-1384 */
+        fftw_complex value = get_camp(W[l], nzp, k);
+        fftw_complex valueFine = get_camp_scaled(W[l], nzp, k, 0.999f);
+        float modulus = value.re * value.re + value.im * value.im;
+        float modulusFine = valueFine.re * valueFine.re + valueFine.im * valueFine.im;
+        float maxMod = std::max(modulus, modulusFine);
+        if (maxMod > 0.0) t.e3[o] = float(1.0 / std::sqrt(maxMod));
+        else t.e3[o] = wn[l] * nzp * nzp * 100.0f;
+      }
+      continue;
+    }
     for (int l = 0; l < nt; ++l) {  /* fillkW, crava.cpp:1336-1344 */
       kW[l].re = float(get_camp(W[l], nzp, k).re);
       kW[l].im = -float(get_camp(W[l], nzp, k).im);

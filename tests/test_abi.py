@@ -49,17 +49,17 @@ def _params(case, **over):
     th = np.ascontiguousarray(case.theta_cov, np.float64)
     v0 = np.ascontiguousarray(case.var0, np.float64)
     f = dict(nxp=case.nxp, nyp=case.nyp, nzp=case.nzp, ntheta=case.ntheta, nz=case.nz, precision=1,
-             lz=case.lz, min_rel_thick=1.0, low_cut=5.0, high_cut=55.0, wnc=0.1)
+             lz=case.lz, min_rel_thick=1.0, low_cut=5.0, high_cut=55.0, wnc=0.1, thickness_mode=0)
     f.update(over)
     p = api.Params(f["nxp"], f["nyp"], f["nzp"], f["ntheta"], f["nz"], f["precision"], f["lz"],
-                   f["min_rel_thick"], f["low_cut"], f["high_cut"], f["wnc"], 0.0,
+                   f["min_rel_thick"], f["low_cut"], f["high_cut"], f["wnc"], f["thickness_mode"],
                    wav.ctypes.data_as(api.F32P), None, A.ctypes.data_as(api.F32P),
                    th.ctypes.data_as(api.F64P), v0.ctypes.data_as(api.F64P))
     return p, (wav, A, th, v0)
 
 
 @pytest.mark.parametrize("over", [dict(nxp=11 * 2), dict(nzp=13), dict(ntheta=0), dict(ntheta=9),
-                                  dict(precision=7), dict(nz=0), dict(lz=0.0)])
+                                  dict(precision=7), dict(nz=0), dict(lz=0.0), dict(thickness_mode=2)])
 def test_create_rejects_bad_parameters(over):
     case = synth.make_case(16, 12, 32, (10.0, 20.0), 0.1, seed=1)
     p, keep = _params(case, **over)

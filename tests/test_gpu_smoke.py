@@ -92,6 +92,33 @@ def test_unit_vs_reference_unit():
         assert rel(g.cpu().numpy()[..., :nx], o[..., :nx]) < 2e-5
 
 
+@pytest.mark.parametrize("shape", [(32, 24, 64), (15, 16, 20)])
+def test_nonconstant_thickness_unit(shape):
+    """The non-constant-thickness branch (K = diag(D) A and its error
+    multipliers, src/crava.cpp:1059-1083): device tables vs the restatement
+    and the whole unit vs the reference's numerics."""
+    case = synth.make_case(*shape, (0.0, 15.0, 30.0), 0.1, seed=13)
+    case.thickness_mode = 1
+    case.min_rel_thick = 0.8
+    ctx = api.Context(case)
+    wd, e1, e2, e3, inv = ctx.kz_tables()
+    owd, oe1, oe2, oe3, oinv = O.kz_tables(case, "orc")
+    assert np.array_equal(inv, oinv)
+    for a, b in [(wd, owd), (e1, oe1), (e2, oe2)]:
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+    m = inv.astype(bool)
+    assert np.abs(e3[m] - oe3[m]).max() <= 1e-6 * np.abs(oe3[m]).max()
+    ctx.set_kz_tables(O.kz_tables(case, "ref" if O.have_ref() else "orc"))
+    d = lambda gs: [api.to_device(g) for g in gs]
+    mu, data, cov, err = d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0]
+    ctx.posterior_unit(mu, data, cov, err, api.FP32)
+    which = "ref" if O.have_ref() else "orc"
+    omu, ores, ocov, ofail = O.unit_fp32(case, which)
+    nx = case.nxp
+    for g, o in zip(mu + data + cov, omu + ores + ocov):
+        assert rel(g.cpu().numpy()[..., :nx], o[..., :nx]) < 2e-5
+
+
 def test_host_entry_matches_device_unit():
     case = synth.make_case(32, 24, 64, (0.0, 15.0, 30.0), 0.1, seed=9)
     ctx = api.Context(case)

@@ -158,3 +158,25 @@ def test_prior_fills_match_synthetic_cases():
         for g, h in zip(cov, case.cov):
             assert np.array_equal(bits(g[..., :nx]), bits(h[..., :nx]))
         assert np.array_equal(bits(O.fill_err_corr(nx, ny, nz, cxy, 0.0, 0.0)), bits(case.err_corr))
+
+
+@pytest.mark.parametrize("shape", [(16, 12, 64), (15, 16, 20), (8, 8, 128)])
+def test_nonconstant_thickness_tables_vs_ref(shape):
+    """Tables of the non-constant-thickness branch (src/crava.cpp:1059-1083):
+    restatement vs the reference's FFTW; the robust inverse wavelet modulus
+    on the inverted planes (elsewhere it inverts spectrum values at the
+    level of rounding noise and the solve does not read it)."""
+    if not O.have_ref():
+        pytest.skip("oracle/_ref not built")
+    from crava_b200 import synth
+
+    case = synth.make_case(*shape, (0.0, 15.0, 30.0), 0.1, seed=3)
+    case.thickness_mode = 1
+    case.min_rel_thick = 0.8
+    a = O.kz_tables(case, "orc")
+    b = O.kz_tables(case, "ref")
+    assert np.array_equal(a[4], b[4])
+    for x, y in zip(a[:3], b[:3]):
+        assert np.abs(x - y).max() <= 1e-6 * np.abs(y).max()
+    inv = b[4].astype(bool)
+    assert np.abs(a[3][inv] - b[3][inv]).max() <= 1e-6 * np.abs(b[3][inv]).max()
