@@ -570,11 +570,14 @@ def run_own(args):
         peak = peaks.get("hbm_gbs") or 6650.0
         achieved = bpl / (tot / n * 1e-3) / 1e9
         traffic = None
-        try:
-            with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-                tr = json.load(f)
+        try:  # DRAM bytes per launch from the committed ncu launch-list summary
+            import re
             key = f"{nxp}x{nyp}x{nzp}"
-            traffic = tr.get(key, {}).get(name)
+            with open(os.path.join(ROOT, "profiles", f"launches_posterior_unit_{key}x{nt}.md")) as f:
+                for line in f:
+                    m = re.match(r"traffic_per_launch (\S+) (\S+) ([0-9.eE+]+)", line)
+                    if m and m.group(1) == name and m.group(2) == key:
+                        traffic = float(m.group(3))
         except Exception:
             pass
         roof = {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak,

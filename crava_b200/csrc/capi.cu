@@ -169,7 +169,15 @@ int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend) {
 }
 
 int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {
-  Scope sc(c, K_SOLVE);
+  // bytes the in-place solve moves: (10+nt) spectra read and (9+nt)
+  // written for an inverted bin, the six covariance spectra both ways for
+  // a band-gated one (the FP32 reference-order kernel moves all of them)
+  const double plane_bytes = (double)c->g.cnxp * c->g.nyp * 8.0;
+  const int nt = c->p.ntheta, nzp = c->p.nzp;
+  const double bytes = precision == CRAVA_SOLVE_FP32
+                           ? (double)(19 + 2 * nt) * nzp * plane_bytes
+                           : ((double)(19 + 2 * nt) * c->n_inverted + 12.0 * (nzp - c->n_inverted)) * plane_bytes;
+  Scope sc(c, K_SOLVE, bytes);
   SolveGrids sg = to_solve_grids(gr, c->p.ntheta);
   return posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
                          precision, c->counters, c->stream);
@@ -369,7 +377,7 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
   if ((rc = kz_tables_build(c->p, &c->tables, c->stream))) return fail(rc);
-  if ((rc = kz_order_build(nzp, &c->tables, c->stream))) return fail(rc);
+  if ((rc = kz_order_build(nzp, &c->tables, c->stream, &c->n_inverted))) return fail(rc);
   *out = c;
   return CRAVA_GPU_OK;
 }
@@ -742,7 +750,7 @@ int crava_gpu_set_kz_tables(crava_gpu_ctx *c, const float *wd, const float *e1, 
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e2, e2, n * sizeof(float2), cudaMemcpyHostToDevice));
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e3, e3, n * sizeof(float), cudaMemcpyHostToDevice));
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.inv, inv, (size_t)c->p.nzp * sizeof(int), cudaMemcpyHostToDevice));
-  return kz_order_build(c->p.nzp, &c->tables, c->stream);
+  return kz_order_build(c->p.nzp, &c->tables, c->stream, &c->n_inverted);
 }
 
 }  // extern "C"

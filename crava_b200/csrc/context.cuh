@@ -47,6 +47,9 @@ struct crava_gpu_ctx {
   bool capture = false;
   // synthetic seismic: per-angle spectral filters [ntheta][nzp] (device)
   float2 *synt_H = nullptr;
+  // inverted kz planes (band flag set): the solve moves every spectrum of
+  // their bins and only the covariance spectra of the others
+  int n_inverted = 0;
   // prior fills: lateral [nyp][nxp] then temporal [nzp] correlation (device)
   float *prior_buf = nullptr;
 };

@@ -255,13 +255,14 @@ void kz_tables_free(KzTables *t) {
   *t = KzTables{};
 }
 
-int kz_order_build(int nzp, KzTables *t, cudaStream_t s) {
+int kz_order_build(int nzp, KzTables *t, cudaStream_t s, int *n_inverted) {
   std::vector<int> inv(nzp), order;
   CRAVA_CUDA_TRY(cudaMemcpyAsync(inv.data(), t->inv, sizeof(int) * nzp, cudaMemcpyDeviceToHost, s));
   CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
   std::vector<int> heavy, light;
   for (int k = 0; k < nzp; ++k) (inv[k] ? heavy : light).push_back(k);
   const long long nh = (long long)heavy.size();
+  if (n_inverted) *n_inverted = (int)nh;
   size_t ih = 0, il = 0;
   for (long long i = 0; i < nzp; ++i) {
     // Bresenham: the i-th slot takes a heavy plane when the heavy share so

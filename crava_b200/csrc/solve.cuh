@@ -41,7 +41,8 @@ int kz_tables_alloc(int nzp, int nt, KzTables *t);
 // Fills t->order from t->inv (synchronises s): inverted (compute-heavy)
 // and band-gated (memory-only) planes interleaved evenly, so the solve's
 // blocks keep both the FP64 pipes and HBM busy.
-int kz_order_build(int nzp, KzTables *t, cudaStream_t s);
+// *n_inverted (optional) receives the number of inverted planes.
+int kz_order_build(int nzp, KzTables *t, cudaStream_t s, int *n_inverted = nullptr);
 void kz_tables_free(KzTables *t);
 // Builds the tables from the wavelets on the device (params: host struct).
 int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s);
