@@ -294,29 +294,35 @@ __global__ void __launch_bounds__(kThreads) k_rows_ip(const __grid_constant__ Ro
   }
   __syncthreads();
   stockham_ip<N, DIR, kRR, 1, P, kThreads>(buf, twl);
+  // One warp per row, lanes along the row: no division by the row length
+  // (N + 1 outputs) and one row address per warp and row.
+  const int warp = tid >> 5, lane = tid & 31;
   if (DIR < 0) {
     // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{h-k})/2, O = -i (Z_k - conj Z_{h-k})/2
-    for (int idx = tid; idx < kRR * (N + 1); idx += kThreads) {
-      const int r = idx / (N + 1), k = idx % (N + 1);
-      if (r >= nrows) continue;
-      const float2 zk = buf[(k == N ? 0 : k) * P + r];
-      float2 zm = buf[(k == 0 ? 0 : N - k) * P + r];
-      zm.y = -zm.y;
-      const float2 e = cscale(cadd(zk, zm), 0.5f);
-      const float2 d = csub(zk, zm);
-      const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
-      reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+    for (int r = warp; r < nrows; r += kThreads / 32) {
+      float2 *orow = reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp);
+      for (int k = lane; k <= N; k += 32) {
+        const float2 zk = buf[(k == N ? 0 : k) * P + r];
+        float2 zm = buf[(k == 0 ? 0 : N - k) * P + r];
+        zm.y = -zm.y;
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 d = csub(zk, zm);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        orow[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+      }
     }
   } else {
-    for (int idx = tid; idx < kRR * (N + 1); idx += kThreads) {
-      const int r = idx / (N + 1), m = idx % (N + 1);
-      if (r >= nrows) continue;
-      float2 v = make_float2(0.f, 0.f);
-      if (m < N) {
-        v = cscale(buf[m * P + r], a.scale);
-        if (a.addend) v = cadd(v, reinterpret_cast<const float2 *>(a.addend + (row0 + r) * a.rnxp)[m]);
+    for (int r = warp; r < nrows; r += kThreads / 32) {
+      float2 *orow = reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp);
+      const float2 *arow = a.addend ? reinterpret_cast<const float2 *>(a.addend + (row0 + r) * a.rnxp) : nullptr;
+      for (int m = lane; m <= N; m += 32) {
+        float2 v = make_float2(0.f, 0.f);
+        if (m < N) {
+          v = cscale(buf[m * P + r], a.scale);
+          if (arow) v = cadd(v, arow[m]);
+        }
+        orow[m] = v;
       }
-      reinterpret_cast<float2 *>(a.grid + (row0 + r) * a.rnxp)[m] = v;
     }
   }
 }
