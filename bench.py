@@ -261,7 +261,7 @@ def run_batch(args, case256, dev, stream, max_over_ranks):
         return max_over_ranks(ev0.elapsed_time(ev1) / runs), (api.launch_count() - n0) // runs
 
     g = api.Batch(vint, api.BATCH_AUTOTUNE, stream=stream)
-    tunings = [{"cols_y_tile": t.cols_y_tile, "cols_z_tile": t.cols_z_tile, "fused": t.fused}
+    tunings = [{"cols_y_tile": t.cols_y_tile, "cols_z_tile": t.cols_z_tile, "fused": t.fused, "lanes": t.lanes}
                for t in (ctx.tuning() for ctx in ctxs)]
     ms_graph, kern = timed(g, 5)
     g.close()

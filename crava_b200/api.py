@@ -61,7 +61,7 @@ class Stats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("cols_y_tile", C.c_int), ("cols_z_tile", C.c_int), ("fused", C.c_int),
-                ("ms", C.c_float)]
+                ("ms", C.c_float), ("lanes", C.c_int)]
 
 
 class Vintage(C.Structure):
@@ -243,8 +243,8 @@ class Context:
         check(self.lib.crava_gpu_get_tuning(self.handle, C.byref(t)), "get_tuning")
         return t
 
-    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0):
-        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0)
+    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0, lanes=2):
+        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0, lanes)
         check(self.lib.crava_gpu_set_tuning(self.handle, C.byref(t)), "set_tuning")
 
     def autotune(self, src, dst, precision=None, reps=2) -> Tuning:

@@ -167,6 +167,7 @@ int crava_gpu_get_tuning(crava_gpu_ctx *c, crava_gpu_tuning *out) {
   out->cols_z_tile = c->plans.tile_z;
   out->fused = c->fused ? 1 : 0;
   out->ms = 0.0f;
+  out->lanes = c->lanes;
   return CRAVA_GPU_OK;
 }
 
@@ -174,9 +175,11 @@ int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   if (!c || !t) return CRAVA_GPU_ERR_ARG;
   auto ok = [](int x) { return x == -1 || x == 0 || x == 8 || x == 16; };
   if (!ok(t->cols_y_tile) || !ok(t->cols_z_tile)) return CRAVA_GPU_ERR_ARG;
+  if (t->lanes != 1 && t->lanes != 2) return CRAVA_GPU_ERR_ARG;
   c->plans.tile_y = t->cols_y_tile;
   c->plans.tile_z = t->cols_z_tile;
   c->fused = t->fused != 0;
+  c->lanes = t->lanes;
   return CRAVA_GPU_OK;
 }
 
@@ -190,11 +193,12 @@ int crava_gpu_autotune(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_
   std::vector<crava_gpu_tuning> cand;
   const bool ty = cols_tunable(c->g.nyp), tz = cols_tunable(c->g.nzp);
   const int tiles[3] = {16, 8, 0};
-  for (int a = 0; a < (ty ? 3 : 1); ++a)
-    for (int z = 0; z < (tz ? 3 : 1); ++z)
-      cand.push_back({ty ? tiles[a] : -1, tz ? tiles[z] : -1, 0, 0.0f});
+  for (int lanes = 1; lanes <= 2; ++lanes)
+    for (int a = 0; a < (ty ? 3 : 1); ++a)
+      for (int z = 0; z < (tz ? 3 : 1); ++z)
+        cand.push_back({ty ? tiles[a] : -1, tz ? tiles[z] : -1, 0, 0.0f, lanes});
   // the fused unit does not use the column passes: one candidate
-  if (c->uplan.ok && precision != CRAVA_SOLVE_FP32) cand.push_back({-1, -1, 1, 0.0f});
+  if (c->uplan.ok && precision != CRAVA_SOLVE_FP32) cand.push_back({-1, -1, 1, 0.0f, 1});
   crava_gpu_tuning saved;
   crava_gpu_get_tuning(c, &saved);
   cudaEvent_t e0 = nullptr, e1 = nullptr;

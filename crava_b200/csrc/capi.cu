@@ -209,6 +209,36 @@ int unit_order(const crava_gpu_ctx *c, const crava_gpu_grids *g, float **ptr, in
   return i;
 }
 
+// Runs `n` independent per-grid steps, step i on lane i % lanes: the lane
+// streams are forked from the context's stream and joined back to it, so
+// kernels of different grids (e.g. an ALU-bound x pass and a shared-memory
+// bound z pass) share the SMs.
+template <typename F>
+int on_lanes(crava_gpu_ctx *c, int n, F step) {
+  const int L = c->lanes > 1 && c->lane_s[0] ? (c->lanes > 2 ? 2 : c->lanes) : 1;
+  if (L == 1) {
+    for (int i = 0; i < n; ++i) {
+      int rc = step(i);
+      if (rc) return rc;
+    }
+    return CRAVA_GPU_OK;
+  }
+  const cudaStream_t s0 = c->stream;
+  CRAVA_CUDA_TRY(cudaEventRecord(c->lane_fork, s0));
+  for (int k = 0; k < L; ++k) CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->lane_s[k], c->lane_fork, 0));
+  int rc = CRAVA_GPU_OK;
+  for (int i = 0; i < n && !rc; ++i) {
+    c->stream = c->lane_s[i % L];
+    rc = step(i);
+  }
+  c->stream = s0;
+  for (int k = 0; k < L; ++k) {
+    CRAVA_CUDA_TRY(cudaEventRecord(c->lane_join[k], c->lane_s[k]));
+    CRAVA_CUDA_TRY(cudaStreamWaitEvent(s0, c->lane_join[k], 0));
+  }
+  return rc;
+}
+
 int stage_event(crava_gpu_ctx *c, int i) {
   if (!c->capture) CRAVA_CUDA_TRY(cudaEventRecord(c->ev[i], c->stream));
   return CRAVA_GPU_OK;
@@ -231,8 +261,10 @@ int simulate_batches(crava_gpu_ctx *c, const float2 *const cv[6], const float *c
                                    c->counters, c->stream)))
         return rc;
     }
-    for (int k = 0; k < 3 * nr; ++k)
-      if ((rc = pass_inverse(c, out[3 * r0 + k], CRAVA_GRID_PARAMETER, post_mean[k % 3]))) return rc;
+    if ((rc = on_lanes(c, 3 * nr, [&](int k) {
+           return pass_inverse(c, out[3 * r0 + k], CRAVA_GRID_PARAMETER, post_mean[k % 3]);
+         })))
+      return rc;
   }
   return CRAVA_GPU_OK;
 }
@@ -285,26 +317,19 @@ int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids 
              int precision) {
   if (use_fused(c, precision)) return run_unit_fused(c, in, out, precision);
   const cudaStream_t s = c->stream;
-  const int nt = c->p.ntheta;
   int rc;
   CRAVA_CUDA_TRY(cudaMemsetAsync(c->counters, 0, sizeof(DevCounters), s));
   if ((rc = stage_event(c, 0))) return rc;
-  for (int q = 0; q < 3; ++q)
-    if ((rc = pass_forward(c, in->mu[q], out->mu[q], CRAVA_GRID_PARAMETER))) return rc;
-  for (int l = 0; l < nt; ++l)
-    if ((rc = pass_forward(c, in->data[l], out->data[l], CRAVA_GRID_DATA))) return rc;
-  for (int t = 0; t < 6; ++t)
-    if ((rc = pass_forward(c, in->cov[t], out->cov[t], CRAVA_GRID_COVARIANCE))) return rc;
-  if ((rc = pass_forward(c, in->err_corr, out->err_corr, CRAVA_GRID_COVARIANCE))) return rc;
+  float *src[kMaxUnitGrids], *dst[kMaxUnitGrids];
+  int type[kMaxUnitGrids];
+  const int G = unit_order(c, in, src, type);
+  unit_order(c, out, dst, type);
+  if ((rc = on_lanes(c, G, [&](int i) { return pass_forward(c, src[i], dst[i], type[i]); }))) return rc;
   if ((rc = stage_event(c, 1))) return rc;
   if ((rc = pass_solve(c, out, precision))) return rc;
   if ((rc = stage_event(c, 2))) return rc;
-  for (int q = 0; q < 3; ++q)
-    if ((rc = pass_inverse(c, out->mu[q], CRAVA_GRID_PARAMETER))) return rc;
-  for (int l = 0; l < nt; ++l)
-    if ((rc = pass_inverse(c, out->data[l], CRAVA_GRID_DATA))) return rc;
-  for (int t = 0; t < 6; ++t)
-    if ((rc = pass_inverse(c, out->cov[t], CRAVA_GRID_COVARIANCE))) return rc;
+  // the noise correlation (last in unit order) is not an output
+  if ((rc = on_lanes(c, G - 1, [&](int i) { return pass_inverse(c, dst[i], type[i]); }))) return rc;
   if ((rc = stage_event(c, 3))) return rc;
   c->timed = !c->capture;
   return CRAVA_GPU_OK;
@@ -376,6 +401,11 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   if (cudaMalloc(&c->counters, sizeof(DevCounters)) != cudaSuccess) return fail(CRAVA_GPU_ERR_ALLOC);
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+  for (auto &ls : c->lane_s)
+    if (cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+  if (cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+  for (auto &e : c->lane_join)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
   if ((rc = kz_tables_build(c->p, &c->tables, c->stream))) return fail(rc);
   if ((rc = kz_order_build(nzp, &c->tables, c->stream, &c->n_inverted))) return fail(rc);
   *out = c;
@@ -389,6 +419,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   else cudaDeviceSynchronize();
   if (c->s_out) cudaStreamSynchronize(c->s_out);
   if (c->s_in) cudaStreamSynchronize(c->s_in);
+  for (auto &ls : c->lane_s) if (ls) cudaStreamSynchronize(ls);
   fft_plans_destroy(&c->plans);
   kz_tables_free(&c->tables);
   cudaFree(c->counters);
@@ -399,6 +430,9 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->grid_ev) if (e) cudaEventDestroy(e);
   for (auto &e : c->slot_done) if (e) cudaEventDestroy(e);
+  for (auto &e : c->lane_join) if (e) cudaEventDestroy(e);
+  if (c->lane_fork) cudaEventDestroy(c->lane_fork);
+  for (auto &ls : c->lane_s) if (ls) cudaStreamDestroy(ls);
   for (auto &r : c->recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto &e : c->pool) cudaEventDestroy(e);
   if (c->s_in) cudaStreamDestroy(c->s_in);
