@@ -175,7 +175,7 @@ int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   if (!c || !t) return CRAVA_GPU_ERR_ARG;
   auto ok = [](int x) { return x == -1 || x == 0 || x == 8 || x == 16; };
   if (!ok(t->cols_y_tile) || !ok(t->cols_z_tile)) return CRAVA_GPU_ERR_ARG;
-  if (t->lanes != 1 && t->lanes != 2) return CRAVA_GPU_ERR_ARG;
+  if (t->lanes < 1 || t->lanes > crava_gpu_ctx::kMaxLanes) return CRAVA_GPU_ERR_ARG;
   c->plans.tile_y = t->cols_y_tile;
   c->plans.tile_z = t->cols_z_tile;
   c->fused = t->fused != 0;

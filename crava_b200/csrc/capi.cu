@@ -215,7 +215,9 @@ int unit_order(const crava_gpu_ctx *c, const crava_gpu_grids *g, float **ptr, in
 // bound z pass) share the SMs.
 template <typename F>
 int on_lanes(crava_gpu_ctx *c, int n, F step) {
-  const int L = c->lanes > 1 && c->lane_s[0] ? (c->lanes > 2 ? 2 : c->lanes) : 1;
+  const int L = c->lanes > 1 && c->lane_s[0]
+                    ? (c->lanes > crava_gpu_ctx::kMaxLanes ? crava_gpu_ctx::kMaxLanes : c->lanes)
+                    : 1;
   if (L == 1) {
     for (int i = 0; i < n; ++i) {
       int rc = step(i);

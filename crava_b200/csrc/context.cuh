@@ -49,9 +49,10 @@ struct crava_gpu_ctx {
   float2 *synt_H = nullptr;
   // independent transforms of a unit run on `lanes` streams (1: the
   // context's stream only), forked from and joined back to it
+  static constexpr int kMaxLanes = 4;
   int lanes = 2;
-  cudaStream_t lane_s[2] = {};
-  cudaEvent_t lane_fork = nullptr, lane_join[2] = {};
+  cudaStream_t lane_s[kMaxLanes] = {};
+  cudaEvent_t lane_fork = nullptr, lane_join[kMaxLanes] = {};
   // inverted kz planes (band flag set): the solve moves every spectrum of
   // their bins and only the covariance spectra of the others
   int n_inverted = 0;

@@ -259,14 +259,15 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
  * out-of-place pass, 8 or 16 the in-place pass; lengths without compiled
  * column kernels ignore it); fused: the fused unit kernels (1) or the
  * three passes (0); ms: one unit's measured time (autotune output only);
- * lanes: 2 lets the transforms of different grids overlap on two streams.
+ * lanes: more than 1 lets the transforms of different grids overlap on
+ * that many streams.
  * No counterpart in the reference (FFTW plans are fixed there). */
 typedef struct crava_gpu_tuning {
   int cols_y_tile;
   int cols_z_tile;
   int fused;
   float ms;
-  int lanes;   /* streams the unit's independent transforms run on (1 or 2) */
+  int lanes;   /* streams the unit's independent transforms run on (1..4) */
 } crava_gpu_tuning;
 int crava_gpu_get_tuning(crava_gpu_ctx *ctx, crava_gpu_tuning *out);
 int crava_gpu_set_tuning(crava_gpu_ctx *ctx, const crava_gpu_tuning *t);
