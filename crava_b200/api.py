@@ -64,6 +64,13 @@ class Tuning(C.Structure):
                 ("ms", C.c_float), ("lanes", C.c_int)]
 
 
+class GridHeader(C.Structure):
+    _fields_ = [("x0", C.c_double), ("y0", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+                ("nx", C.c_int), ("ny", C.c_int), ("il0", C.c_double), ("xl0", C.c_double),
+                ("il_step_x", C.c_double), ("il_step_y", C.c_double), ("xl_step_x", C.c_double),
+                ("xl_step_y", C.c_double), ("angle", C.c_double)]
+
+
 class Vintage(C.Structure):
     _fields_ = [("ctx", C.c_void_p), ("inp", Grids), ("out", Grids), ("precision", C.c_int),
                 ("nsim", C.c_int), ("seed", C.c_uint64), ("first_index", C.c_uint64),
@@ -116,6 +123,8 @@ SYMBOLS = {
     "crava_gpu_posterior_unit_host_async": ([C.c_void_p, C.POINTER(Grids), C.POINTER(Grids), C.c_int],
                                             C.c_int),
     "crava_gpu_host_wait": ([C.c_void_p], C.c_int),
+    "crava_gpu_crava_file_write": ([C.c_void_p, C.c_char_p, C.c_void_p, C.POINTER(GridHeader)], C.c_int),
+    "crava_gpu_crava_file_read": ([C.c_void_p, C.c_char_p, C.c_void_p, C.POINTER(GridHeader)], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -298,6 +307,18 @@ class Context:
         assert cxy.size == self.case.nxp * self.case.nyp
         check(self.lib.crava_gpu_fill_err_corr(self.handle, cxy.ctypes.data_as(F32P), grad_i, grad_j,
                                                _ptr(err)), "fill_err_corr")
+
+    def write_crava_file(self, path, grid, header: "GridHeader"):
+        """FFTGrid::writeCravaFile of a device grid."""
+        check(self.lib.crava_gpu_crava_file_write(self.handle, os.fsencode(path), _ptr(grid), C.byref(header)),
+              "crava_file_write")
+
+    def read_crava_file(self, path, grid) -> "GridHeader":
+        """FFTGrid::readCravaFile into a device grid; returns the header."""
+        h = GridHeader()
+        check(self.lib.crava_gpu_crava_file_read(self.handle, os.fsencode(path), _ptr(grid), C.byref(h)),
+              "crava_file_read")
+        return h
 
     def synt_seismic(self, alpha, beta, rho, outs, nx=0, ny=0):
         """Synthetic seismic of the real parameter grids into outs (one real

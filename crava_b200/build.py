@@ -31,6 +31,7 @@ SOURCES = {
     "loglik.cu": [],
     "forward.cu": [],
     "prior.cu": [],
+    "crava_file.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -53,6 +53,9 @@ struct crava_gpu_ctx {
   int lanes = 2;
   cudaStream_t lane_s[kMaxLanes] = {};
   cudaEvent_t lane_fork = nullptr, lane_join[kMaxLanes] = {};
+  // .crava file staging: pinned host and device buffers of one grid
+  float *file_host = nullptr;
+  float *file_dev = nullptr;
   // inverted kz planes (band flag set): the solve moves every spectrum of
   // their bins and only the covariance spectra of the others
   int n_inverted = 0;

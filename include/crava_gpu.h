@@ -396,6 +396,25 @@ int crava_gpu_fill_prior_cov(crava_gpu_ctx *ctx, const float *corr_xy, const flo
 int crava_gpu_fill_err_corr(crava_gpu_ctx *ctx, const float *corr_xy, float grad_i, float grad_j,
                             float *err_corr);
 
+/* Simbox geometry stored in the header of a .crava grid file
+ * (FFTGrid::writeCravaFile, src/fftgrid.cpp:2399-2433). */
+typedef struct crava_gpu_grid_header {
+  double x0, y0, dx, dy;
+  int nx, ny;
+  double il0, xl0, il_step_x, il_step_y, xl_step_x, xl_step_y, angle;
+} crava_gpu_grid_header;
+
+/* FFTGrid::writeCravaFile / readCravaFile (src/fftgrid.cpp:2399-2487) for a
+ * device grid (real padded layout): the reference's big-endian binary
+ * format, byte-swapped on the device, moved through a pinned staging buffer
+ * of the context.  read rejects a file whose rnxp, nyp, nzp differ from the
+ * context's (CRAVA_GPU_ERR_ARG, as the reference throws); header may be
+ * NULL.  Synchronous. */
+int crava_gpu_crava_file_write(crava_gpu_ctx *ctx, const char *path, const float *grid,
+                               const crava_gpu_grid_header *header);
+int crava_gpu_crava_file_read(crava_gpu_ctx *ctx, const char *path, float *grid,
+                              crava_gpu_grid_header *header);
+
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
 
