@@ -238,50 +238,61 @@ __global__ void __launch_bounds__(kThreads) k_rows_ip(const __grid_constant__ Ro
   const int tid = threadIdx.x;
   for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
   for (int i = tid; i <= N; i += kThreads) post[i] = a.post[i];
+  // One warp per row, lanes along the row: each thread issues all its
+  // loads (RPW rows x C columns) before the first use.
+  const int warp = tid >> 5, lane = tid & 31;
+  constexpr int NW = kThreads / 32;
+  constexpr int RPW = (kRR + NW - 1) / NW;
+  constexpr int C = (N + 31) / 32;
   if (DIR < 0) {
-    // batched loads: U independent loads in flight per thread
-    constexpr int U = 8;
-    for (int base = tid; base < kRR * N; base += kThreads * U) {
-      float2 v[U];
+    float2 v[RPW][C];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int idx = base + u * kThreads;
-        const int r = idx / N, m = idx % N;
-        v[u] = (idx < kRR * N && r < nrows)
-                   ? reinterpret_cast<const float2 *>(a.src + (row0 + r) * a.rnxp)[m]
-                   : make_float2(0.f, 0.f);
+    for (int i = 0; i < RPW; ++i) {
+      const int r = warp + i * NW;
+      const float2 *row = reinterpret_cast<const float2 *>(a.src + (row0 + r) * a.rnxp);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int m = lane + 32 * c;
+        v[i][c] = (r < nrows && m < N) ? row[m] : make_float2(0.f, 0.f);
       }
+    }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int idx = base + u * kThreads;
-        if (idx < kRR * N) buf[(idx % N) * P + idx / N] = v[u];
+    for (int i = 0; i < RPW; ++i) {
+      const int r = warp + i * NW;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int m = lane + 32 * c;
+        if (r < kRR && m < N) buf[m * P + r] = v[i][c];
       }
     }
   } else {
     __syncthreads();
     // Z'[k] = (X_k + conj X_{h-k}) + i W^{-k} (X_k - conj X_{h-k}); the
     // imaginary parts of DC and Nyquist are ignored, as a C2R does.
-    constexpr int U = 4;
-    for (int base = tid; base < kRR * N; base += kThreads * U) {
-      float2 xk[U], xm[U];
+    float2 xk[RPW][C], xm[RPW][C];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int idx = base + u * kThreads;
-        const int r = idx / N, k = idx % N;
-        if (idx < kRR * N && r < nrows) {
-          const float2 *X = reinterpret_cast<const float2 *>(a.grid + (row0 + r) * a.rnxp);
-          xk[u] = X[k];
-          xm[u] = X[N - k];
+    for (int i = 0; i < RPW; ++i) {
+      const int r = warp + i * NW;
+      const float2 *X = reinterpret_cast<const float2 *>(a.grid + (row0 + r) * a.rnxp);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int k = lane + 32 * c;
+        if (r < nrows && k < N) {
+          xk[i][c] = X[k];
+          xm[i][c] = X[N - k];
         } else {
-          xk[u] = xm[u] = make_float2(0.f, 0.f);
+          xk[i][c] = xm[i][c] = make_float2(0.f, 0.f);
         }
       }
+    }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int idx = base + u * kThreads;
-        if (idx >= kRR * N) continue;
-        const int r = idx / N, k = idx % N;
-        float2 x0 = xk[u], x1 = xm[u];
+    for (int i = 0; i < RPW; ++i) {
+      const int r = warp + i * NW;
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const int k = lane + 32 * c;
+        if (r >= kRR || k >= N) continue;
+        float2 x0 = xk[i][c], x1 = xm[i][c];
         if (k == 0) { x0.y = 0.f; x1.y = 0.f; }
         x1.y = -x1.y;
         const float2 e = cadd(x0, x1);
@@ -294,9 +305,8 @@ __global__ void __launch_bounds__(kThreads) k_rows_ip(const __grid_constant__ Ro
   }
   __syncthreads();
   stockham_ip<N, DIR, kRR, 1, P, kThreads>(buf, twl);
-  // One warp per row, lanes along the row: no division by the row length
+  // Output loops, one warp per row as well: no division by the row length
   // (N + 1 outputs) and one row address per warp and row.
-  const int warp = tid >> 5, lane = tid & 31;
   if (DIR < 0) {
     // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{h-k})/2, O = -i (Z_k - conj Z_{h-k})/2
     for (int r = warp; r < nrows; r += kThreads / 32) {
