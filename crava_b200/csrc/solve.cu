@@ -216,14 +216,17 @@ int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
   return CRAVA_GPU_OK;
 }
 
-// Blocks per SM of the solve kernel (register budget 255 / 128 / 80);
-// CRAVA_SOLVE_MINB overrides the default for measurements.
+// Blocks per SM of the solve kernel (register budget 255 / 128 / 80).  With
+// the right-hand-side loop kept rolled, two blocks (16 warps per SM, a few
+// hundred bytes of spills) measured fastest: FP64 1.52 ms, mixed 1.85 ms
+// at 256x256x512x5 against 1.86 / 2.19 with one block.  CRAVA_SOLVE_MINB
+// overrides the default for measurements.
 static int solve_minb() {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("CRAVA_SOLVE_MINB");
-    v = e ? atoi(e) : 1;
-    if (v < 1 || v > 3) v = 1;
+    v = e ? atoi(e) : 2;
+    if (v < 1 || v > 3) v = 2;
   }
   return v;
 }

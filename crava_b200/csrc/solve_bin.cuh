@@ -186,7 +186,9 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
   double2 mp[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
-#pragma unroll
+  // one right-hand side at a time, loop kept rolled: the register budget
+  // then allows two blocks per SM
+#pragma unroll 1
   for (int q = 0; q < 3; ++q) {
     double2 x[NT];
 #pragma unroll
@@ -348,7 +350,8 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
   double2 mp[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
-#pragma unroll
+  // rolled, as in the FP64 form
+#pragma unroll 1
   for (int q = 0; q < 3; ++q) {
     double2 ks[NT];
     float2 x0[NT][3];  // column 0 used; solver works on [.][3] arrays
