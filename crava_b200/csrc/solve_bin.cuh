@@ -47,8 +47,8 @@ __device__ __forceinline__ void prior_f(const float2 c6[6], const double v[6], f
 // the reference's failure rules applied to M / M00.  The reciprocals of the
 // diagonal of L are returned in rd (one division per column, reused by the
 // substitutions).
-template <int NT, typename T2, typename T>
-__device__ __forceinline__ bool cholesky(T2 *L, T *rd) {
+template <int NT, typename T2, typename T, typename LA>
+__device__ __forceinline__ bool cholesky(LA L, T *rd) {
   const T factor = L[0].x;
   if (!(factor > T(0))) return false;
   const T tol = (T)kTol * factor;
@@ -83,8 +83,17 @@ __device__ __forceinline__ bool cholesky(T2 *L, T *rd) {
 template <int NT, typename T2, typename T>
 __device__ __forceinline__ bool cholesky(T2 *L) {
   T rd[NT];
-  return cholesky<NT, T2, T>(L, rd);
+  return cholesky<NT, T2, T, T2 *>(L, rd);
 }
+
+// A per-thread triangle held in shared memory, entries STRIDE apart
+// (structure of arrays over the block: conflict-free, and it frees the
+// registers of the factor).
+template <typename T2, int STRIDE>
+struct SmemTri {
+  T2 *p;
+  __device__ __forceinline__ T2 &operator[](int t) const { return p[t * STRIDE]; }
+};
 
 // Solves L L^H X = B in place for the 3 columns of B.
 template <int NT, typename T2, typename T>
@@ -138,18 +147,17 @@ __device__ __forceinline__ bool fin2(float2 v) { return isfinite(v.x) && isfinit
 // K S the system M x = (K S)_q is solved, the posterior covariance entries
 // (p, q), p <= q, are updated (S_pq - (KS)_p^H x) and the mean correction
 // conj(x)^T (d - K mu) is accumulated.  Same algebra as the dense form.
-template <int NT>
-__device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float2 *__restrict__ wdk,
-                                               const float2 *__restrict__ e1k,
-                                               const float2 *__restrict__ e2k,
-                                               const float *__restrict__ e3k, bool inv,
-                                               float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+template <int NT, typename LA>
+__device__ __forceinline__ bool solve_bin_fp64_in(LA L, const SolveConsts &c, const float2 *__restrict__ wdk,
+                                                  const float2 *__restrict__ e1k,
+                                                  const float2 *__restrict__ e2k,
+                                                  const float *__restrict__ e3k, bool inv,
+                                                  float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
   const Sym3d S = prior_d(c6, c.var0);
   const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
   for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
   if (!inv) return false;
-  double2 L[NT * (NT + 1) / 2];
   {
     const double lam = fabs((double)ec.x);
     const double cc = 0.5 * (1.0 - (double)c.wnc) * lam;
@@ -182,7 +190,7 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
     }
   }
   double rd[NT];
-  if (!cholesky<NT, double2, double>(L, rd)) return true;
+  if (!cholesky<NT, double2, double, LA>(L, rd)) return true;
   double2 mp[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
@@ -264,18 +272,29 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
   return false;
 }
 
+template <int NT>
+__device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float2 *__restrict__ wdk,
+                                               const float2 *__restrict__ e1k,
+                                               const float2 *__restrict__ e2k,
+                                               const float *__restrict__ e3k, bool inv,
+                                               float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+  double2 L[NT * (NT + 1) / 2];
+  return solve_bin_fp64_in<NT, double2 *>(L, c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
+}
+
 // Mixed form, one right-hand side at a time: M is built in FP32 and
 // factorised in FP32 (Lf); M is also kept in FP64 (Md, lower triangle) for
 // the refinement residual.  For each column q of K S: x0 = M^-1 (KS)_q in
 // FP32, r = (KS)_q - M x0 in FP64, x = x0 + M^-1 r (FP32 solve of r, FP64
 // add); the posterior covariance entries S_pq - (KS)_p^H x and the mean
 // correction are formed in FP64.
-template <int NT>
-__device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const float2 *__restrict__ wdk,
-                                                const float2 *__restrict__ e1k,
-                                                const float2 *__restrict__ e2k,
-                                                const float *__restrict__ e3k, bool inv,
-                                                float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+template <int NT, typename LAF, typename LAD>
+__device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, const SolveConsts &c,
+                                                   const float2 *__restrict__ wdk,
+                                                   const float2 *__restrict__ e1k,
+                                                   const float2 *__restrict__ e2k,
+                                                   const float *__restrict__ e3k, bool inv,
+                                                   float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
   const Sym3d S = prior_d(c6, c.var0);
   float sf[6];
   prior_f(c6, c.var0, sf);
@@ -288,8 +307,6 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
     if (p > q) { int t = p; p = q; q = t; }
     return p == 0 ? (q == 0 ? sf[0] : q == 1 ? sf[3] : sf[4]) : p == 1 ? (q == 1 ? sf[1] : sf[5]) : sf[2];
   };
-  float2 Lf[NT * (NT + 1) / 2];
-  double2 Md[NT * (NT + 1) / 2];
   {
     const double lam = fabs((double)ec.x);
     const double cc = 0.5 * (1.0 - (double)c.wnc) * lam;
@@ -344,7 +361,7 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
     }
   }
   float rdf[NT];
-  if (!cholesky<NT, float2, float>(Lf, rdf)) return true;
+  if (!cholesky<NT, float2, float, LAF>(Lf, rdf)) return true;
 #pragma unroll
   for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
   double2 mp[3];
@@ -464,6 +481,17 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
 #pragma unroll
   for (int q = 0; q < 3; ++q) mu[q] = make_float2((float)mp[q].x, (float)mp[q].y);
   return false;
+}
+
+template <int NT>
+__device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const float2 *__restrict__ wdk,
+                                                const float2 *__restrict__ e1k,
+                                                const float2 *__restrict__ e2k,
+                                                const float *__restrict__ e3k, bool inv,
+                                                float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
+  float2 Lf[NT * (NT + 1) / 2];
+  double2 Md[NT * (NT + 1) / 2];
+  return solve_bin_mixed_in<NT, float2 *, double2 *>(Lf, Md, c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
 }
 
 // A band-gated bin: only the prior covariance is written (mu and the data
