@@ -77,6 +77,30 @@ def test_solve_vs_fp64_oracle(prec, tol, noise):
     assert max(errs) < tol, errs
 
 
+@pytest.mark.parametrize("angles", [(20.0,), (0.0, 5.0, 10.0, 15.0, 20.0, 25.0, 30.0, 35.0)])
+def test_solve_one_and_eight_angles(angles):
+    """The smallest and largest angle counts: FP32 form bit for bit with the
+    reference order, FP64 and mixed forms against the FP64 oracle."""
+    case = synth.make_case(12, 10, 32, angles, 0.1, seed=17)
+    sp = O.forward_spectra(case, "orc")
+    tables = O.kz_tables(case, "orc")
+    nx = case.nxp
+    ctx = api.Context(case)
+    ctx.set_kz_tables(tables)
+    mu, data, cov, err = _spectra_dev(case, sp)
+    ctx.posterior(mu, data, cov, err, api.FP32)
+    omu, ores, ocov, _ = O.posterior_fp32_tables(case, sp, tables, "orc")
+    for g, o in zip(mu + data + cov, omu + ores + ocov):
+        a = api.complex_view(g.cpu().numpy(), nx)
+        assert np.array_equal(a.view(np.uint64), O.complex_view(o, nx).view(np.uint64))
+    dmu, dres, dcov, _ = O.posterior_fp64(case, sp)
+    for prec, tol in [(api.FP64, 1e-7), (api.MIXED, 1e-5)]:
+        mu, data, cov, err = _spectra_dev(case, sp)
+        ctx.posterior(mu, data, cov, err, prec)
+        errs = [rel(api.complex_view(g.cpu().numpy(), nx), o) for g, o in zip(mu + data + cov, dmu + dres + dcov)]
+        assert max(errs) < tol, (prec, errs)
+
+
 def test_unit_vs_reference_unit():
     case = synth.config_small()
     ctx = api.Context(case)
