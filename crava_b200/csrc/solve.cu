@@ -196,7 +196,9 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
     // the FP64 factor lives in shared memory, one column of entries per thread
     extern __shared__ double2 lsm[];
     const sb::SmemTri<double2, kThreads> L{lsm + threadIdx.x};
-    fail = sb::solve_bin_fp64_in<NT>(L, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
+    const sb::SmemTri<double, kThreads> AS{
+        reinterpret_cast<double *>(lsm + kThreads * (NT * (NT + 1) / 2)) + threadIdx.x};
+    fail = sb::solve_bin_fp64_in<NT>(L, AS, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
                                      mu, d, c6, ec);
   } else if (PREC == 1 && kSolveFactorInSmem) {
     // the FP64 copy of M in shared memory, the FP32 factor in registers
@@ -222,7 +224,10 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
 template <int PREC, int MINB>
 int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
   dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
-  const size_t smem = kSolveFactorInSmem ? sizeof(double2) * kThreads * (nt * (nt + 1) / 2) : 0;
+  // FP64 form: factor (NT(NT+1)/2 double2) and A S (3 NT doubles) per thread
+  const size_t smem = !kSolveFactorInSmem ? 0
+                      : PREC == 0 ? (sizeof(double2) * (nt * (nt + 1) / 2) + sizeof(double) * 3 * nt) * kThreads
+                                  : sizeof(double2) * kThreads * (nt * (nt + 1) / 2);
   int rc;
 #define CRAVA_SOLVE_CASE(N)                                                          \
   case N:                                                                            \

@@ -147,8 +147,9 @@ __device__ __forceinline__ bool fin2(float2 v) { return isfinite(v.x) && isfinit
 // K S the system M x = (K S)_q is solved, the posterior covariance entries
 // (p, q), p <= q, are updated (S_pq - (KS)_p^H x) and the mean correction
 // conj(x)^T (d - K mu) is accumulated.  Same algebra as the dense form.
-template <int NT, typename LA>
-__device__ __forceinline__ bool solve_bin_fp64_in(LA L, const SolveConsts &c, const float2 *__restrict__ wdk,
+template <int NT, typename LA, typename AA>
+__device__ __forceinline__ bool solve_bin_fp64_in(LA L, AA AS, const SolveConsts &c,
+                                                  const float2 *__restrict__ wdk,
                                                   const float2 *__restrict__ e1k,
                                                   const float2 *__restrict__ e2k,
                                                   const float *__restrict__ e3k, bool inv,
@@ -158,18 +159,19 @@ __device__ __forceinline__ bool solve_bin_fp64_in(LA L, const SolveConsts &c, co
 #pragma unroll
   for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
   if (!inv) return false;
+  // AS = A S (row l at AS[3 l .. 3 l + 2]), formed once
+#pragma unroll
+  for (int l = 0; l < NT; ++l)
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+      AS[3 * l + p] = (double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
+                      (double)c.A[l][2] * sget(S, 2, p);
   {
     const double lam = fabs((double)ec.x);
     const double cc = 0.5 * (1.0 - (double)c.wnc) * lam;
 #pragma unroll
     for (int l = 0; l < NT; ++l) {
-      double as0 = 0, as1 = 0, as2 = 0;  // (A S)_l
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        as0 += (double)c.A[l][r] * sget(S, r, 0);
-        as1 += (double)c.A[l][r] * sget(S, r, 1);
-        as2 += (double)c.A[l][r] * sget(S, r, 2);
-      }
+      const double as0 = AS[3 * l], as1 = AS[3 * l + 1], as2 = AS[3 * l + 2];
       const float2 wl = __ldg(wdk + l), e1l = __ldg(e1k + l), e2l = __ldg(e2k + l);
 #pragma unroll
       for (int m = 0; m <= l; ++m) {
@@ -191,9 +193,19 @@ __device__ __forceinline__ bool solve_bin_fp64_in(LA L, const SolveConsts &c, co
   }
   double rd[NT];
   if (!cholesky<NT, double2, double, LA>(L, rd)) return true;
-  double2 mp[3];
+  // residual of the prior mean, v = d - K mu, formed once
+  double2 v[NT];
 #pragma unroll
-  for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
+  for (int l = 0; l < NT; ++l) {
+    double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      km = dadd(km, make_double2(c.A[l][r] * (double)mu[r].x, c.A[l][r] * (double)mu[r].y));
+    const float2 wl = __ldg(wdk + l);
+    km = dmul(make_double2(wl.x, wl.y), km);
+    v[l] = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
+  }
+  double2 dm[3];  // mean corrections X^H v
   // one right-hand side at a time, loop kept rolled: the register budget
   // then allows two blocks per SM
 #pragma unroll 1
@@ -201,8 +213,7 @@ __device__ __forceinline__ bool solve_bin_fp64_in(LA L, const SolveConsts &c, co
     double2 x[NT];
 #pragma unroll
     for (int l = 0; l < NT; ++l) {
-      const double as = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) +
-                        (double)c.A[l][2] * sget(S, 2, q);
+      const double as = AS[3 * l + q];
       const float2 wl = __ldg(wdk + l);
       x[l] = make_double2(wl.x * as, wl.y * as);
     }
@@ -229,46 +240,46 @@ __device__ __forceinline__ bool solve_bin_fp64_in(LA L, const SolveConsts &c, co
       }
       x[i] = make_double2(s.x * rd[i], s.y * rd[i]);
     }
-    // posterior covariance entries (p, q), p <= q
+    // mean correction conj(x)^T v
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < NT; ++l) acc = dadd(acc, dmulc(v[l], x[l]));
+    if (q == 0) dm[0] = acc;
+    else if (q == 1) dm[1] = acc;
+    else dm[2] = acc;
+    // posterior covariance entries (p, q), p <= q: S_pq - KS_p^H x with
+    // KS = diag(w) AS, i.e. S_pq - sum_l AS_lp u_l, u = conj(w) x
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      const float2 wl = __ldg(wdk + l);
+      x[l] = make_double2(wl.x * x[l].x + wl.y * x[l].y, wl.x * x[l].y - wl.y * x[l].x);
+    }
 #pragma unroll
     for (int p = 0; p <= q; ++p) {
       double2 r = make_double2(0.0, 0.0);
 #pragma unroll
       for (int l = 0; l < NT; ++l) {
-        const double as = (double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
-                          (double)c.A[l][2] * sget(S, 2, p);
-        const float2 wl = __ldg(wdk + l);
-        r = dadd(r, dmulc(x[l], make_double2(wl.x * as, wl.y * as)));  // conj(ks) x
+        const double as = AS[3 * l + p];
+        r.x += as * x[l].x;
+        r.y += as * x[l].y;
       }
       const int t = p == q ? p : (p == 0 ? (q == 1 ? 3 : 4) : 5);
       c6[t] = make_float2((float)(sget(S, p, q) - r.x), (float)(-r.y));
     }
-    // mean correction conj(x)^T (d - K mu)
-    double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int l = 0; l < NT; ++l) {
-      double2 km = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-        km = dadd(km, make_double2(c.A[l][r] * (double)mu[r].x, c.A[l][r] * (double)mu[r].y));
-      const float2 wl = __ldg(wdk + l);
-      km = dmul(make_double2(wl.x, wl.y), km);
-      const double2 v = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
-      acc = dadd(acc, dmulc(v, x[l]));
-    }
-    mp[q] = dadd(mp[q], acc);
   }
+  // residual d - K (mu + dm) = v - K dm; posterior mean mu + dm
 #pragma unroll
   for (int l = 0; l < NT; ++l) {
     double2 km = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * mp[r].x, c.A[l][r] * mp[r].y));
+    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * dm[r].x, c.A[l][r] * dm[r].y));
     const float2 wl = __ldg(wdk + l);
     km = dmul(make_double2(wl.x, wl.y), km);
-    d[l] = make_float2((float)((double)d[l].x - km.x), (float)((double)d[l].y - km.y));
+    d[l] = make_float2((float)(v[l].x - km.x), (float)(v[l].y - km.y));
   }
 #pragma unroll
-  for (int q = 0; q < 3; ++q) mu[q] = make_float2((float)mp[q].x, (float)mp[q].y);
+  for (int q = 0; q < 3; ++q)
+    mu[q] = make_float2((float)((double)mu[q].x + dm[q].x), (float)((double)mu[q].y + dm[q].y));
   return false;
 }
 
@@ -279,7 +290,8 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
                                                const float *__restrict__ e3k, bool inv,
                                                float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
   double2 L[NT * (NT + 1) / 2];
-  return solve_bin_fp64_in<NT, double2 *>(L, c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
+  double AS[3 * NT];
+  return solve_bin_fp64_in<NT, double2 *, double *>(L, AS, c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
 }
 
 // Mixed form, one right-hand side at a time: M is built in FP32 and
