@@ -32,9 +32,8 @@ namespace {
 constexpr int kThreads = 256;
 using sb::tri;
 // Keep the FP64 Cholesky factor (FP64 form) or the FP64 copy of M (mixed
-// form) in shared memory, one entry column per thread, instead of in
-// registers: fewer spills at two blocks per SM (FP64 1.52 -> 1.45 ms, mixed
-// 1.85 -> 1.81 ms at 256x256x512x5).
+// form), and A S, in shared memory, one entry column per thread, instead of
+// in registers: fewer spills at two blocks per SM.
 constexpr bool kSolveFactorInSmem = true;
 
 // ------------------------------------------------------------------ tables
@@ -205,7 +204,9 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
     extern __shared__ double2 lsm[];
     float2 Lf[NT * (NT + 1) / 2];
     const sb::SmemTri<double2, kThreads> Md{lsm + threadIdx.x};
-    fail = sb::solve_bin_mixed_in<NT>(&Lf[0], Md, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o,
+    const sb::SmemTri<double, kThreads> AS{
+        reinterpret_cast<double *>(lsm + kThreads * (NT * (NT + 1) / 2)) + threadIdx.x};
+    fail = sb::solve_bin_mixed_in<NT>(&Lf[0], Md, AS, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o,
                                       inv, mu, d, c6, ec);
   } else {
     fail = sb::solve_bin<NT, PREC>(a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
@@ -225,9 +226,10 @@ template <int PREC, int MINB>
 int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
   dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
   // FP64 form: factor (NT(NT+1)/2 double2) and A S (3 NT doubles) per thread
+  // per thread: the FP64 factor (FP64 form) or the FP64 copy of M (mixed
+  // form), NT(NT+1)/2 double2, and A S, 3 NT doubles
   const size_t smem = !kSolveFactorInSmem ? 0
-                      : PREC == 0 ? (sizeof(double2) * (nt * (nt + 1) / 2) + sizeof(double) * 3 * nt) * kThreads
-                                  : sizeof(double2) * kThreads * (nt * (nt + 1) / 2);
+                      : (sizeof(double2) * (nt * (nt + 1) / 2) + sizeof(double) * 3 * nt) * kThreads;
   int rc;
 #define CRAVA_SOLVE_CASE(N)                                                          \
   case N:                                                                            \

@@ -300,8 +300,8 @@ __device__ __forceinline__ bool solve_bin_fp64(const SolveConsts &c, const float
 // FP32, r = (KS)_q - M x0 in FP64, x = x0 + M^-1 r (FP32 solve of r, FP64
 // add); the posterior covariance entries S_pq - (KS)_p^H x and the mean
 // correction are formed in FP64.
-template <int NT, typename LAF, typename LAD>
-__device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, const SolveConsts &c,
+template <int NT, typename LAF, typename LAD, typename AA>
+__device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, AA AS, const SolveConsts &c,
                                                    const float2 *__restrict__ wdk,
                                                    const float2 *__restrict__ e1k,
                                                    const float2 *__restrict__ e2k,
@@ -319,19 +319,23 @@ __device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, const SolveCo
     if (p > q) { int t = p; p = q; q = t; }
     return p == 0 ? (q == 0 ? sf[0] : q == 1 ? sf[3] : sf[4]) : p == 1 ? (q == 1 ? sf[1] : sf[5]) : sf[2];
   };
+  // AS = A S in FP64 (row l at AS[3 l .. 3 l + 2]), formed once
+#pragma unroll
+  for (int l = 0; l < NT; ++l)
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+      AS[3 * l + p] = (double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
+                      (double)c.A[l][2] * sget(S, 2, p);
   {
     const double lam = fabs((double)ec.x);
     const double cc = 0.5 * (1.0 - (double)c.wnc) * lam;
     const float ccf = (float)cc;
 #pragma unroll
     for (int l = 0; l < NT; ++l) {
-      double as0 = 0, as1 = 0, as2 = 0;
+      const double as0 = AS[3 * l], as1 = AS[3 * l + 1], as2 = AS[3 * l + 2];
       float af0 = 0.f, af1 = 0.f, af2 = 0.f;
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
-        as0 += (double)c.A[l][r] * sget(S, r, 0);
-        as1 += (double)c.A[l][r] * sget(S, r, 1);
-        as2 += (double)c.A[l][r] * sget(S, r, 2);
         af0 += c.A[l][r] * sgf(r, 0);
         af1 += c.A[l][r] * sgf(r, 1);
         af2 += c.A[l][r] * sgf(r, 2);
@@ -376,9 +380,19 @@ __device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, const SolveCo
   if (!cholesky<NT, float2, float, LAF>(Lf, rdf)) return true;
 #pragma unroll
   for (int t = 0; t < 6; ++t) c6[t] = make_float2((float)sget(S, pa[t], pb[t]), 0.f);
-  double2 mp[3];
+  // residual of the prior mean, v = d - K mu (FP64), formed once
+  double2 v[NT];
 #pragma unroll
-  for (int q = 0; q < 3; ++q) mp[q] = make_double2(mu[q].x, mu[q].y);
+  for (int l = 0; l < NT; ++l) {
+    double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      km = dadd(km, make_double2(c.A[l][r] * (double)mu[r].x, c.A[l][r] * (double)mu[r].y));
+    const float2 wl = __ldg(wdk + l);
+    km = dmul(make_double2(wl.x, wl.y), km);
+    v[l] = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
+  }
+  double2 dm[3];  // mean corrections X^H v
   // rolled, as in the FP64 form
 #pragma unroll 1
   for (int q = 0; q < 3; ++q) {
@@ -386,8 +400,7 @@ __device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, const SolveCo
     float2 x0[NT][3];  // column 0 used; solver works on [.][3] arrays
 #pragma unroll
     for (int l = 0; l < NT; ++l) {
-      const double as = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) +
-                        (double)c.A[l][2] * sget(S, 2, q);
+      const double as = AS[3 * l + q];
       const float2 wl = __ldg(wdk + l);
       ks[l] = make_double2(wl.x * as, wl.y * as);
       x0[l][0] = make_float2((float)ks[l].x, (float)ks[l].y);
@@ -453,45 +466,46 @@ __device__ __forceinline__ bool solve_bin_mixed_in(LAF Lf, LAD Md, const SolveCo
 #pragma unroll
     for (int l = 0; l < NT; ++l)
       x[l] = make_double2((double)x0[l][0].x + (double)x0[l][1].x, (double)x0[l][0].y + (double)x0[l][1].y);
-    // FP64 Schur update of the entries (p, q), p <= q
+    // mean correction conj(x)^T v
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < NT; ++l) acc = dadd(acc, dmulc(v[l], x[l]));
+    if (q == 0) dm[0] = acc;
+    else if (q == 1) dm[1] = acc;
+    else dm[2] = acc;
+    // FP64 Schur update of the entries (p, q), p <= q: S_pq - sum_l AS_lp u_l,
+    // u = conj(w) x
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      const float2 wl = __ldg(wdk + l);
+      x[l] = make_double2(wl.x * x[l].x + wl.y * x[l].y, wl.x * x[l].y - wl.y * x[l].x);
+    }
 #pragma unroll
     for (int p = 0; p <= q; ++p) {
       double2 r = make_double2(0.0, 0.0);
 #pragma unroll
       for (int l = 0; l < NT; ++l) {
-        const double as = (double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
-                          (double)c.A[l][2] * sget(S, 2, p);
-        const float2 wl = __ldg(wdk + l);
-        r = dadd(r, dmulc(x[l], make_double2(wl.x * as, wl.y * as)));
+        const double as = AS[3 * l + p];
+        r.x += as * x[l].x;
+        r.y += as * x[l].y;
       }
       const int t = p == q ? p : (p == 0 ? (q == 1 ? 3 : 4) : 5);
       c6[t] = make_float2((float)(sget(S, p, q) - r.x), (float)(-r.y));
     }
-    double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int l = 0; l < NT; ++l) {
-      double2 km = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-        km = dadd(km, make_double2(c.A[l][r] * (double)mu[r].x, c.A[l][r] * (double)mu[r].y));
-      const float2 wl = __ldg(wdk + l);
-      km = dmul(make_double2(wl.x, wl.y), km);
-      const double2 v = make_double2((double)d[l].x - km.x, (double)d[l].y - km.y);
-      acc = dadd(acc, dmulc(v, x[l]));
-    }
-    mp[q] = dadd(mp[q], acc);
   }
+  // residual d - K (mu + dm) = v - K dm; posterior mean mu + dm (FP64)
 #pragma unroll
   for (int l = 0; l < NT; ++l) {
     double2 km = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * mp[r].x, c.A[l][r] * mp[r].y));
+    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * dm[r].x, c.A[l][r] * dm[r].y));
     const float2 wl = __ldg(wdk + l);
     km = dmul(make_double2(wl.x, wl.y), km);
-    d[l] = make_float2((float)((double)d[l].x - km.x), (float)((double)d[l].y - km.y));
+    d[l] = make_float2((float)(v[l].x - km.x), (float)(v[l].y - km.y));
   }
 #pragma unroll
-  for (int q = 0; q < 3; ++q) mu[q] = make_float2((float)mp[q].x, (float)mp[q].y);
+  for (int q = 0; q < 3; ++q)
+    mu[q] = make_float2((float)((double)mu[q].x + dm[q].x), (float)((double)mu[q].y + dm[q].y));
   return false;
 }
 
@@ -503,7 +517,9 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
                                                 float2 mu[3], float2 d[NT], float2 c6[6], float2 ec) {
   float2 Lf[NT * (NT + 1) / 2];
   double2 Md[NT * (NT + 1) / 2];
-  return solve_bin_mixed_in<NT, float2 *, double2 *>(Lf, Md, c, wdk, e1k, e2k, e3k, inv, mu, d, c6, ec);
+  double AS[3 * NT];
+  return solve_bin_mixed_in<NT, float2 *, double2 *, double *>(Lf, Md, AS, c, wdk, e1k, e2k, e3k, inv, mu, d,
+                                                               c6, ec);
 }
 
 // A band-gated bin: only the prior covariance is written (mu and the data
