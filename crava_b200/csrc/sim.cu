@@ -55,33 +55,43 @@ __device__ __forceinline__ float2 normal2(uint64_t seed, uint64_t stream, uint64
   return make_float2(rad * co, rad * s);
 }
 
-// The value FFTGrid::fillInComplexNoise puts in bin i (rules of
-// src/fftgrid.cpp:1221-1257, including the parity test on the linear index
-// for the last x plane).  Each independent draw is made at the counter of
-// the bin the reference draws it for; a mirrored bin re-draws its partner.
-__device__ __forceinline__ float2 noise_bin(long long i, int cnxp, int nyp, int nzp,
-                                            uint64_t seed, uint64_t stream) {
-  const float sd = 0.70710678118654752440f;  // float(1/sqrt(2.0))
+// Where the noise of bin i comes from, under FFTGrid::fillInComplexNoise's
+// rules (src/fftgrid.cpp:1221-1257, including the parity test on the
+// linear index for the last x plane): each independent draw is made at the
+// counter of the bin the reference draws it for; a mirrored bin re-draws
+// its partner.  kind 0: an independent complex value, 1: a self-conjugate
+// bin (real), 2: the conjugate of the partner's value.
+struct NoiseSite {
+  uint64_t ctr;
+  int kind;
+};
+
+__device__ __forceinline__ NoiseSite noise_site(long long i, int cnxp, int nyp, int nzp) {
   const long long xs = i % cnxp;
   if (xs == 0 || (xs == cnxp - 1 && (i % 2) == 1)) {
     const long long jk = (i - xs) / cnxp;
     const long long j = jk % nyp, k = jk / nyp;
     const long long jc = j == 0 ? 0 : nyp - j, kc = k == 0 ? 0 : nzp - k;
     const long long jkc = jc + kc * nyp;
-    if (jkc == jk) {
-      float2 n = normal2(seed, stream, (uint64_t)i);
-      return make_float2(n.x, 0.0f);
-    }
-    if (jkc > jk) {
-      float2 n = normal2(seed, stream, (uint64_t)i);
-      return make_float2(sd * n.x, sd * n.y);
-    }
-    const long long ci = jkc * cnxp + xs;
-    float2 n = normal2(seed, stream, (uint64_t)ci);
-    return make_float2(sd * n.x, -(sd * n.y));
+    if (jkc == jk) return NoiseSite{(uint64_t)i, 1};
+    if (jkc > jk) return NoiseSite{(uint64_t)i, 0};
+    return NoiseSite{(uint64_t)(jkc * cnxp + xs), 2};
   }
-  float2 n = normal2(seed, stream, (uint64_t)i);
+  return NoiseSite{(uint64_t)i, 0};
+}
+
+__device__ __forceinline__ float2 noise_value(NoiseSite site, uint64_t seed, uint64_t stream) {
+  const float sd = 0.70710678118654752440f;  // float(1/sqrt(2.0))
+  const float2 n = normal2(seed, stream, site.ctr);
+  if (site.kind == 1) return make_float2(n.x, 0.0f);
+  if (site.kind == 2) return make_float2(sd * n.x, -(sd * n.y));
   return make_float2(sd * n.x, sd * n.y);
+}
+
+// The value FFTGrid::fillInComplexNoise puts in bin i.
+__device__ __forceinline__ float2 noise_bin(long long i, int cnxp, int nyp, int nzp,
+                                            uint64_t seed, uint64_t stream) {
+  return noise_value(noise_site(i, cnxp, nyp, nzp), seed, stream);
 }
 
 __global__ void __launch_bounds__(kThreads) k_noise(float2 *g, long long csize, int cnxp, int nyp,
@@ -228,10 +238,11 @@ __global__ void __launch_bounds__(kThreads) k_noise_filter_multi(const __grid_co
   P[2][1] = make_float2(P[1][2].x, -P[1][2].y);
   const bool ok = chol3_ref(P) == 0;
   const uint64_t stream0 = a.stream0 + (a.epoch ? a.epoch_mul * *a.epoch : 0ull);
+  const NoiseSite site = noise_site(i, a.cnxp, a.nyp, a.nzp);  // once per bin
   for (int r = 0; r < a.nreal; ++r) {
     float2 z[3], o[3];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) z[q] = noise_bin(i, a.cnxp, a.nyp, a.nzp, a.seed, stream0 + 3ull * r + q);
+    for (int q = 0; q < 3; ++q) z[q] = noise_value(site, a.seed, stream0 + 3ull * r + q);
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
       o[p] = make_float2(0.0f, 0.0f);
