@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-forward", action="store_true")
+    ap.add_argument("--no-state4d", action="store_true")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
     return ap.parse_args()
@@ -325,6 +326,84 @@ def run_prior_fill(ctx, case, dst, dev, stream, max_over_ranks):
             "equal_to_uploaded_grids": same}
 
 
+def run_state4d(ctx, case, dev, stream, max_over_ranks, peak):
+    """The time-lapse state (State4D split / evolve / merge and the whole
+    ModelGeneral::advanceTime step) on 27 state grids of the unit's size:
+    device time per kernel and its HBM rate on the algorithmic bytes
+    (split reads 36 and writes 27 spectra per bin, evolve reads 28 and
+    writes 27, merge reads 27 and writes 9; 8 bytes each)."""
+    import numpy as np
+    import torch
+
+    from crava_b200 import api
+
+    nxp, nyp, nzp = case.nxp, case.nyp, case.nzp
+    shape = (nzp, nyp, 2 * (nxp // 2 + 1))
+    bins = shape[0] * shape[1] * shape[2] // 2
+    gen = torch.Generator(device=dev).manual_seed(5)
+    P, Q = (0, 0, 0, 1, 1, 2), (0, 1, 2, 1, 2, 2)
+    unit = (0, 3, 4, 1, 5, 2)
+    rng = np.random.default_rng(5)
+    G = rng.standard_normal((6, 6))
+    S0 = G @ G.T / 6.0 + 0.5 * np.eye(6)
+    E = np.eye(6) + 0.05 * rng.standard_normal((6, 6))
+    cm = rng.standard_normal(6)
+    Gc = rng.standard_normal((6, 6))
+    cc = Gc @ Gc.T / 6.0 + 0.1 * np.eye(6)
+    with torch.cuda.stream(stream):
+        lam = torch.empty(shape, device=dev)
+        ctx.fill_gen_exp_corr(nxp / 4.0, nyp / 4.0, 6.0, 0.0, 0.0, lam)
+        ctx.fft_r2c(lam, api.COVARIANCE)
+
+        def field():
+            g = torch.randn(shape, device=dev, generator=gen)
+            ctx.fft_r2c(g, api.PARAMETER)
+            return g
+
+        state = {"ms": [field() for _ in range(3)], "md": [field() for _ in range(3)],
+                 "ss": [lam * float(S0[P[r], Q[r]]) for r in range(6)],
+                 "dd": [lam * float(S0[P[r] + 3, Q[r] + 3]) for r in range(6)],
+                 "sd": [lam * float(S0[l, k + 3]) for l in range(3) for k in range(3)]}
+        C = S0[:3, :3] + S0[3:, 3:] + S0[3:, :3] + S0[:3, 3:]
+        mu = [field() for _ in range(3)]
+        cov = [None] * 6
+        for r in range(6):
+            cov[unit[r]] = lam * float(0.6 * C[P[r], Q[r]])
+        work = torch.empty(shape, device=dev)
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=5):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        return max_over_ranks(ev0.elapsed_time(ev1) / reps)
+
+    shortcuts = ctx.state4d_split(state, mu, cov)
+    res = {}
+    for name, fn, nb in [("split", lambda: ctx.state4d_split(state, mu, cov), 63),
+                         ("evolve", lambda: ctx.state4d_evolve(state, E, cm, cc, lam), 55),
+                         ("merge", lambda: ctx.state4d_merge(state, mu, cov), 36)]:
+        ms = timed(fn)
+        gbs = nb * 8 * bins / (ms * 1e-3) / 1e9
+        res[name] = {"ms": round(ms, 4), "bytes_per_launch": nb * 8 * bins, "GB/s": round(gbs, 1),
+                     "frac_of_peak": round(gbs / peak, 4)}
+    # split runs synchronously (it reads back its shortcut count); time the
+    # whole step through advance_time, which also reads it back once
+    step_ms = timed(lambda: ctx.advance_time(state, 1, nxp, nyp, E, cm, cc, mu, cov, work), reps=3)
+    del state, mu, cov, work, lam
+    return {"workload": "State4D split / evolve / merge and advanceTime, 27 state grids %dx%dx%d"
+                        % (nxp, nyp, nzp),
+            "kernels": res, "advance_time_ms": round(step_ms, 4), "split_shortcut_bins": shortcuts,
+            "peak_GB/s": peak}
+
+
 def run_forward(ctx, case, src, dev, stream, max_over_ranks):
     """Synthetic seismic (Crava::computeSyntSeismic) of the three parameter
     grids for all angles: device time per call and HBM rate against the
@@ -560,6 +639,15 @@ def run_own(args):
 
     prior = run_prior_fill(ctx, case, dst, dev, stream, max_over_ranks)
 
+    s4 = None
+    if not args.no_state4d:
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                hbm_peak = json.load(f).get("hbm_gbs") or 6650.0
+        except Exception:
+            hbm_peak = 6650.0
+        s4 = run_state4d(ctx, case, dev, stream, max_over_ranks, hbm_peak)
+
     fwd = None
     if not args.no_forward:
         fwd = run_forward(ctx, case, src, dev, stream, max_over_ranks)
@@ -640,6 +728,7 @@ def run_own(args):
         "adjoint": adjoint,
         "forward_model": fwd,
         "prior_fill": prior,
+        "state4d": s4,
         "profiling_pass_ms_per_step": ms_serial,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,

@@ -53,6 +53,12 @@ class KernelProfile(C.Structure):
                 ("bytes_per_launch", C.c_double)]
 
 
+class State4DGrids(C.Structure):
+    """crava_gpu_state4d: the static/dynamic time-lapse state (State4D)."""
+    _fields_ = [("mu_static", C.c_void_p * 3), ("mu_dynamic", C.c_void_p * 3),
+                ("cov_ss", C.c_void_p * 6), ("cov_dd", C.c_void_p * 6), ("cov_sd", C.c_void_p * 9)]
+
+
 class Stats(C.Structure):
     _fields_ = [("chol_fail_bins", C.c_longlong), ("nonfinite_bins", C.c_longlong),
                 ("ms_forward", C.c_float), ("ms_solve", C.c_float),
@@ -125,6 +131,17 @@ SYMBOLS = {
     "crava_gpu_host_wait": ([C.c_void_p], C.c_int),
     "crava_gpu_crava_file_write": ([C.c_void_p, C.c_char_p, C.c_void_p, C.POINTER(GridHeader)], C.c_int),
     "crava_gpu_crava_file_read": ([C.c_void_p, C.c_char_p, C.c_void_p, C.POINTER(GridHeader)], C.c_int),
+    "crava_gpu_state4d_merge": ([C.c_void_p, C.POINTER(State4DGrids), C.POINTER(C.c_void_p),
+                                 C.POINTER(C.c_void_p)], C.c_int),
+    "crava_gpu_state4d_split": ([C.c_void_p, C.POINTER(State4DGrids), C.POINTER(C.c_void_p),
+                                 C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)], C.c_int),
+    "crava_gpu_fill_gen_exp_corr": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_float,
+                                     C.c_float, C.c_void_p], C.c_int),
+    "crava_gpu_state4d_evolve": ([C.c_void_p, C.POINTER(State4DGrids), F64P, F64P, F64P, C.c_void_p],
+                                 C.c_int),
+    "crava_gpu_state4d_advance_time": ([C.c_void_p, C.POINTER(State4DGrids), C.c_int, C.c_int, C.c_int,
+                                        F64P, F64P, F64P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                        C.c_void_p, C.POINTER(C.c_longlong)], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -307,6 +324,66 @@ class Context:
         assert cxy.size == self.case.nxp * self.case.nyp
         check(self.lib.crava_gpu_fill_err_corr(self.handle, cxy.ctypes.data_as(F32P), grad_i, grad_j,
                                                _ptr(err)), "fill_err_corr")
+
+    # ---- time-lapse state (State4D, src/state4d.cpp) -------------------
+    @staticmethod
+    def _state(state) -> State4DGrids:
+        """state: dict with 'ms', 'md' (3 each), 'ss', 'dd' (6 each) and 'sd'
+        (9) device grids holding Fourier-domain spectra."""
+        st = State4DGrids()
+        for key, field, n in (("ms", "mu_static", 3), ("md", "mu_dynamic", 3), ("ss", "cov_ss", 6),
+                              ("dd", "cov_dd", 6), ("sd", "cov_sd", 9)):
+            assert len(state[key]) == n, key
+            setattr(st, field, (C.c_void_p * n)(*[g.data_ptr() for g in state[key]]))
+        return st
+
+    def state4d_merge(self, state, mu, cov):
+        """State4D::merge (mu None: mergeCov) into Fourier-domain grids."""
+        st = self._state(state)
+        m = (C.c_void_p * 3)(*[g.data_ptr() for g in mu]) if mu is not None else None
+        c = (C.c_void_p * 6)(*[g.data_ptr() for g in cov])
+        check(self.lib.crava_gpu_state4d_merge(self.handle, C.byref(st), m, c), "state4d_merge")
+
+    def state4d_split(self, state, mu, cov) -> int:
+        """State4D::split of the inverted current state; returns the bins
+        whose Cholesky failed (prior kept)."""
+        st = self._state(state)
+        m = (C.c_void_p * 3)(*[g.data_ptr() for g in mu])
+        c = (C.c_void_p * 6)(*[g.data_ptr() for g in cov])
+        n = C.c_longlong(0)
+        check(self.lib.crava_gpu_state4d_split(self.handle, C.byref(st), m, c, C.byref(n)), "state4d_split")
+        return n.value
+
+    def fill_gen_exp_corr(self, rx, ry, rz, grad_i, grad_j, grid):
+        """FFTGrid::fillInGenExpCorr on the device."""
+        check(self.lib.crava_gpu_fill_gen_exp_corr(self.handle, rx, ry, rz, grad_i, grad_j, _ptr(grid)),
+              "fill_gen_exp_corr")
+
+    def state4d_evolve(self, state, evolution, mean_correction, cov_correction, lam):
+        """State4D::evolve with the transformed time-increment correlation."""
+        st = self._state(state)
+        E, cm, cc = (np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+                     for x in (evolution, mean_correction, cov_correction))
+        assert E.size == 36 and cm.size == 6 and cc.size == 36
+        check(self.lib.crava_gpu_state4d_evolve(self.handle, C.byref(st), E.ctypes.data_as(F64P),
+                                                cm.ctypes.data_as(F64P), cc.ctypes.data_as(F64P), _ptr(lam)),
+              "state4d_evolve")
+
+    def advance_time(self, state, time_step, nx, ny, evolution, mean_correction, cov_correction,
+                     mu, cov, lambda_work) -> int:
+        """ModelGeneral::advanceTime: split, evolve, merge, back to the time
+        domain.  Returns the split's shortcut bins."""
+        st = self._state(state)
+        E, cm, cc = (np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+                     for x in (evolution, mean_correction, cov_correction))
+        assert E.size == 36 and cm.size == 6 and cc.size == 36
+        m = (C.c_void_p * 3)(*[g.data_ptr() for g in mu])
+        c = (C.c_void_p * 6)(*[g.data_ptr() for g in cov])
+        n = C.c_longlong(0)
+        check(self.lib.crava_gpu_state4d_advance_time(
+            self.handle, C.byref(st), time_step, nx, ny, E.ctypes.data_as(F64P), cm.ctypes.data_as(F64P),
+            cc.ctypes.data_as(F64P), m, c, _ptr(lambda_work), C.byref(n)), "advance_time")
+        return n.value
 
     def write_crava_file(self, path, grid, header: "GridHeader"):
         """FFTGrid::writeCravaFile of a device grid."""

@@ -32,6 +32,7 @@ SOURCES = {
     "forward.cu": [],
     "prior.cu": [],
     "crava_file.cu": [],
+    "state4d.cu": ["-fmad=false"],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -13,6 +13,7 @@
 // getNextErrorVariance (src/crava.cpp:1297-1334).
 #include <math.h>
 
+#include "lib_matr_ref.cuh"
 #include "solve.cuh"
 
 namespace crava {
@@ -28,80 +29,6 @@ struct RefArgs {
   long long csize, plane;
   DevCounters *counters;
 };
-
-template <int NT>
-__device__ __forceinline__ int chol_ref(float2 (*m)[NT]) {
-  float2 lr;
-  float help;
-  float factor = m[0][0].x;
-  if (factor <= 0) return 1;
-#pragma unroll
-  for (int i = 0; i < NT; ++i)
-#pragma unroll
-    for (int j = 0; j < NT; ++j) { m[i][j].x = m[i][j].x / factor; m[i][j].y = m[i][j].y / factor; }
-#pragma unroll
-  for (int i = 0; i < NT; ++i) {
-    if ((double)m[i][i].x <= 1e-20) return 1;
-#pragma unroll
-    for (int j = 0; j < i; ++j) {
-      lr.x = 0.0f; lr.y = 0.0f;
-#pragma unroll
-      for (int k = 0; k < j; ++k) {
-        lr.x += (m[i][k].x * m[j][k].x) + (m[i][k].y * m[j][k].y);
-        lr.y += -(m[i][k].x * m[j][k].y) + (m[i][k].y * m[j][k].x);
-      }
-      help = m[j][j].x * m[j][j].x + m[j][j].y * m[j][j].y;
-      m[i][j].x = ((m[i][j].x - lr.x) * m[j][j].x + (m[i][j].y - lr.y) * m[j][j].y) / help;
-      m[i][j].y = ((m[i][j].y - lr.y) * m[j][j].x - (m[i][j].x - lr.x) * m[j][j].y) / help;
-    }
-    lr.x = 0.0f;
-#pragma unroll
-    for (int k = 0; k < i; ++k) lr.x += (m[i][k].x * m[i][k].x) + (m[i][k].y * m[i][k].y);
-    lr.x = m[i][i].x - lr.x;
-    if ((double)lr.x <= 1e-20) return 1;
-    m[i][i].x = sqrtf(lr.x);
-    m[i][i].y = 0.0f;
-  }
-  const float sf = sqrtf(factor);
-#pragma unroll
-  for (int i = 0; i < NT; ++i)
-#pragma unroll
-    for (int j = 0; j <= i; ++j) { m[i][j].x *= sf; m[i][j].y *= sf; }
-  return 0;
-}
-
-template <int NT>
-__device__ __forceinline__ void axeqb_ref(float2 (*L)[NT], float2 (*B)[3]) {
-  float2 lx;
-  float help;
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-#pragma unroll
-    for (int i = 0; i < NT; ++i) {
-      lx = B[i][c];
-#pragma unroll
-      for (int j = 0; j < i; ++j) {
-        lx.x -= (B[j][c].x * L[i][j].x - B[j][c].y * L[i][j].y);
-        lx.y -= (B[j][c].y * L[i][j].x + B[j][c].x * L[i][j].y);
-      }
-      help = (L[i][i].x * L[i][i].x + L[i][i].y * L[i][i].y);
-      B[i][c].x = (lx.x * L[i][i].x + lx.y * L[i][i].y) / help;
-      B[i][c].y = (lx.y * L[i][i].x - lx.x * L[i][i].y) / help;
-    }
-#pragma unroll
-    for (int i = NT - 1; i >= 0; --i) {
-      lx = B[i][c];
-#pragma unroll
-      for (int j = NT - 1; j > i; --j) {
-        lx.x = lx.x - (B[j][c].x * L[j][i].x + B[j][c].y * L[j][i].y);
-        lx.y = lx.y - (-B[j][c].x * L[j][i].y + B[j][c].y * L[j][i].x);
-      }
-      help = (L[i][i].x * L[i][i].x + L[i][i].y * L[i][i].y);
-      B[i][c].x = (lx.x * L[i][i].x - lx.y * L[i][i].y) / help;
-      B[i][c].y = (lx.y * L[i][i].x + lx.x * L[i][i].y) / help;
-    }
-  }
-}
 
 template <int NT>
 __global__ void __launch_bounds__(kThreads) k_solve_ref(RefArgs a) {
@@ -193,7 +120,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_ref(RefArgs a) {
       for (int l = 0; l < NT; ++l)
 #pragma unroll
         for (int q = 0; q < 3; ++q) KScc[q][l] = make_float2(KS[l][q].x, -KS[l][q].y);
-      axeqb_ref<NT>(M, KS);
+      axeqb_ref<NT, 3>(M, KS);
 #pragma unroll
       for (int p = 0; p < 3; ++p)
 #pragma unroll

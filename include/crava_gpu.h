@@ -415,6 +415,78 @@ int crava_gpu_crava_file_write(crava_gpu_ctx *ctx, const char *path, const float
 int crava_gpu_crava_file_read(crava_gpu_ctx *ctx, const char *path, float *grid,
                               crava_gpu_grid_header *header);
 
+/* The time-lapse state of State4D (src/state4d.h:44-106): the static and
+ * dynamic parts of the prior, as Fourier-domain device grids (padded real
+ * layout holding the transformed spectra), in the reference's own orders.
+ *   mu_static, mu_dynamic: vp, vs, rho;
+ *   cov_ss, cov_dd: (vp,vp) (vp,vs) (vp,rho) (vs,vs) (vs,rho) (rho,rho) of
+ *     the static-static and dynamic-dynamic blocks;
+ *   cov_sd: static (vp,vs,rho) x dynamic (vp,vs,rho), row-major. */
+typedef struct crava_gpu_state4d {
+  float *mu_static[3];
+  float *mu_dynamic[3];
+  float *cov_ss[6];
+  float *cov_dd[6];
+  float *cov_sd[9];
+} crava_gpu_state4d;
+
+/* State4D::merge (src/state4d.cpp:90-159) and mergeCov (:161-249): the
+ * current state's prior, mu = static + dynamic and cov = the sum of the
+ * four blocks, written into Fourier-domain grids.  mu may be NULL
+ * (mergeCov only).  cov in the crava_gpu_grids order (covAlpha, covBeta,
+ * covRho, crCovAlphaBeta, crCovAlphaRho, crCovBetaRho).  The reference's
+ * float additions in its order: bit-identical grids.  Asynchronous. */
+int crava_gpu_state4d_merge(crava_gpu_ctx *ctx, const crava_gpu_state4d *state,
+                            float *const mu[3], float *const cov[6]);
+
+/* State4D::split (src/state4d.cpp:251-525): the inverted current state
+ * (Fourier-domain posterior mu and cov, crava_gpu_grids order) spread back
+ * over the static and dynamic parts, per bin
+ *   B = Sigma_cur^-1 Sigma_cur,full (lib_matr Cholesky, 6 right-hand sides),
+ *   Sigma_full += B^H (Sigma_post - Sigma_cur) B,  mu_full += B^H (mu_post - mu_cur);
+ * bins whose 3x3 Cholesky fails keep the prior (counted in
+ * crava_gpu_stats.chol_fail_bins, and in *shortcut_bins when that is not
+ * NULL, which makes the call synchronous).  The reference's float
+ * operations in its order: bit-identical grids.  Updates state in place. */
+int crava_gpu_state4d_split(crava_gpu_ctx *ctx, const crava_gpu_state4d *state,
+                            const float *const mu[3], const float *const cov[6],
+                            long long *shortcut_bins);
+
+/* FFTGrid::fillInGenExpCorr (src/fftgrid.cpp:1167-1210): the generalised
+ * exponential correlation exp(-3 sqrt((i/rx)^2 + (j/ry)^2 + (k/rz)^2)) on
+ * the cyclic padded grid, k counter-rotated by the gradients; real padded
+ * layout, padding cells RMISSING.  Asynchronous. */
+int crava_gpu_fill_gen_exp_corr(crava_gpu_ctx *ctx, double rx, double ry, double rz,
+                                float grad_i, float grad_j, float *grid);
+
+/* State4D::evolve (src/state4d.cpp:527-730): the forward transition of the
+ * full state in time, per bin (double arithmetic, rounded to float once)
+ *   mu' = E mu + c_mu s (s = sqrt(nxp nyp nzp) at the zero bin, else 0),
+ *   Sigma' = E Sigma E^T + C Re(lambda)  (imaginary part: E Im(Sigma) E^T),
+ * E the [6][6] row-major evolution matrix, c_mu [6] and C [6][6] row-major
+ * the correction terms (TimeEvolution::getEvolutionMatrix,
+ * getMeanCorrectionTerm, getCovarianceCorrectionTerm), lambda the
+ * transformed correlation grid of the time increment (COVARIANCE
+ * transform of crava_gpu_fill_gen_exp_corr).  Updates state in place.
+ * Asynchronous. */
+int crava_gpu_state4d_evolve(crava_gpu_ctx *ctx, const crava_gpu_state4d *state,
+                             const double evolution[36], const double mean_correction[6],
+                             const double cov_correction[36], const float *lambda);
+
+/* ModelGeneral::advanceTime (src/modelgeneral.cpp:4722-4736): split the
+ * inverted current state (Fourier-domain mu, cov) into the state, build
+ * the time-increment correlation (fillInGenExpCorr(nx/3, ny/3, 50 at step 0
+ * else 5), forward transformed into lambda_work), evolve, merge the next
+ * prior back into mu and cov and transform those to the time domain
+ * (PARAMETER for mu, COVARIANCE for cov).  nx, ny: the unpadded lateral
+ * sizes.  shortcut_bins as in crava_gpu_state4d_split. */
+int crava_gpu_state4d_advance_time(crava_gpu_ctx *ctx, const crava_gpu_state4d *state,
+                                   int time_step, int nx, int ny, const double evolution[36],
+                                   const double mean_correction[6],
+                                   const double cov_correction[36], float *const mu[3],
+                                   float *const cov[6], float *lambda_work,
+                                   long long *shortcut_bins);
+
 /* Number of kernels this library launched so far in this process. */
 long long crava_gpu_launch_count(void);
 

@@ -1036,3 +1036,247 @@ int orc_fill_err_corr(int nxp, int nyp, int nzp, const float *corr_xy,
       }
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Time-lapse state: State4D (src/state4d.cpp)                          */
+/* ------------------------------------------------------------------ */
+/* (p, q) of State4D's upper-triangle order and the same entry's slot in
+ * the posterior's covariance order. */
+static const int s4_p[6] = {0, 0, 0, 1, 1, 2}, s4_q[6] = {0, 1, 2, 1, 2, 2};
+static const int s4_unit[6] = {0, 3, 4, 1, 5, 2};
+
+static cf ld_cf(const float *g, long long b) { cf v = {g[2 * b], g[2 * b + 1]}; return v; }
+static void st_cf(float *g, long long b, cf v) { g[2 * b] = v.re; g[2 * b + 1] = v.im; }
+static cf conj_cf(cf a) { cf v = {a.re, -a.im}; return v; }
+
+/* The full 6x6 prior of one bin: upper triangle from the grids, lower as
+ * its conjugate (src/state4d.cpp:203-225 and :341-380). */
+static void s4_full(long long b, const float *const *ss, const float *const *dd,
+                    const float *const *sd, cf F[6][6]) {
+  for (int r = 0; r < 6; ++r) {
+    F[s4_p[r]][s4_q[r]] = ld_cf(ss[r], b);
+    F[s4_p[r] + 3][s4_q[r] + 3] = ld_cf(dd[r], b);
+  }
+  for (int l = 0; l < 3; ++l)
+    for (int m = 0; m < 3; ++m) F[l][m + 3] = ld_cf(sd[3 * l + m], b);
+  for (int l = 0; l < 6; ++l)
+    for (int m = l + 1; m < 6; ++m) F[m][l] = conj_cf(F[l][m]);
+}
+
+/* State4D::merge (src/state4d.cpp:90-159) and mergeCov (:161-249). */
+void orc_state4d_merge(long long n, const float *const *ms, const float *const *md,
+                       const float *const *ss, const float *const *dd,
+                       const float *const *sd, float *const *mu, float *const *cov) {
+  for (long long b = 0; b < n; ++b) {
+    if (mu)
+      for (int l = 0; l < 3; ++l) {
+        cf s = ld_cf(ms[l], b), d = ld_cf(md[l], b), v = {s.re + d.re, s.im + d.im};
+        st_cf(mu[l], b, v);
+      }
+    cf F[6][6];
+    s4_full(b, ss, dd, sd, F);
+    for (int r = 0; r < 6; ++r) {
+      int l = s4_p[r], m = s4_q[r];
+      cf v;
+      v.re = F[l][m].re; v.re += F[l + 3][m + 3].re; v.re += F[l + 3][m].re; v.re += F[l][m + 3].re;
+      v.im = F[l][m].im; v.im += F[l + 3][m + 3].im; v.im += F[l + 3][m].im; v.im += F[l][m + 3].im;
+      st_cf(cov[s4_unit[r]], b, v);
+    }
+  }
+}
+
+/* lib_matrAXeqBMatCpx (libs/lib/lib_matr.c:330-365) for an n x nc matrix B
+ * stored row-major with leading dimension ldb. */
+static void axeqb_fw(int n, cf L[][ORC_MAXT], cf *B, int ldb, int nc) {
+  cf lx; float help;
+  for (int c = 0; c < nc; ++c) {
+    for (int i = 0; i < n; ++i) {
+      lx = B[i * ldb + c];
+      for (int j = 0; j < i; ++j) {
+        lx.re -= (B[j * ldb + c].re * L[i][j].re - B[j * ldb + c].im * L[i][j].im);
+        lx.im -= (B[j * ldb + c].im * L[i][j].re + B[j * ldb + c].re * L[i][j].im);
+      }
+      help = (L[i][i].re * L[i][i].re + L[i][i].im * L[i][i].im);
+      B[i * ldb + c].re = (lx.re * L[i][i].re + lx.im * L[i][i].im) / help;
+      B[i * ldb + c].im = (lx.im * L[i][i].re - lx.re * L[i][i].im) / help;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      lx = B[i * ldb + c];
+      for (int j = n - 1; j > i; --j) {
+        lx.re = lx.re - (B[j * ldb + c].re * L[j][i].re + B[j * ldb + c].im * L[j][i].im);
+        lx.im = lx.im - (-B[j * ldb + c].re * L[j][i].im + B[j * ldb + c].im * L[j][i].re);
+      }
+      help = (L[i][i].re * L[i][i].re + L[i][i].im * L[i][i].im);
+      B[i * ldb + c].re = (lx.re * L[i][i].re - lx.im * L[i][i].im) / help;
+      B[i * ldb + c].im = (lx.im * L[i][i].re + lx.re * L[i][i].im) / help;
+    }
+  }
+}
+
+/* x += a b in lib_matrProdCpx's form (libs/lib/lib_matr.c:548-566). */
+static void cmac_f(cf *x, cf a, cf b) {
+  x->re += a.re * b.re - a.im * b.im;
+  x->im += a.im * b.re + a.re * b.im;
+}
+
+/* State4D::split (src/state4d.cpp:251-525).  Returns the bins whose 3x3
+ * Cholesky failed (prior kept). */
+long long orc_state4d_split(long long n, float *const *ms, float *const *md,
+                            float *const *ss, float *const *dd, float *const *sd,
+                            const float *const *mu, const float *const *cov) {
+  long long fails = 0;
+  for (long long b = 0; b < n; ++b) {
+    cf F[6][6], muF[6], muP[3], SP[3][3], muC[3], FvC[6][3], SC[3][3];
+    cf L[ORC_MAXT][ORC_MAXT], B[3][6];
+    s4_full(b, (const float *const *)ss, (const float *const *)dd,
+            (const float *const *)sd, F);
+    for (int l = 0; l < 3; ++l) { muF[l] = ld_cf(ms[l], b); muF[l + 3] = ld_cf(md[l], b); }
+    for (int l = 0; l < 3; ++l) muP[l] = ld_cf(mu[l], b);
+    for (int r = 0; r < 6; ++r) {
+      cf v = ld_cf(cov[s4_unit[r]], b);
+      SP[s4_p[r]][s4_q[r]] = v;
+      SP[s4_q[r]][s4_p[r]] = v; /* copied, not conjugated (:370-372) */
+    }
+    for (int l = 0; l < 3; ++l) {
+      muC[l].re = muF[l].re + muF[l + 3].re;
+      muC[l].im = muF[l].im + muF[l + 3].im;
+    }
+    for (int l = 0; l < 6; ++l)
+      for (int m = 0; m < 3; ++m) {
+        FvC[l][m].re = F[l][m].re + F[l][m + 3].re;
+        FvC[l][m].im = F[l][m].im + F[l][m + 3].im;
+      }
+    for (int l = 0; l < 3; ++l)
+      for (int m = 0; m < 3; ++m) {
+        SC[l][m].re = FvC[l][m].re + FvC[l + 3][m].re;
+        SC[l][m].im = FvC[l][m].im + FvC[l + 3][m].im;
+        L[l][m] = SC[l][m];
+      }
+    for (int l = 0; l < 6; ++l)
+      for (int m = 0; m < 3; ++m) B[m][l] = conj_cf(FvC[l][m]);
+    if (chol_f(3, L) == 0) {
+      cf H[3][6], P[6][6], muFP[6];
+      axeqb_fw(3, L, &B[0][0], 6, 6);
+      for (int l = 0; l < 3; ++l)
+        for (int m = 0; m < 3; ++m) { SP[l][m].re -= SC[l][m].re; SP[l][m].im -= SC[l][m].im; }
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 6; ++j) {
+          cf x = {0.0f, 0.0f};
+          for (int k = 0; k < 3; ++k) cmac_f(&x, SP[i][k], B[k][j]);
+          H[i][j] = x;
+        }
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+          cf x = {0.0f, 0.0f};
+          for (int k = 0; k < 3; ++k) cmac_f(&x, conj_cf(B[k][i]), H[k][j]);
+          P[i][j] = x;
+        }
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) { P[i][j].re += F[i][j].re; P[i][j].im += F[i][j].im; }
+      for (int l = 0; l < 3; ++l) { muP[l].re -= muC[l].re; muP[l].im -= muC[l].im; }
+      for (int i = 0; i < 6; ++i) {
+        cf x = {0.0f, 0.0f};
+        for (int k = 0; k < 3; ++k) cmac_f(&x, conj_cf(B[k][i]), muP[k]);
+        muFP[i] = x;
+      }
+      for (int i = 0; i < 6; ++i) { muFP[i].re += muF[i].re; muFP[i].im += muF[i].im; }
+      memcpy(F, P, sizeof F);
+      memcpy(muF, muFP, sizeof muF);
+    } else {
+      ++fails;
+    }
+    for (int r = 0; r < 6; ++r) {
+      st_cf(ss[r], b, F[s4_p[r]][s4_q[r]]);
+      st_cf(dd[r], b, F[s4_p[r] + 3][s4_q[r] + 3]);
+    }
+    for (int l = 0; l < 3; ++l)
+      for (int m = 0; m < 3; ++m) st_cf(sd[3 * l + m], b, F[l][m + 3]);
+    for (int l = 0; l < 3; ++l) { st_cf(ms[l], b, muF[l]); st_cf(md[l], b, muF[l + 3]); }
+  }
+  return fails;
+}
+
+/* State4D::evolve (src/state4d.cpp:527-730): double arithmetic (the
+ * reference's FLENS matrices), each product-sum a chain of fused
+ * multiply-adds in natural order (C99 fma, correctly rounded), one rounding
+ * to float.  Both parts of the 6x6 matrix are mirrored unchanged
+ * (:660-690). */
+void orc_state4d_evolve(long long n, float *const *ms, float *const *md,
+                        float *const *ss, float *const *dd, float *const *sd,
+                        const double *E, const double *cm, const double *cc,
+                        const float *lambda, float zero_scale) {
+  for (long long b = 0; b < n; ++b) {
+    double lam = (double)lambda[2 * b];
+    float sc = b == 0 ? zero_scale : 0.0f;
+    double mr[6], mi[6], Sr[6][6], Si[6][6], Tr[6][6], Ti[6][6];
+    for (int l = 0; l < 3; ++l) {
+      cf s = ld_cf(ms[l], b), d = ld_cf(md[l], b);
+      mr[l] = s.re; mi[l] = s.im; mr[l + 3] = d.re; mi[l + 3] = d.im;
+    }
+    for (int d = 0; d < 6; ++d) {
+      double xr = 0.0, xi = 0.0;
+      for (int e = 0; e < 6; ++e) { xr = fma(E[6 * d + e], mr[e], xr); xi = fma(E[6 * d + e], mi[e], xi); }
+      xr = fma(cm[d], (double)sc, xr);
+      cf v = {(float)xr, (float)xi};
+      st_cf(d < 3 ? ms[d] : md[d - 3], b, v);
+    }
+    for (int r = 0; r < 6; ++r) {
+      int p = s4_p[r], q = s4_q[r];
+      cf s = ld_cf(ss[r], b), d = ld_cf(dd[r], b);
+      Sr[p][q] = Sr[q][p] = s.re; Si[p][q] = Si[q][p] = s.im;
+      Sr[p + 3][q + 3] = Sr[q + 3][p + 3] = d.re; Si[p + 3][q + 3] = Si[q + 3][p + 3] = d.im;
+    }
+    for (int l = 0; l < 3; ++l)
+      for (int m = 0; m < 3; ++m) {
+        cf v = ld_cf(sd[3 * l + m], b);
+        Sr[l][m + 3] = Sr[m + 3][l] = v.re;
+        Si[l][m + 3] = Si[m + 3][l] = v.im;
+      }
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) {
+        double xr = 0.0, xi = 0.0;
+        for (int k = 0; k < 6; ++k) { xr = fma(E[6 * i + k], Sr[k][j], xr); xi = fma(E[6 * i + k], Si[k][j], xi); }
+        Tr[i][j] = xr; Ti[i][j] = xi;
+      }
+    for (int i = 0; i < 6; ++i)
+      for (int j = i; j < 6; ++j) {
+        double xr = 0.0, xi = 0.0;
+        for (int k = 0; k < 6; ++k) { xr = fma(Tr[i][k], E[6 * j + k], xr); xi = fma(Ti[i][k], E[6 * j + k], xi); }
+        xr = fma(cc[6 * i + j], lam, xr);
+        cf v = {(float)xr, (float)xi};
+        if (j < 3) {
+          for (int r = 0; r < 6; ++r) if (s4_p[r] == i && s4_q[r] == j) st_cf(ss[r], b, v);
+        } else if (i < 3) {
+          st_cf(sd[3 * i + j - 3], b, v);
+        } else {
+          for (int r = 0; r < 6; ++r) if (s4_p[r] == i - 3 && s4_q[r] == j - 3) st_cf(dd[r], b, v);
+        }
+      }
+  }
+}
+
+/* FFTGrid::fillInGenExpCorr (src/fftgrid.cpp:1167-1210). */
+int orc_fill_gen_exp_corr(int nxp, int nyp, int nzp, double Rx, double Ry, double Rz,
+                          float gradI, float gradJ, float *out) {
+  int rnxp = 2 * (nxp / 2 + 1);
+  long idx = 0;
+  for (int k = 0; k < nzp; ++k)
+    for (int j = 0; j < nyp; ++j)
+      for (int i = 0; i < rnxp; ++i, ++idx) {
+        float value;
+        if (i < nxp) {
+          int cycleI = cyc(i, nxp), cycleJ = cyc(j, nyp);
+          float subK = k + cycleI * gradI + cycleJ * gradJ;
+          while (subK < -nzp / 2.0) subK += nzp;
+          while (subK >= nzp / 2.0) subK -= nzp;
+          double qDist = (float)(cycleI * cycleI) / (Rx * Rx) + (cycleJ * cycleJ) / (Ry * Ry) +
+                         (subK * subK) / (Rz * Rz);
+          double dist = sqrt(qDist);
+          value = (float)exp(-3.0 * dist);
+        } else {
+          value = -99999.0f; /* RMISSING */
+        }
+        out[idx] = value;
+      }
+  return 0;
+}

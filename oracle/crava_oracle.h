@@ -96,6 +96,22 @@ int orc_fill_prior_cov(int nxp, int nyp, int nzp, const float *corr_xy,
                        const double *var0, float *const *cov);
 int orc_fill_err_corr(int nxp, int nyp, int nzp, const float *corr_xy,
                       float grad_i, float grad_j, float *err_corr);
+/* Time-lapse state (State4D).  Spectra are interleaved float pairs of n
+ * bins; state grids in State4D's orders (mu: vp, vs, rho; ss/dd: (0,0)
+ * (0,1) (0,2) (1,1) (1,2) (2,2); sd: 3x3 row-major), the current state's
+ * covariance in the posterior's order (00, 11, 22, 01, 02, 12). */
+void orc_state4d_merge(long long n, const float *const *ms, const float *const *md,
+                       const float *const *ss, const float *const *dd,
+                       const float *const *sd, float *const *mu, float *const *cov);
+long long orc_state4d_split(long long n, float *const *ms, float *const *md,
+                            float *const *ss, float *const *dd, float *const *sd,
+                            const float *const *mu, const float *const *cov);
+void orc_state4d_evolve(long long n, float *const *ms, float *const *md,
+                        float *const *ss, float *const *dd, float *const *sd,
+                        const double *E, const double *cm, const double *cc,
+                        const float *lambda, float zero_scale);
+int orc_fill_gen_exp_corr(int nxp, int nyp, int nzp, double rx, double ry, double rz,
+                          float grad_i, float grad_j, float *out);
 int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
                      const float *A, const float *wavelet, const float *const *m,
                      float *const *out);
@@ -126,6 +142,12 @@ int ref_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
 int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
                      const float *A, const float *wavelet, const float *const *m,
                      float *const *out);
+void ref_state4d_merge(long long n, const float *const *ms, const float *const *md,
+                       const float *const *ss, const float *const *dd,
+                       const float *const *sd, float *const *mu, float *const *cov);
+long long ref_state4d_split(long long n, float *const *ms, float *const *md,
+                            float *const *ss, float *const *dd, float *const *sd,
+                            const float *const *mu, const float *const *cov);
 
 #ifdef __cplusplus
 }

@@ -110,6 +110,20 @@ def _load(which: str):
         f = lib.orc_sim_filter_fp64
         f.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(F32P), C.POINTER(F32P), C.POINTER(C.c_longlong)]
         f.restype = C.c_int
+    s4 = [C.POINTER(F32P)] * 7
+    f = getattr(lib, f"{p}_state4d_merge")
+    f.argtypes = [C.c_longlong] + s4
+    f.restype = None
+    f = getattr(lib, f"{p}_state4d_split")
+    f.argtypes = [C.c_longlong] + s4
+    f.restype = C.c_longlong
+    if which == "orc":
+        f = lib.orc_state4d_evolve
+        f.argtypes = [C.c_longlong] + [C.POINTER(F32P)] * 5 + [F64P, F64P, F64P, F32P, C.c_float]
+        f.restype = None
+        f = lib.orc_fill_gen_exp_corr
+        f.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [C.c_float, C.c_float, F32P]
+        f.restype = C.c_int
     _libs[which] = lib
     return lib
 
@@ -315,6 +329,45 @@ def fill_err_corr(nxp, nyp, nzp, corr_xy, grad_i, grad_j):
     cxy = np.ascontiguousarray(corr_xy, dtype=np.float32)
     out = np.zeros((nzp, nyp, 2 * (nxp // 2 + 1)), np.float32)
     assert lib.orc_fill_err_corr(nxp, nyp, nzp, _fp(cxy), grad_i, grad_j, _fp(out)) == 0
+    return out
+
+
+STATE_KEYS = ("ms", "md", "ss", "dd", "sd")  # 3, 3, 6, 6, 9 spectra
+
+
+def _state_ptrs(state):
+    return [_ptrs(state[k]) for k in STATE_KEYS]
+
+
+def state4d_merge(state, mu, cov, which="orc"):
+    """State4D::merge / mergeCov into mu (3, or None) and cov (6, posterior
+    order); spectra as float32 arrays of interleaved complex values."""
+    lib = _load(which)
+    n = state["ms"][0].size // 2
+    getattr(lib, f"{which}_state4d_merge")(n, *_state_ptrs(state),
+                                           _ptrs(mu) if mu is not None else None, _ptrs(cov))
+
+
+def state4d_split(state, mu, cov, which="orc"):
+    """State4D::split, in place on state; returns the shortcut bins."""
+    lib = _load(which)
+    n = state["ms"][0].size // 2
+    return int(getattr(lib, f"{which}_state4d_split")(n, *_state_ptrs(state), _ptrs(mu), _ptrs(cov)))
+
+
+def state4d_evolve(state, E, cm, cc, lam, zero_scale):
+    """State4D::evolve (restatement), in place on state."""
+    lib = _load("orc")
+    n = state["ms"][0].size // 2
+    E, cm, cc = (np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in (E, cm, cc))
+    lib.orc_state4d_evolve(n, *_state_ptrs(state), _dp(E), _dp(cm), _dp(cc), _fp(lam), zero_scale)
+
+
+def fill_gen_exp_corr(nxp, nyp, nzp, rx, ry, rz, grad_i, grad_j):
+    """FFTGrid::fillInGenExpCorr (restatement)."""
+    lib = _load("orc")
+    out = np.zeros((nzp, nyp, 2 * (nxp // 2 + 1)), np.float32)
+    assert lib.orc_fill_gen_exp_corr(nxp, nyp, nzp, rx, ry, rz, grad_i, grad_j, _fp(out)) == 0
     return out
 
 

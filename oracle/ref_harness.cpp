@@ -570,4 +570,170 @@ int ref_sim_filter(int nxp, int nyp, int nzp, const float *const *cov_,
   return 0;
 }
 
+/* State4D::merge and mergeCov (src/state4d.cpp:90-249): the reference's
+ * per-bin loops with its getNextComplex order, over interleaved spectra of
+ * n bins; the current covariance in the posterior's order. */
+void ref_state4d_merge(long long n, const float *const *ms_, const float *const *md_,
+                       const float *const *ss_, const float *const *dd_,
+                       const float *const *sd_, float *const *mu_, float *const *cov_) {
+  const fftw_complex *ms[3], *md[3], *ss[6], *dd[6], *sd[9];
+  for (int i = 0; i < 3; ++i) {
+    ms[i] = reinterpret_cast<const fftw_complex *>(ms_[i]);
+    md[i] = reinterpret_cast<const fftw_complex *>(md_[i]);
+  }
+  for (int i = 0; i < 6; ++i) {
+    ss[i] = reinterpret_cast<const fftw_complex *>(ss_[i]);
+    dd[i] = reinterpret_cast<const fftw_complex *>(dd_[i]);
+  }
+  for (int i = 0; i < 9; ++i) sd[i] = reinterpret_cast<const fftw_complex *>(sd_[i]);
+  /* sigma[0..5] = CovAlpha, CrCovAlphaBeta, CrCovAlphaRho, CovBeta,
+   * CrCovBetaRho, CovRho (:150-156) */
+  const int unit[6] = {0, 3, 4, 1, 5, 2};
+  fftw_complex *sigma[6], *mu[3];
+  for (int i = 0; i < 6; ++i) sigma[i] = reinterpret_cast<fftw_complex *>(cov_[unit[i]]);
+  for (int i = 0; i < 3; ++i) mu[i] = mu_ ? reinterpret_cast<fftw_complex *>(mu_[i]) : nullptr;
+  std::vector<std::vector<fftw_complex> > F(6, std::vector<fftw_complex>(6));
+  std::vector<std::vector<fftw_complex> > C(3, std::vector<fftw_complex>(3));
+  for (long long b = 0; b < n; ++b) {
+    if (mu_) {
+      fftw_complex muFullPrior[6], muCurrentPrior[3];
+      for (int l = 0; l < 3; ++l) { muFullPrior[l] = ms[l][b]; muFullPrior[l + 3] = md[l][b]; }
+      for (int l = 0; l < 3; l++) {
+        muCurrentPrior[l].re = muFullPrior[l].re + muFullPrior[l + 3].re;
+        muCurrentPrior[l].im = muFullPrior[l].im + muFullPrior[l + 3].im;
+      }
+      for (int l = 0; l < 3; ++l) mu[l][b] = muCurrentPrior[l];
+    }
+    F[0][0] = ss[0][b]; F[0][1] = ss[1][b]; F[0][2] = ss[2][b];
+    F[0][3] = sd[0][b]; F[0][4] = sd[1][b]; F[0][5] = sd[2][b];
+    F[1][1] = ss[3][b]; F[1][2] = ss[4][b];
+    F[1][3] = sd[3][b]; F[1][4] = sd[4][b]; F[1][5] = sd[5][b];
+    F[2][2] = ss[5][b];
+    F[2][3] = sd[6][b]; F[2][4] = sd[7][b]; F[2][5] = sd[8][b];
+    F[3][3] = dd[0][b]; F[3][4] = dd[1][b]; F[3][5] = dd[2][b];
+    F[4][4] = dd[3][b]; F[4][5] = dd[4][b];
+    F[5][5] = dd[5][b];
+    for (int l = 0; l < 6; l++)
+      for (int m = l + 1; m < 6; m++) {
+        F[m][l].re = F[l][m].re;
+        F[m][l].im = -F[l][m].im;
+      }
+    for (int l = 0; l < 3; l++)
+      for (int m = 0; m < 3; m++) {
+        C[l][m].re = F[l][m].re;
+        C[l][m].re += F[l + 3][m + 3].re;
+        C[l][m].re += F[l + 3][m].re;
+        C[l][m].re += F[l][m + 3].re;
+        C[l][m].im = F[l][m].im;
+        C[l][m].im += F[l + 3][m + 3].im;
+        C[l][m].im += F[l + 3][m].im;
+        C[l][m].im += F[l][m + 3].im;
+      }
+    sigma[0][b] = C[0][0]; sigma[1][b] = C[0][1]; sigma[2][b] = C[0][2];
+    sigma[3][b] = C[1][1]; sigma[4][b] = C[1][2]; sigma[5][b] = C[2][2];
+  }
+}
+
+/* State4D::split (src/state4d.cpp:251-525): the reference's per-bin
+ * sequence of lib_matr calls.  Returns the shortcut (failed Cholesky) bins. */
+long long ref_state4d_split(long long n, float *const *ms_, float *const *md_,
+                            float *const *ss_, float *const *dd_, float *const *sd_,
+                            const float *const *mu_, const float *const *cov_) {
+  fftw_complex *ms[3], *md[3], *ss[6], *dd[6], *sd[9];
+  const fftw_complex *mu[3], *sigma[6];
+  for (int i = 0; i < 3; ++i) {
+    ms[i] = reinterpret_cast<fftw_complex *>(ms_[i]);
+    md[i] = reinterpret_cast<fftw_complex *>(md_[i]);
+    mu[i] = reinterpret_cast<const fftw_complex *>(mu_[i]);
+  }
+  for (int i = 0; i < 6; ++i) {
+    ss[i] = reinterpret_cast<fftw_complex *>(ss_[i]);
+    dd[i] = reinterpret_cast<fftw_complex *>(dd_[i]);
+  }
+  for (int i = 0; i < 9; ++i) sd[i] = reinterpret_cast<fftw_complex *>(sd_[i]);
+  const int unit[6] = {0, 3, 4, 1, 5, 2};
+  for (int i = 0; i < 6; ++i) sigma[i] = reinterpret_cast<const fftw_complex *>(cov_[unit[i]]);
+
+  fftw_complex muFullPrior[6], muFullPosterior[6], muCurrentPrior[3], muCurrentPosterior[3];
+  fftw_complex **sigmaFullPrior = alloc_mat(6, 6), **sigmaFullPosterior = alloc_mat(6, 6);
+  fftw_complex **sigmaFullVsCurrentPrior = alloc_mat(6, 3), **adjointSandwich = alloc_mat(6, 3);
+  fftw_complex **sigmaCurrentPrior = alloc_mat(3, 3), **sigmaCurrentPriorChol = alloc_mat(3, 3);
+  fftw_complex **sigmaCurrentPosterior = alloc_mat(3, 3);
+  fftw_complex **sandwich = alloc_mat(3, 6), **helper = alloc_mat(3, 6);
+  long long counter = 0;
+  for (long long b = 0; b < n; ++b) {
+    for (int l = 0; l < 3; ++l) { muFullPrior[l] = ms[l][b]; muFullPrior[l + 3] = md[l][b]; }
+    fftw_complex **F = sigmaFullPrior;
+    F[0][0] = ss[0][b]; F[0][1] = ss[1][b]; F[0][2] = ss[2][b];
+    F[0][3] = sd[0][b]; F[0][4] = sd[1][b]; F[0][5] = sd[2][b];
+    F[1][1] = ss[3][b]; F[1][2] = ss[4][b];
+    F[1][3] = sd[3][b]; F[1][4] = sd[4][b]; F[1][5] = sd[5][b];
+    F[2][2] = ss[5][b];
+    F[2][3] = sd[6][b]; F[2][4] = sd[7][b]; F[2][5] = sd[8][b];
+    F[3][3] = dd[0][b]; F[3][4] = dd[1][b]; F[3][5] = dd[2][b];
+    F[4][4] = dd[3][b]; F[4][5] = dd[4][b];
+    F[5][5] = dd[5][b];
+    for (int l = 0; l < 3; ++l) muCurrentPosterior[l] = mu[l][b];
+    sigmaCurrentPosterior[0][0] = sigma[0][b]; sigmaCurrentPosterior[0][1] = sigma[1][b];
+    sigmaCurrentPosterior[0][2] = sigma[2][b]; sigmaCurrentPosterior[1][1] = sigma[3][b];
+    sigmaCurrentPosterior[1][2] = sigma[4][b]; sigmaCurrentPosterior[2][2] = sigma[5][b];
+    sigmaCurrentPosterior[1][0] = sigmaCurrentPosterior[0][1];
+    sigmaCurrentPosterior[2][0] = sigmaCurrentPosterior[0][2];
+    sigmaCurrentPosterior[2][1] = sigmaCurrentPosterior[1][2];
+    for (int l = 0; l < 6; l++)
+      for (int m = l + 1; m < 6; m++) {
+        F[m][l].re = F[l][m].re;
+        F[m][l].im = -F[l][m].im;
+      }
+    for (int l = 0; l < 3; l++) {
+      muCurrentPrior[l].re = muFullPrior[l].re + muFullPrior[l + 3].re;
+      muCurrentPrior[l].im = muFullPrior[l].im + muFullPrior[l + 3].im;
+    }
+    for (int l = 0; l < 6; l++)
+      for (int m = 0; m < 3; m++) {
+        sigmaFullVsCurrentPrior[l][m].re = F[l][m].re + F[l][m + 3].re;
+        sigmaFullVsCurrentPrior[l][m].im = F[l][m].im + F[l][m + 3].im;
+      }
+    for (int l = 0; l < 3; l++)
+      for (int m = 0; m < 3; m++) {
+        sigmaCurrentPrior[l][m].re = sigmaFullVsCurrentPrior[l][m].re + sigmaFullVsCurrentPrior[l + 3][m].re;
+        sigmaCurrentPrior[l][m].im = sigmaFullVsCurrentPrior[l][m].im + sigmaFullVsCurrentPrior[l + 3][m].im;
+      }
+    lib_matrCopyCpx(sigmaCurrentPrior, 3, 3, sigmaCurrentPriorChol);
+    lib_matrAdjoint(sigmaFullVsCurrentPrior, 6, 3, sandwich);
+    int flag = lib_matrCholCpx(3, sigmaCurrentPriorChol);
+    if (flag == 0) {
+      lib_matrAXeqBMatCpx(3, sigmaCurrentPriorChol, sandwich, 6);
+      lib_matrSubtMatCpx(sigmaCurrentPrior, 3, 3, sigmaCurrentPosterior);
+      lib_matrProdCpx(sigmaCurrentPosterior, sandwich, 3, 3, 6, helper);
+      lib_matrAdjoint(sandwich, 3, 6, adjointSandwich);
+      lib_matrProdCpx(adjointSandwich, helper, 6, 3, 6, sigmaFullPosterior);
+      lib_matrAddMatCpx(sigmaFullPrior, 6, 6, sigmaFullPosterior);
+      lib_matrSubtVecCpx(muCurrentPrior, 3, muCurrentPosterior);
+      lib_matrProdMatVecCpx(adjointSandwich, muCurrentPosterior, 6, 3, muFullPosterior);
+      lib_matrAddVecCpx(muFullPrior, 6, muFullPosterior);
+    } else {
+      counter++;
+      lib_matrCopyCpx(sigmaFullPrior, 6, 6, sigmaFullPosterior);
+      for (int l = 0; l < 6; l++) muFullPosterior[l] = muFullPrior[l];
+    }
+    fftw_complex **P = sigmaFullPosterior;
+    ss[0][b] = P[0][0]; ss[1][b] = P[0][1]; ss[2][b] = P[0][2];
+    sd[0][b] = P[0][3]; sd[1][b] = P[0][4]; sd[2][b] = P[0][5];
+    ss[3][b] = P[1][1]; ss[4][b] = P[1][2];
+    sd[3][b] = P[1][3]; sd[4][b] = P[1][4]; sd[5][b] = P[1][5];
+    ss[5][b] = P[2][2];
+    sd[6][b] = P[2][3]; sd[7][b] = P[2][4]; sd[8][b] = P[2][5];
+    dd[0][b] = P[3][3]; dd[1][b] = P[3][4]; dd[2][b] = P[3][5];
+    dd[3][b] = P[4][4]; dd[4][b] = P[4][5];
+    dd[5][b] = P[5][5];
+    for (int l = 0; l < 3; ++l) { ms[l][b] = muFullPosterior[l]; md[l][b] = muFullPosterior[l + 3]; }
+  }
+  free_mat(sigmaFullPrior, 6); free_mat(sigmaFullPosterior, 6);
+  free_mat(sigmaFullVsCurrentPrior, 6); free_mat(adjointSandwich, 6);
+  free_mat(sigmaCurrentPrior, 3); free_mat(sigmaCurrentPriorChol, 3);
+  free_mat(sigmaCurrentPosterior, 3); free_mat(sandwich, 3); free_mat(helper, 3);
+  return counter;
+}
+
 }  /* extern "C" */

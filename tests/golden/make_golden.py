@@ -58,11 +58,36 @@ def make_synt():
     print("synt_seismic written")
 
 
+def make_state4d():
+    """State4D merge and split of a seeded state through the reference's
+    lib_matr (oracle/_ref)."""
+    from tests import state4d_cases as SC
+
+    nxp, nyp, nzp = 10, 6, 8
+    state, mu, cov = SC.random_state(nxp, nyp, nzp, seed=404, fail_every=23)
+    out = dict(shape=np.array([nxp, nyp, nzp]), mu_post=np.stack(mu), cov_post=np.stack(cov))
+    for k in SC.KEYS:
+        out[f"in_{k}"] = np.stack(state[k])
+    mmu = [np.zeros_like(mu[0]) for _ in range(3)]
+    mcov = [np.zeros_like(mu[0]) for _ in range(6)]
+    O.state4d_merge(state, mmu, mcov, "ref")
+    out["merge_mu"], out["merge_cov"] = np.stack(mmu), np.stack(mcov)
+    st = SC.copy_state(state)
+    out["split_fail"] = O.state4d_split(st, mu, cov, "ref")
+    for k in SC.KEYS:
+        out[f"split_{k}"] = np.stack(st[k])
+    np.savez_compressed(os.path.join(HERE, "state4d.npz"), **out)
+    print("state4d written, split shortcuts", out["split_fail"])
+
+
 def main():
     if not O.have_ref():
         O.build(ref=True)
     if "--synt-only" in sys.argv:
         make_synt()
+        return
+    if "--state4d-only" in sys.argv:
+        make_state4d()
         return
     for name, spec in CASES.items():
         case = make_case(spec)
@@ -93,6 +118,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "rng_23665.npz"), normals=normals, state=state)
     print("rng written")
     make_synt()
+    make_state4d()
 
 
 if __name__ == "__main__":

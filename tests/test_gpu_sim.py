@@ -32,7 +32,7 @@ def test_filter_bitexact_vs_reference(name):
     assert st.chol_fail_bins == int(z["sim_fail"])
 
 
-@pytest.mark.parametrize("shape", [(16, 12, 32), (15, 10, 21), (64, 48, 96)])
+@pytest.mark.parametrize("shape", [(16, 12, 32), (15, 10, 21), (64, 48, 96), (16, 1, 64)])
 def test_noise_hermitian_rules(shape):
     nx, ny, nz = shape
     case = synth.make_case(nx, ny, nz, (10.0,), 0.1, seed=1)

@@ -13,7 +13,8 @@ def rel(a, b):
 
 
 @pytest.mark.parametrize("shape", [(16, 12, 32), (20, 18, 30), (15, 16, 20), (64, 64, 128),
-                                   (96, 200, 30), (192, 160, 24), (75, 21, 35), (128, 128, 256)])
+                                   (96, 200, 30), (192, 160, 24), (75, 21, 35), (128, 128, 256),
+                                   (16, 1, 32), (15, 1, 20)])
 @pytest.mark.parametrize("gtype", [api.DATA, api.COVARIANCE])
 def test_fft_roundtrip_and_oracle(shape, gtype):
     nx, ny, nz = shape
@@ -108,6 +109,22 @@ def test_unit_vs_reference_unit():
     data = [api.to_device(g) for g in case.data]
     cov = [api.to_device(g) for g in case.cov]
     err = api.to_device(case.err_corr)
+    ctx.posterior_unit(mu, data, cov, err, api.FP32)
+    which = "ref" if O.have_ref() else "orc"
+    omu, ores, ocov, ofail = O.unit_fp32(case, which)
+    nx = case.nxp
+    for g, o in zip(mu + data + cov, omu + ores + ocov):
+        assert rel(g.cpu().numpy()[..., :nx], o[..., :nx]) < 2e-5
+
+
+@pytest.mark.parametrize("shape", [(16, 1, 32), (15, 1, 20)])
+def test_unit_single_line(shape):
+    """A 2-D section (nyp = 1: length-1 y lines, every bin its own y
+    partner) through the whole unit, against the reference's numerics."""
+    case = synth.make_case(*shape, (10.0, 20.0, 30.0), 0.1, seed=5)
+    ctx = api.Context(case)
+    d = lambda gs: [api.to_device(g) for g in gs]
+    mu, data, cov, err = d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0]
     ctx.posterior_unit(mu, data, cov, err, api.FP32)
     which = "ref" if O.have_ref() else "orc"
     omu, ores, ocov, ofail = O.unit_fp32(case, which)

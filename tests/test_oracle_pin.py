@@ -180,3 +180,125 @@ def test_nonconstant_thickness_tables_vs_ref(shape):
         assert np.abs(x - y).max() <= 1e-6 * np.abs(y).max()
     inv = b[4].astype(bool)
     assert np.abs(a[3][inv] - b[3][inv]).max() <= 1e-6 * np.abs(b[3][inv]).max()
+
+
+# ---------------------------------------------------------------- State4D
+def _golden_state4d():
+    from tests import state4d_cases as SC
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "state4d.npz"))
+    state = {k: [np.ascontiguousarray(g) for g in z[f"in_{k}"]] for k in SC.KEYS}
+    return SC, z, state, list(z["mu_post"]), list(z["cov_post"])
+
+
+def test_state4d_merge_split_bitexact_vs_golden():
+    """merge / mergeCov and split restated reproduce the reference's
+    lib_matr sequence (src/state4d.cpp:90-525) bit for bit, shortcut bins
+    included."""
+    SC, z, state, mu, cov = _golden_state4d()
+    mmu = [np.zeros_like(mu[0]) for _ in range(3)]
+    mcov = [np.zeros_like(mu[0]) for _ in range(6)]
+    O.state4d_merge(state, mmu, mcov, "orc")
+    for a, b in zip(mmu + mcov, list(z["merge_mu"]) + list(z["merge_cov"])):
+        assert np.array_equal(bits(a), bits(b))
+    st = SC.copy_state(state)
+    fails = O.state4d_split(st, mu, cov, "orc")
+    assert fails == int(z["split_fail"]) > 0
+    for k in SC.KEYS:
+        for a, b in zip(st[k], z[f"split_{k}"]):
+            assert np.array_equal(bits(a), bits(b)), k
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
+def test_state4d_vs_ref_live():
+    from tests import state4d_cases as SC
+    state, mu, cov = SC.random_state(20, 12, 16, seed=5, fail_every=41)
+    out = {}
+    for which in ("orc", "ref"):
+        mmu = [np.zeros_like(mu[0]) for _ in range(3)]
+        mcov = [np.zeros_like(mu[0]) for _ in range(6)]
+        O.state4d_merge(state, mmu, mcov, which)
+        st = SC.copy_state(state)
+        f = O.state4d_split(st, mu, cov, which)
+        out[which] = (mcov, st, f)
+    assert out["orc"][2] == out["ref"][2] > 0
+    for a, b in zip(out["orc"][0], out["ref"][0]):
+        assert np.array_equal(bits(a), bits(b))
+    for k in SC.KEYS:
+        for a, b in zip(out["orc"][1][k], out["ref"][1][k]):
+            assert np.array_equal(bits(a), bits(b))
+
+
+def test_state4d_split_then_merge_gives_the_posterior():
+    """After split, the merged current prior equals the inverted state it
+    was split from, to float rounding: T B^H = I for T = [I I] and
+    B = Sigma_cur^-1 T Sigma_full.  For the covariance this needs a
+    Hermitian current covariance, which the reference's unconjugated
+    lower-triangle copy keeps only when that covariance is real."""
+    from tests import state4d_cases as SC
+    state, mu, cov = SC.random_state(12, 8, 10, seed=9, fail_every=0, real_post_cov=True)
+    st = SC.copy_state(state)
+    assert O.state4d_split(st, mu, cov, "orc") == 0
+    mmu = [np.zeros_like(mu[0]) for _ in range(3)]
+    mcov = [np.zeros_like(mu[0]) for _ in range(6)]
+    O.state4d_merge(st, mmu, mcov, "orc")
+    for a, b in zip(mmu + mcov, mu + cov):
+        assert rel(SC.to_complex(a), SC.to_complex(b)) < 1e-4
+
+
+def test_state4d_evolve_restatement_vs_numpy():
+    """evolve (src/state4d.cpp:527-730) against an independent float64
+    numpy statement of E S E^T + C Re(lambda) and E mu + c s."""
+    from tests import state4d_cases as SC
+    nxp, nyp, nzp = 8, 6, 10
+    state, _, _ = SC.random_state(nxp, nyp, nzp, seed=3)
+    E, cm, cc = SC.evolution(4)
+    lam = np.random.default_rng(5).standard_normal(SC.grid_shape(nxp, nyp, nzp)).astype(np.float32)
+    scale = np.float32(np.sqrt(float(nxp * nyp * nzp)))
+    st = SC.copy_state(state)
+    O.state4d_evolve(st, E, cm, cc, lam, scale)
+    c = SC.to_complex
+    m = np.stack([c(g) for g in state["ms"] + state["md"]], -1).astype(np.complex128)
+    n = m.shape[0]
+    Sr, Si = np.zeros((n, 6, 6)), np.zeros((n, 6, 6))
+    for r in range(6):
+        for off, key in ((0, "ss"), (3, "dd")):
+            v = c(state[key][r])
+            p, q = SC.P[r] + off, SC.Q[r] + off
+            Sr[:, p, q] = Sr[:, q, p] = v.real
+            Si[:, p, q] = Si[:, q, p] = v.imag
+    for l in range(3):
+        for k in range(3):
+            v = c(state["sd"][3 * l + k])
+            Sr[:, l, k + 3] = Sr[:, k + 3, l] = v.real
+            Si[:, l, k + 3] = Si[:, k + 3, l] = v.imag
+    lr = c(lam).real.astype(np.float64)
+    Nr = E @ Sr @ E.T + cc[None] * lr[:, None, None]
+    Ni = E @ Si @ E.T
+    mr = m.real @ E.T
+    mr[0] += cm * float(scale)
+    mi = m.imag @ E.T
+    got = np.stack([c(g) for g in st["ms"] + st["md"]], -1)
+    assert np.allclose(got.real, mr, rtol=1e-6, atol=1e-6) and np.allclose(got.imag, mi, rtol=1e-6, atol=1e-6)
+    for r in range(6):
+        for off, key in ((0, "ss"), (3, "dd")):
+            v = c(st[key][r])
+            p, q = SC.P[r] + off, SC.Q[r] + off
+            assert np.allclose(v.real, Nr[:, p, q], rtol=1e-6, atol=1e-5)
+            assert np.allclose(v.imag, Ni[:, p, q], rtol=1e-6, atol=1e-5)
+
+
+def test_gen_exp_corr_restatement_vs_numpy():
+    """fillInGenExpCorr (src/fftgrid.cpp:1167-1210) against numpy."""
+    nxp, nyp, nzp, rx, ry, rz, gi, gj = 12, 10, 16, 4.0, 10.0 / 3.0, 5.0, 0.3, -0.2
+    g = O.fill_gen_exp_corr(nxp, nyp, nzp, rx, ry, rz, gi, gj)
+    i = np.arange(nxp)
+    ci = np.where(i < nxp - i, i, i - nxp)
+    j = np.arange(nyp)
+    cj = np.where(j < nyp - j, j, j - nyp)
+    k = np.arange(nzp)
+    sub = (k[:, None, None] + ci[None, None, :] * np.float32(gi) + cj[None, :, None] * np.float32(gj))
+    sub = (sub + nzp / 2.0) % nzp - nzp / 2.0
+    ref = np.exp(-3.0 * np.sqrt((ci ** 2)[None, None, :] / rx ** 2 + (cj ** 2)[None, :, None] / ry ** 2
+                                + sub ** 2 / rz ** 2))
+    assert np.abs(g[..., :nxp] - ref).max() < 1e-6
+    assert np.all(g[..., nxp:] == -99999.0)
