@@ -160,4 +160,81 @@ class CravaDevice {
   int nt_ = 0;
 };
 
+// State4D (src/state4d.h:44-106) on device grids: static and dynamic means
+// and the static-static, dynamic-dynamic and static-dynamic covariance
+// blocks, all holding Fourier-domain spectra, in the reference's orders.
+// The current state's covariance grids are passed in the crava_gpu_grids
+// order (covAlpha, covBeta, covRho, crCovAlphaBeta, crCovAlphaRho,
+// crCovBetaRho).
+class State4DDevice {
+ public:
+  FFTGridDevice *mu_static[3] = {}, *mu_dynamic[3] = {};
+  FFTGridDevice *cov_ss[6] = {}, *cov_dd[6] = {}, *cov_sd[9] = {};
+
+  // State4D::merge (src/state4d.cpp:90-159); mu == nullptr: mergeCov.
+  void merge(CravaDevice &c, FFTGridDevice *mu[3], FFTGridDevice *cov[6]) {
+    crava_gpu_state4d st = raw();
+    float *m[3], *v[6];
+    for (int i = 0; i < 3; ++i) m[i] = mu ? mu[i]->devicePtr() : nullptr;
+    for (int i = 0; i < 6; ++i) v[i] = cov[i]->devicePtr();
+    check(crava_gpu_state4d_merge(c.ctx(), &st, mu ? m : nullptr, v), "State4D::merge");
+    for (int i = 0; i < 6; ++i) cov[i]->setTransformedStatus(true);
+    if (mu)
+      for (int i = 0; i < 3; ++i) mu[i]->setTransformedStatus(true);
+  }
+
+  // State4D::split (src/state4d.cpp:251-525); returns the shortcut bins.
+  long long split(CravaDevice &c, FFTGridDevice *mu[3], FFTGridDevice *cov[6]) {
+    crava_gpu_state4d st = raw();
+    const float *m[3], *v[6];
+    for (int i = 0; i < 3; ++i) m[i] = mu[i]->devicePtr();
+    for (int i = 0; i < 6; ++i) v[i] = cov[i]->devicePtr();
+    long long n = 0;
+    check(crava_gpu_state4d_split(c.ctx(), &st, m, v, &n), "State4D::split");
+    return n;
+  }
+
+  // State4D::evolve (src/state4d.cpp:527-730); lambda: the transformed
+  // correlation of the time increment.
+  void evolve(CravaDevice &c, const double E[36], const double meanCorr[6], const double covCorr[36],
+              FFTGridDevice &lambda) {
+    crava_gpu_state4d st = raw();
+    check(crava_gpu_state4d_evolve(c.ctx(), &st, E, meanCorr, covCorr, lambda.devicePtr()),
+          "State4D::evolve");
+  }
+
+  // ModelGeneral::advanceTime (src/modelgeneral.cpp:4722-4736); on return
+  // mu and cov hold the next prior in the time domain.
+  long long advanceTime(CravaDevice &c, int timeStep, int nx, int ny, const double E[36],
+                        const double meanCorr[6], const double covCorr[36], FFTGridDevice *mu[3],
+                        FFTGridDevice *cov[6], FFTGridDevice &work) {
+    crava_gpu_state4d st = raw();
+    float *m[3], *v[6];
+    for (int i = 0; i < 3; ++i) m[i] = mu[i]->devicePtr();
+    for (int i = 0; i < 6; ++i) v[i] = cov[i]->devicePtr();
+    long long n = 0;
+    check(crava_gpu_state4d_advance_time(c.ctx(), &st, timeStep, nx, ny, E, meanCorr, covCorr, m, v,
+                                         work.devicePtr(), &n),
+          "ModelGeneral::advanceTime");
+    for (int i = 0; i < 3; ++i) mu[i]->setTransformedStatus(false);
+    for (int i = 0; i < 6; ++i) cov[i]->setTransformedStatus(false);
+    return n;
+  }
+
+ private:
+  crava_gpu_state4d raw() const {
+    crava_gpu_state4d st{};
+    for (int i = 0; i < 3; ++i) {
+      st.mu_static[i] = mu_static[i]->devicePtr();
+      st.mu_dynamic[i] = mu_dynamic[i]->devicePtr();
+    }
+    for (int i = 0; i < 6; ++i) {
+      st.cov_ss[i] = cov_ss[i]->devicePtr();
+      st.cov_dd[i] = cov_dd[i]->devicePtr();
+    }
+    for (int i = 0; i < 9; ++i) st.cov_sd[i] = cov_sd[i]->devicePtr();
+    return st;
+  }
+};
+
 }  // namespace crava_b200
