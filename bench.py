@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-forward", action="store_true")
     ap.add_argument("--no-state4d", action="store_true")
+    ap.add_argument("--no-divide", action="store_true")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
     return ap.parse_args()
@@ -404,6 +405,48 @@ def run_state4d(ctx, case, dev, stream, max_over_ranks, peak):
             "peak_GB/s": peak}
 
 
+def run_divide(ctx, case, src, dev, stream, max_over_ranks, peak):
+    """Crava::divideDataByScaleWavelet (non-constant thickness) on all angle
+    stacks: device time per call; the HBM rate counts each stack read and
+    written once (the algorithmic minimum of the per-trace filter)."""
+    import numpy as np
+    import torch
+
+    nxp, nyp, nzp = case.nxp, case.nyp, case.nzp
+    data = [g.clone() for g in src[1]]
+    rng = np.random.default_rng(9)
+    rt = rng.uniform(0.8, 1.2, (nyp, nxp))
+    nz = case.nz
+    dz = float(np.float32(case.lz / nz))
+
+    def once():
+        ctx.divide_data_by_scale_wavelet(data, src[2][0], rt, nxp, nyp, dz)
+
+    # every call starts from the original stacks (copied outside the timed
+    # region): the division is not idempotent
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    reps, total = 5, 0.0
+    for rep in range(2 + reps):
+        with torch.cuda.stream(stream):
+            for d, s0 in zip(data, src[1]):
+                d.copy_(s0)
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        once()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        if rep >= 2:
+            total += ev0.elapsed_time(ev1)
+    ms = max_over_ranks(total / reps)
+    nbytes = 2 * len(data) * data[0].numel() * 4
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    del data
+    return {"workload": "divideDataByScaleWavelet, %d stacks %dx%dx%d" % (case.ntheta, nxp, nyp, nzp),
+            "ms_per_call": round(ms, 4), "GB/s": round(gbs, 1), "frac_of_peak": round(gbs / peak, 4),
+            "passes": "per stack: taper, z transform, per-trace filter, inverse z transform, scale"}
+
+
 def run_forward(ctx, case, src, dev, stream, max_over_ranks):
     """Synthetic seismic (Crava::computeSyntSeismic) of the three parameter
     grids for all angles: device time per call and HBM rate against the
@@ -647,6 +690,14 @@ def run_own(args):
         except Exception:
             hbm_peak = 6650.0
         s4 = run_state4d(ctx, case, dev, stream, max_over_ranks, hbm_peak)
+    div = None
+    if not args.no_divide:
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                hbm_peak = json.load(f).get("hbm_gbs") or 6650.0
+        except Exception:
+            hbm_peak = 6650.0
+        div = run_divide(ctx, case, src, dev, stream, max_over_ranks, hbm_peak)
 
     fwd = None
     if not args.no_forward:
@@ -729,6 +780,7 @@ def run_own(args):
         "forward_model": fwd,
         "prior_fill": prior,
         "state4d": s4,
+        "divide_by_scale_wavelet": div,
         "profiling_pass_ms_per_step": ms_serial,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,

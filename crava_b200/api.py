@@ -142,6 +142,8 @@ SYMBOLS = {
     "crava_gpu_state4d_advance_time": ([C.c_void_p, C.POINTER(State4DGrids), C.c_int, C.c_int, C.c_int,
                                         F64P, F64P, F64P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                         C.c_void_p, C.POINTER(C.c_longlong)], C.c_int),
+    "crava_gpu_divide_data_by_scale_wavelet": ([C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, F64P, C.c_int,
+                                                C.c_int, C.c_float, F32P, F32P], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -324,6 +326,23 @@ class Context:
         assert cxy.size == self.case.nxp * self.case.nyp
         check(self.lib.crava_gpu_fill_err_corr(self.handle, cxy.ctypes.data_as(F32P), grad_i, grad_j,
                                                _ptr(err)), "fill_err_corr")
+
+    def divide_data_by_scale_wavelet(self, data, cov_alpha, rel_thick, nx, ny, dz, shift=None, gain=None):
+        """Crava::divideDataByScaleWavelet (without interpolateSeismic) on
+        the device data grids, in place.  cov_alpha: the real-domain prior
+        covAlpha device grid; rel_thick: [nyp, nxp]; shift, gain:
+        [ntheta, ny, nx] or None."""
+        rt = np.ascontiguousarray(rel_thick, dtype=np.float64)
+        assert rt.size == self.case.nxp * self.case.nyp
+        arr = (C.c_void_p * len(data))(*[g.data_ptr() for g in data])
+        sh = np.ascontiguousarray(shift, dtype=np.float32) if shift is not None else None
+        gn = np.ascontiguousarray(gain, dtype=np.float32) if gain is not None else None
+        for x in (sh, gn):
+            assert x is None or x.size == len(data) * nx * ny
+        check(self.lib.crava_gpu_divide_data_by_scale_wavelet(
+            self.handle, arr, _ptr(cov_alpha), rt.ctypes.data_as(F64P), nx, ny, dz,
+            sh.ctypes.data_as(F32P) if sh is not None else None,
+            gn.ctypes.data_as(F32P) if gn is not None else None), "divide_data_by_scale_wavelet")
 
     # ---- time-lapse state (State4D, src/state4d.cpp) -------------------
     @staticmethod

@@ -33,6 +33,7 @@ SOURCES = {
     "prior.cu": [],
     "crava_file.cu": [],
     "state4d.cu": ["-fmad=false"],
+    "divide.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -396,6 +396,30 @@ int crava_gpu_fill_prior_cov(crava_gpu_ctx *ctx, const float *corr_xy, const flo
 int crava_gpu_fill_err_corr(crava_gpu_ctx *ctx, const float *corr_xy, float grad_i, float grad_j,
                             float *err_corr);
 
+/* Crava::divideDataByScaleWavelet (src/crava.cpp:591-722) with
+ * computeAdjustmentFactor (:725-817) for one-dimensional wavelets: every
+ * padded trace (i, j) of each angle's data grid (real padded layout, in
+ * place) is tapered below nz, transformed along z, multiplied in the band
+ * (lowCut, highCut) by the adjustment factor of its local wavelet (the
+ * context's wavelet stretched by rel_thick[j][i] = Simbox::getRelThick,
+ * shifted and scaled by the local time shift and gain), zeroed outside it
+ * and transformed back; the row padding is kept.  The closing
+ * FFTGrid::interpolateSeismic of low-energy traces is not part of it.
+ *   cov_alpha: device, the real-domain prior covAlpha grid (its (0,0,k)
+ *              column gives the temporal correlation, as
+ *              getPriorCorrTFiltered reads it);
+ *   rel_thick: host [nyp][nxp] doubles;
+ *   nx, ny:    unpadded lateral sizes (the traces' mirrored simbox index);
+ *   dz:        the wavelet's sampling interval (Wavelet::getDz), ms;
+ *   shift, gain: host [ntheta][ny][nx] local time shift (ms) and gain
+ *              grids (Wavelet::getLocalTimeshift / getLocalGainFactor;
+ *              -999 = missing), or NULL.
+ * Asynchronous on the context's stream. */
+int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *ctx, float *const *data,
+                                           const float *cov_alpha, const double *rel_thick,
+                                           int nx, int ny, float dz, const float *shift,
+                                           const float *gain);
+
 /* Simbox geometry stored in the header of a .crava grid file
  * (FFTGrid::writeCravaFile, src/fftgrid.cpp:2399-2433). */
 typedef struct crava_gpu_grid_header {

@@ -1280,3 +1280,194 @@ int orc_fill_gen_exp_corr(int nxp, int nyp, int nzp, double Rx, double Ry, doubl
       }
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Data divided by the local scale wavelet                              */
+/* ------------------------------------------------------------------ */
+/* Real inverse of a half spectrum (FFTW's complex_to_real: the imaginary
+ * parts of bin 0 and of bin n/2 are not read), unnormalised. */
+static void real_inverse(const cf *h, int n, float *out, double scale) {
+  cd *line = (cd *)malloc(sizeof(cd) * n);
+  int c = n / 2 + 1;
+  for (int k = 0; k < c; ++k) { line[k].re = h[k].re; line[k].im = h[k].im; }
+  line[0].im = 0.0;
+  if (n % 2 == 0) line[n / 2].im = 0.0;
+  for (int k = c; k < n; ++k) { line[k].re = h[n - k].re; line[k].im = -h[n - k].im; }
+  dft1d(line, n, +1);
+  for (int i = 0; i < n; ++i) out[i] = (float)(line[i].re * scale);
+  free(line);
+}
+
+/* FFTGrid::getDistToBoundary (src/fftgrid.cpp:1374-1414), i < np. */
+static float dist_to_boundary(int i, int n, int np) {
+  if (i < n) return 0.0f;
+  float taper = (float)((n < np - n ? n : np - n) / 2.1);
+  int below = np - i, above = i - (n - 1);
+  return above < below ? (float)(above / taper) : (float)(below / taper);
+}
+
+/* The simbox index of a padded trace (src/crava.cpp:622-640). */
+static int mirror_index(int i, int n, int np) {
+  if (i > 3 * n - 1) i = 0;
+  if (i > (np + n) / 2) i = np - i;
+  if (i >= n) i = 2 * n - i - 1;
+  return i;
+}
+
+/* Wavelet::findNormWithinFrequencyBand (src/wavelet.cpp:811-833). */
+static float band_norm(const cf *c, int nzp, float dz, float lo, float hi) {
+  int cnzp = nzp / 2 + 1;
+  float dOmega = (float)(1.0 / (nzp * dz * 0.001));
+  int loI = (int)floorf(lo / dOmega), hiI = (int)ceilf(hi / dOmega);
+  if (loI < 0) loI = 0;
+  if (hiI > cnzp) hiI = cnzp;
+  double fac = 1.0 / (double)nzp, norm2 = 0.0;
+  for (int i = loI; i < hiI; ++i) norm2 += (double)(2.0 * fac * (c[i].re * c[i].re + c[i].im * c[i].im));
+  if (loI == 0) norm2 -= fac * (c[0].re * c[0].re + c[0].im * c[0].im);
+  return (float)sqrt(norm2);
+}
+
+/* Crava::divideDataByScaleWavelet (src/crava.cpp:591-722) with
+ * computeAdjustmentFactor (:725-817), 1-D wavelets, without the closing
+ * interpolateSeismic: per trace the local wavelet (shiftAndScale,
+ * src/wavelet1D.cpp:539-561) goes back to the time domain, its
+ * difference wavelets (:420-479) and spectra are formed, and the trace's
+ * in-band bins are multiplied by the adjustment factor. */
+int orc_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
+                    const double *rel_thick, int nx, int ny, float dz, const float *shift,
+                    const float *gain) {
+  const int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta, nz = p->nz;
+  const int cnzp = nzp / 2 + 1, rnxp = 2 * (nxp / 2 + 1);
+  const float RM = -99999.0f, tolFac = 0.05f;
+  float *w = (float *)malloc(sizeof(float) * nzp), *r = (float *)malloc(sizeof(float) * nzp);
+  float *wl = (float *)malloc(sizeof(float) * nzp), *e1 = (float *)malloc(sizeof(float) * nzp);
+  float *e2 = (float *)malloc(sizeof(float) * nzp), *e3 = (float *)malloc(sizeof(float) * nzp);
+  float *tr = (float *)malloc(sizeof(float) * nzp);
+  cf *W = (cf *)malloc(sizeof(cf) * cnzp), *Wl = (cf *)malloc(sizeof(cf) * cnzp);
+  cf *E3 = (cf *)malloc(sizeof(cf) * cnzp), *R = (cf *)malloc(sizeof(cf) * cnzp);
+  cf *D = (cf *)malloc(sizeof(cf) * cnzp), *adj = (cf *)malloc(sizeof(cf) * cnzp);
+  const float sq = (float)sqrtf((float)nzp);
+  for (int l = 0; l < nt; ++l) {
+    memcpy(w, p->wavelet + (size_t)l * nzp, sizeof(float) * nzp);
+    const float wn = p->wavelet_norm ? p->wavelet_norm[l] : time_norm(w, nzp);
+    real_spectrum(w, nzp, W);
+    /* rcCovT: computeReflectionCoefficientTimeCovariance (:476-508) on
+     * getPriorCorrTFiltered (src/seismicparametersholder.cpp:504-530) */
+    double eiVar = 0.0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        eiVar += p->A[3 * l + a] * (float)p->var0[3 * a + b] * p->A[3 * l + b];
+    float constant = cov_col[0];
+    for (int i = 0; i < nzp; ++i) {
+      int refk = i < nzp / 2 + 1 ? i : nzp - i;
+      float corr = refk < nz ? cov_col[refk] / constant : 0.0f;
+      r[i] = (float)(eiVar * corr);
+    }
+    {
+      float first = r[0], prev = r[nzp - 1];
+      for (int i = 0; i < nzp - 1; ++i) {
+        float curr = r[i], next = r[i + 1];
+        r[i] = 2 * curr - next - prev;
+        prev = curr;
+      }
+      r[nzp - 1] = 2 * r[nzp - 1] - first - prev;
+    }
+    real_spectrum(r, nzp, R);
+    float modW = wn;
+    modW *= modW;
+    float maxfrequency = (float)((nzp / 2) * 1000.0 * nz) / (float)(p->lz * nzp);
+    modW *= maxfrequency / p->high_cut;
+    const float errorVar = (float)p->theta_cov[l * nt + l];
+    for (int j = 0; j < nyp; ++j)
+      for (int i = 0; i < nxp; ++i) {
+        int iInd = mirror_index(i, nx, nxp), jInd = mirror_index(j, ny, nyp);
+        /* the local wavelet: shiftAndScale of the spectrum, then back to
+         * the time domain (the Wavelet(wavelet, difftype) constructor) */
+        float ts = 0.0f, g = 1.0f;
+        /* getLocalTimeshift / getLocalGainFactor: only inside the grids
+         * (src/wavelet.cpp:1143-1172) */
+        if (iInd >= 0 && iInd < nx && jInd >= 0 && jInd < ny) {
+          size_t o = (size_t)l * nx * ny + iInd + (size_t)nx * jInd;
+          if (shift && shift[o] != -999.0f) ts = shift[o];
+          if (gain && gain[o] != -999.0f) g = gain[o];
+        }
+        float iShift = ts / dz;
+        for (int k = 0; k < cnzp; ++k) {
+          cf am, t;
+          am.re = (float)(g * cos(2.0 * (3.14159265358979323846 * (iShift) * k) / (float)nzp));
+          am.im = (float)(g * sin(-2.0 * (3.14159265358979323846 * (iShift) * k) / (float)nzp));
+          t.re = am.re * W[k].re - am.im * W[k].im;
+          t.im = am.im * W[k].re + am.re * W[k].im;
+          Wl[k] = t;
+        }
+        real_inverse(Wl, nzp, wl, 1.0 / (double)nzp);
+        for (int n = 0; n < nzp; ++n) e1[n] = (n == nzp - 1) ? wl[0] - wl[n] : wl[n + 1] - wl[n];
+        for (int n = 0; n < nzp; ++n) e2[n] = (n == 0) ? e1[0] - e1[nzp - 1] : e1[n] - e1[n - 1];
+        for (int n = 0; n < nzp; ++n) {
+          float d = (n == 0) ? e2[1] - e2[nzp - 1] : (n == nzp - 1) ? e2[0] - e2[n - 1] : e2[n + 1] - e2[n - 1];
+          e3[n] = (float)(0.5 * d);
+        }
+        real_spectrum(e3, nzp, E3);
+        {
+          float inv = 1.0f / band_norm(E3, nzp, dz, p->low_cut, p->high_cut);
+          float *f = (float *)E3; /* multiplyRAmpByConstant: floats past nzp RMISSING */
+          for (int q = 0; q < 2 * cnzp; ++q) f[q] = q < nzp ? f[q] * inv : RM;
+        }
+        real_spectrum(wl, nzp, Wl); /* wLocal->fft1DInPlace() */
+        double relT = rel_thick[i + (size_t)nxp * j];
+        float sf = (float)(relT * 1.0f);
+        for (int k = 0; k < cnzp; ++k) {
+          cf wLoc = get_camp_scaled(Wl, nzp, k, sf);
+          float wLoc2 = wLoc.re * wLoc.re + wLoc.im * wLoc.im;
+          cf wGlob = W[k];
+          float wGlob2 = wGlob.re * wGlob.re + wGlob.im * wGlob.im;
+          cf v = wLoc;
+          float sizeLoc = (v.re * v.re + v.im * v.im) / (wn * wn);
+          v = get_camp_scaled(E3, nzp, k, sf);
+          sizeLoc += v.re * v.re + v.im * v.im;
+          v = Wl[k];
+          float sizeGlob = (v.re * v.re + v.im * v.im) / (wn * wn);
+          v = E3[k];
+          sizeGlob += v.re * v.re + v.im * v.im;
+          float sigma2Loc = errorVar * (p->wnc + (1.0f - p->wnc) * 0.5f * sizeLoc);
+          float sigma2Glob = errorVar * (p->wnc + (1.0f - p->wnc) * 0.5f * sizeGlob);
+          float tau2 = fabsf(R[k].re);
+          float wGlob2Adj = wGlob2, wLoc2Adj = wLoc2;
+          if (wGlob2 < tolFac * modW) wGlob2Adj = (float)(0.5f * (wGlob2 + tolFac * modW));
+          if (wLoc2 < tolFac * modW) wLoc2Adj = (float)(0.5f * (wLoc2 + tolFac * modW));
+          if (wLoc2Adj < tolFac * wGlob2Adj) {
+            wLoc2Adj = (float)(0.5f * (wLoc2 + tolFac * wGlob2Adj));
+            sigma2Loc *= wLoc2Adj / wLoc2;
+          }
+          adj[k].re = (wLoc.re / (tau2 * wLoc2Adj + sigma2Loc)) / (wGlob2Adj / (tau2 * wGlob2 + sigma2Glob));
+          adj[k].im = (wLoc.im / (tau2 * wLoc2Adj + sigma2Loc)) / (wGlob2Adj / (tau2 * wGlob2 + sigma2Glob));
+        }
+        /* the trace: taper, transform, adjust in band, transform back */
+        float *g0 = data[l] + i + (size_t)rnxp * j;
+        for (int k = 0; k < nzp; ++k) {
+          tr[k] = g0[(size_t)rnxp * nyp * k] / sq;
+          if (k > nz) {
+            float dist = dist_to_boundary(k, nz, nzp);
+            float m = 1 - dist * dist;
+            tr[k] *= m > 0.0f ? m : 0.0f;
+          }
+        }
+        real_spectrum(tr, nzp, D);
+        double deltaF = (double)nz * 1000.0 / (relT * p->lz * (double)nzp);
+        for (int k = 0; k < cnzp; ++k) {
+          if ((deltaF * k < p->high_cut) && (deltaF * k > p->low_cut)) {
+            float tmp = D[k].re * adj[k].re - D[k].im * adj[k].im;
+            D[k].im = D[k].im * adj[k].re + D[k].re * adj[k].im;
+            D[k].re = tmp;
+          } else {
+            D[k].re = 0.0f; D[k].im = 0.0f;
+          }
+        }
+        real_inverse(D, nzp, tr, 1.0);
+        for (int k = 0; k < nzp; ++k) g0[(size_t)rnxp * nyp * k] = tr[k] / sq;
+      }
+  }
+  free(w); free(r); free(wl); free(e1); free(e2); free(e3); free(tr);
+  free(W); free(Wl); free(E3); free(R); free(D); free(adj);
+  return 0;
+}

@@ -110,6 +110,12 @@ void orc_state4d_evolve(long long n, float *const *ms, float *const *md,
                         float *const *ss, float *const *dd, float *const *sd,
                         const double *E, const double *cm, const double *cc,
                         const float *lambda, float zero_scale);
+/* Crava::divideDataByScaleWavelet without interpolateSeismic: data
+ * [ntheta] real padded grids (in place), cov_col [nzp] covAlpha(0,0,k),
+ * rel_thick [nyp][nxp], shift / gain [ntheta][ny][nx] or NULL. */
+int orc_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
+                    const double *rel_thick, int nx, int ny, float dz, const float *shift,
+                    const float *gain);
 int orc_fill_gen_exp_corr(int nxp, int nyp, int nzp, double rx, double ry, double rz,
                           float grad_i, float grad_j, float *out);
 int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
@@ -142,6 +148,9 @@ int ref_circ_corr_t(const float *prior_corr_t, int n, int low_int_cut, int nzp,
 int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,
                      const float *A, const float *wavelet, const float *const *m,
                      float *const *out);
+int ref_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
+                    const double *rel_thick, int nx, int ny, float dz, const float *shift,
+                    const float *gain);
 void ref_state4d_merge(long long n, const float *const *ms, const float *const *md,
                        const float *const *ss, const float *const *dd,
                        const float *const *sd, float *const *mu, float *const *cov);

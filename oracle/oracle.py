@@ -110,6 +110,9 @@ def _load(which: str):
         f = lib.orc_sim_filter_fp64
         f.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(F32P), C.POINTER(F32P), C.POINTER(C.c_longlong)]
         f.restype = C.c_int
+    f = getattr(lib, f"{p}_divide_data")
+    f.argtypes = [C.POINTER(Params), C.POINTER(F32P), F32P, F64P, C.c_int, C.c_int, C.c_float, F32P, F32P]
+    f.restype = C.c_int
     s4 = [C.POINTER(F32P)] * 7
     f = getattr(lib, f"{p}_state4d_merge")
     f.argtypes = [C.c_longlong] + s4
@@ -329,6 +332,23 @@ def fill_err_corr(nxp, nyp, nzp, corr_xy, grad_i, grad_j):
     cxy = np.ascontiguousarray(corr_xy, dtype=np.float32)
     out = np.zeros((nzp, nyp, 2 * (nxp // 2 + 1)), np.float32)
     assert lib.orc_fill_err_corr(nxp, nyp, nzp, _fp(cxy), grad_i, grad_j, _fp(out)) == 0
+    return out
+
+
+def divide_data(case, data, cov_col, rel_thick, nx, ny, dz, shift=None, gain=None, which="orc"):
+    """Crava::divideDataByScaleWavelet without interpolateSeismic: returns
+    new data grids (the inputs are not changed)."""
+    keep = []
+    p, keep = make_params(case, keep)
+    out = [np.ascontiguousarray(g, dtype=np.float32).copy() for g in data]
+    col = np.ascontiguousarray(cov_col, dtype=np.float32)
+    rt = np.ascontiguousarray(rel_thick, dtype=np.float64)
+    sh = np.ascontiguousarray(shift, dtype=np.float32) if shift is not None else None
+    gn = np.ascontiguousarray(gain, dtype=np.float32) if gain is not None else None
+    rc = getattr(_load(which), f"{which}_divide_data")(
+        C.byref(p), _ptrs(out), _fp(col), _dp(rt), nx, ny, dz,
+        _fp(sh) if sh is not None else None, _fp(gn) if gn is not None else None)
+    assert rc == 0
     return out
 
 

@@ -736,4 +736,212 @@ long long ref_state4d_split(long long n, float *const *ms_, float *const *md_,
   return counter;
 }
 
+/* Crava::divideDataByScaleWavelet (src/crava.cpp:591-722) with
+ * computeAdjustmentFactor (:725-817), 1-D wavelets, without the closing
+ * interpolateSeismic, on the reference's FFTW: every transform the
+ * reference makes per trace (the global wavelet back to the time domain by
+ * the local copy's constructor and forward again by computeAdjustmentFactor,
+ * the local wavelet's shiftAndScale, inverse, difference wavelets and
+ * forward transforms, the reflection-coefficient covariance, the data
+ * trace) is made here with rfftwnd in the same order. */
+int ref_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
+                    const double *rel_thick, int nx, int ny, float dz, const float *shift,
+                    const float *gain) {
+  const int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta, nz = p->nz;
+  const int cnzp = nzp / 2 + 1, rnzp = 2 * cnzp, rnxp = 2 * (nxp / 2 + 1);
+  const float RM = -99999.0f, tolFac = 0.05f;
+  rfftwnd_plan fwd = rfftwnd_create_plan(1, &nzp, FFTW_REAL_TO_COMPLEX, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_plan inv = rfftwnd_create_plan(1, &nzp, FFTW_COMPLEX_TO_REAL, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  fftw_real *gw = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));  /* global wavelet */
+  fftw_real *lw = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));  /* local wavelet */
+  fftw_real *e1 = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_real *e2 = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_real *e3 = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_real *rc = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_real *rd = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  std::vector<fftw_complex> adj(cnzp);
+  auto to_c = [](fftw_real *r) { return reinterpret_cast<fftw_complex *>(r); };
+  /* Wavelet::invFFT1DInPlace (src/wavelet.cpp:264-280) */
+  auto inverse = [&](fftw_real *r) {
+    rfftwnd_one_complex_to_real(inv, to_c(r), r);
+    double scale = static_cast<double>(1.0 / static_cast<double>(nzp));
+    for (int i = 0; i < nzp; i++) r[i] = static_cast<fftw_real>(r[i] * scale);
+  };
+  auto forward = [&](fftw_real *r) { rfftwnd_one_real_to_complex(fwd, r, to_c(r)); };
+  /* Wavelet::getCAmp(k, scale), k < cnzp (src/wavelet.cpp:327-385) */
+  auto camp = [&](const fftw_complex *c, int k, float scale) {
+    fftw_complex value;
+    float omega = float(k) / scale;
+    if (omega >= cnzp) { value.re = 0.0f; value.im = 0.0f; }
+    else {
+      int omL = int(std::floor(omega)), omU = int(std::floor(omega)) + 1;
+      if (omU >= cnzp) omU -= 1;
+      float dOmega = omega - float(omL);
+      value.re = c[omL].re * (1.0f - dOmega) + c[omU].re * dOmega;
+      value.im = (c[omL].im * (1.0f - dOmega) + c[omU].im * dOmega);
+    }
+    value.re /= scale; value.im /= scale;
+    return value;
+  };
+  auto band_norm = [&](const fftw_complex *c) {  /* findNormWithinFrequencyBand */
+    double norm2 = 0.0;
+    float dOmega = 1.0 / (nzp * dz * 0.001);
+    int loI = std::max<int>(0, static_cast<int>(std::floor(p->low_cut / dOmega)));
+    int hiI = std::min<int>(cnzp, static_cast<int>(std::ceil(p->high_cut / dOmega)));
+    double fac = 1.0 / double(nzp);
+    for (int i = loI; i < hiI; i++) norm2 += static_cast<double>(2.0 * fac * (c[i].re * c[i].re + c[i].im * c[i].im));
+    if (loI == 0) norm2 -= fac * (c[0].re * c[0].re + c[0].im * c[0].im);
+    return static_cast<float>(std::sqrt(norm2));
+  };
+  const float sq = static_cast<float>(std::sqrt(static_cast<float>(nzp)));
+  for (int l = 0; l < nt; ++l) {
+    for (int i = 0; i < rnzp; ++i) gw[i] = i < nzp ? p->wavelet[static_cast<long>(l) * nzp + i] : 0.0f;
+    bool gReal = true;
+    const float wn = p->wavelet_norm ? p->wavelet_norm[l] : [&] {
+      double s = 0.0;
+      for (int i = 0; i < nzp; i++) s += static_cast<double>(gw[i] * gw[i]);
+      return static_cast<float>(std::sqrt(s));
+    }();
+    const float errorVar = static_cast<float>(p->theta_cov[l * nt + l]);
+    for (int i = 0; i < nxp; i++)
+      for (int j = 0; j < nyp; j++) {
+        int iInd = i, jInd = j;
+        if (iInd > 3 * nx - 1) iInd = 0;
+        if (jInd > 3 * ny - 1) jInd = 0;
+        if ((iInd > (nxp + nx) / 2)) iInd = nxp - iInd;
+        if (iInd >= nx) iInd = 2 * nx - iInd - 1;
+        if (jInd > (nyp + ny) / 2) jInd = nyp - jInd;
+        if (jInd >= ny) jInd = 2 * ny - jInd - 1;
+        /* the data trace */
+        const long t0 = i + static_cast<long>(rnxp) * j, plane = static_cast<long>(rnxp) * nyp;
+        for (int k = 0; k < nzp; k++) {
+          rd[k] = data[l][t0 + k * plane] / sq;
+          if (k > nz) {
+            float dist;
+            {
+              float taper = static_cast<float>((std::min(nz, nzp - nz) / 2.1));
+              int below = nzp - k, above = k - (nz - 1);
+              dist = above < below ? static_cast<float>(above / taper) : static_cast<float>(below / taper);
+            }
+            rd[k] *= std::max<float>(1 - dist * dist, 0);
+          }
+        }
+        forward(rd);
+        /* createLocalWavelet1D: the copy constructor returns the global
+         * wavelet to the time domain, then shiftAndScale */
+        if (!gReal) { inverse(gw); gReal = true; }
+        for (int q = 0; q < rnzp; ++q) lw[q] = q < nzp ? gw[q] : 0.0f;
+        float ts = 0.0f, g = 1.0f;
+        if (iInd >= 0 && iInd < nx && jInd >= 0 && jInd < ny) {  /* src/wavelet.cpp:1143-1172 */
+          const long o = static_cast<long>(l) * nx * ny + iInd + static_cast<long>(nx) * jInd;
+          if (shift && shift[o] != -999.0f) ts = shift[o];
+          if (gain && gain[o] != -999.0f) g = gain[o];
+        }
+        forward(lw);
+        {
+          float iShift = ts / dz;
+          fftw_complex *c = to_c(lw);
+          for (int k = 0; k < cnzp; k++) {
+            fftw_complex am, tmp;
+            am.re = float(g * cos(2.0 * (3.14159265358979323846 * (iShift) * k) / float(nzp)));
+            am.im = float(g * sin(-2.0 * (3.14159265358979323846 * (iShift) * k) / float(nzp)));
+            tmp.re = am.re * c[k].re - am.im * c[k].im;
+            tmp.im = am.im * c[k].re + am.re * c[k].im;
+            c[k] = tmp;
+          }
+        }
+        double relT = rel_thick[i + static_cast<long>(nxp) * j];
+        double sfLoc = relT * 1.0f;
+        /* computeAdjustmentFactor: the reflection-coefficient covariance */
+        {
+          double eiVar = 0.0;
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+              eiVar += p->A[3 * l + a] * static_cast<float>(p->var0[3 * a + b]) * p->A[3 * l + b];
+          float constant = cov_col[0];
+          for (int k = 0; k < nzp; k++) {
+            int refk = k < nzp / 2 + 1 ? k : nzp - k;
+            float corr = refk < nz ? cov_col[refk] / constant : 0.0f;
+            rc[k] = static_cast<fftw_real>(eiVar * corr);
+          }
+          fftw_real first = rc[0], prev = rc[nzp - 1];
+          for (int k = 0; k < nzp - 1; k++) {
+            fftw_real curr = rc[k], next = rc[k + 1];
+            rc[k] = 2 * curr - next - prev;
+            prev = curr;
+          }
+          rc[nzp - 1] = 2 * rc[nzp - 1] - first - prev;
+          forward(rc);
+        }
+        /* difference wavelets of the local wavelet (back in time first) */
+        inverse(lw);
+        for (int k = 0; k < rnzp; k++) e1[k] = k < nzp ? ((k == nzp - 1) ? lw[0] - lw[k] : lw[k + 1] - lw[k]) : RM;
+        for (int k = 0; k < rnzp; k++) e2[k] = k < nzp ? ((k == 0) ? e1[0] - e1[nzp - 1] : e1[k] - e1[k - 1]) : RM;
+        for (int k = 0; k < rnzp; k++) {
+          if (k >= nzp) { e3[k] = RM; continue; }
+          if (k == 0) e3[k] = static_cast<fftw_real>(0.5 * (e2[k + 1] - e2[nzp - 1]));
+          else if (k == nzp - 1) e3[k] = static_cast<fftw_real>(0.5 * (e2[0] - e2[k - 1]));
+          else e3[k] = static_cast<fftw_real>(0.5 * (e2[k + 1] - e2[k - 1]));
+        }
+        forward(e3);
+        {
+          float c3 = 1.0f / band_norm(to_c(e3));
+          for (int k = 0; k < rnzp; k++) e3[k] = k < nzp ? e3[k] * c3 : RM;
+        }
+        forward(lw);
+        if (gReal) { forward(gw); gReal = false; }  /* wGlobal->fft1DInPlace() */
+        float modW = wn;
+        modW *= modW;
+        float maxfrequency = static_cast<float>((nzp / 2) * 1000.0 * nz) / static_cast<float>(p->lz * nzp);
+        modW *= maxfrequency / static_cast<float>(p->high_cut);
+        const fftw_complex *W = to_c(gw), *Wl = to_c(lw), *E3 = to_c(e3), *R = to_c(rc);
+        float sf = static_cast<float>(sfLoc);
+        for (int k = 0; k < cnzp; k++) {
+          fftw_complex wLoc = camp(Wl, k, sf);
+          float wLoc2 = (wLoc.re * wLoc.re + wLoc.im * wLoc.im);
+          fftw_complex wGlob = W[k];
+          float wGlob2 = (wGlob.re * wGlob.re + wGlob.im * wGlob.im);
+          fftw_complex eSkLoc = camp(Wl, k, sf);
+          float sizeESkLoc = (eSkLoc.re * eSkLoc.re + eSkLoc.im * eSkLoc.im) / (wn * wn);
+          eSkLoc = camp(E3, k, sf);
+          sizeESkLoc += eSkLoc.re * eSkLoc.re + eSkLoc.im * eSkLoc.im;
+          fftw_complex eSkGlob = Wl[k];
+          float sizeESkGlob = (eSkGlob.re * eSkGlob.re + eSkGlob.im * eSkGlob.im) / (wn * wn);
+          eSkGlob = E3[k];
+          sizeESkGlob += eSkGlob.re * eSkGlob.re + eSkGlob.im * eSkGlob.im;
+          float sigma2Loc = errorVar * (p->wnc + (1.0f - p->wnc) * 0.5f * sizeESkLoc);
+          float sigma2Glob = errorVar * (p->wnc + (1.0f - p->wnc) * 0.5f * sizeESkGlob);
+          float tau2 = std::fabs(static_cast<float>(R[k].re));
+          float wGlob2Adj = wGlob2, wLoc2Adj = wLoc2;
+          if (wGlob2 < tolFac * modW) wGlob2Adj = float(0.5f * (wGlob2 + tolFac * modW));
+          if (wLoc2 < tolFac * modW) wLoc2Adj = float(0.5f * (wLoc2 + tolFac * modW));
+          if (wLoc2Adj < tolFac * wGlob2Adj) {
+            wLoc2Adj = float(0.5f * (wLoc2 + tolFac * wGlob2Adj));
+            sigma2Loc *= wLoc2Adj / wLoc2;
+          }
+          adj[k].re = (wLoc.re / (tau2 * wLoc2Adj + sigma2Loc)) / (wGlob2Adj / (tau2 * wGlob2 + sigma2Glob));
+          adj[k].im = (wLoc.im / (tau2 * wLoc2Adj + sigma2Loc)) / (wGlob2Adj / (tau2 * wGlob2 + sigma2Glob));
+        }
+        double deltaF = static_cast<double>(nz) * 1000.0 / (relT * p->lz * static_cast<double>(nzp));
+        fftw_complex *cd = to_c(rd);
+        for (int k = 0; k < cnzp; k++) {
+          if ((deltaF * k < p->high_cut) && (deltaF * k > p->low_cut)) {
+            fftw_real tmp = cd[k].re * adj[k].re - cd[k].im * adj[k].im;
+            cd[k].im = cd[k].im * adj[k].re + cd[k].re * adj[k].im;
+            cd[k].re = tmp;
+          } else {
+            cd[k].im = 0.0f;
+            cd[k].re = 0.0f;
+          }
+        }
+        rfftwnd_one_complex_to_real(inv, cd, rd);
+        for (int k = 0; k < nzp; k++) data[l][t0 + k * plane] = rd[k] / sq;
+      }
+  }
+  fftw_free(gw); fftw_free(lw); fftw_free(e1); fftw_free(e2); fftw_free(e3); fftw_free(rc); fftw_free(rd);
+  fftwnd_destroy_plan(fwd);
+  fftwnd_destroy_plan(inv);
+  return 0;
+}
+
 }  /* extern "C" */

@@ -80,6 +80,47 @@ def make_state4d():
     print("state4d written, split shortcuts", out["split_fail"])
 
 
+DIVIDE = {  # golden case -> (nx, ny, nz, with local shift and gain grids)
+    "c3_12x10x16": (10, 8, 12, False),
+    "c2_9x8x20_odd": (7, 6, 16, True),
+}
+
+
+def divide_inputs(case, nx, ny, local, seed=21):
+    """Seeded relative thickness, local shift / gain grids, and dz."""
+    rng = np.random.default_rng(seed)
+    rt = rng.uniform(0.7, 1.3, (case.nyp, case.nxp))
+    shift = gain = None
+    if local:
+        shift = rng.uniform(-6.0, 6.0, (case.ntheta, ny, nx)).astype(np.float32)
+        gain = rng.uniform(0.6, 1.4, (case.ntheta, ny, nx)).astype(np.float32)
+        shift[0, 0, 0] = -999.0  # WELLMISSING: no shift there
+    dz = float(np.float32(case.lz / case.nz))
+    return rt, shift, gain, dz
+
+
+def make_divide():
+    """Crava::divideDataByScaleWavelet through the reference's FFTW
+    (oracle/_ref) on two golden cases."""
+    from tests import golden_cases as GC
+
+    out = {}
+    for name, (nx, ny, nz, local) in DIVIDE.items():
+        case, _ = GC.load(name)
+        case.nz = nz
+        rt, shift, gain, dz = divide_inputs(case, nx, ny, local)
+        col = case.cov[0][:, 0, 0].copy()
+        res = O.divide_data(case, case.data, col, rt, nx, ny, dz, shift, gain, "ref")
+        out[f"{name}_out"] = np.stack(res)
+        out[f"{name}_rel_thick"] = rt
+        out[f"{name}_dz"] = np.float32(dz)
+        out[f"{name}_size"] = np.array([nx, ny, nz])
+        if local:
+            out[f"{name}_shift"], out[f"{name}_gain"] = shift, gain
+    np.savez_compressed(os.path.join(HERE, "divide.npz"), **out)
+    print("divide written")
+
+
 def main():
     if not O.have_ref():
         O.build(ref=True)
@@ -88,6 +129,9 @@ def main():
         return
     if "--state4d-only" in sys.argv:
         make_state4d()
+        return
+    if "--divide-only" in sys.argv:
+        make_divide()
         return
     for name, spec in CASES.items():
         case = make_case(spec)
@@ -119,6 +163,7 @@ def main():
     print("rng written")
     make_synt()
     make_state4d()
+    make_divide()
 
 
 if __name__ == "__main__":

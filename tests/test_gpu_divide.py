@@ -1,0 +1,69 @@
+"""The data divided by the local scale wavelet (Crava::divideDataByScaleWavelet,
+src/crava.cpp:591-722, without interpolateSeismic) on the device: against the
+reference's FFTW sequence (committed fixture) and the restatement, with and
+without local shift and gain grids, even and odd sizes; padding kept."""
+import os
+
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+from oracle import oracle as O
+from tests import golden_cases as GC
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("name", ["c3_12x10x16", "c2_9x8x20_odd"])
+def test_divide_vs_reference_fixture(name):
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "divide.npz"))
+    case, _ = GC.load(name)
+    nx, ny, nz = (int(v) for v in z[f"{name}_size"])
+    case.nz = nz
+    shift = z[f"{name}_shift"] if f"{name}_shift" in z else None
+    gain = z[f"{name}_gain"] if f"{name}_gain" in z else None
+    ctx = api.Context(case)
+    data = [api.to_device(g) for g in case.data]
+    cov = api.to_device(case.cov[0])
+    ctx.divide_data_by_scale_wavelet(data, cov, z[f"{name}_rel_thick"], nx, ny, float(z[f"{name}_dz"]),
+                                     shift, gain)
+    for g, ref, orig in zip(data, z[f"{name}_out"], case.data):
+        out = g.cpu().numpy()
+        assert rel(out[..., :case.nxp], ref[..., :case.nxp]) < 1e-5
+        assert np.array_equal(out[..., case.nxp:], orig[..., case.nxp:])  # row padding kept
+
+
+@pytest.mark.parametrize("shape,nxy,local", [((64, 48, 96), (56, 40), True), ((75, 21, 35), (70, 20), False),
+                                             ((16, 1, 32), (14, 1), True)])
+def test_divide_vs_restatement(shape, nxy, local):
+    nxp, nyp, nzp = shape
+    nx, ny = nxy
+    case = synth.make_case(nxp, nyp, nzp, (0.0, 15.0, 30.0), 0.1, seed=41)
+    case.nz = nzp - 8
+    rng = np.random.default_rng(5)
+    rt = rng.uniform(0.75, 1.25, (nyp, nxp))
+    shift = rng.uniform(-5, 5, (3, ny, nx)).astype(np.float32) if local else None
+    gain = rng.uniform(0.7, 1.3, (3, ny, nx)).astype(np.float32) if local else None
+    dz = float(np.float32(case.lz / case.nz))
+    ctx = api.Context(case)
+    data = [api.to_device(g) for g in case.data]
+    ctx.divide_data_by_scale_wavelet(data, api.to_device(case.cov[0]), rt, nx, ny, dz, shift, gain)
+    ref = O.divide_data(case, case.data, case.cov[0][:, 0, 0].copy(), rt, nx, ny, dz, shift, gain, "orc")
+    for g, r in zip(data, ref):
+        assert rel(g.cpu().numpy()[..., :nxp], r[..., :nxp]) < 1e-5
+
+
+def test_divide_rejects_bad_arguments():
+    case = synth.make_case(16, 12, 32, (10.0,), 0.1, seed=1)
+    ctx = api.Context(case)
+    data = [api.to_device(g) for g in case.data]
+    cov = api.to_device(case.cov[0])
+    rt = np.ones((12, 16))
+    with pytest.raises(api.CravaGpuError):
+        ctx.divide_data_by_scale_wavelet(data, cov, rt, 17, 12, 4.0)  # nx above nxp
+    with pytest.raises(api.CravaGpuError):
+        ctx.divide_data_by_scale_wavelet(data, cov, rt, 16, 12, 0.0)  # dz not positive
