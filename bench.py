@@ -689,7 +689,9 @@ def run_own(args):
                 hbm_peak = json.load(f).get("hbm_gbs") or 6650.0
         except Exception:
             hbm_peak = 6650.0
+        torch.cuda.nvtx.range_push("state4d")  # ncu --nvtx --nvtx-include "state4d/"
         s4 = run_state4d(ctx, case, dev, stream, max_over_ranks, hbm_peak)
+        torch.cuda.nvtx.range_pop()
     div = None
     if not args.no_divide:
         try:
@@ -697,7 +699,9 @@ def run_own(args):
                 hbm_peak = json.load(f).get("hbm_gbs") or 6650.0
         except Exception:
             hbm_peak = 6650.0
+        torch.cuda.nvtx.range_push("divide")  # ncu --nvtx --nvtx-include "divide/"
         div = run_divide(ctx, case, src, dev, stream, max_over_ranks, hbm_peak)
+        torch.cuda.nvtx.range_pop()
 
     fwd = None
     if not args.no_forward:

@@ -429,6 +429,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->W);
   cudaFree(c->synt_H);
   cudaFree(c->prior_buf);
+  cudaFree(c->div_buf);
   cudaFree(c->file_dev);
   if (c->file_host) cudaFreeHost(c->file_host);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);

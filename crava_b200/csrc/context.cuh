@@ -61,6 +61,10 @@ struct crava_gpu_ctx {
   int n_inverted = 0;
   // prior fills: lateral [nyp][nxp] then temporal [nzp] correlation (device)
   float *prior_buf = nullptr;
+  // divideDataByScaleWavelet scratch (tables, per-trace values, row
+  // padding), kept between calls and grown when a call needs more
+  char *div_buf = nullptr;
+  size_t div_bytes = 0;
 };
 
 namespace crava {

@@ -201,31 +201,36 @@ constexpr int kRowsPerBlock = kThreads / 32;
 __global__ void __launch_bounds__(kThreads) k_div_pre(const __grid_constant__ DivPassArgs a) {
   const int row = blockIdx.x * kRowsPerBlock + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (row >= a.nyp * a.nzp) return;
-  const int k = row / a.nyp, cnxp = a.rnxp / 2, npad = a.rnxp - a.nxp;
-  float2 *r = reinterpret_cast<float2 *>(a.grid + (long long)row * a.rnxp);
-  float *pad = a.pads + (long long)row * npad;
+  const int k = row / a.nyp, cnxp = a.rnxp / 2;
+  float2 *__restrict__ r = reinterpret_cast<float2 *>(a.grid + (long long)row * a.rnxp);
   float taper = 1.0f;
   if (k > a.nz) {
     const float d = dist_to_boundary(k, a.nz, a.nzp);
     taper = fmaxf(__fsub_rn(1.0f, __fmul_rn(d, d)), 0.0f);
   }
+  const bool tap = k > a.nz;
   for (int x = lane; x < cnxp; x += 32) {
     float2 v = r[x];
     const int i = 2 * x;
     if (i < a.nxp) {
       v.x = __fdiv_rn(v.x, a.sq);
-      if (k > a.nz) v.x = __fmul_rn(v.x, taper);
-    } else {
-      pad[i - a.nxp] = v.x;
+      if (tap) v.x = __fmul_rn(v.x, taper);
     }
     if (i + 1 < a.nxp) {
       v.y = __fdiv_rn(v.y, a.sq);
-      if (k > a.nz) v.y = __fmul_rn(v.y, taper);
-    } else {
-      pad[i + 1 - a.nxp] = v.y;
+      if (tap) v.y = __fmul_rn(v.y, taper);
     }
     r[x] = v;
   }
+}
+
+// The row padding (x >= nxp) set aside before the passes, one thread per row.
+__global__ void __launch_bounds__(kThreads) k_div_save_pads(const __grid_constant__ DivPassArgs a) {
+  const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= (long long)a.nyp * a.nzp) return;
+  const int npad = a.rnxp - a.nxp;
+  const float *src = a.grid + row * a.rnxp + a.nxp;
+  for (int q = 0; q < npad; ++q) a.pads[row * npad + q] = src[q];
 }
 
 // After the inverse pass: value / sqrt(nzp) (:712-715); padding restored.
@@ -322,7 +327,7 @@ template <bool E3TAB>
 __device__ __forceinline__ float2 camp_scaled(const float2 *tab, int k, float scale, int nzp,
                                               const Local &L, float inv) {
   const int cnzp = nzp / 2 + 1;
-  const float omega = __fdiv_rn((float)k, scale);
+  const float omega = __fdividef((float)k, scale);
   float2 v = make_float2(0.0f, 0.0f);
   if (omega < (float)cnzp) {
     const int omL = (int)floorf(omega);
@@ -334,13 +339,17 @@ __device__ __forceinline__ float2 camp_scaled(const float2 *tab, int k, float sc
     v.x = __fadd_rn(__fmul_rn(a.x, dL), __fmul_rn(b.x, dO));
     v.y = __fadd_rn(__fmul_rn(a.y, dL), __fmul_rn(b.y, dO));
   }
-  return make_float2(__fdiv_rn(v.x, scale), __fdiv_rn(v.y, scale));
+  return make_float2(__fdividef(v.x, scale), __fdividef(v.y, scale));
 }
 
 __device__ __forceinline__ float sq2(float2 v) { return __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)); }
 
 // computeAdjustmentFactor's value at bin k (src/crava.cpp:779-810) times
-// the data bin, or 0 outside the band (:700-710).
+// the data bin, or 0 outside the band (:700-710).  The reference's float
+// operations in its order, with its divisions as multiplications by the
+// approximate reciprocal (__fdividef, 2 ulp): the spectra come from a
+// different transform anyway, and the IEEE divisions made the kernel
+// instruction-bound.
 __device__ float2 adjust(const DivFilterArgs &a, int k, int i, int j, float2 d) {
   const long long tr = i + (long long)a.nxp * j;
   const double deltaF = __ldg(a.df + tr);
@@ -369,9 +378,9 @@ __device__ float2 adjust(const DivFilterArgs &a, int k, int i, int j, float2 d) 
   const float wLoc2 = sq2(wLoc);
   const float2 wGlob = __ldg(a.W + k);
   const float wGlob2 = sq2(wGlob);
-  float sizeLoc = __fdiv_rn(wLoc2, s.wn2);
+  float sizeLoc = __fdividef(wLoc2, s.wn2);
   sizeLoc = __fadd_rn(sizeLoc, sq2(camp_scaled<true>(a.E3, k, sf, a.nzp, L, s.e3_inv)));
-  float sizeGlob = __fdiv_rn(sq2(local_bin(a.W, k, a.nzp, L, L.gain)), s.wn2);
+  float sizeGlob = __fdividef(sq2(local_bin(a.W, k, a.nzp, L, L.gain)), s.wn2);
   sizeGlob = __fadd_rn(sizeGlob, sq2(local_e3(a.E3, k, a.nzp, L, s.e3_inv)));
   const float half = __fmul_rn(__fsub_rn(1.0f, a.wnc), 0.5f);
   float sigma2Loc = __fmul_rn(s.error_var, __fadd_rn(a.wnc, __fmul_rn(half, sizeLoc)));
@@ -383,12 +392,12 @@ __device__ float2 adjust(const DivFilterArgs &a, int k, int i, int j, float2 d) 
   if (wLoc2 < tm) wLoc2Adj = __fmul_rn(0.5f, __fadd_rn(wLoc2, tm));
   if (wLoc2Adj < __fmul_rn(tolFac, wGlob2Adj)) {
     wLoc2Adj = __fmul_rn(0.5f, __fadd_rn(wLoc2, __fmul_rn(tolFac, wGlob2Adj)));
-    sigma2Loc = __fmul_rn(sigma2Loc, __fdiv_rn(wLoc2Adj, wLoc2));
+    sigma2Loc = __fmul_rn(sigma2Loc, __fdividef(wLoc2Adj, wLoc2));
   }
   const float den = __fadd_rn(__fmul_rn(tau2, wLoc2Adj), sigma2Loc);
-  const float glob = __fdiv_rn(wGlob2Adj, __fadd_rn(__fmul_rn(tau2, wGlob2), sigma2Glob));
-  const float fr = __fdiv_rn(__fdiv_rn(wLoc.x, den), glob);
-  const float fi = __fdiv_rn(__fdiv_rn(wLoc.y, den), glob);
+  const float glob = __fdividef(wGlob2Adj, __fadd_rn(__fmul_rn(tau2, wGlob2), sigma2Glob));
+  const float fr = __fdividef(__fdividef(wLoc.x, den), glob);
+  const float fi = __fdividef(__fdividef(wLoc.y, den), glob);
   return make_float2(__fsub_rn(__fmul_rn(d.x, fr), __fmul_rn(d.y, fi)),
                      __fadd_rn(__fmul_rn(d.y, fr), __fmul_rn(d.x, fi)));
 }
@@ -444,7 +453,7 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
   if (tab_smem > 227 * 1024) return CRAVA_GPU_ERR_ARG;
   DeviceGuard guard(c->device);
   const cudaStream_t s = c->stream;
-  // device scratch (one stream-ordered allocation): tables, scalars, the
+  // device scratch (context-owned, grown on demand): tables, scalars, the
   // covAlpha column, relative thickness, shift and gain grids, row
   // padding, the context's wavelets and model constants
   const size_t nxy = (size_t)nx * ny, npad = (size_t)(g.rnxp - g.nxp) * g.nyp * g.nzp;
@@ -478,9 +487,17 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
   };
   carve();  // sizes only (buf is null)
   const size_t bytes = off;
-  if (cudaMallocAsync(reinterpret_cast<void **>(&buf), bytes, s) != cudaSuccess) return CRAVA_GPU_ERR_ALLOC;
+  if (c->div_bytes < bytes) {
+    // the previous calls' work on the stream may still read the old buffer
+    CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+    cudaFree(c->div_buf);
+    c->div_buf = nullptr;
+    c->div_bytes = 0;
+    if (cudaMalloc(reinterpret_cast<void **>(&c->div_buf), bytes) != cudaSuccess) return CRAVA_GPU_ERR_ALLOC;
+    c->div_bytes = bytes;
+  }
+  buf = c->div_buf;
   carve();
-  int rc = CRAVA_GPU_OK;
   auto run = [&]() -> int {
     std::vector<char> hc(nconst);
     std::memcpy(hc.data() + o_wav, c->wavelet.data(), sizeof(float) * nt * nzp);
@@ -525,6 +542,8 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
     const long long rows = (long long)g.nyp * nzp;
     for (int l = 0; l < nt; ++l) {
       pa.grid = data[l];
+      k_div_save_pads<<<(unsigned)((rows + kThreads - 1) / kThreads), kThreads, 0, s>>>(pa);
+      CRAVA_LAUNCH_CHECK();
       k_div_pre<<<(unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock), kThreads, 0, s>>>(pa);
       CRAVA_LAUNCH_CHECK();
       if ((r2 = fft_cols_z(c->plans, reinterpret_cast<float2 *>(data[l]), -1, s))) return r2;
@@ -543,7 +562,5 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
     }
     return CRAVA_GPU_OK;
   };
-  rc = run();
-  cudaFreeAsync(buf, s);
-  return rc;
+  return run();
 }
