@@ -144,6 +144,8 @@ SYMBOLS = {
                                         C.c_void_p, C.POINTER(C.c_longlong)], C.c_int),
     "crava_gpu_divide_data_by_scale_wavelet": ([C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, F64P, C.c_int,
                                                 C.c_int, C.c_float, F32P, F32P], C.c_int),
+    "crava_gpu_interpolate_seismic": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -343,6 +345,14 @@ class Context:
             self.handle, arr, _ptr(cov_alpha), rt.ctypes.data_as(F64P), nx, ny, dz,
             sh.ctypes.data_as(F32P) if sh is not None else None,
             gn.ctypes.data_as(F32P) if gn is not None else None), "divide_data_by_scale_wavelet")
+
+    def interpolate_seismic(self, grid, nx, ny, energy_threshold):
+        """FFTGrid::interpolateSeismic on a device data grid, in place;
+        returns (traces interpolated, of which zero energy)."""
+        ni, n0 = C.c_int(0), C.c_int(0)
+        check(self.lib.crava_gpu_interpolate_seismic(self.handle, _ptr(grid), nx, ny, energy_threshold,
+                                                     C.byref(ni), C.byref(n0)), "interpolate_seismic")
+        return ni.value, n0.value
 
     # ---- time-lapse state (State4D, src/state4d.cpp) -------------------
     @staticmethod

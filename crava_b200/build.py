@@ -34,6 +34,7 @@ SOURCES = {
     "crava_file.cu": [],
     "state4d.cu": ["-fmad=false"],
     "divide.cu": [],
+    "interp.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -420,6 +420,19 @@ int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *ctx, float *const *dat
                                            int nx, int ny, float dz, const float *shift,
                                            const float *gain);
 
+/* FFTGrid::interpolateSeismic (src/fftgrid.cpp:2564-2654) with
+ * interpolateTrace and extrapolateSeismic (:2658-2731), the step that
+ * closes divideDataByScaleWavelet (src/crava.cpp:690): traces of the nx x
+ * ny simbox whose energy over the nz samples is at most energy_threshold
+ * times the mean energy are replaced, in the reference's order, by the
+ * mean of their good neighbours; then every padded trace outside the box
+ * of good traces takes its fill trace times the cube of the taper.  grid:
+ * one device data grid (real padded layout, in place).  n_interpolated,
+ * n_zero (may be NULL): the traces found bad, and of those with zero
+ * energy.  Synchronous (the trace flags are walked on the host). */
+int crava_gpu_interpolate_seismic(crava_gpu_ctx *ctx, float *grid, int nx, int ny,
+                                  float energy_threshold, int *n_interpolated, int *n_zero);
+
 /* Simbox geometry stored in the header of a .crava grid file
  * (FFTGrid::writeCravaFile, src/fftgrid.cpp:2399-2433). */
 typedef struct crava_gpu_grid_header {

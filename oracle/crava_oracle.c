@@ -1471,3 +1471,130 @@ int orc_divide_data(const crava_oracle_params *p, float *const *data, const floa
   free(W); free(Wl); free(E3); free(R); free(D); free(adj);
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Low-energy traces: FFTGrid::interpolateSeismic                       */
+/* ------------------------------------------------------------------ */
+typedef struct { float *g; int nx, ny, nz, nxp, nyp, nzp, rnxp; short *flags; } orc_interp;
+
+static float *orc_at(const orc_interp *s, int i, int j, int k) {
+  return s->g + i + (size_t)s->rnxp * (j + (size_t)s->nyp * k);
+}
+
+/* FFTGrid::interpolateTrace (src/fftgrid.cpp:2658-2695) */
+static int orc_interp_trace(orc_interp *s, int index, int i, int j) {
+  int nx = s->nx, ny = s->ny, nt = 0;
+  int left = i > 0 && (s->flags[index - 1] % 2) == 0;
+  int right = i < nx - 1 && (s->flags[index + 1] % 2) == 0;
+  int up = j > 0 && (s->flags[index - nx] % 2) == 0;
+  int down = j < ny - 1 && (s->flags[index + nx] % 2) == 0;
+  nt = left + right + up + down;
+  if (nt > 1) {
+    float *mean = (float *)malloc(sizeof(float) * s->nzp);
+    for (int k = 0; k < s->nzp; ++k) mean[k] = left ? *orc_at(s, i - 1, j, k) : 0.0f;
+    if (right) for (int k = 0; k < s->nzp; ++k) mean[k] += *orc_at(s, i + 1, j, k);
+    if (up) for (int k = 0; k < s->nzp; ++k) mean[k] += *orc_at(s, i, j - 1, k);
+    if (down) for (int k = 0; k < s->nzp; ++k) mean[k] += *orc_at(s, i, j + 1, k);
+    for (int k = 0; k < s->nzp; ++k) *orc_at(s, i, j, k) = mean[k] / (float)nt;
+    free(mean);
+    s->flags[index]--;
+  }
+  return s->flags[index];
+}
+
+/* FFTGrid::getFillNumber (src/fftgrid.cpp:1319-1357), i < np */
+static int orc_fill_number(int i, int n, int np) {
+  if (i < n) return i;
+  int below = np - i - 1, above = i - n + 1;
+  if (above < below) return n - above > n / 2 ? n - above : n / 2;
+  return below < n / 2 ? below : n / 2;
+}
+
+/* FFTGrid::interpolateSeismic (src/fftgrid.cpp:2564-2654) and
+ * extrapolateSeismic (:2699-2731) on one real padded data grid. */
+int orc_interpolate_seismic(float *grid, int nxp, int nyp, int nzp, int nx, int ny, int nz,
+                            float energy_threshold, int *n_interpolated, int *n_zero) {
+  orc_interp s = {grid, nx, ny, nz, nxp, nyp, nzp, 2 * (nxp / 2 + 1), NULL};
+  short *flags = (short *)malloc(sizeof(short) * nx * ny);
+  float *energyMap = (float *)malloc(sizeof(float) * nx * ny);
+  s.flags = flags;
+  int flag = 0, imin = nx, imax = 0, jmin = ny, jmax = 0, index = 0;
+  float totalEnergy = 0;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      float energy = 0;
+      for (int k = 0; k < nz; k++) {
+        float value = *orc_at(&s, i, j, k);
+        energy += value * value;
+      }
+      energyMap[index] = energy;
+      totalEnergy += energy;
+      index++;
+    }
+  index = 0;
+  float energyLimit = energy_threshold * totalEnergy / (float)(nx * ny);
+  int nInter = 0, nInter0 = 0;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      int curFlag = 0;
+      if (energyMap[index] <= energyLimit) {
+        curFlag = 1;
+        nInter++;
+        if (energyMap[index] == 0.0f) nInter0++;
+      }
+      flags[index] = (short)(flag + curFlag);
+      if (curFlag == 1) flag = 2;
+      else {
+        if (i < imin) imin = i;
+        if (i > imax) imax = i;
+        if (j < jmin) jmin = j;
+        if (j > jmax) jmax = j;
+      }
+      index++;
+    }
+  int curIndex = 0;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      if ((flags[curIndex] % 2) == 1) {
+        if ((orc_interp_trace(&s, curIndex, i, j) % 2) == 0) {
+          index = curIndex - 1;
+          while (index >= 0 && flags[index] > 1) {
+            if ((flags[index] % 2) == 1) orc_interp_trace(&s, index, index % nx, index / nx);
+            index--;
+          }
+          if (index < 0) index = 0;
+          index++;
+          while (flags[index - 1] == 0 && index <= curIndex) {
+            if (flags[index] > 1) flags[index] -= 2;
+            index++;
+          }
+        }
+      }
+      curIndex++;
+    }
+  if (imin <= imax && jmin <= jmax) {
+    for (int j = 0; j < nyp; j++) {
+      int refj = orc_fill_number(j, ny, nyp);
+      if (refj < jmin) refj = jmin; else if (refj > jmax) refj = jmax;
+      for (int i = 0; i < nxp; i++) {
+        if (i < imin || i > imax || j < jmin || j > jmax) {
+          int refi = orc_fill_number(i, nx, nxp);
+          if (refi < imin) refi = imin; else if (refi > imax) refi = imax;
+          for (int k = 0; k < nzp; k++) {
+            float value = *orc_at(&s, refi, refj, k);
+            float distx = dist_to_boundary(i, nx, nxp), disty = dist_to_boundary(j, ny, nyp);
+            float distz = dist_to_boundary(k, nz, nzp);
+            double b = 1.0 - distx * distx - disty * disty - distz * distz;
+            float mult = (float)pow(b > 0.0 ? b : 0.0, 3);
+            *orc_at(&s, i, j, k) = mult * value;
+          }
+        }
+      }
+    }
+  }
+  if (n_interpolated) *n_interpolated = nInter;
+  if (n_zero) *n_zero = nInter0;
+  free(flags);
+  free(energyMap);
+  return 0;
+}

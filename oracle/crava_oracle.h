@@ -116,6 +116,10 @@ void orc_state4d_evolve(long long n, float *const *ms, float *const *md,
 int orc_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
                     const double *rel_thick, int nx, int ny, float dz, const float *shift,
                     const float *gain);
+/* FFTGrid::interpolateSeismic + extrapolateSeismic on one real padded
+ * data grid, in place. */
+int orc_interpolate_seismic(float *grid, int nxp, int nyp, int nzp, int nx, int ny, int nz,
+                            float energy_threshold, int *n_interpolated, int *n_zero);
 int orc_fill_gen_exp_corr(int nxp, int nyp, int nzp, double rx, double ry, double rz,
                           float grad_i, float grad_j, float *out);
 int orc_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int ntheta,

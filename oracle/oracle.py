@@ -113,6 +113,10 @@ def _load(which: str):
     f = getattr(lib, f"{p}_divide_data")
     f.argtypes = [C.POINTER(Params), C.POINTER(F32P), F32P, F64P, C.c_int, C.c_int, C.c_float, F32P, F32P]
     f.restype = C.c_int
+    if which == "orc":
+        f = lib.orc_interpolate_seismic
+        f.argtypes = [F32P] + [C.c_int] * 6 + [C.c_float, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        f.restype = C.c_int
     s4 = [C.POINTER(F32P)] * 7
     f = getattr(lib, f"{p}_state4d_merge")
     f.argtypes = [C.c_longlong] + s4
@@ -350,6 +354,17 @@ def divide_data(case, data, cov_col, rel_thick, nx, ny, dz, shift=None, gain=Non
         _fp(sh) if sh is not None else None, _fp(gn) if gn is not None else None)
     assert rc == 0
     return out
+
+
+def interpolate_seismic(grid, nxp, nyp, nzp, nx, ny, nz, energy_threshold):
+    """FFTGrid::interpolateSeismic + extrapolateSeismic (restatement);
+    returns (new grid, traces interpolated, of which zero energy)."""
+    lib = _load("orc")
+    g = np.ascontiguousarray(grid, dtype=np.float32).copy()
+    ni, n0 = C.c_int(0), C.c_int(0)
+    assert lib.orc_interpolate_seismic(_fp(g), nxp, nyp, nzp, nx, ny, nz, energy_threshold,
+                                       C.byref(ni), C.byref(n0)) == 0
+    return g, ni.value, n0.value
 
 
 STATE_KEYS = ("ms", "md", "ss", "dd", "sd")  # 3, 3, 6, 6, 9 spectra

@@ -67,3 +67,36 @@ def test_divide_rejects_bad_arguments():
         ctx.divide_data_by_scale_wavelet(data, cov, rt, 17, 12, 4.0)  # nx above nxp
     with pytest.raises(api.CravaGpuError):
         ctx.divide_data_by_scale_wavelet(data, cov, rt, 16, 12, 0.0)  # dz not positive
+
+
+def _planted_grid(nxp, nyp, nzp, nx, ny, bad, seed=0):
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((nzp, nyp, 2 * (nxp // 2 + 1))).astype(np.float32)
+    for n, (i, j) in enumerate(bad):
+        g[:, j, i] = 0.0 if n % 2 == 0 else 1e-3  # zero and low-energy traces
+    return g
+
+
+@pytest.mark.parametrize("shape,nxy,bad", [
+    ((16, 12, 24), (12, 10), [(3, 4), (4, 4), (5, 4), (0, 0), (11, 9), (5, 0), (6, 6), (7, 7), (6, 7)]),
+    ((20, 16, 30), (18, 14), [(0, j) for j in range(14)] + [(17, 3), (9, 9), (9, 10), (10, 9), (10, 10)]),
+    ((15, 1, 20), (13, 1), [(2, 0), (3, 0), (12, 0)]),
+])
+def test_interpolate_seismic_vs_restatement(shape, nxy, bad):
+    """interpolateSeismic: energies, the flag walk and the interpolations bit
+    for bit; the extrapolated padding to 1 float ulp (pow of CUDA and of
+    the C library)."""
+    nxp, nyp, nzp = shape
+    nx, ny = nxy
+    case = synth.make_case(nxp, nyp, nzp, (10.0,), 0.1, seed=3)
+    case.nz = nzp - 4
+    ctx = api.Context(case)
+    g = _planted_grid(nxp, nyp, nzp, nx, ny, bad)
+    ref, ni, n0 = O.interpolate_seismic(g, nxp, nyp, nzp, nx, ny, case.nz, 0.05)
+    t = api.to_device(g)
+    gi, g0 = ctx.interpolate_seismic(t, nx, ny, 0.05)
+    assert (gi, g0) == (ni, n0) and ni == len(bad)
+    out = t.cpu().numpy()
+    ob, rb = out.view(np.int32).astype(np.int64), ref.view(np.int32).astype(np.int64)
+    assert np.array_equal(out[:, :ny, :nx], ref[:, :ny, :nx])  # simbox traces
+    assert np.abs(ob - rb).max() <= 1
