@@ -144,6 +144,8 @@ SYMBOLS = {
                                         C.c_void_p, C.POINTER(C.c_longlong)], C.c_int),
     "crava_gpu_divide_data_by_scale_wavelet": ([C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, F64P, C.c_int,
                                                 C.c_int, C.c_float, F32P, F32P], C.c_int),
+    "crava_gpu_multiply_data_by_scale_wavelet": ([C.c_void_p, C.POINTER(C.c_void_p), F64P, C.c_int, C.c_int,
+                                                  C.c_float, F32P, F32P], C.c_int),
     "crava_gpu_interpolate_seismic": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
@@ -345,6 +347,20 @@ class Context:
             self.handle, arr, _ptr(cov_alpha), rt.ctypes.data_as(F64P), nx, ny, dz,
             sh.ctypes.data_as(F32P) if sh is not None else None,
             gn.ctypes.data_as(F32P) if gn is not None else None), "divide_data_by_scale_wavelet")
+
+    def multiply_data_by_scale_wavelet(self, resid, rel_thick, nx, ny, dz, shift=None, gain=None):
+        """Crava::multiplyDataByScaleWaveletAndWriteToFile without the file
+        write: transformed residual grids back to the time domain, each
+        simbox trace times its local wavelet's conjugate spectrum."""
+        rt = np.ascontiguousarray(rel_thick, dtype=np.float64)
+        assert rt.size == self.case.nxp * self.case.nyp
+        arr = (C.c_void_p * len(resid))(*[g.data_ptr() for g in resid])
+        sh = np.ascontiguousarray(shift, dtype=np.float32) if shift is not None else None
+        gn = np.ascontiguousarray(gain, dtype=np.float32) if gain is not None else None
+        check(self.lib.crava_gpu_multiply_data_by_scale_wavelet(
+            self.handle, arr, rt.ctypes.data_as(F64P), nx, ny, dz,
+            sh.ctypes.data_as(F32P) if sh is not None else None,
+            gn.ctypes.data_as(F32P) if gn is not None else None), "multiply_data_by_scale_wavelet")
 
     def interpolate_seismic(self, grid, nx, ny, energy_threshold):
         """FFTGrid::interpolateSeismic on a device data grid, in place;

@@ -96,10 +96,11 @@ __global__ void __launch_bounds__(kTabThreads) k_div_spectra(const __grid_consta
   for (int p = 0; p < 3; ++p)
     for (int k = 0; k < 3; ++k)
       eiVar += (double)__fmul_rn(__fmul_rn(q.A[3 * l + p], (float)q.var0[3 * p + k]), q.A[3 * l + k]);
-  const float constant = q.cov_alpha[0];
+  // (no covariance grid: the wavelet spectrum alone is wanted)
+  const float constant = q.cov_alpha ? q.cov_alpha[0] : 1.0f;
   for (int i = tid; i < nzp; i += nth) {
     const int refk = i < nzp / 2 + 1 ? i : nzp - i;
-    const float corr = refk < q.nz ? __fdiv_rn(q.cov_alpha[refk * q.col_stride], constant) : 0.0f;
+    const float corr = (q.cov_alpha && refk < q.nz) ? __fdiv_rn(q.cov_alpha[refk * q.col_stride], constant) : 0.0f;
     e[i] = (float)(eiVar * (double)corr);
   }
   __syncthreads();
@@ -563,4 +564,210 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
     return CRAVA_GPU_OK;
   };
   return run();
+}
+
+// ------------------------------------------------------ multiply back
+// Crava::multiplyDataByScaleWaveletAndWriteToFile (src/crava.cpp:819-885)
+// before its file write: the residual stacks back in the time domain, each
+// simbox trace (i < nx, j < ny) times the conjugate spectrum of its
+// stretched local wavelet.  The trace pairs are transformed in a scratch
+// grid so that the traces the reference leaves alone stay bit for bit.
+namespace {
+
+struct MulPassArgs {
+  const float *src;
+  float *dst;
+  int nx, ny, nxp, nyp, nzp, rnxp;
+  float sq;  // the divisor of the pass
+};
+
+// grid -> scratch, every value / float(sqrt(float(nzp))) (:846-849)
+__global__ void __launch_bounds__(kThreads) k_mul_pre(const __grid_constant__ MulPassArgs a) {
+  const int row = blockIdx.x * kRowsPerBlock + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (row >= a.nyp * a.nzp) return;
+  const int cnxp = a.rnxp / 2;
+  const float2 *__restrict__ r = reinterpret_cast<const float2 *>(a.src + (long long)row * a.rnxp);
+  float2 *__restrict__ w = reinterpret_cast<float2 *>(a.dst + (long long)row * a.rnxp);
+  for (int x = lane; x < cnxp; x += 32) {
+    const float2 v = r[x];
+    w[x] = make_float2(__fdiv_rn(v.x, a.sq), __fdiv_rn(v.y, a.sq));
+  }
+}
+
+// scratch -> grid for the simbox traces, / float(sqrt(double(nzp))) (:867-870)
+__global__ void __launch_bounds__(kThreads) k_mul_post(const __grid_constant__ MulPassArgs a) {
+  const int row = blockIdx.x * kRowsPerBlock + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (row >= a.nyp * a.nzp) return;
+  const int j = row % a.nyp;
+  if (j >= a.ny) return;
+  const float *__restrict__ r = a.src + (long long)row * a.rnxp;
+  float *__restrict__ w = a.dst + (long long)row * a.rnxp;
+  for (int i = lane; i < a.nx; i += 32) w[i] = __fdiv_rn(r[i], a.sq);
+}
+
+struct MulFilterArgs {
+  float2 *grid;               // scratch, complex view after the forward z pass
+  const float2 *W;            // this angle's wavelet spectrum
+  const float *sf;            // [nyp][nxp] float(relThick) x localStretch
+  const float *shift, *gain;  // [ny][nx] of this angle, or null
+  int nx, ny, nxp, nyp, nzp, cnxp;
+  float dz;
+};
+
+// The data bin times the conjugate of getCAmp(k, sf) of the trace's local
+// wavelet (src/crava.cpp:852-865).
+__device__ __forceinline__ float2 mul_local(const MulFilterArgs &a, int k, int i, int j, float2 d) {
+  Local L{0.0f, 1.0f, false};
+  if (a.shift || a.gain) {
+    constexpr float kWellMissing = -999.0f;  // WELLMISSING, src/definitions.h:39
+    const long long o = i + (long long)a.nx * j;
+    float ts = 0.0f, g = 1.0f;
+    if (a.shift && a.shift[o] != kWellMissing) ts = a.shift[o];
+    if (a.gain && a.gain[o] != kWellMissing) g = a.gain[o];
+    L.ishift = __fdiv_rn(ts, a.dz);
+    L.gain = g;
+    L.on = true;
+  }
+  const float sf = __ldg(a.sf + i + (long long)a.nxp * j);
+  const float2 w = camp_scaled<false>(a.W, k, sf, a.nzp, L, 1.0f);
+  return make_float2(__fadd_rn(__fmul_rn(d.x, w.x), __fmul_rn(d.y, w.y)),
+                     __fsub_rn(__fmul_rn(d.y, w.x), __fmul_rn(d.x, w.y)));
+}
+
+// One thread per (trace pair, line, bin k <= nzp/2), as k_div_filter;
+// traces outside the simbox pass unchanged (they are not written back).
+__global__ void __launch_bounds__(kThreads) k_mul_filter(const __grid_constant__ MulFilterArgs a) {
+  const long long plane = (long long)a.cnxp * a.nyp;
+  const long long n = plane * (a.nzp / 2 + 1);
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int k = (int)(idx / plane);
+  const long long r = idx - (long long)k * plane;
+  const int p = (int)(r % a.cnxp), j = (int)(r / a.cnxp);
+  if (j >= a.ny || 2 * p >= a.nx) return;
+  const int km = k == 0 ? 0 : a.nzp - k;
+  const bool self = km == k;
+  float2 *zk = a.grid + r + (long long)k * plane;
+  float2 *zm = a.grid + r + (long long)km * plane;
+  const float2 Zk = *zk, Zm = *zm;
+  float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+  float2 B = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+  A = mul_local(a, k, 2 * p, j, A);
+  if (self) A.y = 0.0f;  // the real inverse transform reads the real part here
+  if (2 * p + 1 < a.nx) {
+    B = mul_local(a, k, 2 * p + 1, j, B);
+    if (self) B.y = 0.0f;
+  }
+  *zk = make_float2(A.x - B.y, A.y + B.x);
+  if (!self) *zm = make_float2(A.x + B.y, B.x - A.y);
+}
+
+__global__ void __launch_bounds__(kThreads) k_mul_traces(const double *__restrict__ rel_thick, int n, float *sf) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) sf[t] = __fmul_rn((float)rel_thick[t], 1.0f);  // getLocalStretch = 1 for 1-D wavelets
+}
+
+}  // namespace
+
+extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float *const *resid,
+                                                       const double *rel_thick, int nx, int ny, float dz,
+                                                       const float *shift, const float *gain) {
+  if (!c || !resid || !rel_thick || !(dz > 0.0f)) return CRAVA_GPU_ERR_ARG;
+  const Geom &g = c->g;
+  const int nt = c->p.ntheta, nzp = g.nzp, cnzp = nzp / 2 + 1;
+  if (nx < 1 || ny < 1 || nx > g.nxp || ny > g.nyp) return CRAVA_GPU_ERR_ARG;
+  for (int l = 0; l < nt; ++l) if (mis8(resid[l])) return CRAVA_GPU_ERR_ARG;
+  const size_t tab_smem = sizeof(double) * 2 * (size_t)nzp + sizeof(float) * 5 * (size_t)nzp;
+  if (tab_smem > 227 * 1024) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  const cudaStream_t s = c->stream;
+  const size_t nxy = (size_t)nx * ny;
+  char *buf = nullptr;
+  size_t off = 0;
+  auto take = [&](size_t n) { char *q = buf + off; off += (n + 15) & ~size_t(15); return q; };
+  DivTables t;
+  float *dshift, *dgain, *tsf, *scratch;
+  double *rt;
+  char *dconst;
+  const size_t o_wav = 0, o_norm = o_wav + ((sizeof(float) * nt * nzp + 15) & ~size_t(15));
+  const size_t o_A = o_norm + ((sizeof(float) * nt + 15) & ~size_t(15));
+  const size_t o_var = o_A + ((sizeof(float) * 3 * nt + 15) & ~size_t(15));
+  const size_t o_th = o_var + ((sizeof(double) * 9 + 15) & ~size_t(15));
+  const size_t nconst = o_th + sizeof(double) * nt * nt;
+  auto carve = [&]() {
+    off = 0;
+    t.W = reinterpret_cast<float2 *>(take(sizeof(float2) * nt * cnzp));
+    t.E3 = reinterpret_cast<float2 *>(take(sizeof(float2) * nt * cnzp));
+    t.tau2 = reinterpret_cast<float *>(take(sizeof(float) * nt * cnzp));
+    t.sc = reinterpret_cast<DivScalars *>(take(sizeof(DivScalars) * nt));
+    rt = reinterpret_cast<double *>(take(sizeof(double) * g.nxp * g.nyp));
+    tsf = reinterpret_cast<float *>(take(sizeof(float) * g.nxp * g.nyp));
+    dshift = shift ? reinterpret_cast<float *>(take(sizeof(float) * nt * nxy)) : nullptr;
+    dgain = gain ? reinterpret_cast<float *>(take(sizeof(float) * nt * nxy)) : nullptr;
+    dconst = take(nconst);
+    scratch = reinterpret_cast<float *>(take(sizeof(float) * g.rsize));
+  };
+  carve();  // sizes only (buf is null)
+  const size_t bytes = off;
+  if (c->div_bytes < bytes) {
+    CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+    cudaFree(c->div_buf);
+    c->div_buf = nullptr;
+    c->div_bytes = 0;
+    if (cudaMalloc(reinterpret_cast<void **>(&c->div_buf), bytes) != cudaSuccess) return CRAVA_GPU_ERR_ALLOC;
+    c->div_bytes = bytes;
+  }
+  buf = c->div_buf;
+  carve();
+  std::vector<char> hc(nconst);
+  std::memcpy(hc.data() + o_wav, c->wavelet.data(), sizeof(float) * nt * nzp);
+  if (!c->wnorm.empty()) std::memcpy(hc.data() + o_norm, c->wnorm.data(), sizeof(float) * nt);
+  std::memcpy(hc.data() + o_A, c->A.data(), sizeof(float) * 3 * nt);
+  std::memcpy(hc.data() + o_var, c->var0.data(), sizeof(double) * 9);
+  std::memcpy(hc.data() + o_th, c->theta.data(), sizeof(double) * nt * nt);
+  CRAVA_CUDA_TRY(cudaMemcpyAsync(dconst, hc.data(), nconst, cudaMemcpyHostToDevice, s));
+  CRAVA_CUDA_TRY(cudaMemcpyAsync(rt, rel_thick, sizeof(double) * g.nxp * g.nyp, cudaMemcpyHostToDevice, s));
+  if (shift) CRAVA_CUDA_TRY(cudaMemcpyAsync(dshift, shift, sizeof(float) * nt * nxy, cudaMemcpyHostToDevice, s));
+  if (gain) CRAVA_CUDA_TRY(cudaMemcpyAsync(dgain, gain, sizeof(float) * nt * nxy, cudaMemcpyHostToDevice, s));
+  DivConsts q{};
+  q.wav = reinterpret_cast<const float *>(dconst + o_wav);
+  q.wnorm = nullptr;
+  q.A = reinterpret_cast<const float *>(dconst + o_A);
+  q.var0 = reinterpret_cast<const double *>(dconst + o_var);
+  q.theta = reinterpret_cast<const double *>(dconst + o_th);
+  q.cov_alpha = nullptr;  // the wavelet spectrum only
+  q.col_stride = 0;
+  q.nzp = nzp; q.nt = nt; q.nz = c->p.nz; q.lz = c->p.lz; q.dz = dz;
+  q.low_cut = c->p.low_cut; q.high_cut = c->p.high_cut;
+  int rc;
+  if ((rc = func_smem((const void *)k_div_spectra, tab_smem))) return rc;
+  k_div_spectra<<<dim3(nt, (cnzp + kTabThreads - 1) / kTabThreads), kTabThreads, tab_smem, s>>>(q, t);
+  CRAVA_LAUNCH_CHECK();
+  const int ntr = g.nxp * g.nyp;
+  k_mul_traces<<<(ntr + kThreads - 1) / kThreads, kThreads, 0, s>>>(rt, ntr, tsf);
+  CRAVA_LAUNCH_CHECK();
+  const long long rows = (long long)g.nyp * nzp;
+  const long long nfilt = (long long)g.cnxp * g.nyp * (nzp / 2 + 1);
+  MulFilterArgs fa{};
+  fa.sf = tsf;
+  fa.nx = nx; fa.ny = ny; fa.nxp = g.nxp; fa.nyp = g.nyp; fa.nzp = nzp; fa.cnxp = g.cnxp; fa.dz = dz;
+  fa.grid = reinterpret_cast<float2 *>(scratch);
+  for (int l = 0; l < nt; ++l) {
+    // seisData_[l]->invFFTInPlace() (:844)
+    if ((rc = pass_inverse(c, resid[l], CRAVA_GRID_DATA))) return rc;
+    MulPassArgs pa{resid[l], scratch, nx, ny, g.nxp, g.nyp, nzp, g.rnxp, sqrtf((float)nzp)};
+    k_mul_pre<<<(unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock), kThreads, 0, s>>>(pa);
+    CRAVA_LAUNCH_CHECK();
+    if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(scratch), -1, s))) return rc;
+    fa.W = t.W + (size_t)l * cnzp;
+    fa.shift = dshift ? dshift + (size_t)l * nxy : nullptr;
+    fa.gain = dgain ? dgain + (size_t)l * nxy : nullptr;
+    k_mul_filter<<<(unsigned)((nfilt + kThreads - 1) / kThreads), kThreads, 0, s>>>(fa);
+    CRAVA_LAUNCH_CHECK();
+    if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(scratch), 1, s))) return rc;
+    MulPassArgs pb{scratch, resid[l], nx, ny, g.nxp, g.nyp, nzp, g.rnxp, (float)sqrt((double)nzp)};
+    k_mul_post<<<(unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock), kThreads, 0, s>>>(pb);
+    CRAVA_LAUNCH_CHECK();
+  }
+  return CRAVA_GPU_OK;
 }

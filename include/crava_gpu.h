@@ -420,6 +420,19 @@ int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *ctx, float *const *dat
                                            int nx, int ny, float dz, const float *shift,
                                            const float *gain);
 
+/* Crava::multiplyDataByScaleWaveletAndWriteToFile (src/crava.cpp:819-885)
+ * up to its file write: each residual stack (transformed, as the solve
+ * leaves it) is transformed back to the time domain (DATA scaling) and
+ * every simbox trace (i < nx, j < ny) multiplied along z by the conjugate
+ * spectrum of its local wavelet stretched by rel_thick[j][i], shifted and
+ * scaled by the local shift and gain (Wavelet::getCAmp(k, scale)); the
+ * other traces keep their values.  rel_thick, dz, shift, gain as for
+ * crava_gpu_divide_data_by_scale_wavelet (shift / gain indexed by the
+ * trace itself).  Asynchronous. */
+int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *ctx, float *const *resid,
+                                             const double *rel_thick, int nx, int ny, float dz,
+                                             const float *shift, const float *gain);
+
 /* FFTGrid::interpolateSeismic (src/fftgrid.cpp:2564-2654) with
  * interpolateTrace and extrapolateSeismic (:2658-2731), the step that
  * closes divideDataByScaleWavelet (src/crava.cpp:690): traces of the nx x

@@ -1598,3 +1598,50 @@ int orc_interpolate_seismic(float *grid, int nxp, int nyp, int nzp, int nx, int 
   free(energyMap);
   return 0;
 }
+
+/* Crava::multiplyDataByScaleWaveletAndWriteToFile (src/crava.cpp:819-885)
+ * before the file write, on time-domain residual grids (the caller has
+ * made the invFFTInPlace): each simbox trace times the conjugate of
+ * getCAmp(k, sf) of its local wavelet. */
+int orc_multiply_data(const crava_oracle_params *p, float *const *data, const double *rel_thick,
+                      int nx, int ny, float dz, const float *shift, const float *gain) {
+  const int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta;
+  const int cnzp = nzp / 2 + 1, rnxp = 2 * (nxp / 2 + 1);
+  float *w = (float *)malloc(sizeof(float) * nzp), *tr = (float *)malloc(sizeof(float) * nzp);
+  cf *W = (cf *)malloc(sizeof(cf) * cnzp), *Wl = (cf *)malloc(sizeof(cf) * cnzp);
+  cf *D = (cf *)malloc(sizeof(cf) * cnzp);
+  for (int l = 0; l < nt; ++l) {
+    memcpy(w, p->wavelet + (size_t)l * nzp, sizeof(float) * nzp);
+    real_spectrum(w, nzp, W);
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        float sf = (float)rel_thick[i + (size_t)nxp * j] * 1.0f;
+        float *g0 = data[l] + i + (size_t)rnxp * j;
+        for (int k = 0; k < nzp; ++k) tr[k] = g0[(size_t)rnxp * nyp * k] / (float)sqrtf((float)nzp);
+        real_spectrum(tr, nzp, D);
+        float ts = 0.0f, g = 1.0f;
+        size_t o = (size_t)l * nx * ny + i + (size_t)nx * j;
+        if (shift && shift[o] != -999.0f) ts = shift[o];
+        if (gain && gain[o] != -999.0f) g = gain[o];
+        float iShift = ts / dz;
+        for (int k = 0; k < cnzp; ++k) {
+          cf am, t;
+          am.re = (float)(g * cos(2.0 * (3.14159265358979323846 * (iShift) * k) / (float)nzp));
+          am.im = (float)(g * sin(-2.0 * (3.14159265358979323846 * (iShift) * k) / (float)nzp));
+          t.re = am.re * W[k].re - am.im * W[k].im;
+          t.im = am.im * W[k].re + am.re * W[k].im;
+          Wl[k] = t;
+        }
+        for (int k = 0; k < cnzp; ++k) {
+          cf sv = get_camp_scaled(Wl, nzp, k, sf);
+          float tmp = D[k].re * sv.re + D[k].im * sv.im;
+          D[k].im = D[k].im * sv.re - D[k].re * sv.im;
+          D[k].re = tmp;
+        }
+        real_inverse(D, nzp, tr, 1.0);
+        for (int k = 0; k < nzp; ++k) g0[(size_t)rnxp * nyp * k] = tr[k] / (float)sqrt((double)nzp);
+      }
+  }
+  free(w); free(tr); free(W); free(Wl); free(D);
+  return 0;
+}

@@ -116,6 +116,10 @@ void orc_state4d_evolve(long long n, float *const *ms, float *const *md,
 int orc_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
                     const double *rel_thick, int nx, int ny, float dz, const float *shift,
                     const float *gain);
+/* multiplyDataByScaleWaveletAndWriteToFile before the file write, on
+ * time-domain residual grids (in place). */
+int orc_multiply_data(const crava_oracle_params *p, float *const *data, const double *rel_thick,
+                      int nx, int ny, float dz, const float *shift, const float *gain);
 /* FFTGrid::interpolateSeismic + extrapolateSeismic on one real padded
  * data grid, in place. */
 int orc_interpolate_seismic(float *grid, int nxp, int nyp, int nzp, int nx, int ny, int nz,
@@ -155,6 +159,8 @@ int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int nthe
 int ref_divide_data(const crava_oracle_params *p, float *const *data, const float *cov_col,
                     const double *rel_thick, int nx, int ny, float dz, const float *shift,
                     const float *gain);
+int ref_multiply_data(const crava_oracle_params *p, float *const *data, const double *rel_thick,
+                      int nx, int ny, float dz, const float *shift, const float *gain);
 void ref_state4d_merge(long long n, const float *const *ms, const float *const *md,
                        const float *const *ss, const float *const *dd,
                        const float *const *sd, float *const *mu, float *const *cov);

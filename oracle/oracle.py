@@ -113,6 +113,9 @@ def _load(which: str):
     f = getattr(lib, f"{p}_divide_data")
     f.argtypes = [C.POINTER(Params), C.POINTER(F32P), F32P, F64P, C.c_int, C.c_int, C.c_float, F32P, F32P]
     f.restype = C.c_int
+    f = getattr(lib, f"{p}_multiply_data")
+    f.argtypes = [C.POINTER(Params), C.POINTER(F32P), F64P, C.c_int, C.c_int, C.c_float, F32P, F32P]
+    f.restype = C.c_int
     if which == "orc":
         f = lib.orc_interpolate_seismic
         f.argtypes = [F32P] + [C.c_int] * 6 + [C.c_float, C.POINTER(C.c_int), C.POINTER(C.c_int)]
@@ -353,6 +356,21 @@ def divide_data(case, data, cov_col, rel_thick, nx, ny, dz, shift=None, gain=Non
         C.byref(p), _ptrs(out), _fp(col), _dp(rt), nx, ny, dz,
         _fp(sh) if sh is not None else None, _fp(gn) if gn is not None else None)
     assert rc == 0
+    return out
+
+
+def multiply_data(case, data, rel_thick, nx, ny, dz, shift=None, gain=None, which="orc"):
+    """multiplyDataByScaleWaveletAndWriteToFile before the write, on
+    time-domain residual grids (restatement); returns new grids."""
+    keep = []
+    p, keep = make_params(case, keep)
+    out = [np.ascontiguousarray(g, dtype=np.float32).copy() for g in data]
+    rt = np.ascontiguousarray(rel_thick, dtype=np.float64)
+    sh = np.ascontiguousarray(shift, dtype=np.float32) if shift is not None else None
+    gn = np.ascontiguousarray(gain, dtype=np.float32) if gain is not None else None
+    assert getattr(_load(which), f"{which}_multiply_data")(
+        C.byref(p), _ptrs(out), _dp(rt), nx, ny, dz, _fp(sh) if sh is not None else None,
+        _fp(gn) if gn is not None else None) == 0
     return out
 
 

@@ -944,4 +944,68 @@ int ref_divide_data(const crava_oracle_params *p, float *const *data, const floa
   return 0;
 }
 
+/* Crava::multiplyDataByScaleWaveletAndWriteToFile (src/crava.cpp:819-885)
+ * before the file write, on time-domain residual grids, with the
+ * reference's FFTW per trace and the local wavelet made as
+ * createLocalWavelet1D makes it (copy, forward transform, shiftAndScale). */
+int ref_multiply_data(const crava_oracle_params *p, float *const *data, const double *rel_thick,
+                      int nx, int ny, float dz, const float *shift, const float *gain) {
+  const int nxp = p->nxp, nyp = p->nyp, nzp = p->nzp, nt = p->ntheta;
+  const int cnzp = nzp / 2 + 1, rnzp = 2 * cnzp, rnxp = 2 * (nxp / 2 + 1);
+  rfftwnd_plan fwd = rfftwnd_create_plan(1, &nzp, FFTW_REAL_TO_COMPLEX, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_plan inv = rfftwnd_create_plan(1, &nzp, FFTW_COMPLEX_TO_REAL, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  fftw_real *rd = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_real *lw = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_complex *cd = reinterpret_cast<fftw_complex *>(rd), *cw = reinterpret_cast<fftw_complex *>(lw);
+  for (int l = 0; l < nt; l++) {
+    const long plane = static_cast<long>(rnxp) * nyp;
+    for (int i = 0; i < nx; i++)
+      for (int j = 0; j < ny; j++) {
+        float sf = static_cast<float>(rel_thick[i + static_cast<long>(nxp) * j]) * 1.0f;
+        const long t0 = i + static_cast<long>(rnxp) * j;
+        for (int k = 0; k < nzp; k++)
+          rd[k] = data[l][t0 + k * plane] / static_cast<float>(std::sqrt(static_cast<float>(nzp)));
+        rfftwnd_one_real_to_complex(fwd, rd, cd);
+        for (int q = 0; q < rnzp; ++q) lw[q] = q < nzp ? p->wavelet[static_cast<long>(l) * nzp + q] : 0.0f;
+        rfftwnd_one_real_to_complex(fwd, lw, cw);
+        float ts = 0.0f, g = 1.0f;
+        const long o = static_cast<long>(l) * nx * ny + i + static_cast<long>(nx) * j;
+        if (shift && shift[o] != -999.0f) ts = shift[o];
+        if (gain && gain[o] != -999.0f) g = gain[o];
+        float iShift = ts / dz;
+        for (int k = 0; k < cnzp; k++) {
+          fftw_complex am, tmp;
+          am.re = float(g * cos(2.0 * (3.14159265358979323846 * (iShift) * k) / float(nzp)));
+          am.im = float(g * sin(-2.0 * (3.14159265358979323846 * (iShift) * k) / float(nzp)));
+          tmp.re = am.re * cw[k].re - am.im * cw[k].im;
+          tmp.im = am.im * cw[k].re + am.re * cw[k].im;
+          cw[k] = tmp;
+        }
+        for (int k = 0; k < cnzp; k++) {
+          fftw_complex sv;  /* getCAmp(k, sf), k < cnzp */
+          float omega = float(k) / sf;
+          if (omega >= cnzp) { sv.re = 0.0f; sv.im = 0.0f; }
+          else {
+            int omL = int(std::floor(omega)), omU = int(std::floor(omega)) + 1;
+            if (omU >= cnzp) omU -= 1;
+            float dOmega = omega - float(omL);
+            sv.re = cw[omL].re * (1.0f - dOmega) + cw[omU].re * dOmega;
+            sv.im = (cw[omL].im * (1.0f - dOmega) + cw[omU].im * dOmega);
+          }
+          sv.re /= sf; sv.im /= sf;
+          fftw_real tmp = cd[k].re * sv.re + cd[k].im * sv.im;
+          cd[k].im = cd[k].im * sv.re - cd[k].re * sv.im;
+          cd[k].re = tmp;
+        }
+        rfftwnd_one_complex_to_real(inv, cd, rd);
+        for (int k = 0; k < nzp; k++)
+          data[l][t0 + k * plane] = rd[k] / static_cast<float>(std::sqrt(static_cast<double>(nzp)));
+      }
+  }
+  fftw_free(rd); fftw_free(lw);
+  fftwnd_destroy_plan(fwd);
+  fftwnd_destroy_plan(inv);
+  return 0;
+}
+
 }  /* extern "C" */

@@ -100,3 +100,33 @@ def test_interpolate_seismic_vs_restatement(shape, nxy, bad):
     ob, rb = out.view(np.int32).astype(np.int64), ref.view(np.int32).astype(np.int64)
     assert np.array_equal(out[:, :ny, :nx], ref[:, :ny, :nx])  # simbox traces
     assert np.abs(ob - rb).max() <= 1
+
+
+@pytest.mark.parametrize("shape,nxy,local", [((16, 12, 32), (12, 10), True), ((15, 10, 21), (13, 9), False),
+                                             ((16, 1, 32), (14, 1), False)])
+def test_multiply_back_vs_restatement(shape, nxy, local):
+    """multiplyDataByScaleWaveletAndWriteToFile (before the write): the
+    inverse transform of the residual spectra, then each simbox trace times
+    its local wavelet's conjugate spectrum; other traces unchanged."""
+    nxp, nyp, nzp = shape
+    nx, ny = nxy
+    case = synth.make_case(nxp, nyp, nzp, (0.0, 15.0, 30.0), 0.1, seed=44)
+    rng = np.random.default_rng(8)
+    rt = rng.uniform(0.75, 1.25, (nyp, nxp))
+    shift = rng.uniform(-5, 5, (3, ny, nx)).astype(np.float32) if local else None
+    gain = rng.uniform(0.7, 1.3, (3, ny, nx)).astype(np.float32) if local else None
+    dz = float(np.float32(case.lz / case.nz))
+    ctx = api.Context(case)
+    spec = [api.to_device(g) for g in case.data]
+    for g in spec:
+        ctx.fft_r2c(g, api.DATA)
+    timed = [g.clone() for g in spec]
+    for g in timed:
+        ctx.fft_c2r(g, api.DATA)
+    ctx.multiply_data_by_scale_wavelet(spec, rt, nx, ny, dz, shift, gain)
+    ref = O.multiply_data(case, [g.cpu().numpy() for g in timed], rt, nx, ny, dz, shift, gain)
+    for g, r, t0 in zip(spec, ref, timed):
+        out = g.cpu().numpy()
+        assert rel(out[:, :ny, :nx], r[:, :ny, :nx]) < 1e-5
+        assert np.array_equal(out[:, :, nx:nxp], t0.cpu().numpy()[:, :, nx:nxp])  # traces left alone
+        assert np.array_equal(out[:, ny:, :nxp], t0.cpu().numpy()[:, ny:, :nxp])

@@ -325,3 +325,23 @@ def test_divide_data_vs_golden(name):
     for a, b, d in zip(out, z[f"{name}_out"], case.data):
         assert rel(a[..., :case.nxp], b[..., :case.nxp]) < 1e-5
         assert rel(b[..., :case.nxp], d[..., :case.nxp]) > 0.1  # the division did something
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref not built (needs the reference tree)")
+@pytest.mark.parametrize("name,local", [("c3_12x10x16", False), ("c2_9x8x20_odd", True)])
+def test_multiply_data_vs_ref_live(name, local):
+    """multiplyDataByScaleWaveletAndWriteToFile restated vs the reference's
+    FFTW per-trace sequence: < 1e-5."""
+    case, _ = GC.load(name)
+    nx, ny = case.nxp - 2, case.nyp - 2
+    rng = np.random.default_rng(12)
+    rt = rng.uniform(0.7, 1.3, (case.nyp, case.nxp))
+    shift = rng.uniform(-5, 5, (case.ntheta, ny, nx)).astype(np.float32) if local else None
+    gain = rng.uniform(0.7, 1.3, (case.ntheta, ny, nx)).astype(np.float32) if local else None
+    dz = float(np.float32(case.lz / case.nz))
+    a = O.multiply_data(case, case.data, rt, nx, ny, dz, shift, gain, "orc")
+    b = O.multiply_data(case, case.data, rt, nx, ny, dz, shift, gain, "ref")
+    for x, y, d in zip(a, b, case.data):
+        assert rel(x[:, :ny, :nx], y[:, :ny, :nx]) < 1e-5
+        assert np.array_equal(x[:, ny:, :], d[:, ny:, :])
+        assert rel(x[:, :ny, :nx], d[:, :ny, :nx]) > 0.1
