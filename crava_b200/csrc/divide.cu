@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "context.cuh"
+#include "fft_core.cuh"
 
 using namespace crava;
 
@@ -435,6 +436,146 @@ __global__ void __launch_bounds__(kThreads) k_div_filter(const __grid_constant__
   if (!self) *zm = make_float2(A.x + B.y, B.x - A.y);  // conj A + i conj B
 }
 
+// ------------------------------------------------------------- fused
+// The whole per-stack step in one pass over HBM for the transform lengths
+// compiled here: a CTA loads TX trace-pair columns of one y line (the
+// pre-scale and taper applied on the way into shared memory), transforms
+// them along z in place (the compile-time Stockham engine of the 3-D
+// transforms), filters each pair's two spectra at k and nzp - k,
+// transforms back and stores the traces it may write (the post-scale
+// applied on the way out; other traces are not written at all).
+// MODE 0: divideDataByScaleWavelet (every padded trace i < nxp);
+// MODE 1: multiplyDataByScaleWaveletAndWriteToFile (simbox traces only).
+struct FusedArgs {
+  DivFilterArgs f;        // the division's filter inputs (MODE 0)
+  const float2 *Wm;       // the multiply's wavelet spectrum (MODE 1)
+  const float *sfm;       // the multiply's per-trace stretch (MODE 1)
+  float *grid;            // real padded layout
+  const float2 *tw;       // forward twiddles of length nzp
+  float sq_in, sq_out;    // the divisors before and after
+  int nx, ny, nxp, nyp, nzp, cnxp, rnxp, nz;
+};
+
+// The data bin times the conjugate of getCAmp(k, sf) of the trace's local
+// wavelet (src/crava.cpp:852-865); the local shift and gain are read at
+// the trace itself.
+__device__ __forceinline__ float2 mul_conj(const FusedArgs &a, int k, int i, int j, float2 d) {
+  Local L{0.0f, 1.0f, false};
+  if (a.f.shift || a.f.gain) {
+    constexpr float kWellMissing = -999.0f;  // WELLMISSING, src/definitions.h:39
+    const long long o = i + (long long)a.nx * j;
+    float ts = 0.0f, g = 1.0f;
+    if (a.f.shift && a.f.shift[o] != kWellMissing) ts = a.f.shift[o];
+    if (a.f.gain && a.f.gain[o] != kWellMissing) g = a.f.gain[o];
+    L.ishift = __fdiv_rn(ts, a.f.dz);
+    L.gain = g;
+    L.on = true;
+  }
+  const float sf = __ldg(a.sfm + i + (long long)a.nxp * j);
+  const float2 w = camp_scaled<false>(a.Wm, k, sf, a.nzp, L, 1.0f);
+  return make_float2(__fadd_rn(__fmul_rn(d.x, w.x), __fmul_rn(d.y, w.y)),
+                     __fsub_rn(__fmul_rn(d.y, w.x), __fmul_rn(d.x, w.y)));
+}
+
+template <int MODE>
+__device__ __forceinline__ bool fused_trace(const FusedArgs &a, int i, int j) {
+  return MODE == 0 ? i < a.nxp : (i < a.nx && j < a.ny);
+}
+
+template <int N, int TX, int MODE>
+__global__ void __launch_bounds__(kThreads) k_div_fused(const __grid_constant__ FusedArgs a) {
+  extern __shared__ float2 sm[];
+  float2 *twl = sm;
+  float2 *buf = twl + N;
+  const int x0 = blockIdx.x * TX, j = blockIdx.y, tid = threadIdx.x;
+  const long long plane = (long long)a.cnxp * a.nyp;
+  float2 *col = reinterpret_cast<float2 *>(a.grid) + x0 + (long long)a.cnxp * j;
+  for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
+  for (int idx = tid; idx < TX * N; idx += kThreads) {
+    const int t = idx % TX, m = idx / TX, p = x0 + t;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (p < a.cnxp) {
+      v = col[t + m * plane];
+      float taper = 1.0f;
+      if (MODE == 0 && m > a.nz) {
+        const float d = dist_to_boundary(m, a.nz, a.nzp);
+        taper = fmaxf(__fsub_rn(1.0f, __fmul_rn(d, d)), 0.0f);
+      }
+      if (fused_trace<MODE>(a, 2 * p, j)) {
+        v.x = __fdiv_rn(v.x, a.sq_in);
+        if (MODE == 0 && m > a.nz) v.x = __fmul_rn(v.x, taper);
+      }
+      if (fused_trace<MODE>(a, 2 * p + 1, j)) {
+        v.y = __fdiv_rn(v.y, a.sq_in);
+        if (MODE == 0 && m > a.nz) v.y = __fmul_rn(v.y, taper);
+      }
+    }
+    buf[m * TX + t] = v;
+  }
+  __syncthreads();
+  stockham_ip<N, -1, TX, 1, TX, kThreads>(buf, twl);
+  for (int idx = tid; idx < TX * (N / 2 + 1); idx += kThreads) {
+    const int t = idx % TX, k = idx / TX, p = x0 + t;
+    if (p >= a.cnxp) continue;
+    const int km = k == 0 ? 0 : N - k;
+    const bool self = km == k;
+    const float2 Zk = buf[k * TX + t], Zm = buf[km * TX + t];
+    float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    float2 B = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+    if (fused_trace<MODE>(a, 2 * p, j)) {
+      A = MODE == 0 ? adjust(a.f, k, 2 * p, j, A) : mul_conj(a, k, 2 * p, j, A);
+      if (self) A.y = 0.0f;
+    }
+    if (fused_trace<MODE>(a, 2 * p + 1, j)) {
+      B = MODE == 0 ? adjust(a.f, k, 2 * p + 1, j, B) : mul_conj(a, k, 2 * p + 1, j, B);
+      if (self) B.y = 0.0f;
+    }
+    buf[k * TX + t] = make_float2(A.x - B.y, A.y + B.x);
+    if (!self) buf[km * TX + t] = make_float2(A.x + B.y, B.x - A.y);
+  }
+  __syncthreads();
+  stockham_ip<N, 1, TX, 1, TX, kThreads>(buf, twl);
+  float *rowbase = a.grid + (long long)a.rnxp * j;
+  for (int idx = tid; idx < TX * N; idx += kThreads) {
+    const int t = idx % TX, m = idx / TX, p = x0 + t;
+    if (p >= a.cnxp) continue;
+    const float2 v = buf[m * TX + t];
+    const bool w0 = fused_trace<MODE>(a, 2 * p, j), w1 = fused_trace<MODE>(a, 2 * p + 1, j);
+    float *dst = rowbase + 2 * p + (long long)a.rnxp * a.nyp * m;
+    if (w0 && w1) {
+      *reinterpret_cast<float2 *>(dst) = make_float2(__fdiv_rn(v.x, a.sq_out), __fdiv_rn(v.y, a.sq_out));
+    } else {
+      if (w0) dst[0] = __fdiv_rn(v.x, a.sq_out);
+      if (w1) dst[1] = __fdiv_rn(v.y, a.sq_out);
+    }
+  }
+}
+
+// Launches the fused kernel when the transform length is compiled here;
+// returns false (nothing launched) otherwise.
+template <int MODE>
+bool fused_launch(const FusedArgs &a, cudaStream_t s, int *rc) {
+  constexpr int TX = 8;
+  const dim3 grd((unsigned)((a.cnxp + TX - 1) / TX), (unsigned)a.nyp);
+#define CRAVA_DIV_FUSED(NN)                                                         \
+  if (a.nzp == NN) {                                                                \
+    const size_t smem = sizeof(float2) * (NN + (size_t)TX * NN);                    \
+    if ((*rc = func_smem((const void *)k_div_fused<NN, TX, MODE>, smem))) return true; \
+    k_div_fused<NN, TX, MODE><<<grd, kThreads, smem, s>>>(a);                        \
+    const cudaError_t e_ = cudaGetLastError();                                       \
+    if (e_ != cudaSuccess) {                                                         \
+      ::crava::set_last_error(e_, "kernel launch", __FILE__, __LINE__);              \
+      *rc = CRAVA_GPU_ERR_CUDA;                                                      \
+    } else {                                                                         \
+      *rc = CRAVA_GPU_OK;                                                            \
+    }                                                                                \
+    return true;                                                                     \
+  }
+  CRAVA_DIV_FUSED(128) CRAVA_DIV_FUSED(256) CRAVA_DIV_FUSED(512)
+#undef CRAVA_DIV_FUSED
+  return false;
+}
+
 bool mis8(const void *q) { return !q || (reinterpret_cast<uintptr_t>(q) & 7u) != 0; }
 
 }  // namespace
@@ -541,7 +682,24 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
     fa.low_cut = c->p.low_cut; fa.high_cut = c->p.high_cut; fa.wnc = c->p.wnc;
     const long long nfilt = (long long)g.cnxp * g.nyp * (nzp / 2 + 1);
     const long long rows = (long long)g.nyp * nzp;
+    FusedArgs fu{};
+    fu.tw = c->plans.z.tw;
+    fu.sq_in = fu.sq_out = pa.sq;
+    fu.nx = nx; fu.ny = ny; fu.nxp = g.nxp; fu.nyp = g.nyp; fu.nzp = nzp; fu.cnxp = g.cnxp;
+    fu.rnxp = g.rnxp; fu.nz = c->p.nz;
     for (int l = 0; l < nt; ++l) {
+      fa.W = t.W + (size_t)l * cnzp;
+      fa.E3 = t.E3 + (size_t)l * cnzp;
+      fa.tau2 = t.tau2 + (size_t)l * cnzp;
+      fa.sc = t.sc + l;
+      fa.shift = dshift ? dshift + (size_t)l * nxy : nullptr;
+      fa.gain = dgain ? dgain + (size_t)l * nxy : nullptr;
+      fu.f = fa;
+      fu.grid = data[l];
+      if (fused_launch<0>(fu, s, &r2)) {
+        if (r2) return r2;
+        continue;
+      }
       pa.grid = data[l];
       k_div_save_pads<<<(unsigned)((rows + kThreads - 1) / kThreads), kThreads, 0, s>>>(pa);
       CRAVA_LAUNCH_CHECK();
@@ -549,12 +707,6 @@ extern "C" int crava_gpu_divide_data_by_scale_wavelet(crava_gpu_ctx *c, float *c
       CRAVA_LAUNCH_CHECK();
       if ((r2 = fft_cols_z(c->plans, reinterpret_cast<float2 *>(data[l]), -1, s))) return r2;
       fa.grid = reinterpret_cast<float2 *>(data[l]);
-      fa.W = t.W + (size_t)l * cnzp;
-      fa.E3 = t.E3 + (size_t)l * cnzp;
-      fa.tau2 = t.tau2 + (size_t)l * cnzp;
-      fa.sc = t.sc + l;
-      fa.shift = dshift ? dshift + (size_t)l * nxy : nullptr;
-      fa.gain = dgain ? dgain + (size_t)l * nxy : nullptr;
       k_div_filter<<<(unsigned)((nfilt + kThreads - 1) / kThreads), kThreads, 0, s>>>(fa);
       CRAVA_LAUNCH_CHECK();
       if ((r2 = fft_cols_z(c->plans, reinterpret_cast<float2 *>(data[l]), 1, s))) return r2;
@@ -682,6 +834,7 @@ extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float 
   DeviceGuard guard(c->device);
   const cudaStream_t s = c->stream;
   const size_t nxy = (size_t)nx * ny;
+  const bool fused_len = nzp == 128 || nzp == 256 || nzp == 512;  // k_div_fused lengths
   char *buf = nullptr;
   size_t off = 0;
   auto take = [&](size_t n) { char *q = buf + off; off += (n + 15) & ~size_t(15); return q; };
@@ -705,7 +858,7 @@ extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float 
     dshift = shift ? reinterpret_cast<float *>(take(sizeof(float) * nt * nxy)) : nullptr;
     dgain = gain ? reinterpret_cast<float *>(take(sizeof(float) * nt * nxy)) : nullptr;
     dconst = take(nconst);
-    scratch = reinterpret_cast<float *>(take(sizeof(float) * g.rsize));
+    scratch = fused_len ? nullptr : reinterpret_cast<float *>(take(sizeof(float) * g.rsize));
   };
   carve();  // sizes only (buf is null)
   const size_t bytes = off;
@@ -755,6 +908,23 @@ extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float 
   for (int l = 0; l < nt; ++l) {
     // seisData_[l]->invFFTInPlace() (:844)
     if ((rc = pass_inverse(c, resid[l], CRAVA_GRID_DATA))) return rc;
+    if (fused_len) {
+      FusedArgs fu{};
+      fu.Wm = t.W + (size_t)l * cnzp;
+      fu.sfm = tsf;
+      fu.f.shift = dshift ? dshift + (size_t)l * nxy : nullptr;
+      fu.f.gain = dgain ? dgain + (size_t)l * nxy : nullptr;
+      fu.f.dz = dz;
+      fu.grid = resid[l];
+      fu.tw = c->plans.z.tw;
+      fu.sq_in = sqrtf((float)nzp);
+      fu.sq_out = (float)sqrt((double)nzp);
+      fu.nx = nx; fu.ny = ny; fu.nxp = g.nxp; fu.nyp = g.nyp; fu.nzp = nzp; fu.cnxp = g.cnxp;
+      fu.rnxp = g.rnxp; fu.nz = c->p.nz;
+      fused_launch<1>(fu, s, &rc);
+      if (rc) return rc;
+      continue;
+    }
     MulPassArgs pa{resid[l], scratch, nx, ny, g.nxp, g.nyp, nzp, g.rnxp, sqrtf((float)nzp)};
     k_mul_pre<<<(unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock), kThreads, 0, s>>>(pa);
     CRAVA_LAUNCH_CHECK();

@@ -38,7 +38,9 @@ def test_divide_vs_reference_fixture(name):
 
 
 @pytest.mark.parametrize("shape,nxy,local", [((64, 48, 96), (56, 40), True), ((75, 21, 35), (70, 20), False),
-                                             ((16, 1, 32), (14, 1), True)])
+                                             ((16, 1, 32), (14, 1), True),
+                                             ((40, 30, 128), (36, 28), True),   # fused one-pass kernel
+                                             ((35, 12, 256), (30, 12), False)])
 def test_divide_vs_restatement(shape, nxy, local):
     nxp, nyp, nzp = shape
     nx, ny = nxy
@@ -103,7 +105,9 @@ def test_interpolate_seismic_vs_restatement(shape, nxy, bad):
 
 
 @pytest.mark.parametrize("shape,nxy,local", [((16, 12, 32), (12, 10), True), ((15, 10, 21), (13, 9), False),
-                                             ((16, 1, 32), (14, 1), False)])
+                                             ((16, 1, 32), (14, 1), False),
+                                             ((24, 20, 128), (20, 18), True),   # fused one-pass kernel
+                                             ((15, 9, 256), (13, 9), False)])
 def test_multiply_back_vs_restatement(shape, nxy, local):
     """multiplyDataByScaleWaveletAndWriteToFile (before the write): the
     inverse transform of the residual spectra, then each simbox trace times
