@@ -444,7 +444,8 @@ def run_divide(ctx, case, src, dev, stream, max_over_ranks, peak):
     del data
     return {"workload": "divideDataByScaleWavelet, %d stacks %dx%dx%d" % (case.ntheta, nxp, nyp, nzp),
             "ms_per_call": round(ms, 4), "GB/s": round(gbs, 1), "frac_of_peak": round(gbs / peak, 4),
-            "passes": "per stack: taper, z transform, per-trace filter, inverse z transform, scale"}
+            "passes": "per stack one pass over HBM at z lengths 128/256/512 (taper, z transform, "
+                      "per-trace filter, inverse z transform, scale in one kernel); five passes otherwise"}
 
 
 def run_forward(ctx, case, src, dev, stream, max_over_ranks):

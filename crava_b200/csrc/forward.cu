@@ -108,6 +108,90 @@ __global__ void __launch_bounds__(kThreads) k_synt(const __grid_constant__ SyntA
   }
 }
 
+// All angles in one pass: a CTA holds its TX lines of the three parameter
+// grids in registers (read from HBM once) and, per angle, forms the
+// impedance in shared memory, tapers, transforms, filters, transforms back
+// and stores: 3 grid reads + nt writes instead of nt (3 reads + 1 write).
+struct SyntAllArgs {
+  const float2 *m[3];
+  float2 *out[CRAVA_GPU_MAX_THETA];
+  const float2 *H;  // [nt][nzp]
+  const float2 *tw;
+  float A[CRAVA_GPU_MAX_THETA][3];
+  int nt, cnxp, nyp, nzp, nx, ny, nz;
+};
+
+template <int N, int TX>
+__global__ void __launch_bounds__(kThreads, N == 256 ? 1 : 2) k_synt_all(const __grid_constant__ SyntAllArgs a) {
+  static_assert((TX * N) % kThreads == 0, "whole elements per thread");
+  constexpr int E = TX * N / kThreads;
+  extern __shared__ float2 sm[];
+  float2 *twl = sm;
+  float2 *buf = twl + N;
+  const int x0 = blockIdx.x * TX, y = blockIdx.y, tid = threadIdx.x;
+  const long long plane = (long long)a.cnxp * a.nyp;
+  const long long base = x0 + (long long)a.cnxp * y;
+  for (int i = tid; i < N; i += kThreads) twl[i] = a.tw[i];
+  float2 pm[3][E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int idx = tid + e * kThreads, t = idx % TX, m = idx / TX;
+    const bool in = x0 + t < a.cnxp;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) pm[q][e] = in ? a.m[q][base + m * plane + t] : make_float2(0.f, 0.f);
+  }
+  for (int l = 0; l < a.nt; ++l) {
+    const float A[3] = {a.A[l][0], a.A[l][1], a.A[l][2]};
+    __syncthreads();  // the previous angle's stores have read buf
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = tid + e * kThreads, t = idx % TX, m = idx / TX;
+      buf[m * TX + t] = make_float2(imp1(pm[0][e].x, pm[1][e].x, pm[2][e].x, A),
+                                    imp1(pm[0][e].y, pm[1][e].y, pm[2][e].y, A));
+    }
+    __syncthreads();
+    if (y < a.ny && a.nz < N) {
+      for (int idx = tid; idx < TX * (N - a.nz); idx += kThreads) {
+        const int t = idx % TX, m = a.nz + idx / TX;
+        const float2 v0 = buf[t], vl = buf[(a.nz - 1) * TX + t];
+        buf[m * TX + t] = make_float2(taper(v0.x, vl.x, m, a.nz, N), taper(v0.y, vl.y, m, a.nz, N));
+      }
+    }
+    __syncthreads();
+    stockham_ip<N, -1, TX, 1, TX, kThreads>(buf, twl);
+    const float2 *H = a.H + (long long)l * N;
+    for (int idx = tid; idx < TX * N; idx += kThreads) {
+      float2 *b = buf + idx;  // (m, t) at m TX + t = idx
+      *b = cmul(*b, __ldg(H + idx / TX));
+    }
+    __syncthreads();
+    stockham_ip<N, 1, TX, 1, TX, kThreads>(buf, twl);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = tid + e * kThreads, t = idx % TX, m = idx / TX;
+      const int p = x0 + t;
+      if (p >= a.cnxp) continue;
+      float2 v = buf[m * TX + t];
+      const bool fx = 2 * p < a.nx, fy = 2 * p + 1 < a.nx;
+      if (y >= a.ny || !fx) v.x = imp1(pm[0][e].x, pm[1][e].x, pm[2][e].x, A);
+      if (y >= a.ny || !fy) v.y = imp1(pm[0][e].y, pm[1][e].y, pm[2][e].y, A);
+      a.out[l][base + m * plane + t] = v;
+    }
+  }
+}
+
+template <int N>
+int launch_synt_all(const SyntAllArgs &a, cudaStream_t s) {
+  constexpr int TX = 4;
+  const size_t smem = sizeof(float2) * (N + (size_t)TX * N);
+  int rc = func_smem((const void *)k_synt_all<N, TX>, smem);
+  if (rc) return rc;
+  const dim3 grd((unsigned)((a.cnxp + TX - 1) / TX), (unsigned)a.nyp);
+  k_synt_all<N, TX><<<grd, kThreads, smem, s>>>(a);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
 // Generic lengths, step 1: impedance and taper written to the output grid.
 __global__ void __launch_bounds__(kThreads) k_synt_imp(const __grid_constant__ SyntArgs a) {
   const long long plane = (long long)a.cnxp * a.nyp;
@@ -223,6 +307,22 @@ extern "C" int crava_gpu_synt_seismic(crava_gpu_ctx *c, const float *alpha, cons
   const long long n = c->g.csize;
   const dim3 eg((unsigned)((n + kThreads - 1) / kThreads));
   int rc;
+  if (c->g.nzp == 128 || c->g.nzp == 256 || c->g.nzp == 512) {
+    SyntAllArgs b{};
+    for (int q = 0; q < 3; ++q) b.m[q] = a.m[q];
+    for (int l = 0; l < nt; ++l) {
+      b.out[l] = reinterpret_cast<float2 *>(out[l]);
+      for (int q = 0; q < 3; ++q) b.A[l][q] = c->A[3 * l + q];
+    }
+    b.H = c->synt_H;
+    b.tw = a.tw;
+    b.nt = nt; b.cnxp = a.cnxp; b.nyp = a.nyp; b.nzp = a.nzp; b.nx = nx; b.ny = ny; b.nz = nz;
+    switch (c->g.nzp) {
+      case 128: return launch_synt_all<128>(b, s);
+      case 256: return launch_synt_all<256>(b, s);
+      default: return launch_synt_all<512>(b, s);
+    }
+  }
   for (int l = 0; l < nt; ++l) {
     a.out = reinterpret_cast<float2 *>(out[l]);
     a.H = c->synt_H + (size_t)l * c->g.nzp;

@@ -44,10 +44,13 @@ def test_synt_vs_reference_golden(name):
         k += 1
 
 
-# compiled z lengths (fused kernel) and one generic length
+# compiled z lengths (fused kernels) and generic lengths
 @pytest.mark.parametrize("shape,nz,nx,ny", [((16, 12, 64), 50, 13, 10), ((8, 6, 128), 128, 8, 6),
                                              ((10, 4, 96), 90, 10, 4), ((6, 4, 300), 260, 5, 4),
-                                             ((12, 6, 384), 384, 12, 6), ((9, 5, 40), 33, 9, 5)])
+                                             ((12, 6, 384), 384, 12, 6), ((9, 5, 40), 33, 9, 5),
+                                             # all angles in one pass (z lengths 128, 256, 512)
+                                             ((12, 10, 128), 100, 10, 9), ((12, 8, 256), 200, 11, 7),
+                                             ((10, 6, 512), 480, 9, 5)])
 def test_synt_vs_restatement(shape, nz, nx, ny):
     case = synth.make_case(*shape, (0.0, 20.0, 40.0), 0.1, seed=9)
     case.nz = nz
