@@ -149,6 +149,37 @@ class CravaDevice {
     return 0;
   }
 
+  // Crava::divideDataByScaleWavelet (src/crava.cpp:591-722) on the
+  // real-domain stacks, closed by FFTGrid::interpolateSeismic per stack
+  // (energyThreshold = ModelSettings::getEnergyThreshold).  relThick:
+  // [nyp][nxp] Simbox::getRelThick; shift / gain: [ntheta][ny][nx] or null.
+  int divideDataByScaleWavelet(FFTGridDevice **data, FFTGridDevice *covAlpha, const double *relThick,
+                               int nx, int ny, float dz, float energyThreshold,
+                               const float *shift = nullptr, const float *gain = nullptr) {
+    std::vector<float *> d(nt_);
+    for (int l = 0; l < nt_; ++l) d[l] = data[l]->devicePtr();
+    check(crava_gpu_divide_data_by_scale_wavelet(ctx_, d.data(), covAlpha->devicePtr(), relThick, nx, ny, dz,
+                                                 shift, gain),
+          "divideDataByScaleWavelet");
+    for (int l = 0; l < nt_; ++l)
+      check(crava_gpu_interpolate_seismic(ctx_, d[l], nx, ny, energyThreshold, nullptr, nullptr),
+            "interpolateSeismic");
+    return 0;
+  }
+
+  // Crava::multiplyDataByScaleWaveletAndWriteToFile (src/crava.cpp:819-885)
+  // up to the write: the residual spectra back in the time domain, each
+  // simbox trace times its local wavelet's conjugate spectrum.
+  int multiplyDataByScaleWavelet(FFTGridDevice **resid, const double *relThick, int nx, int ny, float dz,
+                                 const float *shift = nullptr, const float *gain = nullptr) {
+    std::vector<float *> d(nt_);
+    for (int l = 0; l < nt_; ++l) d[l] = resid[l]->devicePtr();
+    check(crava_gpu_multiply_data_by_scale_wavelet(ctx_, d.data(), relThick, nx, ny, dz, shift, gain),
+          "multiplyDataByScaleWavelet");
+    for (int l = 0; l < nt_; ++l) resid[l]->setTransformedStatus(false);
+    return 0;
+  }
+
   crava_gpu_stats stats() {
     crava_gpu_stats s{};
     check(crava_gpu_get_stats(ctx_, &s), "get_stats");
