@@ -345,3 +345,111 @@ def test_multiply_data_vs_ref_live(name, local):
         assert rel(x[:, :ny, :nx], y[:, :ny, :nx]) < 1e-5
         assert np.array_equal(x[:, ny:, :], d[:, ny:, :])
         assert rel(x[:, :ny, :nx], d[:, :ny, :nx]) > 0.1
+
+
+def _interpolate_py(g, nxp, nyp, nzp, nx, ny, nz, thr):
+    """FFTGrid::interpolateSeismic / interpolateTrace / extrapolateSeismic
+    (src/fftgrid.cpp:2564-2731) restated again in Python with float32
+    arithmetic, independently of the C restatement."""
+    f32 = np.float32
+    g = g.copy()
+    at = lambda i, j: g[:, j, i]  # a trace, all nzp samples
+    energy = np.zeros(nx * ny, f32)
+    total = f32(0)
+    for j in range(ny):
+        for i in range(nx):
+            e = f32(0)
+            for k in range(nz):
+                v = g[k, j, i]
+                e = f32(e + f32(v * v))
+            energy[i + nx * j] = e
+            total = f32(total + e)
+    limit = f32(f32(f32(thr) * total) / f32(nx * ny))
+    flags = [0] * (nx * ny)
+    flag, imin, imax, jmin, jmax, bad = 0, nx, 0, ny, 0, 0
+    for j in range(ny):
+        for i in range(nx):
+            idx = i + nx * j
+            cur = 1 if energy[idx] <= limit else 0
+            bad += cur
+            flags[idx] = flag + cur
+            if cur:
+                flag = 2
+            else:
+                imin, imax, jmin, jmax = min(imin, i), max(imax, i), min(jmin, j), max(jmax, j)
+
+    def trace(idx, i, j):
+        left = i > 0 and flags[idx - 1] % 2 == 0
+        right = i < nx - 1 and flags[idx + 1] % 2 == 0
+        up = j > 0 and flags[idx - nx] % 2 == 0
+        down = j < ny - 1 and flags[idx + nx] % 2 == 0
+        nt = left + right + up + down
+        if nt > 1:
+            m = at(i - 1, j).copy() if left else np.zeros(nzp, f32)
+            for ok, (a, b) in ((right, (i + 1, j)), (up, (i, j - 1)), (down, (i, j + 1))):
+                if ok:
+                    m = (m + at(a, b)).astype(f32)
+            g[:, j, i] = (m / f32(nt)).astype(f32)
+            flags[idx] -= 1
+        return flags[idx]
+
+    cur = 0
+    for j in range(ny):
+        for i in range(nx):
+            if flags[cur] % 2 == 1 and trace(cur, i, j) % 2 == 0:
+                idx = cur - 1
+                while idx >= 0 and flags[idx] > 1:
+                    if flags[idx] % 2 == 1:
+                        trace(idx, idx % nx, idx // nx)
+                    idx -= 1
+                idx = max(idx, 0) + 1
+                while idx <= cur and flags[idx - 1] == 0:
+                    if flags[idx] > 1:
+                        flags[idx] -= 2
+                    idx += 1
+            cur += 1
+
+    def fill(i, n, npad):
+        if i < n:
+            return i
+        below, above = npad - i - 1, i - n + 1
+        return max(n - above, n // 2) if above < below else min(below, n // 2)
+
+    def dist(i, n, npad):
+        if i < n:
+            return f32(0)
+        taper = f32(min(n, npad - n) / 2.1)
+        below, above = npad - i, i - (n - 1)
+        return f32(f32(above) / taper) if above < below else f32(f32(below) / taper)
+
+    if imin <= imax:
+        for j in range(nyp):
+            rj = min(max(fill(j, ny, nyp), jmin), jmax)
+            for i in range(nxp):
+                if i < imin or i > imax or j < jmin or j > jmax:
+                    ri = min(max(fill(i, nx, nxp), imin), imax)
+                    for k in range(nzp):
+                        dx, dy, dzz = dist(i, nx, nxp), dist(j, ny, nyp), dist(k, nz, nzp)
+                        b = 1.0 - float(f32(dx * dx)) - float(f32(dy * dy)) - float(f32(dzz * dzz))
+                        mult = f32(max(b, 0.0) ** 3)
+                        g[k, j, i] = f32(mult * g[k, rj, ri])
+    return g, bad
+
+
+@pytest.mark.parametrize("bad", [[(3, 4), (4, 4), (5, 4), (0, 0), (11, 9), (5, 0), (6, 6), (7, 7), (6, 7)],
+                                 [(0, j) for j in range(10)] + [(9, 9), (8, 8), (8, 9)]])
+def test_interpolate_seismic_two_restatements(bad):
+    """The C restatement of interpolateSeismic equals an independent Python
+    one: the simbox traces bit for bit, the extrapolated padding to 1 ulp
+    (pow of the two C libraries' callers)."""
+    nxp, nyp, nzp, nx, ny, nz = 16, 12, 12, 12, 10, 9
+    rng = np.random.default_rng(2)
+    g = rng.standard_normal((nzp, nyp, 2 * (nxp // 2 + 1))).astype(np.float32)
+    for n, (i, j) in enumerate(bad):
+        g[:, j, i] = 0.0 if n % 2 == 0 else 1e-3
+    a, ni, _ = O.interpolate_seismic(g, nxp, nyp, nzp, nx, ny, nz, 0.05)
+    b, nb = _interpolate_py(g, nxp, nyp, nzp, nx, ny, nz, 0.05)
+    assert ni == nb == len(bad)
+    assert np.array_equal(a[:, :ny, :nx], b[:, :ny, :nx])
+    d = np.abs(a.view(np.int32).astype(np.int64) - b.view(np.int32).astype(np.int64))
+    assert d[..., :nxp].max() <= 1
