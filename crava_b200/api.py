@@ -148,6 +148,8 @@ SYMBOLS = {
                                                   C.c_float, F32P, F32P], C.c_int),
     "crava_gpu_interpolate_seismic": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "crava_gpu_fft_xy": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
+    "crava_gpu_fft_z": ([C.c_void_p, C.c_void_p, C.c_int], C.c_int),
     "crava_gpu_posterior_noalloc": ([C.POINTER(Params), C.POINTER(Grids), C.c_int, C.c_void_p,
                                      C.POINTER(Stats)], C.c_int),
 }
@@ -251,6 +253,17 @@ class Context:
 
     def fft_c2r(self, grid, grid_type):
         check(self.lib.crava_gpu_fft_c2r(self.handle, _ptr(grid), grid_type), "fft_c2r")
+
+    def fft_xy(self, grid, direction, grid_type, nzp_full=None):
+        """The x and y passes only (-1 forward, +1 inverse), scaled as the
+        whole grid of nzp_full planes (crava_gpu_fft_xy): one z slab of a
+        grid split over GPUs."""
+        nz = self.case.nzp if nzp_full is None else nzp_full
+        check(self.lib.crava_gpu_fft_xy(self.handle, _ptr(grid), direction, grid_type, nz), "fft_xy")
+
+    def fft_z(self, grid, direction):
+        """The unscaled z pass only (crava_gpu_fft_z): one column shard."""
+        check(self.lib.crava_gpu_fft_z(self.handle, _ptr(grid), direction), "fft_z")
 
     def posterior(self, mu, data, cov, err, precision=None):
         g = self.grids(mu, data, cov, err)

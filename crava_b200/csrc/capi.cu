@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include <math.h>
+
 #include "context.cuh"
 
 namespace crava {
@@ -458,6 +460,30 @@ int crava_gpu_fft_c2r(crava_gpu_ctx *c, float *grid, int type) {
   if (type < CRAVA_GRID_DATA || type > CRAVA_GRID_COVARIANCE) return CRAVA_GPU_ERR_ARG;
   DeviceGuard guard(c->device);
   return pass_inverse(c, grid, type);
+}
+
+int crava_gpu_fft_xy(crava_gpu_ctx *c, float *grid, int dir, int type, int nzp_full) {
+  if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
+  if ((dir != -1 && dir != 1) || type < CRAVA_GRID_DATA || type > CRAVA_GRID_COVARIANCE) return CRAVA_GPU_ERR_ARG;
+  if (nzp_full < c->g.nzp) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  // the scale of the whole grid, rounded exactly as the 3-D transforms round it
+  const Geom full = Geom::make(c->g.nxp, c->g.nyp, nzp_full);
+  const float scale = dir < 0 ? forward_scale(full, type) : inverse_scale(full, type);
+  int rc;
+  if (dir < 0) {
+    if ((rc = fft_rows(c->plans, grid, -1, scale, c->stream))) return rc;
+    return fft_cols_y(c->plans, reinterpret_cast<float2 *>(grid), -1, c->stream);
+  }
+  if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc;
+  return fft_rows(c->plans, grid, 1, scale, c->stream);
+}
+
+int crava_gpu_fft_z(crava_gpu_ctx *c, float *grid, int dir) {
+  if (check_ctx(c) || !grid || (reinterpret_cast<uintptr_t>(grid) & 7u)) return CRAVA_GPU_ERR_ARG;
+  if (dir != -1 && dir != 1) return CRAVA_GPU_ERR_ARG;
+  DeviceGuard guard(c->device);
+  return fft_cols_z(c->plans, reinterpret_cast<float2 *>(grid), dir, c->stream);
 }
 
 int crava_gpu_posterior(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {

@@ -1,0 +1,174 @@
+"""One posterior unit whose grids are split over several GPUs.
+
+The reference transforms a whole grid on one host (FFTGrid::fftInPlace,
+src/fftgrid.cpp:1803-1829) and solves every bin in one loop
+(src/crava.cpp:1042-1151).  For a grid too large for one GPU the unit is
+split the way the transform factorises:
+
+* z slabs: rank r holds planes [z0_r, z1_r) of every real grid and runs the
+  x and y passes on them (crava_gpu_fft_xy, scaled as the full grid);
+* one all-to-all moves the spectra to (kx, ky) column shards: rank r then
+  holds rows [y0_r, y1_r) of every kz plane, runs the z pass
+  (crava_gpu_fft_z) and the per-bin solve (crava_gpu_posterior), which
+  needs nothing outside its own bins, and the inverse z pass;
+* one all-to-all back to z slabs and the inverse y and x passes.
+
+Per posterior the exchange moves (10 + nt) grids out and (9 + nt) back,
+each rank sending (P - 1) / P of its share; received blocks land in local
+memory before use.  The transforms and the solve are passed in as
+functions, so the same exchange code runs with the device kernels on GPUs
+(``device_ops``) and with numpy stand-ins in the two-rank gloo tests.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+
+def split_range(n: int, parts: int, r: int):
+    """[lo, hi) of the r-th of `parts` nearly equal pieces of range(n)."""
+    base, extra = divmod(n, parts)
+    lo = r * base + min(r, extra)
+    return lo, lo + base + (1 if r < extra else 0)
+
+
+@dataclass
+class Layout:
+    """z-slab and ky-column partition of an (nxp, nyp, nzp) grid over P ranks."""
+    nxp: int
+    nyp: int
+    nzp: int
+    world: int
+
+    @property
+    def cnxp(self):
+        return self.nxp // 2 + 1
+
+    def z(self, r):
+        return split_range(self.nzp, self.world, r)
+
+    def y(self, r):
+        return split_range(self.nyp, self.world, r)
+
+
+def _exchange(dist, sends, recvs, rank):
+    """Point-to-point all-to-all: sends[d] to rank d, recvs[s] from rank s
+    (the rank's own block is copied).  Works with the nccl and gloo
+    backends alike."""
+    reqs = []
+    for peer in range(len(sends)):
+        if peer == rank:
+            recvs[peer].copy_(sends[peer])
+            continue
+        reqs.append(dist.isend(sends[peer].contiguous(), peer))
+        reqs.append(dist.irecv(recvs[peer], peer))
+    for q in reqs:
+        q.wait()
+
+
+def to_columns(slab, lay: Layout, rank: int, dist):
+    """z slab [nz_r, nyp, 2 cnxp] (float32, complex pairs after the xy
+    passes) -> column shard [nzp, ny_r, 2 cnxp] of this rank."""
+    import torch
+
+    z0, z1 = lay.z(rank)
+    y0, y1 = lay.y(rank)
+    assert tuple(slab.shape) == (z1 - z0, lay.nyp, 2 * lay.cnxp)
+    sends = [slab[:, lay.y(d)[0]:lay.y(d)[1], :].contiguous() for d in range(lay.world)]
+    recvs = [torch.empty((lay.z(s)[1] - lay.z(s)[0], y1 - y0, 2 * lay.cnxp), dtype=slab.dtype,
+                         device=slab.device) for s in range(lay.world)]
+    if dist is None:
+        recvs[0].copy_(sends[0])
+    else:
+        _exchange(dist, sends, recvs, rank)
+    return torch.cat(recvs, dim=0)
+
+
+def to_slabs(cols, lay: Layout, rank: int, dist):
+    """Column shard [nzp, ny_r, 2 cnxp] -> z slab [nz_r, nyp, 2 cnxp]."""
+    import torch
+
+    z0, z1 = lay.z(rank)
+    y0, y1 = lay.y(rank)
+    assert tuple(cols.shape) == (lay.nzp, y1 - y0, 2 * lay.cnxp)
+    sends = [cols[lay.z(d)[0]:lay.z(d)[1]].contiguous() for d in range(lay.world)]
+    recvs = [torch.empty((z1 - z0, lay.y(s)[1] - lay.y(s)[0], 2 * lay.cnxp), dtype=cols.dtype,
+                         device=cols.device) for s in range(lay.world)]
+    if dist is None:
+        recvs[0].copy_(sends[0])
+    else:
+        _exchange(dist, sends, recvs, rank)
+    return torch.cat(recvs, dim=1)
+
+
+# grid types (FFTGrid::gridTypes, src/fftgrid.h:172)
+DATA, PARAMETER, COVARIANCE = 1, 2, 3
+
+
+def scales(n: int, gtype: int):
+    """Forward and inverse scale of a whole grid of n cells (fftInPlace /
+    invFFTInPlace, src/fftgrid.cpp:1817, 1848-1859): the device computes
+    its own; host stand-ins of the passes use these."""
+    if gtype == COVARIANCE:
+        return 1.0, 1.0 / n
+    return 1.0 / math.sqrt(n), 1.0 / math.sqrt(n)
+
+
+def posterior_unit_split(ops, lay: Layout, rank: int, dist, mu, data, cov, err):
+    """The posterior unit on this rank's z slabs (real padded layout,
+    [nz_r, nyp, rnxp] float32), in place: means, stacks and covariances
+    come back as posterior means, residuals and posterior covariances.
+    ops: fft_xy(grid, dir, grid_type) on slabs (scaled as the whole grid
+    of that type), fft_z(grid, dir) and solve(mu, data, cov, err) on
+    column shards."""
+    types = [PARAMETER] * len(mu) + [DATA] * len(data) + [COVARIANCE] * (len(cov) + 1)
+    grids = list(mu) + list(data) + list(cov) + [err]
+    cols = []
+    for g, t in zip(grids, types):
+        ops.fft_xy(g, -1, t)
+        c = to_columns(g, lay, rank, dist)
+        ops.fft_z(c, -1)
+        cols.append(c)
+    nm, nd, nc = len(mu), len(data), len(cov)
+    cm, cd, cc, ce = cols[:nm], cols[nm:nm + nd], cols[nm + nd:nm + nd + nc], cols[-1]
+    ops.solve(cm, cd, cc, ce)
+    for g, c, t in zip(grids[:-1], cols[:-1], types[:-1]):
+        ops.fft_z(c, 1)
+        g.copy_(to_slabs(c, lay, rank, dist))
+        ops.fft_xy(g, 1, t)
+
+
+class device_ops:
+    """The device kernels for posterior_unit_split: x/y passes on a z-slab
+    context, z pass and solve on a column-shard context (crava_b200.api)."""
+
+    def __init__(self, ctx_slab, ctx_cols, precision, nzp_full):
+        self.s, self.c, self.p, self.nzp = ctx_slab, ctx_cols, precision, nzp_full
+
+    def fft_xy(self, g, d, gtype):
+        self.s.fft_xy(g, d, gtype, self.nzp)
+
+    def fft_z(self, g, d):
+        self.c.fft_z(g, d)
+
+    def solve(self, mu, data, cov, err):
+        self.c.posterior(mu, data, cov, err, self.p)
+
+
+def shard_case(case, nyp=None, nzp=None):
+    """The case seen by a slab (nzp planes) or column-shard (nyp rows)
+    context: same model constants, local geometry.  A slab context only
+    transforms along x and y, so its wavelets are the first nzp samples."""
+    from types import SimpleNamespace
+
+    c = SimpleNamespace(**{k: getattr(case, k) for k in
+                           ("nxp", "nyp", "nzp", "ntheta", "nz", "lz", "min_rel_thick", "low_cut",
+                            "high_cut", "wnc", "wavelet", "A", "theta_cov", "var0")})
+    c.thickness_mode = int(getattr(case, "thickness_mode", 0))
+    if nyp is not None:
+        c.nyp = nyp
+    if nzp is not None:
+        c.nzp = nzp
+        c.wavelet = case.wavelet[:, :nzp].copy()
+        c.nz = min(case.nz, nzp)
+    return c

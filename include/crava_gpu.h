@@ -118,6 +118,18 @@ int crava_gpu_fft_r2c(crava_gpu_ctx *ctx, float *grid, int grid_type);
  * FFTGrid::invFFTInPlace, src/fftgrid.cpp:1831-1862. */
 int crava_gpu_fft_c2r(crava_gpu_ctx *ctx, float *grid, int grid_type);
 
+/* The halves of a 3-D transform, for a grid split over GPUs (z slabs for
+ * the x and y passes, (kx, ky) column shards for the z pass):
+ * crava_gpu_fft_xy runs the x then y passes (dir -1, forward) or the y then
+ * x passes (dir +1, inverse) over every plane of a grid of the context's
+ * geometry (a slab: the context's nzp planes of a grid of nzp_full), the
+ * real <-> half-complex x transform scaled as fftInPlace / invFFTInPlace
+ * scale the whole grid of grid_type; crava_gpu_fft_z runs the unscaled
+ * complex z pass over every column.  On one GPU (nzp_full = nzp) they
+ * equal crava_gpu_fft_r2c / _c2r bit for bit. */
+int crava_gpu_fft_xy(crava_gpu_ctx *ctx, float *grid, int dir, int grid_type, int nzp_full);
+int crava_gpu_fft_z(crava_gpu_ctx *ctx, float *grid, int dir);
+
 /* Per-(kx,ky,kz) posterior solve on transformed grids, in place:
  * mu <- posterior mean, data <- residual, cov <- posterior covariance
  * (err_corr is read).  Replaces the loop of
