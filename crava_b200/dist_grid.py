@@ -138,6 +138,47 @@ def posterior_unit_split(ops, lay: Layout, rank: int, dist, mu, data, cov, err):
         ops.fft_xy(g, 1, t)
 
 
+def spectra_to_columns(ops, lay: Layout, rank: int, dist, mu, data, cov, err):
+    """The forward half of the split unit: the slabs' spectra on this
+    rank's column shards (mu, data, cov, err), the slabs left as they were
+    after their x and y passes."""
+    types = [PARAMETER] * len(mu) + [DATA] * len(data) + [COVARIANCE] * (len(cov) + 1)
+    cols = []
+    for g, t in zip(list(mu) + list(data) + list(cov) + [err], types):
+        ops.fft_xy(g, -1, t)
+        c = to_columns(g, lay, rank, dist)
+        ops.fft_z(c, -1)
+        cols.append(c)
+    nm, nd, nc = len(mu), len(data), len(cov)
+    return cols[:nm], cols[nm:nm + nd], cols[nm + nd:nm + nd + nc], cols[-1]
+
+
+def loglik_grad_split(loglik, dist, mu_c, data_c, cov_c, err_c, *args):
+    """The log marginal likelihood and its gradients over a grid split
+    into column shards: every rank evaluates its own bins (`loglik`, e.g.
+    a column-shard context's loglik_grad) and one all-reduce sums the value,
+    the gradients and the failed-bin count (5 + 5 + 2 (nzp/2 + 1) 5 + 2
+    doubles for five angles)."""
+    import numpy as np
+
+    L, gs, gv, gw, nf = loglik(mu_c, data_c, cov_c, err_c, *args)
+    if dist is None:
+        return L, gs, gv, gw, nf
+    import torch
+
+    gw = np.asarray(gw)
+    flat = np.concatenate([[L], gs, gv, gw.real.reshape(-1), gw.imag.reshape(-1), [nf]]).astype(np.float64)
+    t = torch.from_numpy(flat)
+    if dist.get_backend() == "nccl":
+        t = t.cuda()
+    dist.all_reduce(t)
+    f = t.cpu().numpy()
+    nt, nw = len(gs), gw.size
+    gwr = f[1 + 2 * nt:1 + 2 * nt + nw].reshape(gw.shape)
+    gwi = f[1 + 2 * nt + nw:1 + 2 * nt + 2 * nw].reshape(gw.shape)
+    return float(f[0]), f[1:1 + nt], f[1 + nt:1 + 2 * nt], gwr + 1j * gwi, int(round(f[-1]))
+
+
 class device_ops:
     """The device kernels for posterior_unit_split: x/y passes on a z-slab
     context, z pass and solve on a column-shard context (crava_b200.api)."""

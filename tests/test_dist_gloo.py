@@ -185,3 +185,63 @@ def test_split_round_trip_is_identity():
     nx = SPLIT_SHAPE[0]
     for a, b in zip(mu_t + data_t + cov_t, mu + data + cov):
         assert np.allclose(a.numpy()[..., :nx], b[..., :nx], rtol=1e-5, atol=1e-5)
+
+
+def _loglik_worker(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch
+    from crava_b200 import dist as D
+    from crava_b200 import dist_grid as G
+
+    dist = D.init("gloo", timeout_s=60)
+    lay = G.Layout(*SPLIT_SHAPE, world)
+    z0, z1 = lay.z(rank)
+    mu, data, cov, err = _split_inputs()
+    t = lambda gs: [torch.from_numpy(g[z0:z1].copy()) for g in gs]
+    cols = G.spectra_to_columns(_NumpyOps(lay.nxp, lay.nxp * lay.nyp * lay.nzp), lay, rank, dist,
+                                t(mu), t(data), t(cov), t([err])[0])
+    out.put((rank, G.loglik_grad_split(_toy_loglik, dist, *cols)))
+    dist.destroy_process_group()
+
+
+def _toy_loglik(mu, data, cov, err):
+    """A per-bin sum with the shape of the real functional's outputs."""
+    import numpy as np
+    c = lambda g: g.numpy().view(np.complex64).astype(np.complex128)
+    L = float(sum((np.abs(c(d)) ** 2).sum() for d in data))
+    gs = np.array([float(np.abs(c(d)).sum()) for d in data])
+    gv = np.array([float(c(m).real.sum()) for m in mu[:len(data)]])
+    gw = np.stack([c(d).sum(axis=(1, 2)) for d in data], -1)[: SPLIT_SHAPE[2] // 2 + 1]
+    return L, gs, gv, gw, int((np.abs(c(err)) > 1.0).sum())
+
+
+def test_loglik_over_split_grid_sums_the_shards():
+    """The all-reduced per-shard functional over 3 gloo ranks equals the
+    whole grid's."""
+    import numpy as np
+    import torch
+    from crava_b200 import dist_grid as G
+
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_loglik_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    lay = G.Layout(*SPLIT_SHAPE, 1)
+    mu, data, cov, err = _split_inputs()
+    t = lambda gs: [torch.from_numpy(g.copy()) for g in gs]
+    cols = G.spectra_to_columns(_NumpyOps(lay.nxp, lay.nxp * lay.nyp * lay.nzp), lay, 0, None,
+                                t(mu), t(data), t(cov), t([err])[0])
+    L, gs, gv, gw, nf = G.loglik_grad_split(_toy_loglik, None, *cols)
+    for r in range(world):
+        L2, gs2, gv2, gw2, nf2 = res[r]
+        assert np.isclose(L2, L, rtol=1e-6) and nf2 == nf
+        assert np.allclose(gs2, gs, rtol=1e-6) and np.allclose(gv2, gv, rtol=1e-5, atol=1e-6)
+        assert np.allclose(gw2, gw, rtol=1e-5, atol=1e-5)
