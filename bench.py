@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-forward", action="store_true")
     ap.add_argument("--no-state4d", action="store_true")
     ap.add_argument("--no-divide", action="store_true")
+    ap.add_argument("--split-grid", action="store_true",
+                    help="with several ranks, also time one grid split over them (z slabs <-> column shards)")
+    ap.add_argument("--no-split-grid", action="store_true")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
     return ap.parse_args()
@@ -451,6 +454,62 @@ def run_divide(ctx, case, src, dev, stream, max_over_ranks, peak):
                       "per-trace filter, inverse z transform, scale in one kernel); five passes otherwise"}
 
 
+def run_split(case, world, rank, dist, dev, stream, max_over_ranks, prec):
+    """One posterior unit with its grids split over the ranks (z slabs for
+    the x and y passes, column shards for the z pass and the solve, one
+    exchange each way; crava_b200.dist_grid): device time per unit, max
+    over ranks, on pristine inputs every repetition."""
+    import numpy as np
+    import torch
+
+    from crava_b200 import api
+    from crava_b200 import dist_grid as G
+
+    lay = G.Layout(case.nxp, case.nyp, case.nzp, world)
+    G.check_layout(lay)
+    z0, z1 = lay.z(rank)
+    y0, y1 = lay.y(rank)
+    cs = api.Context(G.shard_case(case, nzp=z1 - z0), device=dev, stream=stream, precision=prec)
+    cc = api.Context(G.shard_case(case, nyp=y1 - y0), device=dev, stream=stream, precision=prec)
+    ops = G.device_ops(cs, cc, prec, case.nzp)
+    nt = case.ntheta
+    with torch.cuda.stream(stream):
+        src = [torch.from_numpy(np.ascontiguousarray(g[z0:z1])).to(dev) for g in case.grids()]
+        work = [torch.empty_like(g) for g in src]
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    reps, total = 5, 0.0
+    for rep in range(2 + reps):
+        with torch.cuda.stream(stream):
+            for w, s0 in zip(work, src):
+                w.copy_(s0)
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            G.posterior_unit_split(ops, lay, rank, dist, work[:3], work[3:3 + nt], work[3 + nt:9 + nt],
+                                   work[9 + nt])
+            ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        if rep >= 2:
+            total += ev0.elapsed_time(ev1)
+    ms = max_over_ranks(total / reps)
+    cells = case.nxp * case.nyp * case.nzp
+    grid_bytes = case.mu[0].nbytes
+    out_bytes = (10 + nt) * grid_bytes * (world - 1) / world
+    back_bytes = (9 + nt) * grid_bytes * (world - 1) / world
+    cs.close()
+    cc.close()
+    del src, work
+    return {"workload": "one posterior unit %dx%dx%d, 5 angles, split over %d rank(s)"
+                        % (case.nxp, case.nyp, case.nzp, world),
+            "ranks": world, "ms_per_unit": round(ms, 4), "value": cells / (ms * 1e-3), "unit": "cells/s",
+            "exchange_bytes_per_rank": out_bytes + back_bytes,
+            "note": "one rank: the exchange is a local copy (the path's overhead over the one-GPU unit)"
+                    if world == 1 else "strong scaling of one grid"}
+
+
 def run_forward(ctx, case, src, dev, stream, max_over_ranks):
     """Synthetic seismic (Crava::computeSyntSeismic) of the three parameter
     grids for all angles: device time per call and HBM rate against the
@@ -692,6 +751,12 @@ def run_own(args):
 
     prior = run_prior_fill(ctx, case, dst, dev, stream, max_over_ranks)
 
+    split = None
+    if not args.no_split_grid and (world == 1 or args.split_grid):
+        gcase = case if world == 1 else synth.make_case(nxp, nyp, nzp, ANGLES5, args.noise, seed=2,
+                                                        wavelet_scale_range=(0.8, 1.2))
+        split = run_split(gcase, world, rank, dist, dev, stream, max_over_ranks, prec)
+
     s4 = None
     if not args.no_state4d:
         try:
@@ -798,6 +863,7 @@ def run_own(args):
         "prior_fill": prior,
         "state4d": s4,
         "divide_by_scale_wavelet": div,
+        "split_grid": split,
         "profiling_pass_ms_per_step": ms_serial,
         "stages_ms": {"forward": st.ms_forward, "solve": st.ms_solve, "inverse": st.ms_inverse},
         "kernels": kernels,

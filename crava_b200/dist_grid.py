@@ -51,54 +51,76 @@ class Layout:
         return split_range(self.nyp, self.world, r)
 
 
-def _exchange(dist, sends, recvs, rank):
-    """Point-to-point all-to-all: sends[d] to rank d, recvs[s] from rank s
-    (the rank's own block is copied).  Works with the nccl and gloo
-    backends alike."""
-    reqs = []
-    for peer in range(len(sends)):
-        if peer == rank:
-            recvs[peer].copy_(sends[peer])
-            continue
-        reqs.append(dist.isend(sends[peer].contiguous(), peer))
-        reqs.append(dist.irecv(recvs[peer], peer))
-    for q in reqs:
-        q.wait()
+def _smooth(n: int) -> bool:
+    for f in (2, 3, 5, 7):
+        while n % f == 0:
+            n //= f
+    return n == 1
+
+
+def check_layout(lay: Layout):
+    """Every rank's slab (z planes) and column shard (ky rows) must be a
+    transform length the contexts plan (2, 3, 5, 7-smooth); raises
+    ValueError naming the first that is not."""
+    for r in range(lay.world):
+        nz = lay.z(r)[1] - lay.z(r)[0]
+        ny = lay.y(r)[1] - lay.y(r)[0]
+        if nz < 1 or ny < 1 or not _smooth(nz) or not _smooth(ny):
+            raise ValueError(f"rank {r}: slab of {nz} planes / shard of {ny} rows is not 2,3,5,7-smooth; "
+                             f"choose a rank count that splits nyp={lay.nyp} and nzp={lay.nzp} so")
 
 
 def to_columns(slab, lay: Layout, rank: int, dist):
     """z slab [nz_r, nyp, 2 cnxp] (float32, complex pairs after the xy
-    passes) -> column shard [nzp, ny_r, 2 cnxp] of this rank."""
+    passes) -> column shard [nzp, ny_r, 2 cnxp] of this rank.  Each source's
+    block lands directly in its z slice of the shard."""
     import torch
 
     z0, z1 = lay.z(rank)
     y0, y1 = lay.y(rank)
     assert tuple(slab.shape) == (z1 - z0, lay.nyp, 2 * lay.cnxp)
-    sends = [slab[:, lay.y(d)[0]:lay.y(d)[1], :].contiguous() for d in range(lay.world)]
-    recvs = [torch.empty((lay.z(s)[1] - lay.z(s)[0], y1 - y0, 2 * lay.cnxp), dtype=slab.dtype,
-                         device=slab.device) for s in range(lay.world)]
-    if dist is None:
-        recvs[0].copy_(sends[0])
-    else:
-        _exchange(dist, sends, recvs, rank)
-    return torch.cat(recvs, dim=0)
+    out = torch.empty((lay.nzp, y1 - y0, 2 * lay.cnxp), dtype=slab.dtype, device=slab.device)
+    out[z0:z1].copy_(slab[:, y0:y1, :])
+    if dist is not None and lay.world > 1:
+        reqs = []
+        for peer in range(lay.world):
+            if peer == rank:
+                continue
+            pz0, pz1 = lay.z(peer)
+            py0, py1 = lay.y(peer)
+            reqs.append(dist.isend(slab[:, py0:py1, :].contiguous(), peer))
+            reqs.append(dist.irecv(out[pz0:pz1], peer))  # a contiguous z slice
+        for q in reqs:
+            q.wait()
+    return out
 
 
-def to_slabs(cols, lay: Layout, rank: int, dist):
-    """Column shard [nzp, ny_r, 2 cnxp] -> z slab [nz_r, nyp, 2 cnxp]."""
+def to_slabs(cols, lay: Layout, rank: int, dist, out):
+    """Column shard [nzp, ny_r, 2 cnxp] -> this rank's z slab `out`
+    [nz_r, nyp, 2 cnxp]: each source's block is written into its ky rows."""
     import torch
 
     z0, z1 = lay.z(rank)
     y0, y1 = lay.y(rank)
     assert tuple(cols.shape) == (lay.nzp, y1 - y0, 2 * lay.cnxp)
-    sends = [cols[lay.z(d)[0]:lay.z(d)[1]].contiguous() for d in range(lay.world)]
-    recvs = [torch.empty((z1 - z0, lay.y(s)[1] - lay.y(s)[0], 2 * lay.cnxp), dtype=cols.dtype,
-                         device=cols.device) for s in range(lay.world)]
-    if dist is None:
-        recvs[0].copy_(sends[0])
-    else:
-        _exchange(dist, sends, recvs, rank)
-    return torch.cat(recvs, dim=1)
+    assert tuple(out.shape) == (z1 - z0, lay.nyp, 2 * lay.cnxp)
+    out[:, y0:y1, :].copy_(cols[z0:z1])
+    if dist is not None and lay.world > 1:
+        reqs, blocks = [], []
+        for peer in range(lay.world):
+            if peer == rank:
+                continue
+            pz0, pz1 = lay.z(peer)
+            py0, py1 = lay.y(peer)
+            b = torch.empty((z1 - z0, py1 - py0, 2 * lay.cnxp), dtype=cols.dtype, device=cols.device)
+            reqs.append(dist.isend(cols[pz0:pz1], peer))  # a contiguous z slice
+            reqs.append(dist.irecv(b, peer))
+            blocks.append((py0, py1, b))
+        for q in reqs:
+            q.wait()
+        for py0, py1, b in blocks:
+            out[:, py0:py1, :].copy_(b)
+    return out
 
 
 # grid types (FFTGrid::gridTypes, src/fftgrid.h:172)
@@ -134,7 +156,7 @@ def posterior_unit_split(ops, lay: Layout, rank: int, dist, mu, data, cov, err):
     ops.solve(cm, cd, cc, ce)
     for g, c, t in zip(grids[:-1], cols[:-1], types[:-1]):
         ops.fft_z(c, 1)
-        g.copy_(to_slabs(c, lay, rank, dist))
+        to_slabs(c, lay, rank, dist, g)
         ops.fft_xy(g, 1, t)
 
 

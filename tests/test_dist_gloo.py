@@ -245,3 +245,11 @@ def test_loglik_over_split_grid_sums_the_shards():
         assert np.isclose(L2, L, rtol=1e-6) and nf2 == nf
         assert np.allclose(gs2, gs, rtol=1e-6) and np.allclose(gv2, gv, rtol=1e-5, atol=1e-6)
         assert np.allclose(gw2, gw, rtol=1e-5, atol=1e-5)
+
+
+def test_split_layout_check():
+    from crava_b200 import dist_grid as G
+    G.check_layout(G.Layout(256, 256, 512, 2))
+    G.check_layout(G.Layout(256, 256, 512, 4))
+    with pytest.raises(ValueError):
+        G.check_layout(G.Layout(256, 256, 512, 3))  # 86 / 85 rows
