@@ -1,0 +1,136 @@
+"""Analytic checks of the per-bin solve and the per-output accuracy report.
+
+* closed form: on sampled bins, an independent float64 numpy statement of
+  the Bayesian update (K = diag(D conj W) A, prior S = |Re c / S0| S0, the
+  noise covariance of getNextErrorVariance, M = K S K^H + N,
+  mu_post = mu + (K S)^H M^-1 (d - K mu), S_post = S - (K S)^H M^-1 K S,
+  r = d - K mu_post; src/crava.cpp:1085-1151) against the device's FP64
+  form;
+* Hermitian symmetry: the output spectra of real fields on the kx = 0
+  plane satisfy X(-ky, -kz) = conj X(ky, kz);
+* Loewner order: S - S_post is positive semi-definite on every sampled bin;
+* accuracy report: per output (3 means, ntheta residuals, 6 covariances)
+  the relative L2 error and max-abs / max-ref of the FP64, mixed and FP32
+  forms against the FP64 oracle, at the small plain case and its high-SNR
+  (1 % noise) variant; printed with ``pytest -s``.
+"""
+import numpy as np
+import pytest
+
+from crava_b200 import api, synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PAIRS = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+
+
+def _run(case, prec):
+    sp = O.forward_spectra(case, "orc")
+    ctx = api.Context(case)
+    ctx.set_kz_tables(O.kz_tables(case, "orc"))
+    d = lambda gs: [api.to_device(g) for g in gs]
+    mu, data, cov, err = d(sp["mu"]), d(sp["data"]), d(sp["cov"]), d([sp["err"]])[0]
+    ctx.posterior(mu, data, cov, err, prec)
+    cv = lambda g: api.complex_view(g.cpu().numpy(), case.nxp).astype(np.complex128)
+    return ctx, sp, [cv(g) for g in mu], [cv(g) for g in data], [cv(g) for g in cov]
+
+
+def _prior(case, sp, k, j, i):
+    """getNextParameterCovariance (src/seismicparametersholder.cpp:355-427)."""
+    c = lambda g: O.complex_view(g, case.nxp)[k, j, i].astype(np.complex128)
+    S = np.zeros((3, 3), complex)
+    for t, (p, q) in enumerate(PAIRS):
+        s0 = case.var0[p, q]
+        S[p, q] = S[q, p] = abs(c(sp["cov"][t]).real / s0) * s0 if s0 != 0 else abs(c(sp["cov"][t]).real)
+    return S
+
+
+def _closed_form(tables, case, sp, k, j, i):
+    c = lambda g: O.complex_view(g, case.nxp)[k, j, i].astype(np.complex128)
+    wd, e1, e2, e3, inv = tables
+    mu = np.array([c(g) for g in sp["mu"]])
+    d = np.array([c(g) for g in sp["data"]])
+    S = _prior(case, sp, k, j, i)
+    if not inv[k]:
+        return mu, d, S, False
+    K = wd[k].astype(np.complex128)[:, None] * case.A.astype(np.float64)
+    lam = abs(c(sp["err"]).real)
+    th = case.theta_cov
+    wnc = np.float64(np.float32(case.wnc))
+    e1k, e2k, e3k = e1[k].astype(np.complex128), e2[k].astype(np.complex128), e3[k].astype(np.float64)
+    N = 0.5 * (1.0 - wnc) * th * lam * (np.outer(e1k, e1k.conj()) + np.outer(e2k, e2k.conj()))
+    N = N + np.diag(np.diag(th) * wnc * e3k ** 2)
+    KS = K @ S
+    M = KS @ K.conj().T + N
+    X = np.linalg.solve(M, KS)
+    mu_p = mu + X.conj().T @ (d - K @ mu)
+    S_p = S - KS.conj().T @ X
+    r = d - K @ mu_p
+    return mu_p, r, S_p, True
+
+
+@pytest.mark.parametrize("noise", [0.1, 0.01])
+def test_closed_form_hermitian_and_loewner(noise):
+    case = synth.make_case(24, 20, 64, (0.0, 10.0, 20.0, 30.0, 40.0), noise, seed=21)
+    ctx, sp, mu, res, cov = _run(case, api.FP64)
+    tables = ctx.kz_tables()
+    rng = np.random.default_rng(4)
+    cn = case.nxp // 2 + 1
+    n_inv = 0
+    for _ in range(400):
+        k, j, i = int(rng.integers(case.nzp)), int(rng.integers(case.nyp)), int(rng.integers(cn))
+        mu_p, r, S_p, inverted = _closed_form(tables, case, sp, k, j, i)
+        got_mu = np.array([g[k, j, i] for g in mu])
+        got_r = np.array([g[k, j, i] for g in res])
+        got_S = np.zeros((3, 3), complex)
+        for t, (p, q) in enumerate(PAIRS):
+            got_S[p, q] = cov[t][k, j, i]
+            got_S[q, p] = np.conj(cov[t][k, j, i])
+        assert np.abs(got_mu - mu_p).max() <= 1e-5 * np.abs(mu_p).max() + 1e-7
+        assert np.abs(got_r - r).max() <= 1e-5 * max(np.abs(r).max(), np.abs(got_r).max(), 1e-6) + 1e-7
+        assert np.abs(got_S - S_p).max() <= 1e-5 * max(np.abs(S_p).max(), 1e-30)
+        if inverted:
+            n_inv += 1
+            # the prior minus the posterior covariance is positive semi-definite
+            S = _prior(case, sp, k, j, i)
+            ev = np.linalg.eigvalsh(S - got_S)
+            assert ev.min() >= -1e-5 * max(np.abs(S).max(), 1e-30), ev
+    assert n_inv > 50
+    # Hermitian symmetry of the output spectra on the kx = 0 plane
+    for g in mu + res + cov:
+        p0 = g[:, :, 0]
+        mirror = np.conj(p0[(-np.arange(case.nzp)) % case.nzp][:, (-np.arange(case.nyp)) % case.nyp])
+        assert np.abs(p0 - mirror).max() <= 1e-6 * max(np.abs(p0).max(), 1e-30)
+
+
+def _report(case, label):
+    sp = O.forward_spectra(case, "orc")
+    dmu, dres, dcov, _ = O.posterior_fp64(case, sp)
+    ref = dmu + dres + dcov
+    names = ["mu_alpha", "mu_beta", "mu_rho"] + [f"resid_{l}" for l in range(case.ntheta)] + \
+            ["cov_aa", "cov_bb", "cov_rr", "cov_ab", "cov_ar", "cov_br"]
+    rows = {}
+    for prec, tag in [(api.FP64, "fp64"), (api.MIXED, "mixed"), (api.FP32, "fp32")]:
+        _, _, mu, res, cov = _run(case, prec)
+        for name, a, b in zip(names, mu + res + cov, ref):
+            rl2 = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+            ma = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+            rows.setdefault(name, {})[tag] = (rl2, ma)
+    print(f"\n{label}: per-output error against the FP64 oracle (rel L2 / max-abs over max-ref)")
+    print(f"{'output':10s} {'fp64':>22s} {'mixed':>22s} {'fp32':>22s}")
+    for name in names:
+        cells = "".join(f" {rows[name][t][0]:10.2e}/{rows[name][t][1]:9.2e}" for t in ("fp64", "mixed", "fp32"))
+        print(f"{name:10s}{cells}")
+    return rows
+
+
+@pytest.mark.parametrize("noise,label", [(0.10, "64x64x128, 3 angles, 10 % noise"),
+                                         (0.01, "64x64x128, 3 angles, 1 % noise (high SNR)")])
+def test_accuracy_report(noise, label):
+    case = synth.make_case(64, 64, 128, (10.0, 20.0, 30.0), noise, seed=1)
+    rows = _report(case, label)
+    for name, r in rows.items():
+        assert r["fp64"][0] < 1e-6, (name, r)
+        assert r["mixed"][0] < 1e-5, (name, r)
+        assert r["fp32"][0] < 1e-2, (name, r)  # reported; the FP32 form is checked bit for bit elsewhere
