@@ -2,8 +2,11 @@
 
 The inversion hot path shards by independent units -- posterior units of
 different cases or time-lapse vintages, and posterior realisations -- so
-ranks exchange nothing on the data path.  The only collectives are the
-barrier around a timed region and the max-over-ranks of its duration.
+ranks running independent units exchange nothing on the data path: the
+only collectives are the barrier around a timed region and the
+max-over-ranks of its duration.  One grid too large for a GPU is split
+over the ranks by dist_grid.py, whose exchange is the one data-path
+communication.
 """
 from __future__ import annotations
 
