@@ -14,9 +14,17 @@ written out of place so each step reads pristine inputs; device time with
 CUDA events over K steps, max over ranks.  `e2e` runs the same unit through
 crava_gpu_posterior_unit_host with pinned host buffers (copies timed).
 Reference arm: the reference's own CPU code (FFTW 2.1.2 + lib_matr.c,
-oracle/_ref) on the host cores, on a bounded sample of the same unit.
+oracle/_ref) on the host cores: forked processes, each timing whole units
+of the same workload; value = units x cells / wall time of the timed phase.
 Multi-GPU (torchrun): every rank runs its own independent unit (weak
 scaling, no collective on the data path).
+
+  python bench.py --profile-unit NX,NY,NZ [--profile-precision 0|1|2]
+                  [--profile-fused 0|1] [--profile-reps R] [--profile-ntheta NT]
+
+runs the out-of-place unit R times on a seeded case and prints per-kernel
+device times (CUDA events around every launch); used for ncu captures of
+single kernel families on small cases.
 """
 from __future__ import annotations
 
@@ -35,6 +43,19 @@ sys.path.insert(0, ROOT)
 
 METRIC = "posterior cells/s at 256x256x512x5 angles, mixed vs FP64 form; % HBM roofline"
 ANGLES5 = (0.0, 10.0, 20.0, 30.0, 40.0)
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json
+    (written per pod by the driver), else the pool's earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        pass
+    return 6650.0, "fallback 6650 GB/s"
 
 
 def parse():
@@ -63,63 +84,44 @@ def parse():
     ap.add_argument("--no-split-grid", action="store_true")
     ap.add_argument("--batch-sims", type=int, default=64)
     ap.add_argument("--workers", type=int, default=0, help="reference arm processes (0 = auto)")
+    ap.add_argument("--profile-unit", default=None, metavar="NX,NY,NZ",
+                    help="per-kernel timing of the unit on a small case (for ncu captures), then exit")
+    ap.add_argument("--profile-precision", type=int, default=0, help="0 FP64, 1 mixed, 2 reference FP32")
+    ap.add_argument("--profile-fused", type=int, default=0)
+    ap.add_argument("--profile-reps", type=int, default=3)
+    ap.add_argument("--profile-ntheta", type=int, default=5)
     return ap.parse_args()
 
 
-# ----------------------------------------------------------------- CPU sample
-_SAMPLE_INPUTS = {}
-
-
-def cpu_sample_unit(nxp, nyp, nzp, nt, which="ref", seed=0):
-    """Times the reference CPU path on a bounded sample of one unit and
-    returns (seconds per unit, description).  The sample: one forward
-    transform of a DATA grid, one of a COVARIANCE grid and one inverse
-    transform at the full grid size (FFTW 2.1.2 with its per-call plan, as
-    FFTGrid does), and the per-bin solve on a 64x64xnzp case with the same
-    angles and kz band, scaled per bin.  Unit time = (3+nt) r2c(scaled)
-    + 7 r2c(covariance) + (9+nt) c2r + solve * csize_full / csize_sample."""
-    import numpy as np
-
-    from crava_b200 import synth
+# ----------------------------------------------------------------- CPU reference unit
+def cpu_unit_seconds(case, which="ref"):
+    """One whole posterior unit of the reference's CPU path on this core:
+    29 FFTW 2.1.2 transforms, each planned per call as FFTGrid does
+    (src/fftgrid.cpp:1822-1825), and the per-bin loop with lib_matr.c
+    (src/crava.cpp:1042-1151) -- oracle/_ref, or the restatement when the
+    reference build is absent.  Returns (seconds, failed bins)."""
     from oracle import oracle as O
 
-    key = (nxp, nyp, nzp, nt, seed)
-    if key not in _SAMPLE_INPUTS:  # inputs are made once per process; only the timed calls repeat
-        rng = np.random.default_rng(seed)
-        rnxp = 2 * (nxp // 2 + 1)
-        g = rng.standard_normal((nzp, nyp, rnxp)).astype(np.float32)
-        small = synth.make_case(64, 64, nzp, ANGLES5[:nt] if nt <= 5 else tuple(range(nt)), 0.10, seed + 7)
+    t0 = time.perf_counter()
+    out = O.unit_fp32(case, which)
+    return time.perf_counter() - t0, out[3]
 
-        # spectra with the reference scalings; numpy keeps the set-up short
-        def spec(x, scale):
-            c = np.fft.rfftn(x[..., :64].astype(np.float64), axes=(0, 1, 2)) * scale
-            out = np.zeros(x.shape, np.float32)
-            out.view(np.complex64)[...] = c.astype(np.complex64)
-            return out
-        s = 1.0 / math.sqrt(64 * 64 * nzp)
-        sp = {"mu": [spec(x, s) for x in small.mu], "data": [spec(x, s) for x in small.data],
-              "cov": [spec(x, 1.0) for x in small.cov], "err": spec(small.err_corr, 1.0)}
-        _SAMPLE_INPUTS[key] = (g, small, sp)
-    g, small, sp = _SAMPLE_INPUTS[key]
-    t0 = time.perf_counter(); a = O.fft_r2c(g, nxp, nyp, nzp, 1, which); t_r2c = time.perf_counter() - t0
-    t0 = time.perf_counter(); O.fft_r2c(g, nxp, nyp, nzp, 3, which); t_r2c_cov = time.perf_counter() - t0
-    t0 = time.perf_counter(); O.fft_c2r(a, nxp, nyp, nzp, 1, which); t_c2r = time.perf_counter() - t0
-    del a
-    t0 = time.perf_counter(); O.posterior_fp32(small, sp, which); t_solve = time.perf_counter() - t0
-    csize_full = (nxp // 2 + 1) * nyp * nzp
-    csize_small = 33 * 64 * nzp
-    t_unit = ((3 + nt) * t_r2c + 7 * t_r2c_cov + (9 + nt) * t_c2r
-              + t_solve * csize_full / csize_small)
-    desc = (f"one r2c (DATA), one r2c (COVARIANCE), one c2r at {nxp}x{nyp}x{nzp} "
-            f"({t_r2c:.2f}/{t_r2c_cov:.2f}/{t_c2r:.2f} s) and the per-bin solve on a 64x64x{nzp}x{nt} "
-            f"case ({t_solve:.2f} s), scaled to one unit: {t_unit:.1f} s")
-    return t_unit, desc
+
+_REF_CASE = None
+_REF_BARRIER = None
 
 
 def _ref_worker(args):
-    nxp, nyp, nzp, nt, which, seed = args
-    t, _ = cpu_sample_unit(nxp, nyp, nzp, nt, which, seed)
-    return t
+    """One reference-arm process: `warm` untimed units, then `units` timed
+    units on the case inherited from the parent (fork).  Returns the timed
+    seconds and the wall-clock span of the timed phase."""
+    warm, units = args
+    for _ in range(warm):
+        cpu_unit_seconds(_REF_CASE)
+    _REF_BARRIER.wait(timeout=900)  # every process starts its timed units together
+    t0 = time.time()
+    per = [cpu_unit_seconds(_REF_CASE)[0] for _ in range(units)]
+    return per, t0, time.time()
 
 
 # ----------------------------------------------------------------- clocks
@@ -766,23 +768,13 @@ def run_own(args):
 
     s4 = None
     if not args.no_state4d:
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                hbm_peak = json.load(f).get("hbm_gbs") or 6650.0
-        except Exception:
-            hbm_peak = 6650.0
         torch.cuda.nvtx.range_push("state4d")  # ncu --nvtx --nvtx-include "state4d/"
-        s4 = run_state4d(ctx, case, dev, stream, max_over_ranks, hbm_peak)
+        s4 = run_state4d(ctx, case, dev, stream, max_over_ranks, hbm_peak()[0])
         torch.cuda.nvtx.range_pop()
     div = None
     if not args.no_divide:
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                hbm_peak = json.load(f).get("hbm_gbs") or 6650.0
-        except Exception:
-            hbm_peak = 6650.0
         torch.cuda.nvtx.range_push("divide")  # ncu --nvtx --nvtx-include "divide/"
-        div = run_divide(ctx, case, src, dev, stream, max_over_ranks, hbm_peak)
+        div = run_divide(ctx, case, src, dev, stream, max_over_ranks, hbm_peak()[0])
         torch.cuda.nvtx.range_pop()
 
     fwd = None
@@ -799,32 +791,33 @@ def run_own(args):
                           max_over_ranks)
 
     roof = None
+    peak, peak_source = hbm_peak()
+    gbytes = case.mu[0].nbytes
+    csize = (nxp // 2 + 1) * nyp * nzp
     if prof:
         name, (n, tot, bpl) = max(prof.items(), key=lambda kv: kv[1][1])
-        peaks = {}
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                peaks = json.load(f)
-        except Exception:
-            pass
-        peak = peaks.get("hbm_gbs") or 6650.0
-        achieved = bpl / (tot / n * 1e-3) / 1e9
-        traffic = None
-        try:  # DRAM bytes per launch from the committed ncu launch-list summary
-            import re
-            key = f"{nxp}x{nyp}x{nzp}"
-            with open(os.path.join(ROOT, "profiles", f"launches_posterior_unit_{key}x{nt}.md")) as f:
-                for line in f:
-                    m = re.match(r"traffic_per_launch (\S+) (\S+) ([0-9.eE+]+)", line)
-                    if m and m.group(1) == name and m.group(2) == key:
-                        traffic = float(m.group(3))
-        except Exception:
-            pass
-        roof = {"bound": "hbm", "kernel": name, "measured": "profiling pass, one stream, CUDA events per launch", "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback",
-                "bytes_per_launch": bpl, "launches": n, "avg_ms": round(tot / n, 5),
+        avg_s = tot / n * 1e-3
+        # algorithmic bytes per launch: the solve moves (19 + 2 nt) complex
+        # values per bin (every spectrum read and written once); a
+        # transform pass one read and one write of its grid
+        alg = (19 + 2 * nt) * csize * 8 if name.startswith("posterior_solve") else bpl
+        achieved = alg / avg_s / 1e9
+        roof = {"bound": "hbm", "kernel": name,
+                "measured": "profiling pass, one stream, CUDA events per launch",
+                "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "traffic_note": "DRAM bytes are not measured inside the bench (no ncu); the ncu figure "
+                                "per launch is in profiles/",
+                "peak_source": peak_source, "algorithmic_bytes_per_launch": alg,
+                "moved_bytes_per_launch": bpl,
+                "moved_frac": round(bpl / avg_s / 1e9 / peak, 4),
+                "launches": n, "avg_ms": round(tot / n, 5),
                 "share": round(tot / sum(v[1] for v in prof.values()), 4)}
+    # the whole unit against its algorithmic bytes B_unit = 3 (19 + 2 nt) G
+    b_unit = 3 * (19 + 2 * nt) * gbytes
+    unit_roof = {"bound": "hbm", "algorithmic_bytes": b_unit, "ms": round(ms, 4),
+                 "achieved": round(b_unit / (ms * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                 "frac": round(b_unit / (ms * 1e-3) / 1e9 / peak, 4), "peak_source": peak_source}
     kernels = {k: {"launches": v[0], "ms": round(v[1], 4),
                    "GB/s": round(v[2] / (v[1] / v[0] * 1e-3) / 1e9, 1)} for k, v in prof.items()}
 
@@ -833,9 +826,13 @@ def run_own(args):
         try:
             from oracle import oracle as O
             which = "ref" if O.have_ref() else "orc"
-            t_unit, desc = cpu_sample_unit(nxp, nyp, nzp, nt, which)
+            t_unit, fails = cpu_unit_seconds(case, which)
             cpu = {"value": cells / t_unit, "unit": "cells/s", "cores": 1,
-                   "kind": "reference" if which == "ref" else "port", "sample": desc}
+                   "kind": "reference" if which == "ref" else "port",
+                   "sample": f"one whole posterior unit {nxp}x{nyp}x{nzp}x{nt} on this case (29 FFTW 2.1.2 "
+                             f"transforms planned per call, the per-bin loop with lib_matr.c), "
+                             f"timed once: {t_unit:.1f} s",
+                   "seconds_per_unit": t_unit, "chol_fail_bins": fails}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "cells/s", "cores": 1, "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -858,6 +855,7 @@ def run_own(args):
                 "sync_ms_per_step": e2e_sync},
         "gpu_launches": launches,
         "roofline": roof,
+        "unit_roofline": unit_roof,
         "cpu_baseline": cpu,
         "clocks": clk,
         "fp64_form_value": fp64_value,
@@ -885,6 +883,13 @@ def run_own(args):
 
 # ----------------------------------------------------------------- reference arm
 def run_reference(args):
+    """The reference's own CPU path (oracle/_ref: FFTW 2.1.2 + lib_matr.c in
+    the restated loop) on the host cores.  The case is built once, then P
+    processes forked from this one (no GPU is touched here) each run one
+    untimed unit and ceil(K / P) timed whole units, starting their timed
+    units together.  value = timed units x cells / the wall-clock span of
+    the timed phase (first start to last end)."""
+    global _REF_CASE, _REF_BARRIER
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -893,32 +898,44 @@ def run_reference(args):
 
     nxp, nyp, nzp = (int(x) for x in args.grid.split(","))
     nt = 5
-    which = "ref" if O.have_ref() else "orc"
-    if which != "ref":
+    if not O.have_ref():
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref (the reference's FFTW 2.1.2 + lib_matr.c build) is missing"}))
         return
     import multiprocessing as mp
 
-    ncpu = os.cpu_count() or 1
-    workers = args.workers or max(1, min(ncpu, 16))
-    ctxm = mp.get_context("spawn")
+    from crava_b200 import synth
+
+    _REF_CASE = synth.make_case(nxp, nyp, nzp, ANGLES5, args.noise, seed=2, wavelet_scale_range=(0.8, 1.2))
+    ncpu = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    # each process holds a copy of the unit's grids while it runs
+    unit_bytes = 2 * len(_REF_CASE.grids()) * _REF_CASE.mu[0].nbytes
+    try:
+        import psutil
+        by_mem = max(1, int(psutil.virtual_memory().available * 0.7 // unit_bytes))
+    except Exception:
+        by_mem = ncpu
+    workers = args.workers or max(1, min(ncpu, 16, by_mem))
+    units = max(1, -(-args.steps // workers))
+    ctxm = mp.get_context("fork")
+    _REF_BARRIER = ctxm.Barrier(workers)
+    t_wall0 = time.perf_counter()
     with ctxm.Pool(workers) as pool:
-        for w in range(args.warmup):
-            pool.map(_ref_worker, [(nxp, nyp, nzp, nt, which, 100 + i) for i in range(workers)])
-        per_step = []
-        t_start = time.perf_counter()
-        for s in range(args.steps):
-            ts = pool.map(_ref_worker, [(nxp, nyp, nzp, nt, which, 200 + i) for i in range(workers)])
-            per_step.append(sum(nxp * nyp * nzp / t for t in ts))
-        wall = time.perf_counter() - t_start
-    value = statistics.median(per_step)
-    _, desc = (None, f"each of {workers} processes times the reference CPU path (FFTW 2.1.2 + lib_matr.c) "
-                     f"on a bounded sample of one {nxp}x{nyp}x{nzp}x{nt} unit: one forward DATA, one "
-                     f"forward COVARIANCE and one inverse transform at full size plus the per-bin solve "
-                     f"on a 64x64x{nzp} case, scaled to the unit; value = sum over processes")
+        res = pool.map(_ref_worker, [(min(1, args.warmup), units)] * workers, chunksize=1)
+    wall_total = time.perf_counter() - t_wall0
+    late = max(t0 for _, t0, _ in res) - min(t0 for _, t0, _ in res)
+    span = max(t1 for _, _, t1 in res) - min(t0 for _, t0, _ in res)
+    n_units = sum(len(per) for per, _, _ in res)
+    cells = nxp * nyp * nzp
+    value = n_units * cells / span
+    per_unit = [t for per, _, _ in res for t in per]
+    desc = (f"{workers} processes forked after the case was built, each one untimed and {units} timed "
+            f"whole {nxp}x{nyp}x{nzp}x{nt} units (29 FFTW 2.1.2 transforms planned per call, the "
+            f"per-bin loop with lib_matr.c); {n_units} units in {span:.1f} s wall, "
+            f"{statistics.median(per_unit):.1f} s per unit per process (median)")
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": nxp * nyp * nzp / value * 1e3,
+           "steps": args.steps, "units_timed": n_units, "warmup": args.warmup,
+           "ms_per_step": span / n_units * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic", "config": {"workload": f"posterior unit {nxp}x{nyp}x{nzp}, 5 angles",
                                            "grid": [nxp, nyp, nzp], "ntheta": nt,
@@ -926,13 +943,41 @@ def run_reference(args):
            "cpu_baseline": {"value": value, "unit": "cells/s", "cores": workers, "kind": "reference",
                             "sample": desc},
            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-           "wall_s": wall}
+           "seconds_per_unit_per_process": statistics.median(per_unit),
+           "start_skew_s": round(late, 3), "wall_s": round(wall_total, 1)}
     print(json.dumps(out), flush=True)
+
+
+def run_profile_unit(args):
+    """Per-kernel device times of the out-of-place unit on a seeded case
+    (CUDA events around every launch of the context)."""
+    from crava_b200 import api, synth
+
+    nx, ny, nz = (int(v) for v in args.profile_unit.split(","))
+    nt = args.profile_ntheta
+    case = synth.make_case(nx, ny, nz, tuple(10.0 * i for i in range(nt)), 0.1, seed=2)
+    ctx = api.Context(case)
+    ctx.set_fused(bool(args.profile_fused))
+    d = lambda gs: [api.to_device(g) for g in gs]
+    src = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
+    dst = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
+    ctx.set_profiling(True)
+    for _ in range(args.profile_reps):
+        ctx.posterior_unit_oop(src, dst, args.profile_precision)
+        st = ctx.stats()
+        print("forward %.3f solve %.3f inverse %.3f total %.3f ms" % (
+            st.ms_forward, st.ms_solve, st.ms_inverse, st.ms_total))
+    for k, v in ctx.profile().items():
+        per = v[1] / v[0]
+        print(f"{k:18s} launches {v[0]:4d}  {per:.4f} ms/launch  {v[2] / (per * 1e-3) / 1e9:8.1f} GB/s")
+    ctx.close()
 
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.profile_unit:
+        run_profile_unit(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_own(args)

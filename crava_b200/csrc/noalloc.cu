@@ -16,7 +16,12 @@
 //
 // Set-up: the first call on a device, with that device current, resolves
 // the array's device address with cudaGetSymbolAddress and caches it for
-// that device.  Make that first call before any stream capture.
+// that device.  Make that first call before any stream capture.  The cached
+// address belongs to the device's current primary context: after
+// cudaDeviceReset (or anything else that destroys and re-creates the
+// primary context) the array is re-created elsewhere and the cached address
+// is stale: a process that resets a device must not call this entry point
+// on that device again.
 // Sharing: every call on a device uses the same array and the array keeps
 // the last call's contents; each call rewrites the tables and clears the
 // counters before use.  Calls whose work overlaps on the GPU (different
@@ -90,6 +95,9 @@ extern "C" int crava_gpu_posterior_noalloc(const crava_gpu_params *p, const crav
                                            int precision, void *stream, crava_gpu_stats *stats) {
   if (!p || !g || !p->wavelet || !p->A || !p->theta_cov || !p->var0) return CRAVA_GPU_ERR_ARG;
   if (p->nxp < 2 || p->nyp < 1 || p->nzp < 2 || !smooth_2357(p->nzp)) return CRAVA_GPU_ERR_ARG;
+  // the bounds of crava_gpu_create: they also keep the solve's grid of
+  // ceil((nxp/2+1) nyp / 256) * nzp blocks below 2^31
+  if (p->nxp > 8192 || p->nyp > 4096) return CRAVA_GPU_ERR_ARG;
   if (p->ntheta < 1 || p->ntheta > CRAVA_GPU_MAX_THETA || p->nz < 1 || !(p->lz > 0.0)) return CRAVA_GPU_ERR_ARG;
   if (precision < CRAVA_SOLVE_FP64 || precision > CRAVA_SOLVE_FP32) return CRAVA_GPU_ERR_ARG;
   if (p->thickness_mode != 0 && p->thickness_mode != 1) return CRAVA_GPU_ERR_ARG;

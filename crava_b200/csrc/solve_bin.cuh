@@ -44,17 +44,20 @@ __device__ __forceinline__ void prior_f(const float2 c6[6], const double v[6], f
 }
 
 // Hermitian Cholesky M = L L^H on the lower triangle (tri() indexing), with
-// the reference's failure rules applied to M / M00.  The reciprocals of the
-// diagonal of L are returned in rd (one division per column, reused by the
-// substitutions).
+// the reference's failure rules applied to M / M00 (libs/lib/lib_matr.c:
+// 103-105, 114, 145): M00 <= 0, or a diagonal entry or pivot of M / M00 <=
+// 1e-20, fails.  The comparisons are the reference's (<=), so a NaN in M
+// does not fail: it flows into the outputs as it does there.  The
+// reciprocals of the diagonal of L are returned in rd (one division per
+// column, reused by the substitutions).
 template <int NT, typename T2, typename T, typename LA>
 __device__ __forceinline__ bool cholesky(LA L, T *rd) {
   const T factor = L[0].x;
-  if (!(factor > T(0))) return false;
+  if (factor <= T(0)) return false;
   const T tol = (T)kTol * factor;
 #pragma unroll
   for (int i = 0; i < NT; ++i) {
-    if (!(L[tri(i, i)].x > tol)) return false;
+    if (L[tri(i, i)].x <= tol) return false;
 #pragma unroll
     for (int j = 0; j < i; ++j) {
       T2 s = L[tri(i, j)];
@@ -70,7 +73,7 @@ __device__ __forceinline__ bool cholesky(LA L, T *rd) {
     T d = L[tri(i, i)].x;
 #pragma unroll
     for (int k = 0; k < i; ++k) d -= L[tri(i, k)].x * L[tri(i, k)].x + L[tri(i, k)].y * L[tri(i, k)].y;
-    if (!(d > tol)) return false;
+    if (d <= tol) return false;
     // one reciprocal square root gives both the pivot and its reciprocal
     const T r = rsqrt(d);
     L[tri(i, i)].x = d * r;

@@ -70,6 +70,48 @@ def check_layout(lay: Layout):
                              f"choose a rank count that splits nyp={lay.nyp} and nzp={lay.nzp} so")
 
 
+def exchange_plan(lay: Layout, rank: int, direction: str):
+    """The point-to-point operations of one exchange on this rank, in the
+    order they are posted: a list of (kind, peer, z range, y range) with
+    kind "send" or "recv".
+
+    direction "to_columns": this rank sends rows [py0, py1) of its z slab to
+    each peer and receives the peer's planes [pz0, pz1) of its own rows;
+    "to_slabs" is the reverse.  The list depends on the layout and the rank
+    only (never on the backend), so NCCL and gloo post the same operations;
+    every send of rank r to p has the shape of p's receive from r."""
+    z0, z1 = lay.z(rank)
+    y0, y1 = lay.y(rank)
+    ops = []
+    for peer in range(lay.world):
+        if peer == rank:
+            continue
+        pz0, pz1 = lay.z(peer)
+        py0, py1 = lay.y(peer)
+        if direction == "to_columns":
+            ops.append(("send", peer, (z0, z1), (py0, py1)))
+            ops.append(("recv", peer, (pz0, pz1), (y0, y1)))
+        elif direction == "to_slabs":
+            ops.append(("send", peer, (pz0, pz1), (y0, y1)))
+            ops.append(("recv", peer, (z0, z1), (py0, py1)))
+        else:
+            raise ValueError(direction)
+    return ops
+
+
+def _post(dist, p2p):
+    """Posts one exchange as a single group (dist.batch_isend_irecv) and
+    waits for it.  Grouping lets NCCL match every rank's sends and receives
+    together: posting them one by one in the same order on every rank
+    deadlocks once a send is larger than NCCL's eager buffer (each rank's
+    send waits for a receive queued behind the peer's own send)."""
+    if not p2p:
+        return
+    ops = [dist.P2POp(dist.isend if kind == "send" else dist.irecv, t, peer) for kind, peer, t in p2p]
+    for w in dist.batch_isend_irecv(ops):
+        w.wait()
+
+
 def to_columns(slab, lay: Layout, rank: int, dist):
     """z slab [nz_r, nyp, 2 cnxp] (float32, complex pairs after the xy
     passes) -> column shard [nzp, ny_r, 2 cnxp] of this rank.  Each source's
@@ -82,16 +124,13 @@ def to_columns(slab, lay: Layout, rank: int, dist):
     out = torch.empty((lay.nzp, y1 - y0, 2 * lay.cnxp), dtype=slab.dtype, device=slab.device)
     out[z0:z1].copy_(slab[:, y0:y1, :])
     if dist is not None and lay.world > 1:
-        reqs = []
-        for peer in range(lay.world):
-            if peer == rank:
-                continue
-            pz0, pz1 = lay.z(peer)
-            py0, py1 = lay.y(peer)
-            reqs.append(dist.isend(slab[:, py0:py1, :].contiguous(), peer))
-            reqs.append(dist.irecv(out[pz0:pz1], peer))  # a contiguous z slice
-        for q in reqs:
-            q.wait()
+        p2p = []
+        for kind, peer, (a, b), (c, d) in exchange_plan(lay, rank, "to_columns"):
+            if kind == "send":
+                p2p.append((kind, peer, slab[:, c:d, :].contiguous()))
+            else:
+                p2p.append((kind, peer, out[a:b]))  # a contiguous z slice
+        _post(dist, p2p)
     return out
 
 
@@ -106,20 +145,17 @@ def to_slabs(cols, lay: Layout, rank: int, dist, out):
     assert tuple(out.shape) == (z1 - z0, lay.nyp, 2 * lay.cnxp)
     out[:, y0:y1, :].copy_(cols[z0:z1])
     if dist is not None and lay.world > 1:
-        reqs, blocks = [], []
-        for peer in range(lay.world):
-            if peer == rank:
-                continue
-            pz0, pz1 = lay.z(peer)
-            py0, py1 = lay.y(peer)
-            b = torch.empty((z1 - z0, py1 - py0, 2 * lay.cnxp), dtype=cols.dtype, device=cols.device)
-            reqs.append(dist.isend(cols[pz0:pz1], peer))  # a contiguous z slice
-            reqs.append(dist.irecv(b, peer))
-            blocks.append((py0, py1, b))
-        for q in reqs:
-            q.wait()
-        for py0, py1, b in blocks:
-            out[:, py0:py1, :].copy_(b)
+        p2p, blocks = [], []
+        for kind, peer, (a, b), (c, d) in exchange_plan(lay, rank, "to_slabs"):
+            if kind == "send":
+                p2p.append((kind, peer, cols[a:b]))  # a contiguous z slice
+            else:
+                blk = torch.empty((b - a, d - c, 2 * lay.cnxp), dtype=cols.dtype, device=cols.device)
+                p2p.append((kind, peer, blk))
+                blocks.append((c, d, blk))
+        _post(dist, p2p)
+        for c, d, blk in blocks:
+            out[:, c:d, :].copy_(blk)
     return out
 
 

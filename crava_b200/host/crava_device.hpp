@@ -35,14 +35,37 @@ inline void check(int status, const char *what) {
   if (status != CRAVA_GPU_OK) throw Error(what, status);
 }
 
+// FFTW 2.1.2's complex element (libs/fft/include/fftw.h:58): what the
+// reference's getNextComplex / setNextComplex pass.
+struct fftw_complex {
+  float re, im;
+};
+
 // A padded grid resident in HBM (layout of src/fftgrid.cpp:37-67).
+//
+// The reference reads and writes grids element by element through stateful
+// cursors (getNextReal / setNextReal / getNextComplex / setNextComplex,
+// src/fftgrid.cpp:1418-1431, 1603-1617) bracketed by setAccessMode /
+// endAccess (src/fftgrid.h:168-173; FFTFileGrid, src/fftfilegrid.cpp:104-150,
+// is the precedent for a grid whose values live elsewhere).  Here the values
+// live in HBM, so the cursors work on a host mirror: setAccessMode(READ,
+// READANDWRITE or RANDOMACCESS) downloads the grid into the mirror,
+// endAccess() uploads it back after WRITE, READANDWRITE or a modified
+// RANDOMACCESS, and the cursors walk the mirror in the reference's linear
+// order (x fastest, then y, then z; rnxp reals or cnxp complex per row),
+// wrapping to the start after the last element as the reference does.
+// Copies are ordered on `stream` (the stream of the context's work) and
+// wait for that stream only.
 class FFTGridDevice {
  public:
   // FFTGrid::gridTypes (src/fftgrid.h:172)
   enum gridTypes { CTMISSING, DATA, PARAMETER, COVARIANCE };
+  // FFTGrid::accessMode (src/fftgrid.h:168)
+  enum accessMode { NONE, READ, WRITE, READANDWRITE, RANDOMACCESS };
 
-  FFTGridDevice(crava_gpu_ctx *ctx, int nxp, int nyp, int nzp, int type = PARAMETER)
-      : ctx_(ctx), nxp_(nxp), nyp_(nyp), nzp_(nzp), type_(type) {
+  FFTGridDevice(crava_gpu_ctx *ctx, int nxp, int nyp, int nzp, int type = PARAMETER,
+                cudaStream_t stream = nullptr)
+      : ctx_(ctx), nxp_(nxp), nyp_(nyp), nzp_(nzp), type_(type), stream_(stream) {
     cnxp_ = nxp / 2 + 1;
     rnxp_ = 2 * cnxp_;
     rsize_ = (long long)rnxp_ * nyp * nzp;
@@ -65,29 +88,98 @@ class FFTGridDevice {
   long long getcsize() const { return csize_; }
   long long getrsize() const { return rsize_; }
   float *devicePtr() { return data_; }
+  int getCounterForGet() const { return (int)get_; }
+  int getCounterForSet() const { return (int)set_; }
 
   // FFTGrid::fftInPlace (src/fftgrid.cpp:1803-1829)
   void fftInPlace() {
     if (transformed_) throw Error("fftInPlace on a transformed grid", CRAVA_GPU_ERR_STATE);
+    if (mode_ != NONE) throw Error("fftInPlace during an access", CRAVA_GPU_ERR_STATE);
     check(crava_gpu_fft_r2c(ctx_, data_, type_), "fftInPlace");
     transformed_ = true;
   }
   // FFTGrid::invFFTInPlace (src/fftgrid.cpp:1831-1862)
   void invFFTInPlace() {
     if (!transformed_) throw Error("invFFTInPlace on a real grid", CRAVA_GPU_ERR_STATE);
+    if (mode_ != NONE) throw Error("invFFTInPlace during an access", CRAVA_GPU_ERR_STATE);
     check(crava_gpu_fft_c2r(ctx_, data_, type_), "invFFTInPlace");
     transformed_ = false;
   }
   // Bulk replacements of the setNextReal / getNextReal cursors.
   void upload(const float *host, bool transformed = false) {
-    if (cudaMemcpy(data_, host, sizeof(float) * rsize_, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(data_, host, sizeof(float) * rsize_, cudaMemcpyHostToDevice, stream_) != cudaSuccess ||
+        cudaStreamSynchronize(stream_) != cudaSuccess)
       throw Error("upload", CRAVA_GPU_ERR_CUDA);
     transformed_ = transformed;
   }
   void download(float *host) const {
-    if (cudaDeviceSynchronize() != cudaSuccess ||
-        cudaMemcpy(host, data_, sizeof(float) * rsize_, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpyAsync(host, data_, sizeof(float) * rsize_, cudaMemcpyDeviceToHost, stream_) != cudaSuccess ||
+        cudaStreamSynchronize(stream_) != cudaSuccess)
       throw Error("download", CRAVA_GPU_ERR_CUDA);
+  }
+
+  // FFTGrid::setAccessMode / endAccess (src/fftgrid.h:172-173)
+  void setAccessMode(int mode) {
+    if (mode_ != NONE) throw Error("setAccessMode: previous access not ended", CRAVA_GPU_ERR_STATE);
+    if (mode < NONE || mode > RANDOMACCESS) throw Error("setAccessMode", CRAVA_GPU_ERR_ARG);
+    if (mode != NONE) mirror_.resize((size_t)rsize_);
+    if (mode == READ || mode == READANDWRITE || mode == RANDOMACCESS) download(mirror_.data());
+    mode_ = mode;
+    modified_ = false;
+  }
+  void endAccess() {
+    if ((mode_ == WRITE || mode_ == READANDWRITE || (mode_ == RANDOMACCESS && modified_)))
+      upload(mirror_.data(), transformed_);
+    mode_ = NONE;
+    get_ = set_ = 0;
+  }
+
+  // FFTGrid::getNextComplex / getNextReal (src/fftgrid.cpp:1418-1445)
+  fftw_complex getNextComplex() {
+    if (!transformed_ || (mode_ != READ && mode_ != READANDWRITE))
+      throw Error("getNextComplex", CRAVA_GPU_ERR_STATE);
+    const fftw_complex *c = reinterpret_cast<const fftw_complex *>(mirror_.data());
+    const fftw_complex v = c[get_];
+    if (++get_ == csize_) get_ = 0;
+    return v;
+  }
+  float getNextReal() {
+    if (transformed_ || (mode_ != READ && mode_ != READANDWRITE))
+      throw Error("getNextReal", CRAVA_GPU_ERR_STATE);
+    const float v = mirror_[(size_t)get_];
+    if (++get_ == rsize_) get_ = 0;
+    return v;
+  }
+  // FFTGrid::setNextComplex / setNextReal (src/fftgrid.cpp:1603-1650)
+  int setNextComplex(fftw_complex v) {
+    if (!transformed_ || (mode_ != WRITE && mode_ != READANDWRITE))
+      throw Error("setNextComplex", CRAVA_GPU_ERR_STATE);
+    reinterpret_cast<fftw_complex *>(mirror_.data())[set_] = v;
+    if (++set_ == csize_) set_ = 0;
+    return 0;
+  }
+  int setNextReal(float v) {
+    if (transformed_ || (mode_ != WRITE && mode_ != READANDWRITE))
+      throw Error("setNextReal", CRAVA_GPU_ERR_STATE);
+    mirror_[(size_t)set_] = v;
+    if (++set_ == rsize_) set_ = 0;
+    return 0;
+  }
+  // FFTGrid::getRealValue / setRealValue / getComplexValue (RANDOMACCESS;
+  // src/fftgrid.cpp:1460-1600), inside the padded grid only
+  float getRealValue(int i, int j, int k) const {
+    if (mode_ != RANDOMACCESS || transformed_) throw Error("getRealValue", CRAVA_GPU_ERR_STATE);
+    return mirror_[(size_t)i + (size_t)rnxp_ * (j + (size_t)nyp_ * k)];
+  }
+  int setRealValue(int i, int j, int k, float v) {
+    if (mode_ != RANDOMACCESS || transformed_) throw Error("setRealValue", CRAVA_GPU_ERR_STATE);
+    mirror_[(size_t)i + (size_t)rnxp_ * (j + (size_t)nyp_ * k)] = v;
+    modified_ = true;
+    return 0;
+  }
+  fftw_complex getComplexValue(int i, int j, int k) const {
+    if (mode_ != RANDOMACCESS || !transformed_) throw Error("getComplexValue", CRAVA_GPU_ERR_STATE);
+    return reinterpret_cast<const fftw_complex *>(mirror_.data())[(size_t)i + (size_t)cnxp_ * (j + (size_t)nyp_ * k)];
   }
 
  private:
@@ -95,14 +187,20 @@ class FFTGridDevice {
   int nxp_, nyp_, nzp_, cnxp_, rnxp_;
   long long rsize_, csize_;
   int type_;
+  cudaStream_t stream_ = nullptr;
   bool transformed_ = false;
   float *data_ = nullptr;
+  // cursor state (host mirror of the device values during an access)
+  int mode_ = NONE;
+  bool modified_ = false;
+  long long get_ = 0, set_ = 0;
+  std::vector<float> mirror_;
 };
 
 // The hot path of Crava on device grids.
 class CravaDevice {
  public:
-  CravaDevice(const crava_gpu_params &p, int device = 0, cudaStream_t stream = nullptr) {
+  CravaDevice(const crava_gpu_params &p, int device = 0, cudaStream_t stream = nullptr) : stream_(stream) {
     check(crava_gpu_create(&p, device, stream, &ctx_), "crava_gpu_create");
     nt_ = p.ntheta;
   }
@@ -111,6 +209,13 @@ class CravaDevice {
   CravaDevice &operator=(const CravaDevice &) = delete;
 
   crava_gpu_ctx *ctx() { return ctx_; }
+
+  // Crava::createFFTGrid (src/crava.cpp:1829-1860): a grid of this
+  // context's geometry whose copies run on the context's stream.  The
+  // caller owns it (delete).
+  FFTGridDevice *createFFTGrid(int nxp, int nyp, int nzp, int type = FFTGridDevice::PARAMETER) {
+    return new FFTGridDevice(ctx_, nxp, nyp, nzp, type, stream_);
+  }
 
   // Crava::computePostMeanResidAndFFTCov (src/crava.cpp:887-1295): means
   // and stacks arrive transformed (src/crava.cpp:175-190); the prior
@@ -188,6 +293,7 @@ class CravaDevice {
 
  private:
   crava_gpu_ctx *ctx_ = nullptr;
+  cudaStream_t stream_ = nullptr;
   int nt_ = 0;
 };
 

@@ -258,8 +258,11 @@ int crava_gpu_get_profile(crava_gpu_ctx *ctx, crava_gpu_kernel_profile *out,
  * grids, updated in place as by crava_gpu_posterior; stream: a cudaStream_t
  * (NULL = legacy default stream) on the current device.  stats may be NULL
  * (asynchronous); if given, the call waits for the stream and fills the
- * failure counts (no timings).  The first call on a device sets up the
- * scratch address for that device -- make it before any stream capture.
+ * failure counts (no timings).  nxp <= 8192 and nyp <= 4096 as for
+ * crava_gpu_create.  The first call on a device sets up the scratch address
+ * for that device -- make it before any stream capture.  That address is
+ * cached for the life of the process and is stale after cudaDeviceReset:
+ * do not call this entry point on a device after resetting it.
  * Calls overlapping on the GPU share the scratch and race: serialise them.
  * This entry point has no counterpart in the reference. */
 int crava_gpu_posterior_noalloc(const crava_gpu_params *params,

@@ -20,7 +20,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_LIB = os.path.join(HERE, "build", "libcrava_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcrava_ref.so")
-REF_SRC = "/root/reference"
+# The reference source tree the harness is compiled from (build time only;
+# nothing reads it at run time): CRAVA_REFERENCE_SRC, else its location in
+# the build container.
+REF_SRC = os.environ.get("CRAVA_REFERENCE_SRC", "/root/reference")
 
 F32P = C.POINTER(C.c_float)
 F64P = C.POINTER(C.c_double)
@@ -47,6 +50,9 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(REF_SRC)
     if ref:
+        if not os.path.isfile(os.path.join(REF_SRC, "libs", "lib", "lib_matr.c")):
+            raise FileNotFoundError(f"reference source tree not found at {REF_SRC} "
+                                    "(set CRAVA_REFERENCE_SRC)")
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}", "-j8"], check=True)
 
 

@@ -253,3 +253,66 @@ def test_split_layout_check():
     G.check_layout(G.Layout(256, 256, 512, 4))
     with pytest.raises(ValueError):
         G.check_layout(G.Layout(256, 256, 512, 3))  # 86 / 85 rows
+
+
+def test_exchange_plan_pairs_match():
+    """Every send of rank r to p has the shape of p's receive from r, in
+    both directions, for even and uneven splits."""
+    from crava_b200 import dist_grid as G
+
+    for shape, world in ((SPLIT_SHAPE, 3), ((256, 256, 512), 4), ((16, 10, 7), 3)):
+        lay = G.Layout(*shape, world)
+        for direction in ("to_columns", "to_slabs"):
+            plans = {r: G.exchange_plan(lay, r, direction) for r in range(world)}
+            for r in range(world):
+                sends = {peer: (z, y) for kind, peer, z, y in plans[r] if kind == "send"}
+                for p in range(world):
+                    if p == r:
+                        continue
+                    recv = [(z, y) for kind, peer, z, y in plans[p] if kind == "recv" and peer == r]
+                    assert len(recv) == 1
+                    (sz, sy), (rz, ry) = sends[p], recv[0]
+                    assert (sz[1] - sz[0], sy[1] - sy[0]) == (rz[1] - rz[0], ry[1] - ry[0])
+
+
+class _RecordingDist:
+    """Stands in for torch.distributed: records the grouped point-to-point
+    operations instead of sending them (receive buffers stay as they are)."""
+
+    def __init__(self, backend):
+        self.backend, self.posted = backend, []
+
+    def get_backend(self):
+        return self.backend
+
+    isend, irecv = "isend", "irecv"
+
+    class P2POp:
+        def __init__(self, op, tensor, peer):
+            self.op, self.tensor, self.peer = op, tensor, peer
+
+    def batch_isend_irecv(self, ops):
+        self.posted.append([(o.op, o.peer, tuple(o.tensor.shape)) for o in ops])
+        return []
+
+
+def test_exchange_posts_one_group_and_same_ops_on_both_backends():
+    """Each exchange is one batch_isend_irecv group, and NCCL and gloo are
+    given the same operations in the same order."""
+    import torch
+    from crava_b200 import dist_grid as G
+
+    lay = G.Layout(*SPLIT_SHAPE, 3)
+    rank = 1
+    z0, z1 = lay.z(rank)
+    y0, y1 = lay.y(rank)
+    posted = {}
+    for backend in ("nccl", "gloo"):
+        d = _RecordingDist(backend)
+        slab = torch.zeros((z1 - z0, lay.nyp, 2 * lay.cnxp))
+        cols = G.to_columns(slab, lay, rank, d)
+        G.to_slabs(cols, lay, rank, d, slab)
+        posted[backend] = d.posted
+    assert len(posted["nccl"]) == 2  # one group per direction
+    assert posted["nccl"] == posted["gloo"]
+    assert [op for op, _, _ in posted["nccl"][0]] == ["isend", "irecv"] * 2

@@ -27,8 +27,12 @@ def test_host_mirror_compiles(tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["bulk", "cursor"])
 @pytest.mark.parametrize("name", GC.NAMES)
-def test_host_mirror_matches_reference(tmp_path, name):
+def test_host_mirror_matches_reference(tmp_path, name, mode):
+    """mode "cursor": inputs filled and outputs read through the element
+    cursors (setNextReal / getNextReal / getNextComplex / setNextComplex),
+    which must equal the bulk copies bit for bit."""
     exe = build(str(tmp_path))
     case, z = GC.load(name)
     d = str(tmp_path)
@@ -46,8 +50,10 @@ def test_host_mirror_matches_reference(tmp_path, name):
     for t in range(6):
         case.cov[t].tofile(d + f"/cov{t}.bin")
     case.err_corr.tofile(d + "/err.bin")
-    r = subprocess.run([exe, d], capture_output=True, text=True)
+    r = subprocess.run([exe, d] + (["cursor"] if mode == "cursor" else []), capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+    if mode == "cursor":
+        assert "cursor_mismatch 0" in r.stdout, r.stdout
     nx = case.nxp
     shape = case.mu[0].shape
     names = [f"mu{q}" for q in range(3)] + [f"data{l}" for l in range(case.ntheta)] + [f"cov{t}" for t in range(6)]

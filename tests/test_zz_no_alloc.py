@@ -1,9 +1,15 @@
 """crava_gpu_posterior_noalloc: the per-bin posterior solve for callers that
 cannot allocate device memory (their HBM belongs to their own arena, or they
 cannot take the synchronisation of an allocation).  Its scratch is a static
-device array inside the library.  Checked through the C ABI against the
-regular entry point, crava_gpu_posterior, on two calls in a row (the second
-call finds the previous call's tables and counters in the shared scratch).
+device array inside the library.
+
+Checked through the C ABI against the regular entry point,
+crava_gpu_posterior, on two calls in a row with different cases: the second
+call has other wavelets, the other thickness mode and a smaller nzp and
+ntheta, so it only passes if the call rewrites the tables and counters the
+first call left in the shared scratch.  Both calls run the same kernels on
+the same inputs as the regular entry point, so the outputs must be equal
+bit for bit; device memory in use must not change across the calls.
 
 This file is collected last on purpose."""
 import ctypes as C
@@ -15,6 +21,18 @@ import torch
 from crava_b200 import api, synth
 
 pytestmark = pytest.mark.gpu
+
+
+def _case_first():
+    return synth.make_case(32, 24, 64, (0.0, 10.0, 20.0, 30.0, 40.0), 0.1, seed=31)
+
+
+def _case_second():
+    c = synth.make_case(20, 16, 48, (5.0, 25.0, 45.0), 0.3, seed=32, wavelet_scale_range=(0.8, 1.2),
+                        peak_hz=30.0)
+    c.thickness_mode = 1
+    c.min_rel_thick = 0.8
+    return c
 
 
 def _spectra(ctx, case):
@@ -35,32 +53,49 @@ def _clone(grids):
     return [g.clone() for g in mu], [g.clone() for g in data], [g.clone() for g in cov], err.clone()
 
 
-def _rel(a, b):
-    a = a.double().cpu().numpy()
-    b = b.double().cpu().numpy()
-    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-
-
-@pytest.mark.parametrize("prec", [api.FP64, api.MIXED])
-def test_noalloc_matches_posterior_two_calls(prec):
-    case = synth.make_case(32, 24, 64, (0.0, 10.0, 20.0, 30.0, 40.0), 0.1, seed=31)
+def _prepare(case, prec):
+    """Context, untouched spectra for the allocation-free call, and the
+    regular entry point's outputs and stats on the same spectra."""
     ctx = api.Context(case)
     spec = _spectra(ctx, case)
     ref = _clone(spec)
     ctx.posterior(*ref, prec)
-    ref_stats = ctx.stats()
+    torch.cuda.synchronize()
+    return ctx, _clone(spec), ref, ctx.stats()
+
+
+def _call(lib, ctx, grids, prec, stream):
+    g = ctx.grids(*grids)
+    st = api.Stats()
+    rc = lib.crava_gpu_posterior_noalloc(C.byref(ctx.params), C.byref(g), prec, stream, C.byref(st))
+    assert rc == 0, lib.crava_gpu_status_string(rc)
+    return st
+
+
+@pytest.mark.parametrize("prec", [api.FP64, api.MIXED, api.FP32])
+def test_noalloc_matches_posterior_two_calls(prec):
     lib = api.load_library()
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    for call in range(2):
-        out = _clone(spec)
-        g = ctx.grids(*out)
-        st = api.Stats()
-        rc = lib.crava_gpu_posterior_noalloc(C.byref(ctx.params), C.byref(g), prec, stream, C.byref(st))
-        assert rc == 0, lib.crava_gpu_status_string(rc)
-        assert st.chol_fail_bins == ref_stats.chol_fail_bins
-        assert st.nonfinite_bins == 0
-        for a, b in zip(out[0] + out[1] + out[2], ref[0] + ref[1] + ref[2]):
-            assert _rel(a, b) <= 1e-6
+    first, second = _case_first(), _case_second()
+    assert second.nzp < first.nzp and second.ntheta < first.ntheta
+    ctx1, in1, ref1, st1 = _prepare(first, prec)
+    ctx2, in2, ref2, st2 = _prepare(second, prec)
+    # set-up call (the scratch address of this device; a fresh process
+    # loads the array here), on a throw-away copy of the first case
+    _call(lib, ctx1, _clone(in1), prec, stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    for ctx, grids, ref, ref_st in ((ctx1, in1, ref1, st1), (ctx2, in2, ref2, st2)):
+        st = _call(lib, ctx, grids, prec, stream)
+        torch.cuda.synchronize()
+        assert st.chol_fail_bins == ref_st.chol_fail_bins
+        assert st.nonfinite_bins == ref_st.nonfinite_bins == 0
+        for a, b in zip(grids[0] + grids[1] + grids[2], ref[0] + ref[1] + ref[2]):
+            assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, "device memory changed across the allocation-free calls"
+    assert torch.cuda.memory_reserved() == reserved0
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
@@ -81,3 +116,7 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     rc = lib.crava_gpu_posterior_noalloc(C.byref(p), C.byref(g), api.MIXED, None, None)
     assert rc == 7
     assert b"static scratch" in lib.crava_gpu_status_string(rc)
+    p = api.Params.from_buffer_copy(ctx.params)
+    p.nxp = 16384  # the lateral bounds of crava_gpu_create
+    rc = lib.crava_gpu_posterior_noalloc(C.byref(p), C.byref(g), api.MIXED, None, None)
+    assert rc != 0
