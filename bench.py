@@ -673,9 +673,9 @@ def run_own(args):
     # different grids overlap and per-launch event times would include
     # each other)
     tuned = ctx.tuning()
-    ctx.set_tuning(tuned.cols_y_tile, tuned.cols_z_tile, tuned.fused, 1)
+    ctx.set_tuning(tuned.cols_y_tile, tuned.cols_z_tile, tuned.fused, 1, tuned.rows_x)
     ms_serial, _, prof = timed_steps(prec, max(10, min(args.steps, 30)), True)
-    ctx.set_tuning(tuned.cols_y_tile, tuned.cols_z_tile, tuned.fused, tuned.lanes)
+    ctx.set_tuning(tuned.cols_y_tile, tuned.cols_z_tile, tuned.fused, tuned.lanes, tuned.rows_x)
     ms = max_over_ranks(ms)
     st = ctx.stats()
     cells = nxp * nyp * nzp

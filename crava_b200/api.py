@@ -62,12 +62,12 @@ class State4DGrids(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("chol_fail_bins", C.c_longlong), ("nonfinite_bins", C.c_longlong),
                 ("ms_forward", C.c_float), ("ms_solve", C.c_float),
-                ("ms_inverse", C.c_float), ("ms_total", C.c_float)]
+                ("ms_inverse", C.c_float), ("ms_total", C.c_float), ("refined_bins", C.c_longlong)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("cols_y_tile", C.c_int), ("cols_z_tile", C.c_int), ("fused", C.c_int),
-                ("ms", C.c_float), ("lanes", C.c_int)]
+                ("ms", C.c_float), ("lanes", C.c_int), ("rows_x", C.c_int), ("kappa_refine", C.c_float)]
 
 
 class GridHeader(C.Structure):
@@ -122,6 +122,8 @@ SYMBOLS = {
                                C.POINTER(C.c_longlong)], C.c_int),
     "crava_gpu_synt_seismic": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                 C.POINTER(C.c_void_p)], C.c_int),
+    "crava_gpu_synt_seismic_local": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, F64P,
+                                      C.c_float, F32P, F32P, C.POINTER(C.c_void_p)], C.c_int),
     "crava_gpu_circ_corr_t": ([F32P, C.c_int, C.c_int, C.c_int, F32P], C.c_int),
     "crava_gpu_fill_prior_cov": ([C.c_void_p, F32P, F32P, C.c_float, C.c_float, C.POINTER(C.c_void_p)],
                                  C.c_int),
@@ -288,8 +290,10 @@ class Context:
         check(self.lib.crava_gpu_get_tuning(self.handle, C.byref(t)), "get_tuning")
         return t
 
-    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0, lanes=2):
-        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0, lanes)
+    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0, lanes=2, rows_x=-1, kappa_refine=None):
+        if kappa_refine is None:
+            kappa_refine = self.tuning().kappa_refine
+        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0, lanes, rows_x, kappa_refine)
         check(self.lib.crava_gpu_set_tuning(self.handle, C.byref(t)), "set_tuning")
 
     def autotune(self, src, dst, precision=None, reps=2) -> Tuning:
@@ -461,6 +465,19 @@ class Context:
         arr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
         check(self.lib.crava_gpu_synt_seismic(self.handle, _ptr(alpha), _ptr(beta), _ptr(rho), nx, ny, arr),
               "synt_seismic")
+
+    def synt_seismic_local(self, alpha, beta, rho, outs, rel_thick, dz, shift=None, gain=None, nx=0, ny=0):
+        """Synthetic seismic with every simbox trace's local wavelet
+        (stretch rel_thick [nyp, nxp], local shift / gain [ntheta, ny, nx])."""
+        rt = np.ascontiguousarray(rel_thick, dtype=np.float64)
+        assert rt.size == self.case.nxp * self.case.nyp
+        sh = np.ascontiguousarray(shift, dtype=np.float32) if shift is not None else None
+        gn = np.ascontiguousarray(gain, dtype=np.float32) if gain is not None else None
+        arr = (C.c_void_p * len(outs))(*[o.data_ptr() for o in outs])
+        check(self.lib.crava_gpu_synt_seismic_local(
+            self.handle, _ptr(alpha), _ptr(beta), _ptr(rho), nx, ny, rt.ctypes.data_as(F64P), dz,
+            sh.ctypes.data_as(F32P) if sh is not None else None,
+            gn.ctypes.data_as(F32P) if gn is not None else None, arr), "synt_seismic_local")
 
     def set_fused(self, enable=True):
         check(self.lib.crava_gpu_set_fused(self.handle, int(bool(enable))), "set_fused")

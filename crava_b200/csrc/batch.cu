@@ -168,18 +168,24 @@ int crava_gpu_get_tuning(crava_gpu_ctx *c, crava_gpu_tuning *out) {
   out->fused = c->fused ? 1 : 0;
   out->ms = 0.0f;
   out->lanes = c->lanes;
+  out->rows_x = c->plans.rows_x;
+  out->kappa_refine = c->consts.kappa_refine;
   return CRAVA_GPU_OK;
 }
 
 int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   if (!c || !t) return CRAVA_GPU_ERR_ARG;
-  auto ok = [](int x) { return x == -1 || x == 0 || x == 8 || x == 16; };
+  auto ok = [](int x) { return x == -1 || x == 0 || x == 1 || x == 8 || x == 16; };
   if (!ok(t->cols_y_tile) || !ok(t->cols_z_tile)) return CRAVA_GPU_ERR_ARG;
+  if (t->rows_x < -1 || t->rows_x > 1) return CRAVA_GPU_ERR_ARG;
+  if (!(t->kappa_refine >= 0.0f)) return CRAVA_GPU_ERR_ARG;
   if (t->lanes < 1 || t->lanes > crava_gpu_ctx::kMaxLanes) return CRAVA_GPU_ERR_ARG;
   c->plans.tile_y = t->cols_y_tile;
   c->plans.tile_z = t->cols_z_tile;
   c->fused = t->fused != 0;
   c->lanes = t->lanes;
+  c->plans.rows_x = t->rows_x;
+  c->consts.kappa_refine = t->kappa_refine;
   return CRAVA_GPU_OK;
 }
 
@@ -192,13 +198,21 @@ int crava_gpu_autotune(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_
   DeviceGuard guard(c->device);
   std::vector<crava_gpu_tuning> cand;
   const bool ty = cols_tunable(c->g.nyp), tz = cols_tunable(c->g.nzp);
-  const int tiles[3] = {16, 8, 0};
+  // column choices of a length: the register-resident pass where it
+  // exists, the in-place pass with 16 and 8 columns, the ping-pong pass
+  auto choices = [](int n, bool tunable) {
+    std::vector<int> v;
+    if (cols_rr(n)) v.push_back(1);
+    if (tunable) { v.push_back(16); v.push_back(8); v.push_back(0); }
+    if (v.empty()) v.push_back(-1);
+    return v;
+  };
+  const std::vector<int> cy = choices(c->g.nyp, ty), cz = choices(c->g.nzp, tz);
   for (int lanes = 1; lanes <= 2; ++lanes)
-    for (int a = 0; a < (ty ? 3 : 1); ++a)
-      for (int z = 0; z < (tz ? 3 : 1); ++z)
-        cand.push_back({ty ? tiles[a] : -1, tz ? tiles[z] : -1, 0, 0.0f, lanes});
+    for (int a : cy)
+      for (int z : cz) cand.push_back({a, z, 0, 0.0f, lanes, -1, c->consts.kappa_refine});
   // the fused unit does not use the column passes: one candidate
-  if (c->uplan.ok && precision != CRAVA_SOLVE_FP32) cand.push_back({-1, -1, 1, 0.0f, 1});
+  if (c->uplan.ok && precision != CRAVA_SOLVE_FP32) cand.push_back({-1, -1, 1, 0.0f, 1, -1, c->consts.kappa_refine});
   crava_gpu_tuning saved;
   crava_gpu_get_tuning(c, &saved);
   cudaEvent_t e0 = nullptr, e1 = nullptr;

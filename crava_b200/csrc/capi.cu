@@ -390,6 +390,7 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   c->g = Geom::make(params->nxp, params->nyp, params->nzp);
   c->consts.nt = nt;
   c->consts.wnc = params->wnc;
+  c->consts.kappa_refine = kKappaRefineDefault;
   for (int l = 0; l < nt; ++l) {
     for (int q = 0; q < 3; ++q) c->consts.A[l][q] = c->A[3 * l + q];
     for (int m = 0; m < nt; ++m) c->consts.theta[l][m] = c->theta[l * nt + m];
@@ -782,6 +783,7 @@ int crava_gpu_get_stats(crava_gpu_ctx *c, crava_gpu_stats *st) {
   std::memset(st, 0, sizeof *st);
   st->chol_fail_bins = (long long)h.chol_fail;
   st->nonfinite_bins = (long long)h.nonfinite;
+  st->refined_bins = (long long)h.refined;
   if (c->timed) {
     cudaEventElapsedTime(&st->ms_forward, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(&st->ms_solve, c->ev[1], c->ev[2]);

@@ -98,4 +98,12 @@ int simulate_batches(crava_gpu_ctx *c, const float2 *const cv[6], const float *c
                      uint64_t seed, uint64_t first, int count, float *const *out,
                      const unsigned long long *epoch, unsigned long long epoch_stride);
 
+// Every simbox trace of each grid[l] multiplied by the conjugate of its
+// local wavelet's spectrum getCAmp(k, relThick) (with local shift / gain),
+// divided by pre_div before and post_div after the transforms; the grids
+// are spectra when inverse_first (transformed back first).  (divide.cu)
+int multiply_local_wavelet(crava_gpu_ctx *c, float *const *grids, const double *rel_thick, int nx, int ny,
+                           float dz, const float *shift, const float *gain, float pre_div, float post_div,
+                           bool inverse_first);
+
 }  // namespace crava

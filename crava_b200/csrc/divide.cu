@@ -821,9 +821,16 @@ __global__ void __launch_bounds__(kThreads) k_mul_traces(const double *__restric
 
 }  // namespace
 
-extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float *const *resid,
-                                                       const double *rel_thick, int nx, int ny, float dz,
-                                                       const float *shift, const float *gain) {
+namespace crava {
+
+// Every simbox trace (x < nx, y < ny) of each grid[l] (real domain, or the
+// spectrum when inverse_first, which is transformed back first) multiplied
+// in the Fourier domain by the conjugate of its local wavelet's getCAmp(k,
+// sf): the trace divided by pre_div, transformed, filtered, transformed
+// back and divided by post_div.  Other traces are not touched.
+int multiply_local_wavelet(crava_gpu_ctx *c, float *const *resid, const double *rel_thick, int nx, int ny,
+                           float dz, const float *shift, const float *gain, float pre_div, float post_div,
+                           bool inverse_first) {
   if (!c || !resid || !rel_thick || !(dz > 0.0f)) return CRAVA_GPU_ERR_ARG;
   const Geom &g = c->g;
   const int nt = c->p.ntheta, nzp = g.nzp, cnzp = nzp / 2 + 1;
@@ -907,7 +914,7 @@ extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float 
   fa.grid = reinterpret_cast<float2 *>(scratch);
   for (int l = 0; l < nt; ++l) {
     // seisData_[l]->invFFTInPlace() (:844)
-    if ((rc = pass_inverse(c, resid[l], CRAVA_GRID_DATA))) return rc;
+    if (inverse_first && (rc = pass_inverse(c, resid[l], CRAVA_GRID_DATA))) return rc;
     if (fused_len) {
       FusedArgs fu{};
       fu.Wm = t.W + (size_t)l * cnzp;
@@ -917,15 +924,15 @@ extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float 
       fu.f.dz = dz;
       fu.grid = resid[l];
       fu.tw = c->plans.z.tw;
-      fu.sq_in = sqrtf((float)nzp);
-      fu.sq_out = (float)sqrt((double)nzp);
+      fu.sq_in = pre_div;
+      fu.sq_out = post_div;
       fu.nx = nx; fu.ny = ny; fu.nxp = g.nxp; fu.nyp = g.nyp; fu.nzp = nzp; fu.cnxp = g.cnxp;
       fu.rnxp = g.rnxp; fu.nz = c->p.nz;
       fused_launch<1>(fu, s, &rc);
       if (rc) return rc;
       continue;
     }
-    MulPassArgs pa{resid[l], scratch, nx, ny, g.nxp, g.nyp, nzp, g.rnxp, sqrtf((float)nzp)};
+    MulPassArgs pa{resid[l], scratch, nx, ny, g.nxp, g.nyp, nzp, g.rnxp, pre_div};
     k_mul_pre<<<(unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock), kThreads, 0, s>>>(pa);
     CRAVA_LAUNCH_CHECK();
     if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(scratch), -1, s))) return rc;
@@ -935,9 +942,20 @@ extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float 
     k_mul_filter<<<(unsigned)((nfilt + kThreads - 1) / kThreads), kThreads, 0, s>>>(fa);
     CRAVA_LAUNCH_CHECK();
     if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(scratch), 1, s))) return rc;
-    MulPassArgs pb{scratch, resid[l], nx, ny, g.nxp, g.nyp, nzp, g.rnxp, (float)sqrt((double)nzp)};
+    MulPassArgs pb{scratch, resid[l], nx, ny, g.nxp, g.nyp, nzp, g.rnxp, post_div};
     k_mul_post<<<(unsigned)((rows + kRowsPerBlock - 1) / kRowsPerBlock), kThreads, 0, s>>>(pb);
     CRAVA_LAUNCH_CHECK();
   }
   return CRAVA_GPU_OK;
+}
+
+}  // namespace crava
+
+extern "C" int crava_gpu_multiply_data_by_scale_wavelet(crava_gpu_ctx *c, float *const *resid,
+                                                       const double *rel_thick, int nx, int ny, float dz,
+                                                       const float *shift, const float *gain) {
+  // rData[k] / sqrt(float nzp) before, / sqrt(double nzp) after (src/crava.cpp:853, 871)
+  if (!c) return CRAVA_GPU_ERR_ARG;
+  return crava::multiply_local_wavelet(c, resid, rel_thick, nx, ny, dz, shift, gain, sqrtf((float)c->g.nzp),
+                                       (float)sqrt((double)c->g.nzp), true);
 }

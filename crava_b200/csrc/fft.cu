@@ -12,7 +12,9 @@
 //   cols  (y): each CTA transforms TX adjacent x-columns of one z-plane.
 //   cols  (z): each CTA transforms TX adjacent x-columns of one y-row.
 // Lines live in shared memory and go through the Stockham engine of
-// fft_core.cuh.  The scalings are fused into the first (forward) or last
+// fft_core.cuh; at the power-of-two lengths 64..512 the register-resident
+// passes of fft_rr.cuh are the default (same arithmetic, fewer shared-memory
+// round trips).  The scalings are fused into the first (forward) or last
 // (inverse) pass.
 #include <math.h>
 #include <stdio.h>
@@ -22,6 +24,7 @@
 
 #include "fft.cuh"
 #include "fft_core.cuh"
+#include "fft_rr.cuh"
 
 namespace crava {
 
@@ -365,6 +368,270 @@ __global__ void __launch_bounds__(kThreads) k_cols_ip(const __grid_constant__ Co
   }
 }
 
+// ------------------------------------------------------------------ register-resident passes
+// (fft_rr.cuh).  Column pass: kRrTX lines per CTA; line f starts at
+// base(f) = (f mod A) + (f div A) B and its elements are es apart:
+//   z pass: A = the line count, B = 0  -> base = f, es = cnxp nyp
+//           (the lines of a z plane taken flat: no ragged tiles);
+//   y pass: A = cnxp, B = cnxp nyp     -> lines (kx, z), es = cnxp.
+// CPT lines per thread (2: a float4 shared-memory row access carries both);
+// shared rows hold kRrTX float2 = 128 B, so a phase of 8 (float4) or 16
+// (float2) lanes covers exactly one row: no bank conflicts whatever the
+// stage's index pattern.  VEC: the two lines of a thread are adjacent and
+// 16-byte aligned in global memory (z pass, even es), loaded as one float4.
+constexpr int kRrTX = 16;
+
+struct ColRRArgs {
+  float2 *data;
+  long long nlines;
+  FastDiv fa;
+  uint32_t A;
+  long long B;
+  long long es;
+  const float2 *tw;
+};
+
+template <int N>
+struct RrCols {
+  static constexpr int E = rr::max_radix(N);
+  static constexpr int T = N / E;
+  static constexpr int CPT = E >= 16 ? 1 : 2;
+  static constexpr int NP = kRrTX / CPT;
+  static constexpr int NTH = NP * T;
+  static constexpr int S = CtRadix::count(N);
+};
+
+template <int N, int DIR, int CPT, bool VEC, int S>
+struct RrColStages {
+  // v holds the inputs of stage S (registers (b, q) of radix R_S)
+  static __device__ __forceinline__ void run(float2 (&v)[CPT][RrCols<N>::E], float2 *buf,
+                                             const float2 *tw, int t, int p, float2 *const *gp,
+                                             long long es, const bool *ok) {
+    constexpr int E = RrCols<N>::E, T = RrCols<N>::T, R = CtRadix::at(N, S);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) rr::stage_compute<N, S, DIR, E, T>(v[c], tw, t);
+    if constexpr (S + 1 == CtRadix::count(N)) {
+      // last stage: outputs at the loaded positions, straight to HBM
+#pragma unroll
+      for (int b = 0; b < E / R; ++b)
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const long long e = rr::stage_in<N, S, E, T>(t, b, q);
+          if (VEC) {
+            if (ok[0])
+              *reinterpret_cast<float4 *>(gp[0] + e * es) =
+                  make_float4(v[0][b * R + q].x, v[0][b * R + q].y, v[CPT - 1][b * R + q].x, v[CPT - 1][b * R + q].y);
+          } else {
+#pragma unroll
+            for (int c = 0; c < CPT; ++c)
+              if (ok[c]) gp[c][e * es] = v[c][b * R + q];
+          }
+        }
+    } else {
+      if (S > 0) __syncthreads();  // every thread has read this stage's inputs
+#pragma unroll
+      for (int b = 0; b < E / R; ++b)
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int o = rr::stage_out<N, S, T>(t, b, q);
+          if (CPT == 2)
+            *reinterpret_cast<float4 *>(buf + o * kRrTX + 2 * p) =
+                make_float4(v[0][b * R + q].x, v[0][b * R + q].y, v[CPT - 1][b * R + q].x, v[CPT - 1][b * R + q].y);
+          else
+            buf[o * kRrTX + p] = v[0][b * R + q];
+        }
+      __syncthreads();
+      constexpr int R2 = CtRadix::at(N, S + 1);
+#pragma unroll
+      for (int b = 0; b < E / R2; ++b)
+#pragma unroll
+        for (int q = 0; q < R2; ++q) {
+          const int e = rr::stage_in<N, S + 1, E, T>(t, b, q);
+          if (CPT == 2) {
+            const float4 x = *reinterpret_cast<const float4 *>(buf + e * kRrTX + 2 * p);
+            v[0][b * R2 + q] = make_float2(x.x, x.y);
+            v[CPT - 1][b * R2 + q] = make_float2(x.z, x.w);
+          } else {
+            v[0][b * R2 + q] = buf[e * kRrTX + p];
+          }
+        }
+      RrColStages<N, DIR, CPT, VEC, S + 1>::run(v, buf, tw, t, p, gp, es, ok);
+    }
+  }
+};
+
+template <int N, int DIR, bool VEC>
+__global__ void __launch_bounds__(RrCols<N>::NTH) k_cols_rr(const __grid_constant__ ColRRArgs a) {
+  using C = RrCols<N>;
+  constexpr int E = C::E, T = C::T, CPT = C::CPT, NP = C::NP;
+  constexpr int R0 = CtRadix::at(N, 0);
+  extern __shared__ float4 sm4[];
+  float2 *tw = reinterpret_cast<float2 *>(sm4);
+  float2 *buf = tw + N;  // [N][kRrTX]
+  const int tid = threadIdx.x;
+  const int p = tid % NP, t = tid / NP;
+  for (int i = tid; i < N; i += C::NTH) tw[i] = a.tw[i];
+  float2 *gp[CPT];
+  bool ok[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const long long f = (long long)blockIdx.x * kRrTX + p * CPT + c;
+    ok[c] = f < a.nlines;
+    const uint32_t q = ok[c] ? fdiv((uint32_t)f, a.fa) : 0u;
+    const long long base = ok[c] ? (f - (long long)q * a.A) + (long long)q * a.B : 0;
+    gp[c] = a.data + base;
+  }
+  float2 v[CPT][E];
+#pragma unroll
+  for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+    for (int q = 0; q < R0; ++q) {
+      const long long e = rr::stage_in<N, 0, E, T>(t, b, q);
+      if (VEC) {
+        const float4 x = ok[0] ? __ldg(reinterpret_cast<const float4 *>(gp[0] + e * a.es))
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[0][b * R0 + q] = make_float2(x.x, x.y);
+        v[CPT - 1][b * R0 + q] = make_float2(x.z, x.w);
+      } else {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) v[c][b * R0 + q] = ok[c] ? gp[c][e * a.es] : make_float2(0.f, 0.f);
+      }
+    }
+  __syncthreads();  // twiddles
+  RrColStages<N, DIR, CPT, VEC, 0>::run(v, buf, tw, t, p, gp, a.es, ok);
+}
+
+// Row (x) pass for an even nxp, N = nxp / 2, register-resident: ROWS
+// rows per CTA (32, fewer when the CTA would exceed 512 threads), T threads
+// per row (lanes along the row).  Forward: the
+// packed row's N complex values go global -> registers, through the radix
+// stages, into shared memory for the split X_k = E_k + W^k O_k (which pairs
+// k with N - k), and the N + 1 outputs to HBM.  Inverse: the pre-split
+// Z'_k is built from X_k and X_{N-k} read from HBM into registers, and the
+// last stage writes the real row straight to HBM.  Shared rows are padded
+// (one spare element after every R_0 and a pitch of 8 mod 16 float2) so
+// the first stage's stride-R_0 writes and two rows per phase are free of
+// bank conflicts.
+template <int N>
+struct RrRows {
+  static constexpr int E = rr::max_radix(N);
+  static constexpr int T = N / E;
+  static constexpr int ROWS = 512 / T < 32 ? 512 / T : 32;
+  static constexpr int NTH = ROWS * T;
+  static constexpr int R0 = CtRadix::at(N, 0);
+  static constexpr int P0 = N + N / R0 + 1;  // room for index N in the split
+  static constexpr int P = P0 + ((8 - P0 % 16) + 16) % 16;  // pitch = 8 mod 16
+  static __host__ __device__ constexpr int phys(int e) { return e + e / R0; }
+};
+
+template <int N, int DIR, int S>
+struct RrRowStages {
+  static __device__ __forceinline__ void run(float2 (&v)[RrRows<N>::E], float2 *row, const float2 *tw, int t) {
+    constexpr int E = RrRows<N>::E, T = RrRows<N>::T, R = CtRadix::at(N, S);
+    rr::stage_compute<N, S, DIR, E, T>(v, tw, t);
+    if constexpr (S + 1 < CtRadix::count(N)) {
+      if (S > 0) __syncthreads();
+#pragma unroll
+      for (int b = 0; b < E / R; ++b)
+#pragma unroll
+        for (int q = 0; q < R; ++q) row[RrRows<N>::phys(rr::stage_out<N, S, T>(t, b, q))] = v[b * R + q];
+      __syncthreads();
+      constexpr int R2 = CtRadix::at(N, S + 1);
+#pragma unroll
+      for (int b = 0; b < E / R2; ++b)
+#pragma unroll
+        for (int q = 0; q < R2; ++q) v[b * R2 + q] = row[RrRows<N>::phys(rr::stage_in<N, S + 1, E, T>(t, b, q))];
+      RrRowStages<N, DIR, S + 1>::run(v, row, tw, t);
+    }
+  }
+};
+
+template <int N, int DIR>
+__global__ void __launch_bounds__(RrRows<N>::NTH) k_rows_rr(const __grid_constant__ RowArgs a) {
+  using C = RrRows<N>;
+  constexpr int E = C::E, T = C::T, R0 = C::R0, S = CtRadix::count(N);
+  constexpr int RL = CtRadix::at(N, S - 1);
+  extern __shared__ float4 sm4[];
+  float2 *tw = reinterpret_cast<float2 *>(sm4);  // N
+  float2 *post = tw + N;                          // N + 1
+  float2 *buf = post + N + 1;                     // ROWS rows of pitch P
+  const int tid = threadIdx.x;
+  const int t = tid % T, r = tid / T;
+  for (int i = tid; i < N; i += C::NTH) tw[i] = a.tw[i];
+  for (int i = tid; i <= N; i += C::NTH) post[i] = a.post[i];
+  const long long row_idx = (long long)blockIdx.x * C::ROWS + r;
+  const bool ok = row_idx < a.nrows;
+  float2 *row = buf + r * C::P;
+  float2 v[E];
+  if (DIR < 0) {
+    const float2 *src = reinterpret_cast<const float2 *>(a.src + (ok ? row_idx : 0) * a.rnxp);
+#pragma unroll
+    for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+      for (int q = 0; q < R0; ++q)
+        v[b * R0 + q] = ok ? src[rr::stage_in<N, 0, E, T>(t, b, q)] : make_float2(0.f, 0.f);
+    __syncthreads();  // twiddles
+    RrRowStages<N, DIR, 0>::run(v, row, tw, t);
+    // last stage outputs to shared memory for the split
+    if (S > 1) __syncthreads();
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) row[C::phys(rr::stage_in<N, S - 1, E, T>(t, b, q))] = v[b * RL + q];
+    __syncthreads();
+    if (ok) {
+      // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{N-k})/2, O = -i (Z_k - conj Z_{N-k})/2
+      float2 *orow = reinterpret_cast<float2 *>(a.grid + row_idx * a.rnxp);
+      for (int k = t; k <= N; k += T) {
+        const float2 zk = row[C::phys(k == N ? 0 : k)];
+        float2 zm = row[C::phys(k == 0 ? 0 : N - k)];
+        zm.y = -zm.y;
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 d = csub(zk, zm);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        orow[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+      }
+    }
+  } else {
+    __syncthreads();  // twiddles and post
+    const float2 *X = reinterpret_cast<const float2 *>(a.grid + (ok ? row_idx : 0) * a.rnxp);
+    // Z'[k] = (X_k + conj X_{N-k}) + i W^{-k} (X_k - conj X_{N-k}); the
+    // imaginary parts of DC and Nyquist are ignored, as a C2R does
+#pragma unroll
+    for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+      for (int q = 0; q < R0; ++q) {
+        const int k = rr::stage_in<N, 0, E, T>(t, b, q);
+        float2 x0 = ok ? X[k] : make_float2(0.f, 0.f), x1 = ok ? X[N - k] : make_float2(0.f, 0.f);
+        if (k == 0) { x0.y = 0.f; x1.y = 0.f; }
+        x1.y = -x1.y;
+        const float2 e = cadd(x0, x1);
+        float2 w = post[k];
+        w.y = -w.y;
+        const float2 o = cmul(csub(x0, x1), w);
+        v[b * R0 + q] = make_float2(e.x - o.y, e.y + o.x);
+      }
+    // every thread has read its whole row before any row is overwritten
+    // (in place: the output row is the input row)
+    __syncthreads();
+    RrRowStages<N, DIR, 0>::run(v, row, tw, t);
+    if (ok) {
+      float2 *orow = reinterpret_cast<float2 *>(a.grid + row_idx * a.rnxp);
+      const float2 *arow = a.addend ? reinterpret_cast<const float2 *>(a.addend + row_idx * a.rnxp) : nullptr;
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int q = 0; q < RL; ++q) {
+          const int m = rr::stage_in<N, S - 1, E, T>(t, b, q);
+          float2 x = cscale(v[b * RL + q], a.scale);
+          if (arow) x = cadd(x, arow[m]);
+          orow[m] = x;
+        }
+      if (t == 0) orow[N] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
 int set_smem(const void *fn, size_t bytes) { return func_smem(fn, bytes); }
 
 int line_plan_create(int n, LinePlan *p) {
@@ -460,6 +727,22 @@ int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t 
   a.post = p.xpost;
   a.scale = scale;
   const int n = a.rl.n;
+  if (p.x_even && p.rows_x != 0 && rr::supported(n)) {
+#define CRAVA_ROWS_RR(NN)                                                                      \
+    if (n == NN) {                                                                             \
+      const dim3 g2((unsigned)((a.nrows + RrRows<NN>::ROWS - 1) / RrRows<NN>::ROWS));          \
+      const size_t sm2 = sizeof(float2) * ((size_t)NN + NN + 1 + (size_t)RrRows<NN>::ROWS * RrRows<NN>::P); \
+      const void *f = dir < 0 ? (const void *)k_rows_rr<NN, -1> : (const void *)k_rows_rr<NN, 1>; \
+      int r2 = set_smem(f, sm2);                                                               \
+      if (r2) return r2;                                                                       \
+      if (dir < 0) k_rows_rr<NN, -1><<<g2, RrRows<NN>::NTH, sm2, s>>>(a);                      \
+      else k_rows_rr<NN, 1><<<g2, RrRows<NN>::NTH, sm2, s>>>(a);                               \
+      CRAVA_LAUNCH_CHECK();                                                                    \
+      return CRAVA_GPU_OK;                                                                     \
+    }
+    CRAVA_ROWS_RR(64) CRAVA_ROWS_RR(128) CRAVA_ROWS_RR(256) CRAVA_ROWS_RR(512)
+#undef CRAVA_ROWS_RR
+  }
   if (p.x_even) {
     const size_t sm2 = sizeof(float2) * (n + n + 1 + (size_t)n * (kRR + 1));
     const dim3 g2((unsigned)((a.nrows + kRR - 1) / kRR));
@@ -521,7 +804,43 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
   const int n = lp.rl.n;
   size_t smem = sizeof(float2) * (n + 2 * kColTile * n);
   dim3 grd((ninner + kColTile - 1) / kColTile, nouter);
-  const int tx = tile >= 0 ? tile : cols_tile_width(n);
+  if ((tile == 1 || tile < 0) && rr::supported(n) && scale == 1.0f) {
+    // register-resident pass over the ninner * nouter lines taken flat:
+    // line f = i + ninner o starts at i + outer_stride o
+    ColRRArgs r;
+    r.data = data;
+    r.nlines = (long long)ninner * nouter;
+    r.A = (uint32_t)ninner;
+    r.fa = make_fastdiv((uint32_t)ninner);
+    r.B = outer_stride;
+    r.es = es;
+    r.tw = lp.tw;
+    if (r.nlines >= (1LL << 31)) return CRAVA_GPU_ERR_ARG;
+    const bool flat = outer_stride == ninner;
+    const bool vec = flat && (es % 2 == 0) && (reinterpret_cast<uintptr_t>(data) % 16 == 0);
+    const dim3 g2((unsigned)((r.nlines + kRrTX - 1) / kRrTX));
+#define CRAVA_COLS_RR(NN)                                                                           \
+    if (n == NN) {                                                                                  \
+      const size_t sm2 = sizeof(float2) * ((size_t)NN + (size_t)NN * kRrTX);                        \
+      const void *f = dir < 0 ? (vec ? (const void *)k_cols_rr<NN, -1, true> : (const void *)k_cols_rr<NN, -1, false>) \
+                              : (vec ? (const void *)k_cols_rr<NN, 1, true> : (const void *)k_cols_rr<NN, 1, false>);  \
+      int r2 = set_smem(f, sm2);                                                                    \
+      if (r2) return r2;                                                                            \
+      constexpr int nth = RrCols<NN>::NTH;                                                          \
+      if (dir < 0) {                                                                                \
+        if (vec) k_cols_rr<NN, -1, true><<<g2, nth, sm2, s>>>(r);                                   \
+        else k_cols_rr<NN, -1, false><<<g2, nth, sm2, s>>>(r);                                      \
+      } else {                                                                                      \
+        if (vec) k_cols_rr<NN, 1, true><<<g2, nth, sm2, s>>>(r);                                    \
+        else k_cols_rr<NN, 1, false><<<g2, nth, sm2, s>>>(r);                                       \
+      }                                                                                             \
+      CRAVA_LAUNCH_CHECK();                                                                         \
+      return CRAVA_GPU_OK;                                                                          \
+    }
+    CRAVA_COLS_RR(64) CRAVA_COLS_RR(128) CRAVA_COLS_RR(256) CRAVA_COLS_RR(512)
+#undef CRAVA_COLS_RR
+  }
+  const int tx = tile > 1 || tile == 0 ? tile : cols_tile_width(n);
 #define CRAVA_COLS_CT(NN)                                                                   \
   if (n == NN && tx > 0) {                                                                  \
     const dim3 g2((ninner + tx - 1) / tx, nouter);                                          \
@@ -568,6 +887,8 @@ bool cols_tunable(int n) {
     if (n == m) return true;
   return false;
 }
+
+bool cols_rr(int n) { return rr::supported(n); }
 
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;

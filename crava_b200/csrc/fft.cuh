@@ -22,13 +22,21 @@ struct FftPlans {
   LinePlan z;        // length nzp
   float2 *xpost = nullptr;  // e^{-2 pi i k/nxp}, k = 0..nxp/2 (even nxp)
   // column tile of the y and z passes: -1 default, 0 ping-pong pass,
-  // 8 or 16 columns per CTA in the in-place pass (lengths with compiled
-  // kernels only; other lengths use the generic pass)
+  // 1 register-resident pass (lengths 64, 128, 256, 512), 8 or 16 columns
+  // per CTA in the in-place pass (lengths with compiled kernels only; other
+  // lengths use the generic pass).  The default is the register-resident
+  // pass where it exists, else the in-place pass.
   int tile_y = -1, tile_z = -1;
+  // x pass of an even nxp: -1 default (register-resident where the half
+  // length is 64..512), 0 the in-place pass, 1 register-resident
+  int rows_x = -1;
 };
 
 // Whether length n has compiled column kernels (tile choices 0, 8, 16).
 bool cols_tunable(int n);
+// Whether length n has register-resident kernels (column tile choice 1, and
+// the x pass of nxp = 2 n).
+bool cols_rr(int n);
 
 bool radix_list(int n, RadixList *out);
 int fft_plans_create(const Geom &g, FftPlans *p);

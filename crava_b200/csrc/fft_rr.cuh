@@ -1,0 +1,85 @@
+// fft_rr.cuh -- register-resident transform passes (power-of-two lengths).
+//
+// The in-place passes of fft.cu stage every line in shared memory and run
+// every radix stage shared memory -> registers -> shared memory, with the
+// global load and store going through shared memory as well: about eight
+// shared-memory operations per point and pass, and the passes are
+// issue-bound at 50-69 % of the HBM copy rate.  Here each thread keeps its
+// E points of a line in registers for the whole pass:
+//
+//   global -> registers, stage 0, registers -> shared, [sync],
+//   shared -> registers, stage 1, ...,  last stage, registers -> global
+//
+// so a pass of S radix stages costs S - 1 shared-memory exchanges, and the
+// first and last stages talk to HBM directly.  The arithmetic per butterfly
+// is the Stockham stage of fft_core.cuh (same radices, same twiddle table,
+// same butterflies), so the results equal the in-place passes bit for bit.
+//
+// Stage s of a line of N = R_0 ... R_{S-1} points (Ns = R_0 ... R_{s-1},
+// M = N / R_s): butterfly j reads x[j + q M], q < R_s, multiplies by
+// W_{Ns R}^{(j mod Ns) q}, and writes y[(j / Ns) Ns R + (j mod Ns) + q Ns].
+// With E = max R_s points per thread and T = N / E threads per line,
+// thread t takes the butterflies j = t + T b, b < E / R_s: its inputs are
+// x[t + T (b + q E / R_s)], and in the last stage (Ns R = N) its outputs
+// are y[t + T (b + q E / R)] -- the same stride-T set it loaded.
+#pragma once
+
+#include "fft_core.cuh"
+
+namespace crava {
+namespace rr {
+
+__host__ __device__ constexpr int max_radix(int n) {
+  int m = 0;
+  for (int s = 0; s < CtRadix::count(n); ++s) m = CtRadix::at(n, s) > m ? CtRadix::at(n, s) : m;
+  return m;
+}
+__host__ __device__ constexpr bool is_pow2(int n) { return n > 1 && (n & (n - 1)) == 0; }
+
+// Lengths with register-resident kernels.
+__host__ __device__ constexpr bool supported(int n) { return n == 64 || n == 128 || n == 256 || n == 512; }
+
+// One radix stage on the thread's registers v[b R + q] (b < E / R).
+template <int N, int S, int DIR, int E, int T>
+__device__ __forceinline__ void stage_compute(float2 *v, const float2 *__restrict__ tw, int t) {
+  constexpr int R = CtRadix::at(N, S);
+  constexpr int NS = CtRadix::ns(N, S);
+  constexpr int TSTEP = N / (NS * R);
+#pragma unroll
+  for (int b = 0; b < E / R; ++b) {
+    float2 *w = v + b * R;
+    if (NS > 1) {
+      const int j = t + T * b;
+      const int base = j % NS;
+      if (base != 0) {
+        const int step = base * TSTEP;
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+          float2 x = tw[q * step];
+          if (DIR > 0) x.y = -x.y;
+          w[q] = cmul(w[q], x);
+        }
+      }
+    }
+    Dft<R, DIR>::run(w);
+  }
+}
+
+// Output element of register (b, q) after stage S.
+template <int N, int S, int T>
+__device__ __forceinline__ int stage_out(int t, int b, int q) {
+  constexpr int R = CtRadix::at(N, S);
+  constexpr int NS = CtRadix::ns(N, S);
+  const int j = t + T * b;
+  return (j / NS) * NS * R + (j % NS) + q * NS;
+}
+
+// Input element of register (b, q) for stage S.
+template <int N, int S, int E, int T>
+__device__ __forceinline__ constexpr int stage_in(int t, int b, int q) {
+  constexpr int R = CtRadix::at(N, S);
+  return t + T * (b + q * (E / R));
+}
+
+}  // namespace rr
+}  // namespace crava

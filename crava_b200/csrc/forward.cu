@@ -275,6 +275,70 @@ std::vector<float2> synt_filters(const crava_gpu_ctx *c) {
   return H;
 }
 
+// Synthetic seismic with local wavelets, first step: every angle's
+// impedance imp_l = A_l0 alpha + A_l1 beta + A_l2 rho on every cell (the
+// reference's float sequence), and on the simbox traces (x < nx, y < ny)
+// the tapered trace differenced forward in z (cyclic), the time-domain
+// input of the per-trace wavelet filter (src/crava.cpp:1674-1694).  One
+// thread per padded trace, x fastest; the three parameter grids are read
+// once for all angles.
+struct DiffArgs {
+  const float *m[3];
+  float *out[CRAVA_GPU_MAX_THETA];
+  float A[CRAVA_GPU_MAX_THETA][3];
+  int rnxp, nyp, nzp, nx, ny, nz;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(kThreads) k_synt_diff(const __grid_constant__ DiffArgs a) {
+  const long long plane = (long long)a.rnxp * a.nyp;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= plane) return;
+  const int i = (int)(t % a.rnxp), j = (int)(t / a.rnxp);
+  auto imp = [&](int z, int l) {
+    const long long o = t + (long long)z * plane;
+    return imp1(a.m[0][o], a.m[1][o], a.m[2][o], a.A[l]);
+  };
+  if (!(i < a.nx && j < a.ny)) {
+    for (int z = 0; z < a.nzp; ++z) {
+      const long long o = t + (long long)z * plane;
+      const float x = a.m[0][o], y = a.m[1][o], w = a.m[2][o];
+#pragma unroll
+      for (int l = 0; l < NT; ++l) a.out[l][o] = imp1(x, y, w, a.A[l]);
+    }
+    return;
+  }
+  // fac ((k - nz) imp[0] + (nzp - k - 1) imp[nz - 1]), fac = 1 / (nzp - nz - 1)
+  const float fac = a.nz < a.nzp ? __fdiv_rn(1.0f, (float)(a.nzp - a.nz - 1)) : 0.0f;
+  float v0[NT], vl[NT], prev[NT];
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    v0[l] = imp(0, l);
+    vl[l] = imp(a.nz - 1, l);
+    prev[l] = v0[l];
+  }
+  for (int z = 0; z + 1 < a.nzp; ++z) {
+    const int k = z + 1;
+    float x = 0.f, y = 0.f, w = 0.f;
+    if (k < a.nz) {
+      const long long o = t + (long long)k * plane;
+      x = a.m[0][o]; y = a.m[1][o]; w = a.m[2][o];
+    }
+    const long long oz = t + (long long)z * plane;
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      const float next = k < a.nz ? imp1(x, y, w, a.A[l])
+                                  : __fmul_rn(fac, __fadd_rn(__fmul_rn((float)(k - a.nz), v0[l]),
+                                                             __fmul_rn((float)(a.nzp - k - 1), vl[l])));
+      a.out[l][oz] = __fsub_rn(next, prev[l]);
+      prev[l] = next;
+    }
+  }
+  const long long ol = t + (long long)(a.nzp - 1) * plane;
+#pragma unroll
+  for (int l = 0; l < NT; ++l) a.out[l][ol] = __fsub_rn(v0[l], prev[l]);
+}
+
 }  // namespace
 
 extern "C" int crava_gpu_synt_seismic(crava_gpu_ctx *c, const float *alpha, const float *beta,
@@ -353,4 +417,42 @@ extern "C" int crava_gpu_synt_seismic(crava_gpu_ctx *c, const float *alpha, cons
     if (rc) return rc;
   }
   return CRAVA_GPU_OK;
+}
+
+extern "C" int crava_gpu_synt_seismic_local(crava_gpu_ctx *c, const float *alpha, const float *beta,
+                                            const float *rho, int nx, int ny, const double *rel_thick,
+                                            float dz, const float *shift, const float *gain, float *const *out) {
+  if (!c || !alpha || !beta || !rho || !out || !rel_thick || !(dz > 0.0f)) return CRAVA_GPU_ERR_ARG;
+  const int nt = c->p.ntheta;
+  auto mis = [](const void *p) { return !p || (reinterpret_cast<uintptr_t>(p) & 7u) != 0; };
+  if (mis(alpha) || mis(beta) || mis(rho)) return CRAVA_GPU_ERR_ARG;
+  for (int l = 0; l < nt; ++l) if (mis(out[l])) return CRAVA_GPU_ERR_ARG;
+  if (nx == 0) nx = c->g.nxp;
+  if (ny == 0) ny = c->g.nyp;
+  const int nz = c->p.nz;
+  if (nx < 1 || nx > c->g.nxp || ny < 1 || ny > c->g.nyp || nz < 1 || nz > c->g.nzp) return CRAVA_GPU_ERR_ARG;
+  if (nz == c->g.nzp - 1) return CRAVA_GPU_ERR_ARG;  // the taper divides by nzp - nz - 1
+  DeviceGuard guard(c->device);
+  DiffArgs a{};
+  a.m[0] = alpha; a.m[1] = beta; a.m[2] = rho;
+  for (int l = 0; l < nt; ++l) {
+    a.out[l] = out[l];
+    for (int q = 0; q < 3; ++q) a.A[l][q] = c->A[3 * l + q];
+  }
+  a.rnxp = c->g.rnxp; a.nyp = c->g.nyp; a.nzp = c->g.nzp; a.nx = nx; a.ny = ny; a.nz = nz;
+  const long long ntr = (long long)a.rnxp * a.nyp;
+  const dim3 grd((unsigned)((ntr + kThreads - 1) / kThreads));
+  const cudaStream_t s = c->stream;
+  switch (nt) {
+#define CRAVA_DIFF_CASE(N) case N: k_synt_diff<N><<<grd, kThreads, 0, s>>>(a); break;
+    CRAVA_DIFF_CASE(1) CRAVA_DIFF_CASE(2) CRAVA_DIFF_CASE(3) CRAVA_DIFF_CASE(4)
+    CRAVA_DIFF_CASE(5) CRAVA_DIFF_CASE(6) CRAVA_DIFF_CASE(7) CRAVA_DIFF_CASE(8)
+#undef CRAVA_DIFF_CASE
+    default: return CRAVA_GPU_ERR_ARG;
+  }
+  CRAVA_LAUNCH_CHECK();
+  // resultVec.fft1DInPlace(), times conj(localWavelet->getCAmp(k, sf)),
+  // invFFT1DInPlace() (1 / nzp): the per-trace filter of the multiply-back
+  // with no pre-scale and 1 / nzp after
+  return multiply_local_wavelet(c, out, rel_thick, nx, ny, dz, shift, gain, 1.0f, (float)c->g.nzp, false);
 }

@@ -137,6 +137,7 @@ extern "C" int crava_gpu_posterior_noalloc(const crava_gpu_params *p, const crav
   SolveConsts c{};
   c.nt = nt;
   c.wnc = p->wnc;
+  c.kappa_refine = kKappaRefineDefault;
   for (int l = 0; l < nt; ++l) {
     for (int q = 0; q < 3; ++q) c.A[l][q] = p->A[3 * l + q];
     for (int m = 0; m < nt; ++m) c.theta[l][m] = p->theta_cov[l * nt + m];
@@ -159,6 +160,7 @@ extern "C" int crava_gpu_posterior_noalloc(const crava_gpu_params *p, const crav
     std::memset(stats, 0, sizeof *stats);
     stats->chol_fail_bins = (long long)h.chol_fail;
     stats->nonfinite_bins = (long long)h.nonfinite;
+    stats->refined_bins = (long long)h.refined;
   }
   return CRAVA_GPU_OK;
 }

@@ -222,6 +222,106 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
   if (a.counters) sb::count(a.counters, fail, nonfinite);
 }
 
+// Square-root form (solve_bin.cuh): the FP64 and mixed forms.  One kz
+// plane per CTA: the CTA first stages the plane's per-kz constants of M in
+// shared memory.  Per thread in shared memory, one entry column per
+// thread: FP64 form the factor and the first two columns of Y = L^-1 K S;
+// mixed form the FP32 factor, two FP32 columns of Y and the FP64 prior-mean
+// residual (used by the refinement step).
+template <int NT, int PREC>
+struct SqSmem {
+  static constexpr int NP = NT * (NT + 1) / 2;
+  static constexpr size_t kconst = (sizeof(sb::KzConst<NT>) + 15) / 16 * 16;
+  static constexpr size_t per_thread =
+      PREC == 0 ? sizeof(double2) * (NP + 2 * NT) : sizeof(double2) * NT + sizeof(float2) * (NP + 2 * NT);
+  static constexpr size_t bytes = kconst + per_thread * kThreads;
+};
+
+template <int NT, int PREC, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_solve_sq(SolveArgs a) {
+  extern __shared__ double2 sq_sm[];
+  auto &kc = *reinterpret_cast<sb::KzConst<NT> *>(sq_sm);
+  char *area = reinterpret_cast<char *>(sq_sm) + SqSmem<NT, PREC>::kconst;
+  const int slot = (int)(blockIdx.x / a.bpp);
+  const long long off = (long long)(blockIdx.x % a.bpp) * blockDim.x + threadIdx.x;
+  const int k = a.t.order ? a.t.order[slot] : slot;
+  const bool inv = a.t.inv[k] != 0;
+  const long long o = (long long)k * NT;
+  if (inv) sb::kz_const_fill<NT>(kc, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, threadIdx.x);
+  __syncthreads();
+  if (off >= a.plane) return;
+  const long long idx = (long long)k * a.plane + off;
+  float2 c6[6];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
+  if (!inv) {
+    sb::prior_only<PREC>(a.c, c6);
+    bool nonfinite = false;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
+    if (a.counters) sb::count(a.counters, false, nonfinite);
+    return;
+  }
+  const sb::Sym3d S = sb::prior_exact(c6, a.c.var0);
+  const float2 ec = a.g.err[idx];
+  bool solved, fin = true, refined = false;
+  if (PREC == 0) {
+    double2 *base = reinterpret_cast<double2 *>(area) + threadIdx.x;
+    const sb::SmemTri<double2, kThreads> L{base};
+    const sb::SmemTri<double2, kThreads> Y{base + kThreads * SqSmem<NT, PREC>::NP};
+    solved = sb::solve_bin_fp64_sq<NT>(L, Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, &fin);
+  } else {
+    double2 *vbase = reinterpret_cast<double2 *>(area) + threadIdx.x;
+    float2 *fbase = reinterpret_cast<float2 *>(reinterpret_cast<double2 *>(area) + kThreads * NT) + threadIdx.x;
+    const sb::SmemTri<double2, kThreads> V{vbase};
+    const sb::SmemTri<float2, kThreads> Lf{fbase};
+    const sb::SmemTri<float2, kThreads> Yf{fbase + kThreads * SqSmem<NT, PREC>::NP};
+    solved = sb::solve_bin_mixed_sq<NT>(Lf, Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x), fabs((double)ec.x),
+                                        a.g, idx, &fin, &refined);
+  }
+  if (!solved) {
+    // the reference keeps the prior (src/crava.cpp:1109-1111): the mean and
+    // the data stay, the covariance takes the prior of this form's
+    // arithmetic (FP64: the double prior rounded; mixed: the float prior)
+    sb::prior_only<PREC>(a.c, c6);
+#pragma unroll
+    for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; fin &= sb::fin2(c6[t]); }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) fin &= sb::fin2(a.g.mu[q][idx]);
+#pragma unroll
+    for (int l = 0; l < NT; ++l) fin &= sb::fin2(a.g.data[l][idx]);
+  }
+  if (a.counters) {
+    sb::count(a.counters, !solved, !fin);
+    if (PREC == 1) {
+      const unsigned m = __activemask();
+      const unsigned br = __ballot_sync(m, refined);
+      if (br && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&a.counters->refined, (unsigned long long)__popc(br));
+    }
+  }
+}
+
+template <int PREC, int MINB>
+int launch_solve_sq(const SolveArgs &a, int nt, cudaStream_t s) {
+  dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
+  int rc;
+#define CRAVA_SQ_CASE(N)                                                                        \
+  case N: {                                                                                     \
+    const size_t smem = SqSmem<N, PREC>::bytes;                                                 \
+    if ((rc = func_smem((const void *)k_solve_sq<N, PREC, MINB>, smem))) return rc;             \
+    k_solve_sq<N, PREC, MINB><<<grd, kThreads, smem, s>>>(a);                                   \
+    break;                                                                                      \
+  }
+  switch (nt) {
+    CRAVA_SQ_CASE(1) CRAVA_SQ_CASE(2) CRAVA_SQ_CASE(3) CRAVA_SQ_CASE(4)
+    CRAVA_SQ_CASE(5) CRAVA_SQ_CASE(6) CRAVA_SQ_CASE(7) CRAVA_SQ_CASE(8)
+    default: return CRAVA_GPU_ERR_ARG;
+  }
+#undef CRAVA_SQ_CASE
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
+
 template <int PREC, int MINB>
 int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
   dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
@@ -356,8 +456,9 @@ int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g
   SolveArgs a;
   a.c = c; a.g = g; a.t = t; a.csize = csize; a.plane = plane; a.counters = counters;
   a.bpp = (plane + kThreads - 1) / kThreads;
-  if (precision == CRAVA_SOLVE_FP64) return launch_solve<0>(a, c.nt, s);
-  if (precision == CRAVA_SOLVE_MIXED) return launch_solve<1>(a, c.nt, s);
+  // the square-root form (one kz plane per CTA), two blocks per SM
+  if (precision == CRAVA_SOLVE_FP64) return launch_solve_sq<0, 2>(a, c.nt, s);
+  if (precision == CRAVA_SOLVE_MIXED) return launch_solve_sq<1, 2>(a, c.nt, s);
   return CRAVA_GPU_ERR_ARG;
 }
 

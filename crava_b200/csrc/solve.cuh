@@ -23,6 +23,9 @@ struct SolveConsts {
   float A[CRAVA_GPU_MAX_THETA][3];
   double theta[CRAVA_GPU_MAX_THETA][CRAVA_GPU_MAX_THETA];
   double var0[6];  // (0,0) (1,1) (2,2) (0,1) (0,2) (1,2)
+  // mixed form: a bin whose FP32 factor's condition bound exceeds this
+  // takes one FP64 refinement step (0: every bin; a huge value: none)
+  float kappa_refine;
 };
 
 struct SolveGrids {
@@ -35,7 +38,11 @@ struct SolveGrids {
 struct DevCounters {
   unsigned long long chol_fail;
   unsigned long long nonfinite;
+  unsigned long long refined;  // mixed form: bins that took the FP64 refinement step
 };
+
+// Default condition bound above which the mixed form refines a bin.
+constexpr float kKappaRefineDefault = 1.0e4f;
 
 int kz_tables_alloc(int nzp, int nt, KzTables *t);
 // Fills t->order from t->inv (synchronises s): inverted (compute-heavy)

@@ -525,6 +525,444 @@ __device__ __forceinline__ bool solve_bin_mixed(const SolveConsts &c, const floa
                                                                c6, ec);
 }
 
+// ---------------------------------------------------------------------------
+// Square-root form of the per-bin update (FP64 and mixed forms of the
+// standalone solve kernel).
+//
+// With M = L L^H, X = M^-1 K S and v = d - K mu, the reference's quantities
+// (src/crava.cpp:1114-1129) are Gram products of forward substitutions only:
+//   (K S)^H X = Y^H Y,   X^H v = Y^H z,   Y = L^-1 K S,  z = L^-1 v,
+// so S_post = S - Y^H Y, mu_post = mu + Y^H z, r = d - K mu_post.  No back
+// substitution and no X; the Schur subtraction stays in FP64 (the Gram
+// product accumulates in FP64 in both forms).
+//
+// Per-kz constants (one kz plane per CTA, staged in shared memory): for the
+// lower triangle (l, m <= l), W_lm = wd_l conj(wd_m) and
+// E_lm = (1 - wnc)/2 theta_lm (e1_l conj(e1_m) + e2_l conj(e2_m)), and
+// D_l = wnc theta_ll e3_l^2, so that per bin
+//   M_lm = W_lm (A S A^T)_lm + lambda E_lm  (+ D_l on the diagonal),
+// lambda = |Re(err spectrum)| (getNextErrorVariance, src/crava.cpp:1297-1334).
+template <int NT>
+struct KzConst {
+  static constexpr int NP = NT * (NT + 1) / 2;
+  double2 W[NP], E[NP];
+  float2 Wf[NP], Ef[NP];
+  double D[NT];
+  float Df[NT];
+  float2 wd[NT];
+};
+
+// Fills k for plane kz (call with every thread of the CTA, then sync).
+template <int NT>
+__device__ __forceinline__ void kz_const_fill(KzConst<NT> &k, const SolveConsts &c, const float2 *__restrict__ wdk,
+                                              const float2 *__restrict__ e1k, const float2 *__restrict__ e2k,
+                                              const float *__restrict__ e3k, int tid) {
+  const double hw = 0.5 * (1.0 - (double)c.wnc);
+  if (tid < KzConst<NT>::NP) {
+    int l = 0;
+    while (tri(l + 1, 0) <= tid) ++l;
+    const int m = tid - tri(l, 0);
+    const float2 wl = wdk[l], wm = wdk[m], al = e1k[l], am = e1k[m], bl = e2k[l], bm = e2k[m];
+    const double2 w = dmulc(make_double2(wl.x, wl.y), make_double2(wm.x, wm.y));
+    const double2 n1 = dmulc(make_double2(al.x, al.y), make_double2(am.x, am.y));
+    const double2 n2 = dmulc(make_double2(bl.x, bl.y), make_double2(bm.x, bm.y));
+    const double f = hw * c.theta[l][m];
+    double2 e = make_double2(f * (n1.x + n2.x), f * (n1.y + n2.y));
+    if (l == m) e.y = 0.0;
+    k.W[tid] = l == m ? make_double2(w.x, 0.0) : w;
+    k.E[tid] = e;
+    const float2 wf = cmulc(wl, wm), n1f = cmulc(al, am), n2f = cmulc(bl, bm);
+    const float ff = (float)f;
+    k.Wf[tid] = l == m ? make_float2(wf.x, 0.f) : wf;
+    k.Ef[tid] = make_float2(ff * (n1f.x + n2f.x), l == m ? 0.f : ff * (n1f.y + n2f.y));
+  }
+  if (tid < NT) {
+    const double e3 = (double)e3k[tid];
+    k.D[tid] = (double)c.wnc * c.theta[tid][tid] * e3 * e3;
+    k.Df[tid] = (float)k.D[tid];
+    k.wd[tid] = wdk[tid];
+  }
+}
+
+// The prior in double: |Re(c)/S0| S0 (getNextParameterCovariance,
+// src/seismicparametersholder.cpp:355-427) equals sign(S0) |Re(c)| exactly
+// in double for float c (its rounding error is far below the float ulp),
+// so it is formed without a division.
+__device__ __forceinline__ Sym3d prior_exact(const float2 c6[6], const double v[6]) {
+  double r[6];
+#pragma unroll
+  for (int t = 0; t < 6; ++t) {
+    const double x = fabs((double)c6[t].x);
+    r[t] = v[t] != 0.0 ? copysign(x, v[t]) : x;
+  }
+  return Sym3d{r[0], r[1], r[2], r[3], r[4], r[5]};
+}
+
+// (A S)_{l,p} for p = 0..2 in double.
+template <typename T>
+__device__ __forceinline__ void as_row(const SolveConsts &c, const Sym3d &S, int l, T as[3]) {
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+    as[p] = (T)((double)c.A[l][0] * sget(S, 0, p) + (double)c.A[l][1] * sget(S, 1, p) +
+                (double)c.A[l][2] * sget(S, 2, p));
+}
+
+// Cholesky of the square-root forms: as cholesky() (the reference's failure
+// rules), but the reciprocal pivots 1 / L_ii are stored in the diagonal
+// slots (the substitutions use nothing else of the diagonal), so they need
+// no registers.
+template <int NT, typename T2, typename T, typename LA>
+__device__ __forceinline__ bool cholesky_rd(LA L) {
+  const T factor = L[0].x;
+  if (factor <= T(0)) return false;
+  const T tol = (T)kTol * factor;
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    if (L[tri(i, i)].x <= tol) return false;
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      T2 s = L[tri(i, j)];
+#pragma unroll
+      for (int k = 0; k < j; ++k) {
+        const T2 a = L[tri(i, k)], b = L[tri(j, k)];
+        s.x -= a.x * b.x + a.y * b.y;
+        s.y -= a.y * b.x - a.x * b.y;
+      }
+      const T r = L[tri(j, j)].x;
+      s.x *= r; s.y *= r;
+      L[tri(i, j)] = s;
+    }
+    T d = L[tri(i, i)].x;
+#pragma unroll
+    for (int k = 0; k < i; ++k) d -= L[tri(i, k)].x * L[tri(i, k)].x + L[tri(i, k)].y * L[tri(i, k)].y;
+    if (d <= tol) return false;
+    L[tri(i, i)] = T2{rsqrt(d), T(0)};
+  }
+  return true;
+}
+
+// Forward substitution L x = b in place with 1 / L_ii in the diagonal slots.
+template <int NT, typename T2, typename LA>
+__device__ __forceinline__ void fwd_sub_rd(LA L, T2 *x) {
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    T2 s = x[i];
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      const T2 lij = L[tri(i, j)], xj = x[j];
+      s.x -= lij.x * xj.x - lij.y * xj.y;
+      s.y -= lij.x * xj.y + lij.y * xj.x;
+    }
+    const auto r = L[tri(i, i)].x;
+    x[i].x = s.x * r;
+    x[i].y = s.y * r;
+  }
+}
+
+// Back substitution L^H x = b in place with 1 / L_ii in the diagonal slots.
+template <int NT, typename T2, typename LA>
+__device__ __forceinline__ void bwd_sub_rd(LA L, T2 *x) {
+#pragma unroll
+  for (int i = NT - 1; i >= 0; --i) {
+    T2 s = x[i];
+#pragma unroll
+    for (int j = i + 1; j < NT; ++j) {
+      const T2 lji = L[tri(j, i)], xj = x[j];  // conj(lji) * xj
+      s.x -= lji.x * xj.x + lji.y * xj.y;
+      s.y -= lji.x * xj.y - lji.y * xj.x;
+    }
+    const auto r = L[tri(i, i)].x;
+    x[i].x = s.x * r;
+    x[i].y = s.y * r;
+  }
+}
+
+// v = d - K mu in double, from the bin's spectra in global memory.
+template <int NT>
+__device__ __forceinline__ void prior_resid_g(const SolveConsts &c, const KzConst<NT> &k, const SolveGrids &g,
+                                              long long idx, double2 v[NT]) {
+  double2 m[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const float2 x = g.mu[r][idx];
+    m[r] = make_double2(x.x, x.y);
+  }
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * m[r].x, c.A[l][r] * m[r].y));
+    const float2 wl = k.wd[l], dl = g.data[l][idx];
+    km = dmul(make_double2(wl.x, wl.y), km);
+    v[l] = make_double2((double)dl.x - km.x, (double)dl.y - km.y);
+  }
+}
+
+// Posterior mean mu + dm and residual d - K (mu + dm), written to the bin's
+// spectra (re-read here, so they hold no registers during the solve).
+// Returns whether every output is finite.
+template <int NT>
+__device__ __forceinline__ bool write_mean_resid(const SolveConsts &c, const KzConst<NT> &k, const SolveGrids &g,
+                                                 long long idx, const double2 dm[3]) {
+  double2 mp[3];
+  bool ok = true;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float2 x = g.mu[q][idx];
+    mp[q] = make_double2((double)x.x + dm[q].x, (double)x.y + dm[q].y);
+  }
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    double2 km = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * mp[r].x, c.A[l][r] * mp[r].y));
+    const float2 wl = k.wd[l], dl = g.data[l][idx];
+    km = dmul(make_double2(wl.x, wl.y), km);
+    const float2 r = make_float2((float)((double)dl.x - km.x), (float)((double)dl.y - km.y));
+    g.data[l][idx] = r;
+    ok &= fin2(r);
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const float2 x = make_float2((float)mp[q].x, (float)mp[q].y);
+    g.mu[q][idx] = x;
+    ok &= fin2(x);
+  }
+  return ok;
+}
+
+// Posterior covariance entry (p, q) = S_pq - G_pq, written to its grid.
+__device__ __forceinline__ bool write_cov(const SolveGrids &g, long long idx, int t, double s, double2 G) {
+  const float2 x = make_float2((float)(s - G.x), t < 3 ? 0.f : (float)(-G.y));
+  g.cov[t][idx] = x;
+  return fin2(x);
+}
+
+// The G entries (p, q), p <= q, that column q of Y completes, in the order
+// (0,0) (1,1) (2,2) (0,1) (0,2) (1,2).
+__host__ __device__ constexpr int gidx(int p, int q) { return p == q ? p : (p == 0 ? (q == 1 ? 3 : 4) : 5); }
+
+// Column q of K S: wd_l (A S)_lq.
+template <int NT, typename T2>
+__device__ __forceinline__ void ks_col(const SolveConsts &c, const KzConst<NT> &k, const Sym3d &S, int q, T2 y[NT]) {
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    const double a = (double)c.A[l][0] * sget(S, 0, q) + (double)c.A[l][1] * sget(S, 1, q) +
+                     (double)c.A[l][2] * sget(S, 2, q);
+    const float2 wl = k.wd[l];
+    y[l].x = wl.x * a;
+    y[l].y = wl.y * a;
+  }
+}
+
+// FP64 square-root form of one inverted bin, in place on the grids.  L:
+// the FP64 factor (lower triangle, tri() indexing); Y: room for the first
+// two columns of Y.  Returns false when the factorisation failed (then the
+// caller writes the prior and keeps mu and the data).  *ok: every output
+// finite.
+template <int NT, typename LA, typename YA>
+__device__ __forceinline__ bool solve_bin_fp64_sq(LA L, YA Y, const SolveConsts &c, const KzConst<NT> &k,
+                                                  const Sym3d &S, double lam, const SolveGrids &g, long long idx,
+                                                  bool *ok) {
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    double as[3];
+    as_row(c, S, l, as);
+#pragma unroll
+    for (int m = 0; m <= l; ++m) {
+      const double B = as[0] * c.A[m][0] + as[1] * c.A[m][1] + as[2] * c.A[m][2];
+      const double2 w = k.W[tri(l, m)], e = k.E[tri(l, m)];
+      double2 v = make_double2(w.x * B + lam * e.x, w.y * B + lam * e.y);
+      if (l == m) { v.x += k.D[l]; v.y = 0.0; }
+      L[tri(l, m)] = v;
+    }
+  }
+  if (!cholesky_rd<NT, double2, double, LA>(L)) return false;
+  // Y = L^-1 K S column by column; each column completes its Gram entries
+  // (written at once) and the first two stay for the later columns
+  bool fin = true;
+  double2 y[NT];
+#pragma unroll 1
+  for (int q = 0; q < 3; ++q) {
+    ks_col<NT, double2>(c, k, S, q, y);
+    fwd_sub_rd<NT, double2, LA>(L, y);
+    double2 gq = make_double2(0.0, 0.0), g0 = gq, g1 = gq;
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      gq.x += y[l].x * y[l].x + y[l].y * y[l].y;
+      if (q >= 1) g0 = dadd(g0, dmulc(y[l], Y[l]));       // conj(y0) y
+      if (q >= 2) g1 = dadd(g1, dmulc(y[l], Y[NT + l]));  // conj(y1) y
+      if (q < 2) Y[q * NT + l] = y[l];
+    }
+    fin &= write_cov(g, idx, q, sget(S, q, q), gq);
+    if (q >= 1) fin &= write_cov(g, idx, gidx(0, q), sget(S, 0, q), g0);
+    if (q >= 2) fin &= write_cov(g, idx, gidx(1, q), sget(S, 1, q), g1);
+  }
+  // mean correction Y^H z, z = L^-1 (d - K mu); y holds the last column
+  double2 z[NT];
+  prior_resid_g<NT>(c, k, g, idx, z);
+  fwd_sub_rd<NT, double2, LA>(L, z);
+  double2 dm[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    dm[0] = dadd(dm[0], dmulc(z[l], Y[l]));
+    dm[1] = dadd(dm[1], dmulc(z[l], Y[NT + l]));
+    dm[2] = dadd(dm[2], dmulc(z[l], y[l]));
+  }
+  fin &= write_mean_resid<NT>(c, k, g, idx, dm);
+  *ok = fin;
+  return true;
+}
+
+// Mixed form of one inverted bin: M built and factorised in FP32, Y and z
+// by FP32 forward substitution, the Gram products and the Schur
+// subtraction in FP64.  A bin whose FP32 factor is ill-conditioned --
+// (max L_ii / min L_ii)^2, a lower bound of cond(M), above kappa_refine --
+// instead takes one step of FP64 iterative refinement on X = M^-1 K S: X0
+// from the FP32 factor, the residual K S - M X0 in FP64 (M re-formed in
+// FP64 from the per-kz constants), X = X0 + M^-1 r with the FP32 factor,
+// then S_post = S - (K S)^H X and mu_post = mu + X^H v in FP64.  Lf: the
+// FP32 factor; Yf: two FP32 columns; V: the FP64 prior-mean residual.
+// Returns false when the FP32 factorisation failed.
+template <int NT, typename LA, typename YA, typename VA>
+__device__ __forceinline__ bool solve_bin_mixed_sq(LA Lf, YA Yf, VA V, const SolveConsts &c, const KzConst<NT> &k,
+                                                   const Sym3d &S, float kappa_refine, float lamf, double lam,
+                                                   const SolveGrids &g, long long idx, bool *ok, bool *refined) {
+#pragma unroll
+  for (int l = 0; l < NT; ++l) {
+    float as[3];
+    as_row(c, S, l, as);
+#pragma unroll
+    for (int m = 0; m <= l; ++m) {
+      const float B = as[0] * c.A[m][0] + as[1] * c.A[m][1] + as[2] * c.A[m][2];
+      const float2 w = k.Wf[tri(l, m)], e = k.Ef[tri(l, m)];
+      float2 v = make_float2(w.x * B + lamf * e.x, w.y * B + lamf * e.y);
+      if (l == m) { v.x += k.Df[l]; v.y = 0.f; }
+      Lf[tri(l, m)] = v;
+    }
+  }
+  if (!cholesky_rd<NT, float2, float, LA>(Lf)) return false;
+  // diagonal slots hold 1 / L_ii: cond bound (max L_ii / min L_ii)^2
+  float rmax = 0.f, rmin = 3.0e38f;
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    const float r = Lf[tri(i, i)].x;
+    rmax = fmaxf(rmax, r);
+    rmin = fminf(rmin, r);
+  }
+  const float ratio = rmax / rmin;
+  double2 dm[3];
+  bool fin = true;
+  *refined = ratio * ratio > kappa_refine;
+  if (!*refined) {
+    float2 y[NT];
+#pragma unroll 1
+    for (int q = 0; q < 3; ++q) {
+      ks_col<NT, float2>(c, k, S, q, y);
+      fwd_sub_rd<NT, float2, LA>(Lf, y);
+      double2 gq = make_double2(0.0, 0.0), g0 = gq, g1 = gq;
+#pragma unroll
+      for (int l = 0; l < NT; ++l) {
+        const double2 yl = make_double2(y[l].x, y[l].y);
+        gq.x += yl.x * yl.x + yl.y * yl.y;
+        if (q >= 1) { const float2 t = Yf[l]; g0 = dadd(g0, dmulc(yl, make_double2(t.x, t.y))); }
+        if (q >= 2) { const float2 t = Yf[NT + l]; g1 = dadd(g1, dmulc(yl, make_double2(t.x, t.y))); }
+        if (q < 2) Yf[q * NT + l] = y[l];
+      }
+      fin &= write_cov(g, idx, q, sget(S, q, q), gq);
+      if (q >= 1) fin &= write_cov(g, idx, gidx(0, q), sget(S, 0, q), g0);
+      if (q >= 2) fin &= write_cov(g, idx, gidx(1, q), sget(S, 1, q), g1);
+    }
+    float2 z[NT];
+    {
+      double2 v[NT];
+      prior_resid_g<NT>(c, k, g, idx, v);
+#pragma unroll
+      for (int l = 0; l < NT; ++l) z[l] = make_float2((float)v[l].x, (float)v[l].y);
+    }
+    fwd_sub_rd<NT, float2, LA>(Lf, z);
+    dm[0] = dm[1] = dm[2] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int l = 0; l < NT; ++l) {
+      const double2 zl = make_double2(z[l].x, z[l].y);
+      const float2 y0 = Yf[l], y1 = Yf[NT + l];
+      dm[0] = dadd(dm[0], dmulc(zl, make_double2(y0.x, y0.y)));
+      dm[1] = dadd(dm[1], dmulc(zl, make_double2(y1.x, y1.y)));
+      dm[2] = dadd(dm[2], dmulc(zl, make_double2(y[l].x, y[l].y)));
+    }
+  } else {
+    {
+      double2 v[NT];
+      prior_resid_g<NT>(c, k, g, idx, v);
+#pragma unroll
+      for (int l = 0; l < NT; ++l) V[l] = v[l];
+    }
+#pragma unroll 1
+    for (int q = 0; q < 3; ++q) {
+      float2 x0[NT], r[NT];
+      {
+        double2 ks[NT];
+        ks_col<NT, double2>(c, k, S, q, ks);
+#pragma unroll
+        for (int l = 0; l < NT; ++l) x0[l] = make_float2((float)ks[l].x, (float)ks[l].y);
+        fwd_sub_rd<NT, float2, LA>(Lf, x0);
+        bwd_sub_rd<NT, float2, LA>(Lf, x0);
+        // r = ks - M x0 in FP64, M_lm = W_lm B_lm + lambda E_lm (+ D_l)
+#pragma unroll
+        for (int l = 0; l < NT; ++l) {
+          double asl[3];
+          as_row(c, S, l, asl);
+          double2 acc = ks[l];
+#pragma unroll
+          for (int m = 0; m < NT; ++m) {
+            const int lo = l >= m ? l : m, hi = l >= m ? m : l;
+            const double B = asl[0] * c.A[m][0] + asl[1] * c.A[m][1] + asl[2] * c.A[m][2];
+            const double2 w = k.W[tri(lo, hi)], e = k.E[tri(lo, hi)];
+            double2 Mlm = make_double2(w.x * B + lam * e.x, w.y * B + lam * e.y);
+            if (l < m) Mlm.y = -Mlm.y;  // upper triangle: conj of the stored lower entry
+            if (l == m) { Mlm.x += k.D[l]; Mlm.y = 0.0; }
+            acc = dsub(acc, dmul(Mlm, make_double2(x0[m].x, x0[m].y)));
+          }
+          r[l] = make_float2((float)acc.x, (float)acc.y);
+        }
+      }
+      fwd_sub_rd<NT, float2, LA>(Lf, r);
+      bwd_sub_rd<NT, float2, LA>(Lf, r);
+      double2 x[NT];
+#pragma unroll
+      for (int l = 0; l < NT; ++l) x[l] = make_double2((double)x0[l].x + (double)r[l].x, (double)x0[l].y + (double)r[l].y);
+      double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int l = 0; l < NT; ++l) acc = dadd(acc, dmulc(V[l], x[l]));  // conj(x) v
+      if (q == 0) dm[0] = acc;
+      else if (q == 1) dm[1] = acc;
+      else dm[2] = acc;
+      // (K S)^H X entries (p, q), p <= q: sum_l AS_lp conj(w_l) x_l
+#pragma unroll
+      for (int l = 0; l < NT; ++l) {
+        const float2 wl = k.wd[l];
+        x[l] = make_double2(wl.x * x[l].x + wl.y * x[l].y, wl.x * x[l].y - wl.y * x[l].x);
+      }
+#pragma unroll
+      for (int p = 0; p <= q; ++p) {
+        double2 gg = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int l = 0; l < NT; ++l) {
+          double as[3];
+          as_row(c, S, l, as);
+          const double a = p == 0 ? as[0] : p == 1 ? as[1] : as[2];
+          gg.x += a * x[l].x;
+          gg.y += a * x[l].y;
+        }
+        fin &= write_cov(g, idx, gidx(p, q), sget(S, p, q), gg);
+      }
+    }
+  }
+  fin &= write_mean_resid<NT>(c, k, g, idx, dm);
+  *ok = fin;
+  return true;
+}
+
 // A band-gated bin: only the prior covariance is written (mu and the data
 // stay as they are), in the arithmetic of the PREC form.
 template <int PREC>

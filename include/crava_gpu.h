@@ -97,6 +97,7 @@ typedef struct crava_gpu_stats {
   float ms_solve;             /* device time of the per-bin solve                      */
   float ms_inverse;           /* device time of the inverse transforms                 */
   float ms_total;             /* device time of the whole call                         */
+  long long refined_bins;     /* mixed form: inverted bins that took the FP64 refinement */
 } crava_gpu_stats;
 
 typedef struct crava_gpu_ctx crava_gpu_ctx;
@@ -269,20 +270,27 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
                                 const crava_gpu_grids *grids, int precision,
                                 void *stream, crava_gpu_stats *stats);
 
-/* Launch shapes of a context.  cols_y_tile / cols_z_tile: columns per CTA
- * of the y and z column transforms (-1 the built-in choice, 0 the
- * out-of-place pass, 8 or 16 the in-place pass; lengths without compiled
- * column kernels ignore it); fused: the fused unit kernels (1) or the
- * three passes (0); ms: one unit's measured time (autotune output only);
- * lanes: more than 1 lets the transforms of different grids overlap on
- * that many streams.
- * No counterpart in the reference (FFTW plans are fixed there). */
+/* Launch shapes of a context.  cols_y_tile / cols_z_tile: the y and z
+ * column transforms (-1 the built-in choice, 0 the out-of-place pass, 1 the
+ * register-resident pass of lengths 64/128/256/512, 8 or 16 columns per CTA
+ * in the in-place pass; lengths without compiled column kernels ignore it);
+ * fused: the fused unit kernels (1) or the three passes (0); ms: one unit's
+ * measured time (autotune output only); lanes: more than 1 lets the
+ * transforms of different grids overlap on that many streams; rows_x: the x
+ * pass of an even nxp (-1 built-in, 0 in-place pass, 1 register-resident
+ * pass where nxp / 2 is 64..512).  All these choices give the same values
+ * bit for bit.  kappa_refine (mixed form only, >= 0): an inverted bin whose
+ * FP32 factor has (max L_ii / min L_ii)^2 above it takes one FP64
+ * refinement step (0 refines every bin).  No counterpart in the reference
+ * (FFTW plans are fixed there). */
 typedef struct crava_gpu_tuning {
   int cols_y_tile;
   int cols_z_tile;
   int fused;
   float ms;
   int lanes;   /* streams the unit's independent transforms run on (1..4) */
+  int rows_x;
+  float kappa_refine;
 } crava_gpu_tuning;
 int crava_gpu_get_tuning(crava_gpu_ctx *ctx, crava_gpu_tuning *out);
 int crava_gpu_set_tuning(crava_gpu_ctx *ctx, const crava_gpu_tuning *t);
@@ -379,6 +387,21 @@ int crava_gpu_loglik_grad(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
  * reference's taper divides by nzp - nz - 1).  Asynchronous. */
 int crava_gpu_synt_seismic(crava_gpu_ctx *ctx, const float *alpha, const float *beta,
                            const float *rho, int nx, int ny, float *const *out);
+
+/* Synthetic seismic with each trace's local wavelet, the general form of
+ * Crava::computeSyntSeismic (src/crava.cpp:1666-1719): as
+ * crava_gpu_synt_seismic, but the simbox trace (x, y) is filtered with
+ * conj(getCAmp(k, sf)) of seisWavelet_[l]->createLocalWavelet1D(x, y) --
+ * the wavelet shifted by shift[l][y][x] ms (divided by dz) and scaled by
+ * gain[l][y][x] (Wavelet1D::shiftAndScale, WELLMISSING = none) -- at
+ * sf = rel_thick[y][x] (Simbox::getRelThick; getLocalStretch is 1 for a
+ * 1-D wavelet).  rel_thick: host [nyp][nxp]; shift, gain: host
+ * [ntheta][ny][nx] or NULL; dz: the simbox's dz (> 0).  Synchronous in the
+ * host arrays' upload, then asynchronous. */
+int crava_gpu_synt_seismic_local(crava_gpu_ctx *ctx, const float *alpha, const float *beta,
+                                 const float *rho, int nx, int ny, const double *rel_thick,
+                                 float dz, const float *shift, const float *gain,
+                                 float *const *out);
 
 /* Circular temporal prior correlation on nzp samples:
  * SeismicParametersHolder::computeCircCorrT + makeCircCorrTPosDef

@@ -116,6 +116,11 @@ def _load(which: str):
         f = lib.orc_sim_filter_fp64
         f.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(F32P), C.POINTER(F32P), C.POINTER(C.c_longlong)]
         f.restype = C.c_int
+    if which == "ref":
+        f = lib.ref_synt_seismic_local
+        f.argtypes = [C.c_int] * 7 + [F32P, F32P, C.POINTER(F32P), F64P, C.c_float, F32P, F32P,
+                                      C.POINTER(F32P)]
+        f.restype = C.c_int
     f = getattr(lib, f"{p}_divide_data")
     f.argtypes = [C.POINTER(Params), C.POINTER(F32P), F32P, F64P, C.c_int, C.c_int, C.c_float, F32P, F32P]
     f.restype = C.c_int
@@ -313,6 +318,29 @@ def synt_seismic(case, m, nx=None, ny=None, nz=None, which="orc"):
     wav = np.ascontiguousarray(case.wavelet, dtype=np.float32)
     rc = getattr(lib, f"{which}_synt_seismic")(case.nxp, case.nyp, case.nzp, nx, ny, nz, case.ntheta,
                                                _fp(A), _fp(wav), _ptrs(mm), _ptrs(out))
+    assert rc == 0
+    return out
+
+
+def synt_seismic_local(case, m, rel_thick, dz, shift=None, gain=None, nx=None, ny=None, nz=None):
+    """Synthetic seismic with each trace's local wavelet (relative
+    thickness stretch, local shift and gain): the reference's trace loop on
+    its own FFTW (oracle/_ref only).  rel_thick [nyp, nxp] float64; shift /
+    gain [ntheta, ny, nx] float32 or None."""
+    lib = _load("ref")
+    nx = case.nxp if nx is None else nx
+    ny = case.nyp if ny is None else ny
+    nz = case.nz if nz is None else nz
+    mm = [np.ascontiguousarray(g, dtype=np.float32) for g in m]
+    out = [np.zeros_like(mm[0]) for _ in range(case.ntheta)]
+    A = np.ascontiguousarray(case.A, dtype=np.float32)
+    wav = np.ascontiguousarray(case.wavelet, dtype=np.float32)
+    rt = np.ascontiguousarray(rel_thick, dtype=np.float64)
+    sh = None if shift is None else np.ascontiguousarray(shift, dtype=np.float32)
+    ga = None if gain is None else np.ascontiguousarray(gain, dtype=np.float32)
+    rc = lib.ref_synt_seismic_local(case.nxp, case.nyp, case.nzp, nx, ny, nz, case.ntheta, _fp(A), _fp(wav),
+                                    _ptrs(mm), _dp(rt), float(dz), _fp(sh) if sh is not None else None,
+                                    _fp(ga) if ga is not None else None, _ptrs(out))
     assert rc == 0
     return out
 

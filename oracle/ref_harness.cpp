@@ -303,6 +303,94 @@ int ref_synt_seismic(int nxp, int nyp, int nzp, int nx, int ny, int nz, int nt,
   return 0;
 }
 
+/* Crava::computeSyntSeismic (src/crava.cpp:1666-1719) with the local
+ * wavelet of every trace: seisWavelet_[l]->createLocalWavelet1D(i, j)
+ * (src/wavelet1D.cpp:497-505: a copy shifted and scaled by the local shift
+ * and gain, Wavelet1D::shiftAndScale, src/wavelet1D.cpp:539-561) and
+ * getCAmp(k, sf) with sf = relThick(i, j) * getLocalStretch(i, j) (1 for a
+ * 1-D wavelet, src/wavelet.h:108) (src/wavelet.cpp:327-385).  shift / gain:
+ * [ntheta][ny][nx] (ms / factor; WELLMISSING = no value) or null; rel_thick:
+ * [nyp][nxp]. */
+int ref_synt_seismic_local(int nxp, int nyp, int nzp, int nx, int ny, int nz, int nt,
+                           const float *A, const float *wavelet, const float *const *m,
+                           const double *rel_thick, float dz, const float *shift, const float *gain,
+                           float *const *out) {
+  const int cnxp = nxp / 2 + 1, rnxp = 2 * cnxp, cnzp = nzp / 2 + 1, rnzp = 2 * cnzp;
+  const long plane = static_cast<long>(rnxp) * nyp, rsize = plane * nzp;
+  if (nz < 1 || nz > nzp || nx > nxp || ny > nyp || !rel_thick) return 1;
+  fftw_real *res = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_real *lw = static_cast<fftw_real *>(fftw_malloc(rnzp * sizeof(fftw_real)));
+  fftw_complex *cw = reinterpret_cast<fftw_complex *>(lw);
+  std::vector<float> imp(nzp);
+  rfftwnd_plan fwd = rfftwnd_create_plan(1, &nzp, FFTW_REAL_TO_COMPLEX, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  rfftwnd_plan inv = rfftwnd_create_plan(1, &nzp, FFTW_COMPLEX_TO_REAL, FFTW_ESTIMATE | FFTW_IN_PLACE);
+  for (int l = 0; l < nt; ++l) {
+    float *o = out[l];
+    for (long c = 0; c < rsize; ++c) {  /* computeSeismicImpedance */
+      float v = 0;
+      v += m[0][c] * A[3 * l + 0];
+      v += m[1][c] * A[3 * l + 1];
+      v += m[2][c] * A[3 * l + 2];
+      o[c] = v;
+    }
+    for (int i = 0; i < nx; ++i)
+      for (int j = 0; j < ny; ++j) {
+        const long t = i + static_cast<long>(rnxp) * j;
+        int k;
+        for (k = 0; k < nz; ++k) imp[k] = o[t + k * plane];
+        float fac = 1.0f / static_cast<float>(nzp - nz - 1);
+        for (; k < nzp; ++k) imp[k] = fac * ((k - nz) * imp[0] + (nzp - k - 1) * imp[nz - 1]);
+        for (k = 0; k < nzp; ++k) res[k] = (k == nzp - 1) ? imp[0] - imp[k] : imp[k + 1] - imp[k];
+        for (; k < rnzp; ++k) res[k] = 0.0f;
+        rfftwnd_one_real_to_complex(fwd, res, reinterpret_cast<fftw_complex *>(res));
+        fftw_complex *rc = reinterpret_cast<fftw_complex *>(res);
+        /* the local wavelet: the wavelet's spectrum, shifted and scaled */
+        for (int q = 0; q < rnzp; ++q) lw[q] = q < nzp ? wavelet[static_cast<long>(l) * nzp + q] : 0.0f;
+        rfftwnd_one_real_to_complex(fwd, lw, cw);
+        float ts = 0.0f, g = 1.0f;
+        const long so = static_cast<long>(l) * nx * ny + i + static_cast<long>(nx) * j;
+        if (shift && shift[so] != -999.0f) ts = shift[so];
+        if (gain && gain[so] != -999.0f) g = gain[so];
+        if (shift || gain) {
+          float iShift = ts / dz;
+          for (k = 0; k < cnzp; k++) {
+            fftw_complex am, tmp;
+            am.re = float(g * cos(2.0 * (3.14159265358979323846 * (iShift) * k) / float(nzp)));
+            am.im = float(g * sin(-2.0 * (3.14159265358979323846 * (iShift) * k) / float(nzp)));
+            tmp.re = am.re * cw[k].re - am.im * cw[k].im;
+            tmp.im = am.im * cw[k].re + am.re * cw[k].im;
+            cw[k] = tmp;
+          }
+        }
+        const float sf = static_cast<float>(rel_thick[i + static_cast<long>(nxp) * j]) * 1.0f;
+        for (k = 0; k < cnzp; ++k) {
+          fftw_complex r = rc[k], w, sv;  /* w = getCAmp(k, sf) */
+          float omega = float(k) / sf;
+          if (omega >= cnzp) { w.re = 0.0f; w.im = 0.0f; }
+          else {
+            int omL = int(std::floor(omega)), omU = int(std::floor(omega)) + 1;
+            if (omU >= cnzp) omU -= 1;
+            float dOmega = omega - float(omL);
+            w.re = cw[omL].re * (1.0f - dOmega) + cw[omU].re * dOmega;
+            w.im = (cw[omL].im * (1.0f - dOmega) + cw[omU].im * dOmega);
+          }
+          w.re /= sf; w.im /= sf;
+          sv.re = r.re * w.re + r.im * w.im;
+          sv.im = -r.re * w.im + r.im * w.re;
+          rc[k] = sv;
+        }
+        rfftwnd_one_complex_to_real(inv, rc, res);
+        double scale = static_cast<double>(1.0 / static_cast<double>(nzp));
+        for (k = 0; k < nzp; ++k) o[t + k * plane] = static_cast<fftw_real>(res[k] * scale);
+      }
+  }
+  fftwnd_destroy_plan(fwd);
+  fftwnd_destroy_plan(inv);
+  fftw_free(res);
+  fftw_free(lw);
+  return 0;
+}
+
 /* FFTGrid::fftInPlace, src/fftgrid.cpp:1803-1829 */
 int ref_fft_r2c(float *grid, int nxp, int nyp, int nzp, int type) {
   long rsize = 2L * (nxp / 2 + 1) * nyp * nzp;

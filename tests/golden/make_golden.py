@@ -58,6 +58,36 @@ def make_synt():
     print("synt_seismic written")
 
 
+# Synthetic seismic with local wavelets: golden case -> unpadded sizes and
+# whether local shift / gain grids are given (relative thickness always).
+SYNT_LOCAL = {
+    "c3_12x10x16": (11, 9, 13, False),
+    "c2_9x8x20_odd": (7, 8, 17, True),
+}
+
+
+def make_synt_local():
+    """Crava::computeSyntSeismic with each trace's local wavelet (stretch,
+    shift, gain) through the reference's FFTW (oracle/_ref)."""
+    from tests import golden_cases as GC
+
+    out = {}
+    for name, (nx, ny, nz, local) in SYNT_LOCAL.items():
+        case, _ = GC.load(name)
+        rng = np.random.default_rng(8)
+        m = [rng.standard_normal(case.mu[0].shape).astype(np.float32) for _ in range(3)]
+        rt, shift, gain, dz = divide_inputs(case, nx, ny, local, seed=23)
+        out[f"{name}_m"] = np.stack(m)
+        out[f"{name}_size"] = np.array([nx, ny, nz])
+        out[f"{name}_rel_thick"] = rt
+        out[f"{name}_dz"] = np.float32(dz)
+        if local:
+            out[f"{name}_shift"], out[f"{name}_gain"] = shift, gain
+        out[f"{name}_out"] = np.stack(O.synt_seismic_local(case, m, rt, dz, shift, gain, nx, ny, nz))
+    np.savez_compressed(os.path.join(HERE, "synt_local.npz"), **out)
+    print("synt_local written")
+
+
 def make_state4d():
     """State4D merge and split of a seeded state through the reference's
     lib_matr (oracle/_ref)."""
@@ -127,6 +157,9 @@ def main():
     if "--synt-only" in sys.argv:
         make_synt()
         return
+    if "--synt-local-only" in sys.argv:
+        make_synt_local()
+        return
     if "--state4d-only" in sys.argv:
         make_state4d()
         return
@@ -162,6 +195,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "rng_23665.npz"), normals=normals, state=state)
     print("rng written")
     make_synt()
+    make_synt_local()
     make_state4d()
     make_divide()
 

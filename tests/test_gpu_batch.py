@@ -27,19 +27,47 @@ def test_column_tiles_match_numpy(shape):
     g = case.data[0]
     ref = np.fft.rfftn(g[..., :nx].astype(np.float64), axes=(0, 1, 2)) / np.sqrt(nx * ny * nz)
     res = {}
-    for ty in (16, 8, 0):
-        for tz in (16, 8, 0):
+    for ty in (1, 16, 8, 0):
+        for tz in (1, 16, 8, 0):
             ctx.set_tuning(ty, tz, 0)
             t = api.to_device(g)
             ctx.fft_r2c(t, api.DATA)
             out = api.complex_view(t.cpu().numpy(), nx).copy()
             assert rel(out, ref) < 2e-6, (ty, tz)
             ctx.fft_c2r(t, api.DATA)
-            assert rel(t.cpu().numpy()[..., :nx], g[..., :nx]) < 2e-6, (ty, tz)
-            res[(ty, tz)] = out
-    # the in-place pass does the same arithmetic per line whatever the tile
-    assert np.array_equal(res[(16, 16)], res[(8, 8)])
-    assert np.array_equal(res[(16, 8)], res[(8, 16)])
+            back = t.cpu().numpy()[..., :nx]
+            assert rel(back, g[..., :nx]) < 2e-6, (ty, tz)
+            res[(ty, tz)] = (out, back)
+    # the in-place pass does the same arithmetic per line whatever the
+    # tile, and so does the register-resident pass (1) where it exists
+    same = lambda a, b: all(np.array_equal(x, y) for x, y in zip(res[a], res[b]))
+    assert same((16, 16), (8, 8)) and same((16, 8), (8, 16))
+    assert same((1, 1), (16, 16)) and same((1, 16), (16, 16)) and same((16, 1), (16, 16))
+
+
+# even nxp whose half length has register-resident row kernels, and one without
+@pytest.mark.parametrize("shape", [(128, 24, 32), (256, 8, 16), (512, 6, 8), (1024, 4, 8), (96, 12, 16)])
+def test_row_pass_choices_match(shape):
+    """The register-resident x pass (rows_x 1) and the in-place x pass
+    (rows_x 0) give the same transform bit for bit, forward and inverse,
+    with and without an addend; both match numpy."""
+    nx, ny, nz = shape
+    case = synth.make_case(nx, ny, nz, (10.0,), 0.1, seed=6)
+    ctx = api.Context(case)
+    g = case.data[0]
+    ref = np.fft.rfftn(g[..., :nx].astype(np.float64), axes=(0, 1, 2)) / np.sqrt(nx * ny * nz)
+    res = {}
+    for rx in (1, 0):
+        ctx.set_tuning(-1, -1, 0, 2, rx)
+        t = api.to_device(g)
+        ctx.fft_r2c(t, api.DATA)
+        out = t.cpu().numpy().copy()
+        assert rel(api.complex_view(out, nx), ref) < 2e-6, rx
+        ctx.fft_c2r(t, api.DATA)
+        back = t.cpu().numpy().copy()
+        assert rel(back[..., :nx], g[..., :nx]) < 2e-6, rx
+        res[rx] = (out, back)
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
 
 
 def _dev(case):

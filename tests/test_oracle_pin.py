@@ -453,3 +453,24 @@ def test_interpolate_seismic_two_restatements(bad):
     assert np.array_equal(a[:, :ny, :nx], b[:, :ny, :nx])
     d = np.abs(a.view(np.int32).astype(np.int64) - b.view(np.int32).astype(np.int64))
     assert d[..., :nxp].max() <= 1
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="oracle/_ref (the reference's FFTW build) is not built")
+def test_synt_seismic_local_harness_vs_golden_and_constant_case():
+    """The local-wavelet trace loop (stretch, shift, gain) on the reference's
+    FFTW equals its golden fixture bit for bit, and with unit relative
+    thickness and no shift or gain it equals the constant-thickness loop
+    (itself pinned against synt_seismic.npz) bit for bit."""
+    z = np.load(os.path.join(GC.HERE, "synt_local.npz"))
+    for name in ("c3_12x10x16", "c2_9x8x20_odd"):
+        case, _ = GC.load(name)
+        nx, ny, nz = (int(v) for v in z[f"{name}_size"])
+        m = list(z[f"{name}_m"])
+        sh = z[f"{name}_shift"] if f"{name}_shift" in z else None
+        ga = z[f"{name}_gain"] if f"{name}_gain" in z else None
+        out = O.synt_seismic_local(case, m, z[f"{name}_rel_thick"], float(z[f"{name}_dz"]), sh, ga, nx, ny, nz)
+        assert np.array_equal(np.stack(out), z[f"{name}_out"])
+        ones = np.ones((case.nyp, case.nxp))
+        a = O.synt_seismic_local(case, m, ones, float(z[f"{name}_dz"]), None, None, nx, ny, nz)
+        b = O.synt_seismic(case, m, nx, ny, nz, "ref")
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
