@@ -102,11 +102,11 @@ int check_grids(const crava_gpu_ctx *c, const crava_gpu_grids *gr) {
 
 enum ProfKind {
   K_ROWS_FWD, K_COLS_Y_FWD, K_COLS_Z_FWD, K_SOLVE, K_COLS_Z_INV, K_COLS_Y_INV, K_ROWS_INV,
-  K_SIM, K_PLANE_FWD, K_ZSOLVE, K_PLANE_INV, K_NKINDS
+  K_SIM, K_PLANE_FWD, K_ZSOLVE, K_PLANE_INV, K_XY_FWD, K_XY_INV, K_NKINDS
 };
 const char *kKindName[K_NKINDS] = {"fft_rows_r2c", "fft_cols_y_fwd", "fft_cols_z_fwd", "posterior_solve",
                                    "fft_cols_z_inv", "fft_cols_y_inv", "fft_rows_c2r", "sim_noise_filter",
-                                   "unit_plane_fwd", "unit_zsolve", "unit_plane_inv"};
+                                   "unit_plane_fwd", "unit_zsolve", "unit_plane_inv", "fft_xy_fwd", "fft_xy_inv"};
 
 cudaEvent_t pool_get(crava_gpu_ctx *c) {
   if (!c->pool.empty()) { cudaEvent_t e = c->pool.back(); c->pool.pop_back(); return e; }
@@ -156,6 +156,11 @@ void prof_collect(crava_gpu_ctx *c) {
 
 int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type) {
   int rc;
+  if (use_plane_xy(c->plans)) {
+    { Scope sc(c, K_XY_FWD); if ((rc = plane_xy(c->plans, src, dst, -1, forward_scale(c->g, type), nullptr, c->stream))) return rc; }
+    { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
+    return CRAVA_GPU_OK;
+  }
   { Scope sc(c, K_ROWS_FWD); if ((rc = fft_rows(c->plans, dst, -1, forward_scale(c->g, type), c->stream, nullptr, src))) return rc; }
   { Scope sc(c, K_COLS_Y_FWD); if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
   { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
@@ -165,6 +170,10 @@ int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type) {
 int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend) {
   int rc;
   { Scope sc(c, K_COLS_Z_INV); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc; }
+  if (use_plane_xy(c->plans)) {
+    Scope sc(c, K_XY_INV);
+    return plane_xy(c->plans, grid, grid, 1, inverse_scale(c->g, type), addend, c->stream);
+  }
   { Scope sc(c, K_COLS_Y_INV); if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(grid), 1, c->stream))) return rc; }
   { Scope sc(c, K_ROWS_INV); if ((rc = fft_rows(c->plans, grid, 1, inverse_scale(c->g, type), c->stream, addend))) return rc; }
   return CRAVA_GPU_OK;
@@ -472,6 +481,8 @@ int crava_gpu_fft_xy(crava_gpu_ctx *c, float *grid, int dir, int type, int nzp_f
   const Geom full = Geom::make(c->g.nxp, c->g.nyp, nzp_full);
   const float scale = dir < 0 ? forward_scale(full, type) : inverse_scale(full, type);
   int rc;
+  // the same x and y kernels as the 3-D transforms of this geometry
+  if (use_plane_xy(c->plans)) return plane_xy(c->plans, grid, grid, dir, scale, nullptr, c->stream);
   if (dir < 0) {
     if ((rc = fft_rows(c->plans, grid, -1, scale, c->stream))) return rc;
     return fft_cols_y(c->plans, reinterpret_cast<float2 *>(grid), -1, c->stream);

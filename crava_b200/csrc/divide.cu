@@ -291,13 +291,25 @@ struct Local {
   bool on;
 };
 
+// e^{-2 pi i ishift m / nzp}, the ampMultiplier phase of shiftAndScale.
+// The reference evaluates cos / sin of 2 pi ishift m / nzp in double; here
+// the phase in turns is reduced to (-1/2, 1/2] in double (exact for the
+// float shift and integer bin) and the angle is evaluated in float, which
+// keeps the rotation within a few 1e-7 while the per-(trace, bin) work
+// stays off the FP64 pipe.
+__device__ __forceinline__ float2 phase_rot(const Local &L, int m, int nzp) {
+  const double q = (double)L.ishift * (double)m / (double)nzp;
+  const float f = (float)(q - rint(q));
+  float sn, cs;
+  sincospif(2.0f * f, &sn, &cs);
+  return make_float2(cs, -sn);
+}
+
 __device__ __forceinline__ float2 local_bin(const float2 *tab, int m, int nzp, const Local &L, float gain) {
   const float2 v = __ldg(tab + m);
   if (!L.on) return v;
-  const double x = 2.0 * (3.14159265358979323846 * (double)L.ishift * (double)m) / (double)(float)nzp;
-  double s, c;
-  sincos(x, &s, &c);
-  const float ar = (float)((double)gain * c), ai = (float)((double)gain * -s);
+  const float2 r = phase_rot(L, m, nzp);
+  const float ar = __fmul_rn(gain, r.x), ai = __fmul_rn(gain, r.y);
   return make_float2(__fsub_rn(__fmul_rn(ar, v.x), __fmul_rn(ai, v.y)),
                      __fadd_rn(__fmul_rn(ai, v.x), __fmul_rn(ar, v.y)));
 }
@@ -310,18 +322,28 @@ __device__ __forceinline__ float2 local_e3(const float2 *E3, int m, int nzp, con
   const float2 u = __ldg(E3 + m);
   float2 v = make_float2(__fmul_rn(u.x, inv), __fmul_rn(u.y, inv));
   if (L.on) {
-    const double x = 2.0 * (3.14159265358979323846 * (double)L.ishift * (double)m) / (double)(float)nzp;
-    double sv, cv;
-    sincos(x, &sv, &cv);
-    const float ar = (float)cv, ai = (float)-sv;
-    v = make_float2(__fsub_rn(__fmul_rn(ar, v.x), __fmul_rn(ai, v.y)),
-                    __fadd_rn(__fmul_rn(ai, v.x), __fmul_rn(ar, v.y)));
+    const float2 r = phase_rot(L, m, nzp);
+    v = make_float2(__fsub_rn(__fmul_rn(r.x, v.x), __fmul_rn(r.y, v.y)),
+                    __fadd_rn(__fmul_rn(r.y, v.x), __fmul_rn(r.x, v.y)));
   }
   if (m == nzp / 2) {
     if ((nzp & 1) == 0) v = make_float2(kMissing, kMissing);
     else v.y = kMissing;
   }
   return v;
+}
+
+// |local_e3(E3, m)|^2: the rotation keeps the modulus, so it is needed
+// only at the bin that carries RMISSING in one part (odd nzp).
+__device__ __forceinline__ float local_e3_mag2(const float2 *E3, int m, int nzp, const Local &L, float inv) {
+  if (m == nzp / 2 && (nzp & 1)) {
+    const float2 v = local_e3(E3, m, nzp, L, inv);
+    return __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y));
+  }
+  if (m == nzp / 2) return __fmul_rn(2.0f, __fmul_rn(kMissing, kMissing));
+  const float2 u = __ldg(E3 + m);
+  const float x = __fmul_rn(u.x, inv), y = __fmul_rn(u.y, inv);
+  return __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
 }
 
 // Wavelet::getCAmp(k, scale) for k < cnzp (src/wavelet.cpp:327-385).
@@ -382,8 +404,10 @@ __device__ float2 adjust(const DivFilterArgs &a, int k, int i, int j, float2 d) 
   const float wGlob2 = sq2(wGlob);
   float sizeLoc = __fdividef(wLoc2, s.wn2);
   sizeLoc = __fadd_rn(sizeLoc, sq2(camp_scaled<true>(a.E3, k, sf, a.nzp, L, s.e3_inv)));
-  float sizeGlob = __fdividef(sq2(local_bin(a.W, k, a.nzp, L, L.gain)), s.wn2);
-  sizeGlob = __fadd_rn(sizeGlob, sq2(local_e3(a.E3, k, a.nzp, L, s.e3_inv)));
+  // |shifted and scaled W_k|^2 = gain^2 |W_k|^2 (the rotation keeps the modulus)
+  const float g2 = L.on ? __fmul_rn(L.gain, L.gain) : 1.0f;
+  float sizeGlob = __fdividef(__fmul_rn(g2, wGlob2), s.wn2);
+  sizeGlob = __fadd_rn(sizeGlob, local_e3_mag2(a.E3, k, a.nzp, L, s.e3_inv));
   const float half = __fmul_rn(__fsub_rn(1.0f, a.wnc), 0.5f);
   float sigma2Loc = __fmul_rn(s.error_var, __fadd_rn(a.wnc, __fmul_rn(half, sizeLoc)));
   const float sigma2Glob = __fmul_rn(s.error_var, __fadd_rn(a.wnc, __fmul_rn(half, sizeGlob)));

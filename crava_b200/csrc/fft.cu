@@ -705,12 +705,13 @@ int fft_plans_create(const Geom &g, FftPlans *p) {
     CRAVA_CUDA_TRY(cudaMalloc(&p->xpost, sizeof(float2) * (h + 1)));
     CRAVA_CUDA_TRY(cudaMemcpy(p->xpost, post.data(), sizeof(float2) * (h + 1), cudaMemcpyHostToDevice));
   }
-  return CRAVA_GPU_OK;
+  return plane_xy_tables(g, &p->twq, &p->twy);
 }
 
 void fft_plans_destroy(FftPlans *p) {
   cudaFree(p->x.tw); cudaFree(p->y.tw); cudaFree(p->z.tw); cudaFree(p->xpost);
-  p->x.tw = p->y.tw = p->z.tw = p->xpost = nullptr;
+  cudaFree(p->twq); cudaFree(p->twy);
+  p->x.tw = p->y.tw = p->z.tw = p->xpost = p->twq = p->twy = nullptr;
 }
 
 int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t s,
@@ -902,6 +903,10 @@ int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
 
 int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s) {
   int rc;
+  if (use_plane_xy(p)) {
+    if ((rc = plane_xy(p, grid, grid, -1, forward_scale(p.g, type), nullptr, s))) return rc;
+    return fft_cols_z(p, reinterpret_cast<float2 *>(grid), -1, s);
+  }
   if ((rc = fft_rows(p, grid, -1, forward_scale(p.g, type), s))) return rc;
   if ((rc = fft_cols_y(p, reinterpret_cast<float2 *>(grid), -1, s))) return rc;
   return fft_cols_z(p, reinterpret_cast<float2 *>(grid), -1, s);
@@ -910,6 +915,7 @@ int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s) {
 int fft3d_c2r(const FftPlans &p, float *grid, int type, cudaStream_t s, const float *addend) {
   int rc;
   if ((rc = fft_cols_z(p, reinterpret_cast<float2 *>(grid), 1, s))) return rc;
+  if (use_plane_xy(p)) return plane_xy(p, grid, grid, 1, inverse_scale(p.g, type), addend, s);
   if ((rc = fft_cols_y(p, reinterpret_cast<float2 *>(grid), 1, s))) return rc;
   return fft_rows(p, grid, 1, inverse_scale(p.g, type), s, addend);
 }

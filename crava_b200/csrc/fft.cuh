@@ -30,7 +30,21 @@ struct FftPlans {
   // x pass of an even nxp: -1 default (register-resident where the half
   // length is 64..512), 0 the in-place pass, 1 register-resident
   int rows_x = -1;
+  // x and y passes in one cluster kernel (plane.cu) where the geometry has
+  // one: -1 default (on), 0 off, 1 on; its twiddle tables
+  int plane_xy = -1;
+  float2 *twq = nullptr, *twy = nullptr;
 };
+
+// The fused x + y pass (plane.cu): geometries with a compiled kernel.
+bool plane_xy_supported(const Geom &g);
+int plane_xy_tables(const Geom &g, float2 **twq, float2 **twy);
+// Forward (dir -1: src real -> dst spectrum in x and y, scaled) or inverse
+// (dir +1: dst spectrum -> dst real, scaled, + addend) x and y passes.
+int plane_xy(const FftPlans &p, const float *src, float *dst, int dir, float scale, const float *addend,
+             cudaStream_t s);
+// Whether the transforms of these plans use the fused x + y pass.
+inline bool use_plane_xy(const FftPlans &p) { return p.plane_xy != 0 && p.twq && p.twy; }
 
 // Whether length n has compiled column kernels (tile choices 0, 8, 16).
 bool cols_tunable(int n);

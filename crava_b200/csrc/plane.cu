@@ -1,0 +1,418 @@
+// plane.cu -- the x and y passes of a 3-D transform in one kernel: one
+// thread-block cluster per (grid, z-plane), the plane held in the CTAs'
+// shared memory, so a transform moves 4 grids of HBM traffic (this pass
+// and the z pass each read and write the grid once) instead of 6.
+//
+// A plane of NY rows of nxp = 2 NH reals is split over the CS CTAs of a
+// cluster by rows: CTA r holds the NQ = NY / CS rows y = CS q + r.  The y
+// transform of length NY = NQ CS factorises (ky = k1 + NQ k2):
+//   Y[k1 + NQ k2] = sum_r W_CS^{r k2} [ W_NY^{r k1} sum_q x[CS q + r] W_NQ^{q k1} ],
+// so each CTA first transforms its rows along x (the packed half-length
+// R2C of the x pass), then along its own rows with NQ points and the
+// twiddle W_NY^{r k1}; after a cluster barrier the last radix-CS stage
+// runs across the CTAs: CTA r reads the CS values of its quarter of the
+// k1 range from every CTA's shared memory (distributed shared memory) and
+// writes the CS spectrum rows k1 + NQ k2 straight to HBM.  The inverse
+// runs the same steps backwards: the radix-CS stage from HBM, its results
+// pushed into the owning CTAs' shared memory, the NQ-point inverse along
+// y, and the x C2R to HBM.
+//
+// The per-line arithmetic uses the register-resident Stockham stages of
+// fft_rr.cuh.  The y factorisation differs from the separate y pass
+// (radix CS first instead of the CtRadix list), so the results agree with
+// the three-pass transforms to float rounding, not bit for bit.
+//
+// Replaces the x and y passes of FFTGrid::fftInPlace / invFFTInPlace
+// (src/fftgrid.cpp:1803-1862); the scalings are fused as in fft.cu.
+#include <cooperative_groups.h>
+#include <math.h>
+
+#include <vector>
+
+#include "fft.cuh"
+#include "fft_rr.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace crava {
+
+namespace {
+
+constexpr int kPlaneThreads = 256;
+
+struct PlaneArgs {
+  const float *src;   // forward: real input planes (may equal dst)
+  float *dst;         // forward: spectrum output; inverse: real output
+  const float *add;   // inverse: real addend or null
+  int rnxp, nyp, nplanes;
+  float scale;
+  const float2 *twx;   // NH-point table e^{-2 pi i k / NH}
+  const float2 *post;  // e^{-2 pi i k / nxp}, k <= NH
+  const float2 *twq;   // NQ-point table
+  const float2 *twy;   // NY-point table e^{-2 pi i k / NY}
+};
+
+template <int NH, int NY, int CS>
+struct PlaneCfg {
+  static constexpr int NQ = NY / CS;
+  static constexpr int CX = NH + 1;   // cnxp
+  static constexpr int EX = rr::max_radix(NH), TX = NH / EX;   // x: points / threads per row
+  static constexpr int R0X = CtRadix::at(NH, 0);
+  static constexpr int EQ = rr::max_radix(NQ), TQ = NQ / EQ;  // y: points / threads per column
+  // row pitch: the x exchange layout (one spare after every R0X) and the
+  // CX outputs both fit; 8 mod 16 float2 keeps two rows per phase apart
+  static constexpr int P0 = (NH + NH / R0X) > CX ? (NH + NH / R0X) : CX;
+  static constexpr int P = P0 + ((8 - P0 % 16) + 16) % 16;
+  static constexpr int QK = NQ / CS;  // k1 range of one CTA in the radix-CS stage
+  static __host__ __device__ constexpr int physx(int e) { return e + e / R0X; }
+  static constexpr size_t tab = sizeof(float2) * (NH + NH + 1 + NQ + NQ);
+  static constexpr size_t smem = tab + sizeof(float2) * (size_t)NQ * P;
+};
+
+template <int N, int DIR, int E, int T, int S, typename IDX>
+struct SmemStages {
+  // stages S.. of an N-point line held as v (registers) with exchanges in
+  // shared memory at idx(e); the caller syncs before the first call
+  static __device__ __forceinline__ void run(float2 (&v)[E], float2 *buf, const float2 *tw, int t, bool act,
+                                             IDX idx) {
+    constexpr int R = CtRadix::at(N, S);
+    if (act) rr::stage_compute<N, S, DIR, E, T>(v, tw, t);
+    if constexpr (S + 1 < CtRadix::count(N)) {
+      __syncthreads();  // every thread has read this stage's inputs
+      if (act) {
+#pragma unroll
+        for (int b = 0; b < E / R; ++b)
+#pragma unroll
+          for (int q = 0; q < R; ++q) buf[idx(rr::stage_out<N, S, T>(t, b, q))] = v[b * R + q];
+      }
+      __syncthreads();
+      constexpr int R2 = CtRadix::at(N, S + 1);
+      if (act) {
+#pragma unroll
+        for (int b = 0; b < E / R2; ++b)
+#pragma unroll
+          for (int q = 0; q < R2; ++q) v[b * R2 + q] = buf[idx(rr::stage_in<N, S + 1, E, T>(t, b, q))];
+      }
+      SmemStages<N, DIR, E, T, S + 1, IDX>::run(v, buf, tw, t, act, idx);
+    }
+  }
+};
+
+// ------------------------------------------------------------------ forward
+template <int NH, int NY, int CS>
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_constant__ PlaneArgs a) {
+  using C = PlaneCfg<NH, NY, CS>;
+  constexpr int NQ = C::NQ, CX = C::CX, P = C::P, EX = C::EX, TX = C::TX, EQ = C::EQ, TQ = C::TQ;
+  constexpr int R0X = C::R0X, SX = CtRadix::count(NH), RLX = CtRadix::at(NH, SX - 1);
+  constexpr int R0Q = CtRadix::at(NQ, 0), SQ = CtRadix::count(NQ), RLQ = CtRadix::at(NQ, SQ - 1);
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ float4 sm4[];
+  float2 *twx = reinterpret_cast<float2 *>(sm4);
+  float2 *post = twx + NH;
+  float2 *twq = post + NH + 1;
+  float2 *twr = twq + NQ;  // W_NY^{r k1}, k1 < NQ
+  float2 *A = twr + NQ;    // [NQ][P]
+  const int tid = threadIdx.x, r = (int)cl.block_rank();
+  for (int i = tid; i < NH; i += kPlaneThreads) twx[i] = a.twx[i];
+  for (int i = tid; i <= NH; i += kPlaneThreads) post[i] = a.post[i];
+  for (int i = tid; i < NQ; i += kPlaneThreads) {
+    twq[i] = a.twq[i];
+    twr[i] = a.twy[(r * i) % NY];
+  }
+  const int plane = blockIdx.x / CS;
+  const long long pr = (long long)a.rnxp * a.nyp;  // floats per real plane
+  const float *src = a.src + (long long)plane * pr;
+  float2 *dst = reinterpret_cast<float2 *>(a.dst + (long long)plane * pr);
+  __syncthreads();
+
+  // 1. x: the NQ rows of this CTA, TX threads per row, rounds of
+  //    kPlaneThreads / TX rows
+  constexpr int RPR = kPlaneThreads / TX;  // rows per round
+  constexpr int NRX = (NQ + RPR - 1) / RPR;
+  for (int rd = 0; rd < NRX; ++rd) {
+    const int q = rd * RPR + tid / TX, t = tid % TX;
+    const bool act = q < NQ;
+    float2 *row = A + (act ? q : 0) * P;
+    float2 v[EX];
+    if (act) {
+      const float2 *in = reinterpret_cast<const float2 *>(src + (long long)(CS * q + r) * a.rnxp);
+#pragma unroll
+      for (int b = 0; b < EX / R0X; ++b)
+#pragma unroll
+        for (int qq = 0; qq < R0X; ++qq) v[b * R0X + qq] = in[rr::stage_in<NH, 0, EX, TX>(t, b, qq)];
+    }
+    auto ix = [](int e) { return C::physx(e); };
+    SmemStages<NH, -1, EX, TX, 0, decltype(ix)>::run(v, row, twx, t, act, ix);
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < EX / RLX; ++b)
+#pragma unroll
+        for (int qq = 0; qq < RLX; ++qq) row[C::physx(rr::stage_in<NH, SX - 1, EX, TX>(t, b, qq))] = v[b * RLX + qq];
+    }
+    __syncthreads();
+    // split X_k = E_k + W^k O_k into registers, then the plain layout
+    float2 X[EX + 1];
+    if (act) {
+#pragma unroll
+      for (int m = 0; m <= EX; ++m) {
+        const int k = m < EX ? t + TX * m : NH;
+        if (m == EX && t != 0) break;
+        const float2 zk = row[C::physx(k == NH ? 0 : k)];
+        float2 zm = row[C::physx(k == 0 ? 0 : NH - k)];
+        zm.y = -zm.y;
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 d = csub(zk, zm);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        X[m] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+      }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int m = 0; m < EX; ++m) row[t + TX * m] = X[m];
+      if (t == 0) row[NH] = X[EX];
+    }
+  }
+  __syncthreads();
+
+  // 2. y, local: NQ points along this CTA's rows for every column kx,
+  //    then the twiddle W_NY^{r k1}; in place in A
+  constexpr int CPR = kPlaneThreads / TQ;  // columns per round
+  constexpr int NRQ = (CX + CPR - 1) / CPR;
+  for (int rd = 0; rd < NRQ; ++rd) {
+    const int kx = rd * CPR + tid % CPR, t = tid / CPR;
+    const bool act = kx < CX;
+    float2 v[EQ];
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < EQ / R0Q; ++b)
+#pragma unroll
+        for (int qq = 0; qq < R0Q; ++qq) v[b * R0Q + qq] = A[rr::stage_in<NQ, 0, EQ, TQ>(t, b, qq) * P + kx];
+    }
+    auto iy = [kx](int e) { return e * P + (kx < CX ? kx : 0); };
+    SmemStages<NQ, -1, EQ, TQ, 0, decltype(iy)>::run(v, A, twq, t, act, iy);
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < EQ / RLQ; ++b)
+#pragma unroll
+        for (int qq = 0; qq < RLQ; ++qq) {
+          const int k1 = rr::stage_in<NQ, SQ - 1, EQ, TQ>(t, b, qq);
+          A[k1 * P + kx] = cmul(v[b * RLQ + qq], twr[k1]);
+        }
+    }
+    __syncthreads();
+  }
+
+  // 3. the radix-CS stage across the cluster: this CTA's k1 range, every
+  //    column; the CS outputs are spectrum rows k1 + NQ k2
+  cl.sync();
+  const float2 *Ar[CS];
+#pragma unroll
+  for (int s = 0; s < CS; ++s) Ar[s] = cl.map_shared_rank(A, s);
+  for (int i = tid; i < C::QK * CX; i += kPlaneThreads) {
+    const int k1 = r * C::QK + i / CX, kx = i % CX;
+    float2 v[CS];
+#pragma unroll
+    for (int s = 0; s < CS; ++s) v[s] = Ar[s][k1 * P + kx];
+    Dft<CS, -1>::run(v);
+#pragma unroll
+    for (int k2 = 0; k2 < CS; ++k2) dst[(long long)(k1 + NQ * k2) * CX + kx] = v[k2];
+  }
+  cl.sync();  // partners are done reading this CTA's shared memory
+}
+
+// ------------------------------------------------------------------ inverse
+template <int NH, int NY, int CS>
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_inv(const __grid_constant__ PlaneArgs a) {
+  using C = PlaneCfg<NH, NY, CS>;
+  constexpr int NQ = C::NQ, CX = C::CX, P = C::P, EX = C::EX, TX = C::TX, EQ = C::EQ, TQ = C::TQ;
+  constexpr int R0X = C::R0X, SX = CtRadix::count(NH), RLX = CtRadix::at(NH, SX - 1);
+  constexpr int R0Q = CtRadix::at(NQ, 0), SQ = CtRadix::count(NQ), RLQ = CtRadix::at(NQ, SQ - 1);
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ float4 sm4[];
+  float2 *twx = reinterpret_cast<float2 *>(sm4);
+  float2 *post = twx + NH;
+  float2 *twq = post + NH + 1;
+  float2 *twr = twq + NQ;  // W_NY^{-r k1}
+  float2 *A = twr + NQ;
+  const int tid = threadIdx.x, r = (int)cl.block_rank();
+  for (int i = tid; i < NH; i += kPlaneThreads) twx[i] = a.twx[i];
+  for (int i = tid; i <= NH; i += kPlaneThreads) post[i] = a.post[i];
+  for (int i = tid; i < NQ; i += kPlaneThreads) {
+    twq[i] = a.twq[i];
+    twr[i] = cconj(a.twy[(r * i) % NY]);
+  }
+  const int plane = blockIdx.x / CS;
+  const long long pr = (long long)a.rnxp * a.nyp;
+  const float2 *src = reinterpret_cast<const float2 *>(a.src + (long long)plane * pr);
+  float *dst = a.dst + (long long)plane * pr;
+  const float *add = a.add ? a.add + (long long)plane * pr : nullptr;
+
+  // 1. the inverse radix-CS stage for this CTA's k1 range from HBM; value
+  //    t goes to CTA t's shared memory (every partner is running and done
+  //    with any earlier use of its buffer: cluster barrier first)
+  cl.sync();
+  float2 *At[CS];
+#pragma unroll
+  for (int s = 0; s < CS; ++s) At[s] = cl.map_shared_rank(A, s);
+  for (int i = tid; i < C::QK * CX; i += kPlaneThreads) {
+    const int k1 = r * C::QK + i / CX, kx = i % CX;
+    float2 v[CS];
+#pragma unroll
+    for (int k2 = 0; k2 < CS; ++k2) v[k2] = src[(long long)(k1 + NQ * k2) * CX + kx];
+    Dft<CS, 1>::run(v);
+#pragma unroll
+    for (int s = 0; s < CS; ++s) At[s][k1 * P + kx] = v[s];
+  }
+  cl.sync();
+
+  // 2. y, local: twiddle W_NY^{-r k1}, then the NQ-point inverse along k1
+  //    for every column; outputs are rows p (y = CS p + r), in place
+  constexpr int CPR = kPlaneThreads / TQ;
+  constexpr int NRQ = (CX + CPR - 1) / CPR;
+  for (int rd = 0; rd < NRQ; ++rd) {
+    const int kx = rd * CPR + tid % CPR, t = tid / CPR;
+    const bool act = kx < CX;
+    float2 v[EQ];
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < EQ / R0Q; ++b)
+#pragma unroll
+        for (int qq = 0; qq < R0Q; ++qq) {
+          const int k1 = rr::stage_in<NQ, 0, EQ, TQ>(t, b, qq);
+          v[b * R0Q + qq] = cmul(A[k1 * P + kx], twr[k1]);
+        }
+    }
+    auto iy = [kx](int e) { return e * P + (kx < CX ? kx : 0); };
+    SmemStages<NQ, 1, EQ, TQ, 0, decltype(iy)>::run(v, A, twq, t, act, iy);
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < EQ / RLQ; ++b)
+#pragma unroll
+        for (int qq = 0; qq < RLQ; ++qq) A[rr::stage_in<NQ, SQ - 1, EQ, TQ>(t, b, qq) * P + kx] = v[b * RLQ + qq];
+    }
+    __syncthreads();
+  }
+
+  // 3. x C2R of every row to HBM (scale, addend, zero pad)
+  constexpr int RPR = kPlaneThreads / TX;
+  constexpr int NRX = (NQ + RPR - 1) / RPR;
+  for (int rd = 0; rd < NRX; ++rd) {
+    const int q = rd * RPR + tid / TX, t = tid % TX;
+    const bool act = q < NQ;
+    float2 *row = A + (act ? q : 0) * P;
+    float2 v[EX];
+    if (act) {
+      // Z'[k] = (X_k + conj X_{NH-k}) + i W^{-k} (X_k - conj X_{NH-k}); the
+      // imaginary parts of DC and Nyquist are ignored, as a C2R does
+#pragma unroll
+      for (int b = 0; b < EX / R0X; ++b)
+#pragma unroll
+        for (int qq = 0; qq < R0X; ++qq) {
+          const int k = rr::stage_in<NH, 0, EX, TX>(t, b, qq);
+          float2 x0 = row[k], x1 = row[NH - k];
+          if (k == 0) { x0.y = 0.f; x1.y = 0.f; }
+          x1.y = -x1.y;
+          const float2 e = cadd(x0, x1);
+          float2 w = post[k];
+          w.y = -w.y;
+          const float2 o = cmul(csub(x0, x1), w);
+          v[b * R0X + qq] = make_float2(e.x - o.y, e.y + o.x);
+        }
+    }
+    __syncthreads();  // the row's spectrum is read before the exchanges overwrite it
+    auto ix = [](int e) { return C::physx(e); };
+    SmemStages<NH, 1, EX, TX, 0, decltype(ix)>::run(v, row, twx, t, act, ix);
+    if (act) {
+      const long long ro = (long long)(CS * q + r) * a.rnxp;
+      float2 *orow = reinterpret_cast<float2 *>(dst + ro);
+      const float2 *arow = add ? reinterpret_cast<const float2 *>(add + ro) : nullptr;
+#pragma unroll
+      for (int b = 0; b < EX / RLX; ++b)
+#pragma unroll
+        for (int qq = 0; qq < RLX; ++qq) {
+          const int m = rr::stage_in<NH, SX - 1, EX, TX>(t, b, qq);
+          float2 x = cscale(v[b * RLX + qq], a.scale);
+          if (arow) x = cadd(x, arow[m]);
+          orow[m] = x;
+        }
+      if (t == 0) orow[NH] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();  // the row buffer is free for the next round
+  }
+}
+
+template <int NH, int NY, int CS>
+int launch_plane(const PlaneArgs &a, int dir, cudaStream_t s) {
+  using C = PlaneCfg<NH, NY, CS>;
+  const void *fn = dir < 0 ? (const void *)k_plane_xy_fwd<NH, NY, CS> : (const void *)k_plane_xy_inv<NH, NY, CS>;
+  int rc = func_smem(fn, C::smem);
+  if (rc) return rc;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(a.nplanes * CS));
+  cfg.blockDim = dim3(kPlaneThreads);
+  cfg.dynamicSmemBytes = C::smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (dir < 0) CRAVA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_plane_xy_fwd<NH, NY, CS>, a));
+  else CRAVA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_plane_xy_inv<NH, NY, CS>, a));
+  note_launch();
+  return CRAVA_GPU_OK;
+}
+
+}  // namespace
+
+bool plane_xy_supported(const Geom &g) {
+  return (g.nxp == 256 && g.nyp == 256) || (g.nxp == 128 && g.nyp == 128);
+}
+
+int plane_xy_tables(const Geom &g, float2 **twq, float2 **twy) {
+  *twq = *twy = nullptr;
+  if (!plane_xy_supported(g)) return CRAVA_GPU_OK;
+  const int ny = g.nyp, nq = g.nyp == 256 ? 64 : 64;
+  std::vector<float2> q(nq), y(ny);
+  for (int k = 0; k < nq; ++k) {
+    const double ang = -2.0 * M_PI * (double)k / (double)nq;
+    q[k] = make_float2((float)cos(ang), (float)sin(ang));
+  }
+  for (int k = 0; k < ny; ++k) {
+    const double ang = -2.0 * M_PI * (double)k / (double)ny;
+    y[k] = make_float2((float)cos(ang), (float)sin(ang));
+  }
+  CRAVA_CUDA_TRY(cudaMalloc(twq, sizeof(float2) * nq));
+  CRAVA_CUDA_TRY(cudaMalloc(twy, sizeof(float2) * ny));
+  CRAVA_CUDA_TRY(cudaMemcpy(*twq, q.data(), sizeof(float2) * nq, cudaMemcpyHostToDevice));
+  CRAVA_CUDA_TRY(cudaMemcpy(*twy, y.data(), sizeof(float2) * ny, cudaMemcpyHostToDevice));
+  return CRAVA_GPU_OK;
+}
+
+int plane_xy(const FftPlans &p, const float *src, float *dst, int dir, float scale, const float *addend,
+             cudaStream_t s) {
+  const Geom &g = p.g;
+  if (!plane_xy_supported(g) || !p.twq || !p.twy) return CRAVA_GPU_ERR_ARG;
+  PlaneArgs a{};
+  a.src = src ? src : dst;
+  a.dst = dst;
+  a.add = addend;
+  a.rnxp = g.rnxp;
+  a.nyp = g.nyp;
+  a.nplanes = g.nzp;
+  a.scale = scale;
+  a.twx = p.x.tw;
+  a.post = p.xpost;
+  a.twq = p.twq;
+  a.twy = p.twy;
+  if (g.nxp == 256 && g.nyp == 256) return launch_plane<128, 256, 4>(a, dir, s);
+  return launch_plane<64, 128, 2>(a, dir, s);
+}
+
+}  // namespace crava

@@ -279,7 +279,11 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
  * transforms of different grids overlap on that many streams; rows_x: the x
  * pass of an even nxp (-1 built-in, 0 in-place pass, 1 register-resident
  * pass where nxp / 2 is 64..512).  All these choices give the same values
- * bit for bit.  kappa_refine (mixed form only, >= 0): an inverted bin whose
+ * bit for bit.  xy_fused: the x and y passes as one thread-block-cluster
+ * kernel where the geometry has one (256x256 and 128x128 planes; -1
+ * built-in = on, 0 off, 1 on); it factorises the y transform differently,
+ * so it agrees with the separate passes to float rounding, not bit for
+ * bit.  kappa_refine (mixed form only, >= 0): an inverted bin whose
  * FP32 factor has (max L_ii / min L_ii)^2 above it takes one FP64
  * refinement step (0 refines every bin).  No counterpart in the reference
  * (FFTW plans are fixed there). */
@@ -291,6 +295,7 @@ typedef struct crava_gpu_tuning {
   int lanes;   /* streams the unit's independent transforms run on (1..4) */
   int rows_x;
   float kappa_refine;
+  int xy_fused;
 } crava_gpu_tuning;
 int crava_gpu_get_tuning(crava_gpu_ctx *ctx, crava_gpu_tuning *out);
 int crava_gpu_set_tuning(crava_gpu_ctx *ctx, const crava_gpu_tuning *t);

@@ -162,3 +162,46 @@ def test_batch_rejects_in_place_vintages():
     g = _dev(case)
     with pytest.raises(api.CravaGpuError):
         api.Batch([dict(ctx=ctx, src=g, dst=g, precision=api.FP64)])
+
+
+@pytest.mark.parametrize("shape", [(256, 256, 16), (128, 128, 24), (256, 256, 512)])
+def test_fused_xy_pass_matches_numpy_and_separate_passes(shape):
+    """The x and y passes as one cluster kernel (xy_fused) against numpy
+    and against the separate passes (float rounding: the y transform is
+    factorised differently), forward and inverse, in place."""
+    nx, ny, nz = shape
+    case = synth.make_case(nx, ny, nz, (10.0,), 0.1, seed=12)
+    ctx = api.Context(case)
+    g = case.data[0]
+    ref = np.fft.rfftn(g[..., :nx].astype(np.float64), axes=(0, 1, 2)) / np.sqrt(nx * ny * nz)
+    res = {}
+    for xy in (1, 0):
+        ctx.set_tuning(-1, -1, 0, 2, -1, None, xy)
+        t = api.to_device(g)
+        ctx.fft_r2c(t, api.DATA)
+        out = api.complex_view(t.cpu().numpy(), nx).copy()
+        assert rel(out, ref) < 2e-6, xy
+        ctx.fft_c2r(t, api.DATA)
+        back = t.cpu().numpy()
+        assert rel(back[..., :nx], g[..., :nx]) < 2e-6, xy
+        assert np.all(back[..., nx:] == 0.0)  # the padding floats
+        res[xy] = (out, back)
+    assert rel(res[1][0], res[0][0]) < 1e-6 and rel(res[1][1][..., :nx], res[0][1][..., :nx]) < 1e-6
+
+
+def test_fused_xy_unit_out_of_place_matches_separate_passes():
+    """The whole out-of-place unit (forward transforms read the inputs and
+    write the work grids) with and without the fused x + y pass."""
+    case = synth.make_case(128, 128, 64, (0.0, 15.0, 30.0), 0.1, seed=13)
+    ctx = api.Context(case, precision=api.FP64)
+    src = _dev(case)
+    outs = {}
+    for xy in (1, 0):
+        ctx.set_tuning(-1, -1, 0, 2, -1, None, xy)
+        dst = _dev(case)
+        ctx.posterior_unit_oop(src, dst, api.FP64)
+        outs[xy] = [t.cpu().numpy() for t in dst[0] + dst[1] + dst[2]]
+    for a, b in zip(outs[1], outs[0]):
+        assert rel(a[..., :128], b[..., :128]) < 1e-5
+    for t, h in zip(src[0] + src[1] + src[2] + [src[3]], case.mu + case.data + case.cov + [case.err_corr]):
+        assert np.array_equal(t.cpu().numpy(), h)  # inputs untouched
