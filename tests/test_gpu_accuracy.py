@@ -111,13 +111,18 @@ def _report(case, label):
     names = ["mu_alpha", "mu_beta", "mu_rho"] + [f"resid_{l}" for l in range(case.ntheta)] + \
             ["cov_aa", "cov_bb", "cov_rr", "cov_ab", "cov_ar", "cov_br"]
     rows = {}
+    refined = 0
     for prec, tag in [(api.FP64, "fp64"), (api.MIXED, "mixed"), (api.FP32, "fp32")]:
-        _, _, mu, res, cov = _run(case, prec)
+        ctx, _, mu, res, cov = _run(case, prec)
+        if prec == api.MIXED:
+            refined = ctx.stats().refined_bins
         for name, a, b in zip(names, mu + res + cov, ref):
             rl2 = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
             ma = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
             rows.setdefault(name, {})[tag] = (rl2, ma)
-    print(f"\n{label}: per-output error against the FP64 oracle (rel L2 / max-abs over max-ref)")
+    n_inv = int(ctx.kz_tables()[4].sum()) * case.nyp * case.cnxp
+    print(f"\n{label}: per-output error against the FP64 oracle (rel L2 / max-abs over max-ref); "
+          f"mixed form refined {refined} of {n_inv} inverted bins")
     print(f"{'output':10s} {'fp64':>22s} {'mixed':>22s} {'fp32':>22s}")
     for name in names:
         cells = "".join(f" {rows[name][t][0]:10.2e}/{rows[name][t][1]:9.2e}" for t in ("fp64", "mixed", "fp32"))
