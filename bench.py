@@ -45,6 +45,24 @@ METRIC = "posterior cells/s at 256x256x512x5 angles, mixed vs FP64 form; % HBM r
 ANGLES5 = (0.0, 10.0, 20.0, 30.0, 40.0)
 
 
+FP64_NOMINAL_TFLOPS = 148 * 128 * 1.965e9 / 1e12
+
+
+def solve_flops_per_inverted_bin(nt):
+    """FP64 flops of the square-root form on one inverted bin (an FMA counts
+    2): M built from the per-kz constants (A S rows, (A S A^T)_lm, the
+    complex W_lm B + lambda E_lm), the Cholesky, four forward substitutions
+    (three columns of K S and z), the columns of K S, the Gram entries of
+    S - Y^H Y, the prior-mean residual, Y^H z and the posterior mean and
+    residual."""
+    npair = nt * (nt + 1) // 2
+    build = 15 * nt + 5 * npair + 6 * npair + nt
+    chol = sum(8 * j + 2 for i in range(nt) for j in range(i)) + sum(4 * i + 2 for i in range(nt))
+    fwd = 8 * nt * (nt - 1) // 2 + 2 * nt
+    gram = 3 * 4 * nt + (1 + 2) * 8 * nt
+    return build + chol + 4 * fwd + 3 * 7 * nt + gram + 20 * nt + 3 * 8 * nt + (6 + 20 * nt)
+
+
 def hbm_peak():
     """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json
     (written per pod by the driver), else the pool's earlier measurement."""
@@ -90,6 +108,9 @@ def parse():
     ap.add_argument("--profile-fused", type=int, default=0)
     ap.add_argument("--profile-reps", type=int, default=3)
     ap.add_argument("--profile-ntheta", type=int, default=5)
+    ap.add_argument("--profile-lanes", type=int, default=1,
+                    help="transform streams in the profile run (1: per-launch events time one kernel each)")
+    ap.add_argument("--profile-xy", type=int, default=-1, help="fused x + y pass: -1 built-in, 0 off, 1 on")
     return ap.parse_args()
 
 
@@ -692,6 +713,14 @@ def run_own(args):
     # the other solve form, timed the same way
     fp64_value = value if prec == api.FP64 else None
     mixed_value = value if prec == api.MIXED else None
+    solve_ms = {}
+
+    def solve_time(pr):
+        return pr["posterior_solve"][1] / pr["posterior_solve"][0] if "posterior_solve" in pr else None
+
+    tag = {api.FP64: "fp64", api.MIXED: "mixed", api.FP32: "fp32"}
+    solve_ms[tag[prec]] = solve_time(prof)
+    refined = None
     if not args.no_fp64_compare:
         other = api.MIXED if prec == api.FP64 else api.FP64
         ms_o, _, _ = timed_steps(other, max(10, args.steps // 4), False)
@@ -700,6 +729,16 @@ def run_own(args):
             fp64_value = v_o
         else:
             mixed_value = v_o
+        # the other form's solve time from the same one-stream profiling pass
+        ctx.set_tuning(tuned.cols_y_tile, tuned.cols_z_tile, tuned.fused, 1, tuned.rows_x, tuned.kappa_refine,
+                       tuned.xy_fused)
+        _, _, prof_o = timed_steps(other, max(10, min(args.steps, 30)), True)
+        ctx.set_tuning(tuned.cols_y_tile, tuned.cols_z_tile, tuned.fused, tuned.lanes, tuned.rows_x,
+                       tuned.kappa_refine, tuned.xy_fused)
+        solve_ms[tag[other]] = solve_time(prof_o)
+    if api.MIXED in (prec,) or not args.no_fp64_compare:
+        ctx.posterior_unit_oop(src, dst, api.MIXED)
+        refined = ctx.stats().refined_bins
 
     # e2e through the host-buffer entry points (pinned host memory): every
     # step uploads its 10+nt input grids and downloads its 9+nt outputs.
@@ -826,6 +865,23 @@ def run_own(args):
     unit_roof = {"bound": "hbm", "algorithmic_bytes": b_unit, "ms": round(ms, 4),
                  "achieved": round(b_unit / (ms * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
                  "frac": round(b_unit / (ms * 1e-3) / 1e9 / peak, 4), "peak_source": peak_source}
+    # the solve stage of both forms (one-stream profiling pass): time, the
+    # mixed / FP64 speed ratio, the unit's bound from it, and the FP64
+    # form's arithmetic rate on the analytic flop count of an inverted bin
+    n_inv_bins = int(ctx.kz_tables()[4].sum()) * (nxp // 2 + 1) * nyp
+    solve_stage = {"ms": {k: (round(v, 4) if v else None) for k, v in solve_ms.items()},
+                   "inverted_bins": n_inv_bins, "mixed_refined_bins": refined}
+    if solve_ms.get("fp64") and solve_ms.get("mixed"):
+        solve_stage["mixed_over_fp64_speed"] = round(solve_ms["fp64"] / solve_ms["mixed"], 4)
+        solve_stage["unit_bound_any_solve"] = round(ms / (ms - solve_ms["fp64"]), 4)
+    if solve_ms.get("fp64"):
+        fl = solve_flops_per_inverted_bin(nt) * n_inv_bins
+        tf = fl / (solve_ms["fp64"] * 1e-3) / 1e12
+        solve_stage["fp64_flops_per_inverted_bin"] = solve_flops_per_inverted_bin(nt)
+        solve_stage["fp64_tflops"] = round(tf, 2)
+        solve_stage["fp64_frac_of_nominal"] = round(tf / FP64_NOMINAL_TFLOPS, 4)
+        solve_stage["fp64_peak_note"] = ("nominal FP64 vector rate 148 SMs x 128 flop/clk x 1.965 GHz "
+                                         "(no measured FP64 peak on this pool)")
     kernels = {k: {"launches": v[0], "ms": round(v[1], 4),
                    "GB/s": round(v[2] / (v[1] / v[0] * 1e-3) / 1e9, 1)} for k, v in prof.items()}
 
@@ -869,6 +925,7 @@ def run_own(args):
         "fp64_form_value": fp64_value,
         "mixed_form_value": mixed_value,
         "mixed_over_fp64": (mixed_value / fp64_value) if (mixed_value and fp64_value) else None,
+        "solve_stage": solve_stage,
         "simulation": sim,
         "batch": batch,
         "adjoint": adjoint,
@@ -965,7 +1022,9 @@ def run_profile_unit(args):
     nt = args.profile_ntheta
     case = synth.make_case(nx, ny, nz, tuple(10.0 * i for i in range(nt)), 0.1, seed=2)
     ctx = api.Context(case)
-    ctx.set_fused(bool(args.profile_fused))
+    t = ctx.tuning()
+    ctx.set_tuning(t.cols_y_tile, t.cols_z_tile, int(bool(args.profile_fused)), args.profile_lanes, t.rows_x,
+                   t.kappa_refine, args.profile_xy)
     d = lambda gs: [api.to_device(g) for g in gs]
     src = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
     dst = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
@@ -973,8 +1032,8 @@ def run_profile_unit(args):
     for _ in range(args.profile_reps):
         ctx.posterior_unit_oop(src, dst, args.profile_precision)
         st = ctx.stats()
-        print("forward %.3f solve %.3f inverse %.3f total %.3f ms" % (
-            st.ms_forward, st.ms_solve, st.ms_inverse, st.ms_total))
+        print("forward %.3f solve %.3f inverse %.3f total %.3f ms refined %d" % (
+            st.ms_forward, st.ms_solve, st.ms_inverse, st.ms_total, st.refined_bins))
     for k, v in ctx.profile().items():
         per = v[1] / v[0]
         print(f"{k:18s} launches {v[0]:4d}  {per:.4f} ms/launch  {v[2] / (per * 1e-3) / 1e9:8.1f} GB/s")

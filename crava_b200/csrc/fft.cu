@@ -818,7 +818,10 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
     r.tw = lp.tw;
     if (r.nlines >= (1LL << 31)) return CRAVA_GPU_ERR_ARG;
     const bool flat = outer_stride == ninner;
-    const bool vec = flat && (es % 2 == 0) && (reinterpret_cast<uintptr_t>(data) % 16 == 0);
+    // 16-byte accesses need the two lines of a thread adjacent and aligned:
+    // lengths whose threads hold two lines (CPT 2), flat lines, even stride
+    const bool two = (n == 64 || n == 512);  // RrCols<n>::CPT == 2
+    const bool vec = two && flat && (es % 2 == 0) && (reinterpret_cast<uintptr_t>(data) % 16 == 0);
     const dim3 g2((unsigned)((r.nlines + kRrTX - 1) / kRrTX));
 #define CRAVA_COLS_RR(NN)                                                                           \
     if (n == NN) {                                                                                  \
@@ -890,6 +893,8 @@ bool cols_tunable(int n) {
 }
 
 bool cols_rr(int n) { return rr::supported(n); }
+static_assert(RrCols<64>::CPT == 2 && RrCols<512>::CPT == 2 && RrCols<128>::CPT == 1 && RrCols<256>::CPT == 1,
+              "the 16-byte path of k_cols_rr is chosen for the lengths whose threads hold two lines");
 
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;

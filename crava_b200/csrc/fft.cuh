@@ -31,7 +31,8 @@ struct FftPlans {
   // length is 64..512), 0 the in-place pass, 1 register-resident
   int rows_x = -1;
   // x and y passes in one cluster kernel (plane.cu) where the geometry has
-  // one: -1 default (on), 0 off, 1 on; its twiddle tables
+  // one: -1 default (off: measured slower than the separate
+  // register-resident passes), 0 off, 1 on; its twiddle tables
   int plane_xy = -1;
   float2 *twq = nullptr, *twy = nullptr;
 };
@@ -44,7 +45,7 @@ int plane_xy_tables(const Geom &g, float2 **twq, float2 **twy);
 int plane_xy(const FftPlans &p, const float *src, float *dst, int dir, float scale, const float *addend,
              cudaStream_t s);
 // Whether the transforms of these plans use the fused x + y pass.
-inline bool use_plane_xy(const FftPlans &p) { return p.plane_xy != 0 && p.twq && p.twy; }
+inline bool use_plane_xy(const FftPlans &p) { return p.plane_xy == 1 && p.twq && p.twy; }
 
 // Whether length n has compiled column kernels (tile choices 0, 8, 16).
 bool cols_tunable(int n);

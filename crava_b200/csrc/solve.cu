@@ -224,26 +224,31 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
 
 // Square-root form (solve_bin.cuh): the FP64 and mixed forms.  One kz
 // plane per CTA: the CTA first stages the plane's per-kz constants of M in
-// shared memory.  Per thread in shared memory, one entry column per
-// thread: FP64 form the factor and the first two columns of Y = L^-1 K S;
-// mixed form the FP32 factor, two FP32 columns of Y and the FP64 prior-mean
-// residual (used by the refinement step).
-template <int NT, int PREC>
+// shared memory.  The factor lives either in shared memory, one entry
+// column per thread (LREG false), or in registers (LREG true); the first
+// two columns of Y = L^-1 K S (and, mixed form, the FP64 prior-mean
+// residual used by the refinement step) are in shared memory.  A factor in
+// shared memory costs about 180 16-byte accesses per inverted bin at five
+// angles, which bounds that shape by the SM's shared-memory bandwidth; in
+// registers it costs occupancy instead.
+template <int NT, int PREC, int NTH, bool LREG>
 struct SqSmem {
   static constexpr int NP = NT * (NT + 1) / 2;
   static constexpr size_t kconst = (sizeof(sb::KzConst<NT>) + 15) / 16 * 16;
   static constexpr size_t per_thread =
-      PREC == 0 ? sizeof(double2) * (NP + 2 * NT) : sizeof(double2) * NT + sizeof(float2) * (NP + 2 * NT);
-  static constexpr size_t bytes = kconst + per_thread * kThreads;
+      PREC == 0 ? sizeof(double2) * ((LREG ? 0 : NP) + 2 * NT)
+                : sizeof(double2) * NT + sizeof(float2) * ((LREG ? 0 : NP) + 2 * NT);
+  static constexpr size_t bytes = kconst + per_thread * NTH;
 };
 
-template <int NT, int PREC, int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) k_solve_sq(SolveArgs a) {
+template <int NT, int PREC, int NTH, int MINB, bool LREG>
+__global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
+  using SM = SqSmem<NT, PREC, NTH, LREG>;
   extern __shared__ double2 sq_sm[];
   auto &kc = *reinterpret_cast<sb::KzConst<NT> *>(sq_sm);
-  char *area = reinterpret_cast<char *>(sq_sm) + SqSmem<NT, PREC>::kconst;
+  char *area = reinterpret_cast<char *>(sq_sm) + SM::kconst;
   const int slot = (int)(blockIdx.x / a.bpp);
-  const long long off = (long long)(blockIdx.x % a.bpp) * blockDim.x + threadIdx.x;
+  const long long off = (long long)(blockIdx.x % a.bpp) * NTH + threadIdx.x;
   const int k = a.t.order ? a.t.order[slot] : slot;
   const bool inv = a.t.inv[k] != 0;
   const long long o = (long long)k * NT;
@@ -267,17 +272,30 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve_sq(SolveArgs a) {
   bool solved, fin = true, refined = false;
   if (PREC == 0) {
     double2 *base = reinterpret_cast<double2 *>(area) + threadIdx.x;
-    const sb::SmemTri<double2, kThreads> L{base};
-    const sb::SmemTri<double2, kThreads> Y{base + kThreads * SqSmem<NT, PREC>::NP};
-    solved = sb::solve_bin_fp64_sq<NT>(L, Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, &fin);
+    if (LREG) {
+      double2 L[SM::NP];
+      const sb::SmemTri<double2, NTH> Y{base};
+      solved = sb::solve_bin_fp64_sq<NT>(&L[0], Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, &fin);
+    } else {
+      const sb::SmemTri<double2, NTH> L{base};
+      const sb::SmemTri<double2, NTH> Y{base + NTH * SM::NP};
+      solved = sb::solve_bin_fp64_sq<NT>(L, Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, &fin);
+    }
   } else {
     double2 *vbase = reinterpret_cast<double2 *>(area) + threadIdx.x;
-    float2 *fbase = reinterpret_cast<float2 *>(reinterpret_cast<double2 *>(area) + kThreads * NT) + threadIdx.x;
-    const sb::SmemTri<double2, kThreads> V{vbase};
-    const sb::SmemTri<float2, kThreads> Lf{fbase};
-    const sb::SmemTri<float2, kThreads> Yf{fbase + kThreads * SqSmem<NT, PREC>::NP};
-    solved = sb::solve_bin_mixed_sq<NT>(Lf, Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x), fabs((double)ec.x),
-                                        a.g, idx, &fin, &refined);
+    float2 *fbase = reinterpret_cast<float2 *>(reinterpret_cast<double2 *>(area) + NTH * NT) + threadIdx.x;
+    const sb::SmemTri<double2, NTH> V{vbase};
+    if (LREG) {
+      float2 Lf[SM::NP];
+      const sb::SmemTri<float2, NTH> Yf{fbase};
+      solved = sb::solve_bin_mixed_sq<NT>(&Lf[0], Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x),
+                                          fabs((double)ec.x), a.g, idx, &fin, &refined);
+    } else {
+      const sb::SmemTri<float2, NTH> Lf{fbase};
+      const sb::SmemTri<float2, NTH> Yf{fbase + NTH * SM::NP};
+      solved = sb::solve_bin_mixed_sq<NT>(Lf, Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x),
+                                          fabs((double)ec.x), a.g, idx, &fin, &refined);
+    }
   }
   if (!solved) {
     // the reference keeps the prior (src/crava.cpp:1109-1111): the mean and
@@ -301,16 +319,17 @@ __global__ void __launch_bounds__(kThreads, MINB) k_solve_sq(SolveArgs a) {
   }
 }
 
-template <int PREC, int MINB>
-int launch_solve_sq(const SolveArgs &a, int nt, cudaStream_t s) {
+template <int PREC, int NTH, int MINB, bool LREG>
+int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
+  a.bpp = (a.plane + NTH - 1) / NTH;
   dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
   int rc;
-#define CRAVA_SQ_CASE(N)                                                                        \
-  case N: {                                                                                     \
-    const size_t smem = SqSmem<N, PREC>::bytes;                                                 \
-    if ((rc = func_smem((const void *)k_solve_sq<N, PREC, MINB>, smem))) return rc;             \
-    k_solve_sq<N, PREC, MINB><<<grd, kThreads, smem, s>>>(a);                                   \
-    break;                                                                                      \
+#define CRAVA_SQ_CASE(N)                                                                          \
+  case N: {                                                                                       \
+    const size_t smem = SqSmem<N, PREC, NTH, LREG>::bytes;                                        \
+    if ((rc = func_smem((const void *)k_solve_sq<N, PREC, NTH, MINB, LREG>, smem))) return rc;    \
+    k_solve_sq<N, PREC, NTH, MINB, LREG><<<grd, NTH, smem, s>>>(a);                               \
+    break;                                                                                        \
   }
   switch (nt) {
     CRAVA_SQ_CASE(1) CRAVA_SQ_CASE(2) CRAVA_SQ_CASE(3) CRAVA_SQ_CASE(4)
@@ -320,6 +339,32 @@ int launch_solve_sq(const SolveArgs &a, int nt, cudaStream_t s) {
 #undef CRAVA_SQ_CASE
   CRAVA_LAUNCH_CHECK();
   return CRAVA_GPU_OK;
+}
+
+// Launch shape of the square-root solve: 0 the factor in shared memory
+// (256 threads, two blocks per SM), 1 in registers with 128 threads and
+// three blocks per SM (up to 170 registers), 2 in registers with 256
+// threads and one block per SM (up to 255 registers), 3 in registers with
+// 128 threads and four blocks per SM (up to 128 registers).
+// CRAVA_SOLVE_SHAPE overrides the default for measurements.
+static int solve_shape() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("CRAVA_SOLVE_SHAPE");
+    v = e ? atoi(e) : 1;
+    if (v < 0 || v > 3) v = 1;
+  }
+  return v;
+}
+
+template <int PREC>
+int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
+  switch (solve_shape()) {
+    case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);
+    case 2: return launch_solve_sq<PREC, 256, 1, true>(a, nt, s);
+    case 3: return launch_solve_sq<PREC, 128, 4, true>(a, nt, s);
+    default: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
+  }
 }
 
 template <int PREC, int MINB>
@@ -456,9 +501,9 @@ int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g
   SolveArgs a;
   a.c = c; a.g = g; a.t = t; a.csize = csize; a.plane = plane; a.counters = counters;
   a.bpp = (plane + kThreads - 1) / kThreads;
-  // the square-root form (one kz plane per CTA), two blocks per SM
-  if (precision == CRAVA_SOLVE_FP64) return launch_solve_sq<0, 2>(a, c.nt, s);
-  if (precision == CRAVA_SOLVE_MIXED) return launch_solve_sq<1, 2>(a, c.nt, s);
+  // the square-root form (one kz plane per CTA)
+  if (precision == CRAVA_SOLVE_FP64) return launch_solve_sq_shape<0>(a, c.nt, s);
+  if (precision == CRAVA_SOLVE_MIXED) return launch_solve_sq_shape<1>(a, c.nt, s);
   return CRAVA_GPU_ERR_ARG;
 }
 
