@@ -345,14 +345,16 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
 // (256 threads, two blocks per SM), 1 in registers with 128 threads and
 // three blocks per SM (up to 170 registers), 2 in registers with 256
 // threads and one block per SM (up to 255 registers), 3 in registers with
-// 128 threads and four blocks per SM (up to 128 registers).
-// CRAVA_SOLVE_SHAPE overrides the default for measurements.
+// 128 threads and four blocks per SM (up to 128 registers).  Measured at
+// 256x256x512x5 (B200, one stream): FP64 / mixed 1.34 / 1.14 ms (shape 0),
+// 1.34 / 1.23 (1), 1.76 / 1.74 (2), 1.17 / 1.06 (3); shape 3 is the
+// default.  CRAVA_SOLVE_SHAPE overrides it for measurements.
 static int solve_shape() {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("CRAVA_SOLVE_SHAPE");
-    v = e ? atoi(e) : 1;
-    if (v < 0 || v > 3) v = 1;
+    v = e ? atoi(e) : 3;
+    if (v < 0 || v > 3) v = 3;
   }
   return v;
 }
@@ -361,9 +363,9 @@ template <int PREC>
 int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
   switch (solve_shape()) {
     case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);
+    case 1: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
     case 2: return launch_solve_sq<PREC, 256, 1, true>(a, nt, s);
-    case 3: return launch_solve_sq<PREC, 128, 4, true>(a, nt, s);
-    default: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
+    default: return launch_solve_sq<PREC, 128, 4, true>(a, nt, s);
   }
 }
 
