@@ -22,6 +22,7 @@
 
 #include <vector>
 
+#include "fft_core.cuh"
 #include "solve.cuh"
 #include "solve_bin.cuh"
 
@@ -269,17 +270,18 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
   }
   const sb::Sym3d S = sb::prior_exact(c6, a.c.var0);
   const float2 ec = a.g.err[idx];
+  const sb::GlobalIn gin{&a.g, idx};
   bool solved, fin = true, refined = false;
   if (PREC == 0) {
     double2 *base = reinterpret_cast<double2 *>(area) + threadIdx.x;
     if (LREG) {
       double2 L[SM::NP];
       const sb::SmemTri<double2, NTH> Y{base};
-      solved = sb::solve_bin_fp64_sq<NT>(&L[0], Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, &fin);
+      solved = sb::solve_bin_fp64_sq<NT>(&L[0], Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, gin, &fin);
     } else {
       const sb::SmemTri<double2, NTH> L{base};
       const sb::SmemTri<double2, NTH> Y{base + NTH * SM::NP};
-      solved = sb::solve_bin_fp64_sq<NT>(L, Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, &fin);
+      solved = sb::solve_bin_fp64_sq<NT>(L, Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, gin, &fin);
     }
   } else {
     double2 *vbase = reinterpret_cast<double2 *>(area) + threadIdx.x;
@@ -289,12 +291,12 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
       float2 Lf[SM::NP];
       const sb::SmemTri<float2, NTH> Yf{fbase};
       solved = sb::solve_bin_mixed_sq<NT>(&Lf[0], Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x),
-                                          fabs((double)ec.x), a.g, idx, &fin, &refined);
+                                          fabs((double)ec.x), a.g, idx, gin, &fin, &refined);
     } else {
       const sb::SmemTri<float2, NTH> Lf{fbase};
       const sb::SmemTri<float2, NTH> Yf{fbase + NTH * SM::NP};
       solved = sb::solve_bin_mixed_sq<NT>(Lf, Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x),
-                                          fabs((double)ec.x), a.g, idx, &fin, &refined);
+                                          fabs((double)ec.x), a.g, idx, gin, &fin, &refined);
     }
   }
   if (!solved) {
@@ -317,6 +319,142 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
       if (br && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&a.counters->refined, (unsigned long long)__popc(br));
     }
   }
+}
+
+// The square-root solve with the bin inputs staged ahead of the compute.
+// Each thread runs BPT bins of its kz plane in turn; while bin j computes,
+// the 10 + NT input spectra of bin j + 1 travel by cp.async into the
+// thread's own slot of a two-deep staging buffer in shared memory (a
+// band-gated plane stages only its six covariance spectra), and the bin's
+// inputs are read from there (the end-of-bin re-reads included) instead of
+// from global memory: the loads that stalled the one-bin-per-thread kernel
+// overlap the FP64 work of the previous bin.  Only the thread that staged a
+// slot reads it, so no block barrier is needed between bins.  The factor is
+// in registers; the first two columns of Y (FP64 form) or the FP64
+// prior-mean residual and two FP32 columns of Y (mixed form) are in shared
+// memory.
+template <int NT, int PREC, int NTH>
+struct PfSmem {
+  static constexpr int NIN = 10 + NT;
+  static constexpr size_t kconst = (sizeof(sb::KzConst<NT>) + 15) / 16 * 16;
+  static constexpr size_t scratch =
+      PREC == 0 ? sizeof(double2) * 2 * NT : sizeof(double2) * NT + sizeof(float2) * 2 * NT;
+  static constexpr size_t bytes = kconst + (scratch + sizeof(float2) * 2 * NIN) * NTH;
+};
+
+template <int NT, int PREC, int NTH, int MINB, int BPT>
+__global__ void __launch_bounds__(NTH, MINB) k_solve_pf(SolveArgs a) {
+  using SM = PfSmem<NT, PREC, NTH>;
+  constexpr int NIN = SM::NIN;
+  extern __shared__ double2 pf_sm[];
+  auto &kc = *reinterpret_cast<sb::KzConst<NT> *>(pf_sm);
+  char *area = reinterpret_cast<char *>(pf_sm) + SM::kconst;
+  double2 *dscr = reinterpret_cast<double2 *>(area) + threadIdx.x;
+  float2 *stage = reinterpret_cast<float2 *>(area + SM::scratch * NTH) + threadIdx.x;  // [2][NIN][NTH]
+  const int slot = (int)(blockIdx.x / a.bpp);
+  const long long base = (long long)(blockIdx.x % a.bpp) * NTH * BPT;
+  const int k = a.t.order ? a.t.order[slot] : slot;
+  const bool inv = a.t.inv[k] != 0;
+  const long long o = (long long)k * NT;
+  const long long pbase = (long long)k * a.plane;
+  if (inv) sb::kz_const_fill<NT>(kc, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, threadIdx.x);
+
+  auto issue = [&](int j) {
+    const long long off = base + (long long)j * NTH + threadIdx.x;
+    if (off < a.plane) {
+      const long long idx = pbase + off;
+      float2 *dst = stage + (j & 1) * NIN * NTH;
+      if (inv) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) cp_async8(dst + q * NTH, a.g.mu[q] + idx);
+#pragma unroll
+        for (int l = 0; l < NT; ++l) cp_async8(dst + (3 + l) * NTH, a.g.data[l] + idx);
+        cp_async8(dst + (9 + NT) * NTH, a.g.err + idx);
+      }
+#pragma unroll
+      for (int t = 0; t < 6; ++t) cp_async8(dst + (3 + NT + t) * NTH, a.g.cov[t] + idx);
+    }
+    cp_async_commit();
+  };
+  issue(0);
+  __syncthreads();  // the per-kz constants
+  for (int j = 0; j < BPT; ++j) {
+    if (j + 1 < BPT) issue(j + 1);
+    else cp_async_commit();  // an empty group keeps the wait count uniform
+    cp_async_wait<1>();      // bin j has landed in its slot
+    const long long off = base + (long long)j * NTH + threadIdx.x;
+    if (off >= a.plane) continue;
+    const long long idx = pbase + off;
+    const sb::StagedIn<NT, NTH> in{stage + (j & 1) * NIN * NTH};
+    float2 c6[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c6[t] = in.cov(t);
+    if (!inv) {
+      sb::prior_only<PREC>(a.c, c6);
+      bool nonfinite = false;
+#pragma unroll
+      for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
+      if (a.counters) sb::count(a.counters, false, nonfinite);
+      continue;
+    }
+    const sb::Sym3d S = sb::prior_exact(c6, a.c.var0);
+    const float2 ec = in.err();
+    bool solved, fin = true, refined = false;
+    if (PREC == 0) {
+      double2 L[NT * (NT + 1) / 2];
+      const sb::SmemTri<double2, NTH> Y{dscr};
+      solved = sb::solve_bin_fp64_sq<NT>(&L[0], Y, a.c, kc, S, fabs((double)ec.x), a.g, idx, in, &fin);
+    } else {
+      float2 Lf[NT * (NT + 1) / 2];
+      const sb::SmemTri<double2, NTH> V{dscr};
+      const sb::SmemTri<float2, NTH> Yf{reinterpret_cast<float2 *>(reinterpret_cast<double2 *>(area) + NTH * NT) +
+                                        threadIdx.x};
+      solved = sb::solve_bin_mixed_sq<NT>(&Lf[0], Yf, V, a.c, kc, S, a.c.kappa_refine, fabsf(ec.x),
+                                          fabs((double)ec.x), a.g, idx, in, &fin, &refined);
+    }
+    if (!solved) {
+      // the reference keeps the prior (src/crava.cpp:1109-1111)
+      sb::prior_only<PREC>(a.c, c6);
+#pragma unroll
+      for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; fin &= sb::fin2(c6[t]); }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) fin &= sb::fin2(in.mu(q));
+#pragma unroll
+      for (int l = 0; l < NT; ++l) fin &= sb::fin2(in.d(l));
+    }
+    if (a.counters) {
+      sb::count(a.counters, !solved, !fin);
+      if (PREC == 1) {
+        const unsigned m = __activemask();
+        const unsigned br = __ballot_sync(m, refined);
+        if (br && (threadIdx.x & 31) == __ffs(m) - 1)
+          atomicAdd(&a.counters->refined, (unsigned long long)__popc(br));
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+template <int PREC, int NTH, int MINB, int BPT>
+int launch_solve_pf(SolveArgs a, int nt, cudaStream_t s) {
+  a.bpp = (a.plane + (long long)NTH * BPT - 1) / ((long long)NTH * BPT);
+  dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
+  int rc;
+#define CRAVA_PF_CASE(N)                                                                          \
+  case N: {                                                                                       \
+    const size_t smem = PfSmem<N, PREC, NTH>::bytes;                                              \
+    if ((rc = func_smem((const void *)k_solve_pf<N, PREC, NTH, MINB, BPT>, smem))) return rc;     \
+    k_solve_pf<N, PREC, NTH, MINB, BPT><<<grd, NTH, smem, s>>>(a);                                \
+    break;                                                                                        \
+  }
+  switch (nt) {
+    CRAVA_PF_CASE(1) CRAVA_PF_CASE(2) CRAVA_PF_CASE(3) CRAVA_PF_CASE(4)
+    CRAVA_PF_CASE(5) CRAVA_PF_CASE(6) CRAVA_PF_CASE(7) CRAVA_PF_CASE(8)
+    default: return CRAVA_GPU_ERR_ARG;
+  }
+#undef CRAVA_PF_CASE
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
 }
 
 template <int PREC, int NTH, int MINB, bool LREG>
@@ -345,7 +483,9 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
 // (256 threads, two blocks per SM), 1 in registers with 128 threads and
 // three blocks per SM (up to 170 registers), 2 in registers with 256
 // threads and one block per SM (up to 255 registers), 3 in registers with
-// 128 threads and four blocks per SM (up to 128 registers).  Measured at
+// 128 threads and four blocks per SM (up to 128 registers); 4 and 5 the
+// pipelined kernel (k_solve_pf) with 128 threads, four blocks per SM and 4
+// or 8 bins per thread.  Measured at
 // 256x256x512x5 (B200, one stream): FP64 / mixed 1.34 / 1.14 ms (shape 0),
 // 1.34 / 1.23 (1), 1.76 / 1.74 (2), 1.17 / 1.06 (3); shape 3 is the
 // default.  CRAVA_SOLVE_SHAPE overrides it for measurements.
@@ -354,7 +494,7 @@ static int solve_shape() {
   if (v < 0) {
     const char *e = getenv("CRAVA_SOLVE_SHAPE");
     v = e ? atoi(e) : 3;
-    if (v < 0 || v > 3) v = 3;
+    if (v < 0 || v > 5) v = 3;
   }
   return v;
 }
@@ -365,6 +505,8 @@ int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
     case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);
     case 1: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
     case 2: return launch_solve_sq<PREC, 256, 1, true>(a, nt, s);
+    case 4: return launch_solve_pf<PREC, 128, 4, 4>(a, nt, s);
+    case 5: return launch_solve_pf<PREC, 128, 4, 8>(a, nt, s);
     default: return launch_solve_sq<PREC, 128, 4, true>(a, nt, s);
   }
 }

@@ -677,14 +677,33 @@ __device__ __forceinline__ void bwd_sub_rd(LA L, T2 *x) {
   }
 }
 
-// v = d - K mu in double, from the bin's spectra in global memory.
-template <int NT>
-__device__ __forceinline__ void prior_resid_g(const SolveConsts &c, const KzConst<NT> &k, const SolveGrids &g,
-                                              long long idx, double2 v[NT]) {
+// Where a bin's input spectra are read from: the grids themselves
+// (GlobalIn) or a per-thread staging slot in shared memory filled
+// asynchronously ahead of the computation (StagedIn: the inputs mu 0..2,
+// data 0..NT-1, cov 0..5 and err, each entry STRIDE float2 apart).
+struct GlobalIn {
+  const SolveGrids *g;
+  long long idx;
+  __device__ __forceinline__ float2 mu(int q) const { return g->mu[q][idx]; }
+  __device__ __forceinline__ float2 d(int l) const { return g->data[l][idx]; }
+};
+template <int NT, int STRIDE>
+struct StagedIn {
+  const float2 *s;
+  __device__ __forceinline__ float2 mu(int q) const { return s[q * STRIDE]; }
+  __device__ __forceinline__ float2 d(int l) const { return s[(3 + l) * STRIDE]; }
+  __device__ __forceinline__ float2 cov(int t) const { return s[(3 + NT + t) * STRIDE]; }
+  __device__ __forceinline__ float2 err() const { return s[(9 + NT) * STRIDE]; }
+};
+
+// v = d - K mu in double, from the bin's input spectra.
+template <int NT, typename IN>
+__device__ __forceinline__ void prior_resid_g(const SolveConsts &c, const KzConst<NT> &k, const IN &in,
+                                              double2 v[NT]) {
   double2 m[3];
 #pragma unroll
   for (int r = 0; r < 3; ++r) {
-    const float2 x = g.mu[r][idx];
+    const float2 x = in.mu(r);
     m[r] = make_double2(x.x, x.y);
   }
 #pragma unroll
@@ -692,23 +711,23 @@ __device__ __forceinline__ void prior_resid_g(const SolveConsts &c, const KzCons
     double2 km = make_double2(0.0, 0.0);
 #pragma unroll
     for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * m[r].x, c.A[l][r] * m[r].y));
-    const float2 wl = k.wd[l], dl = g.data[l][idx];
+    const float2 wl = k.wd[l], dl = in.d(l);
     km = dmul(make_double2(wl.x, wl.y), km);
     v[l] = make_double2((double)dl.x - km.x, (double)dl.y - km.y);
   }
 }
 
 // Posterior mean mu + dm and residual d - K (mu + dm), written to the bin's
-// spectra (re-read here, so they hold no registers during the solve).
-// Returns whether every output is finite.
-template <int NT>
+// spectra (the inputs re-read here, so they hold no registers during the
+// solve).  Returns whether every output is finite.
+template <int NT, typename IN>
 __device__ __forceinline__ bool write_mean_resid(const SolveConsts &c, const KzConst<NT> &k, const SolveGrids &g,
-                                                 long long idx, const double2 dm[3]) {
+                                                 long long idx, const IN &in, const double2 dm[3]) {
   double2 mp[3];
   bool ok = true;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
-    const float2 x = g.mu[q][idx];
+    const float2 x = in.mu(q);
     mp[q] = make_double2((double)x.x + dm[q].x, (double)x.y + dm[q].y);
   }
 #pragma unroll
@@ -716,7 +735,7 @@ __device__ __forceinline__ bool write_mean_resid(const SolveConsts &c, const KzC
     double2 km = make_double2(0.0, 0.0);
 #pragma unroll
     for (int r = 0; r < 3; ++r) km = dadd(km, make_double2(c.A[l][r] * mp[r].x, c.A[l][r] * mp[r].y));
-    const float2 wl = k.wd[l], dl = g.data[l][idx];
+    const float2 wl = k.wd[l], dl = in.d(l);
     km = dmul(make_double2(wl.x, wl.y), km);
     const float2 r = make_float2((float)((double)dl.x - km.x), (float)((double)dl.y - km.y));
     g.data[l][idx] = r;
@@ -760,10 +779,10 @@ __device__ __forceinline__ void ks_col(const SolveConsts &c, const KzConst<NT> &
 // two columns of Y.  Returns false when the factorisation failed (then the
 // caller writes the prior and keeps mu and the data).  *ok: every output
 // finite.
-template <int NT, typename LA, typename YA>
+template <int NT, typename LA, typename YA, typename IN>
 __device__ __forceinline__ bool solve_bin_fp64_sq(LA L, YA Y, const SolveConsts &c, const KzConst<NT> &k,
                                                   const Sym3d &S, double lam, const SolveGrids &g, long long idx,
-                                                  bool *ok) {
+                                                  const IN &in, bool *ok) {
 #pragma unroll
   for (int l = 0; l < NT; ++l) {
     double as[3];
@@ -800,7 +819,7 @@ __device__ __forceinline__ bool solve_bin_fp64_sq(LA L, YA Y, const SolveConsts 
   }
   // mean correction Y^H z, z = L^-1 (d - K mu); y holds the last column
   double2 z[NT];
-  prior_resid_g<NT>(c, k, g, idx, z);
+  prior_resid_g<NT>(c, k, in, z);
   fwd_sub_rd<NT, double2, LA>(L, z);
   double2 dm[3] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
 #pragma unroll
@@ -809,7 +828,7 @@ __device__ __forceinline__ bool solve_bin_fp64_sq(LA L, YA Y, const SolveConsts 
     dm[1] = dadd(dm[1], dmulc(z[l], Y[NT + l]));
     dm[2] = dadd(dm[2], dmulc(z[l], y[l]));
   }
-  fin &= write_mean_resid<NT>(c, k, g, idx, dm);
+  fin &= write_mean_resid<NT>(c, k, g, idx, in, dm);
   *ok = fin;
   return true;
 }
@@ -824,10 +843,11 @@ __device__ __forceinline__ bool solve_bin_fp64_sq(LA L, YA Y, const SolveConsts 
 // then S_post = S - (K S)^H X and mu_post = mu + X^H v in FP64.  Lf: the
 // FP32 factor; Yf: two FP32 columns; V: the FP64 prior-mean residual.
 // Returns false when the FP32 factorisation failed.
-template <int NT, typename LA, typename YA, typename VA>
+template <int NT, typename LA, typename YA, typename VA, typename IN>
 __device__ __forceinline__ bool solve_bin_mixed_sq(LA Lf, YA Yf, VA V, const SolveConsts &c, const KzConst<NT> &k,
                                                    const Sym3d &S, float kappa_refine, float lamf, double lam,
-                                                   const SolveGrids &g, long long idx, bool *ok, bool *refined) {
+                                                   const SolveGrids &g, long long idx, const IN &in, bool *ok,
+                                                   bool *refined) {
 #pragma unroll
   for (int l = 0; l < NT; ++l) {
     float as[3];
@@ -876,7 +896,7 @@ __device__ __forceinline__ bool solve_bin_mixed_sq(LA Lf, YA Yf, VA V, const Sol
     float2 z[NT];
     {
       double2 v[NT];
-      prior_resid_g<NT>(c, k, g, idx, v);
+      prior_resid_g<NT>(c, k, in, v);
 #pragma unroll
       for (int l = 0; l < NT; ++l) z[l] = make_float2((float)v[l].x, (float)v[l].y);
     }
@@ -893,7 +913,7 @@ __device__ __forceinline__ bool solve_bin_mixed_sq(LA Lf, YA Yf, VA V, const Sol
   } else {
     {
       double2 v[NT];
-      prior_resid_g<NT>(c, k, g, idx, v);
+      prior_resid_g<NT>(c, k, in, v);
 #pragma unroll
       for (int l = 0; l < NT; ++l) V[l] = v[l];
     }
@@ -958,7 +978,7 @@ __device__ __forceinline__ bool solve_bin_mixed_sq(LA Lf, YA Yf, VA V, const Sol
       }
     }
   }
-  fin &= write_mean_resid<NT>(c, k, g, idx, dm);
+  fin &= write_mean_resid<NT>(c, k, g, idx, in, dm);
   *ok = fin;
   return true;
 }
