@@ -522,6 +522,9 @@ struct RrRows {
   static constexpr int P0 = N + N / R0 + 1;  // room for index N in the split
   static constexpr int P = P0 + ((8 - P0 % 16) + 16) % 16;  // pitch = 8 mod 16
   static __host__ __device__ constexpr int phys(int e) { return e + e / R0; }
+  // register holding position t + T m in stage s's layout (radix R):
+  // b = m mod (E / R), q = m div (E / R), register b R + q
+  static __host__ __device__ constexpr int reg(int m, int R) { return (m % (E / R)) * R + m / (E / R); }
 };
 
 template <int N, int DIR, int S>
@@ -572,24 +575,57 @@ __global__ void __launch_bounds__(RrRows<N>::NTH) k_rows_rr(const __grid_constan
         v[b * R0 + q] = ok ? src[rr::stage_in<N, 0, E, T>(t, b, q)] : make_float2(0.f, 0.f);
     __syncthreads();  // twiddles
     RrRowStages<N, DIR, 0>::run(v, row, tw, t);
-    // last stage outputs to shared memory for the split
-    if (S > 1) __syncthreads();
+    if constexpr (T <= 32) {
+      // the split pairs position k = t + T m with N - k, which thread
+      // T - t of the same row holds at m' = E - 1 - m (thread 0: its own
+      // position E - m): one warp shuffle per output instead of a
+      // shared-memory round trip
+      const int lane = threadIdx.x & 31;
+      const int src = lane - t + (T - t) % T;
+      float2 *orow = reinterpret_cast<float2 *>(a.grid + (ok ? row_idx : 0) * a.rnxp);
 #pragma unroll
-    for (int b = 0; b < E / RL; ++b)
-#pragma unroll
-      for (int q = 0; q < RL; ++q) row[C::phys(rr::stage_in<N, S - 1, E, T>(t, b, q))] = v[b * RL + q];
-    __syncthreads();
-    if (ok) {
-      // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{N-k})/2, O = -i (Z_k - conj Z_{N-k})/2
-      float2 *orow = reinterpret_cast<float2 *>(a.grid + row_idx * a.rnxp);
-      for (int k = t; k <= N; k += T) {
-        const float2 zk = row[C::phys(k == N ? 0 : k)];
-        float2 zm = row[C::phys(k == 0 ? 0 : N - k)];
+      for (int m = 0; m < E; ++m) {
+        const float2 send = v[C::reg(E - 1 - m, RL)];
+        float2 zm = make_float2(__shfl_sync(0xffffffffu, send.x, src), __shfl_sync(0xffffffffu, send.y, src));
+        if (t == 0) zm = v[C::reg(m == 0 ? 0 : E - m, RL)];
+        const float2 zk = v[C::reg(m, RL)];
         zm.y = -zm.y;
         const float2 e = cscale(cadd(zk, zm), 0.5f);
         const float2 d = csub(zk, zm);
         const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
-        orow[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+        const int k = t + T * m;
+        if (ok) orow[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+      }
+      if (ok && t == 0) {
+        // X_N from Z_0 alone
+        const float2 zk = v[C::reg(0, RL)];
+        float2 zm = zk;
+        zm.y = -zm.y;
+        const float2 e = cscale(cadd(zk, zm), 0.5f);
+        const float2 d = csub(zk, zm);
+        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+        orow[N] = cscale(cadd(e, cmul(post[N], o)), a.scale);
+      }
+    } else {
+      // last stage outputs to shared memory for the split
+      if (S > 1) __syncthreads();
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int q = 0; q < RL; ++q) row[C::phys(rr::stage_in<N, S - 1, E, T>(t, b, q))] = v[b * RL + q];
+      __syncthreads();
+      if (ok) {
+        // X_k = E_k + W^k O_k, E = (Z_k + conj Z_{N-k})/2, O = -i (Z_k - conj Z_{N-k})/2
+        float2 *orow = reinterpret_cast<float2 *>(a.grid + row_idx * a.rnxp);
+        for (int k = t; k <= N; k += T) {
+          const float2 zk = row[C::phys(k == N ? 0 : k)];
+          float2 zm = row[C::phys(k == 0 ? 0 : N - k)];
+          zm.y = -zm.y;
+          const float2 e = cscale(cadd(zk, zm), 0.5f);
+          const float2 d = csub(zk, zm);
+          const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+          orow[k] = cscale(cadd(e, cmul(post[k], o)), a.scale);
+        }
       }
     }
   } else {
@@ -597,20 +633,42 @@ __global__ void __launch_bounds__(RrRows<N>::NTH) k_rows_rr(const __grid_constan
     const float2 *X = reinterpret_cast<const float2 *>(a.grid + (ok ? row_idx : 0) * a.rnxp);
     // Z'[k] = (X_k + conj X_{N-k}) + i W^{-k} (X_k - conj X_{N-k}); the
     // imaginary parts of DC and Nyquist are ignored, as a C2R does
+    auto pre = [&](int k, float2 x0, float2 x1) {
+      if (k == 0) { x0.y = 0.f; x1.y = 0.f; }
+      x1.y = -x1.y;
+      const float2 e = cadd(x0, x1);
+      float2 w = post[k];
+      w.y = -w.y;
+      const float2 o = cmul(csub(x0, x1), w);
+      return make_float2(e.x - o.y, e.y + o.x);
+    };
+    if constexpr (T <= 32) {
+      // each thread loads its own positions k = t + T m; X_{N-k} comes
+      // from thread T - t of the row by a warp shuffle (thread 0: its own
+      // position E - m, and X_N, loaded once)
+      float2 xk[E];
 #pragma unroll
-    for (int b = 0; b < E / R0; ++b)
+      for (int m = 0; m < E; ++m) xk[m] = ok ? X[t + T * m] : make_float2(0.f, 0.f);
+      const float2 xN = (ok && t == 0) ? X[N] : make_float2(0.f, 0.f);
+      const int lane = threadIdx.x & 31;
+      const int src = lane - t + (T - t) % T;
 #pragma unroll
-      for (int q = 0; q < R0; ++q) {
-        const int k = rr::stage_in<N, 0, E, T>(t, b, q);
-        float2 x0 = ok ? X[k] : make_float2(0.f, 0.f), x1 = ok ? X[N - k] : make_float2(0.f, 0.f);
-        if (k == 0) { x0.y = 0.f; x1.y = 0.f; }
-        x1.y = -x1.y;
-        const float2 e = cadd(x0, x1);
-        float2 w = post[k];
-        w.y = -w.y;
-        const float2 o = cmul(csub(x0, x1), w);
-        v[b * R0 + q] = make_float2(e.x - o.y, e.y + o.x);
+      for (int m = 0; m < E; ++m) {
+        const float2 send = xk[E - 1 - m];
+        float2 x1 = make_float2(__shfl_sync(0xffffffffu, send.x, src), __shfl_sync(0xffffffffu, send.y, src));
+        if (t == 0) x1 = m == 0 ? xN : xk[E - m];
+        v[C::reg(m, R0)] = pre(t + T * m, xk[m], x1);
       }
+    } else {
+#pragma unroll
+      for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+        for (int q = 0; q < R0; ++q) {
+          const int k = rr::stage_in<N, 0, E, T>(t, b, q);
+          const float2 x0 = ok ? X[k] : make_float2(0.f, 0.f), x1 = ok ? X[N - k] : make_float2(0.f, 0.f);
+          v[b * R0 + q] = pre(k, x0, x1);
+        }
+    }
     // every thread has read its whole row before any row is overwritten
     // (in place: the output row is the input row)
     __syncthreads();

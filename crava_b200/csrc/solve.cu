@@ -32,10 +32,6 @@ namespace {
 
 constexpr int kThreads = 256;
 using sb::tri;
-// Keep the FP64 Cholesky factor (FP64 form) or the FP64 copy of M (mixed
-// form), and A S, in shared memory, one entry column per thread, instead of
-// in registers: fewer spills at two blocks per SM.
-constexpr bool kSolveFactorInSmem = true;
 
 // ------------------------------------------------------------------ tables
 __global__ void k_kz_tables(const float *__restrict__ wav,
@@ -160,68 +156,6 @@ struct SolveArgs {
   long long bpp;  // blocks per kz plane
   DevCounters *counters;
 };
-
-// Block b works on plane order[b / bpp] (bpp blocks per kz plane), so
-// every block sees one band flag.  Band-gated bins read and write only the
-// six covariance spectra: the solve runs in place, and their mean and data
-// spectra stay as they are.
-template <int NT, int PREC, int MINB>
-__global__ void __launch_bounds__(kThreads, MINB) k_solve(SolveArgs a) {
-  const int slot = (int)(blockIdx.x / a.bpp);
-  const long long off = (long long)(blockIdx.x % a.bpp) * blockDim.x + threadIdx.x;
-  if (off >= a.plane) return;
-  const int k = a.t.order ? a.t.order[slot] : slot;
-  const long long idx = (long long)k * a.plane + off;
-  const bool inv = a.t.inv[k] != 0;
-  float2 c6[6];
-#pragma unroll
-  for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
-  if (!inv) {
-    sb::prior_only<PREC>(a.c, c6);
-    bool nonfinite = false;
-#pragma unroll
-    for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
-    if (a.counters) sb::count(a.counters, false, nonfinite);
-    return;
-  }
-  float2 mu[3], d[NT];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) mu[q] = a.g.mu[q][idx];
-#pragma unroll
-  for (int l = 0; l < NT; ++l) d[l] = a.g.data[l][idx];
-  const float2 ec = a.g.err[idx];
-  const long long o = (long long)k * NT;
-  bool fail;
-  if (PREC == 0 && kSolveFactorInSmem) {
-    // the FP64 factor lives in shared memory, one column of entries per thread
-    extern __shared__ double2 lsm[];
-    const sb::SmemTri<double2, kThreads> L{lsm + threadIdx.x};
-    const sb::SmemTri<double, kThreads> AS{
-        reinterpret_cast<double *>(lsm + kThreads * (NT * (NT + 1) / 2)) + threadIdx.x};
-    fail = sb::solve_bin_fp64_in<NT>(L, AS, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
-                                     mu, d, c6, ec);
-  } else if (PREC == 1 && kSolveFactorInSmem) {
-    // the FP64 copy of M in shared memory, the FP32 factor in registers
-    extern __shared__ double2 lsm[];
-    float2 Lf[NT * (NT + 1) / 2];
-    const sb::SmemTri<double2, kThreads> Md{lsm + threadIdx.x};
-    const sb::SmemTri<double, kThreads> AS{
-        reinterpret_cast<double *>(lsm + kThreads * (NT * (NT + 1) / 2)) + threadIdx.x};
-    fail = sb::solve_bin_mixed_in<NT>(&Lf[0], Md, AS, a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o,
-                                      inv, mu, d, c6, ec);
-  } else {
-    fail = sb::solve_bin<NT, PREC>(a.c, a.t.wd + o, a.t.e1 + o, a.t.e2 + o, a.t.e3 + o, inv,
-                                   mu, d, c6, ec);
-  }
-  bool nonfinite = false;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) { a.g.mu[q][idx] = mu[q]; nonfinite |= !sb::fin2(mu[q]); }
-#pragma unroll
-  for (int l = 0; l < NT; ++l) { a.g.data[l][idx] = d[l]; nonfinite |= !sb::fin2(d[l]); }
-#pragma unroll
-  for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
-  if (a.counters) sb::count(a.counters, fail, nonfinite);
-}
 
 // Square-root form (solve_bin.cuh): the FP64 and mixed forms.  One kz
 // plane per CTA: the CTA first stages the plane's per-kz constants of M in
@@ -485,77 +419,35 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
 // threads and one block per SM (up to 255 registers), 3 in registers with
 // 128 threads and four blocks per SM (up to 128 registers); 4 and 5 the
 // pipelined kernel (k_solve_pf) with 128 threads, four blocks per SM and 4
-// or 8 bins per thread.  Measured at
-// 256x256x512x5 (B200, one stream): FP64 / mixed 1.34 / 1.14 ms (shape 0),
-// 1.34 / 1.23 (1), 1.76 / 1.74 (2), 1.17 / 1.06 (3); shape 3 is the
-// default.  CRAVA_SOLVE_SHAPE overrides it for measurements.
-static int solve_shape() {
-  static int v = -1;
-  if (v < 0) {
+// or 8 bins per thread.  Measured at 256x256x512x5 (B200, one stream),
+// FP64 / mixed: 1.34 / 1.14 ms (shape 0), 1.34 / 1.23 (1), 1.76 / 1.74 (2),
+// 1.17 / 1.06 (3), 1.03 / 1.11 (4), 1.01 / 1.09 (5).  The FP64 form is
+// latency-bound on its global loads, which the pipelined kernel hides; the
+// mixed form carries the FP32 factor and the FP64 refinement operands in
+// registers, and the staging buffers cost it more occupancy than they
+// save.  So the default is shape 5 for FP64 and shape 3 for mixed;
+// CRAVA_SOLVE_SHAPE (0-5) overrides both, for measurements.
+static int solve_shape_override() {
+  static int v = -2;
+  if (v == -2) {
     const char *e = getenv("CRAVA_SOLVE_SHAPE");
-    v = e ? atoi(e) : 3;
-    if (v < 0 || v > 5) v = 3;
+    v = e ? atoi(e) : -1;
+    if (v < 0 || v > 5) v = -1;
   }
   return v;
 }
 
 template <int PREC>
 int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
-  switch (solve_shape()) {
+  int shape = solve_shape_override();
+  if (shape < 0) shape = PREC == 0 ? 5 : 3;
+  switch (shape) {
     case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);
     case 1: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
     case 2: return launch_solve_sq<PREC, 256, 1, true>(a, nt, s);
     case 4: return launch_solve_pf<PREC, 128, 4, 4>(a, nt, s);
     case 5: return launch_solve_pf<PREC, 128, 4, 8>(a, nt, s);
     default: return launch_solve_sq<PREC, 128, 4, true>(a, nt, s);
-  }
-}
-
-template <int PREC, int MINB>
-int launch_solve_b(const SolveArgs &a, int nt, cudaStream_t s) {
-  dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
-  // FP64 form: factor (NT(NT+1)/2 double2) and A S (3 NT doubles) per thread
-  // per thread: the FP64 factor (FP64 form) or the FP64 copy of M (mixed
-  // form), NT(NT+1)/2 double2, and A S, 3 NT doubles
-  const size_t smem = !kSolveFactorInSmem ? 0
-                      : (sizeof(double2) * (nt * (nt + 1) / 2) + sizeof(double) * 3 * nt) * kThreads;
-  int rc;
-#define CRAVA_SOLVE_CASE(N)                                                          \
-  case N:                                                                            \
-    if ((rc = func_smem((const void *)k_solve<N, PREC, MINB>, smem))) return rc;     \
-    k_solve<N, PREC, MINB><<<grd, kThreads, smem, s>>>(a);                           \
-    break;
-  switch (nt) {
-    CRAVA_SOLVE_CASE(1) CRAVA_SOLVE_CASE(2) CRAVA_SOLVE_CASE(3) CRAVA_SOLVE_CASE(4)
-    CRAVA_SOLVE_CASE(5) CRAVA_SOLVE_CASE(6) CRAVA_SOLVE_CASE(7) CRAVA_SOLVE_CASE(8)
-    default: return CRAVA_GPU_ERR_ARG;
-  }
-#undef CRAVA_SOLVE_CASE
-  CRAVA_LAUNCH_CHECK();
-  return CRAVA_GPU_OK;
-}
-
-// Blocks per SM of the solve kernel (register budget 255 / 128 / 80).  With
-// the right-hand-side loop kept rolled, two blocks (16 warps per SM, a few
-// hundred bytes of spills) measured fastest: FP64 1.52 ms, mixed 1.85 ms
-// at 256x256x512x5 against 1.86 / 2.19 with one block.  CRAVA_SOLVE_MINB
-// overrides the default for measurements.
-static int solve_minb() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("CRAVA_SOLVE_MINB");
-    v = e ? atoi(e) : 2;
-    if (v < 1 || v > 3) v = 2;
-  }
-  return v;
-}
-
-template <int PREC>
-int launch_solve(const SolveArgs &a, int nt, cudaStream_t s) {
-  switch (solve_minb()) {
-    case 2: return launch_solve_b<PREC, 2>(a, nt, s);
-    case 3: return launch_solve_b<PREC, 3>(a, nt, s);
-    default: return launch_solve_b<PREC, 1>(a, nt, s);
   }
 }
 
