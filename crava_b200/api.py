@@ -68,7 +68,7 @@ class Stats(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("cols_y_tile", C.c_int), ("cols_z_tile", C.c_int), ("fused", C.c_int),
                 ("ms", C.c_float), ("lanes", C.c_int), ("rows_x", C.c_int), ("kappa_refine", C.c_float),
-                ("xy_fused", C.c_int)]
+                ("xy_fused", C.c_int), ("solve_shape", C.c_int)]
 
 
 class GridHeader(C.Structure):
@@ -292,13 +292,15 @@ class Context:
         return t
 
     def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0, lanes=2, rows_x=-1, kappa_refine=None,
-                   xy_fused=None):
+                   xy_fused=None, solve_shape=None):
         cur = self.tuning()
         if kappa_refine is None:
             kappa_refine = cur.kappa_refine
         if xy_fused is None:
             xy_fused = cur.xy_fused
-        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0, lanes, rows_x, kappa_refine, xy_fused)
+        if solve_shape is None:
+            solve_shape = cur.solve_shape
+        t = Tuning(cols_y_tile, cols_z_tile, fused, 0.0, lanes, rows_x, kappa_refine, xy_fused, solve_shape)
         check(self.lib.crava_gpu_set_tuning(self.handle, C.byref(t)), "set_tuning")
 
     def autotune(self, src, dst, precision=None, reps=2) -> Tuning:

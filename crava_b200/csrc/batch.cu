@@ -171,6 +171,7 @@ int crava_gpu_get_tuning(crava_gpu_ctx *c, crava_gpu_tuning *out) {
   out->rows_x = c->plans.rows_x;
   out->kappa_refine = c->consts.kappa_refine;
   out->xy_fused = c->plans.plane_xy;
+  out->solve_shape = c->consts.solve_shape;
   return CRAVA_GPU_OK;
 }
 
@@ -181,6 +182,7 @@ int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   if (t->rows_x < -1 || t->rows_x > 1) return CRAVA_GPU_ERR_ARG;
   if (!(t->kappa_refine >= 0.0f)) return CRAVA_GPU_ERR_ARG;
   if (t->xy_fused < -1 || t->xy_fused > 1) return CRAVA_GPU_ERR_ARG;
+  if (t->solve_shape < -1 || t->solve_shape > 5) return CRAVA_GPU_ERR_ARG;
   if (t->lanes < 1 || t->lanes > crava_gpu_ctx::kMaxLanes) return CRAVA_GPU_ERR_ARG;
   c->plans.tile_y = t->cols_y_tile;
   c->plans.tile_z = t->cols_z_tile;
@@ -189,6 +191,7 @@ int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   c->plans.rows_x = t->rows_x;
   c->consts.kappa_refine = t->kappa_refine;
   c->plans.plane_xy = t->xy_fused;
+  c->consts.solve_shape = t->solve_shape;
   return CRAVA_GPU_OK;
 }
 
@@ -214,13 +217,13 @@ int crava_gpu_autotune(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_
   const bool xy = plane_xy_supported(c->g);
   for (int lanes = 1; lanes <= 2; ++lanes) {
     for (int a : cy)
-      for (int z : cz) cand.push_back({a, z, 0, 0.0f, lanes, -1, c->consts.kappa_refine, 0});
+      for (int z : cz) cand.push_back({a, z, 0, 0.0f, lanes, -1, c->consts.kappa_refine, 0, c->consts.solve_shape});
     // the fused x + y pass replaces the y pass: only the z choices matter
     if (xy)
-      for (int z : cz) cand.push_back({-1, z, 0, 0.0f, lanes, -1, c->consts.kappa_refine, 1});
+      for (int z : cz) cand.push_back({-1, z, 0, 0.0f, lanes, -1, c->consts.kappa_refine, 1, c->consts.solve_shape});
   }
   // the fused unit does not use the column passes: one candidate
-  if (c->uplan.ok && precision != CRAVA_SOLVE_FP32) cand.push_back({-1, -1, 1, 0.0f, 1, -1, c->consts.kappa_refine, 0});
+  if (c->uplan.ok && precision != CRAVA_SOLVE_FP32) cand.push_back({-1, -1, 1, 0.0f, 1, -1, c->consts.kappa_refine, 0, c->consts.solve_shape});
   crava_gpu_tuning saved;
   crava_gpu_get_tuning(c, &saved);
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -400,6 +400,7 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   c->consts.nt = nt;
   c->consts.wnc = params->wnc;
   c->consts.kappa_refine = kKappaRefineDefault;
+  c->consts.solve_shape = -1;
   for (int l = 0; l < nt; ++l) {
     for (int q = 0; q < 3; ++q) c->consts.A[l][q] = c->A[3 * l + q];
     for (int m = 0; m < nt; ++m) c->consts.theta[l][m] = c->theta[l * nt + m];

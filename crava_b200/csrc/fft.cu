@@ -398,7 +398,6 @@ struct RrCols {
   static constexpr int CPT = E >= 16 ? 1 : 2;
   static constexpr int NP = kRrTX / CPT;
   static constexpr int NTH = NP * T;
-  static constexpr int S = CtRadix::count(N);
 };
 
 template <int N, int DIR, int CPT, bool VEC, int S>
@@ -505,10 +504,12 @@ __global__ void __launch_bounds__(RrCols<N>::NTH) k_cols_rr(const __grid_constan
 // rows per CTA (32, fewer when the CTA would exceed 512 threads), T threads
 // per row (lanes along the row).  Forward: the
 // packed row's N complex values go global -> registers, through the radix
-// stages, into shared memory for the split X_k = E_k + W^k O_k (which pairs
-// k with N - k), and the N + 1 outputs to HBM.  Inverse: the pre-split
-// Z'_k is built from X_k and X_{N-k} read from HBM into registers, and the
-// last stage writes the real row straight to HBM.  Shared rows are padded
+// stages, to the split X_k = E_k + W^k O_k (which pairs k with N - k), and
+// the N + 1 outputs to HBM.  Inverse: the pre-split Z'_k is built from X_k
+// and X_{N-k}, and the last stage writes the real row straight to HBM.
+// Where a row's T threads lie in one warp (T <= 32) the pairing is a warp
+// shuffle; otherwise (N = 512) the split goes through shared memory and the
+// pre-split reads X_{N-k} from HBM a second time.  Shared rows are padded
 // (one spare element after every R_0 and a pitch of 8 mod 16 float2) so
 // the first stage's stride-R_0 writes and two rows per phase are free of
 // bank conflicts.

@@ -138,6 +138,7 @@ extern "C" int crava_gpu_posterior_noalloc(const crava_gpu_params *p, const crav
   c.nt = nt;
   c.wnc = p->wnc;
   c.kappa_refine = kKappaRefineDefault;
+  c.solve_shape = -1;
   for (int l = 0; l < nt; ++l) {
     for (int q = 0; q < 3; ++q) c.A[l][q] = p->A[3 * l + q];
     for (int m = 0; m < nt; ++m) c.theta[l][m] = p->theta_cov[l * nt + m];

@@ -425,8 +425,9 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
 // latency-bound on its global loads, which the pipelined kernel hides; the
 // mixed form carries the FP32 factor and the FP64 refinement operands in
 // registers, and the staging buffers cost it more occupancy than they
-// save.  So the default is shape 5 for FP64 and shape 3 for mixed;
-// CRAVA_SOLVE_SHAPE (0-5) overrides both, for measurements.
+// save.  So the default is shape 5 for FP64 and shape 3 for mixed.  The
+// context's tuning (SolveConsts::solve_shape) picks one explicitly, and
+// CRAVA_SOLVE_SHAPE (0-5) overrides the built-in choice for measurements.
 static int solve_shape_override() {
   static int v = -2;
   if (v == -2) {
@@ -439,7 +440,7 @@ static int solve_shape_override() {
 
 template <int PREC>
 int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
-  int shape = solve_shape_override();
+  int shape = a.c.solve_shape >= 0 ? a.c.solve_shape : solve_shape_override();
   if (shape < 0) shape = PREC == 0 ? 5 : 3;
   switch (shape) {
     case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);

@@ -26,6 +26,9 @@ struct SolveConsts {
   // mixed form: a bin whose FP32 factor's condition bound exceeds this
   // takes one FP64 refinement step (0: every bin; a huge value: none)
   float kappa_refine;
+  // launch shape of the FP64 / mixed solve (-1: the built-in choice of the
+  // precision; 0-5: solve.cu)
+  int solve_shape;
 };
 
 struct SolveGrids {

@@ -281,12 +281,17 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
  * pass where nxp / 2 is 64..512).  All these choices give the same values
  * bit for bit.  xy_fused: the x and y passes as one thread-block-cluster
  * kernel where the geometry has one (256x256 and 128x128 planes; -1
- * built-in = on, 0 off, 1 on); it factorises the y transform differently,
- * so it agrees with the separate passes to float rounding, not bit for
- * bit.  kappa_refine (mixed form only, >= 0): an inverted bin whose
+ * built-in = off, 0 off, 1 on; it measured slower than the separate
+ * register-resident passes on B200); it factorises the y transform
+ * differently, so it agrees with the separate passes to float rounding,
+ * not bit for bit.  kappa_refine (mixed form only, >= 0): an inverted bin whose
  * FP32 factor has (max L_ii / min L_ii)^2 above it takes one FP64
- * refinement step (0 refines every bin).  No counterpart in the reference
- * (FFTW plans are fixed there). */
+ * refinement step (0 refines every bin).  solve_shape: the launch shape of
+ * the FP64 and mixed solves (-1 built-in: the pipelined kernel with 8 bins
+ * per thread for FP64, the register-factor kernel with four 128-thread
+ * blocks per SM for mixed; 0-5 one shape for both); every shape gives the
+ * same values bit for bit.  No counterpart in the reference (FFTW plans
+ * are fixed there). */
 typedef struct crava_gpu_tuning {
   int cols_y_tile;
   int cols_z_tile;
@@ -296,6 +301,7 @@ typedef struct crava_gpu_tuning {
   int rows_x;
   float kappa_refine;
   int xy_fused;
+  int solve_shape;
 } crava_gpu_tuning;
 int crava_gpu_get_tuning(crava_gpu_ctx *ctx, crava_gpu_tuning *out);
 int crava_gpu_set_tuning(crava_gpu_ctx *ctx, const crava_gpu_tuning *t);

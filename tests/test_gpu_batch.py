@@ -70,6 +70,44 @@ def test_row_pass_choices_match(shape):
     assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
 
 
+# planes of 21 x 36 bins (fewer than one CTA's bins in every shape) and of
+# 33 x 40; five and two angles
+@pytest.mark.parametrize("shape,angles", [((40, 36, 96), (0.0, 10.0, 20.0, 30.0, 40.0)),
+                                          ((64, 40, 64), (10.0, 30.0))])
+@pytest.mark.parametrize("prec,kappa", [(api.FP64, None), (api.MIXED, None), (api.MIXED, 0.0)])
+def test_solve_shapes_match(shape, angles, prec, kappa):
+    """Every launch shape of the FP64 and mixed solves (solve_shape 0-5 and
+    the built-in choice) gives the same outputs and counters bit for bit;
+    kappa_refine 0 sends every inverted bin of the mixed form through the
+    FP64 refinement step."""
+    nx, ny, nz = shape
+    case = synth.make_case(nx, ny, nz, angles, 0.1, seed=12)
+    ctx = api.Context(case)
+    spec = _dev(case)
+    mu, data, cov, err = spec
+    for g in mu:
+        ctx.fft_r2c(g, api.PARAMETER)
+    for g in data:
+        ctx.fft_r2c(g, api.DATA)
+    for g in cov + [err]:
+        ctx.fft_r2c(g, api.COVARIANCE)
+    res = {}
+    for sh in (-1, 0, 1, 2, 3, 4, 5):
+        ctx.set_tuning(-1, -1, 0, 2, -1, kappa, None, sh)
+        assert ctx.tuning().solve_shape == sh
+        m, d, c = [g.clone() for g in mu], [g.clone() for g in data], [g.clone() for g in cov]
+        ctx.posterior(m, d, c, err, prec)
+        st = ctx.stats()
+        res[sh] = ([g.cpu().numpy() for g in m + d + c], st.chol_fail_bins, st.nonfinite_bins, st.refined_bins)
+    if kappa == 0.0:
+        assert res[0][3] > 0
+    for sh in res:
+        assert res[sh][1:] == res[0][1:], sh
+        assert all(np.array_equal(a, b) for a, b in zip(res[sh][0], res[0][0])), sh
+    with pytest.raises(api.CravaGpuError):
+        ctx.set_tuning(-1, -1, 0, 2, -1, None, None, 6)
+
+
 def _dev(case):
     d = lambda gs: [api.to_device(g) for g in gs]
     return d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0]
