@@ -111,6 +111,8 @@ def parse():
     ap.add_argument("--profile-lanes", type=int, default=1,
                     help="transform streams in the profile run (1: per-launch events time one kernel each)")
     ap.add_argument("--profile-xy", type=int, default=-1, help="fused x + y pass: -1 built-in, 0 off, 1 on")
+    ap.add_argument("--profile-tile-z", type=int, default=None,
+                    help="z pass: -1 built-in, 1 register-resident, 2 register-resident with TMA tile loads")
     return ap.parse_args()
 
 
@@ -1023,7 +1025,8 @@ def run_profile_unit(args):
     case = synth.make_case(nx, ny, nz, tuple(10.0 * i for i in range(nt)), 0.1, seed=2)
     ctx = api.Context(case)
     t = ctx.tuning()
-    ctx.set_tuning(t.cols_y_tile, t.cols_z_tile, int(bool(args.profile_fused)), args.profile_lanes, t.rows_x,
+    tz = t.cols_z_tile if args.profile_tile_z is None else args.profile_tile_z
+    ctx.set_tuning(t.cols_y_tile, tz, int(bool(args.profile_fused)), args.profile_lanes, t.rows_x,
                    t.kappa_refine, args.profile_xy)
     d = lambda gs: [api.to_device(g) for g in gs]
     src = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])

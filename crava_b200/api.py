@@ -62,7 +62,8 @@ class State4DGrids(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("chol_fail_bins", C.c_longlong), ("nonfinite_bins", C.c_longlong),
                 ("ms_forward", C.c_float), ("ms_solve", C.c_float),
-                ("ms_inverse", C.c_float), ("ms_total", C.c_float), ("refined_bins", C.c_longlong)]
+                ("ms_inverse", C.c_float), ("ms_total", C.c_float), ("refined_bins", C.c_longlong),
+                ("tile_wait_timeouts", C.c_longlong)]
 
 
 class Tuning(C.Structure):

@@ -22,6 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SOURCES = {
     "capi.cu": [],
     "fft.cu": [],
+    "cols_tma.cu": [],
     "plane.cu": [],
     "solve.cu": [],
     "solve_ref.cu": ["-fmad=false"],

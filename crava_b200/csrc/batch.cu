@@ -178,7 +178,7 @@ int crava_gpu_get_tuning(crava_gpu_ctx *c, crava_gpu_tuning *out) {
 int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   if (!c || !t) return CRAVA_GPU_ERR_ARG;
   auto ok = [](int x) { return x == -1 || x == 0 || x == 1 || x == 8 || x == 16; };
-  if (!ok(t->cols_y_tile) || !ok(t->cols_z_tile)) return CRAVA_GPU_ERR_ARG;
+  if (!ok(t->cols_y_tile) || !(ok(t->cols_z_tile) || t->cols_z_tile == 2)) return CRAVA_GPU_ERR_ARG;
   if (t->rows_x < -1 || t->rows_x > 1) return CRAVA_GPU_ERR_ARG;
   if (!(t->kappa_refine >= 0.0f)) return CRAVA_GPU_ERR_ARG;
   if (t->xy_fused < -1 || t->xy_fused > 1) return CRAVA_GPU_ERR_ARG;
@@ -213,7 +213,15 @@ int crava_gpu_autotune(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_
     if (v.empty()) v.push_back(-1);
     return v;
   };
-  const std::vector<int> cy = choices(c->g.nyp, ty), cz = choices(c->g.nzp, tz);
+  const std::vector<int> cy = choices(c->g.nyp, ty);
+  std::vector<int> cz = choices(c->g.nzp, tz);
+  // the TMA z pass, where the grids allow it
+  bool tma = cols_z_tma_supported(c->g, in->err_corr) && cols_z_tma_supported(c->g, out->err_corr);
+  for (int q = 0; q < 3; ++q) tma = tma && cols_z_tma_supported(c->g, in->mu[q]) && cols_z_tma_supported(c->g, out->mu[q]);
+  for (int l = 0; l < c->p.ntheta; ++l)
+    tma = tma && cols_z_tma_supported(c->g, in->data[l]) && cols_z_tma_supported(c->g, out->data[l]);
+  for (int q = 0; q < 6; ++q) tma = tma && cols_z_tma_supported(c->g, in->cov[q]) && cols_z_tma_supported(c->g, out->cov[q]);
+  if (tma) cz.insert(cz.begin(), 2);
   const bool xy = plane_xy_supported(c->g);
   for (int lanes = 1; lanes <= 2; ++lanes) {
     for (int a : cy)

@@ -796,6 +796,9 @@ int crava_gpu_get_stats(crava_gpu_ctx *c, crava_gpu_stats *st) {
   st->chol_fail_bins = (long long)h.chol_fail;
   st->nonfinite_bins = (long long)h.nonfinite;
   st->refined_bins = (long long)h.refined;
+  unsigned long long waits = 0;
+  if (tile_wait_timeouts(&waits)) return CRAVA_GPU_ERR_CUDA;
+  st->tile_wait_timeouts = (long long)waits;
   if (c->timed) {
     cudaEventElapsedTime(&st->ms_forward, c->ev[0], c->ev[1]);
     cudaEventElapsedTime(&st->ms_solve, c->ev[1], c->ev[2]);

@@ -957,12 +957,13 @@ static_assert(RrCols<64>::CPT == 2 && RrCols<512>::CPT == 2 && RrCols<128>::CPT 
 
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  return cols(p.y, grid, g.cnxp, g.cnxp, (long long)g.cnxp * g.nyp, g.nzp, dir, 1.0f, p.tile_y, s);
+  return cols(p.y, grid, g.cnxp, g.cnxp, (long long)g.cnxp * g.nyp, g.nzp, dir, 1.0f, p.tile_y == 2 ? -1 : p.tile_y, s);
 }
 
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z, s);
+  if (p.tile_z == 2 && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
+  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z == 2 ? -1 : p.tile_z, s);
 }
 
 int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s) {

@@ -24,8 +24,9 @@ struct FftPlans {
   // column tile of the y and z passes: -1 default, 0 ping-pong pass,
   // 1 register-resident pass (lengths 64, 128, 256, 512), 8 or 16 columns
   // per CTA in the in-place pass (lengths with compiled kernels only; other
-  // lengths use the generic pass).  The default is the register-resident
-  // pass where it exists, else the in-place pass.
+  // lengths use the generic pass), 2 (z only) the register-resident pass
+  // with TMA tile loads where cols_z_tma_supported.  The default is the
+  // register-resident pass where it exists, else the in-place pass.
   int tile_y = -1, tile_z = -1;
   // x pass of an even nxp: -1 default (register-resident where the half
   // length is 64..512), 0 the in-place pass, 1 register-resident
@@ -69,6 +70,14 @@ int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t 
              const float *addend = nullptr, const float *src = nullptr);
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
+
+// z pass with TMA tile loads (cols_tma.cu; column tile choice 2): lengths
+// 64..512, an even number of lines per z plane, a 16-byte aligned grid.
+bool cols_z_tma_supported(const Geom &g, const void *data);
+int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
+// Tile waits of the TMA z pass that hit their limit (device-wide, since the
+// library was loaded; synchronous).
+int tile_wait_timeouts(unsigned long long *out);
 
 float forward_scale(const Geom &g, int type);
 float inverse_scale(const Geom &g, int type);

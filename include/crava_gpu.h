@@ -98,6 +98,10 @@ typedef struct crava_gpu_stats {
   float ms_inverse;           /* device time of the inverse transforms                 */
   float ms_total;             /* device time of the whole call                         */
   long long refined_bins;     /* mixed form: inverted bins that took the FP64 refinement */
+  long long tile_wait_timeouts; /* TMA tile loads of the z pass not seen complete within
+                                   the wait limit (device-wide since the library was
+                                   loaded; 0 in a healthy run, else the outputs of
+                                   that pass are incomplete) */
 } crava_gpu_stats;
 
 typedef struct crava_gpu_ctx crava_gpu_ctx;

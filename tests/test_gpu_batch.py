@@ -14,9 +14,11 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-30))
 
 
-# every column length with compiled kernels, as y and as z
+# every column length with compiled kernels, as y and as z; z planes of 30
+# lines (a ragged last TMA tile) and of 35 (odd: no TMA box, the choice
+# falls back to the register-resident pass)
 TILE_SHAPES = [(8, 64, 128), (8, 256, 512), (8, 96, 160), (8, 192, 200), (8, 300, 384),
-               (8, 128, 64), (8, 384, 300)]
+               (8, 128, 64), (8, 384, 300), (8, 96, 256), (8, 6, 512), (8, 7, 64)]
 
 
 @pytest.mark.parametrize("shape", TILE_SHAPES)
@@ -28,7 +30,7 @@ def test_column_tiles_match_numpy(shape):
     ref = np.fft.rfftn(g[..., :nx].astype(np.float64), axes=(0, 1, 2)) / np.sqrt(nx * ny * nz)
     res = {}
     for ty in (1, 16, 8, 0):
-        for tz in (1, 16, 8, 0):
+        for tz in (1, 16, 8, 0, 2):
             ctx.set_tuning(ty, tz, 0)
             t = api.to_device(g)
             ctx.fft_r2c(t, api.DATA)
@@ -39,10 +41,13 @@ def test_column_tiles_match_numpy(shape):
             assert rel(back, g[..., :nx]) < 2e-6, (ty, tz)
             res[(ty, tz)] = (out, back)
     # the in-place pass does the same arithmetic per line whatever the
-    # tile, and so does the register-resident pass (1) where it exists
+    # tile, and so do the register-resident pass (1) where it exists and its
+    # TMA-fed z pass (2)
     same = lambda a, b: all(np.array_equal(x, y) for x, y in zip(res[a], res[b]))
     assert same((16, 16), (8, 8)) and same((16, 8), (8, 16))
     assert same((1, 1), (16, 16)) and same((1, 16), (16, 16)) and same((16, 1), (16, 16))
+    assert same((1, 2), (1, 1)) and same((16, 2), (16, 1))
+    assert ctx.stats().tile_wait_timeouts == 0
 
 
 # even nxp whose half length has register-resident row kernels, and one without
@@ -106,6 +111,24 @@ def test_solve_shapes_match(shape, angles, prec, kappa):
         assert all(np.array_equal(a, b) for a, b in zip(res[sh][0], res[0][0])), sh
     with pytest.raises(api.CravaGpuError):
         ctx.set_tuning(-1, -1, 0, 2, -1, None, None, 6)
+
+
+def test_tma_z_pass_unit_matches():
+    """The whole out-of-place unit at 128x128x512, 5 angles, with the
+    TMA-fed z pass equals the unit with the register-resident z pass bit
+    for bit, FP64 and mixed."""
+    case = synth.make_case(128, 128, 512, (0.0, 10.0, 20.0, 30.0, 40.0), 0.1, seed=21)
+    ctx = api.Context(case)
+    src = _dev(case)
+    for prec in (api.FP64, api.MIXED):
+        outs = {}
+        for tz in (1, 2):
+            ctx.set_tuning(-1, tz, 0)
+            dst = _dev(case)
+            ctx.posterior_unit_oop(src, dst, prec)
+            outs[tz] = [g.cpu().numpy() for g in dst[0] + dst[1] + dst[2]]
+        assert all(np.array_equal(a, b) for a, b in zip(outs[1], outs[2])), prec
+    assert ctx.stats().tile_wait_timeouts == 0
 
 
 def _dev(case):
