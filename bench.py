@@ -111,6 +111,8 @@ def parse():
     ap.add_argument("--profile-lanes", type=int, default=1,
                     help="transform streams in the profile run (1: per-launch events time one kernel each)")
     ap.add_argument("--profile-xy", type=int, default=-1, help="fused x + y pass: -1 built-in, 0 off, 1 on")
+    ap.add_argument("--profile-fft", default=None, metavar="NX,NY,NZ",
+                    help="per-pass timing of the forward and inverse transform of one grid, then exit")
     ap.add_argument("--profile-tile-z", type=int, default=None,
                     help="z pass: -1 built-in, 1 register-resident, 2 register-resident with TMA tile loads")
     return ap.parse_args()
@@ -1043,9 +1045,38 @@ def run_profile_unit(args):
     ctx.close()
 
 
+def run_profile_fft(args):
+    """Per-pass device times of the forward and inverse transform of one
+    grid (CUDA events around every launch): one grid on the device, so a
+    full-size pass can be captured with little memory held."""
+    import torch
+
+    from crava_b200 import api, synth
+
+    nx, ny, nz = (int(v) for v in args.profile_fft.split(","))
+    case = synth.make_case(nx, ny, nz, (10.0,), 0.1, seed=3)
+    ctx = api.Context(case)
+    t = ctx.tuning()
+    tz = t.cols_z_tile if args.profile_tile_z is None else args.profile_tile_z
+    ctx.set_tuning(t.cols_y_tile, tz, 0, 1, t.rows_x, t.kappa_refine, args.profile_xy)
+    g = api.to_device(case.data[0])
+    ctx.set_profiling(True)
+    for _ in range(args.profile_reps):
+        ctx.fft_r2c(g, api.DATA)
+        ctx.fft_c2r(g, api.DATA)
+    torch.cuda.synchronize()
+    for k, v in ctx.profile().items():
+        per = v[1] / v[0]
+        print(f"{k:18s} launches {v[0]:4d}  {per:.4f} ms/launch  {v[2] / (per * 1e-3) / 1e9:8.1f} GB/s")
+    print("tile_wait_timeouts", ctx.stats().tile_wait_timeouts)
+    ctx.close()
+
+
 def main():
     args = parse()
-    if args.profile_unit:
+    if args.profile_fft:
+        run_profile_fft(args)
+    elif args.profile_unit:
         run_profile_unit(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -64,7 +64,7 @@ struct ZT {
   static constexpr int NBOX = N / BOXROWS;
   static constexpr uint32_t BYTES = (uint32_t)BUF * 8u;
   static __device__ __forceinline__ int phys(int o) { return o ^ ((o >> K0) & 1); }
-  static constexpr size_t smem() { return 1024 + 2 * (size_t)BYTES + 8 * (size_t)N + 16; }
+  static constexpr size_t smem() { return 1024 + 2 * (size_t)BYTES + 8 * (size_t)rr::tw_slots<N>() + 16; }
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -134,7 +134,7 @@ struct ZTmaStages {
                                              float2 *g, long long L, bool ok) {
     constexpr int E = Z::E, T = Z::T, CPT = Z::CPT, R = CtRadix::at(N, S);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) rr::stage_compute<N, S, DIR, E, T>(v[c], tw, t);
+    for (int c = 0; c < CPT; ++c) rr::stage_compute_st<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: the outputs sit at the positions loaded, straight to HBM
       if (ok) {
@@ -189,14 +189,14 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
   using Z = ZT<N>;
   constexpr int E = Z::E, T = Z::T, CPT = Z::CPT, NP = Z::NP, R0 = CtRadix::at(N, 0);
   extern __shared__ unsigned char smraw[];
-  // two tile buffers on a 1024-byte boundary, then the twiddles and the
-  // two tile barriers
+  // two tile buffers on a 1024-byte boundary, then the per-stage twiddle
+  // tables and the two tile barriers
   const uint32_t s0 = smem_u32(smraw);
   const uint32_t pad = ((s0 + 1023u) & ~1023u) - s0;
   float2 *buf = reinterpret_cast<float2 *>(smraw + pad);
   float2 *tw = buf + 2 * Z::BUF;
   const uint32_t bufs = s0 + pad;
-  const uint32_t mbs = smem_u32(tw + N);
+  const uint32_t mbs = smem_u32(tw + rr::tw_slots<N>());
   const int tid = threadIdx.x;
   const int p = tid % NP, t = tid / NP;
   if (tid == 0) {
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
     mbar_init(mbs + 8, 1);
     mbar_init_fence();
   }
-  for (int i = tid; i < N; i += Z::NTH) tw[i] = a.tw[i];
+  rr::tw_stages_fill<N>(tw, a.tw, tid, Z::NTH);
   __syncthreads();
   const int G = (int)gridDim.x;
   int tile = (int)blockIdx.x;

@@ -408,7 +408,7 @@ struct RrColStages {
                                              long long es, const bool *ok) {
     constexpr int E = RrCols<N>::E, T = RrCols<N>::T, R = CtRadix::at(N, S);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) rr::stage_compute<N, S, DIR, E, T>(v[c], tw, t);
+    for (int c = 0; c < CPT; ++c) rr::stage_compute_st<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: outputs at the loaded positions, straight to HBM
 #pragma unroll
@@ -465,11 +465,11 @@ __global__ void __launch_bounds__(RrCols<N>::NTH) k_cols_rr(const __grid_constan
   constexpr int E = C::E, T = C::T, CPT = C::CPT, NP = C::NP;
   constexpr int R0 = CtRadix::at(N, 0);
   extern __shared__ float4 sm4[];
-  float2 *tw = reinterpret_cast<float2 *>(sm4);
-  float2 *buf = tw + N;  // [N][kRrTX]
+  float2 *tw = reinterpret_cast<float2 *>(sm4);  // per-stage twiddle tables
+  float2 *buf = tw + rr::tw_slots<N>();          // [N][kRrTX]
   const int tid = threadIdx.x;
   const int p = tid % NP, t = tid / NP;
-  for (int i = tid; i < N; i += C::NTH) tw[i] = a.tw[i];
+  rr::tw_stages_fill<N>(tw, a.tw, tid, C::NTH);
   float2 *gp[CPT];
   bool ok[CPT];
 #pragma unroll
@@ -532,7 +532,7 @@ template <int N, int DIR, int S>
 struct RrRowStages {
   static __device__ __forceinline__ void run(float2 (&v)[RrRows<N>::E], float2 *row, const float2 *tw, int t) {
     constexpr int E = RrRows<N>::E, T = RrRows<N>::T, R = CtRadix::at(N, S);
-    rr::stage_compute<N, S, DIR, E, T>(v, tw, t);
+    rr::stage_compute_st<N, S, DIR, E, T>(v, tw, t);
     if constexpr (S + 1 < CtRadix::count(N)) {
       if (S > 0) __syncthreads();
 #pragma unroll
@@ -556,12 +556,12 @@ __global__ void __launch_bounds__(RrRows<N>::NTH) k_rows_rr(const __grid_constan
   constexpr int E = C::E, T = C::T, R0 = C::R0, S = CtRadix::count(N);
   constexpr int RL = CtRadix::at(N, S - 1);
   extern __shared__ float4 sm4[];
-  float2 *tw = reinterpret_cast<float2 *>(sm4);  // N
-  float2 *post = tw + N;                          // N + 1
+  float2 *tw = reinterpret_cast<float2 *>(sm4);  // per-stage twiddle tables
+  float2 *post = tw + rr::tw_slots<N>();          // N + 1
   float2 *buf = post + N + 1;                     // ROWS rows of pitch P
   const int tid = threadIdx.x;
   const int t = tid % T, r = tid / T;
-  for (int i = tid; i < N; i += C::NTH) tw[i] = a.tw[i];
+  rr::tw_stages_fill<N>(tw, a.tw, tid, C::NTH);
   for (int i = tid; i <= N; i += C::NTH) post[i] = a.post[i];
   const long long row_idx = (long long)blockIdx.x * C::ROWS + r;
   const bool ok = row_idx < a.nrows;
@@ -791,7 +791,7 @@ int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t 
 #define CRAVA_ROWS_RR(NN)                                                                      \
     if (n == NN) {                                                                             \
       const dim3 g2((unsigned)((a.nrows + RrRows<NN>::ROWS - 1) / RrRows<NN>::ROWS));          \
-      const size_t sm2 = sizeof(float2) * ((size_t)NN + NN + 1 + (size_t)RrRows<NN>::ROWS * RrRows<NN>::P); \
+      const size_t sm2 = sizeof(float2) * ((size_t)rr::tw_slots<NN>() + NN + 1 + (size_t)RrRows<NN>::ROWS * RrRows<NN>::P); \
       const void *f = dir < 0 ? (const void *)k_rows_rr<NN, -1> : (const void *)k_rows_rr<NN, 1>; \
       int r2 = set_smem(f, sm2);                                                               \
       if (r2) return r2;                                                                       \
@@ -884,7 +884,7 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
     const dim3 g2((unsigned)((r.nlines + kRrTX - 1) / kRrTX));
 #define CRAVA_COLS_RR(NN)                                                                           \
     if (n == NN) {                                                                                  \
-      const size_t sm2 = sizeof(float2) * ((size_t)NN + (size_t)NN * kRrTX);                        \
+      const size_t sm2 = sizeof(float2) * ((size_t)rr::tw_slots<NN>() + (size_t)NN * kRrTX);        \
       const void *f = dir < 0 ? (vec ? (const void *)k_cols_rr<NN, -1, true> : (const void *)k_cols_rr<NN, -1, false>) \
                               : (vec ? (const void *)k_cols_rr<NN, 1, true> : (const void *)k_cols_rr<NN, 1, false>);  \
       int r2 = set_smem(f, sm2);                                                                    \

@@ -65,6 +65,70 @@ __device__ __forceinline__ void stage_compute(float2 *v, const float2 *__restric
   }
 }
 
+// Per-stage twiddle tables.  Stage S >= 1 multiplies input q of butterfly
+// j by W_N^{q (j mod NS) TSTEP}; reading those from the length-N table puts
+// the threads of a warp on addresses that are multiples of TSTEP apart,
+// most of them in the same bank.  The stage's own table holds the same
+// values at q NS + (j mod NS), so the lanes of a warp, which differ in j,
+// read consecutive entries: no bank conflicts, and the same floats (the
+// outputs do not change).  Stage 0 (NS = 1) has no twiddles.
+template <int N>
+struct TwStages {
+  __host__ __device__ static constexpr int off(int s) {
+    int o = 0;
+    for (int i = 1; i < s; ++i) o += CtRadix::at(N, i) * CtRadix::ns(N, i);
+    return o;
+  }
+  __host__ __device__ static constexpr int size() { return off(CtRadix::count(N)); }
+};
+
+// Shared-memory float2 slots of the per-stage tables (at least N, so the
+// layouts that held the length-N table keep their offsets' alignment).
+template <int N>
+__host__ __device__ constexpr int tw_slots() {
+  return TwStages<N>::size() > N ? TwStages<N>::size() : N;
+}
+
+// Fills the per-stage tables of length N from the length-N table tw (one
+// pass of the CTA's nth threads).
+template <int N>
+__device__ __forceinline__ void tw_stages_fill(float2 *tws, const float2 *__restrict__ tw, int tid, int nth) {
+  for (int i = tid; i < TwStages<N>::size(); i += nth) {
+    int s = 1, o = 0;
+    while (o + CtRadix::at(N, s) * CtRadix::ns(N, s) <= i) {
+      o += CtRadix::at(N, s) * CtRadix::ns(N, s);
+      ++s;
+    }
+    const int ns = CtRadix::ns(N, s), r = i - o, q = r / ns, base = r % ns;
+    tws[i] = tw[q * base * (N / (ns * CtRadix::at(N, s)))];
+  }
+}
+
+// stage_compute with the twiddles from the per-stage tables.
+template <int N, int S, int DIR, int E, int T>
+__device__ __forceinline__ void stage_compute_st(float2 *v, const float2 *__restrict__ tws, int t) {
+  constexpr int R = CtRadix::at(N, S);
+  constexpr int NS = CtRadix::ns(N, S);
+  constexpr int OFF = TwStages<N>::off(S);
+#pragma unroll
+  for (int b = 0; b < E / R; ++b) {
+    float2 *w = v + b * R;
+    if (NS > 1) {
+      const int j = t + T * b;
+      const int base = j % NS;
+      if (base != 0) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+          float2 x = tws[OFF + q * NS + base];
+          if (DIR > 0) x.y = -x.y;
+          w[q] = cmul(w[q], x);
+        }
+      }
+    }
+    Dft<R, DIR>::run(w);
+  }
+}
+
 // Output element of register (b, q) after stage S.
 template <int N, int S, int T>
 __device__ __forceinline__ int stage_out(int t, int b, int q) {
