@@ -1033,6 +1033,8 @@ def run_profile_unit(args):
     d = lambda gs: [api.to_device(g) for g in gs]
     src = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
     dst = (d(case.mu), d(case.data), d(case.cov), d([case.err_corr])[0])
+    # untimed warm-up: the first launch of every kernel loads its module
+    ctx.posterior_unit_oop(src, dst, args.profile_precision)
     ctx.set_profiling(True)
     for _ in range(args.profile_reps):
         ctx.posterior_unit_oop(src, dst, args.profile_precision)
@@ -1060,6 +1062,10 @@ def run_profile_fft(args):
     tz = t.cols_z_tile if args.profile_tile_z is None else args.profile_tile_z
     ctx.set_tuning(t.cols_y_tile, tz, 0, 1, t.rows_x, t.kappa_refine, args.profile_xy)
     g = api.to_device(case.data[0])
+    # untimed warm-up: the first launch of every kernel loads its module
+    ctx.fft_r2c(g, api.DATA)
+    ctx.fft_c2r(g, api.DATA)
+    torch.cuda.synchronize()
     ctx.set_profiling(True)
     for _ in range(args.profile_reps):
         ctx.fft_r2c(g, api.DATA)

@@ -408,7 +408,7 @@ struct RrColStages {
                                              long long es, const bool *ok) {
     constexpr int E = RrCols<N>::E, T = RrCols<N>::T, R = CtRadix::at(N, S);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) rr::stage_compute_st<N, S, DIR, E, T>(v[c], tw, t);
+    for (int c = 0; c < CPT; ++c) rr::stage_compute<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: outputs at the loaded positions, straight to HBM
 #pragma unroll
@@ -465,11 +465,11 @@ __global__ void __launch_bounds__(RrCols<N>::NTH) k_cols_rr(const __grid_constan
   constexpr int E = C::E, T = C::T, CPT = C::CPT, NP = C::NP;
   constexpr int R0 = CtRadix::at(N, 0);
   extern __shared__ float4 sm4[];
-  float2 *tw = reinterpret_cast<float2 *>(sm4);  // per-stage twiddle tables
-  float2 *buf = tw + rr::tw_slots<N>();          // [N][kRrTX]
+  float2 *tw = reinterpret_cast<float2 *>(sm4);
+  float2 *buf = tw + N;  // [N][kRrTX]
   const int tid = threadIdx.x;
   const int p = tid % NP, t = tid / NP;
-  rr::tw_stages_fill<N>(tw, a.tw, tid, C::NTH);
+  for (int i = tid; i < N; i += C::NTH) tw[i] = a.tw[i];
   float2 *gp[CPT];
   bool ok[CPT];
 #pragma unroll
@@ -532,7 +532,10 @@ template <int N, int DIR, int S>
 struct RrRowStages {
   static __device__ __forceinline__ void run(float2 (&v)[RrRows<N>::E], float2 *row, const float2 *tw, int t) {
     constexpr int E = RrRows<N>::E, T = RrRows<N>::T, R = CtRadix::at(N, S);
-    rr::stage_compute_st<N, S, DIR, E, T>(v, tw, t);
+    // the inverse reads its twiddles from the per-stage tables (measured
+    // faster there; the forward is faster with the length-N table)
+    if constexpr (DIR > 0) rr::stage_compute_st<N, S, DIR, E, T>(v, tw, t);
+    else rr::stage_compute<N, S, DIR, E, T>(v, tw, t);
     if constexpr (S + 1 < CtRadix::count(N)) {
       if (S > 0) __syncthreads();
 #pragma unroll
@@ -556,12 +559,16 @@ __global__ void __launch_bounds__(RrRows<N>::NTH) k_rows_rr(const __grid_constan
   constexpr int E = C::E, T = C::T, R0 = C::R0, S = CtRadix::count(N);
   constexpr int RL = CtRadix::at(N, S - 1);
   extern __shared__ float4 sm4[];
-  float2 *tw = reinterpret_cast<float2 *>(sm4);  // per-stage twiddle tables
+  float2 *tw = reinterpret_cast<float2 *>(sm4);  // twiddles (per-stage tables in the inverse)
   float2 *post = tw + rr::tw_slots<N>();          // N + 1
   float2 *buf = post + N + 1;                     // ROWS rows of pitch P
   const int tid = threadIdx.x;
   const int t = tid % T, r = tid / T;
-  rr::tw_stages_fill<N>(tw, a.tw, tid, C::NTH);
+  if constexpr (DIR > 0) {
+    rr::tw_stages_fill<N>(tw, a.tw, tid, C::NTH);
+  } else {
+    for (int i = tid; i < N; i += C::NTH) tw[i] = a.tw[i];
+  }
   for (int i = tid; i <= N; i += C::NTH) post[i] = a.post[i];
   const long long row_idx = (long long)blockIdx.x * C::ROWS + r;
   const bool ok = row_idx < a.nrows;
@@ -884,7 +891,7 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
     const dim3 g2((unsigned)((r.nlines + kRrTX - 1) / kRrTX));
 #define CRAVA_COLS_RR(NN)                                                                           \
     if (n == NN) {                                                                                  \
-      const size_t sm2 = sizeof(float2) * ((size_t)rr::tw_slots<NN>() + (size_t)NN * kRrTX);        \
+      const size_t sm2 = sizeof(float2) * ((size_t)NN + (size_t)NN * kRrTX);                        \
       const void *f = dir < 0 ? (vec ? (const void *)k_cols_rr<NN, -1, true> : (const void *)k_cols_rr<NN, -1, false>) \
                               : (vec ? (const void *)k_cols_rr<NN, 1, true> : (const void *)k_cols_rr<NN, 1, false>);  \
       int r2 = set_smem(f, sm2);                                                                    \
@@ -962,7 +969,8 @@ int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
 
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  if (p.tile_z == 2 && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
+  // the TMA-fed pass is the default where the grid allows it
+  if ((p.tile_z == 2 || p.tile_z == -1) && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
   return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z == 2 ? -1 : p.tile_z, s);
 }
 
