@@ -32,6 +32,7 @@
 // bounded, for the copies it still has in flight, and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <stdlib.h>
 
 #include "fft.cuh"
 #include "fft_rr.cuh"
@@ -123,6 +124,7 @@ struct ZTmaArgs {
   float2 *data;
   long long L;  // lines, = complex values per z plane
   int ntiles;
+  int tpc;  // tiles per CTA (0: persistent grid of the resident CTAs)
   const float2 *tw;
 };
 
@@ -206,15 +208,18 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
   }
   rr::tw_stages_fill<N>(tw, a.tw, tid, Z::NTH);
   __syncthreads();
-  const int G = (int)gridDim.x;
-  int tile = (int)blockIdx.x;
+  // tiles of this CTA: blockIdx.x, + gridDim.x, ... (persistent grid,
+  // tpc 0) or the run of tpc tiles from blockIdx.x * tpc
+  const int G = a.tpc > 0 ? 1 : (int)gridDim.x;
+  int tile = a.tpc > 0 ? (int)blockIdx.x * a.tpc : (int)blockIdx.x;
+  const int end = a.tpc > 0 ? min(tile + a.tpc, a.ntiles) : a.ntiles;
   if (tid == 0) {
-    if (tile < a.ntiles) issue_tile<N>(&tm, bufs, mbs, tile);
-    if (tile + G < a.ntiles) issue_tile<N>(&tm, bufs + Z::BYTES, mbs + 8, tile + G);
+    if (tile < end) issue_tile<N>(&tm, bufs, mbs, tile);
+    if (tile + G < end) issue_tile<N>(&tm, bufs + Z::BYTES, mbs + 8, tile + G);
   }
   int k = 0;
   bool gave_up = false;
-  for (; tile < a.ntiles; tile += G, ++k) {
+  for (; tile < end; tile += G, ++k) {
     const int sb = k & 1;
     float2 *B = buf + sb * Z::BUF;
     const bool landed = mbar_wait_bounded(mbs + 8u * sb, (uint32_t)(k >> 1) & 1u);
@@ -241,14 +246,27 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
     ZTmaStages<N, DIR, 0>::run(v, B, tw, t, p, a.data + f, a.L, f < a.L);
     fence_proxy_async_smem();
     __syncthreads();  // every thread is done with this buffer
-    if (tid == 0 && tile + 2 * G < a.ntiles) issue_tile<N>(&tm, bufs + sb * Z::BYTES, mbs + 8u * sb, tile + 2 * G);
+    if (tid == 0 && tile + 2 * G < end) issue_tile<N>(&tm, bufs + sb * Z::BYTES, mbs + 8u * sb, tile + 2 * G);
   }
   if (gave_up && tid == 0) {
     atomicAdd(&g_tile_wait_timeouts, 1ull);
     // the copies still in flight: this tile's and the next one's
     mbar_wait_bounded(mbs + 8u * (k & 1), (uint32_t)(k >> 1) & 1u);
-    if (tile + G < a.ntiles) mbar_wait_bounded(mbs + 8u * ((k + 1) & 1), (uint32_t)((k + 1) >> 1) & 1u);
+    if (tile + G < end) mbar_wait_bounded(mbs + 8u * ((k + 1) & 1), (uint32_t)((k + 1) >> 1) & 1u);
   }
+}
+
+// Tiles per CTA: a run of a few tiles per CTA leaves the hardware to
+// balance the CTAs (and lets kernels of other grids, on other streams,
+// share the SMs), where a persistent grid fixes every CTA's share up
+// front.  CRAVA_ZTMA_TPC overrides it for measurements (0: persistent).
+int tiles_per_cta() {
+  static const int v = [] {
+    const char *e = getenv("CRAVA_ZTMA_TPC");
+    const int x = e ? atoi(e) : 4;
+    return x < 0 || x > 64 ? 4 : x;
+  }();
+  return v;
 }
 
 using EncodeTiled = PFN_cuTensorMapEncodeTiled_v12000;
@@ -283,7 +301,7 @@ int launch_z_tma(const CUtensorMap &tm, const ZTmaArgs &a, cudaStream_t s) {
   if ((rc = func_smem(fn, Z::smem()))) return rc;
   int ctas = 0;
   if ((rc = resident_ctas(fn, Z::NTH, Z::smem(), &ctas))) return rc;
-  const int grid = a.ntiles < ctas ? a.ntiles : ctas;
+  const int grid = a.tpc > 0 ? (a.ntiles + a.tpc - 1) / a.tpc : (a.ntiles < ctas ? a.ntiles : ctas);
   k_cols_z_tma<N, DIR><<<grid, Z::NTH, Z::smem(), s>>>(tm, a);
   CRAVA_LAUNCH_CHECK();
   return CRAVA_GPU_OK;
@@ -315,6 +333,7 @@ int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   a.data = grid;
   a.L = L;
   a.ntiles = (int)((L + kTileLines - 1) / kTileLines);
+  a.tpc = tiles_per_cta();
   a.tw = p.z.tw;
   switch (n) {
     case 64: return dir < 0 ? launch_z_tma<64, -1>(tm, a, s) : launch_z_tma<64, 1>(tm, a, s);
