@@ -63,6 +63,16 @@ def solve_flops_per_inverted_bin(nt):
     return build + chol + 4 * fwd + 3 * 7 * nt + gram + 20 * nt + 3 * 8 * nt + (6 + 20 * nt)
 
 
+def wb_flops_per_inverted_bin(nt):
+    """FP64 flops of the Woodbury form on one inverted bin (an FMA counts
+    2): the prior-mean residual d - K mu, t = T r with the per-plane
+    whitening T, the weights c_i = 1 / (lambda m_i + 1), g = W^H diag(c) t,
+    P = sum_i c_i H_i, the 3x3 prior Cholesky, Q = LS^T P LS, the 3x3
+    complex Cholesky of I + Q, Z = R^-1 LS^T, S_post = Z^H Z, the mean
+    update S_post g and the residual."""
+    return 8 * nt * nt + 87 * nt + 403
+
+
 def hbm_peak():
     """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json
     (written per pod by the driver), else the pool's earlier measurement."""
@@ -879,9 +889,14 @@ def run_own(args):
         solve_stage["mixed_over_fp64_speed"] = round(solve_ms["fp64"] / solve_ms["mixed"], 4)
         solve_stage["unit_bound_any_solve"] = round(ms / (ms - solve_ms["fp64"]), 4)
     if solve_ms.get("fp64"):
-        fl = solve_flops_per_inverted_bin(nt) * n_inv_bins
+        # the FP64 form of a context runs the Woodbury kernel unless its
+        # tuning picks a square-root shape (0-5)
+        woodbury = ctx.tuning().solve_shape in (-1, 6)
+        fpb = wb_flops_per_inverted_bin(nt) if woodbury else solve_flops_per_inverted_bin(nt)
+        fl = fpb * n_inv_bins
         tf = fl / (solve_ms["fp64"] * 1e-3) / 1e12
-        solve_stage["fp64_flops_per_inverted_bin"] = solve_flops_per_inverted_bin(nt)
+        solve_stage["fp64_form"] = "woodbury" if woodbury else "square-root"
+        solve_stage["fp64_flops_per_inverted_bin"] = fpb
         solve_stage["fp64_tflops"] = round(tf, 2)
         solve_stage["fp64_frac_of_nominal"] = round(tf / FP64_NOMINAL_TFLOPS, 4)
         solve_stage["fp64_peak_note"] = ("nominal FP64 vector rate 148 SMs x 128 flop/clk x 1.965 GHz "

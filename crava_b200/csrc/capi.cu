@@ -421,8 +421,10 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   if (cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
   for (auto &e : c->lane_join)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+  if ((rc = kz_woodbury_alloc(nzp, (long long)c->g.cnxp * c->g.nyp, &c->tables))) return fail(rc);
   if ((rc = kz_tables_build(c->p, &c->tables, c->stream))) return fail(rc);
   if ((rc = kz_order_build(nzp, &c->tables, c->stream, &c->n_inverted))) return fail(rc);
+  if ((rc = kz_woodbury_build(c->consts, nzp, c->tables, c->stream))) return fail(rc);
   *out = c;
   return CRAVA_GPU_OK;
 }
@@ -832,7 +834,9 @@ int crava_gpu_set_kz_tables(crava_gpu_ctx *c, const float *wd, const float *e1, 
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e2, e2, n * sizeof(float2), cudaMemcpyHostToDevice));
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.e3, e3, n * sizeof(float), cudaMemcpyHostToDevice));
   CRAVA_CUDA_TRY(cudaMemcpy(c->tables.inv, inv, (size_t)c->p.nzp * sizeof(int), cudaMemcpyHostToDevice));
-  return kz_order_build(c->p.nzp, &c->tables, c->stream, &c->n_inverted);
+  int rc = kz_order_build(c->p.nzp, &c->tables, c->stream, &c->n_inverted);
+  if (rc) return rc;
+  return kz_woodbury_build(c->consts, c->p.nzp, c->tables, c->stream);
 }
 
 }  // extern "C"

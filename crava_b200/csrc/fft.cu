@@ -969,8 +969,9 @@ int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
 
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  // the TMA-fed pass is the default where the grid allows it
-  if ((p.tile_z == 2 || p.tile_z == -1) && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
+  // the TMA-fed pass (tile choice 2): faster alone, slower in the unit's
+  // two-lane overlap, so not the built-in choice
+  if (p.tile_z == 2 && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
   return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z == 2 ? -1 : p.tile_z, s);
 }
 

@@ -26,8 +26,7 @@ struct FftPlans {
   // per CTA in the in-place pass (lengths with compiled kernels only; other
   // lengths use the generic pass), 2 (z only) the register-resident pass
   // with TMA tile loads where cols_z_tma_supported.  The default is the
-  // TMA-fed pass (z) where supported, else the register-resident pass
-  // where it exists, else the in-place pass.
+  // register-resident pass where it exists, else the in-place pass.
   int tile_y = -1, tile_z = -1;
   // x pass of an even nxp: -1 default (register-resident where the half
   // length is 64..512), 0 the in-place pass, 1 register-resident

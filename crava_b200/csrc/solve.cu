@@ -25,6 +25,7 @@
 #include "fft_core.cuh"
 #include "solve.cuh"
 #include "solve_bin.cuh"
+#include "woodbury.cuh"
 
 namespace crava {
 
@@ -155,6 +156,11 @@ struct SolveArgs {
   long long csize, plane;
   long long bpp;  // blocks per kz plane
   DevCounters *counters;
+  // Woodbury form: the per-plane tables and the deferral flags it writes;
+  // `only` (the square-root kernel after it): run only the flagged blocks
+  const sb::WbTable *wb = nullptr;
+  unsigned char *defer = nullptr;
+  const unsigned char *only = nullptr;
 };
 
 // Square-root form (solve_bin.cuh): the FP64 and mixed forms.  One kz
@@ -182,6 +188,7 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
   extern __shared__ double2 sq_sm[];
   auto &kc = *reinterpret_cast<sb::KzConst<NT> *>(sq_sm);
   char *area = reinterpret_cast<char *>(sq_sm) + SM::kconst;
+  if (a.only && !a.only[blockIdx.x]) return;  // a block the Woodbury kernel solved
   const int slot = (int)(blockIdx.x / a.bpp);
   const long long off = (long long)(blockIdx.x % a.bpp) * NTH + threadIdx.x;
   const int k = a.t.order ? a.t.order[slot] : slot;
@@ -413,6 +420,101 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
   return CRAVA_GPU_OK;
 }
 
+// FP64 solve in the Woodbury form (woodbury.cuh), one bin per thread and
+// one kz plane per block (the grid of k_solve_sq with NTH threads, so the
+// square-root kernel that follows can take over a block).  A block stages
+// its plane's table in shared memory; if any of its bins cannot use the
+// form (plane table not usable, prior not positive definite, lambda m_i + 1
+// not positive), the block writes nothing but its deferral flag, and the
+// square-root kernel solves that block.  Band-gated blocks write the prior
+// covariance as k_solve_sq does.
+template <int NT, int NTH, int MINB>
+__global__ void __launch_bounds__(NTH, MINB) k_solve_wb(SolveArgs a) {
+  __shared__ sb::WbTable wt;
+  __shared__ float2 wds[NT];
+  const int slot = (int)(blockIdx.x / a.bpp);
+  const long long off = (long long)(blockIdx.x % a.bpp) * NTH + threadIdx.x;
+  const int k = a.t.order ? a.t.order[slot] : slot;
+  const bool inv = a.t.inv[k] != 0;
+  const bool valid = off < a.plane;
+  const long long idx = (long long)k * a.plane + (valid ? off : 0);
+  if (!inv) {
+    if (threadIdx.x == 0) a.defer[blockIdx.x] = 0;
+    if (!valid) return;
+    float2 c6[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
+    sb::prior_only<0>(a.c, c6);
+    bool nonfinite = false;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) { a.g.cov[t][idx] = c6[t]; nonfinite |= !sb::fin2(c6[t]); }
+    if (a.counters) sb::count(a.counters, false, nonfinite);
+    return;
+  }
+  {
+    const double *src = reinterpret_cast<const double *>(a.wb + k);
+    double *dst = reinterpret_cast<double *>(&wt);
+    for (int i = threadIdx.x; i < (int)(sizeof(sb::WbTable) / sizeof(double)); i += NTH) dst[i] = src[i];
+    if (threadIdx.x < NT) wds[threadIdx.x] = a.t.wd[(long long)k * NT + threadIdx.x];
+  }
+  __syncthreads();
+  double L[6], cw[NT];
+  bool ok = true;
+  if (valid) {
+    float2 c6[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
+    const sb::Sym3d S = sb::prior_exact(c6, a.c.var0);
+    const double lam = fabs((double)a.g.err[idx].x);
+    ok = wt.ok != 0;
+    ok = sb::chol3(S, L) && ok;
+    ok = sb::wb_weights<NT>(wt, lam, cw) && ok;
+  }
+  const bool defer = __syncthreads_or(!ok);
+  if (threadIdx.x == 0) a.defer[blockIdx.x] = defer ? 1 : 0;
+  if (defer || !valid) return;
+  const sb::GlobalIn gin{&a.g, idx};
+  const bool fin = sb::solve_bin_wb<NT>(wt, a.c, wds, L, cw, a.g, idx, gin);
+  if (a.counters) sb::count(a.counters, false, !fin);
+}
+
+// Per-plane Woodbury tables, one thread per kz plane.
+template <int NT>
+__global__ void k_kz_wb(SolveConsts c, KzTables t, int nzp) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nzp) return;
+  sb::WbTable *w = reinterpret_cast<sb::WbTable *>(t.wb) + k;
+  const long long o = (long long)k * NT;
+  sb::WbTable tmp;
+  sb::wb_table_fill<NT>(tmp, c, t.wd + o, t.e1 + o, t.e2 + o, t.e3 + o);
+  if (!t.inv[k]) tmp.ok = 0;
+  *w = tmp;
+}
+
+template <int NTH, int MINB>
+int launch_solve_wb(SolveArgs a, int nt, cudaStream_t s) {
+  a.bpp = (a.plane + NTH - 1) / NTH;
+  const long long nblk = a.bpp * (a.csize / a.plane);
+  if (nblk > a.t.defer_n) return CRAVA_GPU_ERR_ARG;
+  a.wb = reinterpret_cast<const sb::WbTable *>(a.t.wb);
+  a.defer = a.t.defer;
+  dim3 grd((unsigned)nblk);
+#define CRAVA_WB_CASE(N)                                 \
+  case N:                                                \
+    k_solve_wb<N, NTH, MINB><<<grd, NTH, 0, s>>>(a);     \
+    break;
+  switch (nt) {
+    CRAVA_WB_CASE(1) CRAVA_WB_CASE(2) CRAVA_WB_CASE(3) CRAVA_WB_CASE(4)
+    CRAVA_WB_CASE(5) CRAVA_WB_CASE(6) CRAVA_WB_CASE(7) CRAVA_WB_CASE(8)
+    default: return CRAVA_GPU_ERR_ARG;
+  }
+#undef CRAVA_WB_CASE
+  CRAVA_LAUNCH_CHECK();
+  // the deferred blocks: the square-root form (same grid, same blocks)
+  a.only = a.t.defer;
+  return launch_solve_sq<0, NTH, 4, true>(a, nt, s);
+}
+
 // Launch shape of the square-root solve: 0 the factor in shared memory
 // (256 threads, two blocks per SM), 1 in registers with 128 threads and
 // three blocks per SM (up to 170 registers), 2 in registers with 256
@@ -425,15 +527,19 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
 // latency-bound on its global loads, which the pipelined kernel hides; the
 // mixed form carries the FP32 factor and the FP64 refinement operands in
 // registers, and the staging buffers cost it more occupancy than they
-// save.  So the default is shape 5 for FP64 and shape 3 for mixed.  The
-// context's tuning (SolveConsts::solve_shape) picks one explicitly, and
-// CRAVA_SOLVE_SHAPE (0-5) overrides the built-in choice for measurements.
+// save.  Shape 6 is the FP64 solve in the Woodbury form (k_solve_wb, 128
+// threads, six blocks per SM), with the square-root form of shape 3 for the
+// blocks it defers; it needs the context's Woodbury tables (not built for
+// the allocation-free entry point).  Defaults: shape 6 for FP64 where the
+// tables exist, else 5; shape 3 for mixed.  The context's tuning
+// (SolveConsts::solve_shape) picks one explicitly, and CRAVA_SOLVE_SHAPE
+// (0-6) overrides the built-in choice for measurements.
 static int solve_shape_override() {
   static int v = -2;
   if (v == -2) {
     const char *e = getenv("CRAVA_SOLVE_SHAPE");
     v = e ? atoi(e) : -1;
-    if (v < 0 || v > 5) v = -1;
+    if (v < 0 || v > 6) v = -1;
   }
   return v;
 }
@@ -441,8 +547,12 @@ static int solve_shape_override() {
 template <int PREC>
 int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
   int shape = a.c.solve_shape >= 0 ? a.c.solve_shape : solve_shape_override();
-  if (shape < 0) shape = PREC == 0 ? 5 : 3;
+  // the Woodbury form (FP64 only) needs the context's tables and flags
+  const bool wb = PREC == 0 && a.t.wb && a.t.defer;
+  if (shape < 0) shape = PREC == 0 ? (wb ? 6 : 5) : 3;
+  if (shape == 6 && !wb) shape = PREC == 0 ? 5 : 3;
   switch (shape) {
+    case 6: return launch_solve_wb<128, 6>(a, nt, s);
     case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);
     case 1: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
     case 2: return launch_solve_sq<PREC, 256, 1, true>(a, nt, s);
@@ -467,7 +577,30 @@ int kz_tables_alloc(int nzp, int nt, KzTables *t) {
 void kz_tables_free(KzTables *t) {
   cudaFree(t->wd); cudaFree(t->e1); cudaFree(t->e2); cudaFree(t->e3); cudaFree(t->inv);
   cudaFree(t->order);
+  cudaFree(t->wb);
+  cudaFree(t->defer);
   *t = KzTables{};
+}
+
+int kz_woodbury_alloc(int nzp, long long plane, KzTables *t) {
+  const long long nblk = (plane + 127) / 128 * nzp;
+  CRAVA_CUDA_TRY(cudaMalloc(&t->wb, (size_t)nzp * sizeof(sb::WbTable)));
+  CRAVA_CUDA_TRY(cudaMalloc(&t->defer, (size_t)nblk));
+  t->defer_n = nblk;
+  return CRAVA_GPU_OK;
+}
+
+int kz_woodbury_build(const SolveConsts &c, int nzp, const KzTables &t, cudaStream_t s) {
+  if (!t.wb) return CRAVA_GPU_OK;
+  const int nth = 64, nb = (nzp + nth - 1) / nth;
+  switch (c.nt) {
+#define CRAVA_KWB(N) case N: k_kz_wb<N><<<nb, nth, 0, s>>>(c, t, nzp); break;
+    CRAVA_KWB(1) CRAVA_KWB(2) CRAVA_KWB(3) CRAVA_KWB(4) CRAVA_KWB(5) CRAVA_KWB(6) CRAVA_KWB(7) CRAVA_KWB(8)
+#undef CRAVA_KWB
+    default: return CRAVA_GPU_ERR_ARG;
+  }
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
 }
 
 int kz_order_build(int nzp, KzTables *t, cudaStream_t s, int *n_inverted) {

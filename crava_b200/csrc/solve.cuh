@@ -14,6 +14,12 @@ struct KzTables {
   int *inv = nullptr;    // [nzp]      invert_frequency
   int *order = nullptr;  // [nzp]      plane visiting order of the solve
                          //            (null: natural order)
+  // FP64 solve in the Woodbury form (woodbury.cuh): the per-plane tables
+  // (sb::WbTable [nzp]) and one deferral flag per block of the solve's
+  // grid (128 bins per block); null: the form is not used
+  void *wb = nullptr;
+  unsigned char *defer = nullptr;
+  long long defer_n = 0;
 };
 
 // Constants of the solve, passed by value (kernel parameter space).
@@ -54,6 +60,12 @@ int kz_tables_alloc(int nzp, int nt, KzTables *t);
 // *n_inverted (optional) receives the number of inverted planes.
 int kz_order_build(int nzp, KzTables *t, cudaStream_t s, int *n_inverted = nullptr);
 void kz_tables_free(KzTables *t);
+// Allocates the Woodbury tables and the deferral flags for a grid of
+// `plane` bins per kz plane (the FP64 solve's default form).
+int kz_woodbury_alloc(int nzp, long long plane, KzTables *t);
+// Fills the Woodbury tables from the kz tables (one kernel on s; call after
+// the tables change).
+int kz_woodbury_build(const SolveConsts &c, int nzp, const KzTables &t, cudaStream_t s);
 // Builds the tables from the wavelets on the device (params: host struct).
 int kz_tables_build(const crava_gpu_params &p, KzTables *t, cudaStream_t s);
 

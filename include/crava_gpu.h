@@ -278,8 +278,8 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
  * column transforms (-1 the built-in choice, 0 the out-of-place pass, 1 the
  * register-resident pass of lengths 64/128/256/512, 8 or 16 columns per CTA
  * in the in-place pass, 2 (z only) the register-resident pass fed by TMA
- * tile loads, the built-in choice where the grid has an even number of
- * lines per z plane; lengths without compiled column kernels ignore it);
+ * tile loads, where the grid has an even number of lines per z plane;
+ * lengths without compiled column kernels ignore it);
  * fused: the fused unit kernels (1) or the three passes (0); ms: one unit's
  * measured time (autotune output only); lanes: more than 1 lets the
  * transforms of different grids overlap on that many streams; rows_x: the x

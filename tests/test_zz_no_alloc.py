@@ -9,7 +9,11 @@ call has other wavelets, the other thickness mode and a smaller nzp and
 ntheta, so it only passes if the call rewrites the tables and counters the
 first call left in the shared scratch.  Both calls run the same kernels on
 the same inputs as the regular entry point, so the outputs must be equal
-bit for bit; device memory in use must not change across the calls.
+bit for bit; device memory in use must not change across the calls.  (The
+FP64 form of a context defaults to the Woodbury kernel, whose per-plane
+tables live in the context; the allocation-free entry point runs the
+square-root kernel, so the regular call it is compared with selects that
+kernel, solve_shape 5.)
 
 This file is collected last on purpose."""
 import ctypes as C
@@ -57,6 +61,7 @@ def _prepare(case, prec):
     """Context, untouched spectra for the allocation-free call, and the
     regular entry point's outputs and stats on the same spectra."""
     ctx = api.Context(case)
+    ctx.set_tuning(-1, -1, 0, 2, -1, None, None, 5)
     spec = _spectra(ctx, case)
     ref = _clone(spec)
     ctx.posterior(*ref, prec)
