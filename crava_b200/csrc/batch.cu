@@ -182,7 +182,7 @@ int crava_gpu_set_tuning(crava_gpu_ctx *c, const crava_gpu_tuning *t) {
   if (t->rows_x < -1 || t->rows_x > 1) return CRAVA_GPU_ERR_ARG;
   if (!(t->kappa_refine >= 0.0f)) return CRAVA_GPU_ERR_ARG;
   if (t->xy_fused < -1 || t->xy_fused > 1) return CRAVA_GPU_ERR_ARG;
-  if (t->solve_shape < -1 || t->solve_shape > 6) return CRAVA_GPU_ERR_ARG;
+  if (t->solve_shape < -1 || t->solve_shape > 8) return CRAVA_GPU_ERR_ARG;
   if (t->lanes < 1 || t->lanes > crava_gpu_ctx::kMaxLanes) return CRAVA_GPU_ERR_ARG;
   c->plans.tile_y = t->cols_y_tile;
   c->plans.tile_z = t->cols_z_tile;

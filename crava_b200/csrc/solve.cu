@@ -20,6 +20,8 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
+
 #include <vector>
 
 #include "fft_core.cuh"
@@ -156,11 +158,10 @@ struct SolveArgs {
   long long csize, plane;
   long long bpp;  // blocks per kz plane
   DevCounters *counters;
-  // Woodbury form: the per-plane tables and the deferral flags it writes;
-  // `only` (the square-root kernel after it): run only the flagged blocks
+  // Woodbury form: the per-plane tables and the list of the blocks it
+  // defers to the square-root kernel
   const sb::WbTable *wb = nullptr;
-  unsigned char *defer = nullptr;
-  const unsigned char *only = nullptr;
+  int *list = nullptr;  // deferred blocks (count in counters->deferred)
 };
 
 // Square-root form (solve_bin.cuh): the FP64 and mixed forms.  One kz
@@ -182,15 +183,16 @@ struct SqSmem {
   static constexpr size_t bytes = kconst + per_thread * NTH;
 };
 
-template <int NT, int PREC, int NTH, int MINB, bool LREG>
-__global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
+// One block's bins (block blk of the solve's grid); every thread reaches
+// the one barrier, after which threads without a bin return.
+template <int NT, int PREC, int NTH, bool LREG>
+__device__ __forceinline__ void sq_block(const SolveArgs &a, long long blk) {
   using SM = SqSmem<NT, PREC, NTH, LREG>;
   extern __shared__ double2 sq_sm[];
   auto &kc = *reinterpret_cast<sb::KzConst<NT> *>(sq_sm);
   char *area = reinterpret_cast<char *>(sq_sm) + SM::kconst;
-  if (a.only && !a.only[blockIdx.x]) return;  // a block the Woodbury kernel solved
-  const int slot = (int)(blockIdx.x / a.bpp);
-  const long long off = (long long)(blockIdx.x % a.bpp) * NTH + threadIdx.x;
+  const int slot = (int)(blk / a.bpp);
+  const long long off = (long long)(blk % a.bpp) * NTH + threadIdx.x;
   const int k = a.t.order ? a.t.order[slot] : slot;
   const bool inv = a.t.inv[k] != 0;
   const long long o = (long long)k * NT;
@@ -259,6 +261,23 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
       const unsigned br = __ballot_sync(m, refined);
       if (br && (threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(&a.counters->refined, (unsigned long long)__popc(br));
     }
+  }
+}
+
+template <int NT, int PREC, int NTH, int MINB, bool LREG>
+__global__ void __launch_bounds__(NTH, MINB) k_solve_sq(SolveArgs a) {
+  sq_block<NT, PREC, NTH, LREG>(a, blockIdx.x);
+}
+
+// The blocks the Woodbury kernel deferred (a.list, a.counters->deferred of
+// them), walked by a small fixed grid: with no deferred block it costs one
+// counter read per CTA.
+template <int NT, int NTH, int MINB>
+__global__ void __launch_bounds__(NTH, MINB) k_solve_sq_list(SolveArgs a) {
+  const unsigned long long n = *(volatile unsigned long long *)&a.counters->deferred;
+  for (unsigned long long i = blockIdx.x; i < n; i += gridDim.x) {
+    __syncthreads();  // the previous block's per-kz constants are no longer read
+    sq_block<NT, 0, NTH, true>(a, a.list[i]);
   }
 }
 
@@ -422,12 +441,25 @@ int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
 
 // FP64 solve in the Woodbury form (woodbury.cuh), one bin per thread and
 // one kz plane per block (the grid of k_solve_sq with NTH threads, so the
-// square-root kernel that follows can take over a block).  A block stages
-// its plane's table in shared memory; if any of its bins cannot use the
-// form (plane table not usable, prior not positive definite, lambda m_i + 1
-// not positive), the block writes nothing but its deferral flag, and the
-// square-root kernel solves that block.  Band-gated blocks write the prior
-// covariance as k_solve_sq does.
+// square-root kernel can take over a block).  A thread first issues the
+// loads of all its bin's inputs, then the block stages the part of its
+// plane's table the nt angles use in shared memory (the loads are in
+// flight meanwhile).  If any bin of the block cannot use the form (plane
+// table not usable, prior not positive definite, lambda m_i + 1 not
+// positive), the block writes nothing, appends its index to the deferred
+// list, and k_solve_sq_list solves it in the square-root form.  Band-gated
+// blocks write the prior covariance as k_solve_sq does.
+template <int NT>
+struct RegIn {  // a bin's inputs held in registers
+  float2 m[3], d[NT];
+};
+template <int NT>
+struct RegInAcc {
+  const RegIn<NT> *r;
+  __device__ __forceinline__ float2 mu(int q) const { return r->m[q]; }
+  __device__ __forceinline__ float2 d(int l) const { return r->d[l]; }
+};
+
 template <int NT, int NTH, int MINB>
 __global__ void __launch_bounds__(NTH, MINB) k_solve_wb(SolveArgs a) {
   __shared__ sb::WbTable wt;
@@ -439,7 +471,6 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_wb(SolveArgs a) {
   const bool valid = off < a.plane;
   const long long idx = (long long)k * a.plane + (valid ? off : 0);
   if (!inv) {
-    if (threadIdx.x == 0) a.defer[blockIdx.x] = 0;
     if (!valid) return;
     float2 c6[6];
 #pragma unroll
@@ -451,31 +482,48 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_wb(SolveArgs a) {
     if (a.counters) sb::count(a.counters, false, nonfinite);
     return;
   }
+  float2 c6[6], ec = make_float2(0.f, 0.f);
+  RegIn<NT> in;
+  if (valid) {
+#pragma unroll
+    for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
+    ec = a.g.err[idx];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) in.m[q] = a.g.mu[q][idx];
+#pragma unroll
+    for (int l = 0; l < NT; ++l) in.d[l] = a.g.data[l][idx];
+  }
   {
-    const double *src = reinterpret_cast<const double *>(a.wb + k);
-    double *dst = reinterpret_cast<double *>(&wt);
-    for (int i = threadIdx.x; i < (int)(sizeof(sb::WbTable) / sizeof(double)); i += NTH) dst[i] = src[i];
-    if (threadIdx.x < NT) wds[threadIdx.x] = a.t.wd[(long long)k * NT + threadIdx.x];
+    // the rows i < NT of T (NT entries each), W and H, m, ok
+    const sb::WbTable &src = a.wb[k];
+    for (int e = threadIdx.x; e < NT * NT; e += NTH) wt.T[e / NT][e % NT] = src.T[e / NT][e % NT];
+    for (int e = threadIdx.x; e < NT * 3; e += NTH) wt.W[e / 3][e % 3] = src.W[e / 3][e % 3];
+    for (int e = threadIdx.x; e < NT * 9; e += NTH) wt.H[e / 9][e % 9] = src.H[e / 9][e % 9];
+    if (threadIdx.x < NT) {
+      wt.m[threadIdx.x] = src.m[threadIdx.x];
+      wds[threadIdx.x] = a.t.wd[(long long)k * NT + threadIdx.x];
+    }
+    if (threadIdx.x == 0) wt.ok = src.ok;
   }
   __syncthreads();
   double L[6], cw[NT];
   bool ok = true;
   if (valid) {
-    float2 c6[6];
-#pragma unroll
-    for (int t = 0; t < 6; ++t) c6[t] = a.g.cov[t][idx];
     const sb::Sym3d S = sb::prior_exact(c6, a.c.var0);
-    const double lam = fabs((double)a.g.err[idx].x);
     ok = wt.ok != 0;
     ok = sb::chol3(S, L) && ok;
-    ok = sb::wb_weights<NT>(wt, lam, cw) && ok;
+    ok = sb::wb_weights<NT>(wt, fabs((double)ec.x), cw) && ok;
   }
-  const bool defer = __syncthreads_or(!ok);
-  if (threadIdx.x == 0) a.defer[blockIdx.x] = defer ? 1 : 0;
-  if (defer || !valid) return;
-  const sb::GlobalIn gin{&a.g, idx};
-  const bool fin = sb::solve_bin_wb<NT>(wt, a.c, wds, L, cw, a.g, idx, gin);
-  if (a.counters) sb::count(a.counters, false, !fin);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      const unsigned long long i = atomicAdd(&a.counters->deferred, 1ull);
+      a.list[i] = (int)blockIdx.x;
+    }
+    return;
+  }
+  if (!valid) return;
+  const bool fin = sb::solve_bin_wb<NT>(wt, a.c, wds, L, cw, a.g, idx, RegInAcc<NT>{&in});
+  sb::count(a.counters, false, !fin);
 }
 
 // Per-plane Woodbury tables, one thread per kz plane.
@@ -495,24 +543,34 @@ template <int NTH, int MINB>
 int launch_solve_wb(SolveArgs a, int nt, cudaStream_t s) {
   a.bpp = (a.plane + NTH - 1) / NTH;
   const long long nblk = a.bpp * (a.csize / a.plane);
-  if (nblk > a.t.defer_n) return CRAVA_GPU_ERR_ARG;
+  if (nblk > a.t.defer_n || nblk >= (1LL << 31) || !a.counters) return CRAVA_GPU_ERR_ARG;
   a.wb = reinterpret_cast<const sb::WbTable *>(a.t.wb);
-  a.defer = a.t.defer;
+  a.list = a.t.defer_list;
   dim3 grd((unsigned)nblk);
-#define CRAVA_WB_CASE(N)                                 \
-  case N:                                                \
-    k_solve_wb<N, NTH, MINB><<<grd, NTH, 0, s>>>(a);     \
-    break;
+  // the deferred blocks: the square-root form, on a fixed grid of resident
+  // blocks (k_solve_sq's shape 3: four 128-thread blocks per SM)
+  int dev = 0, sms = 0;
+  CRAVA_CUDA_TRY(cudaGetDevice(&dev));
+  CRAVA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const unsigned g2 = (unsigned)std::min<long long>(nblk, 4LL * sms);
+  int rc;
+#define CRAVA_WB_CASE(N)                                                                           \
+  case N: {                                                                                        \
+    k_solve_wb<N, NTH, MINB><<<grd, NTH, 0, s>>>(a);                                               \
+    CRAVA_LAUNCH_CHECK();                                                                          \
+    const size_t smem = SqSmem<N, 0, NTH, true>::bytes;                                            \
+    if ((rc = func_smem((const void *)k_solve_sq_list<N, NTH, 4>, smem))) return rc;               \
+    k_solve_sq_list<N, NTH, 4><<<g2, NTH, smem, s>>>(a);                                           \
+    CRAVA_LAUNCH_CHECK();                                                                          \
+    break;                                                                                         \
+  }
   switch (nt) {
     CRAVA_WB_CASE(1) CRAVA_WB_CASE(2) CRAVA_WB_CASE(3) CRAVA_WB_CASE(4)
     CRAVA_WB_CASE(5) CRAVA_WB_CASE(6) CRAVA_WB_CASE(7) CRAVA_WB_CASE(8)
     default: return CRAVA_GPU_ERR_ARG;
   }
 #undef CRAVA_WB_CASE
-  CRAVA_LAUNCH_CHECK();
-  // the deferred blocks: the square-root form (same grid, same blocks)
-  a.only = a.t.defer;
-  return launch_solve_sq<0, NTH, 4, true>(a, nt, s);
+  return CRAVA_GPU_OK;
 }
 
 // Launch shape of the square-root solve: 0 the factor in shared memory
@@ -539,7 +597,7 @@ static int solve_shape_override() {
   if (v == -2) {
     const char *e = getenv("CRAVA_SOLVE_SHAPE");
     v = e ? atoi(e) : -1;
-    if (v < 0 || v > 6) v = -1;
+    if (v < 0 || v > 8) v = -1;
   }
   return v;
 }
@@ -548,11 +606,13 @@ template <int PREC>
 int launch_solve_sq_shape(const SolveArgs &a, int nt, cudaStream_t s) {
   int shape = a.c.solve_shape >= 0 ? a.c.solve_shape : solve_shape_override();
   // the Woodbury form (FP64 only) needs the context's tables and flags
-  const bool wb = PREC == 0 && a.t.wb && a.t.defer;
+  const bool wb = PREC == 0 && a.t.wb && a.t.defer_list && a.counters;
   if (shape < 0) shape = PREC == 0 ? (wb ? 6 : 5) : 3;
-  if (shape == 6 && !wb) shape = PREC == 0 ? 5 : 3;
+  if (shape >= 6 && !wb) shape = PREC == 0 ? 5 : 3;
   switch (shape) {
     case 6: return launch_solve_wb<128, 6>(a, nt, s);
+    case 7: return launch_solve_wb<128, 5>(a, nt, s);
+    case 8: return launch_solve_wb<128, 4>(a, nt, s);
     case 0: return launch_solve_sq<PREC, 256, 2, false>(a, nt, s);
     case 1: return launch_solve_sq<PREC, 128, 3, true>(a, nt, s);
     case 2: return launch_solve_sq<PREC, 256, 1, true>(a, nt, s);
@@ -578,14 +638,14 @@ void kz_tables_free(KzTables *t) {
   cudaFree(t->wd); cudaFree(t->e1); cudaFree(t->e2); cudaFree(t->e3); cudaFree(t->inv);
   cudaFree(t->order);
   cudaFree(t->wb);
-  cudaFree(t->defer);
+  cudaFree(t->defer_list);
   *t = KzTables{};
 }
 
 int kz_woodbury_alloc(int nzp, long long plane, KzTables *t) {
   const long long nblk = (plane + 127) / 128 * nzp;
   CRAVA_CUDA_TRY(cudaMalloc(&t->wb, (size_t)nzp * sizeof(sb::WbTable)));
-  CRAVA_CUDA_TRY(cudaMalloc(&t->defer, (size_t)nblk));
+  CRAVA_CUDA_TRY(cudaMalloc(&t->defer_list, (size_t)nblk * sizeof(int)));
   t->defer_n = nblk;
   return CRAVA_GPU_OK;
 }

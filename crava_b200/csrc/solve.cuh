@@ -15,10 +15,11 @@ struct KzTables {
   int *order = nullptr;  // [nzp]      plane visiting order of the solve
                          //            (null: natural order)
   // FP64 solve in the Woodbury form (woodbury.cuh): the per-plane tables
-  // (sb::WbTable [nzp]) and one deferral flag per block of the solve's
-  // grid (128 bins per block); null: the form is not used
+  // (sb::WbTable [nzp]) and room for the list of the blocks it defers
+  // (defer_n = blocks of its grid, 128 bins per block); null: the form is
+  // not used
   void *wb = nullptr;
-  unsigned char *defer = nullptr;
+  int *defer_list = nullptr;
   long long defer_n = 0;
 };
 
@@ -48,6 +49,7 @@ struct DevCounters {
   unsigned long long chol_fail;
   unsigned long long nonfinite;
   unsigned long long refined;  // mixed form: bins that took the FP64 refinement step
+  unsigned long long deferred; // FP64 Woodbury form: blocks left to the square-root kernel
 };
 
 // Default condition bound above which the mixed form refines a bin.
@@ -60,7 +62,7 @@ int kz_tables_alloc(int nzp, int nt, KzTables *t);
 // *n_inverted (optional) receives the number of inverted planes.
 int kz_order_build(int nzp, KzTables *t, cudaStream_t s, int *n_inverted = nullptr);
 void kz_tables_free(KzTables *t);
-// Allocates the Woodbury tables and the deferral flags for a grid of
+// Allocates the Woodbury tables and the deferred-block list for a grid of
 // `plane` bins per kz plane (the FP64 solve's default form).
 int kz_woodbury_alloc(int nzp, long long plane, KzTables *t);
 // Fills the Woodbury tables from the kz tables (one kernel on s; call after

@@ -100,7 +100,7 @@ def test_solve_shapes_match(shape, angles, prec, kappa):
     for g in cov + [err]:
         ctx.fft_r2c(g, api.COVARIANCE)
     res = {}
-    for sh in (-1, 0, 1, 2, 3, 4, 5, 6):
+    for sh in (-1, 0, 1, 2, 3, 4, 5, 6, 7, 8):
         ctx.set_tuning(-1, -1, 0, 2, -1, kappa, None, sh)
         assert ctx.tuning().solve_shape == sh
         m, d, c = [g.clone() for g in mu], [g.clone() for g in data], [g.clone() for g in cov]
@@ -109,7 +109,7 @@ def test_solve_shapes_match(shape, angles, prec, kappa):
         res[sh] = ([g.cpu().numpy() for g in m + d + c], st.chol_fail_bins, st.nonfinite_bins, st.refined_bins)
     if kappa == 0.0:
         assert res[0][3] > 0
-    woodbury = (-1, 6) if prec == api.FP64 else ()
+    woodbury = (-1, 6, 7, 8) if prec == api.FP64 else ()
     for sh in res:
         assert res[sh][1:] == res[0][1:], sh
         if sh in woodbury:
@@ -121,7 +121,7 @@ def test_solve_shapes_match(shape, angles, prec, kappa):
     if prec == api.FP64:  # the Woodbury kernel ran (its roundings differ somewhere)
         assert not all(np.array_equal(a, b) for a, b in zip(res[6][0], res[0][0]))
     with pytest.raises(api.CravaGpuError):
-        ctx.set_tuning(-1, -1, 0, 2, -1, None, None, 7)
+        ctx.set_tuning(-1, -1, 0, 2, -1, None, None, 9)
 
 
 def test_tma_z_pass_unit_matches():
