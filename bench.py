@@ -783,10 +783,38 @@ def run_own(args):
         ctx.posterior_unit_host(hmu, hdata, hcov, herr, prec)
         e2e_sync_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_sync = max_over_ranks(statistics.median(e2e_sync_ms))
-    del outs
     gbytes = case.mu[0].nbytes
     h2d = (10 + nt) * gbytes
     d2h = (9 + nt) * gbytes
+    # the host link on the same bytes and buffers: a unit's uploads alone,
+    # its downloads alone, and both at once on two streams (one copy per
+    # grid), the time the end-to-end step cannot go below
+    dev_grids = list(dst[0]) + list(dst[1]) + list(dst[2]) + [dst[3]]
+    s_up, s_dn = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def link_ms(up, down):
+        best = float("inf")
+        for _ in range(3):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            if up:
+                with torch.cuda.stream(s_up):
+                    for h, d in zip(host, dev_grids):
+                        d.copy_(h, non_blocking=True)
+            if down:
+                with torch.cuda.stream(s_dn):
+                    for h, d in zip(outs[1][:9 + nt], dev_grids[:9 + nt]):
+                        h.copy_(d, non_blocking=True)
+            torch.cuda.synchronize(dev)
+            best = min(best, (time.perf_counter() - t0) * 1e3)
+        return best
+
+    up_ms, down_ms, both_ms = link_ms(True, False), link_ms(False, True), link_ms(True, True)
+    link = {"h2d_GBps": round(h2d / (up_ms * 1e-3) / 1e9, 1), "d2h_GBps": round(d2h / (down_ms * 1e-3) / 1e9, 1),
+            "both_ms": round(both_ms, 2), "frac_of_link_bound": round(both_ms / e2e_step, 3),
+            "how": "the unit's input grids up and output grids down, pinned buffers, one copy per grid, "
+                   "two streams at once; best of 3"}
+    del outs
 
     # simulation: realisations of the posterior (Crava::simulate) from the
     # posterior covariance spectra, 8 realisations per call
@@ -935,7 +963,7 @@ def run_own(args):
         "e2e": {"value": world * cells / (e2e_step * 1e-3), "unit": "cells/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step,
                 "steps": k_e2e, "pipelined": "two steps in flight (crava_gpu_posterior_unit_host_async)",
-                "sync_ms_per_step": e2e_sync},
+                "sync_ms_per_step": e2e_sync, "host_link": link},
         "gpu_launches": launches,
         "roofline": roof,
         "unit_roofline": unit_roof,

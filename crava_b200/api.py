@@ -292,7 +292,7 @@ class Context:
         check(self.lib.crava_gpu_get_tuning(self.handle, C.byref(t)), "get_tuning")
         return t
 
-    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0, lanes=2, rows_x=-1, kappa_refine=None,
+    def set_tuning(self, cols_y_tile=-1, cols_z_tile=-1, fused=0, lanes=3, rows_x=-1, kappa_refine=None,
                    xy_fused=None, solve_shape=None):
         cur = self.tuning()
         if kappa_refine is None:

@@ -223,7 +223,7 @@ int crava_gpu_autotune(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_
   for (int q = 0; q < 6; ++q) tma = tma && cols_z_tma_supported(c->g, in->cov[q]) && cols_z_tma_supported(c->g, out->cov[q]);
   if (tma) cz.insert(cz.begin(), 2);
   const bool xy = plane_xy_supported(c->g);
-  for (int lanes = 1; lanes <= 2; ++lanes) {
+  for (int lanes = 1; lanes <= 3; ++lanes) {
     for (int a : cy)
       for (int z : cz) cand.push_back({a, z, 0, 0.0f, lanes, -1, c->consts.kappa_refine, 0, c->consts.solve_shape});
     // the fused x + y pass replaces the y pass: only the z choices matter

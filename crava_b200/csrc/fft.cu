@@ -526,6 +526,14 @@ struct RrRows {
   // register holding position t + T m in stage s's layout (radix R):
   // b = m mod (E / R), q = m div (E / R), register b R + q
   static __host__ __device__ constexpr int reg(int m, int R) { return (m % (E / R)) * R + m / (E / R); }
+  // A row's T threads are consecutive; with T <= 32 (a power of two) they
+  // lie in one warp, and a warp barrier orders the row's shared-memory
+  // exchanges (and its in-place global reads before writes); a row of
+  // 64 threads spans two warps and takes the block barrier.
+  static __device__ __forceinline__ void row_sync() {
+    if constexpr (T <= 32) __syncwarp();
+    else __syncthreads();
+  }
 };
 
 template <int N, int DIR, int S>
@@ -537,12 +545,12 @@ struct RrRowStages {
     if constexpr (DIR > 0) rr::stage_compute_st<N, S, DIR, E, T>(v, tw, t);
     else rr::stage_compute<N, S, DIR, E, T>(v, tw, t);
     if constexpr (S + 1 < CtRadix::count(N)) {
-      if (S > 0) __syncthreads();
+      if (S > 0) RrRows<N>::row_sync();
 #pragma unroll
       for (int b = 0; b < E / R; ++b)
 #pragma unroll
         for (int q = 0; q < R; ++q) row[RrRows<N>::phys(rr::stage_out<N, S, T>(t, b, q))] = v[b * R + q];
-      __syncthreads();
+      RrRows<N>::row_sync();
       constexpr int R2 = CtRadix::at(N, S + 1);
 #pragma unroll
       for (int b = 0; b < E / R2; ++b)
@@ -679,7 +687,8 @@ __global__ void __launch_bounds__(RrRows<N>::NTH) k_rows_rr(const __grid_constan
     }
     // every thread has read its whole row before any row is overwritten
     // (in place: the output row is the input row)
-    __syncthreads();
+    if constexpr (T <= 32) __syncwarp();
+    else __syncthreads();
     RrRowStages<N, DIR, 0>::run(v, row, tw, t);
     if (ok) {
       float2 *orow = reinterpret_cast<float2 *>(a.grid + row_idx * a.rnxp);
@@ -969,9 +978,12 @@ int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
 
 int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   const Geom &g = p.g;
-  // the TMA-fed pass (tile choice 2): faster alone, slower in the unit's
-  // two-lane overlap, so not the built-in choice
-  if (p.tile_z == 2 && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
+  // the TMA-fed pass (tile choice 2): faster alone; in the unit's lane
+  // overlap it pays beside the fused x + y pass (5.23 against 5.85 ms per
+  // 256x256x512x5 unit) and not beside the separate passes (5.92 against
+  // 5.40 ms), so it is built in where the fused pass is
+  const bool tma = p.tile_z == 2 || (p.tile_z == -1 && use_plane_xy(p));
+  if (tma && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
   return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z == 2 ? -1 : p.tile_z, s);
 }
 

@@ -26,14 +26,16 @@ struct FftPlans {
   // per CTA in the in-place pass (lengths with compiled kernels only; other
   // lengths use the generic pass), 2 (z only) the register-resident pass
   // with TMA tile loads where cols_z_tma_supported.  The default is the
-  // register-resident pass where it exists, else the in-place pass.
+  // TMA-fed pass where the fused x + y pass is in use and the grid allows
+  // it, else the register-resident pass where it exists, else the in-place
+  // pass.
   int tile_y = -1, tile_z = -1;
   // x pass of an even nxp: -1 default (register-resident where the half
   // length is 64..512), 0 the in-place pass, 1 register-resident
   int rows_x = -1;
   // x and y passes in one cluster kernel (plane.cu) where the geometry has
-  // one: -1 default (off: measured slower than the separate
-  // register-resident passes), 0 off, 1 on; its twiddle tables
+  // one: -1 default (on where the geometry has the kernel), 0 off, 1 on;
+  // its twiddle tables (null where the geometry has none)
   int plane_xy = -1;
   float2 *twq = nullptr, *twy = nullptr;
 };
@@ -46,7 +48,12 @@ int plane_xy_tables(const Geom &g, float2 **twq, float2 **twy);
 int plane_xy(const FftPlans &p, const float *src, float *dst, int dir, float scale, const float *addend,
              cudaStream_t s);
 // Whether the transforms of these plans use the fused x + y pass.
-inline bool use_plane_xy(const FftPlans &p) { return p.plane_xy == 1 && p.twq && p.twy; }
+// Built in where the geometry has the kernel: alone it is slower than the
+// separate register-resident x and y passes (131 / 112 us against 59 + 54 /
+// 56 + 52 us per 256x256x512 grid, forward / inverse), but it moves two
+// grids of HBM traffic instead of four, and in the unit, with the TMA-fed
+// z pass and three transform lanes, it gave 5.23 ms against 5.40 ms.
+inline bool use_plane_xy(const FftPlans &p) { return p.plane_xy != 0 && p.twq && p.twy; }
 
 // Whether length n has compiled column kernels (tile choices 0, 8, 16).
 bool cols_tunable(int n);

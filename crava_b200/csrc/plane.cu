@@ -38,7 +38,11 @@ namespace crava {
 
 namespace {
 
-constexpr int kPlaneThreads = 256;
+// 288 threads: the y stage covers the cnxp = NH + 1 columns in two rounds
+// (72 per round at 4 threads a column) instead of two full rounds and a
+// third holding the Nyquist column alone; three CTAs per SM
+constexpr int kPlaneThreads = 288;
+constexpr int kPlaneMinBlocks = 3;
 
 struct PlaneArgs {
   const float *src;   // forward: real input planes (may equal dst)
@@ -69,7 +73,17 @@ struct PlaneCfg {
   static constexpr size_t smem = tab + sizeof(float2) * (size_t)NQ * P;
 };
 
-template <int N, int DIR, int E, int T, int S, typename IDX>
+// Barrier of a line's exchanges: a warp barrier where the line's threads
+// lie in one warp (the x rows: TX consecutive threads, TX a power of two
+// <= 32), the block barrier otherwise (the y columns: 4 threads a column,
+// strided by the columns of a round).
+template <bool WARP>
+__device__ __forceinline__ void line_sync() {
+  if constexpr (WARP) __syncwarp();
+  else __syncthreads();
+}
+
+template <int N, int DIR, int E, int T, int S, bool WARP, typename IDX>
 struct SmemStages {
   // stages S.. of an N-point line held as v (registers) with exchanges in
   // shared memory at idx(e); the caller syncs before the first call
@@ -78,14 +92,14 @@ struct SmemStages {
     constexpr int R = CtRadix::at(N, S);
     if (act) rr::stage_compute<N, S, DIR, E, T>(v, tw, t);
     if constexpr (S + 1 < CtRadix::count(N)) {
-      __syncthreads();  // every thread has read this stage's inputs
+      line_sync<WARP>();  // every thread has read this stage's inputs
       if (act) {
 #pragma unroll
         for (int b = 0; b < E / R; ++b)
 #pragma unroll
           for (int q = 0; q < R; ++q) buf[idx(rr::stage_out<N, S, T>(t, b, q))] = v[b * R + q];
       }
-      __syncthreads();
+      line_sync<WARP>();
       constexpr int R2 = CtRadix::at(N, S + 1);
       if (act) {
 #pragma unroll
@@ -93,14 +107,21 @@ struct SmemStages {
 #pragma unroll
           for (int q = 0; q < R2; ++q) v[b * R2 + q] = buf[idx(rr::stage_in<N, S + 1, E, T>(t, b, q))];
       }
-      SmemStages<N, DIR, E, T, S + 1, IDX>::run(v, buf, tw, t, act, idx);
+      SmemStages<N, DIR, E, T, S + 1, WARP, IDX>::run(v, buf, tw, t, act, idx);
     }
   }
 };
 
+// Register of position t + T m after the last stage of radix RL: the
+// stage's inputs t + T (b + q E / RL) sit at register b RL + q.
+template <int E, int RL>
+__device__ __forceinline__ constexpr int last_reg(int m) {
+  return (m % (E / RL)) * RL + m / (E / RL);
+}
+
 // ------------------------------------------------------------------ forward
 template <int NH, int NY, int CS>
-__global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_constant__ PlaneArgs a) {
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_fwd(const __grid_constant__ PlaneArgs a) {
   using C = PlaneCfg<NH, NY, CS>;
   constexpr int NQ = C::NQ, CX = C::CX, P = C::P, EX = C::EX, TX = C::TX, EQ = C::EQ, TQ = C::TQ;
   constexpr int R0X = C::R0X, SX = CtRadix::count(NH), RLX = CtRadix::at(NH, SX - 1);
@@ -123,6 +144,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_con
   const long long pr = (long long)a.rnxp * a.nyp;  // floats per real plane
   const float *src = a.src + (long long)plane * pr;
   float2 *dst = reinterpret_cast<float2 *>(a.dst + (long long)plane * pr);
+
   __syncthreads();
 
   // 1. x: the NQ rows of this CTA, TX threads per row, rounds of
@@ -142,32 +164,37 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_con
         for (int qq = 0; qq < R0X; ++qq) v[b * R0X + qq] = in[rr::stage_in<NH, 0, EX, TX>(t, b, qq)];
     }
     auto ix = [](int e) { return C::physx(e); };
-    SmemStages<NH, -1, EX, TX, 0, decltype(ix)>::run(v, row, twx, t, act, ix);
-    __syncthreads();
-    if (act) {
-#pragma unroll
-      for (int b = 0; b < EX / RLX; ++b)
-#pragma unroll
-        for (int qq = 0; qq < RLX; ++qq) row[C::physx(rr::stage_in<NH, SX - 1, EX, TX>(t, b, qq))] = v[b * RLX + qq];
-    }
-    __syncthreads();
-    // split X_k = E_k + W^k O_k into registers, then the plain layout
+    SmemStages<NH, -1, EX, TX, 0, true, decltype(ix)>::run(v, row, twx, t, act, ix);
+    // split X_k = E_k + W^k O_k in registers: position k = t + TX m pairs
+    // with NH - k, which thread TX - t of the row holds at m' = EX - 1 - m
+    // (thread 0: its own position EX - m), one warp shuffle per output
+    static_assert(TX <= 32 && (32 % TX) == 0, "a row's threads lie in one warp");
+    const int lane = threadIdx.x & 31;
+    const int srcl = lane - t + (TX - t) % TX;
     float2 X[EX + 1];
-    if (act) {
 #pragma unroll
-      for (int m = 0; m <= EX; ++m) {
-        const int k = m < EX ? t + TX * m : NH;
-        if (m == EX && t != 0) break;
-        const float2 zk = row[C::physx(k == NH ? 0 : k)];
-        float2 zm = row[C::physx(k == 0 ? 0 : NH - k)];
-        zm.y = -zm.y;
-        const float2 e = cscale(cadd(zk, zm), 0.5f);
-        const float2 d = csub(zk, zm);
-        const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
-        X[m] = cscale(cadd(e, cmul(post[k], o)), a.scale);
-      }
+    for (int m = 0; m < EX; ++m) {
+      const float2 send = v[last_reg<EX, RLX>(EX - 1 - m)];
+      float2 zm = make_float2(__shfl_sync(0xffffffffu, send.x, srcl), __shfl_sync(0xffffffffu, send.y, srcl));
+      if (t == 0) zm = v[last_reg<EX, RLX>(m == 0 ? 0 : EX - m)];
+      const float2 zk = v[last_reg<EX, RLX>(m)];
+      zm.y = -zm.y;
+      const float2 e = cscale(cadd(zk, zm), 0.5f);
+      const float2 d = csub(zk, zm);
+      const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+      X[m] = cscale(cadd(e, cmul(post[t + TX * m], o)), a.scale);
     }
-    __syncthreads();
+    {
+      // X_NH from Z_0 alone (thread 0)
+      const float2 zk = v[last_reg<EX, RLX>(0)];
+      float2 zm = zk;
+      zm.y = -zm.y;
+      const float2 e = cscale(cadd(zk, zm), 0.5f);
+      const float2 d = csub(zk, zm);
+      const float2 o = make_float2(0.5f * d.y, -0.5f * d.x);
+      X[EX] = cscale(cadd(e, cmul(post[NH], o)), a.scale);
+    }
+    __syncwarp();  // the row's exchange reads are done before the plain layout overwrites them
     if (act) {
 #pragma unroll
       for (int m = 0; m < EX; ++m) row[t + TX * m] = X[m];
@@ -191,8 +218,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_con
         for (int qq = 0; qq < R0Q; ++qq) v[b * R0Q + qq] = A[rr::stage_in<NQ, 0, EQ, TQ>(t, b, qq) * P + kx];
     }
     auto iy = [kx](int e) { return e * P + (kx < CX ? kx : 0); };
-    SmemStages<NQ, -1, EQ, TQ, 0, decltype(iy)>::run(v, A, twq, t, act, iy);
-    __syncthreads();
+    SmemStages<NQ, -1, EQ, TQ, 0, false, decltype(iy)>::run(v, A, twq, t, act, iy);
+    // the last stage's outputs go to the very slots its inputs came from
+    // (the stride-TQ set of this thread), and a round owns its columns:
+    // no barrier before the write-back or between rounds
     if (act) {
 #pragma unroll
       for (int b = 0; b < EQ / RLQ; ++b)
@@ -202,7 +231,6 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_con
           A[k1 * P + kx] = cmul(v[b * RLQ + qq], twr[k1]);
         }
     }
-    __syncthreads();
   }
 
   // 3. the radix-CS stage across the cluster: this CTA's k1 range, every
@@ -211,21 +239,35 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_fwd(const __grid_con
   const float2 *Ar[CS];
 #pragma unroll
   for (int s = 0; s < CS; ++s) Ar[s] = cl.map_shared_rank(A, s);
-  for (int i = tid; i < C::QK * CX; i += kPlaneThreads) {
-    const int k1 = r * C::QK + i / CX, kx = i % CX;
-    float2 v[CS];
+  // two items per thread and step: the 2 CS loads from the partners'
+  // shared memory are issued before either item's butterfly
+  constexpr int NI = C::QK * CX;
+  for (int i0 = tid; i0 < NI; i0 += 2 * kPlaneThreads) {
+    const int i1 = i0 + kPlaneThreads;
+    const bool two = i1 < NI;
+    const int k1a = r * C::QK + i0 / CX, kxa = i0 % CX;
+    const int k1b = r * C::QK + (two ? i1 : i0) / CX, kxb = (two ? i1 : i0) % CX;
+    float2 va[CS], vb[CS];
 #pragma unroll
-    for (int s = 0; s < CS; ++s) v[s] = Ar[s][k1 * P + kx];
-    Dft<CS, -1>::run(v);
+    for (int s = 0; s < CS; ++s) {
+      va[s] = Ar[s][k1a * P + kxa];
+      vb[s] = Ar[s][k1b * P + kxb];
+    }
+    Dft<CS, -1>::run(va);
 #pragma unroll
-    for (int k2 = 0; k2 < CS; ++k2) dst[(long long)(k1 + NQ * k2) * CX + kx] = v[k2];
+    for (int k2 = 0; k2 < CS; ++k2) dst[(long long)(k1a + NQ * k2) * CX + kxa] = va[k2];
+    if (two) {
+      Dft<CS, -1>::run(vb);
+#pragma unroll
+      for (int k2 = 0; k2 < CS; ++k2) dst[(long long)(k1b + NQ * k2) * CX + kxb] = vb[k2];
+    }
   }
   cl.sync();  // partners are done reading this CTA's shared memory
 }
 
 // ------------------------------------------------------------------ inverse
 template <int NH, int NY, int CS>
-__global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_inv(const __grid_constant__ PlaneArgs a) {
+__global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_inv(const __grid_constant__ PlaneArgs a) {
   using C = PlaneCfg<NH, NY, CS>;
   constexpr int NQ = C::NQ, CX = C::CX, P = C::P, EX = C::EX, TX = C::TX, EQ = C::EQ, TQ = C::TQ;
   constexpr int R0X = C::R0X, SX = CtRadix::count(NH), RLX = CtRadix::at(NH, SX - 1);
@@ -257,14 +299,28 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_inv(const __grid_con
   float2 *At[CS];
 #pragma unroll
   for (int s = 0; s < CS; ++s) At[s] = cl.map_shared_rank(A, s);
-  for (int i = tid; i < C::QK * CX; i += kPlaneThreads) {
-    const int k1 = r * C::QK + i / CX, kx = i % CX;
-    float2 v[CS];
+  // two items per thread and step: their 2 CS loads from HBM are in
+  // flight together
+  constexpr int NI = C::QK * CX;
+  for (int i0 = tid; i0 < NI; i0 += 2 * kPlaneThreads) {
+    const int i1 = i0 + kPlaneThreads;
+    const bool two = i1 < NI;
+    const int k1a = r * C::QK + i0 / CX, kxa = i0 % CX;
+    const int k1b = r * C::QK + (two ? i1 : i0) / CX, kxb = (two ? i1 : i0) % CX;
+    float2 va[CS], vb[CS];
 #pragma unroll
-    for (int k2 = 0; k2 < CS; ++k2) v[k2] = src[(long long)(k1 + NQ * k2) * CX + kx];
-    Dft<CS, 1>::run(v);
+    for (int k2 = 0; k2 < CS; ++k2) {
+      va[k2] = src[(long long)(k1a + NQ * k2) * CX + kxa];
+      vb[k2] = src[(long long)(k1b + NQ * k2) * CX + kxb];
+    }
+    Dft<CS, 1>::run(va);
 #pragma unroll
-    for (int s = 0; s < CS; ++s) At[s][k1 * P + kx] = v[s];
+    for (int s = 0; s < CS; ++s) At[s][k1a * P + kxa] = va[s];
+    if (two) {
+      Dft<CS, 1>::run(vb);
+#pragma unroll
+      for (int s = 0; s < CS; ++s) At[s][k1b * P + kxb] = vb[s];
+    }
   }
   cl.sync();
 
@@ -286,16 +342,17 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_inv(const __grid_con
         }
     }
     auto iy = [kx](int e) { return e * P + (kx < CX ? kx : 0); };
-    SmemStages<NQ, 1, EQ, TQ, 0, decltype(iy)>::run(v, A, twq, t, act, iy);
-    __syncthreads();
+    SmemStages<NQ, 1, EQ, TQ, 0, false, decltype(iy)>::run(v, A, twq, t, act, iy);
+    // outputs to the slots of the last stage's inputs; rounds own their
+    // columns (see the forward)
     if (act) {
 #pragma unroll
       for (int b = 0; b < EQ / RLQ; ++b)
 #pragma unroll
         for (int qq = 0; qq < RLQ; ++qq) A[rr::stage_in<NQ, SQ - 1, EQ, TQ>(t, b, qq) * P + kx] = v[b * RLQ + qq];
     }
-    __syncthreads();
   }
+  __syncthreads();  // every column is done before the rows are read
 
   // 3. x C2R of every row to HBM (scale, addend, zero pad)
   constexpr int RPR = kPlaneThreads / TX;
@@ -323,9 +380,9 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_inv(const __grid_con
           v[b * R0X + qq] = make_float2(e.x - o.y, e.y + o.x);
         }
     }
-    __syncthreads();  // the row's spectrum is read before the exchanges overwrite it
+    __syncwarp();  // the row's spectrum is read before the exchanges overwrite it (a row lies in one warp)
     auto ix = [](int e) { return C::physx(e); };
-    SmemStages<NH, 1, EX, TX, 0, decltype(ix)>::run(v, row, twx, t, act, ix);
+    SmemStages<NH, 1, EX, TX, 0, true, decltype(ix)>::run(v, row, twx, t, act, ix);
     if (act) {
       const long long ro = (long long)(CS * q + r) * a.rnxp;
       float2 *orow = reinterpret_cast<float2 *>(dst + ro);
@@ -341,7 +398,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_plane_xy_inv(const __grid_con
         }
       if (t == 0) orow[NH] = make_float2(0.f, 0.f);
     }
-    __syncthreads();  // the row buffer is free for the next round
+    // the next round works on other rows: no barrier
   }
 }
 

@@ -279,7 +279,8 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
  * register-resident pass of lengths 64/128/256/512, 8 or 16 columns per CTA
  * in the in-place pass, 2 (z only) the register-resident pass fed by TMA
  * tile loads, where the grid has an even number of lines per z plane;
- * lengths without compiled column kernels ignore it);
+ * lengths without compiled column kernels ignore it; the built-in z choice
+ * is 2 where the fused x + y pass is in use and the grid allows it);
  * fused: the fused unit kernels (1) or the three passes (0); ms: one unit's
  * measured time (autotune output only); lanes: more than 1 lets the
  * transforms of different grids overlap on that many streams; rows_x: the x
@@ -287,16 +288,18 @@ int crava_gpu_posterior_noalloc(const crava_gpu_params *params,
  * pass where nxp / 2 is 64..512).  All these choices give the same values
  * bit for bit.  xy_fused: the x and y passes as one thread-block-cluster
  * kernel where the geometry has one (256x256 and 128x128 planes; -1
- * built-in = off, 0 off, 1 on; it measured slower than the separate
- * register-resident passes on B200); it factorises the y transform
+ * built-in = on where the geometry has it, 0 off, 1 on; alone it is
+ * slower than the separate register-resident passes on B200, in the unit
+ * beside the TMA-fed z pass faster); it factorises the y transform
  * differently, so it agrees with the separate passes to float rounding,
  * not bit for bit.  kappa_refine (mixed form only, >= 0): an inverted bin whose
  * FP32 factor has (max L_ii / min L_ii)^2 above it takes one FP64
  * refinement step (0 refines every bin).  solve_shape: the launch shape of
- * the FP64 and mixed solves (-1 built-in: the pipelined kernel with 8 bins
- * per thread for FP64, the register-factor kernel with four 128-thread
- * blocks per SM for mixed; 0-5 one shape for both); every shape gives the
- * same values bit for bit.  No counterpart in the reference (FFTW plans
+ * the FP64 and mixed solves (-1 built-in: the Woodbury kernel (shape 6)
+ * for FP64 on a context, the register-factor kernel with four 128-thread
+ * blocks per SM (shape 3) for mixed; 0-5 square-root shapes for both, 6-8
+ * Woodbury shapes for FP64); every square-root shape gives the same values
+ * bit for bit, the Woodbury shapes agree with them to FP64 rounding.  No counterpart in the reference (FFTW plans
  * are fixed there). */
 typedef struct crava_gpu_tuning {
   int cols_y_tile;
