@@ -445,6 +445,8 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->synt_H);
   cudaFree(c->prior_buf);
   cudaFree(c->div_buf);
+  cudaFree(c->ll_buf);
+  if (c->ll_host) cudaFreeHost(c->ll_host);
   cudaFree(c->file_dev);
   if (c->file_host) cudaFreeHost(c->file_host);
   for (auto &e : c->ev) if (e) cudaEventDestroy(e);

@@ -67,6 +67,12 @@ struct crava_gpu_ctx {
   // padding), kept between calls and grown when a call needs more
   char *div_buf = nullptr;
   size_t div_bytes = 0;
+  // log marginal likelihood: device operator table, per-block partial sums
+  // and failure count, and their pinned host copy, kept between calls
+  char *ll_buf = nullptr;
+  size_t ll_bytes = 0;
+  char *ll_host = nullptr;
+  size_t ll_host_bytes = 0;
 };
 
 namespace crava {

@@ -341,28 +341,49 @@ extern "C" int crava_gpu_loglik_grad(crava_gpu_ctx *c, const crava_gpu_grids *gr
   a.bpp = (int)bpp;
   const int NV = 1 + 4 * nt;
   const size_t part_n = (size_t)nzp * a.bpp * NV;
-  double2 *dw = nullptr;
-  double *dpart = nullptr;
-  unsigned long long *dfail = nullptr;
-  auto cleanup = [&]() { cudaFree(dw); cudaFree(dpart); cudaFree(dfail); };
-  if (cudaMalloc(&dw, w.size() * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&dpart, part_n * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&dfail, sizeof(unsigned long long)) != cudaSuccess) {
-    cleanup();
-    return CRAVA_GPU_ERR_ALLOC;
+  // the operator table, the partial sums and the failure count live in one
+  // device buffer kept on the context (grown when a call needs more), the
+  // partial sums come back into a pinned host buffer: no allocation, and no
+  // device-wide synchronisation, after the first call
+  const size_t w_bytes = (w.size() * sizeof(double) + 255) / 256 * 256;
+  const size_t p_bytes = (part_n * sizeof(double) + 255) / 256 * 256;
+  const size_t need = w_bytes + p_bytes + 256;
+  const size_t host_need = p_bytes + 256;
+  if (c->ll_bytes < need) {
+    cudaFree(c->ll_buf);
+    c->ll_buf = nullptr;
+    c->ll_bytes = 0;
+    if (cudaMalloc(&c->ll_buf, need) != cudaSuccess) return CRAVA_GPU_ERR_ALLOC;
+    c->ll_bytes = need;
   }
-  std::vector<double> part(part_n);
-  unsigned long long hfail = 0;
+  if (c->ll_host_bytes < host_need) {
+    if (c->ll_host) cudaFreeHost(c->ll_host);
+    c->ll_host = nullptr;
+    c->ll_host_bytes = 0;
+    if (cudaMallocHost(&c->ll_host, host_need) != cudaSuccess) return CRAVA_GPU_ERR_ALLOC;
+    c->ll_host_bytes = host_need;
+  }
+  double2 *dw = reinterpret_cast<double2 *>(c->ll_buf);
+  double *dpart = reinterpret_cast<double *>(c->ll_buf + w_bytes);
+  unsigned long long *dfail = reinterpret_cast<unsigned long long *>(c->ll_buf + w_bytes + p_bytes);
+  const double *part = reinterpret_cast<const double *>(c->ll_host);
+  const unsigned long long *hfail_p = reinterpret_cast<const unsigned long long *>(c->ll_host + p_bytes);
   cudaError_t e = cudaMemcpyAsync(dw, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dfail, 0, sizeof(unsigned long long), c->stream);
-  if (e != cudaSuccess) { set_last_error(e, "loglik upload", __FILE__, __LINE__); cleanup(); return CRAVA_GPU_ERR_CUDA; }
+  if (e != cudaSuccess) { set_last_error(e, "loglik upload", __FILE__, __LINE__); return CRAVA_GPU_ERR_CUDA; }
   a.w = dw; a.part = dpart; a.fail = dfail;
-  if ((rc = launch_loglik(a, nt, nzp, c->stream))) { cleanup(); return rc; }
-  e = cudaMemcpyAsync(part.data(), dpart, part_n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&hfail, dfail, sizeof hfail, cudaMemcpyDeviceToHost, c->stream);
+  // stage events around the kernel: crava_gpu_get_stats then reports its
+  // device time as ms_solve and ms_total
+  if ((rc = stage_event(c, 0)) || (rc = stage_event(c, 1))) return rc;
+  if ((rc = launch_loglik(a, nt, nzp, c->stream))) return rc;
+  if ((rc = stage_event(c, 2)) || (rc = stage_event(c, 3))) return rc;
+  c->timed = true;
+  e = cudaMemcpyAsync(c->ll_host, dpart, part_n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->ll_host + p_bytes, dfail, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cleanup();
   if (e != cudaSuccess) { set_last_error(e, "loglik download", __FILE__, __LINE__); return CRAVA_GPU_ERR_CUDA; }
+  const unsigned long long hfail = *hfail_p;
   // fixed-order reduction on the host
   double Lsum = 0.0;
   std::vector<double> gs(nt, 0.0), gv(nt, 0.0), gw((size_t)nzp * nt * 2, 0.0);

@@ -145,23 +145,37 @@ __global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_fwd
   const float *src = a.src + (long long)plane * pr;
   float2 *dst = reinterpret_cast<float2 *>(a.dst + (long long)plane * pr);
 
-  __syncthreads();
-
   // 1. x: the NQ rows of this CTA, TX threads per row, rounds of
-  //    kPlaneThreads / TX rows
+  //    kPlaneThreads / TX rows.  Every round's input rows travel into A by
+  //    cp.async before the first round computes (one commit group per
+  //    round; 8-byte copies, as a row of odd index starts 8 bytes off a
+  //    16-byte boundary), so the HBM reads of a later round run under the
+  //    arithmetic of the earlier one.
   constexpr int RPR = kPlaneThreads / TX;  // rows per round
   constexpr int NRX = (NQ + RPR - 1) / RPR;
+  static_assert(NRX <= 2, "the commit-group waits below cover two rounds");
+#pragma unroll
+  for (int rd = 0; rd < NRX; ++rd) {
+    const int q0 = rd * RPR, nr = NQ - q0 < RPR ? NQ - q0 : RPR;
+    for (int i = tid; i < nr * NH; i += kPlaneThreads) {
+      const int q = q0 + i / NH, e = i % NH;
+      cp_async8(A + q * P + e, reinterpret_cast<const float2 *>(src + (long long)(CS * q + r) * a.rnxp) + e);
+    }
+    cp_async_commit();
+  }
   for (int rd = 0; rd < NRX; ++rd) {
     const int q = rd * RPR + tid / TX, t = tid % TX;
     const bool act = q < NQ;
     float2 *row = A + (act ? q : 0) * P;
+    if (rd + 1 < NRX) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    __syncthreads();  // this round's rows (every thread's copies) and the tables
     float2 v[EX];
     if (act) {
-      const float2 *in = reinterpret_cast<const float2 *>(src + (long long)(CS * q + r) * a.rnxp);
 #pragma unroll
       for (int b = 0; b < EX / R0X; ++b)
 #pragma unroll
-        for (int qq = 0; qq < R0X; ++qq) v[b * R0X + qq] = in[rr::stage_in<NH, 0, EX, TX>(t, b, qq)];
+        for (int qq = 0; qq < R0X; ++qq) v[b * R0X + qq] = row[rr::stage_in<NH, 0, EX, TX>(t, b, qq)];
     }
     auto ix = [](int e) { return C::physx(e); };
     SmemStages<NH, -1, EX, TX, 0, true, decltype(ix)>::run(v, row, twx, t, act, ix);

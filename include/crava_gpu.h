@@ -386,7 +386,10 @@ int crava_gpu_batch_destroy(crava_gpu_batch *b);
  * context's wavelets).  Outputs may be NULL except loglik; failed_bins:
  * inverted bins whose M did not factor (left out).  The noise colouring
  * tables (e1, e2, e3) stay fixed.  FP64; synchronous.  Recomputes M and
- * its factor per bin (nothing of a forward pass is stored).  No
+ * its factor per bin (nothing of a forward pass is stored).  Its device
+ * buffers (a few hundred KB) are kept on the context after the first
+ * call; crava_gpu_get_stats then reports the kernel's device time as
+ * ms_solve and ms_total (ms_forward and ms_inverse 0).  No
  * counterpart in the reference (its wavelet and noise estimates are not
  * gradient-based). */
 int crava_gpu_loglik_grad(crava_gpu_ctx *ctx, const crava_gpu_grids *grids,
