@@ -77,11 +77,16 @@ int run_vintage(const crava_gpu_batch::Vintage &v, const unsigned long long *epo
     if ((rc = pass_forward(c, in.mu[q], out.mu[q], CRAVA_GRID_PARAMETER))) return rc;
   for (int l = 0; l < nt; ++l)
     if ((rc = pass_forward(c, in.data[l], out.data[l], CRAVA_GRID_DATA))) return rc;
+  // the band-gated covariance rule in the forward z passes (as run_unit)
+  ZPrior zp[6];
+  bool gated = false;
+  if ((rc = gated_prior_setup(c, v.precision, zp, &gated))) return rc;
   for (int t = 0; t < 6; ++t)
-    if ((rc = pass_forward(c, in.cov[t], out.cov[t], CRAVA_GRID_COVARIANCE))) return rc;
+    if ((rc = pass_forward(c, in.cov[t], out.cov[t], CRAVA_GRID_COVARIANCE, gated ? &zp[t] : nullptr))) return rc;
   if ((rc = pass_forward(c, in.err_corr, out.err_corr, CRAVA_GRID_COVARIANCE))) return rc;
+  if (gated && (rc = gated_prior_count(c))) return rc;
   if ((rc = stage_event(c, 1))) return rc;
-  if ((rc = pass_solve(c, &out, v.precision))) return rc;
+  if ((rc = pass_solve(c, &out, v.precision, gated))) return rc;
   if ((rc = stage_event(c, 2))) return rc;
   for (int q = 0; q < 3; ++q)
     if ((rc = pass_inverse(c, out.mu[q], CRAVA_GRID_PARAMETER))) return rc;

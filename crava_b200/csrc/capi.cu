@@ -154,17 +154,46 @@ void prof_collect(crava_gpu_ctx *c) {
   c->recs.clear();
 }
 
-int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type) {
+int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type, const ZPrior *zp) {
   int rc;
   if (use_plane_xy(c->plans)) {
     { Scope sc(c, K_XY_FWD); if ((rc = plane_xy(c->plans, src, dst, -1, forward_scale(c->g, type), nullptr, c->stream))) return rc; }
-    { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
+    { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream, zp))) return rc; }
     return CRAVA_GPU_OK;
   }
   { Scope sc(c, K_ROWS_FWD); if ((rc = fft_rows(c->plans, dst, -1, forward_scale(c->g, type), c->stream, nullptr, src))) return rc; }
   { Scope sc(c, K_COLS_Y_FWD); if ((rc = fft_cols_y(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
-  { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream))) return rc; }
+  { Scope sc(c, K_COLS_Z_FWD); if ((rc = fft_cols_z(c->plans, reinterpret_cast<float2 *>(dst), -1, c->stream, zp))) return rc; }
   return CRAVA_GPU_OK;
+}
+
+int gated_prior_setup(crava_gpu_ctx *c, int precision, ZPrior zp[6], bool *on) {
+  *on = (precision == CRAVA_SOLVE_FP64 || precision == CRAVA_SOLVE_MIXED) && z_prior_supported(c->plans) &&
+        c->tables.n_inv >= 0 && c->tables.order_inv;
+  if (!*on) return CRAVA_GPU_OK;
+  if (!c->gated_nf) {
+    const long long words = (c->g.csize + 31) / 32;
+    if (cudaMalloc(&c->gated_nf, (size_t)(words + 1) * sizeof(unsigned)) != cudaSuccess) {
+      c->gated_nf = nullptr;
+      return CRAVA_GPU_ERR_ALLOC;
+    }
+    CRAVA_CUDA_TRY(cudaMemsetAsync(c->gated_nf, 0, (size_t)(words + 1) * sizeof(unsigned), c->stream));
+    c->gated_nf_words = words;
+  }
+  for (int t = 0; t < 6; ++t) {
+    zp[t] = ZPrior{};
+    zp[t].inv = c->tables.inv;
+    zp[t].v = c->consts.var0[t];  // (0,0) (1,1) (2,2) (0,1) (0,2) (1,2): the cov grid order
+    zp[t].mode = precision == CRAVA_SOLVE_FP64 ? 1 : 2;
+    zp[t].nf_bits = c->gated_nf;
+    zp[t].nf_any = c->gated_nf + c->gated_nf_words;
+  }
+  return CRAVA_GPU_OK;
+}
+
+int gated_prior_count(crava_gpu_ctx *c) {
+  return gated_nonfinite_count(c->gated_nf, c->gated_nf_words, c->gated_nf + c->gated_nf_words, c->counters,
+                               c->stream);
 }
 
 int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend) {
@@ -179,19 +208,21 @@ int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend) {
   return CRAVA_GPU_OK;
 }
 
-int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision) {
+int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision, bool gated_done) {
   // bytes the in-place solve moves: (10+nt) spectra read and (9+nt)
   // written for an inverted bin, the six covariance spectra both ways for
-  // a band-gated one (the FP32 reference-order kernel moves all of them)
+  // a band-gated one unless the forward z passes did those (the FP32
+  // reference-order kernel moves all of them)
   const double plane_bytes = (double)c->g.cnxp * c->g.nyp * 8.0;
   const int nt = c->p.ntheta, nzp = c->p.nzp;
+  const double gated = gated_done ? 0.0 : 12.0 * (nzp - c->n_inverted);
   const double bytes = precision == CRAVA_SOLVE_FP32
                            ? (double)(19 + 2 * nt) * nzp * plane_bytes
-                           : ((double)(19 + 2 * nt) * c->n_inverted + 12.0 * (nzp - c->n_inverted)) * plane_bytes;
+                           : ((double)(19 + 2 * nt) * c->n_inverted + gated) * plane_bytes;
   Scope sc(c, K_SOLVE, bytes);
   SolveGrids sg = to_solve_grids(gr, c->p.ntheta);
   return posterior_solve(c->consts, c->tables, sg, c->g.csize, (long long)c->g.cnxp * c->g.nyp,
-                         precision, c->counters, c->stream);
+                         precision, c->counters, c->stream, gated_done);
 }
 
 int valid_precision(int prec) {
@@ -337,9 +368,21 @@ int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids 
   int type[kMaxUnitGrids];
   const int G = unit_order(c, in, src, type);
   unit_order(c, out, dst, type);
-  if ((rc = on_lanes(c, G, [&](int i) { return pass_forward(c, src[i], dst[i], type[i]); }))) return rc;
+  // the band-gated bins of the six covariance grids: done by their forward
+  // z passes where the plans allow it, and the solve visits the inverted
+  // planes only
+  ZPrior zp[6];
+  bool gated = false;
+  if ((rc = gated_prior_setup(c, precision, zp, &gated))) return rc;
+  const int c0 = 3 + c->p.ntheta;  // first covariance grid in unit order
+  if ((rc = on_lanes(c, G, [&](int i) {
+         const ZPrior *z = gated && i >= c0 && i < c0 + 6 ? &zp[i - c0] : nullptr;
+         return pass_forward(c, src[i], dst[i], type[i], z);
+       })))
+    return rc;
+  if (gated && (rc = gated_prior_count(c))) return rc;
   if ((rc = stage_event(c, 1))) return rc;
-  if ((rc = pass_solve(c, out, precision))) return rc;
+  if ((rc = pass_solve(c, out, precision, gated))) return rc;
   if ((rc = stage_event(c, 2))) return rc;
   // the noise correlation (last in unit order) is not an output
   if ((rc = on_lanes(c, G - 1, [&](int i) { return pass_inverse(c, dst[i], type[i]); }))) return rc;
@@ -446,6 +489,7 @@ int crava_gpu_destroy(crava_gpu_ctx *c) {
   cudaFree(c->prior_buf);
   cudaFree(c->div_buf);
   cudaFree(c->ll_buf);
+  cudaFree(c->gated_nf);
   if (c->ll_host) cudaFreeHost(c->ll_host);
   cudaFree(c->file_dev);
   if (c->file_host) cudaFreeHost(c->file_host);
@@ -657,6 +701,9 @@ static int enqueue_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hin, const
   CRAVA_CUDA_TRY(cudaStreamWaitEvent(c->s_in, c->slot_done[slot], 0));
   const bool fused = use_fused(c, precision);
   if (fused && (rc = ensure_workspace(c))) return rc;
+  ZPrior zp[6];
+  bool gated = false;  // the band-gated covariance rule in the forward z passes
+  if (!fused && (rc = gated_prior_setup(c, precision, zp, &gated))) return rc;
   const double gb = (double)c->g.csize * 8.0, wb = (double)c->uplan.wgrid * 8.0;
   for (int k = 0; k < ngrid; ++k) {
     CRAVA_CUDA_TRY(cudaMemcpyAsync(dev[k], hsrc[k], gbytes, cudaMemcpyHostToDevice, c->s_in));
@@ -668,17 +715,19 @@ static int enqueue_unit_host(crava_gpu_ctx *c, const crava_gpu_grids *hin, const
       const float fsc = forward_scale(c->g, type[k]);
       const float *src = dev[k];
       if ((rc = unit_plane_forward(c->uplan, c->plans, &src, &wk, &fsc, 1, s))) return rc;
-    } else if ((rc = pass_forward(c, dev[k], dev[k], type[k]))) {
+    } else if ((rc = pass_forward(c, dev[k], dev[k], type[k],
+                                  gated && k >= 3 + nt && k < 9 + nt ? &zp[k - 3 - nt] : nullptr))) {
       return rc;
     }
   }
+  if (gated && (rc = gated_prior_count(c))) return rc;
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   if (fused) {
     float2 *w[kMaxUnitGrids];
     for (int k = 0; k < ngrid; ++k) w[k] = c->W + (size_t)k * c->uplan.wgrid;
     Scope sc(c, K_ZSOLVE, (2 * ngrid - 1) * wb);
     if ((rc = unit_zsolve(c->uplan, c->plans, c->consts, c->tables, w, precision, c->counters, s))) return rc;
-  } else if ((rc = pass_solve(c, &dg, precision))) {
+  } else if ((rc = pass_solve(c, &dg, precision, gated))) {
     return rc;
   }
   CRAVA_CUDA_TRY(cudaEventRecord(c->ev[2], s));

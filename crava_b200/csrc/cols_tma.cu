@@ -126,6 +126,7 @@ struct ZTmaArgs {
   int ntiles;
   int tpc;  // tiles per CTA (0: persistent grid of the resident CTAs)
   const float2 *tw;
+  ZPrior zp;  // forward pass of a covariance grid: the band-gated rule (inv null: none)
 };
 
 template <int N, int DIR, int S>
@@ -133,12 +134,27 @@ struct ZTmaStages {
   using Z = ZT<N>;
   // v holds the inputs of stage S
   static __device__ __forceinline__ void run(float2 (&v)[Z::CPT][Z::E], float2 *B, const float2 *tw, int t, int p,
-                                             float2 *g, long long L, bool ok) {
+                                             float2 *g, long long L, bool ok, const ZPrior &zp, long long f) {
     constexpr int E = Z::E, T = Z::T, CPT = Z::CPT, R = CtRadix::at(N, S);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) rr::stage_compute_st<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: the outputs sit at the positions loaded, straight to HBM
+      if (DIR < 0 && zp.inv && ok) {
+        // band-gated kz planes of a covariance grid: the prior rule (the
+        // CPT lines of a thread are f, f + 1: L is even)
+#pragma unroll
+        for (int b = 0; b < E / R; ++b)
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            const int e = rr::stage_in<N, S, E, T>(t, b, q);
+            if (__ldg(zp.inv + e) == 0) {
+#pragma unroll
+              for (int c = 0; c < CPT; ++c)
+                v[c][b * R + q] = zprior_apply(zp, v[c][b * R + q], f + c + (long long)e * L);
+            }
+          }
+      }
       if (ok) {
 #pragma unroll
         for (int b = 0; b < E / R; ++b)
@@ -180,7 +196,7 @@ struct ZTmaStages {
             v[0][b * R2 + q] = B[e * kTileLines + p];
           }
         }
-      ZTmaStages<N, DIR, S + 1>::run(v, B, tw, t, p, g, L, ok);
+      ZTmaStages<N, DIR, S + 1>::run(v, B, tw, t, p, g, L, ok, zp, f);
     }
   }
 };
@@ -243,7 +259,7 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
       }
     __syncthreads();  // the landed tile is read before the first exchange overwrites it
     const long long f = (long long)tile * kTileLines + p * CPT;
-    ZTmaStages<N, DIR, 0>::run(v, B, tw, t, p, a.data + f, a.L, f < a.L);
+    ZTmaStages<N, DIR, 0>::run(v, B, tw, t, p, a.data + f, a.L, f < a.L, a.zp, f);
     fence_proxy_async_smem();
     __syncthreads();  // every thread is done with this buffer
     if (tid == 0 && tile + 2 * G < end) issue_tile<N>(&tm, bufs + sb * Z::BYTES, mbs + 8u * sb, tile + 2 * G);
@@ -315,7 +331,7 @@ bool cols_z_tma_supported(const Geom &g, const void *data) {
          (L + kTileLines - 1) / kTileLines < (1LL << 31) && encode_tiled() != nullptr;
 }
 
-int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
+int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s, const ZPrior *zp) {
   const Geom &g = p.g;
   if (!cols_z_tma_supported(g, grid)) return CRAVA_GPU_ERR_ARG;
   const long long L = (long long)g.cnxp * g.nyp;
@@ -335,6 +351,7 @@ int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   a.ntiles = (int)((L + kTileLines - 1) / kTileLines);
   a.tpc = tiles_per_cta();
   a.tw = p.z.tw;
+  if (zp && dir < 0) a.zp = *zp;
   switch (n) {
     case 64: return dir < 0 ? launch_z_tma<64, -1>(tm, a, s) : launch_z_tma<64, 1>(tm, a, s);
     case 128: return dir < 0 ? launch_z_tma<128, -1>(tm, a, s) : launch_z_tma<128, 1>(tm, a, s);

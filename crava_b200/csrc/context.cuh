@@ -73,6 +73,11 @@ struct crava_gpu_ctx {
   size_t ll_bytes = 0;
   char *ll_host = nullptr;
   size_t ll_host_bytes = 0;
+  // bins whose band-gated prior (written by the forward z pass) is not
+  // finite: one bit per bin, then the any-flag word (zeroed once; the
+  // counting kernel clears what it counts)
+  unsigned *gated_nf = nullptr;
+  long long gated_nf_words = 0;
 };
 
 namespace crava {
@@ -89,11 +94,21 @@ struct DeviceGuard {
 int check_grids(const crava_gpu_ctx *c, const crava_gpu_grids *gr);
 int valid_precision(int prec);
 bool use_fused(const crava_gpu_ctx *c, int precision);
-// Forward transform of one grid, src -> dst (src == dst: in place).
-int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type);
+// Forward transform of one grid, src -> dst (src == dst: in place); zp
+// (optional): the band-gated covariance rule in the z pass's store.
+int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type, const ZPrior *zp = nullptr);
 // Inverse transform in place; addend (optional) is added to the real output.
 int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend = nullptr);
-int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision);
+// gated_done: the forward z passes applied the band-gated rule (the
+// zp of gated_prior_setup) to the six covariance grids.
+int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision, bool gated_done = false);
+// Whether the unit's forward z passes can take over the band-gated bins of
+// the solve (FP64 and mixed forms, z passes that have the rule, the plane
+// order built); if so fills zp[6] (cov grids in unit order) and makes sure
+// the non-finite flags exist.
+int gated_prior_setup(crava_gpu_ctx *c, int precision, ZPrior zp[6], bool *on);
+// After the forward passes that took zp: the flagged bins into the counters.
+int gated_prior_count(crava_gpu_ctx *c);
 // Transforms, solve and inverse transforms (in == out: in place).
 int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids *out,
              int precision);

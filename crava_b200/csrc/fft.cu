@@ -389,6 +389,7 @@ struct ColRRArgs {
   long long B;
   long long es;
   const float2 *tw;
+  ZPrior zp;  // forward z pass of a covariance grid: the band-gated rule (inv null: none)
 };
 
 template <int N>
@@ -405,12 +406,27 @@ struct RrColStages {
   // v holds the inputs of stage S (registers (b, q) of radix R_S)
   static __device__ __forceinline__ void run(float2 (&v)[CPT][RrCols<N>::E], float2 *buf,
                                              const float2 *tw, int t, int p, float2 *const *gp,
-                                             long long es, const bool *ok) {
+                                             long long es, const bool *ok, const ZPrior &zp,
+                                             const float2 *base) {
     constexpr int E = RrCols<N>::E, T = RrCols<N>::T, R = CtRadix::at(N, S);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) rr::stage_compute<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: outputs at the loaded positions, straight to HBM
+      if (DIR < 0 && zp.inv) {
+        // band-gated kz planes of a covariance grid: the prior rule
+#pragma unroll
+        for (int b = 0; b < E / R; ++b)
+#pragma unroll
+          for (int q = 0; q < R; ++q) {
+            const int e = rr::stage_in<N, S, E, T>(t, b, q);
+            if (__ldg(zp.inv + e) == 0) {
+#pragma unroll
+              for (int c = 0; c < CPT; ++c)
+                if (ok[c]) v[c][b * R + q] = zprior_apply(zp, v[c][b * R + q], (long long)(gp[c] - base) + (long long)e * es);
+            }
+          }
+      }
 #pragma unroll
       for (int b = 0; b < E / R; ++b)
 #pragma unroll
@@ -454,7 +470,7 @@ struct RrColStages {
             v[0][b * R2 + q] = buf[e * kRrTX + p];
           }
         }
-      RrColStages<N, DIR, CPT, VEC, S + 1>::run(v, buf, tw, t, p, gp, es, ok);
+      RrColStages<N, DIR, CPT, VEC, S + 1>::run(v, buf, tw, t, p, gp, es, ok, zp, base);
     }
   }
 };
@@ -497,7 +513,7 @@ __global__ void __launch_bounds__(RrCols<N>::NTH) k_cols_rr(const __grid_constan
       }
     }
   __syncthreads();  // twiddles
-  RrColStages<N, DIR, CPT, VEC, 0>::run(v, buf, tw, t, p, gp, a.es, ok);
+  RrColStages<N, DIR, CPT, VEC, 0>::run(v, buf, tw, t, p, gp, a.es, ok, a.zp, a.data);
 }
 
 // Row (x) pass for an even nxp, N = nxp / 2, register-resident: ROWS
@@ -868,7 +884,8 @@ static int cols_tile_width(int n) {
 }
 
 static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
-                long long outer_stride, int nouter, int dir, float scale, int tile, cudaStream_t s) {
+                long long outer_stride, int nouter, int dir, float scale, int tile, cudaStream_t s,
+                const ZPrior *zp = nullptr) {
   ColArgs a;
   a.data = data;
   a.ninner = ninner;
@@ -891,6 +908,7 @@ static int cols(const LinePlan &lp, float2 *data, int ninner, long long es,
     r.B = outer_stride;
     r.es = es;
     r.tw = lp.tw;
+    if (zp && dir < 0) r.zp = *zp;
     if (r.nlines >= (1LL << 31)) return CRAVA_GPU_ERR_ARG;
     const bool flat = outer_stride == ninner;
     // 16-byte accesses need the two lines of a thread adjacent and aligned:
@@ -976,15 +994,24 @@ int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
   return cols(p.y, grid, g.cnxp, g.cnxp, (long long)g.cnxp * g.nyp, g.nzp, dir, 1.0f, p.tile_y == 2 ? -1 : p.tile_y, s);
 }
 
-int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s) {
+bool z_prior_supported(const FftPlans &p) {
+  // the register-resident pass (tile -1 / 1) or its TMA-fed form (2); the
+  // TMA pass falls back to the register-resident one where a grid does not
+  // allow it, which applies the rule too
+  return rr::supported(p.g.nzp) && (p.tile_z == -1 || p.tile_z == 1 || p.tile_z == 2);
+}
+
+int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s, const ZPrior *zp) {
   const Geom &g = p.g;
+  if (zp && zp->inv && !z_prior_supported(p)) return CRAVA_GPU_ERR_ARG;
   // the TMA-fed pass (tile choice 2): faster alone; in the unit's lane
   // overlap it pays beside the fused x + y pass (5.23 against 5.85 ms per
   // 256x256x512x5 unit) and not beside the separate passes (5.92 against
   // 5.40 ms), so it is built in where the fused pass is
   const bool tma = p.tile_z == 2 || (p.tile_z == -1 && use_plane_xy(p));
-  if (tma && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s);
-  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z == 2 ? -1 : p.tile_z, s);
+  if (tma && cols_z_tma_supported(g, grid)) return cols_z_tma(p, grid, dir, s, zp);
+  return cols(p.z, grid, g.cnxp, (long long)g.cnxp * g.nyp, g.cnxp, g.nyp, dir, 1.0f, p.tile_z == 2 ? -1 : p.tile_z, s,
+              zp);
 }
 
 int fft3d_r2c(const FftPlans &p, float *grid, int type, cudaStream_t s) {

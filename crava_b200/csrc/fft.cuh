@@ -49,7 +49,7 @@ int plane_xy(const FftPlans &p, const float *src, float *dst, int dir, float sca
              cudaStream_t s);
 // Whether the transforms of these plans use the fused x + y pass.
 // Built in where the geometry has the kernel: alone it is slower than the
-// separate register-resident x and y passes (131 / 112 us against 59 + 54 /
+// separate register-resident x and y passes (129 / 113 us against 59 + 54 /
 // 56 + 52 us per 256x256x512 grid, forward / inverse), but it moves two
 // grids of HBM traffic instead of four, and in the unit, with the TMA-fed
 // z pass and three transform lanes, it gave 5.23 ms against 5.40 ms.
@@ -76,12 +76,63 @@ int fft3d_c2r(const FftPlans &p, float *grid, int type, cudaStream_t s,
 int fft_rows(const FftPlans &p, float *grid, int dir, float scale, cudaStream_t s,
              const float *addend = nullptr, const float *src = nullptr);
 int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
-int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
+
+// The band-gated covariance rule, applied by the forward z pass of a prior
+// covariance grid as it stores the spectrum.  On a kz plane outside the
+// inversion band (inv[kz] == 0) the per-bin loop of the reference only
+// rewrites the prior covariance, |Re c / S0| S0 with Im 0
+// (getNextParameterCovariance, src/seismicparametersholder.cpp:355-427;
+// src/crava.cpp:1098-1147): done here, the solve visits the inverted planes
+// alone and never reads or writes the band-gated bins.  mode 1: the FP64
+// form's rule (the double expression rounded to float; for a finite c it
+// equals sign(S0) |Re c| exactly, as the double error is far below half a
+// float ulp); mode 2: the mixed form's float operations.  A bin whose
+// output is not finite sets its bit in nf_bits (and nf_any), so that the
+// bins are counted once however many of the six grids hold a non-finite
+// value (crava_gpu_stats.nonfinite_bins counts bins).
+struct ZPrior {
+  const int *inv = nullptr;     // [nzp] band flags; null: no epilogue
+  double v = 0.0;               // this grid's Sigma0 entry
+  int mode = 0;                 // 1 FP64 form, 2 mixed form
+  unsigned *nf_bits = nullptr;  // one bit per bin of the grid
+  unsigned *nf_any = nullptr;
+};
+
+__device__ __forceinline__ float2 zprior_apply(const ZPrior &z, float2 x, long long bin) {
+  float r;
+  if (z.mode == 1) {
+    if (isfinite(x.x)) {
+      const float a = fabsf(x.x);
+      r = z.v != 0.0 ? (z.v < 0.0 ? -a : a) : a;
+    } else {
+      const double d = (double)x.x;
+      r = (float)(z.v != 0.0 ? fabs(d / z.v) * z.v : fabs(d));
+    }
+  } else {
+    const float vf = (float)z.v;
+    float y = x.x;
+    if (z.v != 0.0) y = y / vf;
+    r = fabsf(y) * vf;
+  }
+  if (!isfinite(r)) {
+    atomicOr(z.nf_bits + (bin >> 5), 1u << (unsigned)(bin & 31));
+    *(volatile unsigned *)z.nf_any = 1u;
+  }
+  return make_float2(r, 0.f);
+}
+
+// z pass; zp (forward only, optional): the band-gated covariance rule in
+// its store (where z_prior_supported says the pass has it).
+int fft_cols_z(const FftPlans &p, float2 *grid, int dir, cudaStream_t s, const ZPrior *zp = nullptr);
+// Whether fft_cols_z applies a ZPrior under these plans for every grid of
+// the geometry: the register-resident z pass and its TMA-fed form (lengths
+// 64..512) do, the in-place and generic passes do not.
+bool z_prior_supported(const FftPlans &p);
 
 // z pass with TMA tile loads (cols_tma.cu; column tile choice 2): lengths
 // 64..512, an even number of lines per z plane, a 16-byte aligned grid.
 bool cols_z_tma_supported(const Geom &g, const void *data);
-int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
+int cols_z_tma(const FftPlans &p, float2 *grid, int dir, cudaStream_t s, const ZPrior *zp = nullptr);
 // Tile waits of the TMA z pass that hit their limit (device-wide, since the
 // library was loaded; synchronous).
 int tile_wait_timeouts(unsigned long long *out);

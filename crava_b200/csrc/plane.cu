@@ -69,7 +69,10 @@ struct PlaneCfg {
   static constexpr int P = P0 + ((8 - P0 % 16) + 16) % 16;
   static constexpr int QK = NQ / CS;  // k1 range of one CTA in the radix-CS stage
   static __host__ __device__ constexpr int physx(int e) { return e + e / R0X; }
-  static constexpr size_t tab = sizeof(float2) * (NH + NH + 1 + NQ + NQ);
+  // tables, padded to an even float2 count so the plane buffer A starts on
+  // a 16-byte boundary (16-byte cp.async copies land in it)
+  static constexpr int TABN = NH + NH + 1 + NQ + NQ;
+  static constexpr size_t tab = sizeof(float2) * (TABN + (TABN & 1));
   static constexpr size_t smem = tab + sizeof(float2) * (size_t)NQ * P;
 };
 
@@ -132,7 +135,7 @@ __global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_fwd
   float2 *post = twx + NH;
   float2 *twq = post + NH + 1;
   float2 *twr = twq + NQ;  // W_NY^{r k1}, k1 < NQ
-  float2 *A = twr + NQ;    // [NQ][P]
+  float2 *A = twx + C::TABN + (C::TABN & 1);  // [NQ][P], 16-byte aligned
   const int tid = threadIdx.x, r = (int)cl.block_rank();
   for (int i = tid; i < NH; i += kPlaneThreads) twx[i] = a.twx[i];
   for (int i = tid; i <= NH; i += kPlaneThreads) post[i] = a.post[i];
@@ -148,18 +151,42 @@ __global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_fwd
   // 1. x: the NQ rows of this CTA, TX threads per row, rounds of
   //    kPlaneThreads / TX rows.  Every round's input rows travel into A by
   //    cp.async before the first round computes (one commit group per
-  //    round; 8-byte copies, as a row of odd index starts 8 bytes off a
-  //    16-byte boundary), so the HBM reads of a later round run under the
-  //    arithmetic of the earlier one.
+  //    round), so the HBM reads of a later round run under the arithmetic of
+  //    the earlier one.  A row y starts on a 16-byte boundary when y is even
+  //    (rnxp * 4 = 8 (NH + 1) bytes a row, NH + 1 odd); y = CS q + r has the
+  //    parity of r, the same for every row of this CTA.  Even rows are
+  //    copied as NH / 2 16-byte pairs into row[0 ..]; odd rows land one
+  //    element further, row[1 ..]: element 0 by an 8-byte copy, then the
+  //    pairs (1, 2) .. (NH - 1, NH) (element NH is the row's padding, inside
+  //    the row) as 16-byte copies.  A grid that is not 16-byte aligned takes
+  //    8-byte copies throughout.
   constexpr int RPR = kPlaneThreads / TX;  // rows per round
   constexpr int NRX = (NQ + RPR - 1) / RPR;
   static_assert(NRX <= 2, "the commit-group waits below cover two rounds");
+  static_assert((P % 2) == 0 && NH + 1 < P, "16-byte aligned rows with room for the shifted landing");
+  const bool wide = (reinterpret_cast<uintptr_t>(a.src) & 15u) == 0;
+  const int off = (wide && (r & 1)) ? 1 : 0;  // landing offset of this CTA's rows
 #pragma unroll
   for (int rd = 0; rd < NRX; ++rd) {
     const int q0 = rd * RPR, nr = NQ - q0 < RPR ? NQ - q0 : RPR;
-    for (int i = tid; i < nr * NH; i += kPlaneThreads) {
-      const int q = q0 + i / NH, e = i % NH;
-      cp_async8(A + q * P + e, reinterpret_cast<const float2 *>(src + (long long)(CS * q + r) * a.rnxp) + e);
+    if (wide) {
+      constexpr int TPR = NH / 2 + 1;  // tasks per row: the odd rows' single, then the pairs
+      for (int i = tid; i < nr * TPR; i += kPlaneThreads) {
+        const int q = q0 + i / TPR, j = i % TPR;
+        const float2 *in = reinterpret_cast<const float2 *>(src + (long long)(CS * q + r) * a.rnxp);
+        float2 *row = A + q * P;
+        if (j == 0) {
+          if (off) cp_async8(row + 1, in);
+        } else {
+          const int e = 2 * (j - 1) + off;  // first element of the pair
+          cp_async16(row + off + e, in + e);
+        }
+      }
+    } else {
+      for (int i = tid; i < nr * NH; i += kPlaneThreads) {
+        const int q = q0 + i / NH, e = i % NH;
+        cp_async8(A + q * P + e, reinterpret_cast<const float2 *>(src + (long long)(CS * q + r) * a.rnxp) + e);
+      }
     }
     cp_async_commit();
   }
@@ -175,7 +202,7 @@ __global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_fwd
 #pragma unroll
       for (int b = 0; b < EX / R0X; ++b)
 #pragma unroll
-        for (int qq = 0; qq < R0X; ++qq) v[b * R0X + qq] = row[rr::stage_in<NH, 0, EX, TX>(t, b, qq)];
+        for (int qq = 0; qq < R0X; ++qq) v[b * R0X + qq] = row[off + rr::stage_in<NH, 0, EX, TX>(t, b, qq)];
     }
     auto ix = [](int e) { return C::physx(e); };
     SmemStages<NH, -1, EX, TX, 0, true, decltype(ix)>::run(v, row, twx, t, act, ix);
@@ -292,7 +319,7 @@ __global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_inv
   float2 *post = twx + NH;
   float2 *twq = post + NH + 1;
   float2 *twr = twq + NQ;  // W_NY^{-r k1}
-  float2 *A = twr + NQ;
+  float2 *A = twx + C::TABN + (C::TABN & 1);
   const int tid = threadIdx.x, r = (int)cl.block_rank();
   for (int i = tid; i < NH; i += kPlaneThreads) twx[i] = a.twx[i];
   for (int i = tid; i <= NH; i += kPlaneThreads) post[i] = a.post[i];

@@ -157,6 +157,7 @@ struct SolveArgs {
   KzTables t;
   long long csize, plane;
   long long bpp;  // blocks per kz plane
+  long long nslots = 0;  // kz planes visited (t.order[0 .. nslots))
   DevCounters *counters;
   // Woodbury form: the per-plane tables and the list of the blocks it
   // defers to the square-root kernel
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(NTH, MINB) k_solve_pf(SolveArgs a) {
 template <int PREC, int NTH, int MINB, int BPT>
 int launch_solve_pf(SolveArgs a, int nt, cudaStream_t s) {
   a.bpp = (a.plane + (long long)NTH * BPT - 1) / ((long long)NTH * BPT);
-  dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
+  dim3 grd((unsigned)(a.bpp * a.nslots));
   int rc;
 #define CRAVA_PF_CASE(N)                                                                          \
   case N: {                                                                                       \
@@ -420,7 +421,7 @@ int launch_solve_pf(SolveArgs a, int nt, cudaStream_t s) {
 template <int PREC, int NTH, int MINB, bool LREG>
 int launch_solve_sq(SolveArgs a, int nt, cudaStream_t s) {
   a.bpp = (a.plane + NTH - 1) / NTH;
-  dim3 grd((unsigned)(a.bpp * (a.csize / a.plane)));
+  dim3 grd((unsigned)(a.bpp * a.nslots));
   int rc;
 #define CRAVA_SQ_CASE(N)                                                                          \
   case N: {                                                                                       \
@@ -542,7 +543,7 @@ __global__ void k_kz_wb(SolveConsts c, KzTables t, int nzp) {
 template <int NTH, int MINB>
 int launch_solve_wb(SolveArgs a, int nt, cudaStream_t s) {
   a.bpp = (a.plane + NTH - 1) / NTH;
-  const long long nblk = a.bpp * (a.csize / a.plane);
+  const long long nblk = a.bpp * a.nslots;
   if (nblk > a.t.defer_n || nblk >= (1LL << 31) || !a.counters) return CRAVA_GPU_ERR_ARG;
   a.wb = reinterpret_cast<const sb::WbTable *>(a.t.wb);
   a.list = a.t.defer_list;
@@ -637,6 +638,7 @@ int kz_tables_alloc(int nzp, int nt, KzTables *t) {
 void kz_tables_free(KzTables *t) {
   cudaFree(t->wd); cudaFree(t->e1); cudaFree(t->e2); cudaFree(t->e3); cudaFree(t->inv);
   cudaFree(t->order);
+  cudaFree(t->order_inv);
   cudaFree(t->wb);
   cudaFree(t->defer_list);
   *t = KzTables{};
@@ -679,8 +681,11 @@ int kz_order_build(int nzp, KzTables *t, cudaStream_t s, int *n_inverted) {
     order.push_back(take_heavy ? heavy[ih++] : light[il++]);
   }
   if (!t->order) CRAVA_CUDA_TRY(cudaMalloc(&t->order, sizeof(int) * nzp));
+  if (!t->order_inv) CRAVA_CUDA_TRY(cudaMalloc(&t->order_inv, sizeof(int) * nzp));
   CRAVA_CUDA_TRY(cudaMemcpyAsync(t->order, order.data(), sizeof(int) * nzp, cudaMemcpyHostToDevice, s));
+  if (nh) CRAVA_CUDA_TRY(cudaMemcpyAsync(t->order_inv, heavy.data(), sizeof(int) * nh, cudaMemcpyHostToDevice, s));
   CRAVA_CUDA_TRY(cudaStreamSynchronize(s));
+  t->n_inv = (int)nh;
   return CRAVA_GPU_OK;
 }
 
@@ -726,15 +731,56 @@ int kz_tables_build_device(const crava_gpu_params &p, const float *d_wavelet,
 
 int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g,
                     long long csize, long long plane, int precision,
-                    DevCounters *counters, cudaStream_t s) {
-  if (precision == CRAVA_SOLVE_FP32) return posterior_solve_fp32ref(c, t, g, csize, plane, counters, s);
+                    DevCounters *counters, cudaStream_t s, bool gated_done) {
+  if (precision == CRAVA_SOLVE_FP32) {
+    if (gated_done) return CRAVA_GPU_ERR_ARG;  // the reference-order kernel visits every bin
+    return posterior_solve_fp32ref(c, t, g, csize, plane, counters, s);
+  }
   SolveArgs a;
   a.c = c; a.g = g; a.t = t; a.csize = csize; a.plane = plane; a.counters = counters;
   a.bpp = (plane + kThreads - 1) / kThreads;
+  a.nslots = csize / plane;
+  if (gated_done) {
+    if (t.n_inv < 0 || !t.order_inv) return CRAVA_GPU_ERR_ARG;
+    a.t.order = t.order_inv;
+    a.nslots = t.n_inv;
+    if (a.nslots == 0) return CRAVA_GPU_OK;  // no inverted plane: nothing left to solve
+  }
   // the square-root form (one kz plane per CTA)
   if (precision == CRAVA_SOLVE_FP64) return launch_solve_sq_shape<0>(a, c.nt, s);
   if (precision == CRAVA_SOLVE_MIXED) return launch_solve_sq_shape<1>(a, c.nt, s);
   return CRAVA_GPU_ERR_ARG;
+}
+
+}  // namespace crava
+
+namespace crava {
+
+namespace {
+
+__global__ void __launch_bounds__(1024) k_gated_nonfinite(unsigned *bits, long long nwords, unsigned *any,
+                                                          DevCounters *ctr) {
+  if (*(volatile unsigned *)any == 0u) return;  // every thread reads the flag before thread 0 clears it
+  unsigned long long n = 0;
+  for (long long i = threadIdx.x; i < nwords; i += blockDim.x) {
+    const unsigned w = bits[i];
+    if (w) {
+      n += (unsigned long long)__popc(w);
+      bits[i] = 0u;
+    }
+  }
+  if (n) atomicAdd(&ctr->nonfinite, n);
+  __syncthreads();
+  if (threadIdx.x == 0) *any = 0u;
+}
+
+}  // namespace
+
+int gated_nonfinite_count(unsigned *nf_bits, long long nwords, unsigned *nf_any, DevCounters *counters,
+                          cudaStream_t s) {
+  k_gated_nonfinite<<<1, 1024, 0, s>>>(nf_bits, nwords, nf_any, counters);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
 }
 
 }  // namespace crava

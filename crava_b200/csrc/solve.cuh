@@ -14,6 +14,10 @@ struct KzTables {
   int *inv = nullptr;    // [nzp]      invert_frequency
   int *order = nullptr;  // [nzp]      plane visiting order of the solve
                          //            (null: natural order)
+  int *order_inv = nullptr;  // [n_inv]  the inverted planes alone (the
+                             //          solve when the band-gated planes
+                             //          were done by the forward z pass)
+  int n_inv = -1;            // inverted planes (-1: order not built)
   // FP64 solve in the Woodbury form (woodbury.cuh): the per-plane tables
   // (sb::WbTable [nzp]) and room for the list of the blocks it defers
   // (defer_n = blocks of its grid, 128 bins per block); null: the form is
@@ -77,9 +81,17 @@ int kz_tables_build_device(const crava_gpu_params &p, const float *d_wavelet,
                            const float *d_norm, KzTables *t, cudaStream_t s);
 
 // Per-bin solve over csize bins; plane = cnxp * nyp bins per kz.
+// gated_done (FP64 and mixed forms, with the order built): the band-gated
+// planes already hold the prior covariance (the forward z pass's ZPrior
+// rule, fft.cuh), so only the inverted planes are visited.
 int posterior_solve(const SolveConsts &c, const KzTables &t, const SolveGrids &g,
                     long long csize, long long plane, int precision,
-                    DevCounters *counters, cudaStream_t s);
+                    DevCounters *counters, cudaStream_t s, bool gated_done = false);
+// Counts the bins flagged by ZPrior epilogues (nf_bits, nwords words, and
+// nf_any) into counters->nonfinite and clears the flags; one block, which
+// returns at once when nothing was flagged.
+int gated_nonfinite_count(unsigned *nf_bits, long long nwords, unsigned *nf_any, DevCounters *counters,
+                          cudaStream_t s);
 // FP32 form with the reference's operation order (separate translation
 // unit compiled without FMA contraction).
 int posterior_solve_fp32ref(const SolveConsts &c, const KzTables &t,
