@@ -134,21 +134,23 @@ struct ZTmaStages {
   using Z = ZT<N>;
   // v holds the inputs of stage S
   static __device__ __forceinline__ void run(float2 (&v)[Z::CPT][Z::E], float2 *B, const float2 *tw, int t, int p,
-                                             float2 *g, long long L, bool ok, const ZPrior &zp, long long f) {
+                                             float2 *g, long long L, bool ok, const ZPrior &zp, long long f,
+                                             unsigned gmask) {
     constexpr int E = Z::E, T = Z::T, CPT = Z::CPT, R = CtRadix::at(N, S);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) rr::stage_compute_st<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: the outputs sit at the positions loaded, straight to HBM
-      if (DIR < 0 && zp.inv && ok) {
-        // band-gated kz planes of a covariance grid: the prior rule (the
-        // CPT lines of a thread are f, f + 1: L is even)
+      if (DIR < 0 && gmask && ok) {
+        // band-gated kz planes of a covariance grid (gmask: this thread's
+        // output registers on them): the prior rule (the CPT lines of a
+        // thread are f, f + 1: L is even)
 #pragma unroll
         for (int b = 0; b < E / R; ++b)
 #pragma unroll
           for (int q = 0; q < R; ++q) {
-            const int e = rr::stage_in<N, S, E, T>(t, b, q);
-            if (__ldg(zp.inv + e) == 0) {
+            if ((gmask >> (b * R + q)) & 1u) {
+              const int e = rr::stage_in<N, S, E, T>(t, b, q);
 #pragma unroll
               for (int c = 0; c < CPT; ++c)
                 v[c][b * R + q] = zprior_apply(zp, v[c][b * R + q], f + c + (long long)e * L);
@@ -196,7 +198,7 @@ struct ZTmaStages {
             v[0][b * R2 + q] = B[e * kTileLines + p];
           }
         }
-      ZTmaStages<N, DIR, S + 1>::run(v, B, tw, t, p, g, L, ok, zp, f);
+      ZTmaStages<N, DIR, S + 1>::run(v, B, tw, t, p, g, L, ok, zp, f, gmask);
     }
   }
 };
@@ -223,6 +225,7 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
     mbar_init_fence();
   }
   rr::tw_stages_fill<N>(tw, a.tw, tid, Z::NTH);
+  const unsigned gmask = DIR < 0 ? zprior_mask<N, E, T>(a.zp, t) : 0u;
   __syncthreads();
   // tiles of this CTA: blockIdx.x, + gridDim.x, ... (persistent grid,
   // tpc 0) or the run of tpc tiles from blockIdx.x * tpc
@@ -259,7 +262,7 @@ __global__ void __launch_bounds__(ZT<N>::NTH, ZT<N>::MINB) k_cols_z_tma(const __
       }
     __syncthreads();  // the landed tile is read before the first exchange overwrites it
     const long long f = (long long)tile * kTileLines + p * CPT;
-    ZTmaStages<N, DIR, 0>::run(v, B, tw, t, p, a.data + f, a.L, f < a.L, a.zp, f);
+    ZTmaStages<N, DIR, 0>::run(v, B, tw, t, p, a.data + f, a.L, f < a.L, a.zp, f, gmask);
     fence_proxy_async_smem();
     __syncthreads();  // every thread is done with this buffer
     if (tid == 0 && tile + 2 * G < end) issue_tile<N>(&tm, bufs + sb * Z::BYTES, mbs + 8u * sb, tile + 2 * G);

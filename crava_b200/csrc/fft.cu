@@ -407,20 +407,21 @@ struct RrColStages {
   static __device__ __forceinline__ void run(float2 (&v)[CPT][RrCols<N>::E], float2 *buf,
                                              const float2 *tw, int t, int p, float2 *const *gp,
                                              long long es, const bool *ok, const ZPrior &zp,
-                                             const float2 *base) {
+                                             const float2 *base, unsigned gmask) {
     constexpr int E = RrCols<N>::E, T = RrCols<N>::T, R = CtRadix::at(N, S);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) rr::stage_compute<N, S, DIR, E, T>(v[c], tw, t);
     if constexpr (S + 1 == CtRadix::count(N)) {
       // last stage: outputs at the loaded positions, straight to HBM
-      if (DIR < 0 && zp.inv) {
-        // band-gated kz planes of a covariance grid: the prior rule
+      if (DIR < 0 && gmask) {
+        // band-gated kz planes of a covariance grid (gmask: this thread's
+        // output registers on them): the prior rule
 #pragma unroll
         for (int b = 0; b < E / R; ++b)
 #pragma unroll
           for (int q = 0; q < R; ++q) {
-            const int e = rr::stage_in<N, S, E, T>(t, b, q);
-            if (__ldg(zp.inv + e) == 0) {
+            if ((gmask >> (b * R + q)) & 1u) {
+              const int e = rr::stage_in<N, S, E, T>(t, b, q);
 #pragma unroll
               for (int c = 0; c < CPT; ++c)
                 if (ok[c]) v[c][b * R + q] = zprior_apply(zp, v[c][b * R + q], (long long)(gp[c] - base) + (long long)e * es);
@@ -470,7 +471,7 @@ struct RrColStages {
             v[0][b * R2 + q] = buf[e * kRrTX + p];
           }
         }
-      RrColStages<N, DIR, CPT, VEC, S + 1>::run(v, buf, tw, t, p, gp, es, ok, zp, base);
+      RrColStages<N, DIR, CPT, VEC, S + 1>::run(v, buf, tw, t, p, gp, es, ok, zp, base, gmask);
     }
   }
 };
@@ -513,7 +514,8 @@ __global__ void __launch_bounds__(RrCols<N>::NTH) k_cols_rr(const __grid_constan
       }
     }
   __syncthreads();  // twiddles
-  RrColStages<N, DIR, CPT, VEC, 0>::run(v, buf, tw, t, p, gp, a.es, ok, a.zp, a.data);
+  const unsigned gmask = DIR < 0 ? zprior_mask<N, E, T>(a.zp, t) : 0u;
+  RrColStages<N, DIR, CPT, VEC, 0>::run(v, buf, tw, t, p, gp, a.es, ok, a.zp, a.data, gmask);
 }
 
 // Row (x) pass for an even nxp, N = nxp / 2, register-resident: ROWS

@@ -3,6 +3,7 @@
 
 #include "common.cuh"
 #include "fft_core.cuh"
+#include "fft_rr.cuh"
 
 namespace crava {
 
@@ -98,6 +99,17 @@ struct ZPrior {
   unsigned *nf_any = nullptr;
 };
 
+// The rare paths out of line: the FP64 form's double expression for a
+// non-finite value, and the flagging of a non-finite output.
+static __device__ __noinline__ float zprior_fp64_nonfinite(double v, float x) {
+  const double d = (double)x;
+  return (float)(v != 0.0 ? fabs(d / v) * v : fabs(d));
+}
+static __device__ __noinline__ void zprior_flag(unsigned *bits, unsigned *any, long long bin) {
+  atomicOr(bits + (bin >> 5), 1u << (unsigned)(bin & 31));
+  *(volatile unsigned *)any = 1u;
+}
+
 __device__ __forceinline__ float2 zprior_apply(const ZPrior &z, float2 x, long long bin) {
   float r;
   if (z.mode == 1) {
@@ -105,8 +117,7 @@ __device__ __forceinline__ float2 zprior_apply(const ZPrior &z, float2 x, long l
       const float a = fabsf(x.x);
       r = z.v != 0.0 ? (z.v < 0.0 ? -a : a) : a;
     } else {
-      const double d = (double)x.x;
-      r = (float)(z.v != 0.0 ? fabs(d / z.v) * z.v : fabs(d));
+      r = zprior_fp64_nonfinite(z.v, x.x);
     }
   } else {
     const float vf = (float)z.v;
@@ -114,11 +125,26 @@ __device__ __forceinline__ float2 zprior_apply(const ZPrior &z, float2 x, long l
     if (z.v != 0.0) y = y / vf;
     r = fabsf(y) * vf;
   }
-  if (!isfinite(r)) {
-    atomicOr(z.nf_bits + (bin >> 5), 1u << (unsigned)(bin & 31));
-    *(volatile unsigned *)z.nf_any = 1u;
-  }
+  if (!isfinite(r)) zprior_flag(z.nf_bits, z.nf_any, bin);
   return make_float2(r, 0.f);
+}
+
+// Bit b R + q set where the last stage's output register (b, q) of thread
+// t lies on a band-gated kz plane: the band flags are read once per thread,
+// not per tile.
+template <int N, int E, int T>
+__device__ __forceinline__ unsigned zprior_mask(const ZPrior &z, int t) {
+  constexpr int S = CtRadix::count(N) - 1, R = CtRadix::at(N, S);
+  static_assert(E <= 32, "one bit per register of a line");
+  unsigned m = 0u;
+  if (z.inv) {
+#pragma unroll
+    for (int b = 0; b < E / R; ++b)
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        if (__ldg(z.inv + rr::stage_in<N, S, E, T>(t, b, q)) == 0) m |= 1u << (b * R + q);
+  }
+  return m;
 }
 
 // z pass; zp (forward only, optional): the band-gated covariance rule in
