@@ -289,48 +289,63 @@ __device__ __forceinline__ int mirror(int i, int n, int np) {
 struct Local {
   float ishift, gain;
   bool on;
+  double q1;  // ishift / nzp: the phase step per bin, in turns (set with on)
 };
+
+// The phase step of a local wavelet: one division per trace and bin where
+// each rotation below would otherwise divide by nzp.  For a power-of-two
+// nzp (the fused lengths) q1 * m equals ishift * m / nzp exactly; for other
+// lengths it differs by at most an ulp of the double phase.
+__device__ __forceinline__ void local_on(Local &L, float ishift, float gain, int nzp) {
+  L.ishift = ishift;
+  L.gain = gain;
+  L.on = true;
+  L.q1 = (double)ishift / (double)nzp;
+}
 
 // e^{-2 pi i ishift m / nzp}, the ampMultiplier phase of shiftAndScale.
 // The reference evaluates cos / sin of 2 pi ishift m / nzp in double; here
-// the phase in turns is reduced to (-1/2, 1/2] in double (exact for the
-// float shift and integer bin) and the angle is evaluated in float, which
-// keeps the rotation within a few 1e-7 while the per-(trace, bin) work
-// stays off the FP64 pipe.
-__device__ __forceinline__ float2 phase_rot(const Local &L, int m, int nzp) {
-  const double q = (double)L.ishift * (double)m / (double)nzp;
+// the phase in turns is reduced to (-1/2, 1/2] in double (ishift m / nzp for
+// the float shift and integer bin) and the angle is evaluated in float,
+// which keeps the rotation within a few 1e-7 while the per-(trace, bin)
+// work stays off the FP64 pipe.
+__device__ __forceinline__ float2 phase_rot(const Local &L, int m) {
+  const double q = L.q1 * (double)m;
   const float f = (float)(q - rint(q));
   float sn, cs;
   sincospif(2.0f * f, &sn, &cs);
   return make_float2(cs, -sn);
 }
 
-__device__ __forceinline__ float2 local_bin(const float2 *tab, int m, int nzp, const Local &L, float gain) {
+// Bin m of the wavelet table as the local wavelet holds it, its rotation r
+// (phase_rot(L, m)) given: gain x r x value in float.
+__device__ __forceinline__ float2 local_bin_r(const float2 *tab, int m, const Local &L, float2 r) {
   const float2 v = __ldg(tab + m);
   if (!L.on) return v;
-  const float2 r = phase_rot(L, m, nzp);
-  const float ar = __fmul_rn(gain, r.x), ai = __fmul_rn(gain, r.y);
+  const float ar = __fmul_rn(L.gain, r.x), ai = __fmul_rn(L.gain, r.y);
   return make_float2(__fsub_rn(__fmul_rn(ar, v.x), __fmul_rn(ai, v.y)),
                      __fadd_rn(__fmul_rn(ai, v.x), __fmul_rn(ar, v.y)));
 }
 
 // The normalised third difference of the local wavelet: the global one
-// times 1/normF3, rotated (its gain cancels in the normalisation); the
+// times 1/normF3, rotated by r (its gain cancels in the normalisation); the
 // floats past nzp carry multiplyRAmpByConstant's RMISSING
 // (src/wavelet.cpp:466-474).
-__device__ __forceinline__ float2 local_e3(const float2 *E3, int m, int nzp, const Local &L, float inv) {
+__device__ __forceinline__ float2 local_e3_r(const float2 *E3, int m, int nzp, const Local &L, float inv, float2 r) {
   const float2 u = __ldg(E3 + m);
   float2 v = make_float2(__fmul_rn(u.x, inv), __fmul_rn(u.y, inv));
-  if (L.on) {
-    const float2 r = phase_rot(L, m, nzp);
+  if (L.on)
     v = make_float2(__fsub_rn(__fmul_rn(r.x, v.x), __fmul_rn(r.y, v.y)),
                     __fadd_rn(__fmul_rn(r.y, v.x), __fmul_rn(r.x, v.y)));
-  }
   if (m == nzp / 2) {
     if ((nzp & 1) == 0) v = make_float2(kMissing, kMissing);
     else v.y = kMissing;
   }
   return v;
+}
+
+__device__ __forceinline__ float2 local_e3(const float2 *E3, int m, int nzp, const Local &L, float inv) {
+  return local_e3_r(E3, m, nzp, L, inv, L.on ? phase_rot(L, m) : make_float2(1.0f, 0.0f));
 }
 
 // |local_e3(E3, m)|^2: the rotation keeps the modulus, so it is needed
@@ -346,24 +361,33 @@ __device__ __forceinline__ float local_e3_mag2(const float2 *E3, int m, int nzp,
   return __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
 }
 
-// Wavelet::getCAmp(k, scale) for k < cnzp (src/wavelet.cpp:327-385).
-template <bool E3TAB>
-__device__ __forceinline__ float2 camp_scaled(const float2 *tab, int k, float scale, int nzp,
-                                              const Local &L, float inv) {
+// Wavelet::getCAmp(k, scale) for k < cnzp (src/wavelet.cpp:327-385) of the
+// local wavelet (w) and, when e3 is given, of its normalised third
+// difference, from one pair of interpolation bins and one pair of
+// rotations.
+__device__ __forceinline__ void camp_scaled2(const float2 *W, const float2 *E3, int k, float scale, int nzp,
+                                             const Local &L, float inv, float2 *w, float2 *e3) {
   const int cnzp = nzp / 2 + 1;
   const float omega = __fdividef((float)k, scale);
-  float2 v = make_float2(0.0f, 0.0f);
+  float2 vw = make_float2(0.0f, 0.0f), ve = make_float2(0.0f, 0.0f);
   if (omega < (float)cnzp) {
     const int omL = (int)floorf(omega);
     int omU = omL + 1;
     if (omU >= cnzp) omU -= 1;
     const float dO = __fsub_rn(omega, (float)omL), dL = __fsub_rn(1.0f, dO);
-    const float2 a = E3TAB ? local_e3(tab, omL, nzp, L, inv) : local_bin(tab, omL, nzp, L, L.gain);
-    const float2 b = E3TAB ? local_e3(tab, omU, nzp, L, inv) : local_bin(tab, omU, nzp, L, L.gain);
-    v.x = __fadd_rn(__fmul_rn(a.x, dL), __fmul_rn(b.x, dO));
-    v.y = __fadd_rn(__fmul_rn(a.y, dL), __fmul_rn(b.y, dO));
+    const float2 rL = L.on ? phase_rot(L, omL) : make_float2(1.0f, 0.0f);
+    const float2 rU = L.on ? phase_rot(L, omU) : make_float2(1.0f, 0.0f);
+    const float2 a = local_bin_r(W, omL, L, rL), b = local_bin_r(W, omU, L, rU);
+    vw.x = __fadd_rn(__fmul_rn(a.x, dL), __fmul_rn(b.x, dO));
+    vw.y = __fadd_rn(__fmul_rn(a.y, dL), __fmul_rn(b.y, dO));
+    if (e3) {
+      const float2 c = local_e3_r(E3, omL, nzp, L, inv, rL), d = local_e3_r(E3, omU, nzp, L, inv, rU);
+      ve.x = __fadd_rn(__fmul_rn(c.x, dL), __fmul_rn(d.x, dO));
+      ve.y = __fadd_rn(__fmul_rn(c.y, dL), __fmul_rn(d.y, dO));
+    }
   }
-  return make_float2(__fdividef(v.x, scale), __fdividef(v.y, scale));
+  *w = make_float2(__fdividef(vw.x, scale), __fdividef(vw.y, scale));
+  if (e3) *e3 = make_float2(__fdividef(ve.x, scale), __fdividef(ve.y, scale));
 }
 
 __device__ __forceinline__ float sq2(float2 v) { return __fadd_rn(__fmul_rn(v.x, v.x), __fmul_rn(v.y, v.y)); }
@@ -378,7 +402,7 @@ __device__ float2 adjust(const DivFilterArgs &a, int k, int i, int j, float2 d) 
   const long long tr = i + (long long)a.nxp * j;
   const double deltaF = __ldg(a.df + tr);
   if (!(deltaF * k < (double)a.high_cut && deltaF * k > (double)a.low_cut)) return make_float2(0.0f, 0.0f);
-  Local L{0.0f, 1.0f, false};
+  Local L{0.0f, 1.0f, false, 0.0};
   if (a.shift || a.gain) {
     const int ii = mirror(i, a.nx, a.nxp), jj = mirror(j, a.ny, a.nyp);
     constexpr float kWellMissing = -999.0f;  // WELLMISSING, src/definitions.h:39
@@ -391,19 +415,18 @@ __device__ float2 adjust(const DivFilterArgs &a, int k, int i, int j, float2 d) 
       if (a.shift && a.shift[o] != kWellMissing) ts = a.shift[o];
       if (a.gain && a.gain[o] != kWellMissing) g = a.gain[o];
     }
-    L.ishift = __fdiv_rn(ts, a.dz);
-    L.gain = g;
-    L.on = true;
+    local_on(L, __fdiv_rn(ts, a.dz), g, a.nzp);
   }
   const float sf = __ldg(a.sf + tr);
   const DivScalars s = *a.sc;
   const float tolFac = 0.05f;
-  const float2 wLoc = camp_scaled<false>(a.W, k, sf, a.nzp, L, 1.0f);
+  float2 wLoc, e3Loc;
+  camp_scaled2(a.W, a.E3, k, sf, a.nzp, L, s.e3_inv, &wLoc, &e3Loc);
   const float wLoc2 = sq2(wLoc);
   const float2 wGlob = __ldg(a.W + k);
   const float wGlob2 = sq2(wGlob);
   float sizeLoc = __fdividef(wLoc2, s.wn2);
-  sizeLoc = __fadd_rn(sizeLoc, sq2(camp_scaled<true>(a.E3, k, sf, a.nzp, L, s.e3_inv)));
+  sizeLoc = __fadd_rn(sizeLoc, sq2(e3Loc));
   // |shifted and scaled W_k|^2 = gain^2 |W_k|^2 (the rotation keeps the modulus)
   const float g2 = L.on ? __fmul_rn(L.gain, L.gain) : 1.0f;
   float sizeGlob = __fdividef(__fmul_rn(g2, wGlob2), s.wn2);
@@ -484,19 +507,18 @@ struct FusedArgs {
 // wavelet (src/crava.cpp:852-865); the local shift and gain are read at
 // the trace itself.
 __device__ __forceinline__ float2 mul_conj(const FusedArgs &a, int k, int i, int j, float2 d) {
-  Local L{0.0f, 1.0f, false};
+  Local L{0.0f, 1.0f, false, 0.0};
   if (a.f.shift || a.f.gain) {
     constexpr float kWellMissing = -999.0f;  // WELLMISSING, src/definitions.h:39
     const long long o = i + (long long)a.nx * j;
     float ts = 0.0f, g = 1.0f;
     if (a.f.shift && a.f.shift[o] != kWellMissing) ts = a.f.shift[o];
     if (a.f.gain && a.f.gain[o] != kWellMissing) g = a.f.gain[o];
-    L.ishift = __fdiv_rn(ts, a.f.dz);
-    L.gain = g;
-    L.on = true;
+    local_on(L, __fdiv_rn(ts, a.f.dz), g, a.nzp);
   }
   const float sf = __ldg(a.sfm + i + (long long)a.nxp * j);
-  const float2 w = camp_scaled<false>(a.Wm, k, sf, a.nzp, L, 1.0f);
+  float2 w;
+  camp_scaled2(a.Wm, nullptr, k, sf, a.nzp, L, 1.0f, &w, nullptr);
   return make_float2(__fadd_rn(__fmul_rn(d.x, w.x), __fmul_rn(d.y, w.y)),
                      __fsub_rn(__fmul_rn(d.y, w.x), __fmul_rn(d.x, w.y)));
 }
@@ -793,19 +815,18 @@ struct MulFilterArgs {
 // The data bin times the conjugate of getCAmp(k, sf) of the trace's local
 // wavelet (src/crava.cpp:852-865).
 __device__ __forceinline__ float2 mul_local(const MulFilterArgs &a, int k, int i, int j, float2 d) {
-  Local L{0.0f, 1.0f, false};
+  Local L{0.0f, 1.0f, false, 0.0};
   if (a.shift || a.gain) {
     constexpr float kWellMissing = -999.0f;  // WELLMISSING, src/definitions.h:39
     const long long o = i + (long long)a.nx * j;
     float ts = 0.0f, g = 1.0f;
     if (a.shift && a.shift[o] != kWellMissing) ts = a.shift[o];
     if (a.gain && a.gain[o] != kWellMissing) g = a.gain[o];
-    L.ishift = __fdiv_rn(ts, a.dz);
-    L.gain = g;
-    L.on = true;
+    local_on(L, __fdiv_rn(ts, a.dz), g, a.nzp);
   }
   const float sf = __ldg(a.sf + i + (long long)a.nxp * j);
-  const float2 w = camp_scaled<false>(a.W, k, sf, a.nzp, L, 1.0f);
+  float2 w;
+  camp_scaled2(a.W, nullptr, k, sf, a.nzp, L, 1.0f, &w, nullptr);
   return make_float2(__fadd_rn(__fmul_rn(d.x, w.x), __fmul_rn(d.y, w.y)),
                      __fsub_rn(__fmul_rn(d.y, w.x), __fmul_rn(d.x, w.y)));
 }
