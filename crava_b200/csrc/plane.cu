@@ -43,6 +43,9 @@ namespace {
 // third holding the Nyquist column alone; three CTAs per SM
 constexpr int kPlaneThreads = 288;
 constexpr int kPlaneMinBlocks = 3;
+// items per thread whose HBM loads the inverse's radix-CS stage keeps in
+// flight together
+constexpr int kInvItems = 4;
 
 struct PlaneArgs {
   const float *src;   // forward: real input planes (may equal dst)
@@ -340,27 +343,29 @@ __global__ void __launch_bounds__(kPlaneThreads, kPlaneMinBlocks) k_plane_xy_inv
   float2 *At[CS];
 #pragma unroll
   for (int s = 0; s < CS; ++s) At[s] = cl.map_shared_rank(A, s);
-  // two items per thread and step: their 2 CS loads from HBM are in
-  // flight together
+  // kInvItems items per thread and step: their kInvItems x CS loads from
+  // HBM are in flight together (an item past the end reloads item i0 and
+  // stores nothing)
   constexpr int NI = C::QK * CX;
-  for (int i0 = tid; i0 < NI; i0 += 2 * kPlaneThreads) {
-    const int i1 = i0 + kPlaneThreads;
-    const bool two = i1 < NI;
-    const int k1a = r * C::QK + i0 / CX, kxa = i0 % CX;
-    const int k1b = r * C::QK + (two ? i1 : i0) / CX, kxb = (two ? i1 : i0) % CX;
-    float2 va[CS], vb[CS];
+  constexpr int IPS = kInvItems;
+  for (int i0 = tid; i0 < NI; i0 += IPS * kPlaneThreads) {
+    float2 v[IPS][CS];
+    int k1[IPS], kx[IPS];
 #pragma unroll
-    for (int k2 = 0; k2 < CS; ++k2) {
-      va[k2] = src[(long long)(k1a + NQ * k2) * CX + kxa];
-      vb[k2] = src[(long long)(k1b + NQ * k2) * CX + kxb];
+    for (int u = 0; u < IPS; ++u) {
+      const int i = i0 + u * kPlaneThreads < NI ? i0 + u * kPlaneThreads : i0;
+      k1[u] = r * C::QK + i / CX;
+      kx[u] = i % CX;
+#pragma unroll
+      for (int k2 = 0; k2 < CS; ++k2) v[u][k2] = src[(long long)(k1[u] + NQ * k2) * CX + kx[u]];
     }
-    Dft<CS, 1>::run(va);
 #pragma unroll
-    for (int s = 0; s < CS; ++s) At[s][k1a * P + kxa] = va[s];
-    if (two) {
-      Dft<CS, 1>::run(vb);
+    for (int u = 0; u < IPS; ++u) {
+      if (i0 + u * kPlaneThreads < NI) {
+        Dft<CS, 1>::run(v[u]);
 #pragma unroll
-      for (int s = 0; s < CS; ++s) At[s][k1b * P + kxb] = vb[s];
+        for (int s = 0; s < CS; ++s) At[s][k1[u] * P + kx[u]] = v[u][s];
+      }
     }
   }
   cl.sync();
