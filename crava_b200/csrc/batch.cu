@@ -15,6 +15,7 @@ struct crava_gpu_batch {
     int nsim;
     uint64_t seed, first;
     std::vector<float *> sim;
+    float2 **d_sim = nullptr;  // device copy of sim (the persistent filter's output table)
   };
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -61,11 +62,13 @@ bool disjoint(const crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu
   return true;
 }
 
-// One vintage on its context's stream.  Without realisations this is the
-// unit (fused or three-pass, as tuned); with them it follows the
-// reference's order: the covariance spectra stay in the Fourier domain
-// until the realisations are drawn (src/crava.cpp:1165-1181, 1415-1599).
-int run_vintage(const crava_gpu_batch::Vintage &v, const unsigned long long *epoch) {
+// One vintage on its context's stream, up to its realisations.  Without
+// realisations this is the whole unit (fused or three-pass, as tuned); with
+// them it follows the reference's order: the covariance spectra stay in
+// the Fourier domain until the realisations are drawn
+// (src/crava.cpp:1165-1181, 1415-1599), so this part ends after the
+// inverse transforms of the means and residuals.
+int run_vintage_head(const crava_gpu_batch::Vintage &v) {
   crava_gpu_ctx *c = v.ctx;
   if (v.nsim == 0) return run_unit(c, &v.in, &v.out, v.precision);
   const int nt = c->p.ntheta;
@@ -92,17 +95,50 @@ int run_vintage(const crava_gpu_batch::Vintage &v, const unsigned long long *epo
     if ((rc = pass_inverse(c, out.mu[q], CRAVA_GRID_PARAMETER))) return rc;
   for (int l = 0; l < nt; ++l)
     if ((rc = pass_inverse(c, out.data[l], CRAVA_GRID_DATA))) return rc;
-  const float2 *cv[6];
-  for (int t = 0; t < 6; ++t) cv[t] = reinterpret_cast<const float2 *>(out.cov[t]);
+  return CRAVA_GPU_OK;
+}
+
+// The rest of a vintage with realisations, after the batch's realisation
+// filter: each realisation's three inverse transforms with the posterior
+// mean added, then the inverse transforms of the covariances.
+int run_vintage_tail(const crava_gpu_batch::Vintage &v) {
+  crava_gpu_ctx *c = v.ctx;
+  if (v.nsim == 0) return CRAVA_GPU_OK;
+  const crava_gpu_grids &out = v.out;
+  int rc;
   const float *pm[3] = {out.mu[0], out.mu[1], out.mu[2]};
-  if ((rc = simulate_batches(c, cv, pm, v.seed, v.first, v.nsim, v.sim.data(), epoch,
-                             (unsigned long long)v.nsim)))
-    return rc;
+  if ((rc = inverse_realisations(c, v.sim.data(), 3 * v.nsim, pm))) return rc;
   for (int t = 0; t < 6; ++t)
     if ((rc = pass_inverse(c, out.cov[t], CRAVA_GRID_COVARIANCE))) return rc;
   if ((rc = stage_event(c, 3))) return rc;
   c->timed = !c->capture;
   return CRAVA_GPU_OK;
+}
+
+// The realisation filter of every vintage with realisations, one
+// persistent launch on the batch stream (noise_filter_vintages).
+int filter_vintages(crava_gpu_batch *b) {
+  SimVintage sv[kMaxSimVintages];
+  int nv = 0;
+  for (const auto &v : b->v) {
+    if (v.nsim == 0) continue;
+    if (nv == kMaxSimVintages) return CRAVA_GPU_ERR_ARG;
+    crava_gpu_ctx *c = v.ctx;
+    SimVintage &w = sv[nv++];
+    for (int t = 0; t < 6; ++t) w.cov[t] = reinterpret_cast<const float2 *>(v.out.cov[t]);
+    w.out = v.d_sim;
+    w.csize = c->g.csize;
+    w.cnxp = c->g.cnxp; w.nyp = c->g.nyp; w.nzp = c->g.nzp;
+    w.nsim = v.nsim;
+    w.seed = v.seed;
+    w.stream0 = 3ull * v.first;
+    w.epoch_mul = 3ull * (unsigned long long)v.nsim;
+    w.counters = c->counters;
+  }
+  if (nv == 0) return CRAVA_GPU_OK;
+  int rc = noise_filter_vintages(sv, nv, b->epoch, b->stream);
+  if (!rc) note_launch();
+  return rc;
 }
 
 // Enqueues one run: fork from the batch stream into one branch per
@@ -122,15 +158,37 @@ int enqueue(crava_gpu_batch *b, bool capture, bool advance) {
     set_last_error(e, "batch fork", __FILE__, __LINE__);
     rc = CRAVA_GPU_ERR_CUDA;
   }
-  for (size_t k = 0; k < b->v.size() && !rc; ++k) rc = run_vintage(b->v[k], b->epoch);
-  for (size_t i = 0; i < nc && !rc; ++i) {
-    e = cudaEventRecord(b->join[i], b->cstream[i]);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[i], 0);
-    if (e != cudaSuccess) {
-      set_last_error(e, "batch join", __FILE__, __LINE__);
-      rc = CRAVA_GPU_ERR_CUDA;
+  auto join = [&]() {
+    for (size_t i = 0; i < nc && !rc; ++i) {
+      e = cudaEventRecord(b->join[i], b->cstream[i]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->join[i], 0);
+      if (e != cudaSuccess) {
+        set_last_error(e, "batch join", __FILE__, __LINE__);
+        rc = CRAVA_GPU_ERR_CUDA;
+      }
     }
+  };
+  // the vintages up to their realisations, one branch per context
+  for (size_t k = 0; k < b->v.size() && !rc; ++k) rc = run_vintage_head(b->v[k]);
+  bool sims = false;
+  for (const auto &v : b->v) sims = sims || v.nsim > 0;
+  if (sims && !rc) {
+    // every vintage's realisation filter in one persistent launch on the
+    // batch stream, then the branches again for the realisations' inverse
+    // transforms and the covariances
+    join();
+    if (!rc) rc = filter_vintages(b);
+    if (!rc) {
+      e = cudaEventRecord(b->fork, b->stream);
+      for (size_t i = 0; i < nc && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(b->cstream[i], b->fork, 0);
+      if (e != cudaSuccess) {
+        set_last_error(e, "batch fork", __FILE__, __LINE__);
+        rc = CRAVA_GPU_ERR_CUDA;
+      }
+    }
+    for (size_t k = 0; k < b->v.size() && !rc; ++k) rc = run_vintage_tail(b->v[k]);
   }
+  join();
   if (!rc && advance) {
     k_epoch_advance<<<1, 1, 0, b->stream>>>(b->epoch);
     cudaError_t le = cudaGetLastError();
@@ -158,6 +216,7 @@ void batch_free(crava_gpu_batch *b) {
   for (cudaEvent_t e : b->join) if (e) cudaEventDestroy(e);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->epoch) cudaFree(b->epoch);
+  for (auto &v : b->v) if (v.d_sim) cudaFree(v.d_sim);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -274,6 +333,9 @@ int crava_gpu_batch_create(const crava_gpu_vintage *vin, int n, int flags, void 
   if (!out) return CRAVA_GPU_ERR_ARG;
   *out = nullptr;
   if (!vin || n < 1 || (flags & ~(CRAVA_BATCH_AUTOTUNE | CRAVA_BATCH_NO_GRAPH))) return CRAVA_GPU_ERR_ARG;
+  int with_sims = 0;
+  for (int k = 0; k < n; ++k) with_sims += vin[k].nsim > 0;
+  if (with_sims > kMaxSimVintages) return CRAVA_GPU_ERR_ARG;  // one persistent filter launch holds them
   int rc;
   const int dev = vin[0].ctx ? vin[0].ctx->device : -1;
   for (int k = 0; k < n; ++k) {
@@ -301,6 +363,13 @@ int crava_gpu_batch_create(const crava_gpu_vintage *vin, int n, int flags, void 
     w.seed = v.seed; w.first = v.first_index;
     if (v.nsim > 0) w.sim.assign(v.sim_out, v.sim_out + 3 * v.nsim);
     b->v.push_back(std::move(w));
+    if (v.nsim > 0) {
+      // the output table of the persistent realisation filter
+      crava_gpu_batch::Vintage &bv = b->v.back();
+      const size_t bytes = sizeof(float2 *) * 3 * (size_t)v.nsim;
+      if (cudaMalloc(&bv.d_sim, bytes) != cudaSuccess) { bv.d_sim = nullptr; return fail(CRAVA_GPU_ERR_ALLOC); }
+      if (cudaMemcpy(bv.d_sim, bv.sim.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+    }
     bool seen = false;
     for (auto *c : b->ctxs) seen = seen || c == v.ctx;
     if (!seen) b->ctxs.push_back(v.ctx);

@@ -288,6 +288,10 @@ int stage_event(crava_gpu_ctx *c, int i) {
   return CRAVA_GPU_OK;
 }
 
+int inverse_realisations(crava_gpu_ctx *c, float *const *grids, int n, const float *const post_mean[3]) {
+  return on_lanes(c, n, [&](int k) { return pass_inverse(c, grids[k], CRAVA_GRID_PARAMETER, post_mean[k % 3]); });
+}
+
 int simulate_batches(crava_gpu_ctx *c, const float2 *const cv[6], const float *const post_mean[3],
                      uint64_t seed, uint64_t first, int count, float *const *out,
                      const unsigned long long *epoch, unsigned long long epoch_stride) {

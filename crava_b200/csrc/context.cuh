@@ -114,6 +114,9 @@ int run_unit(crava_gpu_ctx *c, const crava_gpu_grids *in, const crava_gpu_grids 
              int precision);
 // Records stage event i on the context's stream (skipped during capture).
 int stage_event(crava_gpu_ctx *c, int i);
+// Inverse transforms of n realisation grids (parameter p = k % 3 of grid
+// k) with post_mean[p] added, spread over the context's transform lanes.
+int inverse_realisations(crava_gpu_ctx *c, float *const *grids, int n, const float *const post_mean[3]);
 // count realisations from the posterior covariance spectra cv: realisation
 // r uses noise streams 3 (first + r) + p, plus 3 epoch_stride (*epoch) when
 // epoch is given (a device counter), and gets post_mean added.

@@ -265,7 +265,84 @@ __global__ void __launch_bounds__(kThreads) k_noise_filter_multi(const __grid_co
   }
 }
 
+struct SimAllArgs {
+  SimVintage v[kMaxSimVintages];
+  long long first_block[kMaxSimVintages + 1];  // prefix of the vintages' 256-bin blocks
+  int nv;
+  const unsigned long long *epoch;
+};
+
+__global__ void __launch_bounds__(kThreads) k_noise_filter_vintages(const __grid_constant__ SimAllArgs a) {
+  const long long nblocks = a.first_block[a.nv];
+  const unsigned long long ep = a.epoch ? *a.epoch : 0ull;
+  for (long long w = blockIdx.x; w < nblocks; w += gridDim.x) {
+    int v = 0;
+    while (v + 1 < a.nv && w >= a.first_block[v + 1]) ++v;
+    const SimVintage &V = a.v[v];
+    const long long i = (w - a.first_block[v]) * kThreads + threadIdx.x;
+    if (i < V.csize) {
+      float2 P[3][3];
+      P[0][0] = V.cov[0][i]; P[1][1] = V.cov[1][i]; P[2][2] = V.cov[2][i];
+      P[0][1] = V.cov[3][i]; P[0][2] = V.cov[4][i]; P[1][2] = V.cov[5][i];
+      P[1][0] = make_float2(P[0][1].x, -P[0][1].y);
+      P[2][0] = make_float2(P[0][2].x, -P[0][2].y);
+      P[2][1] = make_float2(P[1][2].x, -P[1][2].y);
+      const bool ok = chol3_ref(P) == 0;
+      const uint64_t stream0 = V.stream0 + V.epoch_mul * ep;
+      const NoiseSite site = noise_site(i, V.cnxp, V.nyp, V.nzp);  // once per bin
+      for (int r = 0; r < V.nsim; ++r) {
+        float2 z[3], o[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) z[q] = noise_value(site, V.seed, stream0 + 3ull * r + q);
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          o[p] = make_float2(0.0f, 0.0f);
+          if (ok) {
+#pragma unroll
+            for (int b = 0; b < p + 1; ++b) {
+              o[p].x += P[p][b].x * z[b].x - P[p][b].y * z[b].y;
+              o[p].y += P[p][b].x * z[b].y + P[p][b].y * z[b].x;
+            }
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < 3; ++p) V.out[3 * r + p][i] = o[p];
+      }
+      if (V.counters) {
+        const unsigned m = __activemask();
+        const unsigned b = __ballot_sync(m, !ok);
+        if (b && (threadIdx.x & 31) == __ffs(m) - 1)
+          atomicAdd(&V.counters->chol_fail, (unsigned long long)__popc(b) * (unsigned long long)V.nsim);
+      }
+    }
+  }
+}
+
 }  // namespace
+
+int noise_filter_vintages(const SimVintage *v, int nv, const unsigned long long *epoch, cudaStream_t s) {
+  if (nv < 1 || nv > kMaxSimVintages) return CRAVA_GPU_ERR_ARG;
+  SimAllArgs a;
+  a.nv = nv;
+  a.epoch = epoch;
+  a.first_block[0] = 0;
+  for (int k = 0; k < nv; ++k) {
+    if (v[k].nsim < 1 || !v[k].out) return CRAVA_GPU_ERR_ARG;
+    a.v[k] = v[k];
+    a.first_block[k + 1] = a.first_block[k] + (v[k].csize + kThreads - 1) / kThreads;
+  }
+  // persistent: the resident blocks of the device walk every vintage's blocks
+  int dev = 0, sms = 0, per = 0;
+  CRAVA_CUDA_TRY(cudaGetDevice(&dev));
+  CRAVA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CRAVA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_noise_filter_vintages, kThreads, 0));
+  const long long resident = (long long)(per > 0 ? per : 1) * sms;
+  const long long nb = a.first_block[nv];
+  dim3 grd((unsigned)(nb < resident ? nb : resident));
+  k_noise_filter_vintages<<<grd, kThreads, 0, s>>>(a);
+  CRAVA_LAUNCH_CHECK();
+  return CRAVA_GPU_OK;
+}
 
 int noise_filter_multi(const Geom &g, const float2 *const cov[6], float2 *const *out, int nreal,
                        uint64_t seed, uint64_t stream0, const unsigned long long *epoch,

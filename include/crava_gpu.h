@@ -335,7 +335,9 @@ int crava_gpu_autotune(crava_gpu_ctx *ctx, const crava_gpu_grids *in,
  * inverse transforms of the six covariance grids.  Run e (0, 1, ...) draws
  * realisations first_index + e*nsim + r, r < nsim, each with the noise of
  * crava_gpu_simulate for that index, so replays give fresh, reproducible
- * realisations.  Vintages run on separate branches of the graph. */
+ * realisations.  Vintages run on separate branches of the graph, joined
+ * for the realisation filter of all vintages, which is one persistent
+ * launch (at most 16 vintages with realisations). */
 typedef struct crava_gpu_vintage {
   crava_gpu_ctx *ctx;
   crava_gpu_grids in;      /* real inputs (read, not written)            */
