@@ -168,18 +168,11 @@ int pass_forward(crava_gpu_ctx *c, const float *src, float *dst, int type, const
 }
 
 int gated_prior_setup(crava_gpu_ctx *c, int precision, ZPrior zp[6], bool *on) {
+  // (the flags are allocated with the context where the z pass has the
+  // rule; a tuning that selects another z pass turns the rule off)
   *on = (precision == CRAVA_SOLVE_FP64 || precision == CRAVA_SOLVE_MIXED) && z_prior_supported(c->plans) &&
-        c->tables.n_inv >= 0 && c->tables.order_inv;
+        c->tables.n_inv >= 0 && c->tables.order_inv && c->gated_nf;
   if (!*on) return CRAVA_GPU_OK;
-  if (!c->gated_nf) {
-    const long long words = (c->g.csize + 31) / 32;
-    if (cudaMalloc(&c->gated_nf, (size_t)(words + 1) * sizeof(unsigned)) != cudaSuccess) {
-      c->gated_nf = nullptr;
-      return CRAVA_GPU_ERR_ALLOC;
-    }
-    CRAVA_CUDA_TRY(cudaMemsetAsync(c->gated_nf, 0, (size_t)(words + 1) * sizeof(unsigned), c->stream));
-    c->gated_nf_words = words;
-  }
   for (int t = 0; t < 6; ++t) {
     zp[t] = ZPrior{};
     zp[t].inv = c->tables.inv;
@@ -472,6 +465,18 @@ int crava_gpu_create(const crava_gpu_params *params, int device, void *stream,
   if ((rc = kz_tables_build(c->p, &c->tables, c->stream))) return fail(rc);
   if ((rc = kz_order_build(nzp, &c->tables, c->stream, &c->n_inverted))) return fail(rc);
   if ((rc = kz_woodbury_build(c->consts, nzp, c->tables, c->stream))) return fail(rc);
+  // the flags of non-finite band-gated bins (ZPrior): one bit per bin and
+  // the any-flag word, allocated here so that the unit allocates nothing
+  // (and can be captured into a CUDA graph on its first call)
+  if (z_prior_supported(c->plans)) {
+    const long long words = (c->g.csize + 31) / 32;
+    if (cudaMalloc(&c->gated_nf, (size_t)(words + 1) * sizeof(unsigned)) != cudaSuccess) {
+      c->gated_nf = nullptr;
+      return fail(CRAVA_GPU_ERR_ALLOC);
+    }
+    if (cudaMemset(c->gated_nf, 0, (size_t)(words + 1) * sizeof(unsigned)) != cudaSuccess) return fail(CRAVA_GPU_ERR_CUDA);
+    c->gated_nf_words = words;
+  }
   *out = c;
   return CRAVA_GPU_OK;
 }

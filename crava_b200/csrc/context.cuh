@@ -74,8 +74,8 @@ struct crava_gpu_ctx {
   char *ll_host = nullptr;
   size_t ll_host_bytes = 0;
   // bins whose band-gated prior (written by the forward z pass) is not
-  // finite: one bit per bin, then the any-flag word (zeroed once; the
-  // counting kernel clears what it counts)
+  // finite: one bit per bin, then the any-flag word (allocated and zeroed
+  // with the context; the counting kernel clears what it counts)
   unsigned *gated_nf = nullptr;
   long long gated_nf_words = 0;
 };
@@ -104,8 +104,8 @@ int pass_inverse(crava_gpu_ctx *c, float *grid, int type, const float *addend = 
 int pass_solve(crava_gpu_ctx *c, const crava_gpu_grids *gr, int precision, bool gated_done = false);
 // Whether the unit's forward z passes can take over the band-gated bins of
 // the solve (FP64 and mixed forms, z passes that have the rule, the plane
-// order built); if so fills zp[6] (cov grids in unit order) and makes sure
-// the non-finite flags exist.
+// order built, the flags allocated with the context); if so fills zp[6]
+// (cov grids in unit order).  Allocates nothing.
 int gated_prior_setup(crava_gpu_ctx *c, int precision, ZPrior zp[6], bool *on);
 // After the forward passes that took zp: the flagged bins into the counters.
 int gated_prior_count(crava_gpu_ctx *c);
