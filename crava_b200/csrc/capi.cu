@@ -177,7 +177,12 @@ int gated_prior_setup(crava_gpu_ctx *c, int precision, ZPrior zp[6], bool *on) {
     zp[t] = ZPrior{};
     zp[t].inv = c->tables.inv;
     zp[t].v = c->consts.var0[t];  // (0,0) (1,1) (2,2) (0,1) (0,2) (1,2): the cov grid order
-    zp[t].mode = precision == CRAVA_SOLVE_FP64 ? 1 : 2;
+    // FP64 form: sign(S0) |c| equals the rounded double rule while |S0|
+    // keeps c / S0 and its product with S0 normal (fft.cuh); else the
+    // double expression for every value
+    const double av = fabs(zp[t].v);
+    const bool exact = av == 0.0 || (av >= 1e-200 && av <= 1e200);
+    zp[t].mode = precision == CRAVA_SOLVE_FP64 ? (exact ? 1 : 3) : 2;
     zp[t].nf_bits = c->gated_nf;
     zp[t].nf_any = c->gated_nf + c->gated_nf_words;
   }

@@ -87,14 +87,19 @@ int fft_cols_y(const FftPlans &p, float2 *grid, int dir, cudaStream_t s);
 // alone and never reads or writes the band-gated bins.  mode 1: the FP64
 // form's rule (the double expression rounded to float; for a finite c it
 // equals sign(S0) |Re c| exactly, as the double error is far below half a
-// float ulp); mode 2: the mixed form's float operations.  A bin whose
+// float ulp, which needs c / S0 and its product with S0 to stay normal
+// doubles: for any float c that holds for 1e-200 <= |S0| <= 1e200, and the
+// host chooses mode 3, the double expression for every value, outside
+// that range); mode 2: the mixed form's float operations.  A bin whose
 // output is not finite sets its bit in nf_bits (and nf_any), so that the
 // bins are counted once however many of the six grids hold a non-finite
 // value (crava_gpu_stats.nonfinite_bins counts bins).
 struct ZPrior {
   const int *inv = nullptr;     // [nzp] band flags; null: no epilogue
   double v = 0.0;               // this grid's Sigma0 entry
-  int mode = 0;                 // 1 FP64 form, 2 mixed form
+  // 1 FP64 form, |v| in [1e-200, 1e200] (or 0): sign(v) |c| for a finite c;
+  // 3 FP64 form, other v: the double expression always; 2 mixed form
+  int mode = 0;
   unsigned *nf_bits = nullptr;  // one bit per bin of the grid
   unsigned *nf_any = nullptr;
 };
@@ -112,7 +117,9 @@ static __device__ __noinline__ void zprior_flag(unsigned *bits, unsigned *any, l
 
 __device__ __forceinline__ float2 zprior_apply(const ZPrior &z, float2 x, long long bin) {
   float r;
-  if (z.mode == 1) {
+  if (z.mode == 3) {
+    r = zprior_fp64_nonfinite(z.v, x.x);
+  } else if (z.mode == 1) {
     if (isfinite(x.x)) {
       const float a = fabsf(x.x);
       r = z.v != 0.0 ? (z.v < 0.0 ? -a : a) : a;
