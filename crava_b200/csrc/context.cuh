@@ -25,7 +25,7 @@ struct crava_gpu_ctx {
   bool timed = false;               // events of the last call are valid
   // fused unit (plane kernels + z/solve kernel) and its workspace
   crava::UnitPlan uplan{};
-  bool fused = false;  // the three-pass path is faster today; set_fused(1) selects the fused kernels
+  bool fused = false;  // the pass-by-pass path is faster; set_fused(1) selects the fused unit kernels
   float2 *W = nullptr;  // (10 + ntheta) grids in the column-pair layout
   // per-kernel profiling (events around each launch when enabled)
   bool prof = false;
