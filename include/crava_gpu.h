@@ -219,7 +219,9 @@ int crava_gpu_kz_tables(crava_gpu_ctx *ctx, float *wd, float *e1, float *e2,
 
 /* Replaces the per-kz tables with caller-supplied ones (same layout as
  * crava_gpu_kz_tables), e.g. spectra computed by the reference's own FFTW
- * (src/crava.cpp:952-976, 1024-1058).  Host pointers; synchronous. */
+ * (src/crava.cpp:952-976, 1024-1058).  Host pointers; synchronous.  The
+ * number of inverted planes sets the solve's launch shape, so a batch
+ * graph captured on this context before the call must be created again. */
 int crava_gpu_set_kz_tables(crava_gpu_ctx *ctx, const float *wd, const float *e1,
                             const float *e2, const float *e3, const int *inv);
 
